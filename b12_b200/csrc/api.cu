@@ -1,0 +1,825 @@
+// Host side of libb12g: the tree object that owns device memory and a stream, and
+// the C ABI declared in include/b12g.h.  Each entry point restates the reference
+// member function named in the header on top of the device kernels.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "csr.h"
+#include "kernels.h"
+#include "tree.h"
+
+using namespace b12g;
+using namespace b12g::host;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+uint64_t ipow(uint64_t b, uint32_t e)
+{
+  uint64_t r = 1;
+  while (e--) r *= b;
+  return r;
+}
+
+
+}  // namespace
+
+namespace b12g {
+namespace host {
+
+b12g_status fail(b12g_status s, const char* fmt, ...)
+{
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return s;
+}
+
+b12g_status cuda_fail(cudaError_t e, const char* where)
+{
+  return fail(e == cudaErrorMemoryAllocation ? B12G_ERR_OOM : B12G_ERR_CUDA, "%s: %s", where, cudaGetErrorString(e));
+}
+
+b12g_status sync(b12g_tree* t, const char* where)
+{
+  cudaError_t e = cudaStreamSynchronize(t->stream);
+  if (e != cudaSuccess) return cuda_fail(e, where);
+  return B12G_OK;
+}
+
+b12g_status read_ctr(b12g_tree* t, int first, int count)
+{
+  CK(cudaMemcpyAsync(t->h_ctr + first, t->ctr.p + first, count * sizeof(uint32_t), cudaMemcpyDeviceToHost, t->stream));
+  return sync(t, "read counters");
+}
+
+b12g_status set_ctr(b12g_tree* t, int slot, uint32_t v)
+{
+  t->h_ctr[slot] = v;
+  CK(cudaMemcpyAsync(t->ctr.p + slot, t->h_ctr + slot, sizeof(uint32_t), cudaMemcpyHostToDevice, t->stream));
+  return B12G_OK;
+}
+
+b12g_status reserve(b12g_tree* t, uint64_t n_boxes)
+{
+  if (n_boxes > 0xFFFFFFF0ull) return fail(B12G_ERR_CAPACITY, "at most 2^32-16 boxes per tree");
+  const size_t keep = t->n;
+  for (int b = 0; b < 2; ++b) {
+    ST(t->code[b].grow_keep(n_boxes, b == t->cur ? keep : 0, t->stream, "leaf codes"));
+    ST(t->flags[b].grow_keep(n_boxes, b == t->cur ? keep : 0, t->stream, "leaf flags"));
+  }
+  if (t->hit.n < n_boxes) {
+    ST(t->hit.ensure(n_boxes, "hit mask"));
+    CK(cudaMemsetAsync(t->hit.p, 0, t->hit.n, t->stream));
+  }
+  // tiles cover the largest array a compaction or scan can run over
+  const size_t most = std::max({size_t(n_boxes), t->hit.n, t->code[0].n, t->code[1].n}) + 1;
+  ST(t->tiles_a.ensure(compact_tiles(most) + 2, "tile counts"));
+  ST(t->tiles_b.ensure(compact_tiles(most) + 2, "tile offsets"));
+  return B12G_OK;
+}
+
+b12g_status prepare(b12g_tree* t, const b12g_scheme* sc, Prepared& pr)
+{
+  if (!sc) return fail(B12G_ERR_INVALID, "scheme is NULL");
+  const b12g_map& m = sc->map;
+  const b12g_grid& g = sc->grid;
+  const uint32_t D = t->domain.dim;
+  if (!image_supported(m.kind, m.arith, g.kind, D))
+    return fail(B12G_ERR_INVALID, "unsupported map/arith/grid/dimension combination (%u,%u,%u,%u)", m.kind, m.arith,
+                g.kind, D);
+  ImageArgs& a = pr.a;
+  a.dom = t->dom;
+  MapParams& mp = a.map;
+  mp.h = m.h;
+  mp.h2 = m.h / 2.0;
+  mp.h3 = m.h / 3.0;
+  mp.h6 = m.h / 6.0;
+  for (int i = 0; i < 6; ++i) mp.p[i] = m.p[i];
+  mp.steps = m.steps;
+  mp.table = nullptr;
+  if (m.kind == B12G_MAP_FORCED_DUFFING) {
+    // cos at the stage times t = j * h / 2 (period = steps * h)
+    std::vector<double> tab(2 * size_t(m.steps) + 1);
+    const double period = m.h * double(m.steps);
+    for (size_t j = 0; j < tab.size(); ++j) tab[j] = std::cos(double(j) * (period / double(2 * m.steps)));
+    ST(t->table.ensure(tab.size(), "forcing table"));
+    CK(cudaMemcpyAsync(t->table.p, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, t->stream));
+    CK(cudaStreamSynchronize(t->stream));
+    mp.table = t->table.p;
+  }
+  GridParams& gp = a.grid;
+  if (g.kind == B12G_GRID_INNER || g.kind == B12G_GRID_FULL) {
+    if (g.n < 1 || g.n > 64) return fail(B12G_ERR_INVALID, "grid points per dimension must be 1..64");
+    if (g.kind == B12G_GRID_FULL && g.n < 2) return fail(B12G_ERR_INVALID, "full grid needs n >= 2");
+    gp.n = g.n;
+    pr.P = ipow(g.n, D);
+    const double nn = double(g.n);
+    for (uint32_t d = 0; d < 64; ++d) {
+      if (g.kind == B12G_GRID_INNER) gp.coord[d] = ((double(d) * 2.0 + 1.0) - nn) / nn;   // Grids.hpp:113-116
+      else gp.coord[d] = (double(d) * 2.0) / double(uint64_t(g.n) - 1) - 1.0;           // Grids.hpp:75-78
+    }
+    gp.eps1 = 1.0 + g.eps;
+  } else {
+    if (g.points < 1) return fail(B12G_ERR_INVALID, "philox grid needs points >= 1");
+    gp.n = 1;
+    pr.P = g.points;
+    for (double& c : gp.coord) c = 0.0;
+  }
+  gp.points = pr.P;
+  gp.seed = g.seed;
+  a.points = pr.P;
+  a.codes = t->codes();
+  a.n_leaves = t->dn();
+  a.depth = t->depth;
+  a.children = 0;
+  a.src = nullptr;
+  a.n_src = nullptr;
+  a.hit = t->hit.p;
+  a.hit_cap = uint32_t(std::min<size_t>(t->hit.n, 0xFFFFFFFFu));
+  a.error = t->ctr.p + C_ERROR;
+  a.cand_count = t->ctr.p + C_CAND;
+  return B12G_OK;
+}
+
+b12g_status check_depth(b12g_tree* t, uint8_t depth)
+{
+  if (depth == B12G_LEAF_DEPTH || depth == t->depth) return B12G_OK;
+  return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "depth %u is neither the leaf depth (%u) nor 255", depth, t->depth);
+}
+
+// source boxes of a scheme: all leaves, or the leaves with all flags_to_check set
+b12g_status select_sources(b12g_tree* t, const b12g_scheme* sc, Prepared& pr, uint32_t& n_src)
+{
+  if (sc->depth != B12G_LEAF_DEPTH && sc->depth != t->depth)
+    return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "scheme depth %u is not the leaf depth %u", sc->depth, t->depth);
+  if (sc->flags_to_check == 0) {
+    n_src = t->n;
+    return B12G_OK;
+  }
+  ST(t->src.ensure(std::max<uint32_t>(t->n, 1), "source list"));
+  CompactArgs ca{};
+  ca.code = t->codes();
+  ca.flags = t->flg();
+  ca.n = t->dn();
+  ca.keep_flags = sc->flags_to_check;
+  ca.out_index = t->src.p;
+  ca.n_out = t->ctr.p + C_NSRC;
+  ca.out_cap = uint32_t(t->src.n);
+  ca.error = t->ctr.p + C_ERROR;
+  CK(compact(ca, {t->tiles_a.p, t->tiles_b.p}, t->n, t->stream));
+  count_launches(3);
+  ST(read_ctr(t, C_NSRC, 1));
+  n_src = t->h_ctr[C_NSRC];
+  pr.a.src = t->src.p;
+  pr.a.n_src = t->ctr.p + C_NSRC;
+  return B12G_OK;
+}
+
+b12g_status check_error(b12g_tree* t, const char* where)
+{
+  ST(read_ctr(t, C_ERROR, 1));
+  if (t->h_ctr[C_ERROR]) {
+    const uint32_t e = t->h_ctr[C_ERROR];
+    set_ctr(t, C_ERROR, 0);
+    if (e & 2u) return fail(B12G_ERR_TIMEOUT, "%s: a bounded device wait gave up", where);
+    return fail(B12G_ERR_CAPACITY, "%s: device buffer capacity exceeded", where);
+  }
+  return B12G_OK;
+}
+
+// make the tree the single surrounding box (insertSurroundingBoxIfEmpty)
+b12g_status set_root(b12g_tree* t, uint8_t flags)
+{
+  const uint64_t zero = 0;
+  CK(cudaMemcpyAsync(t->codes(), &zero, 8, cudaMemcpyHostToDevice, t->stream));
+  CK(cudaMemsetAsync(t->flg(), flags, 1, t->stream));
+  t->n = 1;
+  t->depth = 0;
+  ST(set_ctr(t, t->ncur, 1));
+  return sync(t, "set root");
+}
+
+b12g_status flag_call(b12g_tree* t, int op, uint8_t u, uint8_t f, uint8_t depth, uint32_t* n_changed)
+{
+  if (!t) return fail(B12G_ERR_INVALID, "NULL tree");
+  if (depth != 0) ST(check_depth(t, depth));
+  ST(set_ctr(t, C_CHANGED, 0));
+  CK(flag_op(t->flg(), t->dn(), op, u, f, t->ctr.p + C_CHANGED, t->n, t->stream));
+  count_launches(1);
+  ST(read_ctr(t, C_CHANGED, 1));
+  uint32_t c = t->h_ctr[C_CHANGED];
+  if (depth == 0 && t->depth != 0) {
+    // depth 0 is the surrounding box, whose flags combine its leaves' flags
+    // (countIfFlags depth-0 branch, ImplicitBoxTree.hpp:1119-1127): one box, changed
+    // if the combination matched before the update.  The combination is recomputed
+    // from the per-leaf counts: AND-combination for set/change, OR for unset.
+    if (op == 0) c = c > 0 ? 1u : 0u;            // not all leaves had f  <=> AND lacks f
+    else if (op == 1) c = c > 0 ? 1u : 0u;       // some leaf had any of f <=> OR has one
+    else c = (c == t->n) ? 1u : 0u;              // all leaves had u      <=> AND has u
+  }
+  if (n_changed) *n_changed = c;
+  return B12G_OK;
+}
+
+void prof_mark(b12g_tree* t, int kind)
+{
+  if (!t->profile) return;
+  auto& v = t->prof_events[kind];
+  if (t->prof_used[kind] == v.size()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    v.push_back(e);
+  }
+  cudaEventRecord(v[t->prof_used[kind]++], t->stream);
+}
+
+static void sum_pairs(const std::vector<cudaEvent_t>& v, size_t used, double& ms, uint64_t& launches)
+{
+  for (size_t i = 0; i + 1 < used; i += 2) {
+    float x = 0.f;
+    if (cudaEventElapsedTime(&x, v[i], v[i + 1]) == cudaSuccess) { ms += x; ++launches; }
+  }
+  cudaGetLastError();
+}
+
+// after a stream sync: fold recorded event pairs into the per-kind totals
+b12g_status prof_collect(b12g_tree* t)
+{
+  if (!t->profile) return B12G_OK;
+  for (int k = 0; k < 2; ++k) {
+    sum_pairs(t->prof_events[k], t->prof_used[k], t->prof_ms[k], t->prof_launches[k]);
+    t->prof_used[k] = 0;
+  }
+  return B12G_OK;
+}
+
+}  // namespace host
+}  // namespace b12g
+
+// =====================================================================================
+extern "C" {
+
+const char* b12g_last_error(void) { return g_last_error.c_str(); }
+
+const char* b12g_version(void) { return "b12g 0.1 (sm_100a)"; }
+
+b12g_status b12g_tree_create(const b12g_domain* domain, b12g_tree** out)
+{
+  if (!domain || !out) return fail(B12G_ERR_INVALID, "NULL argument");
+  if (domain->dim < 1 || domain->dim > B12G_MAX_DIM) return fail(B12G_ERR_INVALID, "dim must be 1..4");
+  for (uint32_t j = 0; j < domain->dim; ++j)
+    if (!(domain->radius[j] > 0.0)) return fail(B12G_ERR_INVALID, "radius must be positive");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(B12G_ERR_NO_DEVICE, "no CUDA device");
+  }
+  b12g_tree* t = new b12g_tree();
+  cudaGetDevice(&t->device);
+  t->domain = *domain;
+  for (uint32_t j = 0; j < B12G_MAX_DIM; ++j) {
+    const double c = j < domain->dim ? domain->center[j] : 0.0, r = j < domain->dim ? domain->radius[j] : 1.0;
+    t->dom.c[j] = c;
+    t->dom.r[j] = r;
+    t->dom.lo[j] = c - r;
+    t->dom.hi[j] = c + r;
+  }
+  b12g_status st = B12G_OK;
+  if (cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking) != cudaSuccess) st = cuda_fail(cudaGetLastError(), "stream");
+  if (st == B12G_OK && cudaMallocHost(&t->h_ctr, C_COUNT * sizeof(uint32_t)) != cudaSuccess)
+    st = cuda_fail(cudaGetLastError(), "pinned counters");
+  if (st == B12G_OK) st = t->ctr.ensure(C_COUNT, "counters");
+  if (st == B12G_OK && cudaMemsetAsync(t->ctr.p, 0, C_COUNT * sizeof(uint32_t), t->stream) != cudaSuccess)
+    st = cuda_fail(cudaGetLastError(), "memset");
+  if (st == B12G_OK) st = reserve(t, 1024);
+  if (st == B12G_OK) st = set_root(t, B12G_NONE);
+  if (st != B12G_OK) {
+    b12g_tree_destroy(t);
+    return st;
+  }
+  *out = t;
+  return B12G_OK;
+}
+
+b12g_status b12g_tree_destroy(b12g_tree* t)
+{
+  if (!t) return B12G_OK;
+  if (t->stream) cudaStreamSynchronize(t->stream);
+  if (t->sub_graph) cudaGraphExecDestroy(t->sub_graph);
+  for (int k = 0; k < 2; ++k) {
+    for (cudaEvent_t e : t->prof_events[k]) cudaEventDestroy(e);
+    for (cudaEvent_t e : t->graph_prof[k]) cudaEventDestroy(e);
+  }
+  for (int b = 0; b < 2; ++b) { t->code[b].release(); t->flags[b].release(); }
+  t->hit.release(); t->ctr.release(); t->tiles_a.release(); t->tiles_b.release();
+  t->src.release(); t->out.release(); t->stage_col.release(); t->stage_cnt.release();
+  t->row_count.release(); t->rowptr.release(); t->cand.release(); t->cand2.release();
+  t->sort_idx.release(); t->table.release(); t->step_counts.release(); t->sort_tmp.release();
+  if (t->h_ctr) cudaFreeHost(t->h_ctr);
+  if (t->stream) cudaStreamDestroy(t->stream);
+  delete t;
+  return B12G_OK;
+}
+
+b12g_status b12g_tree_reserve(b12g_tree* t, uint64_t n_boxes)
+{
+  if (!t) return fail(B12G_ERR_INVALID, "NULL tree");
+  ST(reserve(t, n_boxes));
+  return sync(t, "reserve");
+}
+
+b12g_status b12g_count(b12g_tree* t, uint8_t depth, uint32_t* count)
+{
+  if (!t || !count) return fail(B12G_ERR_INVALID, "NULL argument");
+  // count(depth) (ImplicitBoxTree.hpp:1061-1095) for a uniform-depth tree
+  if (depth == 0) *count = 1;
+  else if (depth == B12G_LEAF_DEPTH || depth == t->depth) *count = t->n;
+  else if (depth > t->depth) *count = 0;
+  else return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "count of inner depth %u", depth);
+  return B12G_OK;
+}
+
+b12g_status b12g_depth(b12g_tree* t, uint8_t* depth)
+{
+  if (!t || !depth) return fail(B12G_ERR_INVALID, "NULL argument");
+  *depth = t->depth;
+  return B12G_OK;
+}
+
+b12g_status b12g_leaves(b12g_tree* t, uint64_t* codes, uint8_t* depths, uint8_t* flags)
+{
+  if (!t) return fail(B12G_ERR_INVALID, "NULL tree");
+  if (codes) CK(cudaMemcpyAsync(codes, t->codes(), size_t(t->n) * 8, cudaMemcpyDeviceToHost, t->stream));
+  if (flags) CK(cudaMemcpyAsync(flags, t->flg(), t->n, cudaMemcpyDeviceToHost, t->stream));
+  ST(sync(t, "leaves"));
+  if (depths) std::memset(depths, t->depth, t->n);
+  return B12G_OK;
+}
+
+b12g_status b12g_load_leaves(b12g_tree* t, const uint64_t* codes, const uint8_t* depths, const uint8_t* flags,
+                             uint32_t n)
+{
+  if (!t || !codes || !depths || !flags) return fail(B12G_ERR_INVALID, "NULL argument");
+  if (n == 0) return set_root(t, B12G_NONE);
+  const uint8_t d = depths[0];
+  if (d > 64) return fail(B12G_ERR_INVALID, "depth %u above the maximal depth 64", d);
+  for (uint32_t i = 0; i < n; ++i) {
+    if (depths[i] != d) return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "leaves of mixed depth");
+    if (d < 64 && (codes[i] >> d) != 0) return fail(B12G_ERR_INVALID, "code %u has bits above its depth", i);
+    if (i && codes[i] <= codes[i - 1]) return fail(B12G_ERR_INVALID, "codes must be sorted and unique");
+  }
+  ST(reserve(t, n));
+  CK(cudaMemcpyAsync(t->codes(), codes, size_t(n) * 8, cudaMemcpyHostToDevice, t->stream));
+  CK(cudaMemcpyAsync(t->flg(), flags, n, cudaMemcpyHostToDevice, t->stream));
+  t->n = n;
+  t->depth = d;
+  ST(set_ctr(t, t->ncur, n));
+  return sync(t, "load leaves");
+}
+
+// ---- flags ----
+b12g_status b12g_set_flags(b12g_tree* t, uint8_t flags, uint8_t depth, uint32_t* n_changed)
+{
+  return flag_call(t, 0, 0, flags, depth, n_changed);
+}
+
+b12g_status b12g_unset_flags(b12g_tree* t, uint8_t flags, uint8_t depth, uint32_t* n_changed)
+{
+  return flag_call(t, 1, 0, flags, depth, n_changed);
+}
+
+b12g_status b12g_change_flags(b12g_tree* t, uint8_t to_unset, uint8_t to_set, uint8_t depth, uint32_t* n_changed)
+{
+  return flag_call(t, 2, to_unset, to_set, depth, n_changed);
+}
+
+// ---- structure ------------------------------------------------------------------------
+b12g_status b12g_subdivide(b12g_tree* t, uint8_t flags, uint32_t* n_subdivided)
+{
+  if (!t) return fail(B12G_ERR_INVALID, "NULL tree");
+  // IsSubdividableFunctor (Functors.hpp:332-335): all flags set and depth < 64
+  uint32_t m = 0;
+  if (t->depth < 64) {
+    ST(set_ctr(t, C_TMP, 0));
+    CK(count_flags(t->flg(), t->dn(), flags, t->ctr.p + C_TMP, t->n, t->stream));
+    count_launches(1);
+    ST(read_ctr(t, C_TMP, 1));
+    m = t->h_ctr[C_TMP];
+  }
+  if (m != 0 && m != t->n)
+    return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "subdividing %u of %u leaves would mix depths", m, t->n);
+  if (m == t->n) {
+    ST(reserve(t, 2ull * t->n));
+    const int o = 1 - t->cur, no = 1 - t->ncur;
+    CK(split_codes(t->codes(), t->flg(), t->dn(), t->code[o].p, t->flags[o].p, t->ctr.p + no, t->n, t->stream));
+    count_launches(1);
+    ST(sync(t, "subdivide"));
+    t->cur = o;
+    t->ncur = no;
+    t->n *= 2;
+    t->depth += 1;
+  }
+  if (n_subdivided) *n_subdivided = m;
+  return B12G_OK;
+}
+
+b12g_status b12g_remove(b12g_tree* t, uint8_t flags, uint32_t* n_removed)
+{
+  if (!t) return fail(B12G_ERR_INVALID, "NULL tree");
+  const int o = 1 - t->cur, no = 1 - t->ncur;
+  CompactArgs ca{};
+  ca.code = t->codes();
+  ca.flags = t->flg();
+  ca.n = t->dn();
+  ca.keep_flags = flags;
+  ca.out_code = t->code[o].p;
+  ca.out_flags = t->flags[o].p;
+  ca.n_out = t->ctr.p + no;
+  ca.out_cap = uint32_t(std::min<size_t>(t->code[o].n, t->flags[o].n));
+  ca.error = t->ctr.p + C_ERROR;
+  CK(compact(ca, {t->tiles_a.p, t->tiles_b.p}, t->n, t->stream));
+  count_launches(3);
+  ST(read_ctr(t, no, 1));
+  ST(check_error(t, "remove"));
+  const uint32_t kept = t->h_ctr[no];
+  const uint32_t removed = t->n - kept;
+  t->cur = o;
+  t->ncur = no;
+  t->n = kept;
+  if (kept == 0) ST(set_root(t, B12G_NONE));  // insertSurroundingBoxIfEmpty
+  if (n_removed) *n_removed = removed;
+  return B12G_OK;
+}
+
+b12g_status b12g_delete_depth(b12g_tree* t, uint8_t depth, uint32_t* n_deleted)
+{
+  if (!t) return fail(B12G_ERR_INVALID, "NULL tree");
+  uint32_t c = 0;
+  if (depth == 0) {
+    ST(set_root(t, B12G_NONE));
+    c = 1;
+  } else if (depth == B12G_LEAF_DEPTH || depth > t->depth) {
+    c = 0;
+  } else {
+    return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "deleteDepth(%u) of a depth-%u tree", depth, t->depth);
+  }
+  if (n_deleted) *n_deleted = c;
+  return B12G_OK;
+}
+
+// ---- box images -------------------------------------------------------------------------
+b12g_status b12g_set_flags_by_image(b12g_tree* t, const b12g_scheme* sc, uint8_t flags, uint8_t depth,
+                                    uint32_t* n_changed)
+{
+  if (!t) return fail(B12G_ERR_INVALID, "NULL tree");
+  ST(check_depth(t, depth));
+  Prepared pr;
+  ST(prepare(t, sc, pr));
+  uint32_t n_src = 0;
+  ST(select_sources(t, sc, pr, n_src));
+  ST(set_ctr(t, C_CHANGED, 0));
+  pr.a.hit_cap = uint32_t(std::min<size_t>(t->hit.n, 0xFFFFFFFFu));
+  prof_mark(t, 0);
+  CK(launch_image(sc->map.kind, sc->map.arith, sc->grid.kind, t->domain.dim, ImageMode::Hit, pr.a,
+                  uint64_t(n_src) * pr.P, t->stream));
+  prof_mark(t, 0);
+  CK(apply_hits(t->flg(), t->hit.p, t->dn(), flags, t->ctr.p + C_CHANGED, t->n, t->stream));
+  count_launches(2);
+  ST(read_ctr(t, C_CHANGED, 1));
+  ST(prof_collect(t));
+  ST(check_error(t, "set_flags_by_image"));
+  if (n_changed) *n_changed = t->h_ctr[C_CHANGED];
+  return B12G_OK;
+}
+
+b12g_status b12g_search_by_image(b12g_tree* t, const b12g_scheme* sc, uint8_t depth, uint32_t* out, uint64_t capacity,
+                                 uint64_t* n_points)
+{
+  if (!t) return fail(B12G_ERR_INVALID, "NULL tree");
+  ST(check_depth(t, depth));
+  Prepared pr;
+  ST(prepare(t, sc, pr));
+  uint32_t n_src = 0;
+  ST(select_sources(t, sc, pr, n_src));
+  const uint64_t np = uint64_t(n_src) * pr.P;
+  if (n_points) *n_points = np;
+  if (!out) return B12G_OK;
+  if (capacity < np) return fail(B12G_ERR_CAPACITY, "output holds %llu of %llu points", (unsigned long long)capacity,
+                                 (unsigned long long)np);
+  ST(t->out.ensure(std::max<uint64_t>(np, 1), "search output"));
+  pr.a.out = t->out.p;
+  CK(launch_image(sc->map.kind, sc->map.arith, sc->grid.kind, t->domain.dim, ImageMode::Search, pr.a, np, t->stream));
+  count_launches(1);
+  CK(cudaMemcpyAsync(out, t->out.p, np * 4, cudaMemcpyDeviceToHost, t->stream));
+  return sync(t, "search_by_image");
+}
+
+// ---- transition matrix -----------------------------------------------------------------
+b12g_status b12g_transition_matrix(b12g_tree* t, const b12g_scheme* sc, int absolute, int invalid_column,
+                                   b12g_csr** out)
+{
+  if (!t || !out) return fail(B12G_ERR_INVALID, "NULL argument");
+  Prepared pr;
+  ST(prepare(t, sc, pr));
+  if (pr.P > kMaxRowPoints) return fail(B12G_ERR_CAPACITY, "transition rows support up to %u points per box",
+                                        kMaxRowPoints);
+  if (sc->flags_to_check != 0 || (sc->depth != B12G_LEAF_DEPTH && sc->depth != t->depth))
+    return fail(B12G_ERR_INVALID, "transitionMatrixForLeaves maps every leaf");
+  const uint32_t n = t->n;
+  const uint64_t stage = uint64_t(n) * pr.P;
+  ST(t->stage_col.ensure(stage, "row staging"));
+  ST(t->stage_cnt.ensure(stage, "row staging"));
+  ST(t->row_count.ensure(n + 1, "row counts"));
+  ST(t->rowptr.ensure(n + 1, "row pointers"));
+  RowArgs ra{};
+  ra.img = pr.a;
+  ra.stage_col = t->stage_col.p;
+  ra.stage_cnt = t->stage_cnt.p;
+  ra.row_count = t->row_count.p;
+  ra.keep_lost = invalid_column ? 1 : 0;
+  ra.lost_col = n + 1;  // ImplicitBoxTree.hpp:3075-3090: nColumns += 1, lost entries get index nColumns
+  prof_mark(t, 1);
+  CK(launch_rows(sc->map.kind, sc->map.arith, sc->grid.kind, t->domain.dim, ra, n, t->stream));
+  prof_mark(t, 1);
+  CK(exclusive_scan_u32(t->row_count.p, t->rowptr.p, t->dn(), t->tiles_a.p, n, t->stream));
+  CK(cudaMemcpyAsync(t->h_ctr + C_NNZ, t->rowptr.p + n, 4, cudaMemcpyDeviceToHost, t->stream));
+  count_launches(4);
+  ST(sync(t, "transition rows"));
+  ST(prof_collect(t));
+  const uint32_t nnz32 = t->h_ctr[C_NNZ];
+  // an existing matrix passed in *out is refilled in place (its buffers only grow)
+  const bool fresh = *out == nullptr;
+  b12g_csr* m = fresh ? new b12g_csr() : *out;
+  m->device = t->device;
+  m->n_rows = n;
+  m->n_cols = invalid_column ? n + 1 : n;
+  m->nnz = nnz32;
+  m->has_transpose = false;
+  b12g_status st = B12G_OK;
+  if (!m->stream && cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking) != cudaSuccess)
+    st = cuda_fail(cudaGetLastError(), "stream");
+  if (st == B12G_OK) st = m->rowptr.ensure(n + 1, "rowptr");
+  if (st == B12G_OK) st = m->cols.ensure(std::max<uint64_t>(m->nnz, 1), "cols");
+  if (st == B12G_OK) st = m->vals.ensure(std::max<uint64_t>(m->nnz, 1), "vals");
+  if (st == B12G_OK) st = m->ctr.ensure(16, "csr counters");
+  if (st == B12G_OK) {
+    cudaMemcpyAsync(m->rowptr.p, t->rowptr.p, size_t(n + 1) * 4, cudaMemcpyDeviceToDevice, t->stream);
+    gather_rows(t->stage_col.p, t->stage_cnt.p, uint32_t(pr.P), t->row_count.p, t->rowptr.p, t->dn(), m->cols.p,
+                m->vals.p, absolute, double(pr.P), n, t->stream);
+    count_launches(1);
+    st = sync(t, "gather rows");
+  }
+  if (st != B12G_OK) {
+    if (fresh) b12g_csr_destroy(m);
+    return st;
+  }
+  *out = m;
+  return B12G_OK;
+}
+
+b12g_status b12g_csr_shape(const b12g_csr* m, uint32_t* n_rows, uint32_t* n_cols, uint64_t* nnz)
+{
+  if (!m) return fail(B12G_ERR_INVALID, "NULL matrix");
+  if (n_rows) *n_rows = m->n_rows;
+  if (n_cols) *n_cols = m->n_cols;
+  if (nnz) *nnz = m->nnz;
+  return B12G_OK;
+}
+
+b12g_status b12g_csr_copy(const b12g_csr* m, uint32_t* rowptr, uint32_t* cols, double* vals)
+{
+  if (!m) return fail(B12G_ERR_INVALID, "NULL matrix");
+  if (rowptr) CK(cudaMemcpyAsync(rowptr, m->rowptr.p, size_t(m->n_rows + 1) * 4, cudaMemcpyDeviceToHost, m->stream));
+  if (cols && m->nnz) CK(cudaMemcpyAsync(cols, m->cols.p, m->nnz * 4, cudaMemcpyDeviceToHost, m->stream));
+  if (vals && m->nnz) CK(cudaMemcpyAsync(vals, m->vals.p, m->nnz * 8, cudaMemcpyDeviceToHost, m->stream));
+  CK(cudaStreamSynchronize(m->stream));
+  return B12G_OK;
+}
+
+b12g_status b12g_csr_destroy(b12g_csr* m)
+{
+  if (!m) return B12G_OK;
+  if (m->stream) cudaStreamSynchronize(m->stream);
+  m->rowptr.release(); m->cols.release(); m->vals.release(); m->tptr.release(); m->trows.release();
+  m->work.release(); m->tiles.release(); m->tvals.release(); m->w0.release(); m->w1.release();
+  m->partial.release(); m->vout.release(); m->ctr.release();
+  if (m->stream) cudaStreamDestroy(m->stream);
+  delete m;
+  return B12G_OK;
+}
+
+b12g_status b12g_invariant_measure(b12g_csr* m, uint32_t iters, double* v)
+{
+  if (!m) return fail(B12G_ERR_INVALID, "NULL matrix");
+  const uint32_t n = m->n_rows;
+  if (n == 0) return B12G_OK;
+  cudaStream_t s = m->stream;
+  if (!m->has_transpose) {
+    ST(m->tptr.ensure(n + 1, "transpose"));
+    ST(m->trows.ensure(std::max<uint64_t>(m->nnz, 1), "transpose"));
+    ST(m->tvals.ensure(std::max<uint64_t>(m->nnz, 1), "transpose"));
+    ST(m->work.ensure(n + 1, "transpose"));
+    ST(m->tiles.ensure(compact_tiles(n + 1) + 2, "transpose"));
+    uint32_t h[3] = {n, uint32_t(m->nnz), n};
+    CK(cudaMemcpyAsync(m->ctr.p, h, sizeof h, cudaMemcpyHostToDevice, s));
+    CK(transpose_csr(m->rowptr.p, m->cols.p, m->vals.p, m->ctr.p, m->ctr.p + 1, n, m->nnz, n, m->tptr.p,
+                     m->trows.p, m->tvals.p, m->work.p, m->tiles.p, m->ctr.p + 2, s));
+    CK(cudaStreamSynchronize(s));
+    count_launches(6);
+    m->has_transpose = true;
+  }
+  ST(m->w0.ensure(n, "measure"));
+  ST(m->w1.ensure(n, "measure"));
+  ST(m->vout.ensure(n, "measure"));
+  const int slots = measure_partial_slots();
+  ST(m->partial.ensure(slots, "measure"));
+  CK(invariant_measure(m->tptr.p, m->trows.p, m->tvals.p, n, iters, m->w0.p, m->w1.p, m->partial.p, uint32_t(slots),
+                       m->vout.p, m->ctr.p + 8, s));
+  count_launches(1);
+  if (v) CK(cudaMemcpyAsync(v, m->vout.p, size_t(n) * 8, cudaMemcpyDeviceToHost, s));
+  uint32_t err = 0;
+  CK(cudaMemcpyAsync(&err, m->ctr.p + 10, 4, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (err & 2u) return fail(B12G_ERR_TIMEOUT, "invariant measure: grid barrier gave up");
+  return B12G_OK;
+}
+
+b12g_status b12g_csr_measure(const b12g_csr* m, double* v)
+{
+  if (!m || !v) return fail(B12G_ERR_INVALID, "NULL argument");
+  if (m->vout.n < m->n_rows) return fail(B12G_ERR_INVALID, "no invariant measure computed yet");
+  CK(cudaMemcpyAsync(v, m->vout.p, size_t(m->n_rows) * 8, cudaMemcpyDeviceToHost, m->stream));
+  CK(cudaStreamSynchronize(m->stream));
+  return B12G_OK;
+}
+
+// ---- fused subdivision loop --------------------------------------------------------------
+b12g_status b12g_subdivision_run(b12g_tree* t, const b12g_scheme* sc, uint32_t steps, uint32_t* counts)
+{
+  if (!t || !sc) return fail(B12G_ERR_INVALID, "NULL argument");
+  if (steps == 0) return B12G_OK;
+  if (sc->flags_to_check != 0 || sc->depth != B12G_LEAF_DEPTH)
+    return fail(B12G_ERR_INVALID, "the subdivision loop maps every leaf (depth 255, no flag filter)");
+  if (int(t->depth) + int(steps) > 64) return fail(B12G_ERR_INVALID, "depth would exceed 64");
+  // setFlags(SD) on every leaf (subdivision.m:16, B12_doc.tex:266)
+  ST(flag_call(t, 0, 0, B12G_SD, B12G_LEAF_DEPTH, nullptr));
+
+  // keep the initial state so that a capacity overflow can be retried with more room
+  const uint32_t n0 = t->n;
+  const uint8_t d0 = t->depth;
+  std::vector<uint64_t> c0(n0);
+  std::vector<uint8_t> f0(n0);
+  CK(cudaMemcpyAsync(c0.data(), t->codes(), size_t(n0) * 8, cudaMemcpyDeviceToHost, t->stream));
+  CK(cudaMemcpyAsync(f0.data(), t->flg(), n0, cudaMemcpyDeviceToHost, t->stream));
+  ST(sync(t, "snapshot"));
+  ST(t->step_counts.ensure(steps + 1, "step counts"));
+
+  uint64_t cap = std::max<uint64_t>(t->code[0].n, std::max<uint64_t>(4ull * n0, 1ull << 16));
+  for (int attempt = 0; attempt < 12; ++attempt) {
+    ST(reserve(t, cap));
+    Prepared pr;
+    ST(prepare(t, sc, pr));
+    // key of the captured graph: every pointer and parameter the launches bake in
+    std::vector<uint8_t> key(sizeof(b12g_scheme) + 64);
+    std::memcpy(key.data(), sc, sizeof(b12g_scheme));
+    uint64_t extra[8] = {steps, cap, uint64_t(t->cur) | uint64_t(t->ncur) << 1 | uint64_t(t->profile) << 2, uint64_t(d0),
+                         uint64_t(uintptr_t(t->code[0].p)), uint64_t(uintptr_t(t->hit.p)), uint64_t(uintptr_t(t->table.p)),
+                         uint64_t(uintptr_t(t->code[1].p))};
+    std::memcpy(key.data() + sizeof(b12g_scheme), extra, sizeof extra);
+
+    if (!t->sub_graph || key != t->sub_key) {
+      if (t->sub_graph) { cudaGraphExecDestroy(t->sub_graph); t->sub_graph = nullptr; }
+      cudaGraph_t g = nullptr;
+      for (int k = 0; k < 2; ++k) {
+        for (cudaEvent_t e : t->graph_prof[k]) cudaEventDestroy(e);
+        t->graph_prof[k].clear();
+      }
+      t->prof_used[0] = t->prof_used[1] = 0;
+      CK(cudaStreamBeginCapture(t->stream, cudaStreamCaptureModeThreadLocal));
+      int cur = t->cur, ncur = t->ncur;
+      cudaError_t err = cudaSuccess;
+      for (uint32_t s = 0; s < steps && err == cudaSuccess; ++s) {
+        const int o = 1 - cur, no = 1 - ncur;
+        ImageArgs a = pr.a;
+        a.codes = t->code[cur].p;
+        a.n_leaves = t->ctr.p + ncur;
+        a.depth = int(d0) + int(s) + 1;
+        a.children = 1;
+        a.hit_cap = uint32_t(std::min<size_t>(t->hit.n, 0xFFFFFFFFu));
+        prof_mark(t, 0);
+        err = launch_image(sc->map.kind, sc->map.arith, sc->grid.kind, t->domain.dim, ImageMode::Hit, a,
+                           2ull * cap * pr.P, t->stream);
+        prof_mark(t, 0);
+        if (err != cudaSuccess) break;
+        CompactArgs ca{};
+        ca.code = t->code[cur].p;
+        ca.flags = t->flags[cur].p;
+        ca.n = t->ctr.p + ncur;
+        ca.hit = t->hit.p;
+        ca.children = 1;
+        ca.hit_cap = a.hit_cap;
+        ca.out_code = t->code[o].p;
+        ca.out_flags = t->flags[o].p;
+        ca.n_out = t->ctr.p + no;
+        ca.n_out2 = t->step_counts.p + s;
+        ca.out_cap = uint32_t(std::min<size_t>(t->code[o].n, 0xFFFFFFFFu));
+        ca.error = t->ctr.p + C_ERROR;
+        err = compact(ca, {t->tiles_a.p, t->tiles_b.p}, uint32_t(std::min<uint64_t>(cap, 0xFFFFFFFFu)), t->stream);
+        cur = o;
+        ncur = no;
+      }
+      cudaError_t e2 = cudaStreamEndCapture(t->stream, &g);
+      if (err != cudaSuccess) { if (g) cudaGraphDestroy(g); return cuda_fail(err, "capture subdivision"); }
+      if (e2 != cudaSuccess) return cuda_fail(e2, "end capture");
+      cudaError_t e3 = cudaGraphInstantiate(&t->sub_graph, g, 0);
+      cudaGraphDestroy(g);
+      if (e3 != cudaSuccess) { t->sub_graph = nullptr; return cuda_fail(e3, "instantiate"); }
+      t->sub_key = key;
+      t->sub_graph_kernels = 4ull * steps;
+      // the events recorded during capture belong to the graph from now on
+      for (int k = 0; k < 2; ++k) {
+        t->graph_prof[k].assign(t->prof_events[k].begin(), t->prof_events[k].begin() + t->prof_used[k]);
+        t->prof_events[k].erase(t->prof_events[k].begin(), t->prof_events[k].begin() + t->prof_used[k]);
+        t->prof_used[k] = 0;
+      }
+    }
+    CK(cudaGraphLaunch(t->sub_graph, t->stream));
+    count_launches(t->sub_graph_kernels);
+    std::vector<uint32_t> hc(steps);
+    CK(cudaMemcpyAsync(hc.data(), t->step_counts.p, steps * 4, cudaMemcpyDeviceToHost, t->stream));
+    CK(cudaMemcpyAsync(t->h_ctr + C_ERROR, t->ctr.p + C_ERROR, 4, cudaMemcpyDeviceToHost, t->stream));
+    ST(sync(t, "subdivision run"));
+    if (t->profile)
+      for (int k = 0; k < 2; ++k)
+        sum_pairs(t->graph_prof[k], t->graph_prof[k].size(), t->prof_ms[k], t->prof_launches[k]);
+    if (t->h_ctr[C_ERROR] & 1u) {
+      // capacity exceeded: restore the initial leaves and retry with 4x the room
+      ST(set_ctr(t, C_ERROR, 0));
+      cap *= 4;
+      ST(reserve(t, cap));
+      CK(cudaMemsetAsync(t->hit.p, 0, t->hit.n, t->stream));
+      CK(cudaMemcpyAsync(t->codes(), c0.data(), size_t(n0) * 8, cudaMemcpyHostToDevice, t->stream));
+      CK(cudaMemcpyAsync(t->flg(), f0.data(), n0, cudaMemcpyHostToDevice, t->stream));
+      ST(set_ctr(t, t->ncur, n0));
+      ST(sync(t, "restore"));
+      t->n = n0;
+      t->depth = d0;
+      continue;
+    }
+    // steps alternate the buffers: after an odd number of steps the other one is current
+    if (steps & 1u) { t->cur = 1 - t->cur; t->ncur = 1 - t->ncur; }
+    uint32_t final_n = hc[steps - 1];
+    uint32_t done = steps;
+    for (uint32_t s = 0; s < steps; ++s)
+      if (hc[s] == 0) { done = s; break; }
+    if (done < steps) {
+      // a step removed every box: the reference re-inserts the surrounding box, which
+      // has no SD flag and so stays the only leaf
+      for (uint32_t s = done; s < steps; ++s) hc[s] = 1;
+      ST(set_root(t, B12G_NONE));
+      final_n = 1;
+    } else {
+      t->n = final_n;
+      t->depth = uint8_t(d0 + steps);
+    }
+    if (counts) std::memcpy(counts, hc.data(), steps * 4);
+    return B12G_OK;
+  }
+  return fail(B12G_ERR_CAPACITY, "subdivision run: capacity retries exhausted");
+}
+
+// ---- measurement hooks --------------------------------------------------------------------
+b12g_status b12g_tree_stream(b12g_tree* t, void** stream)
+{
+  if (!t || !stream) return fail(B12G_ERR_INVALID, "NULL argument");
+  *stream = (void*)t->stream;
+  return B12G_OK;
+}
+
+b12g_status b12g_profile_enable(b12g_tree* t, int enable)
+{
+  if (!t) return fail(B12G_ERR_INVALID, "NULL tree");
+  t->profile = enable != 0;
+  return B12G_OK;
+}
+
+b12g_status b12g_profile_read(b12g_tree* t, uint32_t kind, double* ms_total, uint64_t* launches, int reset)
+{
+  if (!t || kind > 1) return fail(B12G_ERR_INVALID, "bad argument");
+  if (ms_total) *ms_total = t->prof_ms[kind];
+  if (launches) *launches = t->prof_launches[kind];
+  if (reset) { t->prof_ms[kind] = 0.0; t->prof_launches[kind] = 0; }
+  return B12G_OK;
+}
+
+}  // extern "C"

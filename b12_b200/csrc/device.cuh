@@ -1,0 +1,339 @@
+// Device building blocks of the box-image path: arithmetic policies, box geometry,
+// grids, maps and point location.  Everything here is FP64 and written with explicit
+// rounding intrinsics, so the generated code does not depend on contraction flags:
+//   strict  - __dmul_rn / __dadd_rn / __dsub_rn / __ddiv_rn, one rounding per op, the
+//             same values as the reference built with -fmad=false on both sides;
+//   fma     - __fma_rn where the map is written with explicit fused multiply-adds.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/b12g.h"
+
+namespace b12g {
+
+constexpr uint32_t kInvalidIndex = 0xFFFFFFFFu;
+constexpr uint64_t kInvalidCode = ~uint64_t(0);
+
+// ---------------------------------------------------------------------------------
+// arithmetic policies
+// ---------------------------------------------------------------------------------
+struct Strict {
+  static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+  static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+  static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+  // a*b + c with two roundings
+  static __device__ __forceinline__ double madd(double a, double b, double c) { return __dadd_rn(__dmul_rn(a, b), c); }
+};
+
+struct Fused {
+  static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+  static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+  static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+  static __device__ __forceinline__ double madd(double a, double b, double c) { return __fma_rn(a, b, c); }
+};
+
+// exact multiplication by 2^e for |e| <= 1000 (the ldexp of the reference's
+// coordinateFunctions.hpp for the normal range that box coordinates live in)
+__device__ __forceinline__ double pow2(int e) { return __longlong_as_double((long long)(1023 + e) << 52); }
+
+// ---------------------------------------------------------------------------------
+// job constants shared by every kernel of one tree + scheme
+// ---------------------------------------------------------------------------------
+struct Domain {
+  double c[B12G_MAX_DIM];
+  double r[B12G_MAX_DIM];
+  double lo[B12G_MAX_DIM];   // c - r, rounded as the reference does (isPointInBox)
+  double hi[B12G_MAX_DIM];   // c + r
+};
+
+struct MapParams {
+  double h, h2, h3, h6;      // step and h/2, h/3, h/6 (the reference divides at every use; same values)
+  double p[6];
+  uint32_t steps;
+  const double* table;       // forced Duffing cos table on the device
+};
+
+struct GridParams {
+  uint32_t n;                // points per dimension
+  uint64_t points;           // points per box
+  uint64_t seed;
+  double eps1;               // 1 + eps (full grid)
+  double coord[64];          // 1-D grid coordinates for index 0..n-1 (inner / full, before eps)
+};
+
+// ---------------------------------------------------------------------------------
+// box geometry (computeCoordinatesOfBoxFixedSdScheme, coordinateFunctions.hpp:130-159;
+// computeBoxFromPointFixedSdScheme, coordinateFunctions.hpp:63-93)
+// The depth-d code holds d bits; bit t counted from the top (t = 0 is the first
+// bisection) lies at position d-1-t and bisects dimension t mod D.
+// ---------------------------------------------------------------------------------
+template<int D>
+__device__ __forceinline__ int bisections(int depth, int j) { return depth / D + (j < depth % D ? 1 : 0); }
+
+// extract the k bits of dimension j from a depth-d code, first bisection = MSB
+template<int D>
+__device__ __forceinline__ uint32_t deinterleave(uint64_t code, int depth, int j)
+{
+  uint32_t bits = 0;
+  for (int t = j; t < depth; t += D) bits = (bits << 1) | uint32_t((code >> (depth - 1 - t)) & 1u);
+  return bits;
+}
+
+template<int D>
+__device__ __forceinline__ uint64_t interleave(const uint32_t (&bits)[D], const int (&k)[D], int depth)
+{
+  uint64_t code = 0;
+  const int rounds = (depth + D - 1) / D;
+#pragma unroll 1
+  for (int m = 0; m < rounds; ++m) {
+#pragma unroll
+    for (int j = 0; j < D; ++j)
+      if (m * D + j < depth) code = (code << 1) | uint64_t((bits[j] >> (k[j] - 1 - m)) & 1u);
+  }
+  return code;
+}
+
+// centre and radius of a box
+template<int D>
+__device__ __forceinline__ void box_coordinates(const Domain& dom, uint64_t code, int depth, double* c, double* r)
+{
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    const int k = bisections<D>(depth, j);
+    const uint32_t bits = deinterleave<D>(code, depth, j);
+    r[j] = dom.r[j] * pow2(-k);
+    const double t = __dsub_rn(__dmul_rn(double(bits) * pow2(-k), 2.0), 1.0);
+    c[j] = __dadd_rn(__dadd_rn(__dmul_rn(t, dom.r[j]), dom.c[j]), r[j]);
+  }
+}
+
+// depth-d code of the box that contains p; false if p lies outside the domain.
+// floor(u * 2^64bits) >> (64bits - k) == floor(u * 2^k) for u >= 0 and exact scaling,
+// so the code equals the reference's depth-64 code shifted to depth d, including the
+// u == 1.0 rounding case where the overflow bit is dropped.
+template<int D>
+__device__ __forceinline__ bool point_code(const Domain& dom, const double* p, int depth, uint64_t& code)
+{
+  bool inside = true;
+#pragma unroll
+  for (int j = 0; j < D; ++j) inside = inside && (dom.lo[j] <= p[j]) && (p[j] < dom.hi[j]);
+  if (!inside) return false;
+  uint32_t bits[D];
+  int k[D];
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    k[j] = bisections<D>(depth, j);
+    const double u = __dmul_rn(__dadd_rn(__ddiv_rn(__dsub_rn(p[j], dom.c[j]), dom.r[j]), 1.0), 0.5);
+    const double s = floor(u * pow2(k[j]));
+    bits[j] = uint32_t((unsigned long long)s & ((1ull << k[j]) - 1ull));
+  }
+  code = interleave<D>(bits, k, depth);
+  return true;
+}
+
+// ---------------------------------------------------------------------------------
+// point location among sorted leaf codes of one depth (searchByIterators leaf branch,
+// ImplicitBoxTree.hpp:2394-2432, with ComputeSearchIndexFunctor, Functors.hpp:289-315).
+// For a uniform-depth tree the reference returns the index of the leaf whose code
+// equals the point's depth-d code, else "invalid"; a point outside the domain is
+// matched to the last leaf exactly when that leaf's code is 0 (hasSamePath of the
+// invalid box with a zero code), which this reproduces.
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t locate(const uint64_t* __restrict__ codes, uint32_t n, bool valid, uint64_t code)
+{
+  if (n == 0) return kInvalidIndex;
+  if (!valid) return __ldg(codes + n - 1) == 0 ? n - 1 : kInvalidIndex;
+  uint32_t lo = 0, len = n;
+  while (len > 1) {
+    const uint32_t half = len >> 1;
+    const uint64_t v = __ldg(codes + lo + half);
+    lo = (v <= code) ? lo + half : lo;
+    len -= half;
+  }
+  return __ldg(codes + lo) == code ? lo : kInvalidIndex;
+}
+
+// ---------------------------------------------------------------------------------
+// grids (Grids.hpp)
+// ---------------------------------------------------------------------------------
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11)
+__device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1)
+{
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    if (r > 0) { k0 += 0x9E3779B9u; k1 += 0xBB67AE85u; }
+    const uint32_t lo0 = 0xD2511F53u * c[0], hi0 = __umulhi(0xD2511F53u, c[0]);
+    const uint32_t lo1 = 0xCD9E8D57u * c[2], hi1 = __umulhi(0xCD9E8D57u, c[2]);
+    const uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
+    c[0] = n0; c[1] = lo1; c[2] = n2; c[3] = lo0;
+  }
+}
+
+__device__ __forceinline__ double philox_signed(uint32_t hi, uint32_t lo)
+{
+  const unsigned long long m = ((unsigned long long)hi << 32 | lo) >> 11;
+  return __dsub_rn(__dmul_rn(2.0, double(m) * 0x1p-53), 1.0);
+}
+
+struct InnerGrid {
+  // InnerGrid::operator() (Grids.hpp:105-120): coordinate table built on the host
+  template<int D>
+  static __device__ __forceinline__ void point(const GridParams& g, const double* coord, uint64_t /*i*/,
+                                               uint32_t k, double* res)
+  {
+#pragma unroll
+    for (int j = 0; j < D; ++j) { res[j] = coord[k % g.n]; k /= g.n; }
+  }
+};
+
+struct FullGrid {
+  // FullGrid::operator() (Grids.hpp:67-83)
+  template<int D>
+  static __device__ __forceinline__ void point(const GridParams& g, const double* coord, uint64_t /*i*/,
+                                               uint32_t k, double* res)
+  {
+#pragma unroll
+    for (int j = 0; j < D; ++j) { res[j] = __dmul_rn(coord[k % g.n], g.eps1); k /= g.n; }
+  }
+};
+
+struct PhiloxGrid {
+  // uniform points in [-1,1)^D keyed by (seed, global point index i)
+  template<int D>
+  static __device__ __forceinline__ void point(const GridParams& g, const double* /*coord*/, uint64_t i,
+                                               uint32_t /*k*/, double* res)
+  {
+#pragma unroll
+    for (int j = 0; j < D; j += 2) {
+      uint32_t c[4] = {uint32_t(i), uint32_t(i >> 32), uint32_t(j / 2), 0u};
+      philox4x32_10(c, uint32_t(g.seed), uint32_t(g.seed >> 32));
+      res[j] = philox_signed(c[0], c[1]);
+      if (j + 1 < D) res[j + 1] = philox_signed(c[2], c[3]);
+    }
+  }
+};
+
+// ---------------------------------------------------------------------------------
+// maps
+// ---------------------------------------------------------------------------------
+// Henon through IteratingMap (Map_Henon.h:11-40, MapTools.hpp:10-32)
+struct HenonMap {
+  static constexpr int D = 2;
+  static __device__ __forceinline__ void step(const MapParams& m, const double* x, double* y)
+  {
+    y[0] = __dadd_rn(__dsub_rn(1.0, __dmul_rn(__dmul_rn(m.p[0], x[0]), x[0])), x[1]);
+    y[1] = __dmul_rn(m.p[1], x[0]);
+  }
+  static __device__ __forceinline__ void apply(const MapParams& m, const double* x, double* res)
+  {
+    uint32_t i = 0;
+    if (m.steps & 1u) { step(m, x, res); i = 1; }
+    else { res[0] = x[0]; res[1] = x[1]; }
+    for (; i < m.steps; i += 2) { double t[2]; step(m, res, t); step(m, t, res); }
+  }
+};
+
+// Lorenz through RK4Auto (Map_Lorenz.h:10-44, MapTools.hpp:118-182)
+template<class A>
+struct LorenzMap {
+  static constexpr int D = 3;
+  static __device__ __forceinline__ void rhs(const MapParams& m, const double* x, double* r);
+  static __device__ __forceinline__ void apply(const MapParams& m, const double* x0, double* res)
+  {
+    double x0_ = x0[0], x1 = x0[1], x2 = x0[2];
+    double x[3] = {x0_, x1, x2}, k[3], a[3];
+#pragma unroll 1
+    for (uint32_t s = 0; s < m.steps; ++s) {
+      rhs(m, x, k);
+#pragma unroll
+      for (int j = 0; j < 3; ++j) { res[j] = A::madd(m.h6, k[j], x[j]); a[j] = A::madd(m.h2, k[j], x[j]); }
+      rhs(m, a, k);
+#pragma unroll
+      for (int j = 0; j < 3; ++j) { res[j] = A::madd(m.h3, k[j], res[j]); a[j] = A::madd(m.h2, k[j], x[j]); }
+      rhs(m, a, k);
+#pragma unroll
+      for (int j = 0; j < 3; ++j) { res[j] = A::madd(m.h3, k[j], res[j]); a[j] = A::madd(m.h, k[j], x[j]); }
+      rhs(m, a, k);
+#pragma unroll
+      for (int j = 0; j < 3; ++j) { res[j] = A::madd(m.h6, k[j], res[j]); x[j] = res[j]; }
+    }
+  }
+};
+
+// LorenzRHS (Map_Lorenz.h:10-24): (sigma (y-x), rho x - y - x z, -beta z + x y)
+template<>
+__device__ __forceinline__ void LorenzMap<Strict>::rhs(const MapParams& m, const double* x, double* r)
+{
+  r[0] = __dmul_rn(m.p[0], __dsub_rn(x[1], x[0]));
+  r[1] = __dsub_rn(__dsub_rn(__dmul_rn(m.p[1], x[0]), x[1]), __dmul_rn(x[0], x[2]));
+  r[2] = __dadd_rn(__dmul_rn(-m.p[2], x[2]), __dmul_rn(x[0], x[1]));
+}
+
+template<>
+__device__ __forceinline__ void LorenzMap<Fused>::rhs(const MapParams& m, const double* x, double* r)
+{
+  r[0] = __dmul_rn(m.p[0], __dsub_rn(x[1], x[0]));
+  r[1] = __fma_rn(-x[0], x[2], __fma_rn(m.p[1], x[0], -x[1]));
+  r[2] = __fma_rn(x[0], x[1], __dmul_rn(-m.p[2], x[2]));
+}
+
+// coupled Duffing Hamiltonian through SymplecticIntegratorAuto order 2
+// (MapTools.hpp:371-421): half q-step, full p-step, half q-step
+struct CoupledDuffingMap {
+  static constexpr int D = 4;
+  static __device__ __forceinline__ void apply(const MapParams& m, const double* x, double* res)
+  {
+    double q0 = x[0], q1 = x[1], p0 = x[2], p1 = x[3];
+#pragma unroll 1
+    for (uint32_t s = 0; s < m.steps; ++s) {
+      q0 = __dadd_rn(q0, __dmul_rn(__dmul_rn(0.5, p0), m.h));
+      q1 = __dadd_rn(q1, __dmul_rn(__dmul_rn(0.5, p1), m.h));
+      const double f0 = __dsub_rn(__dsub_rn(q0, __dmul_rn(__dmul_rn(q0, q0), q0)),
+                                  __dmul_rn(__dmul_rn(__dmul_rn(0.2, q0), q1), q1));
+      const double f1 = __dsub_rn(__dmul_rn(-1.69, q1), __dmul_rn(__dmul_rn(__dmul_rn(0.2, q0), q0), q1));
+      p0 = __dadd_rn(p0, __dmul_rn(f0, m.h));
+      p1 = __dadd_rn(p1, __dmul_rn(f1, m.h));
+      q0 = __dadd_rn(q0, __dmul_rn(__dmul_rn(0.5, p0), m.h));
+      q1 = __dadd_rn(q1, __dmul_rn(__dmul_rn(0.5, p1), m.h));
+    }
+    res[0] = q0; res[1] = q1; res[2] = p0; res[3] = p1;
+  }
+};
+
+// forced Duffing x'' + delta x' + alpha x + beta x^3 = gamma cos t, exactly `steps`
+// classical RK4 steps (MapTools.hpp:42-108 without the floating-point t loop), the
+// forcing at the stage times read from a host-computed cos table
+struct ForcedDuffingMap {
+  static constexpr int D = 2;
+  static __device__ __forceinline__ void rhs(const MapParams& m, double c, const double* x, double* r)
+  {
+    r[0] = x[1];
+    r[1] = __dadd_rn(__dsub_rn(__dsub_rn(__dmul_rn(-m.p[0], x[1]), __dmul_rn(m.p[1], x[0])),
+                               __dmul_rn(m.p[2], __dmul_rn(__dmul_rn(x[0], x[0]), x[0]))),
+                     __dmul_rn(m.p[3], c));
+  }
+  static __device__ __forceinline__ void apply(const MapParams& m, const double* x0, double* res)
+  {
+    double x[2] = {x0[0], x0[1]}, k[2], a[2];
+#pragma unroll 1
+    for (uint32_t s = 0; s < m.steps; ++s) {
+      const double c0 = __ldg(m.table + 2 * s), c1 = __ldg(m.table + 2 * s + 1), c2 = __ldg(m.table + 2 * s + 2);
+      rhs(m, c0, x, k);
+#pragma unroll
+      for (int j = 0; j < 2; ++j) { res[j] = Strict::madd(m.h6, k[j], x[j]); a[j] = Strict::madd(m.h2, k[j], x[j]); }
+      rhs(m, c1, a, k);
+#pragma unroll
+      for (int j = 0; j < 2; ++j) { res[j] = Strict::madd(m.h3, k[j], res[j]); a[j] = Strict::madd(m.h2, k[j], x[j]); }
+      rhs(m, c1, a, k);
+#pragma unroll
+      for (int j = 0; j < 2; ++j) { res[j] = Strict::madd(m.h3, k[j], res[j]); a[j] = Strict::madd(m.h, k[j], x[j]); }
+      rhs(m, c2, a, k);
+#pragma unroll
+      for (int j = 0; j < 2; ++j) { res[j] = Strict::madd(m.h6, k[j], res[j]); x[j] = res[j]; }
+    }
+  }
+};
+
+}  // namespace b12g

@@ -1,0 +1,327 @@
+// Fused box-image kernels: per test point, box centre -> grid point -> map -> depth-d
+// code -> leaf index, all in FP64 registers.  This is the reference's
+// GridPointsFunctor (Functors.hpp:476-511) consumed by thrust::lower_bound and
+// ComputeSearchIndexFunctor (ImplicitBoxTree.hpp:2394-2432), evaluated once per point
+// instead of twice and without the point stream ever being stored.
+#include "kernels.h"
+
+namespace b12g {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+// the source box of point (rank, k) and the leaf index its image lands in
+template<class Map, class Grid>
+struct PointImage {
+  static constexpr int D = Map::D;
+
+  static __device__ __forceinline__ uint64_t source_code(const ImageArgs& a, uint32_t leaf)
+  {
+    return a.children ? ((__ldg(a.codes + (leaf >> 1)) << 1) | uint64_t(leaf & 1u)) : __ldg(a.codes + leaf);
+  }
+
+  // returns the target code validity; `tcode` the depth-d code of the image point
+  static __device__ __forceinline__ bool image(const ImageArgs& a, const double* coord, uint64_t code,
+                                               uint64_t i, uint32_t k, uint64_t& tcode)
+  {
+    double c[D], r[D], g[D], x[D], y[D];
+    box_coordinates<D>(a.dom, code, a.depth, c, r);
+    Grid::template point<D>(a.grid, coord, i, k, g);
+#pragma unroll
+    for (int j = 0; j < D; ++j) x[j] = __dadd_rn(c[j], __dmul_rn(g[j], r[j]));
+    Map::apply(a.map, x, y);
+    return point_code<D>(a.dom, y, a.depth, tcode);
+  }
+
+  static __device__ __forceinline__ uint32_t target(const ImageArgs& a, uint32_t n, bool valid, uint64_t tcode)
+  {
+    if (!a.children) return locate(a.codes, n, valid, tcode);
+    if (!valid) return kInvalidIndex;
+    const uint32_t p = locate(a.codes, n, true, tcode >> 1);
+    return p == kInvalidIndex ? kInvalidIndex : 2u * p + uint32_t(tcode & 1u);
+  }
+};
+
+__device__ __forceinline__ void load_coords(const GridParams& g, double* smem)
+{
+  for (uint32_t i = threadIdx.x; i < 64; i += blockDim.x) smem[i] = g.coord[i];
+  __syncthreads();
+}
+
+template<class Map, class Grid, ImageMode M>
+__global__ void __launch_bounds__(kThreads) image_points_kernel(const ImageArgs a)
+{
+  using PI = PointImage<Map, Grid>;
+  __shared__ double coord[64];
+  load_coords(a.grid, coord);
+
+  const uint32_t n = *a.n_leaves;
+  const uint32_t nboxes = a.n_src ? *a.n_src : (a.children ? 2u * n : n);
+  const uint64_t P = a.points;
+  const uint64_t total = uint64_t(nboxes) * P;
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  const int lane = threadIdx.x & 31;
+  if (M == ImageMode::Hit && a.children && 2ull * n > a.hit_cap) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(a.error, 1u);
+    return;
+  }
+
+  // the loop trip count is uniform per warp so that warp collectives stay converged
+  for (uint64_t base = uint64_t(blockIdx.x) * blockDim.x + (threadIdx.x & ~31u); base < total; base += stride) {
+    const uint64_t g = base + lane;
+    const bool active = g < total;
+    uint32_t t = kInvalidIndex;
+    uint64_t tcode = 0;
+    bool valid = false;
+    if (active) {
+      uint64_t rank;
+      uint32_t k;
+      if (total <= 0xFFFFFFFFull) {
+        const uint32_t g32 = uint32_t(g), P32 = uint32_t(P);
+        rank = g32 / P32;
+        k = g32 - uint32_t(rank) * P32;
+      } else {
+        rank = g / P;
+        k = uint32_t(g - rank * P);
+      }
+      const uint32_t leaf = a.src ? __ldg(a.src + rank) : uint32_t(rank);
+      const uint64_t code = PI::source_code(a, leaf);
+      valid = PI::image(a, coord, code, g, k, tcode);
+      t = PI::target(a, n, valid, tcode);
+    }
+    if constexpr (M == ImageMode::Hit) {
+      // one store per distinct target in the warp
+      const unsigned peers = __match_any_sync(0xFFFFFFFFu, t);
+      if (active && t != kInvalidIndex && lane == __ffs(peers) - 1) a.hit[t] = 1;
+    } else if constexpr (M == ImageMode::Search) {
+      if (active) a.out[g] = t;
+    } else {
+      // candidates: valid images that are not leaves; deduplicated within the warp and
+      // appended with one atomic per warp
+      if (a.hit && active && t != kInvalidIndex) {
+        const unsigned hp = __match_any_sync(__activemask(), t);
+        if (lane == __ffs(hp) - 1) a.hit[t] = 1;
+      }
+      const bool is_cand = active && valid && t == kInvalidIndex;
+      const uint64_t key = is_cand ? tcode : kInvalidCode;
+      const unsigned peers = __match_any_sync(0xFFFFFFFFu, key);
+      const bool leader = is_cand && lane == __ffs(peers) - 1;
+      const unsigned lead_mask = __ballot_sync(0xFFFFFFFFu, leader);
+      uint32_t slot = 0;
+      if (lane == 0 && lead_mask) slot = atomicAdd(a.cand_count, uint32_t(__popc(lead_mask)));
+      slot = __shfl_sync(0xFFFFFFFFu, slot, 0);
+      if (leader) {
+        const uint32_t pos = slot + __popc(lead_mask & ((1u << lane) - 1u));
+        if (pos < a.cand_cap) a.cand[pos] = tcode;
+        else atomicOr(a.error, 1u);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------
+// transition rows: warp per source box; the box's P <= 128 targets are sorted in
+// shared memory and run-length counted, giving the row's (column, count) pairs in
+// column order - the reference's packed (row, col) radix sort plus reverse
+// inclusive_scan_by_key and unique_by_key (ImplicitBoxTree.hpp:3007-3038) done per row
+// ---------------------------------------------------------------------------------
+constexpr int kRowWarps = kThreads / 32;
+
+__device__ __forceinline__ void warp_bitonic_128(uint32_t* s, int lane)
+{
+#pragma unroll 1
+  for (int k = 2; k <= 128; k <<= 1) {
+#pragma unroll 1
+    for (int j = k >> 1; j > 0; j >>= 1) {
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int c = lane + 32 * q;                           // comparator 0..63
+        const int i = ((c & ~(j - 1)) << 1) | (c & (j - 1));    // insert a zero bit at log2(j)
+        const int l = i | j;
+        const bool up = (i & k) == 0;
+        const uint32_t x = s[i], y = s[l];
+        if ((x > y) == up) { s[i] = y; s[l] = x; }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+template<class Map, class Grid>
+__global__ void __launch_bounds__(kThreads) transition_rows_kernel(const RowArgs ra)
+{
+  using PI = PointImage<Map, Grid>;
+  const ImageArgs& a = ra.img;
+  __shared__ double coord[64];
+  __shared__ uint32_t keys[kRowWarps][128];
+  __shared__ uint32_t bounds[kRowWarps][4];
+  load_coords(a.grid, coord);
+
+  const uint32_t n = *a.n_leaves;
+  const uint32_t nrows = a.n_src ? *a.n_src : n;
+  const uint32_t P = uint32_t(a.points);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  uint32_t* s = keys[w];
+  const uint32_t warps = gridDim.x * kRowWarps;
+
+  for (uint32_t row = blockIdx.x * kRowWarps + w; row < nrows; row += warps) {
+    const uint32_t leaf = a.src ? __ldg(a.src + row) : row;
+    const uint64_t code = PI::source_code(a, leaf);
+#pragma unroll 1
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t k = uint32_t(lane) + 32u * q;
+      uint32_t key = kPadKey;
+      if (k < P) {
+        uint64_t tcode;
+        const bool valid = PI::image(a, coord, code, uint64_t(row) * P + k, k, tcode);
+        const uint32_t t = PI::target(a, n, valid, tcode);
+        key = t == kInvalidIndex ? kLostKey : t;
+      }
+      s[lane + 32 * q] = key;
+    }
+    if (lane < 4) bounds[w][lane] = 0;
+    __syncwarp();
+    warp_bitonic_128(s, lane);
+
+    // run boundaries: position p starts a run if p == 0 or s[p] != s[p-1]
+    uint32_t nib = 0;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int p = lane * 4 + r;
+      if (p == 0 || s[p] != s[p - 1]) nib |= 1u << r;
+    }
+    atomicOr(&bounds[w][lane >> 3], nib << ((lane & 7) * 4));
+    __syncwarp();
+
+    const uint32_t ws[4] = {bounds[w][0], bounds[w][1], bounds[w][2], bounds[w][3]};
+    uint32_t cols[4], cnts[4], emit = 0;
+    bool take[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int p = lane * 4 + r;
+      const uint32_t key = s[p];
+      take[r] = ((nib >> r) & 1u) && key != kPadKey && (key != kLostKey || ra.keep_lost);
+      // the run ends at the next boundary after p (or at P, where the padding starts)
+      int end = int(P);
+      bool found = false;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int first = q * 32, from = p + 1;
+        if (found || from >= first + 32) continue;
+        const uint32_t m = from > first ? ws[q] & (0xFFFFFFFFu << (from - first)) : ws[q];
+        if (m) { end = min(int(P), first + __ffs(m) - 1); found = true; }
+      }
+      cols[r] = key == kLostKey ? ra.lost_col : key;
+      cnts[r] = uint32_t(end - p);
+      emit += take[r] ? 1u : 0u;
+    }
+    // warp exclusive scan of emit counts
+    uint32_t off = emit;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, off, d);
+      if (lane >= d) off += v;
+    }
+    const uint32_t total = __shfl_sync(0xFFFFFFFFu, off, 31);
+    off -= emit;
+    uint32_t* sc = ra.stage_col + size_t(row) * P;
+    uint32_t* sn = ra.stage_cnt + size_t(row) * P;
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+      if (take[r]) { sc[off] = cols[r]; sn[off] = cnts[r]; ++off; }
+    if (lane == 0) ra.row_count[row] = total;
+    __syncwarp();
+  }
+}
+
+template<class Map, class Grid>
+cudaError_t launch_image_t(ImageMode mode, const ImageArgs& a, uint64_t max_points, cudaStream_t s)
+{
+  static int blocks_per_sm[3] = {0, 0, 0};
+  const int m = int(mode);
+  if (!blocks_per_sm[m]) {
+    int b = 0;
+    if (mode == ImageMode::Hit)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, image_points_kernel<Map, Grid, ImageMode::Hit>, kThreads, 0);
+    else if (mode == ImageMode::Search)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, image_points_kernel<Map, Grid, ImageMode::Search>, kThreads, 0);
+    else
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, image_points_kernel<Map, Grid, ImageMode::Insert>, kThreads, 0);
+    blocks_per_sm[m] = b > 0 ? b : 1;
+  }
+  const uint64_t want = (max_points + kThreads - 1) / kThreads;
+  const uint64_t cap = uint64_t(device_sm_count()) * blocks_per_sm[m];
+  const unsigned grid = unsigned(want < 1 ? 1 : (want < cap ? want : cap));
+  if (mode == ImageMode::Hit) image_points_kernel<Map, Grid, ImageMode::Hit><<<grid, kThreads, 0, s>>>(a);
+  else if (mode == ImageMode::Search) image_points_kernel<Map, Grid, ImageMode::Search><<<grid, kThreads, 0, s>>>(a);
+  else image_points_kernel<Map, Grid, ImageMode::Insert><<<grid, kThreads, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+template<class Map, class Grid>
+cudaError_t launch_rows_t(const RowArgs& a, uint32_t max_rows, cudaStream_t s)
+{
+  static int blocks_per_sm = 0;
+  if (!blocks_per_sm) {
+    int b = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, transition_rows_kernel<Map, Grid>, kThreads, 0);
+    blocks_per_sm = b > 0 ? b : 1;
+  }
+  const uint64_t want = (uint64_t(max_rows) + kRowWarps - 1) / kRowWarps;
+  const uint64_t cap = uint64_t(device_sm_count()) * blocks_per_sm;
+  const unsigned grid = unsigned(want < 1 ? 1 : (want < cap ? want : cap));
+  transition_rows_kernel<Map, Grid><<<grid, kThreads, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+// (map, arith, grid) dispatch; each map has a fixed dimension
+template<class F>
+cudaError_t dispatch(uint32_t map_kind, uint32_t arith, uint32_t grid_kind, uint32_t dim, F&& f)
+{
+  auto with_grid = [&](auto map_tag) -> cudaError_t {
+    using Map = decltype(map_tag);
+    if (dim != uint32_t(Map::D)) return cudaErrorInvalidValue;
+    switch (grid_kind) {
+      case B12G_GRID_INNER: return f(Map{}, InnerGrid{});
+      case B12G_GRID_FULL: return f(Map{}, FullGrid{});
+      case B12G_GRID_PHILOX: return f(Map{}, PhiloxGrid{});
+      default: return cudaErrorInvalidValue;
+    }
+  };
+  switch (map_kind) {
+    case B12G_MAP_HENON: return arith == B12G_ARITH_STRICT ? with_grid(HenonMap{}) : cudaErrorInvalidValue;
+    case B12G_MAP_LORENZ:
+      return arith == B12G_ARITH_FMA ? with_grid(LorenzMap<Fused>{}) : with_grid(LorenzMap<Strict>{});
+    case B12G_MAP_COUPLED_DUFFING:
+      return arith == B12G_ARITH_STRICT ? with_grid(CoupledDuffingMap{}) : cudaErrorInvalidValue;
+    case B12G_MAP_FORCED_DUFFING:
+      return arith == B12G_ARITH_STRICT ? with_grid(ForcedDuffingMap{}) : cudaErrorInvalidValue;
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace
+
+bool image_supported(uint32_t map_kind, uint32_t arith, uint32_t grid_kind, uint32_t dim)
+{
+  return dispatch(map_kind, arith, grid_kind, dim, [](auto, auto) { return cudaSuccess; }) == cudaSuccess;
+}
+
+cudaError_t launch_image(uint32_t map_kind, uint32_t arith, uint32_t grid_kind, uint32_t dim, ImageMode mode,
+                         const ImageArgs& a, uint64_t max_points, cudaStream_t s)
+{
+  return dispatch(map_kind, arith, grid_kind, dim, [&](auto map, auto grid) {
+    return launch_image_t<decltype(map), decltype(grid)>(mode, a, max_points, s);
+  });
+}
+
+cudaError_t launch_rows(uint32_t map_kind, uint32_t arith, uint32_t grid_kind, uint32_t dim, const RowArgs& a,
+                        uint32_t max_rows, cudaStream_t s)
+{
+  return dispatch(map_kind, arith, grid_kind, dim, [&](auto map, auto grid) {
+    return launch_rows_t<decltype(map), decltype(grid)>(a, max_rows, s);
+  });
+}
+
+}  // namespace b12g

@@ -1,0 +1,174 @@
+// Host-side objects of libb12g shared by the C ABI translation units.
+#pragma once
+
+#include <algorithm>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "kernels.h"
+
+namespace b12g {
+namespace host {
+
+b12g_status fail(b12g_status s, const char* fmt, ...);
+b12g_status cuda_fail(cudaError_t e, const char* where);
+
+#define CK(call)                                                   \
+  do {                                                             \
+    cudaError_t e_ = (call);                                       \
+    if (e_ != cudaSuccess) return ::b12g::host::cuda_fail(e_, #call); \
+  } while (0)
+
+#define ST(call)                                                   \
+  do {                                                             \
+    b12g_status s_ = (call);                                       \
+    if (s_ != B12G_OK) return s_;                                  \
+  } while (0)
+
+// grow-only device buffer
+template<class T>
+struct Buf {
+  T* p = nullptr;
+  size_t n = 0;
+  b12g_status ensure(size_t count, const char* what)
+  {
+    if (count <= n) return B12G_OK;
+    size_t want = std::max<size_t>(count, n + n / 2);
+    want = std::max<size_t>(want, 256);
+    T* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, want * sizeof(T));
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return fail(B12G_ERR_OOM, "cannot allocate %zu bytes for %s", want * sizeof(T), what);
+    }
+    if (p) cudaFree(p);
+    p = q;
+    n = want;
+    return B12G_OK;
+  }
+  // grow keeping the first `keep` elements
+  b12g_status grow_keep(size_t count, size_t keep, cudaStream_t s, const char* what)
+  {
+    if (count <= n) return B12G_OK;
+    T* old = p;
+    size_t oldn = n;
+    p = nullptr;
+    n = 0;
+    b12g_status st = ensure(count, what);
+    if (st != B12G_OK) { p = old; n = oldn; return st; }
+    if (old) {
+      if (keep) cudaMemcpyAsync(p, old, keep * sizeof(T), cudaMemcpyDeviceToDevice, s);
+      cudaStreamSynchronize(s);
+      cudaFree(old);
+    }
+    return B12G_OK;
+  }
+  void release()
+  {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+
+// device counter slots
+enum : int {
+  C_N0 = 0,        // leaf count (ping)
+  C_N1 = 1,        // leaf count (pong)
+  C_CHANGED = 2,
+  C_ERROR = 3,
+  C_CAND = 4,
+  C_NSRC = 5,
+  C_TMP = 6,
+  C_NNZ = 7,
+  C_NCOLS = 8,
+  C_SYNC = 9,      // 3 words for the grid barrier
+  C_NNEW = 12,
+  C_COUNT = 16
+};
+
+}  // namespace host
+}  // namespace b12g
+
+struct b12g_tree {
+  template<class T> using Buf = b12g::host::Buf<T>;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  b12g_domain domain{};
+  b12g::Domain dom{};
+  uint32_t n = 1;
+  uint8_t depth = 0;
+  int cur = 0;     // current code/flags buffer
+  int ncur = 0;    // current count slot (C_N0 / C_N1)
+  Buf<uint64_t> code[2];
+  Buf<uint8_t> flags[2];
+  Buf<uint8_t> hit;
+  Buf<uint32_t> ctr;
+  Buf<uint32_t> tiles_a, tiles_b;
+  Buf<uint32_t> src, out, stage_col, stage_cnt, row_count, rowptr;
+  Buf<uint64_t> cand, cand2;
+  Buf<uint32_t> sort_idx;
+  Buf<double> table;
+  Buf<double> points;
+  Buf<uint32_t> step_counts;
+  Buf<uint8_t> sort_tmp;
+  uint32_t* h_ctr = nullptr;   // pinned mirror of ctr
+  // graph cache of the fused subdivision loop
+  cudaGraphExec_t sub_graph = nullptr;
+  std::vector<uint8_t> sub_key;
+  uint64_t sub_graph_kernels = 0;
+  // optional per-kernel timing: event pairs around image / transition-row launches
+  bool profile = false;
+  std::vector<cudaEvent_t> prof_events[2];   // [kind] start/stop pairs, reused
+  size_t prof_used[2] = {0, 0};
+  double prof_ms[2] = {0.0, 0.0};
+  uint64_t prof_launches[2] = {0, 0};
+  std::vector<cudaEvent_t> graph_prof[2];    // events baked into the captured loop
+
+  uint64_t* codes() { return code[cur].p; }
+  uint8_t* flg() { return flags[cur].p; }
+  uint32_t* dn() { return ctr.p + ncur; }
+};
+
+struct b12g_csr {
+  template<class T> using Buf = b12g::host::Buf<T>;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  uint32_t n_rows = 0, n_cols = 0;
+  uint64_t nnz = 0;
+  Buf<uint32_t> rowptr, cols;
+  Buf<double> vals;
+  // P^T, built on first use by the invariant measure
+  Buf<uint32_t> tptr, trows, work, tiles;
+  Buf<double> tvals, w0, w1, partial, vout;
+  Buf<uint32_t> ctr;
+  bool has_transpose = false;
+};
+
+namespace b12g {
+void count_launches(unsigned long long k);
+namespace host {
+
+// host-side validation and kernel argument set-up for a scheme
+struct Prepared {
+  ImageArgs a{};
+  uint64_t P = 0;
+};
+
+b12g_status sync(b12g_tree* t, const char* where);
+b12g_status read_ctr(b12g_tree* t, int first, int count);
+b12g_status set_ctr(b12g_tree* t, int slot, uint32_t v);
+b12g_status reserve(b12g_tree* t, uint64_t n_boxes);
+b12g_status prepare(b12g_tree* t, const b12g_scheme* sc, Prepared& pr);
+b12g_status check_depth(b12g_tree* t, uint8_t depth);
+b12g_status select_sources(b12g_tree* t, const b12g_scheme* sc, Prepared& pr, uint32_t& n_src);
+b12g_status check_error(b12g_tree* t, const char* where);
+b12g_status set_root(b12g_tree* t, uint8_t flags);
+b12g_status flag_call(b12g_tree* t, int op, uint8_t u, uint8_t f, uint8_t depth, uint32_t* n_changed);
+// record a timing event of `kind` (0: box-image kernel, 1: transition rows) on the tree stream
+void prof_mark(b12g_tree* t, int kind);
+b12g_status prof_collect(b12g_tree* t);
+
+}  // namespace host
+}  // namespace b12g

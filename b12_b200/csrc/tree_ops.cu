@@ -1,0 +1,339 @@
+// Leaf-array kernels: flag updates, subdivision split, stream compaction, scans.
+// All kernels read element counts from device memory and run grid-stride loops over a
+// persistent-sized grid, so a sequence of them needs no host round trip and can be
+// captured in a CUDA graph.
+#include <algorithm>
+
+#include "kernels.h"
+
+namespace b12g {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kItems = kCompactTile / kThreads;  // 16 elements per thread per tile
+
+__device__ __forceinline__ bool has_all(uint8_t f, uint8_t check) { return uint8_t(f & check) == check; }
+
+// block-wide sum of one value per thread (all threads must call)
+__device__ __forceinline__ uint32_t block_sum(uint32_t v, uint32_t* red)
+{
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, d);
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  uint32_t t = 0;
+  for (int i = 0; i < int(blockDim.x >> 5); ++i) t += red[i];
+  return t;
+}
+
+// block-wide exclusive scan of one value per thread; returns the prefix, *total the sum
+__device__ __forceinline__ uint32_t block_exclusive(uint32_t v, uint32_t* red, uint32_t* total)
+{
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint32_t x = v;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d);
+    if (lane >= d) x += y;
+  }
+  __syncthreads();
+  if (lane == 31) red[w] = x;
+  __syncthreads();
+  uint32_t before = 0, all = 0;
+  for (int i = 0; i < int(blockDim.x >> 5); ++i) {
+    const uint32_t r = red[i];
+    before += i < w ? r : 0u;
+    all += r;
+  }
+  *total = all;
+  return before + x - v;
+}
+
+int grid_for(uint64_t work, int per_block, int blocks_per_sm)
+{
+  const uint64_t want = (work + per_block - 1) / per_block;
+  const uint64_t cap = uint64_t(device_sm_count()) * blocks_per_sm;
+  return int(std::max<uint64_t>(1, std::min(want, cap)));
+}
+
+// ---------------------------------------------------------------------------------
+__global__ void apply_hits_kernel(uint8_t* flags, uint8_t* hit, const uint32_t* n_ptr, uint8_t f, uint32_t* changed)
+{
+  __shared__ uint32_t red[32];
+  const uint32_t n = *n_ptr;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  uint32_t c = 0;
+  const uint32_t iters = (n + stride - 1) / stride;
+  for (uint32_t it = 0, i = blockIdx.x * blockDim.x + threadIdx.x; it < iters; ++it, i += stride) {
+    if (i < n && hit[i]) {
+      const uint8_t old = flags[i];
+      c += has_all(old, f) ? 0u : 1u;
+      flags[i] = old | f;
+      hit[i] = 0;
+    }
+  }
+  c = block_sum(c, red);
+  if (threadIdx.x == 0 && c) atomicAdd(changed, c);
+}
+
+// op 0: set f (count boxes lacking f); 1: unset f (count boxes having any of f);
+// 2: change u -> f (count boxes having all of u)
+__global__ void flag_op_kernel(uint8_t* flags, const uint32_t* n_ptr, int op, uint8_t u, uint8_t f, uint32_t* changed)
+{
+  __shared__ uint32_t red[32];
+  const uint32_t n = *n_ptr;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  uint32_t c = 0;
+  const uint32_t iters = (n + stride - 1) / stride;
+  for (uint32_t it = 0, i = blockIdx.x * blockDim.x + threadIdx.x; it < iters; ++it, i += stride) {
+    if (i >= n) continue;
+    const uint8_t old = flags[i];
+    if (op == 0) { c += has_all(old, f) ? 0u : 1u; flags[i] = old | f; }
+    else if (op == 1) { c += (old & f) ? 1u : 0u; flags[i] = old & uint8_t(~f); }
+    else if (has_all(old, u)) { ++c; flags[i] = uint8_t((old & ~u) | f); }
+  }
+  c = block_sum(c, red);
+  if (threadIdx.x == 0 && c && changed) atomicAdd(changed, c);
+}
+
+__global__ void count_flags_kernel(const uint8_t* flags, const uint32_t* n_ptr, uint8_t f, uint32_t* count)
+{
+  __shared__ uint32_t red[32];
+  const uint32_t n = *n_ptr;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  uint32_t c = 0;
+  const uint32_t iters = (n + stride - 1) / stride;
+  for (uint32_t it = 0, i = blockIdx.x * blockDim.x + threadIdx.x; it < iters; ++it, i += stride)
+    if (i < n && has_all(flags[i], f)) ++c;
+  c = block_sum(c, red);
+  if (threadIdx.x == 0 && c) atomicAdd(count, c);
+}
+
+// subdivide: incrementDepthBy(1) + computeOtherHalf (Box.hpp:140-147, 234-239); the
+// children of a sorted parent array, written adjacently, are sorted
+__global__ void split_kernel(const uint64_t* code, const uint8_t* flags, const uint32_t* n_ptr, uint64_t* out_code,
+                             uint8_t* out_flags, uint32_t* n_out)
+{
+  const uint32_t n = *n_ptr;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const uint64_t c = code[i] << 1;
+    const uint8_t f = flags[i];
+    reinterpret_cast<ulonglong2*>(out_code)[i] = make_ulonglong2(c, c | 1u);
+    out_flags[2 * i] = f;
+    out_flags[2 * i + 1] = f;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *n_out = 2 * n;
+}
+
+// ---------------------------------------------------------------------------------
+// compaction: tile counts -> single-block tile scan -> ordered scatter
+// ---------------------------------------------------------------------------------
+// element count; 0 (with error bit 0) if the children do not fit the hit mask
+__device__ __forceinline__ uint32_t compact_n(const CompactArgs& a)
+{
+  if (!a.children) return *a.n;
+  const uint64_t c = 2ull * *a.n;
+  return c <= a.hit_cap ? uint32_t(c) : 0u;
+}
+
+__device__ __forceinline__ bool compact_keep(const CompactArgs& a, uint32_t i)
+{
+  return a.children ? a.hit[i] != 0 : has_all(a.flags[i], a.keep_flags);
+}
+
+__global__ void compact_count_kernel(const CompactArgs a, uint32_t* tile_counts)
+{
+  __shared__ uint32_t red[32];
+  const uint32_t n = compact_n(a);
+  const uint32_t tiles = (n + kCompactTile - 1) / kCompactTile;
+  for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+    uint32_t c = 0;
+#pragma unroll 4
+    for (int k = 0; k < kItems; ++k) {
+      const uint32_t i = t * kCompactTile + k * kThreads + threadIdx.x;
+      if (i < n && compact_keep(a, i)) ++c;
+    }
+    c = block_sum(c, red);
+    if (threadIdx.x == 0) tile_counts[t] = c;
+  }
+}
+
+// one block: exclusive scan of the tile counts; total -> *n_out
+__global__ void compact_scan_kernel(const CompactArgs a, const uint32_t* tile_counts, uint32_t* tile_offsets)
+{
+  __shared__ uint32_t red[32];
+  const uint32_t n = compact_n(a);
+  const uint32_t tiles = (n + kCompactTile - 1) / kCompactTile;
+  uint32_t carry = 0;
+  for (uint32_t base = 0; base < tiles; base += blockDim.x) {
+    const uint32_t t = base + threadIdx.x;
+    const uint32_t v = t < tiles ? tile_counts[t] : 0u;
+    uint32_t total;
+    const uint32_t ex = block_exclusive(v, red, &total);
+    if (t < tiles) tile_offsets[t] = carry + ex;
+    carry += total;
+  }
+  if (threadIdx.x == 0) {
+    if (carry > a.out_cap || (a.children && 2ull * *a.n > a.hit_cap)) atomicOr(a.error, 1u);
+    if (carry > a.out_cap) carry = a.out_cap;
+    *a.n_out = carry;
+    if (a.n_out2) *a.n_out2 = carry;
+  }
+}
+
+__global__ void compact_scatter_kernel(const CompactArgs a, const uint32_t* tile_offsets)
+{
+  __shared__ uint32_t red[32];
+  const uint32_t n = compact_n(a);
+  const uint32_t tiles = (n + kCompactTile - 1) / kCompactTile;
+  for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+    uint32_t off = tile_offsets[t];
+    for (int k = 0; k < kItems; ++k) {
+      const uint32_t i = t * kCompactTile + k * kThreads + threadIdx.x;
+      const bool keep = i < n && compact_keep(a, i);
+      uint32_t total;
+      const uint32_t ex = block_exclusive(keep ? 1u : 0u, red, &total);
+      if (keep) {
+        const uint32_t pos = off + ex;
+        if (pos < a.out_cap) {
+          if (a.out_index) {
+            a.out_index[pos] = i;
+          } else if (a.children) {
+            a.out_code[pos] = (a.code[i >> 1] << 1) | uint64_t(i & 1u);
+            a.out_flags[pos] = a.flags[i >> 1] & uint8_t(~a.clear_flags);
+          } else {
+            a.out_code[pos] = a.code[i];
+            a.out_flags[pos] = a.flags[i] & uint8_t(~a.clear_flags);
+          }
+        }
+      }
+      if (a.children && i < n) a.hit[i] = 0;
+      off += total;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------
+// exclusive scan u32 -> u32 with out[n] = total
+// ---------------------------------------------------------------------------------
+__global__ void scan_tiles_kernel(const uint32_t* in, const uint32_t* n_ptr, uint32_t* tile_sums)
+{
+  __shared__ uint32_t red[32];
+  const uint32_t n = *n_ptr;
+  const uint32_t tiles = (n + kCompactTile - 1) / kCompactTile;
+  for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+    uint32_t c = 0;
+    for (int k = 0; k < kItems; ++k) {
+      const uint32_t i = t * kCompactTile + k * kThreads + threadIdx.x;
+      if (i < n) c += in[i];
+    }
+    c = block_sum(c, red);
+    if (threadIdx.x == 0) tile_sums[t] = c;
+  }
+}
+
+__global__ void scan_tile_offsets_kernel(const uint32_t* n_ptr, uint32_t* tile_sums, uint32_t* out)
+{
+  __shared__ uint32_t red[32];
+  const uint32_t n = *n_ptr;
+  const uint32_t tiles = (n + kCompactTile - 1) / kCompactTile;
+  uint32_t carry = 0;
+  for (uint32_t base = 0; base < tiles; base += blockDim.x) {
+    const uint32_t t = base + threadIdx.x;
+    const uint32_t v = t < tiles ? tile_sums[t] : 0u;
+    uint32_t total;
+    const uint32_t ex = block_exclusive(v, red, &total);
+    __syncthreads();
+    if (t < tiles) tile_sums[t] = carry + ex;
+    carry += total;
+  }
+  if (threadIdx.x == 0) out[n] = carry;
+}
+
+__global__ void scan_down_kernel(const uint32_t* in, const uint32_t* n_ptr, const uint32_t* tile_offsets, uint32_t* out)
+{
+  __shared__ uint32_t red[32];
+  const uint32_t n = *n_ptr;
+  const uint32_t tiles = (n + kCompactTile - 1) / kCompactTile;
+  for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+    uint32_t off = tile_offsets[t];
+    for (int k = 0; k < kItems; ++k) {
+      const uint32_t i = t * kCompactTile + k * kThreads + threadIdx.x;
+      const uint32_t v = i < n ? in[i] : 0u;
+      uint32_t total;
+      const uint32_t ex = block_exclusive(v, red, &total);
+      if (i < n) out[i] = off + ex;
+      off += total;
+    }
+  }
+}
+
+}  // namespace
+
+int device_sm_count()
+{
+  static int sms[64] = {0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) dev = 0;
+  if (!sms[dev]) {
+    int v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    sms[dev] = v > 0 ? v : 1;
+  }
+  return sms[dev];
+}
+
+cudaError_t apply_hits(uint8_t* flags, uint8_t* hit, const uint32_t* n, uint8_t f, uint32_t* changed, uint32_t max_n,
+                       cudaStream_t s)
+{
+  apply_hits_kernel<<<grid_for(max_n, kThreads, 8), kThreads, 0, s>>>(flags, hit, n, f, changed);
+  return cudaGetLastError();
+}
+
+cudaError_t flag_op(uint8_t* flags, const uint32_t* n, int op, uint8_t u, uint8_t f, uint32_t* changed,
+                    uint32_t max_n, cudaStream_t s)
+{
+  flag_op_kernel<<<grid_for(max_n, kThreads, 8), kThreads, 0, s>>>(flags, n, op, u, f, changed);
+  return cudaGetLastError();
+}
+
+cudaError_t count_flags(const uint8_t* flags, const uint32_t* n, uint8_t f, uint32_t* count, uint32_t max_n,
+                        cudaStream_t s)
+{
+  count_flags_kernel<<<grid_for(max_n, kThreads, 8), kThreads, 0, s>>>(flags, n, f, count);
+  return cudaGetLastError();
+}
+
+cudaError_t split_codes(const uint64_t* code, const uint8_t* flags, const uint32_t* n, uint64_t* out_code,
+                        uint8_t* out_flags, uint32_t* n_out, uint32_t max_n, cudaStream_t s)
+{
+  split_kernel<<<grid_for(max_n, kThreads, 8), kThreads, 0, s>>>(code, flags, n, out_code, out_flags, n_out);
+  return cudaGetLastError();
+}
+
+cudaError_t compact(const CompactArgs& a, const CompactScratch& sc, uint32_t max_in, cudaStream_t s)
+{
+  const uint64_t elems = a.children ? 2ull * max_in : uint64_t(max_in);
+  const int g = grid_for(elems, kCompactTile, 4);
+  compact_count_kernel<<<g, kThreads, 0, s>>>(a, sc.tile_counts);
+  compact_scan_kernel<<<1, 1024, 0, s>>>(a, sc.tile_counts, sc.tile_offsets);
+  compact_scatter_kernel<<<g, kThreads, 0, s>>>(a, sc.tile_offsets);
+  return cudaGetLastError();
+}
+
+cudaError_t exclusive_scan_u32(const uint32_t* in, uint32_t* out, const uint32_t* n, uint32_t* tile_sums,
+                               uint32_t max_n, cudaStream_t s)
+{
+  const int g = grid_for(max_n, kCompactTile, 4);
+  scan_tiles_kernel<<<g, kThreads, 0, s>>>(in, n, tile_sums);
+  scan_tile_offsets_kernel<<<1, 1024, 0, s>>>(n, tile_sums, out);
+  scan_down_kernel<<<g, kThreads, 0, s>>>(in, n, tile_sums, out);
+  return cudaGetLastError();
+}
+
+}  // namespace b12g

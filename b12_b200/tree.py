@@ -1,0 +1,346 @@
+"""Python mirror of the reference's ImplicitBoxTree for the box-image path.
+
+Method names follow the reference (B12c/src/include/ImplicitBoxTree.h:72-603) in
+snake_case; the reference's camelCase names are provided as aliases.  Every call goes
+through the C ABI of libb12g.so (include/b12g.h) and runs on the GPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib as L
+from ._lib import check, lib
+
+LEAF = L.LEAF_DEPTH
+
+
+# ----------------------------------------------------------------------------- schemes
+@dataclass
+class MapSpec:
+    kind: int
+    steps: int = 1
+    h: float = 0.0
+    p: tuple = ()
+    arith: int = L.ARITH_STRICT
+
+    def to_c(self) -> L.Map:
+        m = L.Map()
+        m.kind, m.arith, m.steps, m.h = self.kind, self.arith, self.steps, self.h
+        for i, v in enumerate(self.p):
+            m.p[i] = v
+        return m
+
+
+@dataclass
+class GridSpec:
+    kind: int
+    n: int = 1
+    points: int = 1
+    seed: int = 0
+    eps: float = 0.0
+
+    def to_c(self) -> L.Grid:
+        g = L.Grid()
+        g.kind, g.n, g.points, g.seed, g.eps = self.kind, self.n, self.points, self.seed, self.eps
+        return g
+
+    def points_per_box(self, dim: int) -> int:
+        return self.points if self.kind == L.GRID_PHILOX else self.n ** dim
+
+
+def henon(a: float = 1.4, b: float = 0.3, steps: int = 1) -> MapSpec:
+    """Henon<2,double>(a, b, steps) (Map_Henon.h:27-40)."""
+    return MapSpec(L.MAP_HENON, steps=steps, p=(a, b))
+
+
+def lorenz(sigma: float = 10.0, rho: float = 28.0, beta: float = 8.0 / 3.0, h: float = 0.01, steps: int = 20,
+           fma: bool = False) -> MapSpec:
+    """Lorenz<3,double>(sigma, rho, beta, h, steps) (Map_Lorenz.h:27-44); fma=True uses
+    explicit fused multiply-adds in the integrator."""
+    return MapSpec(L.MAP_LORENZ, steps=steps, h=h, p=(sigma, rho, beta), arith=L.ARITH_FMA if fma else L.ARITH_STRICT)
+
+
+def coupled_duffing(h: float = 0.05, steps: int = 10) -> MapSpec:
+    """Stormer-Verlet map of H = |p|^2/2 - q1^2/2 + q1^4/4 + 1.69 q2^2/2 + 0.1 q1^2 q2^2."""
+    return MapSpec(L.MAP_COUPLED_DUFFING, steps=steps, h=h)
+
+
+FORCED_PERIOD = 2.0 * 3.14159265358979323846
+
+
+def forced_duffing(steps: int = 200, delta: float = 0.25, alpha: float = -1.0, beta: float = 1.0,
+                   gamma: float = 0.3) -> MapSpec:
+    """Period-2pi map of x'' + delta x' + alpha x + beta x^3 = gamma cos t, `steps` RK4 steps."""
+    return MapSpec(L.MAP_FORCED_DUFFING, steps=steps, h=FORCED_PERIOD / steps, p=(delta, alpha, beta, gamma))
+
+
+def inner_grid(n: int) -> GridSpec:
+    """InnerGrid<DIM,double>(n) (Grids.hpp:103-134)."""
+    return GridSpec(L.GRID_INNER, n=n)
+
+
+def full_grid(n: int, eps: float = 0.0) -> GridSpec:
+    """FullGrid<DIM,double>(n, eps) (Grids.hpp:60-95)."""
+    return GridSpec(L.GRID_FULL, n=n, eps=eps)
+
+
+def philox_grid(points: int, seed: int = 0) -> GridSpec:
+    """`points` uniform points per box from Philox4x32-10 keyed by (seed, point index)."""
+    return GridSpec(L.GRID_PHILOX, points=points, seed=seed)
+
+
+@dataclass
+class Scheme:
+    """The Matlab driver's {grid, map, depth, flags} point-iterator description."""
+    map: MapSpec
+    grid: GridSpec
+    depth: int = LEAF
+    flags_to_check: int = 0
+
+    def to_c(self) -> L.Scheme:
+        s = L.Scheme()
+        s.map = self.map.to_c()
+        s.grid = self.grid.to_c()
+        s.depth = self.depth
+        s.flags_to_check = self.flags_to_check
+        return s
+
+
+# ----------------------------------------------------------------------------- matrices
+class CsrMatrix:
+    """Row-major transition matrix resident on the GPU (row = source leaf)."""
+
+    def __init__(self, handle: C.c_void_p):
+        self._h = handle
+        r, c, z = C.c_uint32(), C.c_uint32(), C.c_uint64()
+        check(lib().b12g_csr_shape(self._h, C.byref(r), C.byref(c), C.byref(z)), "csr_shape")
+        self.n_rows, self.n_cols, self.nnz = r.value, c.value, z.value
+
+    def to_host(self):
+        rowptr = np.zeros(self.n_rows + 1, dtype=np.uint32)
+        cols = np.zeros(max(self.nnz, 1), dtype=np.uint32)
+        vals = np.zeros(max(self.nnz, 1), dtype=np.float64)
+        check(lib().b12g_csr_copy(self._h, rowptr.ctypes.data, cols.ctypes.data, vals.ctypes.data), "csr_copy")
+        return rowptr, cols[: self.nnz], vals[: self.nnz]
+
+    def invariant_measure(self, iters: int = 200, out=None, keep_on_device: bool = False):
+        """FP64 power iteration; returns the measure (into `out` if given), or None with
+        keep_on_device=True (fetch it later with measure())."""
+        if keep_on_device:
+            check(lib().b12g_invariant_measure(self._h, iters, None), "invariant_measure")
+            return None
+        v = np.zeros(self.n_rows, dtype=np.float64) if out is None else out
+        check(lib().b12g_invariant_measure(self._h, iters, v.ctypes.data), "invariant_measure")
+        return v
+
+    def measure(self, out=None) -> np.ndarray:
+        v = np.zeros(self.n_rows, dtype=np.float64) if out is None else out
+        check(lib().b12g_csr_measure(self._h, v.ctypes.data), "csr_measure")
+        return v
+
+    def to_host_into(self, rowptr, cols, vals):
+        check(lib().b12g_csr_copy(self._h, rowptr.ctypes.data, cols.ctypes.data, vals.ctypes.data), "csr_copy")
+
+    def close(self):
+        if self._h:
+            lib().b12g_csr_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def launch_count() -> int:
+    n = C.c_uint64()
+    check(lib().b12g_launch_count(C.byref(n)), "launch_count")
+    return n.value
+
+
+def probe_fp64_fma(seconds: float = 0.2):
+    """FP64 FMA throughput of the current device in TFLOP/s (and the probe's seconds)."""
+    tf, sec = C.c_double(), C.c_double()
+    check(lib().b12g_probe_fp64_fma(seconds, C.byref(tf), C.byref(sec)), "probe_fp64_fma")
+    return tf.value, sec.value
+
+
+# ----------------------------------------------------------------------------- tree
+class ImplicitBoxTree:
+    """ImplicitBoxTree<CUDA, DIM, double, 64> on one B200 (uniform leaf depth)."""
+
+    def __init__(self, center, radius):
+        center = list(map(float, center))
+        radius = list(map(float, radius))
+        if len(center) != len(radius) or not 1 <= len(center) <= L.MAX_DIM:
+            raise ValueError("center and radius must have the same length 1..4")
+        d = L.Domain()
+        d.dim = len(center)
+        for j in range(d.dim):
+            d.center[j] = center[j]
+            d.radius[j] = radius[j]
+        self.dim = d.dim
+        self._h = C.c_void_p()
+        check(lib().b12g_tree_create(C.byref(d), C.byref(self._h)), "tree_create")
+
+    def close(self):
+        if self._h:
+            lib().b12g_tree_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- queries
+    def count(self, depth: int = LEAF) -> int:
+        c = C.c_uint32()
+        check(lib().b12g_count(self._h, depth, C.byref(c)), "count")
+        return c.value
+
+    def depth(self) -> int:
+        d = C.c_uint8()
+        check(lib().b12g_depth(self._h, C.byref(d)), "depth")
+        return d.value
+
+    def leaves(self):
+        n = self.count()
+        codes = np.zeros(n, dtype=np.uint64)
+        depth = np.zeros(n, dtype=np.uint8)
+        flags = np.zeros(n, dtype=np.uint8)
+        check(lib().b12g_leaves(self._h, codes.ctypes.data, depth.ctypes.data, flags.ctypes.data), "leaves")
+        return codes, depth, flags
+
+    def load_leaves(self, codes, depth, flags):
+        codes = np.ascontiguousarray(codes, dtype=np.uint64)
+        depth = np.ascontiguousarray(depth, dtype=np.uint8)
+        flags = np.ascontiguousarray(flags, dtype=np.uint8)
+        check(lib().b12g_load_leaves(self._h, codes.ctypes.data, depth.ctypes.data, flags.ctypes.data, len(codes)),
+              "load_leaves")
+
+    def reserve(self, n_boxes: int):
+        check(lib().b12g_tree_reserve(self._h, n_boxes), "reserve")
+
+    # ---- flags
+    def _n(self, fn, *args):
+        c = C.c_uint32()
+        check(getattr(lib(), fn)(self._h, *args, C.byref(c)), fn)
+        return c.value
+
+    def set_flags(self, flags: int, depth: int = LEAF) -> int:
+        return self._n("b12g_set_flags", flags, depth)
+
+    def unset_flags(self, flags: int, depth: int = LEAF) -> int:
+        return self._n("b12g_unset_flags", flags, depth)
+
+    def change_flags(self, to_unset: int, to_set: int, depth: int = LEAF) -> int:
+        return self._n("b12g_change_flags", to_unset, to_set, depth)
+
+    # ---- structure
+    def subdivide(self, flags: int = L.SD) -> int:
+        return self._n("b12g_subdivide", flags)
+
+    def remove(self, flags: int) -> int:
+        return self._n("b12g_remove", flags)
+
+    def delete_depth(self, depth: int) -> int:
+        return self._n("b12g_delete_depth", depth)
+
+    # ---- box images
+    def set_flags_by_image(self, scheme: Scheme, flags: int, depth: int = LEAF) -> int:
+        s = scheme.to_c()
+        return self._n("b12g_set_flags_by_image", C.byref(s), flags, depth)
+
+    def search_by_image(self, scheme: Scheme, depth: int = LEAF) -> np.ndarray:
+        s = scheme.to_c()
+        n = C.c_uint64()
+        check(lib().b12g_search_by_image(self._h, C.byref(s), depth, None, 0, C.byref(n)), "search_by_image")
+        out = np.zeros(max(n.value, 1), dtype=np.uint32)
+        check(lib().b12g_search_by_image(self._h, C.byref(s), depth, out.ctypes.data, len(out), C.byref(n)),
+              "search_by_image")
+        return out[: n.value]
+
+    def insert_points(self, points, depth: int, flags_for_inserted: int = L.INS, flags_for_hit: int = L.NONE) -> int:
+        pts = np.ascontiguousarray(points, dtype=np.float64)
+        return self._n("b12g_insert_points", pts.ctypes.data, pts.size // self.dim, depth, flags_for_inserted,
+                       flags_for_hit)
+
+    def insert_by_image(self, scheme: Scheme, depth: int, flags_for_inserted: int = L.INS,
+                        flags_for_hit: int = L.NONE) -> int:
+        s = scheme.to_c()
+        return self._n("b12g_insert_by_image", C.byref(s), depth, flags_for_inserted, flags_for_hit)
+
+    def transition_matrix(self, scheme: Scheme, absolute: bool = False, invalid_column: bool = False,
+                          into: "CsrMatrix | None" = None) -> CsrMatrix:
+        """Build the matrix; `into` refills an existing matrix in place (no new device memory)."""
+        s = scheme.to_c()
+        h = C.c_void_p(into._h if into is not None else None)
+        check(lib().b12g_transition_matrix(self._h, C.byref(s), int(absolute), int(invalid_column), C.byref(h)),
+              "transition_matrix")
+        if into is not None:
+            into.__init__(h)
+            return into
+        return CsrMatrix(h)
+
+    # ---- measurement hooks
+    def stream_handle(self) -> int:
+        p = C.c_void_p()
+        check(lib().b12g_tree_stream(self._h, C.byref(p)), "tree_stream")
+        return p.value or 0
+
+    def profile(self, enable: bool = True) -> None:
+        check(lib().b12g_profile_enable(self._h, int(enable)), "profile_enable")
+
+    def profile_read(self, kind: int, reset: bool = True):
+        ms, n = C.c_double(), C.c_uint64()
+        check(lib().b12g_profile_read(self._h, kind, C.byref(ms), C.byref(n), int(reset)), "profile_read")
+        return ms.value, n.value
+
+    # ---- fused drivers
+    def subdivision_run(self, scheme: Scheme, steps: int) -> np.ndarray:
+        counts = np.zeros(max(steps, 1), dtype=np.uint32)
+        s = scheme.to_c()
+        check(lib().b12g_subdivision_run(self._h, C.byref(s), steps, counts.ctypes.data), "subdivision_run")
+        return counts[:steps]
+
+    def continuation_run(self, scheme: Scheme, x0, depth: int, max_sweeps: int = 100000) -> np.ndarray:
+        x0 = np.ascontiguousarray(x0, dtype=np.float64)
+        counts = np.zeros(max_sweeps, dtype=np.uint32)
+        k = C.c_uint32()
+        s = scheme.to_c()
+        check(lib().b12g_continuation_run(self._h, C.byref(s), x0.ctypes.data, x0.size // self.dim, depth,
+                                          max_sweeps, counts.ctypes.data, C.byref(k)), "continuation_run")
+        return counts[: k.value]
+
+    # ---- the reference's member names
+    setFlags = set_flags
+    unsetFlags = unset_flags
+    changeFlags = change_flags
+    deleteDepth = delete_depth
+    insertByPoints = insert_points
+
+    def setFlagsByIterators(self, scheme: Scheme, flags: int, depth: int = LEAF) -> int:
+        return self.set_flags_by_image(scheme, flags, depth)
+
+    def searchByIterators(self, scheme: Scheme, depth: int = LEAF) -> np.ndarray:
+        return self.search_by_image(scheme, depth)
+
+    def insertByIterators(self, scheme: Scheme, depth: int, flags_for_inserted: int = L.INS,
+                          flags_for_hit: int = L.NONE) -> int:
+        return self.insert_by_image(scheme, depth, flags_for_inserted, flags_for_hit)
+
+    def transitionMatrixForLeaves(self, grid: GridSpec, map_: MapSpec, use_absolute_values: bool = False,
+                                  use_invalid_nr_boxes: bool = False) -> CsrMatrix:
+        return self.transition_matrix(Scheme(map_, grid), use_absolute_values, use_invalid_nr_boxes)

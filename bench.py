@@ -1,0 +1,358 @@
+#!/usr/bin/env python
+"""Benchmark of the box-image path: Lorenz, depth 27, on B200.
+
+One step = one whole Lorenz job of the reference's subdivision driver
+(subdivision.m:18-45): 27 subdivision steps (sigma=10, rho=28, beta=8/3, RK4 h=0.01 x 20,
+5x5x5 inner grid, domain centre (0,0,27) radius (30,30,40)), the CSR transition matrix
+on the final boxes, and 200 FP64 power iterations for the invariant measure.
+
+metric = box-images per second (a box-image is one box's 125 test points sampled,
+integrated and located): the subdivision steps image 2*n(k-1) boxes each, the transition
+matrix n(27).  Inputs are synthetic: the workload is defined entirely by its parameters.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun (N > 1) every rank runs its own job (weak scaling, no collective on the
+data path); value = all ranks' box-images / the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+DEPTH = 27
+MEASURE_ITERS = 200
+P = 125
+FLOP_PER_POINT = 20 * 78          # RK4 step: 4 right-hand sides (9 FLOP) + 42 update FLOP
+METRIC = "Lorenz box-images/s"
+UNIT = "box-images/s"
+CONFIG = {"workload": "lorenz-rk4-depth27", "sigma": 10.0, "rho": 28.0, "beta": 8.0 / 3.0, "h": 0.01,
+          "rk4_steps": 20, "grid": "inner 5x5x5", "depth": DEPTH, "tm": "csr", "measure_iters": MEASURE_ITERS,
+          "l2": "flushed between timed steps (256 MiB write)", "arith": "strict"}
+NOMINAL_FP64_TFLOPS = 37.0
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ------------------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------------------ CPU arms
+def reference_binary():
+    exe = os.path.join(REPO, "oracle", "_ref", "ref_lorenz")
+    return exe if os.path.exists(exe) else None
+
+
+def cpu_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def run_reference_sample(steps: int, buf: int, threads: int):
+    """The reference's own Thrust code (OMP backend) on the Lorenz subdivision loop."""
+    exe = reference_binary()
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    res = subprocess.run([exe, "--steps", str(steps), "--buf", str(buf), "--tm", "0"], env=env, check=True,
+                         capture_output=True, text=True)
+    rec = json.loads(res.stdout.strip().splitlines()[-1])
+    return rec["box_images"], rec["subdivision_s"], rec
+
+
+def run_port_sample(steps: int):
+    """The oracle restatement (OpenMP C) on the same loop, when the reference build is absent."""
+    from oracle import oracle as O
+    o = O.Oracle(O.lorenz_spec())
+    t0 = time.perf_counter()
+    _, bi = o.subdivision(steps)
+    return bi, time.perf_counter() - t0, {}
+
+
+CPU_SAMPLE_STEPS = 24
+CPU_SAMPLE_BUF = 1 << 30
+
+
+def cpu_baseline(threads: int):
+    if reference_binary():
+        bi, sec, _ = run_reference_sample(CPU_SAMPLE_STEPS, CPU_SAMPLE_BUF, threads)
+        kind = "reference"
+    else:
+        from oracle import oracle as O
+        threads = O.lib().orc_num_threads()
+        bi, sec, _ = run_port_sample(CPU_SAMPLE_STEPS)
+        kind = "port"
+    return {"value": bi / sec, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"Lorenz subdivision steps 1-{CPU_SAMPLE_STEPS} ({bi} box-images, {sec:.2f} s"
+                      + (f", nHostBufferBytes {CPU_SAMPLE_BUF >> 20} MiB, OMP backend)" if kind == "reference"
+                         else ", OpenMP C restatement)")}
+
+
+def reference_arm(args, rank: int, world: int):
+    if rank != 0:
+        return 0
+    threads = cpu_cores()
+    kind = "reference" if reference_binary() else "port"
+    samples = []
+    for i in range(args.warmup + args.steps):
+        if kind == "reference":
+            bi, sec, _ = run_reference_sample(CPU_SAMPLE_STEPS, CPU_SAMPLE_BUF, threads)
+        else:
+            bi, sec, _ = run_port_sample(CPU_SAMPLE_STEPS)
+        if i >= args.warmup:
+            samples.append((bi, sec))
+    tot_bi = sum(s[0] for s in samples)
+    tot_s = sum(s[1] for s in samples)
+    value = tot_bi / tot_s
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * tot_s / len(samples), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": dict(CONFIG, sample=f"subdivision steps 1-{CPU_SAMPLE_STEPS} per step"),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                             "sample": f"Lorenz subdivision steps 1-{CPU_SAMPLE_STEPS} per step, "
+                                       f"{tot_bi // len(samples)} box-images, nHostBufferBytes "
+                                       f"{CPU_SAMPLE_BUF >> 20} MiB, Thrust OMP backend"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------------------ GPU arm
+def box_images_of(counts) -> tuple[int, int]:
+    prev = np.concatenate([[1], counts[:-1]]).astype(np.int64)
+    return int(2 * prev.sum()), int(counts[-1])
+
+
+def gpu_arm(args, rank: int, world: int, dist):
+    import torch
+    import b12_b200 as B
+    from b12_b200 import tree as T
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    sc = B.Scheme(B.lorenz(rho=28.0, fma=args.fma), B.inner_grid(5))
+    tree = B.ImplicitBoxTree([0.0, 0.0, 27.0], [30.0, 30.0, 40.0])
+    tree.reserve(1 << 20)
+    stream = torch.cuda.ExternalStream(tree.stream_handle(), device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    csr = None
+
+    def job(profile: bool):
+        nonlocal csr
+        tree.delete_depth(0)
+        counts = tree.subdivision_run(sc, DEPTH)
+        csr = tree.transition_matrix(sc, into=csr)
+        csr.invariant_measure(MEASURE_ITERS, keep_on_device=True)
+        return counts
+
+    # FP64 roofline denominator, measured on this device
+    peak_tflops, _ = T.probe_fp64_fma(0.25)
+
+    counts = None
+    for _ in range(args.warmup):
+        counts = job(False)
+    bi_sub, n_final = box_images_of(counts)
+    box_images = bi_sub + n_final
+
+    tree.profile(True)
+    tree.profile_read(0)
+    tree.profile_read(1)
+    launches0 = T.launch_count()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(dev) as clocks:
+        for i in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                ev[i][0].record(stream)
+            c = job(True)
+            with torch.cuda.stream(stream):
+                ev[i][1].record(stream)
+            if list(c) != list(counts):
+                raise RuntimeError("box counts changed between steps")
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    launches = T.launch_count() - launches0
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = sum(step_ms)
+    img_ms, img_n = tree.profile_read(0)
+    row_ms, row_n = tree.profile_read(1)
+    tree.profile(False)
+
+    if dist:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * args.steps * box_images / (total_ms * 1e-3)
+
+    # dominant kernel: the fused box-image kernel (subdivision steps)
+    flops_img = args.steps * bi_sub * P * FLOP_PER_POINT
+    achieved = flops_img / (img_ms * 1e-3) / 1e12 if img_ms > 0 else None
+    flops_rows = args.steps * n_final * P * FLOP_PER_POINT
+    rows_tflops = flops_rows / (row_ms * 1e-3) / 1e12 if row_ms > 0 else None
+
+    # end to end through the public API: results copied to pinned host memory each step
+    if True:
+        codes = torch.empty(n_final, dtype=torch.int64, pin_memory=True).numpy().view(np.uint64)
+        depth = torch.empty(n_final, dtype=torch.uint8, pin_memory=True).numpy()
+        flags = torch.empty(n_final, dtype=torch.uint8, pin_memory=True).numpy()
+        rowptr = torch.empty(n_final + 1, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+        cols = torch.empty(max(csr.nnz, 1), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+        vals = torch.empty(max(csr.nnz, 1), dtype=torch.float64, pin_memory=True).numpy()
+        meas = torch.empty(n_final, dtype=torch.float64, pin_memory=True).numpy()
+        root = (np.zeros(1, np.uint64), np.zeros(1, np.uint8), np.zeros(1, np.uint8))
+        h2d = 8 + 1 + 1
+        d2h = codes.nbytes + depth.nbytes + flags.nbytes + rowptr.nbytes + cols.nbytes + vals.nbytes + meas.nbytes
+        e2e_steps = max(1, min(args.steps, 5))
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            tree.load_leaves(*root)                       # the job's input: the surrounding box
+            tree.subdivision_run(sc, DEPTH)
+            csr = tree.transition_matrix(sc, into=csr)
+            csr.invariant_measure(MEASURE_ITERS, out=meas)
+            lib_leaves(tree, codes, depth, flags)
+            csr.to_host_into(rowptr, cols, vals)
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t0
+        if dist:
+            t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        e2e = {"value": world * e2e_steps * box_images / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": int(d2h), "steps": e2e_steps, "timer": "host wall clock, synchronous API"}
+
+    cpu = cpu_baseline(cpu_cores()) if (rank == 0 and world == 1 and not args.no_cpu) else None
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": dict(CONFIG, arith="fma" if args.fma else "strict",
+                               parallelism=f"{world} independent jobs" if world > 1 else "1 job",
+                               box_images_per_step=box_images, final_boxes=n_final, nnz=csr.nnz),
+                "e2e": e2e, "gpu_launches": int(launches),
+                "roofline": {"bound": "fp64", "kernel": "image_points_kernel (fused sample/RK4/locate)",
+                             "achieved": achieved, "peak": peak_tflops, "unit": "TFLOP/s",
+                             "frac": (achieved / peak_tflops) if achieved else None, "traffic": None,
+                             "peak_source": "measured: FP64 FMA-chain probe kernel on this device "
+                                            f"(nominal {NOMINAL_FP64_TFLOPS} TFLOP/s)",
+                             "flop_per_box_image": P * FLOP_PER_POINT, "launches": img_n,
+                             "kernel_ms_per_step": img_ms / args.steps,
+                             "transition_rows_tflops": rows_tflops},
+                "clocks": clocks.summary(), "cpu_baseline": cpu,
+                "counts": [int(c) for c in counts]}
+        print(json.dumps(line), flush=True)
+    tree.close()
+    return 0
+
+
+def lib_leaves(tree, codes, depth, flags):
+    from b12_b200._lib import check, lib
+    check(lib().b12g_leaves(tree._h, codes.ctypes.data, depth.ctypes.data, flags.ctypes.data), "leaves")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--fma", action="store_true", help="explicit-FMA integrator arithmetic")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        return reference_arm(args, rank, world)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as D
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        D.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = D
+    try:
+        return gpu_arm(args, rank, world, dist)
+    finally:
+        if dist:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,222 @@
+/*
+ * b12g - B200-native (sm_100a) box-image path of an implicit box tree.
+ *
+ * C ABI of libb12g.so.  It replaces, for the set-oriented box-image path, the
+ * reference's C++ template class ImplicitBoxTree<A,DIM,REAL,N>
+ * (B12c/src/include/ImplicitBoxTree.h:32-640) and the Matlab MEX dispatcher that binds
+ * it (B12c/src/matlab/general_implicit_box_tree_interface_mex.hpp.in:21-1858).  Each
+ * entry point below cites the reference member function it stands in for.
+ *
+ * Conventions
+ *   - Every call returns a b12g_status; B12G_OK == 0.  b12g_last_error() gives a
+ *     human-readable reason for the last failure on the calling thread.
+ *   - A tree lives on one GPU (the device current at b12g_tree_create) and owns one
+ *     CUDA stream.  Calls on one tree are not thread-safe (as in the reference);
+ *     different trees may be used from different threads.
+ *   - Depth is uint8_t as in the reference (TypeDefinitions.h:19-57): 255 means
+ *     "leaves" (getLeafDepth), 254 "unsubdividable" (not supported here).
+ *   - Leaf index results use 0xFFFFFFFF for "not found" (getInvalidNrBoxes).
+ *   - Flags are the reference's 8-bit flags (Flags.h:10-23).
+ *   - All leaves of a tree share one depth.  Operations whose reference result would
+ *     mix depths return B12G_ERR_UNSUPPORTED_MIXED_DEPTH and leave the tree unchanged.
+ *   - Host pointers are plain host memory (pinned or pageable); the library owns all
+ *     device memory of a tree and of a CSR matrix.
+ */
+#ifndef B12G_H
+#define B12G_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define B12G_MAX_DIM 4
+#define B12G_LEAF_DEPTH 255u
+#define B12G_INVALID_INDEX 0xFFFFFFFFu
+
+typedef enum {
+  B12G_OK = 0,
+  B12G_ERR_INVALID = 1,                 /* bad argument */
+  B12G_ERR_OOM = 2,                     /* device allocation failed */
+  B12G_ERR_CUDA = 3,                    /* CUDA runtime error (see b12g_last_error) */
+  B12G_ERR_TIMEOUT = 4,                 /* a bounded device-side wait gave up */
+  B12G_ERR_UNSUPPORTED_MIXED_DEPTH = 5, /* result would mix leaf depths */
+  B12G_ERR_CAPACITY = 6,                /* a size limit of the call was exceeded */
+  B12G_ERR_NO_DEVICE = 7                /* no CUDA device / kernels not loadable */
+} b12g_status;
+
+/* Flags.h:10-23 */
+enum {
+  B12G_NONE = 0x00, B12G_HIT = 0x01, B12G_INS = 0x02, B12G_EXPD = 0x04, B12G_SD = 0x08,
+  B12G_EQU = 0x10, B12G_ENTR = 0x20, B12G_EXTR = 0x40, B12G_ALL = 0xFF
+};
+
+/* map functors (reference: Map_Henon.h, Map_Lorenz.h, MapTools.hpp; the coupled and
+ * forced Duffing maps are user plug-ins in the reference's sense, B12_doc.tex:107-146) */
+typedef enum {
+  B12G_MAP_HENON = 1,           /* p = {a, b}; steps = iterates (IteratingMap) */
+  B12G_MAP_LORENZ = 2,          /* p = {sigma, rho, beta}; h, steps (RK4Auto) */
+  B12G_MAP_COUPLED_DUFFING = 3, /* h, steps (SymplecticIntegratorAuto, order 2) */
+  B12G_MAP_FORCED_DUFFING = 4   /* p = {delta, alpha, beta, gamma}; h = period/steps */
+} b12g_map_kind;
+
+typedef enum {
+  B12G_ARITH_STRICT = 0,        /* every FP64 op rounded separately (reference -fmad=false) */
+  B12G_ARITH_FMA = 1            /* explicit fused multiply-adds (Lorenz only) */
+} b12g_arith;
+
+typedef enum {
+  B12G_GRID_INNER = 1,          /* InnerGrid(n): n^DIM cell-centre points (Grids.hpp:103-134) */
+  B12G_GRID_FULL = 2,           /* FullGrid(n, eps) (Grids.hpp:60-95) */
+  B12G_GRID_PHILOX = 3          /* `points` uniform points from Philox4x32-10 keyed by (seed, point index) */
+} b12g_grid_kind;
+
+typedef struct {
+  uint32_t dim;                 /* 1..B12G_MAX_DIM */
+  uint32_t pad;
+  double center[B12G_MAX_DIM];
+  double radius[B12G_MAX_DIM];
+} b12g_domain;
+
+typedef struct {
+  uint32_t kind;                /* b12g_map_kind */
+  uint32_t arith;               /* b12g_arith */
+  uint32_t steps;
+  uint32_t pad;
+  double h;
+  double p[6];
+} b12g_map;
+
+typedef struct {
+  uint32_t kind;                /* b12g_grid_kind */
+  uint32_t n;                   /* points per dimension (inner, full) */
+  uint64_t points;              /* points per box (philox) */
+  uint64_t seed;                /* philox key */
+  double eps;                   /* full grid stretch */
+} b12g_grid;
+
+/* A "scheme" is the Matlab driver's {grid, map, depth, flags} cell
+ * (subdivision.m:5, continuation.m:24): the point iterator of
+ * makePointIteratorPairOverLeaves / makePointIteratorPairByFlags
+ * (ImplicitBoxTree.hpp:2167-2196, 2303-2341). */
+typedef struct {
+  b12g_map map;
+  b12g_grid grid;
+  uint8_t depth;                /* source depth; 255 = leaves */
+  uint8_t flags_to_check;       /* only boxes with all these flags are mapped (0 = all) */
+  uint8_t pad[6];
+} b12g_scheme;
+
+typedef struct b12g_tree b12g_tree;
+typedef struct b12g_csr b12g_csr;
+
+/* ---- library ---------------------------------------------------------------- */
+const char* b12g_last_error(void);
+const char* b12g_version(void);
+
+/* ---- construction (ImplicitBoxTree.hpp:122-128, 28-45) ------------------------ */
+/* ImplicitBoxTree(center, radius): one leaf, the surrounding box (0, depth 0, NONE) */
+b12g_status b12g_tree_create(const b12g_domain* domain, b12g_tree** tree);
+b12g_status b12g_tree_destroy(b12g_tree* tree);
+/* reserve device capacity for `n_boxes` leaves (optional; trees grow on demand) */
+b12g_status b12g_tree_reserve(b12g_tree* tree, uint64_t n_boxes);
+
+/* ---- queries ------------------------------------------------------------------ */
+/* count(depth) (ImplicitBoxTree.hpp:1061-1095) */
+b12g_status b12g_count(b12g_tree* tree, uint8_t depth, uint32_t* count);
+/* depth() (ImplicitBoxTree.hpp:1265-1271) */
+b12g_status b12g_depth(b12g_tree* tree, uint8_t* depth);
+/* the leaves in tree order: codes, depths, flags (host arrays of count(255) entries;
+ * any pointer may be NULL).  Mirrors getBitPatternVector/getDepthVector/getFlagsVector. */
+b12g_status b12g_leaves(b12g_tree* tree, uint64_t* codes, uint8_t* depths, uint8_t* flags);
+/* replace the leaves (sorted, unique, one depth) - the load half of save/load */
+b12g_status b12g_load_leaves(b12g_tree* tree, const uint64_t* codes, const uint8_t* depths,
+                             const uint8_t* flags, uint32_t n);
+
+/* ---- flags (ImplicitBoxTree.hpp:2684-2688, 3208-3411, 787-1058) ----------------- */
+/* setFlags(flags, depth): returns the number of boxes that did not have them */
+b12g_status b12g_set_flags(b12g_tree* tree, uint8_t flags, uint8_t depth, uint32_t* n_changed);
+/* unsetFlags(flags, depth): returns the number of boxes that had any of them */
+b12g_status b12g_unset_flags(b12g_tree* tree, uint8_t flags, uint8_t depth, uint32_t* n_changed);
+/* changeFlags(to_unset, to_set, depth): boxes with all of to_unset get them replaced */
+b12g_status b12g_change_flags(b12g_tree* tree, uint8_t to_unset, uint8_t to_set, uint8_t depth,
+                              uint32_t* n_changed);
+
+/* ---- structure ------------------------------------------------------------------ */
+/* subdivide(flags) (ImplicitBoxTree.hpp:2884-2930) */
+b12g_status b12g_subdivide(b12g_tree* tree, uint8_t flags, uint32_t* n_subdivided);
+/* remove(flags): drop leaves that do NOT have all `flags` (ImplicitBoxTree.hpp:2344-2371) */
+b12g_status b12g_remove(b12g_tree* tree, uint8_t flags, uint32_t* n_removed);
+/* deleteDepth(depth) (ImplicitBoxTree.hpp:1217-1228); depth 0 and 255 supported */
+b12g_status b12g_delete_depth(b12g_tree* tree, uint8_t depth, uint32_t* n_deleted);
+
+/* ---- box images -------------------------------------------------------------------- */
+/* setFlagsByIterators(makePointIteratorPair...(scheme), flags, depth)
+ * (ImplicitBoxTree.hpp:2691-2694 via searchCompacted 2624-2681 and setFlagsBySearch 2717-2775) */
+b12g_status b12g_set_flags_by_image(b12g_tree* tree, const b12g_scheme* scheme, uint8_t flags, uint8_t depth,
+                                    uint32_t* n_changed);
+/* searchByIterators(makePointIteratorPair...(scheme), depth) (ImplicitBoxTree.hpp:2375-2432):
+ * one leaf index per mapped point, point index = source rank * points per box + grid index.
+ * `out` is a host array of `capacity` entries; *n_points receives the number of points. */
+b12g_status b12g_search_by_image(b12g_tree* tree, const b12g_scheme* scheme, uint8_t depth,
+                                 uint32_t* out, uint64_t capacity, uint64_t* n_points);
+/* insertByPoints(points, depth, ins, hit) (ImplicitBoxTree.hpp:1927-1946); points are
+ * n_points x dim doubles, row-major */
+b12g_status b12g_insert_points(b12g_tree* tree, const double* points, uint64_t n_points, uint8_t depth,
+                               uint8_t flags_for_inserted, uint8_t flags_for_hit, uint32_t* n_inserted);
+/* insertByIterators(makePointIteratorPairByFlags(scheme), depth, ins, hit)
+ * (ImplicitBoxTree.hpp:1615-1910) */
+b12g_status b12g_insert_by_image(b12g_tree* tree, const b12g_scheme* scheme, uint8_t depth,
+                                 uint8_t flags_for_inserted, uint8_t flags_for_hit, uint32_t* n_inserted);
+
+/* ---- transition matrix (ImplicitBoxTree.hpp:2934-3193, CooMatrix.hpp:14-56) ---------- */
+/* transitionMatrixForLeaves<double>(grid, map, absolute, rowMajor=true, invalid):
+ * row = source leaf, column = target leaf, value = count (absolute) or count / P.
+ * The result is a row-major CSR that stays on the device.  *csr must be NULL (a new
+ * matrix is created) or a matrix from an earlier call, which is refilled in place. */
+b12g_status b12g_transition_matrix(b12g_tree* tree, const b12g_scheme* scheme, int absolute,
+                                   int invalid_column, b12g_csr** csr);
+b12g_status b12g_csr_shape(const b12g_csr* csr, uint32_t* n_rows, uint32_t* n_cols, uint64_t* nnz);
+/* copy to host: rowptr[n_rows+1], cols[nnz], vals[nnz] (any may be NULL) */
+b12g_status b12g_csr_copy(const b12g_csr* csr, uint32_t* rowptr, uint32_t* cols, double* vals);
+b12g_status b12g_csr_destroy(b12g_csr* csr);
+/* invariant measure: v <- P^T v / |P^T v|_1, `iters` times from the uniform vector,
+ * FP64 (the eigenvector step of subdivisionByNim.m:30-58).  v: host array of n_rows,
+ * or NULL to keep the result on the device (b12g_csr_measure copies it later). */
+b12g_status b12g_invariant_measure(b12g_csr* csr, uint32_t iters, double* v);
+/* copy the last invariant measure of `csr` to the host array v (n_rows entries) */
+b12g_status b12g_csr_measure(const b12g_csr* csr, double* v);
+
+/* ---- fused drivers ------------------------------------------------------------------- */
+/* The subdivision loop of B12_doc.tex:269-290 / subdivision.m:18-45,
+ *   setFlags(SD); repeat steps: subdivide(SD); setFlagsByIterators(scheme, HIT);
+ *   remove(HIT); unsetFlags(HIT)
+ * run on the device without host round trips.  counts[k] = leaves after step k+1
+ * (host array of `steps` entries, may be NULL). */
+b12g_status b12g_subdivision_run(b12g_tree* tree, const b12g_scheme* scheme, uint32_t steps, uint32_t* counts);
+/* The continuation loop of continuation.m:13-44 at one depth: deleteDepth(0);
+ * insertByPoints(x0, depth, INS); repeat { changeFlags(INS, EXPD); insert(scheme on
+ * EXPD boxes, INS); unsetFlags(EXPD) } until the count stops growing (or max_sweeps).
+ * counts: host array of max_sweeps entries (may be NULL); *n_sweeps receives the sweeps. */
+b12g_status b12g_continuation_run(b12g_tree* tree, const b12g_scheme* scheme, const double* x0, uint64_t n_x0,
+                                  uint8_t depth, uint32_t max_sweeps, uint32_t* counts, uint32_t* n_sweeps);
+
+/* ---- measurement hooks (no counterpart in the reference) ---------------------------------- */
+/* the CUDA stream (cudaStream_t) every kernel of this tree runs on */
+b12g_status b12g_tree_stream(b12g_tree* tree, void** stream);
+/* time every box-image (kind 0) and transition-row (kind 1) kernel launch with CUDA
+ * events on the tree's stream; read the accumulated device milliseconds and launches */
+b12g_status b12g_profile_enable(b12g_tree* tree, int enable);
+b12g_status b12g_profile_read(b12g_tree* tree, uint32_t kind, double* ms_total, uint64_t* launches, int reset);
+/* kernels this process has launched through the library (graph replays included) */
+b12g_status b12g_launch_count(uint64_t* launches);
+/* FP64 fused multiply-add throughput of the current device (TFLOP/s, FMA = 2 FLOPs),
+ * measured with a launch of about `seconds_hint` seconds */
+b12g_status b12g_probe_fp64_fma(double seconds_hint, double* tflops, double* seconds);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* B12G_H */

@@ -1,0 +1,665 @@
+/*
+ * ORACLE - test infrastructure only (see b12_oracle.h).
+ *
+ * Plain-C restatement of the reference's box-image path.  Every function cites the
+ * reference file:line it restates (paths relative to B12c/src/include unless noted).
+ * Build: gcc -O2 -fopenmp -ffp-contract=off -fPIC -shared (oracle/Makefile).
+ */
+#include "b12_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define NONE_FLAGS 0u
+#define INVALID_CODE (~(uint64_t)0)
+
+int orc_num_threads(void)
+{
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+/* safeLeftShift / safeRightShift for 64-bit patterns (BitPattern.hpp:3-28) */
+static inline uint64_t sls(uint64_t b, int i) { return i <= 0 ? b : (i >= 64 ? 0 : b << i); }
+static inline uint64_t srs(uint64_t b, int i) { return i <= 0 ? b : (i >= 64 ? 0 : b >> i); }
+
+/* ------------------------------------------------------------------------------
+ * grids (Grids.hpp:12-162)
+ * ---------------------------------------------------------------------------- */
+static uint64_t ipow_u64(uint64_t b, uint32_t e)
+{
+  uint64_t r = 1;
+  while (e--) r *= b;
+  return r;
+}
+
+/* getNumberOfPointsPerBox (Grids.hpp:79-83, 131-134, 158-162) */
+uint64_t orc_grid_points_per_box(const orc_grid* g, uint32_t dim)
+{
+  return g->kind == ORC_GRID_PHILOX ? g->points : ipow_u64(g->n, dim);
+}
+
+/* Philox4x32-10 (Salmon et al., SC'11): published round multipliers and Weyl steps */
+void orc_philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1)
+{
+  for (int r = 0; r < 10; ++r) {
+    if (r > 0) { k0 += 0x9E3779B9u; k1 += 0xBB67AE85u; }
+    const uint64_t p0 = (uint64_t)0xD2511F53u * c[0];
+    const uint64_t p1 = (uint64_t)0xCD9E8D57u * c[2];
+    const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c[1] ^ k0;
+    const uint32_t n2 = (uint32_t)(p0 >> 32) ^ c[3] ^ k1;
+    c[0] = n0; c[1] = (uint32_t)p1; c[2] = n2; c[3] = (uint32_t)p0;
+  }
+}
+
+static inline double philox_signed(uint32_t hi, uint32_t lo)
+{
+  const uint64_t m = (((uint64_t)hi << 32) | (uint64_t)lo) >> 11;
+  return 2.0 * ((double)m * 0x1p-53) - 1.0;
+}
+
+void orc_grid_point(const orc_grid* g, uint32_t dim, uint64_t i, double* res)
+{
+  if (g->kind == ORC_GRID_INNER) {
+    /* InnerGrid::operator() (Grids.hpp:105-120) */
+    const uint64_t n = g->n;
+    uint64_t tmp = 1;
+    for (uint32_t j = 0; j < dim; ++j) {
+      res[j] = (((double)((i / tmp) % n) * 2.0 + 1.0) - (double)n) / (double)n;
+      tmp *= n;
+    }
+  } else if (g->kind == ORC_GRID_FULL) {
+    /* FullGrid::operator() (Grids.hpp:67-83) */
+    const uint64_t n = g->n;
+    uint64_t tmp = 1;
+    for (uint32_t j = 0; j < dim; ++j) {
+      res[j] = ((double)((i / tmp) % n) * 2.0) / (double)(n - 1) - 1.0;
+      res[j] *= 1.0 + g->eps;
+      tmp *= n;
+    }
+  } else {
+    /* Philox plug-in keyed by (seed, global point index), replacing UniformGrid
+     * (Grids.hpp:143-162), whose host and device generators differ */
+    for (uint32_t j = 0; j < dim; j += 2) {
+      uint32_t c[4] = {(uint32_t)i, (uint32_t)(i >> 32), j / 2, 0u};
+      orc_philox4x32_10(c, (uint32_t)g->seed, (uint32_t)(g->seed >> 32));
+      res[j] = philox_signed(c[0], c[1]);
+      if (j + 1 < dim) res[j + 1] = philox_signed(c[2], c[3]);
+    }
+  }
+}
+
+/* ------------------------------------------------------------------------------
+ * maps
+ * ---------------------------------------------------------------------------- */
+/* HenonMap (Map_Henon.h:11-24) */
+static inline void henon(const double* p, double a, double b, double* r)
+{
+  r[0] = (1.0 - (a * p[0]) * p[0]) + p[1];
+  r[1] = b * p[0];
+}
+
+/* LorenzRHS (Map_Lorenz.h:10-24) */
+static inline void lorenz_rhs(const double* s, const double* p, double* r)
+{
+  r[0] = s[0] * (p[1] - p[0]);
+  r[1] = (s[1] * p[0] - p[1]) - p[0] * p[2];
+  r[2] = (-s[2]) * p[2] + p[0] * p[1];
+}
+
+static inline void lorenz_rhs_fma(const double* s, const double* p, double* r)
+{
+  r[0] = s[0] * (p[1] - p[0]);
+  r[1] = fma(-p[0], p[2], fma(s[1], p[0], -p[1]));
+  r[2] = fma(p[0], p[1], (-s[2]) * p[2]);
+}
+
+/* RK4Auto::operator() (MapTools.hpp:118-182) with the Lorenz right-hand side */
+static void lorenz_map(const orc_map* m, const double* x0, double* res)
+{
+  double x[3] = {x0[0], x0[1], x0[2]}, k[3], a[3];
+  const double h = m->h;
+  for (uint32_t s = 0; s < m->steps; ++s) {
+    if (!m->fma) {
+      lorenz_rhs(m->p, x, k);
+      for (int j = 0; j < 3; ++j) res[j] = x[j] + (h / 6.0) * k[j];
+      for (int j = 0; j < 3; ++j) a[j] = x[j] + (h / 2.0) * k[j];
+      lorenz_rhs(m->p, a, k);
+      for (int j = 0; j < 3; ++j) res[j] += (h / 3.0) * k[j];
+      for (int j = 0; j < 3; ++j) a[j] = x[j] + (h / 2.0) * k[j];
+      lorenz_rhs(m->p, a, k);
+      for (int j = 0; j < 3; ++j) res[j] += (h / 3.0) * k[j];
+      for (int j = 0; j < 3; ++j) a[j] = x[j] + h * k[j];
+      lorenz_rhs(m->p, a, k);
+      for (int j = 0; j < 3; ++j) res[j] += (h / 6.0) * k[j];
+    } else {
+      const double h6 = h / 6.0, h3 = h / 3.0, h2 = h / 2.0;
+      lorenz_rhs_fma(m->p, x, k);
+      for (int j = 0; j < 3; ++j) { res[j] = fma(h6, k[j], x[j]); a[j] = fma(h2, k[j], x[j]); }
+      lorenz_rhs_fma(m->p, a, k);
+      for (int j = 0; j < 3; ++j) { res[j] = fma(h3, k[j], res[j]); a[j] = fma(h2, k[j], x[j]); }
+      lorenz_rhs_fma(m->p, a, k);
+      for (int j = 0; j < 3; ++j) { res[j] = fma(h3, k[j], res[j]); a[j] = fma(h, k[j], x[j]); }
+      lorenz_rhs_fma(m->p, a, k);
+      for (int j = 0; j < 3; ++j) res[j] = fma(h6, k[j], res[j]);
+    }
+    for (int j = 0; j < 3; ++j) x[j] = res[j];
+  }
+}
+
+/* SymplecticIntegratorAuto order 2 (MapTools.hpp:371-421) with the coupled-Duffing
+ * right-hand sides: RHS1(p) = p, RHS2(q) = -grad V(q) */
+static void coupled_duffing_map(const orc_map* m, const double* x0, double* res)
+{
+  double t[2];
+  const double h = m->h;
+  for (int j = 0; j < 4; ++j) res[j] = x0[j];
+  for (uint32_t s = 0; s < m->steps; ++s) {
+    t[0] = res[2]; t[1] = res[3];
+    for (int j = 0; j < 2; ++j) res[j] += (0.5 * t[j]) * h;
+    t[0] = (res[0] - (res[0] * res[0]) * res[0]) - ((0.2 * res[0]) * res[1]) * res[1];
+    t[1] = (-1.69 * res[1]) - ((0.2 * res[0]) * res[0]) * res[1];
+    for (int j = 0; j < 2; ++j) res[2 + j] += t[j] * h;
+    t[0] = res[2]; t[1] = res[3];
+    for (int j = 0; j < 2; ++j) res[j] += (0.5 * t[j]) * h;
+  }
+}
+
+/* forced Duffing: exactly `steps` RK4 steps (the classical RK4 of MapTools.hpp:42-108
+ * with the stage forcing read from a host cos table) */
+static inline void forced_rhs(const double* q, double c, const double* p, double* r)
+{
+  r[0] = p[1];
+  r[1] = (((-q[0] * p[1]) - q[1] * p[0]) - q[2] * ((p[0] * p[0]) * p[0])) + q[3] * c;
+}
+
+static void forced_duffing_map(const orc_map* m, const double* x0, double* res)
+{
+  const double h = m->h, h6 = h / 6.0, h3 = h / 3.0, h2 = h / 2.0;
+  double x[2] = {x0[0], x0[1]}, k[2], a[2];
+  for (uint32_t s = 0; s < m->steps; ++s) {
+    const double c0 = m->table[2 * s], c1 = m->table[2 * s + 1], c2 = m->table[2 * s + 2];
+    forced_rhs(m->p, c0, x, k);
+    for (int j = 0; j < 2; ++j) { res[j] = x[j] + h6 * k[j]; a[j] = x[j] + h2 * k[j]; }
+    forced_rhs(m->p, c1, a, k);
+    for (int j = 0; j < 2; ++j) { res[j] += h3 * k[j]; a[j] = x[j] + h2 * k[j]; }
+    forced_rhs(m->p, c1, a, k);
+    for (int j = 0; j < 2; ++j) { res[j] += h3 * k[j]; a[j] = x[j] + h * k[j]; }
+    forced_rhs(m->p, c2, a, k);
+    for (int j = 0; j < 2; ++j) { res[j] += h6 * k[j]; x[j] = res[j]; }
+  }
+}
+
+void orc_forced_duffing_table(uint32_t steps, double period, double* table)
+{
+  for (uint32_t j = 0; j <= 2 * steps; ++j) table[j] = cos((double)j * (period / (double)(2 * steps)));
+}
+
+void orc_map_apply(const orc_map* m, const double* x, double* res)
+{
+  switch (m->kind) {
+    case ORC_MAP_HENON: {
+      /* IteratingMap (MapTools.hpp:10-32) */
+      uint32_t i = 0;
+      double tmp[2];
+      if (m->steps & 1u) { henon(x, m->p[0], m->p[1], res); i = 1; }
+      else { res[0] = x[0]; res[1] = x[1]; }
+      for (; i < m->steps; i += 2) { henon(res, m->p[0], m->p[1], tmp); henon(tmp, m->p[0], m->p[1], res); }
+      break;
+    }
+    case ORC_MAP_LORENZ: lorenz_map(m, x, res); break;
+    case ORC_MAP_COUPLED_DUFFING: coupled_duffing_map(m, x, res); break;
+    case ORC_MAP_FORCED_DUFFING: forced_duffing_map(m, x, res); break;
+    default: break;
+  }
+}
+
+/* ------------------------------------------------------------------------------
+ * geometry (coordinateFunctions.hpp)
+ * ---------------------------------------------------------------------------- */
+/* computeCoordinatesOfBoxFixedSdScheme (coordinateFunctions.hpp:130-159) */
+void orc_box_coordinates(const orc_domain* d, uint64_t code, uint32_t depth, double* center, double* radius)
+{
+  const int D = (int)d->dim;
+  for (int j = 0; j < D; ++j) {
+    uint64_t bits = 0;
+    const int initialShift = (D + (int)depth - 1 - j) % D;
+    for (int i = 0; i * D < 64; ++i)
+      bits |= srs(code, i * (D - 1) + initialShift) & sls(1, i);
+    const int k = (int)depth / D + (j < (int)depth % D ? 1 : 0);
+    radius[j] = ldexp(d->radius[j], -k);
+    center[j] = ((ldexp((double)bits, -k) * 2.0 - 1.0) * d->radius[j] + d->center[j]) + radius[j];
+  }
+}
+
+/* isPointInBox + computeBoxFromPointFixedSdScheme (coordinateFunctions.hpp:9-19, 63-93) */
+int orc_point_code64(const orc_domain* d, const double* p, uint64_t* code64)
+{
+  const int D = (int)d->dim;
+  for (int j = 0; j < D; ++j)
+    if (!(d->center[j] - d->radius[j] <= p[j] && p[j] < d->center[j] + d->radius[j])) {
+      *code64 = INVALID_CODE;
+      return 0;
+    }
+  uint64_t res = 0;
+  for (int j = 0; j < D; ++j) {
+    const int m = 64 / D + (j < 64 % D ? 1 : 0);
+    const uint64_t bits = (uint64_t)floor(ldexp(((p[j] - d->center[j]) / d->radius[j] + 1.0) / 2.0, m));
+    const int initialShift = (63 - j) % D;
+    for (int i = 0; i * D + initialShift < 64; ++i)
+      res |= sls(bits, i * (D - 1) + initialShift) & sls(1, i * D + initialShift);
+  }
+  *code64 = res;
+  return 1;
+}
+
+/* ------------------------------------------------------------------------------
+ * tree order and search (Box.hpp:67-135, ImplicitBoxTree.hpp:2394-2432,
+ * Functors.hpp:289-315)
+ * ---------------------------------------------------------------------------- */
+static inline uint64_t comparable(uint64_t code, uint32_t depth)
+{
+  const int d = 64 - (int)depth;
+  return sls(code, d) | (sls(1, d - 1) - 1);
+}
+
+static inline int is_invalid_depth(uint32_t depth) { return depth > 64; }
+
+/* isStrictlyPreceding (Box.hpp:124-135) */
+static inline int strictly_preceding(uint64_t c1, uint32_t d1, uint64_t c2, uint32_t d2)
+{
+  if (is_invalid_depth(d1)) return 0;
+  if (is_invalid_depth(d2)) return 1;
+  const uint64_t b1 = comparable(c1, d1), b2 = comparable(c2, d2);
+  return b1 < b2 || (b1 == b2 && d2 < d1);
+}
+
+/* hasSamePath (Box.hpp:76-83) */
+static inline int same_path(uint64_t c1, uint32_t d1, uint64_t c2, uint32_t d2)
+{
+  const int diff = (int)d1 - (int)d2;
+  return (is_invalid_depth(d1) && is_invalid_depth(d2)) || srs(c1, diff) == srs(c2, -diff);
+}
+
+uint32_t orc_search(const orc_tree* t, uint64_t code64, int valid)
+{
+  const uint32_t pd = valid ? 64u : ORC_LEAF_DEPTH;
+  const uint64_t pc = valid ? code64 : INVALID_CODE;
+  /* thrust::lower_bound with IsStrictlyPrecedingFunctor */
+  uint64_t lo = 0, hi = t->n;
+  while (lo < hi) {
+    const uint64_t mid = lo + (hi - lo) / 2;
+    if (strictly_preceding(t->code[mid], t->depth[mid], pc, pd)) lo = mid + 1;
+    else hi = mid;
+  }
+  const uint32_t idx = (uint32_t)lo;
+  /* ComputeSearchIndexFunctor: candidates Box[max(idx-1,0)] and Box[min(idx,n-1)] */
+  const uint32_t a = idx > 0 ? idx - 1 : 0;
+  const uint32_t b = idx < t->n - 1 ? idx : (uint32_t)(t->n - 1);
+  if (pd >= t->depth[a] && same_path(pc, pd, t->code[a], t->depth[a])) return idx > 0 ? idx - 1 : 0;
+  if (pd >= t->depth[b] && same_path(pc, pd, t->code[b], t->depth[b])) return idx;
+  return ORC_INVALID;
+}
+
+/* ------------------------------------------------------------------------------
+ * tree storage
+ * ---------------------------------------------------------------------------- */
+static void tree_reserve(orc_tree* t, uint64_t cap)
+{
+  if (cap <= t->cap) return;
+  t->code = (uint64_t*)realloc(t->code, cap * 8);
+  t->depth = (uint8_t*)realloc(t->depth, cap);
+  t->flags = (uint8_t*)realloc(t->flags, cap);
+  t->cap = cap;
+}
+
+void orc_tree_init(orc_tree* t, const orc_domain* d)
+{
+  memset(t, 0, sizeof *t);
+  t->dom = *d;
+  tree_reserve(t, 16);
+  t->n = 1;
+  t->code[0] = 0;
+  t->depth[0] = 0;
+  t->flags[0] = NONE_FLAGS;
+}
+
+void orc_tree_free(orc_tree* t)
+{
+  free(t->code); free(t->depth); free(t->flags);
+  memset(t, 0, sizeof *t);
+}
+
+void orc_tree_load(orc_tree* t, const uint64_t* code, const uint8_t* depth, const uint8_t* flags, uint64_t n)
+{
+  tree_reserve(t, n ? n : 1);
+  memcpy(t->code, code, n * 8);
+  memcpy(t->depth, depth, n);
+  memcpy(t->flags, flags, n);
+  t->n = n;
+}
+
+/* insertSurroundingBoxIfEmpty (ImplicitBoxTree.hpp:1961-1970) */
+static void insert_surrounding_if_empty(orc_tree* t)
+{
+  if (t->n == 0) { tree_reserve(t, 1); t->n = 1; t->code[0] = 0; t->depth[0] = 0; t->flags[0] = 0; }
+}
+
+static inline int flags_set(uint8_t f, uint8_t check) { return (uint8_t)(f & check) == check; }
+
+/* setFlags / setFlagsByStencil on the leaves (ImplicitBoxTree.hpp:2684-2688) */
+uint32_t orc_set_flags(orc_tree* t, uint8_t flags)
+{
+  uint32_t c = 0;
+  for (uint64_t i = 0; i < t->n; ++i) { c += !flags_set(t->flags[i], flags); t->flags[i] |= flags; }
+  return c;
+}
+
+/* unsetFlags / unsetFlagsByStencil on the leaves (ImplicitBoxTree.hpp:3336-3360) */
+uint32_t orc_unset_flags(orc_tree* t, uint8_t flags)
+{
+  uint32_t c = 0;
+  for (uint64_t i = 0; i < t->n; ++i) { c += (t->flags[i] & flags) != 0; t->flags[i] &= (uint8_t)~flags; }
+  return c;
+}
+
+/* changeFlags / changeFlagsByStencil on the leaves (ImplicitBoxTree.hpp:934-957, Flags.hpp:22-26) */
+uint32_t orc_change_flags(orc_tree* t, uint8_t to_unset, uint8_t to_set)
+{
+  uint32_t c = 0;
+  for (uint64_t i = 0; i < t->n; ++i)
+    if (flags_set(t->flags[i], to_unset)) { ++c; t->flags[i] = (uint8_t)((t->flags[i] & ~to_unset) | to_set); }
+  return c;
+}
+
+/* sortBoxes (helpFunctions.hpp:40-98): tree order = comparable pattern, then deeper first */
+static const orc_tree* g_sort_tree;
+static int cmp_box(const void* a, const void* b)
+{
+  const uint64_t i = *(const uint64_t*)a, j = *(const uint64_t*)b;
+  const orc_tree* t = g_sort_tree;
+  if (strictly_preceding(t->code[i], t->depth[i], t->code[j], t->depth[j])) return -1;
+  if (strictly_preceding(t->code[j], t->depth[j], t->code[i], t->depth[i])) return 1;
+  return i < j ? -1 : (i > j); /* stable */
+}
+
+static void sort_tree(orc_tree* t)
+{
+  uint64_t* idx = (uint64_t*)malloc(t->n * 8);
+  for (uint64_t i = 0; i < t->n; ++i) idx[i] = i;
+  g_sort_tree = t;
+  qsort(idx, t->n, 8, cmp_box);
+  uint64_t* c = (uint64_t*)malloc(t->n * 8);
+  uint8_t* d = (uint8_t*)malloc(t->n);
+  uint8_t* f = (uint8_t*)malloc(t->n);
+  for (uint64_t i = 0; i < t->n; ++i) { c[i] = t->code[idx[i]]; d[i] = t->depth[idx[i]]; f[i] = t->flags[idx[i]]; }
+  memcpy(t->code, c, t->n * 8); memcpy(t->depth, d, t->n); memcpy(t->flags, f, t->n);
+  free(c); free(d); free(f); free(idx);
+}
+
+/* subdivide (ImplicitBoxTree.hpp:2884-2930): flagged leaves below the maximal depth
+ * become their two halves (incrementDepthBy / computeOtherHalf, Box.hpp:140-147,
+ * 234-239); flags are inherited; the result is re-sorted */
+uint32_t orc_subdivide(orc_tree* t, uint8_t flags)
+{
+  uint64_t n = t->n, m = 0;
+  for (uint64_t i = 0; i < n; ++i) m += flags_set(t->flags[i], flags) && t->depth[i] < 64;
+  tree_reserve(t, n + m);
+  uint64_t k = n;
+  for (uint64_t i = 0; i < n; ++i) {
+    if (flags_set(t->flags[i], flags) && t->depth[i] < 64) {
+      t->code[i] <<= 1;
+      t->depth[i] += 1;
+      t->code[k] = t->code[i] | 1u;
+      t->depth[k] = t->depth[i];
+      t->flags[k] = t->flags[i];
+      ++k;
+    }
+  }
+  t->n = n + m;
+  sort_tree(t);
+  return (uint32_t)m;
+}
+
+/* remove (ImplicitBoxTree.hpp:2344-2371): keep leaves that have all `flags` set */
+uint32_t orc_remove(orc_tree* t, uint8_t flags)
+{
+  uint64_t k = 0;
+  const uint64_t n = t->n;
+  for (uint64_t i = 0; i < n; ++i)
+    if (flags_set(t->flags[i], flags)) { t->code[k] = t->code[i]; t->depth[k] = t->depth[i]; t->flags[k] = t->flags[i]; ++k; }
+  t->n = k;
+  insert_surrounding_if_empty(t);
+  return (uint32_t)(n - k);
+}
+
+/* ------------------------------------------------------------------------------
+ * box images: GridPointsFunctor::operator() (Functors.hpp:476-511) + search
+ * ---------------------------------------------------------------------------- */
+static uint32_t image_target(const orc_tree* t, const orc_map* m, const orc_grid* g,
+                             uint64_t code, uint32_t depth, uint64_t i)
+{
+  const uint32_t D = t->dom.dim;
+  double c[ORC_MAX_DIM], r[ORC_MAX_DIM], gp[ORC_MAX_DIM], y[ORC_MAX_DIM];
+  orc_box_coordinates(&t->dom, code, depth, c, r);
+  orc_grid_point(g, D, i, gp);
+  for (uint32_t j = 0; j < D; ++j) c[j] += gp[j] * r[j];
+  orc_map_apply(m, c, y);
+  uint64_t code64;
+  const int valid = orc_point_code64(&t->dom, y, &code64);
+  return orc_search(t, code64, valid);
+}
+
+#define points_per_box orc_grid_points_per_box
+
+void orc_search_by_image(const orc_tree* t, const orc_map* m, const orc_grid* g,
+                         const uint32_t* src, uint64_t n_src, uint32_t* out)
+{
+  const uint64_t P = points_per_box(g, t->dom.dim);
+  const int64_t total = (int64_t)(n_src * P);
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < total; ++i) {
+    const uint32_t b = src[(uint64_t)i / P];
+    out[i] = image_target(t, m, g, t->code[b], t->depth[b], (uint64_t)i);
+  }
+}
+
+/* setFlagsByIterators over makePointIteratorPairOverLeaves
+ * (ImplicitBoxTree.hpp:2691-2694, 2624-2681, 2717-2775, 2167-2196) */
+uint32_t orc_set_flags_by_image(orc_tree* t, const orc_map* m, const orc_grid* g, uint8_t flags)
+{
+  const uint64_t n = t->n, P = points_per_box(g, t->dom.dim);
+  uint32_t* src = (uint32_t*)malloc(n * 4);
+  for (uint64_t i = 0; i < n; ++i) src[i] = (uint32_t)i;
+  uint32_t* tgt = (uint32_t*)malloc(n * P * 4);
+  orc_search_by_image(t, m, g, src, n, tgt);
+  uint8_t* hit = (uint8_t*)calloc(n, 1);
+  for (uint64_t i = 0; i < n * P; ++i) if (tgt[i] != ORC_INVALID) hit[tgt[i]] = 1;
+  uint32_t c = 0;
+  for (uint64_t i = 0; i < n; ++i)
+    if (hit[i]) { c += !flags_set(t->flags[i], flags); t->flags[i] |= flags; }
+  free(hit); free(tgt); free(src);
+  return c;
+}
+
+uint64_t orc_subdivision(orc_tree* t, const orc_map* m, const orc_grid* g, uint32_t steps, uint32_t* counts)
+{
+  /* subdivision loop (B12_doc.tex:269-290, subdivision.m:18-45) */
+  uint64_t box_images = 0;
+  orc_set_flags(t, 8u /* SD */);
+  for (uint32_t s = 0; s < steps; ++s) {
+    orc_subdivide(t, 8u);
+    box_images += t->n;
+    orc_set_flags_by_image(t, m, g, 1u /* HIT */);
+    orc_remove(t, 1u);
+    orc_unset_flags(t, 1u);
+    if (counts) counts[s] = (uint32_t)t->n;
+  }
+  return box_images;
+}
+
+/* ------------------------------------------------------------------------------
+ * transition matrix (ImplicitBoxTree.hpp:2934-3159): row = source leaf, column =
+ * target leaf, value = count (absolute) or count / P; row-major, columns ascending;
+ * lost points dropped, or sent to column n+1 with nColumns = n+1 (invalid)
+ * ---------------------------------------------------------------------------- */
+static int cmp_u32(const void* a, const void* b)
+{
+  const uint32_t x = *(const uint32_t*)a, y = *(const uint32_t*)b;
+  return x < y ? -1 : (x > y);
+}
+
+uint64_t orc_transition_matrix(const orc_tree* t, const orc_map* m, const orc_grid* g, int absolute, int invalid,
+                               uint32_t* rowptr, uint32_t* cols, double* vals, uint32_t* n_cols)
+{
+  const uint64_t n = t->n, P = points_per_box(g, t->dom.dim);
+  uint32_t* src = (uint32_t*)malloc(n * 4);
+  for (uint64_t i = 0; i < n; ++i) src[i] = (uint32_t)i;
+  uint32_t* tgt = (uint32_t*)malloc(n * P * 4);
+  orc_search_by_image(t, m, g, src, n, tgt);
+  const uint32_t nc = invalid ? (uint32_t)n + 1 : (uint32_t)n;
+  uint64_t nnz = 0;
+  if (rowptr) rowptr[0] = 0;
+  for (uint64_t r = 0; r < n; ++r) {
+    uint32_t* row = tgt + r * P;
+    qsort(row, P, 4, cmp_u32);
+    for (uint64_t k = 0; k < P;) {
+      uint64_t e = k;
+      while (e < P && row[e] == row[k]) ++e;
+      const uint32_t col = row[k];
+      if (col != ORC_INVALID || invalid) {
+        if (cols) {
+          cols[nnz] = col == ORC_INVALID ? nc : col;
+          vals[nnz] = absolute ? (double)(e - k) : (double)(e - k) / (double)P;
+        }
+        ++nnz;
+      }
+      k = e;
+    }
+    if (rowptr) rowptr[r + 1] = (uint32_t)nnz;
+  }
+  if (n_cols) *n_cols = nc;
+  free(tgt); free(src);
+  return nnz;
+}
+
+/* ------------------------------------------------------------------------------
+ * invariant measure: power iteration v <- P^T v / |P^T v|_1 from the uniform vector
+ * (subdivisionByNim.m:30-58 computes it with eigs / powerMethodMPE, not shipped)
+ * ---------------------------------------------------------------------------- */
+void orc_invariant_measure(uint32_t n, const uint32_t* rowptr, const uint32_t* cols, const double* vals,
+                           uint32_t iters, double* v)
+{
+  double* w = (double*)malloc((size_t)n * 8);
+  for (uint32_t i = 0; i < n; ++i) v[i] = 1.0 / (double)n;
+  for (uint32_t it = 0; it < iters; ++it) {
+    memset(w, 0, (size_t)n * 8);
+    for (uint32_t i = 0; i < n; ++i)
+      for (uint32_t e = rowptr[i]; e < rowptr[i + 1]; ++e)
+        if (cols[e] < n) w[cols[e]] += vals[e] * v[i];
+    double s = 0.0;
+    for (uint32_t j = 0; j < n; ++j) s += fabs(w[j]);
+    for (uint32_t j = 0; j < n; ++j) v[j] = w[j] / s;
+  }
+  free(w);
+}
+
+/* ------------------------------------------------------------------------------
+ * continuation (insertByIterators at a uniform depth, ImplicitBoxTree.hpp:1615-1910,
+ * makePointIteratorPairByFlags 2303-2341, insertByPoints 1927-1946, deleteDepth 1217-1228)
+ * ---------------------------------------------------------------------------- */
+void orc_delete_depth0(orc_tree* t)
+{
+  t->n = 0;
+  insert_surrounding_if_empty(t);
+}
+
+static int cmp_u64(const void* a, const void* b)
+{
+  const uint64_t x = *(const uint64_t*)a, y = *(const uint64_t*)b;
+  return x < y ? -1 : (x > y);
+}
+
+/* merge sorted unique new depth-d codes (flags `ins`) into a uniform-depth tree */
+static void merge_new(orc_tree* t, const uint64_t* nc, uint64_t m, uint32_t depth, uint8_t ins)
+{
+  const uint64_t n = t->n;
+  uint64_t* c = (uint64_t*)malloc((n + m) * 8);
+  uint8_t* d = (uint8_t*)malloc(n + m);
+  uint8_t* f = (uint8_t*)malloc(n + m);
+  uint64_t i = 0, j = 0, k = 0;
+  while (i < n || j < m) {
+    if (j >= m || (i < n && t->code[i] < nc[j])) { c[k] = t->code[i]; d[k] = t->depth[i]; f[k] = t->flags[i]; ++i; }
+    else { c[k] = nc[j]; d[k] = (uint8_t)depth; f[k] = ins; ++j; }
+    ++k;
+  }
+  tree_reserve(t, n + m);
+  memcpy(t->code, c, k * 8); memcpy(t->depth, d, k); memcpy(t->flags, f, k);
+  t->n = k;
+  free(c); free(d); free(f);
+}
+
+uint32_t orc_insert_points(orc_tree* t, const double* pts, uint64_t n_points, uint32_t depth, uint8_t ins)
+{
+  /* only the start of a continuation is restated: the tree holds just the surrounding
+   * box, which merges into the new boxes (its path is shared by every box) */
+  const uint32_t D = t->dom.dim;
+  uint64_t* nc = (uint64_t*)malloc((n_points ? n_points : 1) * 8);
+  uint64_t m = 0;
+  for (uint64_t p = 0; p < n_points; ++p) {
+    uint64_t c64;
+    if (orc_point_code64(&t->dom, pts + p * D, &c64)) nc[m++] = srs(c64, 64 - (int)depth);
+  }
+  qsort(nc, m, 8, cmp_u64);
+  uint64_t u = 0;
+  for (uint64_t k = 0; k < m; ++k) if (u == 0 || nc[k] != nc[u - 1]) nc[u++] = nc[k];
+  const int root_only = t->n == 1 && t->depth[0] == 0;
+  uint8_t root_flags = root_only ? t->flags[0] : 0;
+  if (root_only && u > 0) t->n = 0;
+  merge_new(t, nc, u, depth, ins);
+  if (root_only && u > 0) t->flags[0] |= root_flags;
+  free(nc);
+  return (uint32_t)u;
+}
+
+uint32_t orc_insert_by_image(orc_tree* t, const orc_map* m, const orc_grid* g, uint8_t flags_to_check,
+                             uint8_t ins, uint8_t hit)
+{
+  const uint64_t n = t->n, P = points_per_box(g, t->dom.dim);
+  const uint32_t depth = t->depth[0];
+  uint64_t ns = 0;
+  uint32_t* src = (uint32_t*)malloc((n ? n : 1) * 4);
+  for (uint64_t i = 0; i < n; ++i) if (flags_set(t->flags[i], flags_to_check)) src[ns++] = (uint32_t)i;
+  uint64_t* cand = (uint64_t*)malloc((ns * P > 0 ? ns * P : 1) * 8);
+  uint32_t* tgt = (uint32_t*)malloc((ns * P > 0 ? ns * P : 1) * 4);
+  const int64_t total = (int64_t)(ns * P);
+  const uint32_t D = t->dom.dim;
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < total; ++i) {
+    const uint32_t b = src[(uint64_t)i / P];
+    double c[ORC_MAX_DIM], r[ORC_MAX_DIM], gp[ORC_MAX_DIM], y[ORC_MAX_DIM];
+    orc_box_coordinates(&t->dom, t->code[b], t->depth[b], c, r);
+    orc_grid_point(g, D, (uint64_t)i, gp);
+    for (uint32_t j = 0; j < D; ++j) c[j] += gp[j] * r[j];
+    orc_map_apply(m, c, y);
+    uint64_t code64;
+    const int valid = orc_point_code64(&t->dom, y, &code64);
+    tgt[i] = orc_search(t, code64, valid);
+    cand[i] = valid && tgt[i] == ORC_INVALID ? srs(code64, 64 - (int)depth) : INVALID_CODE;
+  }
+  if (hit)
+    for (int64_t i = 0; i < total; ++i) if (tgt[i] != ORC_INVALID) t->flags[tgt[i]] |= hit;
+  qsort(cand, (size_t)total, 8, cmp_u64);
+  uint64_t u = 0;
+  for (int64_t k = 0; k < total && cand[k] != INVALID_CODE; ++k) if (u == 0 || cand[k] != cand[u - 1]) cand[u++] = cand[k];
+  merge_new(t, cand, u, depth, ins);
+  free(cand); free(tgt); free(src);
+  return (uint32_t)u;
+}

@@ -1,0 +1,130 @@
+"""Generate the golden fixtures from the reference itself.
+
+Runs the reference's own ImplicitBoxTree (compiled from its headers with the Thrust
+OMP backend into oracle/_ref by oracle/ref/Makefile) on the workloads below and
+stores, per subdivision step, the leaf count and SHA-256 digests of the leaf codes and
+flags, plus the transition matrix as CSR digests; small cases are also stored in full
+(<name>.npz).  The GPU tests compare the CUDA library against these files, which is
+why they are committed: the reference is not available where the GPU tests run.
+
+    python tests/golden/make_golden.py [name ...]
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+REF = os.path.join(REPO, "oracle", "_ref")
+
+# name -> (binary, args, spec for the library/oracle, full-array limit)
+WORKLOADS = {
+    "henon_d20": ("ref_henon", ["--steps", "20", "--tm", "1"], dict(map="henon", a=1.4, b=0.3, grid=4, steps=20)),
+    "henon_d12_abs": ("ref_henon", ["--steps", "12", "--tm", "2"],
+                      dict(map="henon", a=1.4, b=0.3, grid=4, steps=12, absolute=True)),
+    "henon_d12_lost": ("ref_henon", ["--steps", "12", "--tm", "3", "--grid", "6"],
+                       dict(map="henon", a=1.4, b=0.3, grid=6, steps=12, invalid=True)),
+    "henon_a1.0_d16": ("ref_henon", ["--steps", "16", "--tm", "1", "--a", "1.0"],
+                       dict(map="henon", a=1.0, b=0.3, grid=4, steps=16)),
+    "lorenz_d15": ("ref_lorenz", ["--steps", "15", "--tm", "1"], dict(map="lorenz", rho=28.0, grid=5, steps=15)),
+    "lorenz_d27": ("ref_lorenz", ["--steps", "27", "--tm", "1", "--buf", "1073741824"],
+                   dict(map="lorenz", rho=28.0, grid=5, steps=27)),
+    "lorenz_fma_d27": ("ref_lorenz", ["--steps", "27", "--tm", "1", "--fma", "1", "--buf", "1073741824"],
+                       dict(map="lorenz", rho=28.0, grid=5, steps=27, fma=True)),
+    "lorenz_rho15_d18": ("ref_lorenz", ["--steps", "18", "--tm", "1", "--rho", "15"],
+                         dict(map="lorenz", rho=15.0, grid=5, steps=18)),
+    "lorenz_rho35_d18": ("ref_lorenz", ["--steps", "18", "--tm", "1", "--rho", "35"],
+                         dict(map="lorenz", rho=35.0, grid=5, steps=18)),
+    "forced_duffing_d16": ("ref_forced", ["--steps", "16", "--tm", "1"],
+                           dict(map="forced_duffing", grid=4, steps=16)),
+    "coupled_duffing_cont_d8": ("ref_duffing", ["--steps", "8"], dict(map="coupled_duffing", points=64, seed=0,
+                                                                          depth=8)),
+    "coupled_duffing_cont_d12": ("ref_duffing", ["--steps", "12"], dict(map="coupled_duffing", points=64, seed=0,
+                                                                            depth=12)),
+}
+
+FULL_LIMIT = 20000  # store leaf arrays of steps with at most this many leaves
+
+
+def sha(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def read_leaves(path):
+    with open(path, "rb") as f:
+        n = int(np.frombuffer(f.read(8), dtype="<u8")[0])
+        codes = np.frombuffer(f.read(8 * n), dtype="<u8").copy()
+        depth = np.frombuffer(f.read(n), dtype=np.uint8).copy()
+        flags = np.frombuffer(f.read(n), dtype=np.uint8).copy()
+    return codes, depth, flags
+
+
+def read_coo(path):
+    with open(path, "rb") as f:
+        nnz = int(np.frombuffer(f.read(8), dtype="<u8")[0])
+        nr, nc = np.frombuffer(f.read(8), dtype="<u4")
+        rows = np.frombuffer(f.read(4 * nnz), dtype="<u4").copy()
+        cols = np.frombuffer(f.read(4 * nnz), dtype="<u4").copy()
+        vals = np.frombuffer(f.read(8 * nnz), dtype="<f8").copy()
+    return int(nr), int(nc), rows, cols, vals
+
+
+def coo_to_csr(nr, rows):
+    counts = np.bincount(rows, minlength=nr).astype(np.uint64)
+    rowptr = np.zeros(nr + 1, dtype=np.uint32)
+    rowptr[1:] = np.cumsum(counts).astype(np.uint32)
+    return rowptr
+
+
+def generate(name: str) -> None:
+    binary, args, spec = WORKLOADS[name]
+    exe = os.path.join(REF, binary)
+    if not os.path.exists(exe):
+        raise SystemExit(f"{exe} missing: build it with `make -C oracle/ref`")
+    with tempfile.TemporaryDirectory() as tmp:
+        cmd = [exe, "--out", tmp] + args
+        if "--buf" not in args:
+            cmd += ["--buf", str(64 << 20)]
+        res = subprocess.run(cmd, check=True, capture_output=True, text=True)
+        timing = json.loads(res.stdout.strip().splitlines()[-1])
+        out = dict(workload=name, spec=spec, reference_cmd=" ".join([binary] + args), timing=timing, steps=[])
+        arrays = {}
+        is_cont = binary == "ref_duffing"
+        prefix = "cont_" if is_cont else "leaves_"
+        files = sorted(f for f in os.listdir(tmp) if f.startswith(prefix))
+        for fn in files:
+            k = int(fn[len(prefix):-4])
+            codes, depth, flags = read_leaves(os.path.join(tmp, fn))
+            out["steps"].append(dict(step=k, n=int(len(codes)), depth=int(depth[0]) if len(depth) else 0,
+                                     uniform_depth=bool((depth == depth[0]).all()) if len(depth) else True,
+                                     codes_sha256=sha(codes), flags_sha256=sha(flags)))
+            if len(codes) <= FULL_LIMIT:
+                arrays[f"codes_{k:02d}"] = codes
+                arrays[f"flags_{k:02d}"] = flags
+        tm_path = os.path.join(tmp, "tm.bin")
+        if os.path.exists(tm_path):
+            nr, nc, rows, cols, vals = read_coo(tm_path)
+            rowptr = coo_to_csr(nr, rows)
+            out["tm"] = dict(n_rows=nr, n_cols=nc, nnz=int(len(vals)), rowptr_sha256=sha(rowptr),
+                             cols_sha256=sha(cols), vals_sha256=sha(vals))
+            if len(vals) <= 60000:
+                arrays["tm_rowptr"] = rowptr
+                arrays["tm_cols"] = cols
+                arrays["tm_vals"] = vals
+    with open(os.path.join(HERE, f"{name}.json"), "w") as f:
+        json.dump(out, f, indent=1)
+    if arrays:
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **arrays)
+    print(name, "steps", len(out["steps"]), "tm", out.get("tm", {}).get("nnz"), flush=True)
+
+
+if __name__ == "__main__":
+    for name in sys.argv[1:] or list(WORKLOADS):
+        generate(name)

@@ -1,0 +1,229 @@
+"""GPU parity: the CUDA library (through its C ABI) against the reference's golden
+fixtures and the oracle.  Leaf sets, flags, counts and sparsity patterns must be
+bit-exact; transition probabilities are bit-exact too (count / P is one IEEE
+division on both sides; the stated tolerance is 1e-13 relative); the invariant
+measure is compared to the oracle's FP64 power iteration in L1."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from workloads import csr_digests, domain, oracle_spec, scheme, sha
+
+pytestmark = pytest.mark.gpu
+
+B = pytest.importorskip("b12_b200")
+
+TM_RTOL = 1e-13
+MEASURE_L1 = 1e-12
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _device():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+def make_tree(spec):
+    c, r = domain(spec)
+    return B.ImplicitBoxTree(c, r)
+
+
+# ------------------------------------------------------------------ subdivision
+def test_henon_step_by_step_api_matches_reference(golden):
+    """The reference's loop (B12_doc.tex:269-290) call by call, with return values."""
+    meta, arrays = golden("henon_d20")
+    spec = meta["spec"]
+    t = make_tree(spec)
+    o = O.Oracle(oracle_spec(spec))
+    sc = scheme(spec)
+    assert t.set_flags(B.SD, 0) == o.set_flags(8) == 1
+    for st in meta["steps"]:
+        assert t.subdivide(B.SD) == o.subdivide(8)
+        assert t.set_flags_by_image(sc, B.HIT) == o.set_flags_by_image(1)
+        assert t.remove(B.HIT) == o.remove(1)
+        assert t.unset_flags(B.HIT) == o.unset_flags(1)
+        codes, depth, flags = t.leaves()
+        assert t.count() == st["n"] and t.depth() == st["step"]
+        assert sha(codes) == st["codes_sha256"], f"step {st['step']}"
+        assert sha(flags) == st["flags_sha256"], f"step {st['step']}"
+        if f"codes_{st['step']:02d}" in arrays:
+            np.testing.assert_array_equal(codes, arrays[f"codes_{st['step']:02d}"])
+
+
+@pytest.mark.parametrize("name", ["henon_d20", "henon_a1.0_d16", "lorenz_d15", "forced_duffing_d16",
+                                  "lorenz_rho15_d18", "lorenz_rho35_d18"])
+def test_fused_subdivision_matches_reference(golden, name):
+    meta, arrays = golden(name)
+    spec = meta["spec"]
+    t = make_tree(spec)
+    counts = t.subdivision_run(scheme(spec), len(meta["steps"]))
+    assert list(counts) == [s["n"] for s in meta["steps"]]
+    codes, depth, flags = t.leaves()
+    last = meta["steps"][-1]
+    assert sha(codes) == last["codes_sha256"]
+    assert sha(flags) == last["flags_sha256"]
+    assert (depth == last["step"]).all()
+
+
+@pytest.mark.parametrize("name", ["lorenz_d27", "lorenz_fma_d27"])
+def test_lorenz_depth27_box_sets_bit_identical(golden, name):
+    try:
+        meta, _ = golden(name)
+    except FileNotFoundError:
+        pytest.skip(f"{name} fixture not generated")
+    spec = meta["spec"]
+    t = make_tree(spec)
+    steps = len(meta["steps"])
+    # run the steps one fused call at a time so that every intermediate leaf set is checked
+    for st in meta["steps"]:
+        t.subdivision_run(scheme(spec), 1)
+        codes, _, flags = t.leaves()
+        assert len(codes) == st["n"], f"step {st['step']}"
+        assert sha(codes) == st["codes_sha256"], f"step {st['step']}"
+    assert t.depth() == steps
+    m = t.transition_matrix(scheme(spec))
+    d = csr_digests(*m.to_host())
+    for k in ("nnz", "rowptr_sha256", "cols_sha256", "vals_sha256"):
+        assert d[k] == meta["tm"][k], k
+
+
+def test_fused_and_step_api_agree():
+    spec = dict(map="lorenz", rho=28.0, grid=3, steps=12)
+    a, b = make_tree(spec), make_tree(spec)
+    sc = scheme(spec)
+    counts = a.subdivision_run(sc, 12)
+    b.set_flags(B.SD)
+    for k in range(12):
+        b.subdivide(B.SD)
+        b.set_flags_by_image(sc, B.HIT)
+        b.remove(B.HIT)
+        b.unset_flags(B.HIT)
+        assert b.count() == counts[k]
+    for x, y in zip(a.leaves(), b.leaves()):
+        np.testing.assert_array_equal(x, y)
+
+
+# ------------------------------------------------------------------ transition matrix
+@pytest.mark.parametrize("name,absolute,invalid", [
+    ("henon_d20", False, False), ("henon_d12_abs", True, False), ("henon_d12_lost", False, True),
+    ("lorenz_d15", False, False), ("forced_duffing_d16", False, False), ("lorenz_rho15_d18", False, False)])
+def test_transition_matrix_matches_reference(golden, name, absolute, invalid):
+    meta, arrays = golden(name)
+    spec = meta["spec"]
+    t = make_tree(spec)
+    sc = scheme(spec)
+    t.subdivision_run(sc, len(meta["steps"]))
+    m = t.transition_matrix(sc, absolute=absolute, invalid_column=invalid)
+    assert m.n_rows == meta["tm"]["n_rows"] and m.n_cols == meta["tm"]["n_cols"]
+    rowptr, cols, vals = m.to_host()
+    d = csr_digests(rowptr, cols, vals)
+    for k in ("nnz", "rowptr_sha256", "cols_sha256"):
+        assert d[k] == meta["tm"][k], k
+    if "tm_vals" in arrays:
+        np.testing.assert_allclose(vals, arrays["tm_vals"], rtol=TM_RTOL, atol=0)
+        np.testing.assert_array_equal(cols, arrays["tm_cols"])
+    assert d["vals_sha256"] == meta["tm"]["vals_sha256"]
+
+
+def test_invariant_measure_against_oracle():
+    spec = dict(map="henon", a=1.4, b=0.3, grid=4)
+    t = make_tree(spec)
+    sc = scheme(spec)
+    t.subdivision_run(sc, 16)
+    m = t.transition_matrix(sc)
+    rowptr, cols, vals = m.to_host()
+    v = m.invariant_measure(200)
+    ref = O.invariant_measure(rowptr, cols, vals, 200)
+    l1 = np.abs(v - ref).sum()
+    assert l1 < MEASURE_L1, l1
+    assert abs(v.sum() - 1.0) < 1e-12
+    # a second call reuses the transposed matrix and gives the same vector
+    np.testing.assert_array_equal(v, m.invariant_measure(200))
+
+
+# ------------------------------------------------------------------ search and flags
+@pytest.mark.parametrize("spec", [dict(map="henon", a=1.4, b=0.3, grid=4),
+                                  dict(map="lorenz", rho=28.0, grid=3),
+                                  dict(map="forced_duffing", grid=3)])
+def test_search_by_image_matches_oracle(spec):
+    t = make_tree(spec)
+    o = O.Oracle(oracle_spec(spec))
+    sc = scheme(spec)
+    t.subdivision_run(sc, 10)
+    o.subdivision(10)
+    np.testing.assert_array_equal(t.leaves()[0], o.leaves()[0])
+    np.testing.assert_array_equal(t.search_by_image(sc), o.search_by_image())
+
+
+def test_search_on_root_matches_reference_quirk():
+    """On the root-only tree every mapped point, inside the domain or not, is found in
+    leaf 0 (the reference's hasSamePath of an invalid box with code 0)."""
+    spec = dict(map="henon", a=1.4, b=0.3, grid=4)
+    t = make_tree(spec)
+    o = O.Oracle(oracle_spec(spec))
+    got = t.search_by_image(scheme(spec))
+    np.testing.assert_array_equal(got, o.search_by_image())
+    assert (got == 0).all()
+
+
+def test_flag_operations_match_oracle():
+    spec = dict(map="henon", a=1.4, b=0.3, grid=4)
+    t = make_tree(spec)
+    o = O.Oracle(oracle_spec(spec))
+    t.subdivision_run(scheme(spec), 8)
+    o.subdivision(8)
+    rng = np.random.default_rng(1)
+    codes, depth, _ = o.leaves()
+    flags = rng.integers(0, 256, size=len(codes)).astype(np.uint8)
+    t.load_leaves(codes, depth, flags)
+    o.load(codes, depth, flags)
+    for op, args in [("set", (B.INS,)), ("unset", (B.HIT | B.EXPD,)), ("change", (B.INS, B.EXPD)),
+                     ("set", (B.SD | B.EQU,)), ("change", (B.SD | B.HIT, B.NONE))]:
+        if op == "set":
+            assert t.set_flags(*args) == o.set_flags(*args)
+        elif op == "unset":
+            assert t.unset_flags(*args) == o.unset_flags(*args)
+        else:
+            assert t.change_flags(*args) == o.change_flags(*args)
+        np.testing.assert_array_equal(t.leaves()[2], o.leaves()[2])
+    assert t.remove(B.EQU) == o.remove(0x10)
+    for x, y in zip(t.leaves(), o.leaves()):
+        np.testing.assert_array_equal(x, y)
+
+
+def test_remove_everything_leaves_the_root():
+    spec = dict(map="henon", a=1.4, b=0.3, grid=4)
+    t = make_tree(spec)
+    t.subdivision_run(scheme(spec), 6)
+    n = t.count()
+    assert t.remove(B.EXPD) == n
+    codes, depth, flags = t.leaves()
+    assert list(codes) == [0] and list(depth) == [0] and list(flags) == [0]
+    assert t.depth() == 0
+
+
+def test_mixed_depth_is_refused_and_tree_unchanged():
+    spec = dict(map="henon", a=1.4, b=0.3, grid=4)
+    t = make_tree(spec)
+    t.subdivision_run(scheme(spec), 4)
+    codes, depth, flags = t.leaves()
+    flags = flags.copy()
+    flags[0] |= B.INS
+    t.load_leaves(codes, depth, flags)
+    with pytest.raises(B.B12gError) as e:
+        t.subdivide(B.INS)
+    assert e.value.status == 5
+    for x, y in zip(t.leaves(), (codes, depth, flags)):
+        np.testing.assert_array_equal(x, y)
+
+
+def test_capacity_retry_in_fused_run():
+    """The fused loop starts with a small buffer and must grow it transparently."""
+    spec = dict(map="lorenz", rho=28.0, grid=5, steps=21)
+    t = make_tree(spec)
+    counts = t.subdivision_run(scheme(spec), 21)
+    o = O.Oracle(oracle_spec(spec))
+    oc, _ = o.subdivision(21)
+    np.testing.assert_array_equal(counts, oc)
+    np.testing.assert_array_equal(t.leaves()[0], o.leaves()[0])
