@@ -240,7 +240,12 @@ void prof_mark(b12g_tree* t, int kind)
     cudaEventCreate(&e);
     v.push_back(e);
   }
-  cudaEventRecord(v[t->prof_used[kind]++], t->stream);
+  // during capture an external record becomes a real event node of the graph
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(t->stream, &cs);
+  cudaEvent_t e = v[t->prof_used[kind]++];
+  if (cs == cudaStreamCaptureStatusActive) cudaEventRecordWithFlags(e, t->stream, cudaEventRecordExternal);
+  else cudaEventRecord(e, t->stream);
 }
 
 static void sum_pairs(const std::vector<cudaEvent_t>& v, size_t used, double& ms, uint64_t& launches)

@@ -87,7 +87,9 @@ __global__ void transpose_sort_kernel(const uint32_t* tptr, uint32_t n_cols, uin
 // ---- power iteration ----------------------------------------------------------------
 // A sense-reversal grid barrier whose waits give up after a bounded number of polls;
 // co-residency of all blocks is guaranteed by the cooperative launch.
-constexpr unsigned long long kBarrierPolls = 1ull << 22;  // ~ 1 s with the 256 ns back-off
+constexpr unsigned long long kBarrierPolls = 1ull << 24;  // far beyond any real wait (~1 s)
+constexpr int kMeasureThreads = 512;
+constexpr int kRowLanes = 8;                                // lanes per row of P^T
 
 __device__ bool grid_barrier(unsigned* count, unsigned* gen, unsigned* error)
 {
@@ -106,7 +108,7 @@ __device__ bool grid_barrier(unsigned* count, unsigned* gen, unsigned* error)
       unsigned long long polls = 0;
       while (*vgen == g) {
         if (++polls > kBarrierPolls) { atomicOr(error, 2u); ok = 0; break; }
-        __nanosleep(256);
+        if ((polls & 1023u) == 0) __nanosleep(64);
       }
     }
     __threadfence();
@@ -130,26 +132,53 @@ struct MeasureArgs {
   unsigned* error;
 };
 
-__global__ void __launch_bounds__(kThreads) invariant_measure_kernel(const MeasureArgs a)
+// sum of the per-block partials in one fixed order, identical in every block
+__device__ double sum_partials(const double* part, uint32_t nb, double* bcast)
 {
-  __shared__ double red[kThreads / 32];
+  if (threadIdx.x < 32) {
+    double x = 0.0;
+    for (uint32_t i = threadIdx.x; i < nb; i += 32) x = __dadd_rn(x, __ldcg(part + i));
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) x = __dadd_rn(x, __shfl_xor_sync(0xFFFFFFFFu, x, d));
+    if (threadIdx.x == 0) *bcast = x;
+  }
+  __syncthreads();
+  return *bcast;
+}
+
+// v <- P^T v / |P^T v|_1; rows of P^T are handled by groups of 8 lanes; the previous
+// iterate is scaled by 1/s on the fly, so one grid barrier per iteration suffices
+__global__ void __launch_bounds__(kMeasureThreads) invariant_measure_kernel(const MeasureArgs a)
+{
+  __shared__ double red[kMeasureThreads / 32];
+  __shared__ double bcast;
   const uint32_t n = a.n;
-  const uint32_t stride = gridDim.x * blockDim.x;
+  const uint32_t lane8 = threadIdx.x & (kRowLanes - 1);
+  const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) / kRowLanes;
+  const uint32_t groups = gridDim.x * blockDim.x / kRowLanes;
   const double v0 = __ddiv_rn(1.0, double(n));
-  double s_prev = 1.0;
+  double inv = 1.0;
   for (uint32_t it = 0; it < a.iters; ++it) {
     const double* wp = (it & 1u) ? a.w0 : a.w1;
     double* wc = (it & 1u) ? a.w1 : a.w0;
     double local = 0.0;
-    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
+    // the loop runs over the warp's first group so that every lane of a warp takes the
+    // same number of trips (the shuffles below need the whole warp)
+    for (uint32_t jb = group & ~3u; jb < n; jb += groups) {
+      const uint32_t j = jb + (group & 3u);
+      const bool row = j < n;
       double acc = 0.0;
-      const uint32_t b = a.tptr[j], e = a.tptr[j + 1];
-      for (uint32_t k = b; k < e; ++k) {
-        const double v = it == 0 ? v0 : __ddiv_rn(wp[a.trows[k]], s_prev);
-        acc = __dadd_rn(acc, __dmul_rn(a.tvals[k], v));
+      const uint32_t b = row ? __ldg(a.tptr + j) : 0u, e = row ? __ldg(a.tptr + j + 1) : 0u;
+      for (uint32_t k = b + lane8; k < e; k += kRowLanes) {
+        const double v = it == 0 ? v0 : __dmul_rn(__ldcg(wp + __ldg(a.trows + k)), inv);
+        acc = __fma_rn(__ldg(a.tvals + k), v, acc);
       }
-      wc[j] = acc;
-      local = __dadd_rn(local, fabs(acc));
+#pragma unroll
+      for (int d = kRowLanes / 2; d > 0; d >>= 1) acc = __dadd_rn(acc, __shfl_xor_sync(0xFFFFFFFFu, acc, d));
+      if (lane8 == 0 && row) {
+        __stcg(wc + j, acc);
+        local = __dadd_rn(local, fabs(acc));
+      }
     }
 #pragma unroll
     for (int d = 16; d > 0; d >>= 1) local = __dadd_rn(local, __shfl_xor_sync(0xFFFFFFFFu, local, d));
@@ -157,18 +186,15 @@ __global__ void __launch_bounds__(kThreads) invariant_measure_kernel(const Measu
     __syncthreads();
     if (threadIdx.x == 0) {
       double t = 0.0;
-      for (int i = 0; i < kThreads / 32; ++i) t = __dadd_rn(t, red[i]);
-      a.partial[(it & 1u) * gridDim.x + blockIdx.x] = t;
+      for (int i = 0; i < kMeasureThreads / 32; ++i) t = __dadd_rn(t, red[i]);
+      __stcg(a.partial + (it & 1u) * gridDim.x + blockIdx.x, t);
     }
     if (!grid_barrier(a.bar_count, a.bar_gen, a.error)) return;
-    // every block sums the partials in the same order: one value of s everywhere
-    double s = 0.0;
-    for (uint32_t i = 0; i < gridDim.x; ++i) s = __dadd_rn(s, a.partial[(it & 1u) * gridDim.x + i]);
-    s_prev = s;
+    inv = __ddiv_rn(1.0, sum_partials(a.partial + (it & 1u) * gridDim.x, gridDim.x, &bcast));
   }
   const double* wl = (a.iters & 1u) ? a.w0 : a.w1;
-  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride)
-    a.out[j] = a.iters ? __ddiv_rn(wl[j], s_prev) : v0;
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+    a.out[j] = a.iters ? __dmul_rn(__ldcg(wl + j), inv) : v0;
 }
 
 }  // namespace
@@ -206,16 +232,17 @@ cudaError_t invariant_measure(const uint32_t* tptr, const uint32_t* trows, const
   static int blocks_per_sm = 0;
   if (!blocks_per_sm) {
     int b = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, invariant_measure_kernel, kThreads, 0);
-    blocks_per_sm = b > 0 ? b : 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, invariant_measure_kernel, kMeasureThreads, 0);
+    blocks_per_sm = b > 0 ? (b < 2 ? b : 2) : 1;
   }
-  int grid = grid_for(n, kThreads, blocks_per_sm);
+  int grid = grid_for(uint64_t(n) * kRowLanes, kMeasureThreads, blocks_per_sm);
   if (grid > int(partial_cap / 2)) grid = int(partial_cap / 2);
   if (grid < 1) grid = 1;
   cudaMemsetAsync(sync_words, 0, 3 * sizeof(unsigned), s);
   MeasureArgs a{tptr, trows, tvals, n, iters, w0, w1, partial, out, sync_words, sync_words + 1, sync_words + 2};
   void* params[] = {&a};
-  return cudaLaunchCooperativeKernel((const void*)invariant_measure_kernel, dim3(grid), dim3(kThreads), params, 0, s);
+  return cudaLaunchCooperativeKernel((const void*)invariant_measure_kernel, dim3(grid), dim3(kMeasureThreads), params,
+                                     0, s);
 }
 
 int measure_partial_slots()

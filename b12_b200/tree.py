@@ -286,7 +286,7 @@ class ImplicitBoxTree:
                           into: "CsrMatrix | None" = None) -> CsrMatrix:
         """Build the matrix; `into` refills an existing matrix in place (no new device memory)."""
         s = scheme.to_c()
-        h = C.c_void_p(into._h if into is not None else None)
+        h = C.c_void_p(into._h.value if into is not None else None)
         check(lib().b12g_transition_matrix(self._h, C.byref(s), int(absolute), int(invalid_column), C.byref(h)),
               "transition_matrix")
         if into is not None:

@@ -75,6 +75,12 @@ class ClockSampler:
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
+    def wait_first(self, timeout: float = 5.0):
+        """block until nvidia-smi has produced its first sample (it starts slowly)"""
+        t0 = time.time()
+        while self.proc and not self.lines and time.time() - t0 < timeout:
+            time.sleep(0.02)
+
     def __exit__(self, *exc):
         if self.proc:
             self.proc.terminate()
@@ -221,6 +227,21 @@ def gpu_arm(args, rank: int, world: int, dist):
     bi_sub, n_final = box_images_of(counts)
     box_images = bi_sub + n_final
 
+    # phase breakdown of one job (host clock around the synchronous API calls)
+    phases = {}
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    tree.delete_depth(0)
+    t1 = time.perf_counter()
+    tree.subdivision_run(sc, DEPTH)
+    t2 = time.perf_counter()
+    csr = tree.transition_matrix(sc, into=csr)
+    t3 = time.perf_counter()
+    csr.invariant_measure(MEASURE_ITERS, keep_on_device=True)
+    t4 = time.perf_counter()
+    phases = {"reset_ms": 1e3 * (t1 - t0), "subdivision_ms": 1e3 * (t2 - t1), "transition_matrix_ms": 1e3 * (t3 - t2),
+              "invariant_measure_ms": 1e3 * (t4 - t3)}
+
     tree.profile(True)
     tree.profile_read(0)
     tree.profile_read(1)
@@ -230,6 +251,7 @@ def gpu_arm(args, rank: int, world: int, dist):
         dist.barrier()
     torch.cuda.synchronize()
     with ClockSampler(dev) as clocks:
+        clocks.wait_first()
         for i in range(args.steps):
             with torch.cuda.stream(stream):
                 flush.zero_()
@@ -312,7 +334,7 @@ def gpu_arm(args, rank: int, world: int, dist):
                              "flop_per_box_image": P * FLOP_PER_POINT, "launches": img_n,
                              "kernel_ms_per_step": img_ms / args.steps,
                              "transition_rows_tflops": rows_tflops},
-                "clocks": clocks.summary(), "cpu_baseline": cpu,
+                "clocks": clocks.summary(), "cpu_baseline": cpu, "phases_ms": phases,
                 "counts": [int(c) for c in counts]}
         print(json.dumps(line), flush=True)
     tree.close()
@@ -327,7 +349,7 @@ def lib_leaves(tree, codes, depth, flags):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--fma", action="store_true", help="explicit-FMA integrator arithmetic")
