@@ -87,6 +87,8 @@ _SIGS = {
     "b12g_csr_destroy": (C.c_int, [C.c_void_p]),
     "b12g_invariant_measure": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p]),
     "b12g_csr_measure": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "b12g_invariant_measure_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32,
+                                                 C.c_void_p, C.c_void_p]),
     "b12g_subdivision_run": (C.c_int, [C.c_void_p, C.POINTER(Scheme), C.c_uint32, C.c_void_p]),
     "b12g_continuation_run": (C.c_int, [C.c_void_p, C.POINTER(Scheme), C.c_void_p, C.c_uint64, C.c_uint8,
                                         C.c_uint32, C.c_void_p, C.POINTER(C.c_uint32)]),

@@ -188,6 +188,17 @@ b12g_status b12g_csr_destroy(b12g_csr* csr);
 b12g_status b12g_invariant_measure(b12g_csr* csr, uint32_t iters, double* v);
 /* copy the last invariant measure of `csr` to the host array v (n_rows entries) */
 b12g_status b12g_csr_measure(const b12g_csr* csr, double* v);
+/* Allocation-free invariant measure (no counterpart in the reference): for callers that
+ * cannot let the library allocate device memory - a process whose own memory pool owns
+ * the free HBM, or a latency-critical loop where cudaMalloc/cudaFree would synchronize
+ * the device.  Same power iteration as b12g_invariant_measure, on the CSR of P^T given
+ * as device arrays (tptr[n+1], trows[nnz], tvals[nnz]; sources ascending in each row),
+ * result in the device array v[n].  Its scratch is one fixed __device__ array shared by
+ * all calls: at most 262,144 boxes (B12G_ERR_CAPACITY above that), and calls that overlap
+ * on the GPU race.  The first call on a device looks up the array's device address, so
+ * make it before any stream capture.  Returns after the work on `stream` has finished. */
+b12g_status b12g_invariant_measure_noalloc(const uint32_t* tptr, const uint32_t* trows, const double* tvals,
+                                           uint32_t n, uint32_t iters, double* v, void* stream);
 
 /* ---- fused drivers ------------------------------------------------------------------- */
 /* The subdivision loop of B12_doc.tex:269-290 / subdivision.m:18-45,
