@@ -231,6 +231,49 @@ b12g_status flag_call(b12g_tree* t, int op, uint8_t u, uint8_t f, uint8_t depth,
   return B12G_OK;
 }
 
+static uint32_t host_hash_log2(uint64_t n)
+{
+  uint32_t l = 6;
+  while ((1ull << l) < 2ull * n) ++l;
+  return l;
+}
+
+b12g_status ensure_hash(b12g_tree* t, uint64_t max_n)
+{
+  const uint32_t l = host_hash_log2(std::max<uint64_t>(max_n, 1));
+  if (t->hash.p && l <= t->hash_log2) return B12G_OK;
+  t->hash.release();
+  ST(t->hash.ensure(size_t(1) << l, "leaf lookup table"));
+  CK(cudaMemsetAsync(t->hash.p, 0, t->hash.n * sizeof(ulonglong2), t->stream));
+  t->hash_log2 = l;
+  t->hash_tag = 0;
+  return B12G_OK;
+}
+
+b12g_status next_hash_tag(b12g_tree* t, uint32_t* tag)
+{
+  if (t->hash_tag >= 255) {
+    CK(cudaMemsetAsync(t->hash.p, 0, t->hash.n * sizeof(ulonglong2), t->stream));
+    t->hash_tag = 0;
+  }
+  *tag = ++t->hash_tag;
+  return B12G_OK;
+}
+
+b12g_status build_current_hash(b12g_tree* t, Prepared& pr)
+{
+  pr.a.hash = LeafHash{nullptr, 0, 0};
+  if (t->depth > kHashMaxDepth || t->n == 0) return B12G_OK;
+  ST(ensure_hash(t, t->n));
+  uint32_t tag = 0;
+  ST(next_hash_tag(t, &tag));
+  const LeafHash h{t->hash.p, tag, t->hash_log2};
+  CK(build_leaf_hash(t->codes(), t->dn(), h, t->ctr.p + C_ERROR, t->n, t->stream));
+  count_launches(1);
+  pr.a.hash = h;
+  return B12G_OK;
+}
+
 void prof_mark(b12g_tree* t, int kind)
 {
   if (!t->profile) return;
@@ -492,6 +535,7 @@ b12g_status b12g_set_flags_by_image(b12g_tree* t, const b12g_scheme* sc, uint8_t
   ST(prepare(t, sc, pr));
   uint32_t n_src = 0;
   ST(select_sources(t, sc, pr, n_src));
+  ST(build_current_hash(t, pr));
   ST(set_ctr(t, C_CHANGED, 0));
   pr.a.hit_cap = uint32_t(std::min<size_t>(t->hit.n, 0xFFFFFFFFu));
   prof_mark(t, 0);
@@ -522,6 +566,7 @@ b12g_status b12g_search_by_image(b12g_tree* t, const b12g_scheme* sc, uint8_t de
   if (capacity < np) return fail(B12G_ERR_CAPACITY, "output holds %llu of %llu points", (unsigned long long)capacity,
                                  (unsigned long long)np);
   ST(t->out.ensure(std::max<uint64_t>(np, 1), "search output"));
+  ST(build_current_hash(t, pr));
   pr.a.out = t->out.p;
   CK(launch_image(sc->map.kind, sc->map.arith, sc->grid.kind, t->domain.dim, ImageMode::Search, pr.a, np, t->stream));
   count_launches(1);
@@ -546,6 +591,7 @@ b12g_status b12g_transition_matrix(b12g_tree* t, const b12g_scheme* sc, int abso
   ST(t->stage_cnt.ensure(stage, "row staging"));
   ST(t->row_count.ensure(n + 1, "row counts"));
   ST(t->rowptr.ensure(n + 1, "row pointers"));
+  ST(build_current_hash(t, pr));
   RowArgs ra{};
   ra.img = pr.a;
   ra.stage_col = t->stage_col.p;
@@ -576,7 +622,7 @@ b12g_status b12g_transition_matrix(b12g_tree* t, const b12g_scheme* sc, int abso
   if (st == B12G_OK) st = m->rowptr.ensure(n + 1, "rowptr");
   if (st == B12G_OK) st = m->cols.ensure(std::max<uint64_t>(m->nnz, 1), "cols");
   if (st == B12G_OK) st = m->vals.ensure(std::max<uint64_t>(m->nnz, 1), "vals");
-  if (st == B12G_OK) st = m->ctr.ensure(16, "csr counters");
+  if (st == B12G_OK) st = m->ctr.ensure(256, "csr counters");
   if (st == B12G_OK) {
     cudaMemcpyAsync(m->rowptr.p, t->rowptr.p, size_t(n + 1) * 4, cudaMemcpyDeviceToDevice, t->stream);
     gather_rows(t->stage_col.p, t->stage_cnt.p, uint32_t(pr.P), t->row_count.p, t->rowptr.p, t->dn(), m->cols.p,
@@ -618,6 +664,7 @@ b12g_status b12g_csr_destroy(b12g_csr* m)
   m->rowptr.release(); m->cols.release(); m->vals.release(); m->tptr.release(); m->trows.release();
   m->work.release(); m->tiles.release(); m->tvals.release(); m->w0.release(); m->w1.release();
   m->partial.release(); m->vout.release(); m->ctr.release();
+  m->long_flag.release(); m->long_pos.release(); m->long_list.release(); m->mid_list.release();
   if (m->stream) cudaStreamDestroy(m->stream);
   delete m;
   return B12G_OK;
@@ -639,8 +686,20 @@ b12g_status b12g_invariant_measure(b12g_csr* m, uint32_t iters, double* v)
     CK(cudaMemcpyAsync(m->ctr.p, h, sizeof h, cudaMemcpyHostToDevice, s));
     CK(transpose_csr(m->rowptr.p, m->cols.p, m->vals.p, m->ctr.p, m->ctr.p + 1, n, m->nnz, n, m->tptr.p,
                      m->trows.p, m->tvals.p, m->work.p, m->tiles.p, m->ctr.p + 2, s));
+    ST(m->long_flag.ensure(n + 1, "row classes"));
+    ST(m->long_pos.ensure(n + 1, "row classes"));
+    ST(m->long_list.ensure(n + 1, "row classes"));
+    ST(m->mid_list.ensure(n + 1, "row classes"));
+    uint32_t counts[2] = {0, 0};
+    CK(class_rows(m->tptr.p, n, 1, m->long_flag.p, m->long_pos.p, m->mid_list.p, m->ctr.p, m->tiles.p, s));
+    CK(cudaMemcpyAsync(&counts[0], m->long_pos.p + n, 4, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
-    count_launches(6);
+    CK(class_rows(m->tptr.p, n, 2, m->long_flag.p, m->long_pos.p, m->long_list.p, m->ctr.p, m->tiles.p, s));
+    CK(cudaMemcpyAsync(&counts[1], m->long_pos.p + n, 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    m->n_mid = counts[0];
+    m->n_long = counts[1];
+    count_launches(16);
     m->has_transpose = true;
   }
   ST(m->w0.ensure(n, "measure"));
@@ -648,12 +707,12 @@ b12g_status b12g_invariant_measure(b12g_csr* m, uint32_t iters, double* v)
   ST(m->vout.ensure(n, "measure"));
   const int slots = measure_partial_slots();
   ST(m->partial.ensure(slots, "measure"));
-  CK(invariant_measure(m->tptr.p, m->trows.p, m->tvals.p, n, iters, m->w0.p, m->w1.p, m->partial.p, uint32_t(slots),
-                       m->vout.p, m->ctr.p + 8, s));
+  CK(invariant_measure(m->tptr.p, m->trows.p, m->tvals.p, m->mid_list.p, m->n_mid, m->long_list.p, m->n_long, n,
+                       iters, m->w0.p, m->w1.p, m->partial.p, uint32_t(slots), m->vout.p, m->ctr.p + 64, s));
   count_launches(1);
   if (v) CK(cudaMemcpyAsync(v, m->vout.p, size_t(n) * 8, cudaMemcpyDeviceToHost, s));
   uint32_t err = 0;
-  CK(cudaMemcpyAsync(&err, m->ctr.p + 10, 4, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(&err, m->ctr.p + 64 + 64, 4, cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   if (err & 2u) return fail(B12G_ERR_TIMEOUT, "invariant measure: grid barrier gave up");
   return B12G_OK;
@@ -692,6 +751,8 @@ b12g_status b12g_subdivision_run(b12g_tree* t, const b12g_scheme* sc, uint32_t s
   uint64_t cap = std::max<uint64_t>(t->code[0].n, std::max<uint64_t>(4ull * n0, 1ull << 16));
   for (int attempt = 0; attempt < 12; ++attempt) {
     ST(reserve(t, cap));
+    const bool use_hash = int(d0) + int(steps) - 1 <= kHashMaxDepth;
+    if (use_hash) ST(ensure_hash(t, cap));
     Prepared pr;
     ST(prepare(t, sc, pr));
     // key of the captured graph: every pointer and parameter the launches bake in
@@ -699,7 +760,7 @@ b12g_status b12g_subdivision_run(b12g_tree* t, const b12g_scheme* sc, uint32_t s
     std::memcpy(key.data(), sc, sizeof(b12g_scheme));
     uint64_t extra[8] = {steps, cap, uint64_t(t->cur) | uint64_t(t->ncur) << 1 | uint64_t(t->profile) << 2, uint64_t(d0),
                          uint64_t(uintptr_t(t->code[0].p)), uint64_t(uintptr_t(t->hit.p)), uint64_t(uintptr_t(t->table.p)),
-                         uint64_t(uintptr_t(t->code[1].p))};
+                         uint64_t(uintptr_t(t->code[1].p)) ^ (uint64_t(uintptr_t(t->hash.p)) << 1)};
     std::memcpy(key.data() + sizeof(b12g_scheme), extra, sizeof extra);
 
     if (!t->sub_graph || key != t->sub_key) {
@@ -713,9 +774,18 @@ b12g_status b12g_subdivision_run(b12g_tree* t, const b12g_scheme* sc, uint32_t s
       CK(cudaStreamBeginCapture(t->stream, cudaStreamCaptureModeThreadLocal));
       int cur = t->cur, ncur = t->ncur;
       cudaError_t err = cudaSuccess;
+      // the lookup table starts clean at every replay; step s builds with tag s + 1
+      if (use_hash) err = cudaMemsetAsync(t->hash.p, 0, t->hash.n * sizeof(ulonglong2), t->stream);
       for (uint32_t s = 0; s < steps && err == cudaSuccess; ++s) {
         const int o = 1 - cur, no = 1 - ncur;
         ImageArgs a = pr.a;
+        a.hash = LeafHash{nullptr, 0, 0};
+        if (use_hash) {
+          a.hash = LeafHash{t->hash.p, s + 1, t->hash_log2};
+          err = build_leaf_hash(t->code[cur].p, t->ctr.p + ncur, a.hash, t->ctr.p + C_ERROR,
+                                uint32_t(std::min<uint64_t>(cap, 0xFFFFFFFFu)), t->stream);
+          if (err != cudaSuccess) break;
+        }
         a.codes = t->code[cur].p;
         a.n_leaves = t->ctr.p + ncur;
         a.depth = int(d0) + int(s) + 1;
@@ -750,7 +820,7 @@ b12g_status b12g_subdivision_run(b12g_tree* t, const b12g_scheme* sc, uint32_t s
       cudaGraphDestroy(g);
       if (e3 != cudaSuccess) { t->sub_graph = nullptr; return cuda_fail(e3, "instantiate"); }
       t->sub_key = key;
-      t->sub_graph_kernels = 4ull * steps;
+      t->sub_graph_kernels = (use_hash ? 5ull : 4ull) * steps;
       // the events recorded during capture belong to the graph from now on
       for (int k = 0; k < 2; ++k) {
         t->graph_prof[k].assign(t->prof_events[k].begin(), t->prof_events[k].begin() + t->prof_used[k]);
@@ -760,6 +830,7 @@ b12g_status b12g_subdivision_run(b12g_tree* t, const b12g_scheme* sc, uint32_t s
     }
     CK(cudaGraphLaunch(t->sub_graph, t->stream));
     count_launches(t->sub_graph_kernels);
+    if (use_hash) t->hash_tag = steps;
     std::vector<uint32_t> hc(steps);
     CK(cudaMemcpyAsync(hc.data(), t->step_counts.p, steps * 4, cudaMemcpyDeviceToHost, t->stream));
     CK(cudaMemcpyAsync(t->h_ctr + C_ERROR, t->ctr.p + C_ERROR, 4, cudaMemcpyDeviceToHost, t->stream));

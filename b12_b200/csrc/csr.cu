@@ -88,39 +88,19 @@ __global__ void transpose_sort_kernel(const uint32_t* tptr, uint32_t n_cols, uin
 // A sense-reversal grid barrier whose waits give up after a bounded number of polls;
 // co-residency of all blocks is guaranteed by the cooperative launch.
 constexpr unsigned long long kBarrierPolls = 1ull << 24;  // far beyond any real wait (~1 s)
-constexpr int kMeasureThreads = 512;
-constexpr int kRowLanes = 8;                                // lanes per row of P^T
-
-__device__ bool grid_barrier(unsigned* count, unsigned* gen, unsigned* error)
-{
-  __shared__ int ok;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    ok = 1;
-    volatile unsigned* vgen = gen;
-    const unsigned g = *vgen;
-    __threadfence();
-    if (atomicAdd(count, 1u) == gridDim.x - 1) {
-      atomicExch(count, 0u);
-      __threadfence();
-      atomicAdd(gen, 1u);
-    } else {
-      unsigned long long polls = 0;
-      while (*vgen == g) {
-        if (++polls > kBarrierPolls) { atomicOr(error, 2u); ok = 0; break; }
-        if ((polls & 1023u) == 0) __nanosleep(64);
-      }
-    }
-    __threadfence();
-  }
-  __syncthreads();
-  return ok && !(*(volatile unsigned*)error & 2u);
-}
+constexpr int kMeasureThreads = 1024;
+constexpr uint32_t kShortRow = 8;                           // rows of P^T with more entries get 8 lanes
+constexpr uint32_t kMidRow = 64;                            // ... and with more than this a warp
 
 struct MeasureArgs {
   const uint32_t* tptr;      // CSR of P^T
   const uint32_t* trows;
   const double* tvals;
+  const uint32_t* mid_rows;  // rows longer than short_limit, up to kMidRow entries: 8 lanes each
+  uint32_t n_mid;
+  const uint32_t* long_rows; // longer rows: a warp each
+  uint32_t n_long;
+  uint32_t short_limit;      // kShortRow with row lists, else no limit
   uint32_t n;
   uint32_t iters;
   double* w0;
@@ -130,71 +110,176 @@ struct MeasureArgs {
   unsigned* bar_count;
   unsigned* bar_gen;
   unsigned* error;
+  double* totals;            // 2 slots: the L1 norm of the last two iterates
+  unsigned gen_seen;         // completed barriers before the current one
 };
 
-// sum of the per-block partials in one fixed order, identical in every block
-__device__ double sum_partials(const double* part, uint32_t nb, double* bcast)
+// Grid barrier that also reduces: every block has written its partial sum; the last
+// block to arrive adds all partials in one fixed order (lane-strided, then a fixed
+// shuffle tree), publishes the total and releases the others, who poll a generation
+// word with a bounded number of polls.  Returns false when a wait gave up.
+__device__ bool barrier_sum(const MeasureArgs& a, const double* part, double* total_slot, double* total)
 {
-  if (threadIdx.x < 32) {
-    double x = 0.0;
-    for (uint32_t i = threadIdx.x; i < nb; i += 32) x = __dadd_rn(x, __ldcg(part + i));
-#pragma unroll
-    for (int d = 16; d > 0; d >>= 1) x = __dadd_rn(x, __shfl_xor_sync(0xFFFFFFFFu, x, d));
-    if (threadIdx.x == 0) *bcast = x;
+  __shared__ int last;
+  __shared__ int ok;
+  __shared__ double bcast;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ok = 1;
+    __threadfence();
+    last = atomicAdd(a.bar_count, 1u) == gridDim.x - 1;
   }
   __syncthreads();
-  return *bcast;
+  if (last) {
+    if (threadIdx.x < 32) {
+      double x = 0.0;
+#pragma unroll 4
+      for (uint32_t i = threadIdx.x; i < gridDim.x; i += 32) x = __dadd_rn(x, __ldcg(part + i));
+#pragma unroll
+      for (int d = 16; d > 0; d >>= 1) x = __dadd_rn(x, __shfl_xor_sync(0xFFFFFFFFu, x, d));
+      if (threadIdx.x == 0) {
+        __stcg(total_slot, x);
+        bcast = x;
+        atomicExch(a.bar_count, 0u);
+        __threadfence();
+        atomicAdd(a.bar_gen, 1u);
+      }
+    }
+  } else if (threadIdx.x == 0) {
+    volatile unsigned* vgen = a.bar_gen;
+    const unsigned g = a.gen_seen;
+    unsigned long long polls = 0;
+    while (*vgen == g) {
+      if (++polls > kBarrierPolls) { atomicOr(a.error, 2u); ok = 0; break; }
+    }
+    __threadfence();
+    bcast = __ldcg(total_slot);
+  }
+  __syncthreads();
+  *total = bcast;
+  return ok && !(*(volatile unsigned*)a.error & 2u);
 }
 
-// v <- P^T v / |P^T v|_1; rows of P^T are handled by groups of 8 lanes; the previous
-// iterate is scaled by 1/s on the fly, so one grid barrier per iteration suffices
-__global__ void __launch_bounds__(kMeasureThreads) invariant_measure_kernel(const MeasureArgs a)
+__device__ __forceinline__ double iterate_value(const double* wp, uint32_t src, uint32_t it, double v0, double inv)
+{
+  return it == 0 ? v0 : __dmul_rn(__ldcg(wp + src), inv);
+}
+
+// sum of tvals[k] * v(trows[k]) over k = b + off, b + off + step, ... < e, with all
+// index loads issued before the gathers (8 entries per round) so that a round costs two
+// dependent memory latencies whatever its length
+__device__ __forceinline__ double dot_strided(const MeasureArgs& a, const double* wp, uint32_t b, uint32_t e,
+                                              uint32_t off, uint32_t step, uint32_t it, double v0, double inv)
+{
+  double acc = 0.0;
+  for (uint32_t k0 = b + off; k0 < e; k0 += 8 * step) {
+    uint32_t src[8];
+    double val[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const uint32_t k = k0 + q * step;
+      src[q] = k < e ? __ldg(a.trows + k) : 0u;
+      val[q] = k < e ? __ldg(a.tvals + k) : 0.0;
+    }
+    double v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = k0 + q * step < e ? iterate_value(wp, src[q], it, v0, inv) : 0.0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) acc = __fma_rn(val[q], v[q], acc);
+  }
+  return acc;
+}
+
+// v <- P^T v / |P^T v|_1.  Rows of P^T are short (a target box has a handful of source
+// boxes): rows of up to 8 entries get one thread, rows of up to 64 a group of 8 lanes,
+// longer ones a warp, so that every row of an iteration is in flight at once and no
+// thread walks a long dependent chain.  The previous iterate is scaled by 1/s on the
+// fly, so one grid barrier per iteration suffices.
+__global__ void __launch_bounds__(kMeasureThreads) invariant_measure_kernel(MeasureArgs a)
 {
   __shared__ double red[kMeasureThreads / 32];
-  __shared__ double bcast;
   const uint32_t n = a.n;
-  const uint32_t lane8 = threadIdx.x & (kRowLanes - 1);
-  const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) / kRowLanes;
-  const uint32_t groups = gridDim.x * blockDim.x / kRowLanes;
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t nthreads = gridDim.x * blockDim.x;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t warp = tid >> 5, nwarps = nthreads >> 5;
+  const uint32_t group = tid >> 3, ngroups = nthreads >> 3, lane8 = threadIdx.x & 7;
   const double v0 = __ddiv_rn(1.0, double(n));
   double inv = 1.0;
   for (uint32_t it = 0; it < a.iters; ++it) {
     const double* wp = (it & 1u) ? a.w0 : a.w1;
     double* wc = (it & 1u) ? a.w1 : a.w0;
     double local = 0.0;
-    // the loop runs over the warp's first group so that every lane of a warp takes the
-    // same number of trips (the shuffles below need the whole warp)
-    for (uint32_t jb = group & ~3u; jb < n; jb += groups) {
-      const uint32_t j = jb + (group & 3u);
-      const bool row = j < n;
-      double acc = 0.0;
+    // short rows: a thread each
+    for (uint32_t j = tid; j < n; j += nthreads) {
+      const uint32_t b = __ldg(a.tptr + j), e = __ldg(a.tptr + j + 1);
+      if (e - b > a.short_limit) continue;
+      const double acc = dot_strided(a, wp, b, e, 0u, 1u, it, v0, inv);
+      __stcg(wc + j, acc);
+      local = __dadd_rn(local, fabs(acc));
+    }
+    // medium rows: 8 lanes each (trip counts uniform per warp for the shuffles)
+    for (uint32_t qb = group & ~3u; qb < a.n_mid; qb += ngroups) {
+      const uint32_t q = qb + (group & 3u);
+      const bool row = q < a.n_mid;
+      const uint32_t j = row ? __ldg(a.mid_rows + q) : 0u;
       const uint32_t b = row ? __ldg(a.tptr + j) : 0u, e = row ? __ldg(a.tptr + j + 1) : 0u;
-      for (uint32_t k = b + lane8; k < e; k += kRowLanes) {
-        const double v = it == 0 ? v0 : __dmul_rn(__ldcg(wp + __ldg(a.trows + k)), inv);
-        acc = __fma_rn(__ldg(a.tvals + k), v, acc);
-      }
+      double acc = dot_strided(a, wp, b, e, lane8, 8u, it, v0, inv);
 #pragma unroll
-      for (int d = kRowLanes / 2; d > 0; d >>= 1) acc = __dadd_rn(acc, __shfl_xor_sync(0xFFFFFFFFu, acc, d));
-      if (lane8 == 0 && row) {
+      for (int d = 4; d > 0; d >>= 1) acc = __dadd_rn(acc, __shfl_xor_sync(0xFFFFFFFFu, acc, d));
+      if (row && lane8 == 0) {
+        __stcg(wc + j, acc);
+        local = __dadd_rn(local, fabs(acc));
+      }
+    }
+    // long rows: a warp each
+    for (uint32_t q = warp; q < a.n_long; q += nwarps) {
+      const uint32_t j = __ldg(a.long_rows + q);
+      const uint32_t b = __ldg(a.tptr + j), e = __ldg(a.tptr + j + 1);
+      double acc = dot_strided(a, wp, b, e, lane, 32u, it, v0, inv);
+#pragma unroll
+      for (int d = 16; d > 0; d >>= 1) acc = __dadd_rn(acc, __shfl_xor_sync(0xFFFFFFFFu, acc, d));
+      if (lane == 0) {
         __stcg(wc + j, acc);
         local = __dadd_rn(local, fabs(acc));
       }
     }
 #pragma unroll
     for (int d = 16; d > 0; d >>= 1) local = __dadd_rn(local, __shfl_xor_sync(0xFFFFFFFFu, local, d));
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = local;
+    if (lane == 0) red[threadIdx.x >> 5] = local;
     __syncthreads();
     if (threadIdx.x == 0) {
       double t = 0.0;
       for (int i = 0; i < kMeasureThreads / 32; ++i) t = __dadd_rn(t, red[i]);
       __stcg(a.partial + (it & 1u) * gridDim.x + blockIdx.x, t);
     }
-    if (!grid_barrier(a.bar_count, a.bar_gen, a.error)) return;
-    inv = __ddiv_rn(1.0, sum_partials(a.partial + (it & 1u) * gridDim.x, gridDim.x, &bcast));
+    a.gen_seen = it;  // the generation counts completed barriers
+    double s_it;
+    if (!barrier_sum(a, a.partial + (it & 1u) * gridDim.x, a.totals + (it & 1u), &s_it)) return;
+    inv = __ddiv_rn(1.0, s_it);
   }
   const double* wl = (a.iters & 1u) ? a.w0 : a.w1;
+  for (uint32_t j = tid; j < n; j += nthreads) a.out[j] = a.iters ? __dmul_rn(__ldcg(wl + j), inv) : v0;
+}
+
+// the rows of P^T of one length class (1: medium, 2: long), ascending (flag, scan, scatter)
+__device__ __forceinline__ uint32_t row_class(const uint32_t* tptr, uint32_t j)
+{
+  const uint32_t len = tptr[j + 1] - tptr[j];
+  return len <= kShortRow ? 0u : (len <= kMidRow ? 1u : 2u);
+}
+
+__global__ void class_flag_kernel(const uint32_t* tptr, uint32_t n, uint32_t cls, uint32_t* flag)
+{
   for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
-    a.out[j] = a.iters ? __dmul_rn(__ldcg(wl + j), inv) : v0;
+    flag[j] = row_class(tptr, j) == cls ? 1u : 0u;
+}
+
+__global__ void class_scatter_kernel(const uint32_t* tptr, uint32_t n, uint32_t cls, const uint32_t* pos,
+                                     uint32_t* list)
+{
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+    if (row_class(tptr, j) == cls) list[pos[j]] = j;
 }
 
 }  // namespace
@@ -225,21 +310,38 @@ cudaError_t transpose_csr(const uint32_t* rowptr, const uint32_t* cols, const do
   return cudaGetLastError();
 }
 
-cudaError_t invariant_measure(const uint32_t* tptr, const uint32_t* trows, const double* tvals, uint32_t n,
-                              uint32_t iters, double* w0, double* w1, double* partial, uint32_t partial_cap,
-                              double* out, unsigned* sync_words, cudaStream_t s)
+cudaError_t class_rows(const uint32_t* tptr, uint32_t n, uint32_t cls, uint32_t* flag, uint32_t* pos,
+                       uint32_t* list, const uint32_t* n_dev, uint32_t* tile_sums, cudaStream_t s)
+{
+  class_flag_kernel<<<grid_for(n, kThreads, 8), kThreads, 0, s>>>(tptr, n, cls, flag);
+  cudaError_t e = exclusive_scan_u32(flag, pos, n_dev, tile_sums, n, s);
+  if (e != cudaSuccess) return e;
+  class_scatter_kernel<<<grid_for(n, kThreads, 8), kThreads, 0, s>>>(tptr, n, cls, pos, list);
+  return cudaGetLastError();
+}
+
+cudaError_t invariant_measure(const uint32_t* tptr, const uint32_t* trows, const double* tvals,
+                              const uint32_t* mid_list, uint32_t n_mid, const uint32_t* long_list, uint32_t n_long,
+                              uint32_t n, uint32_t iters, double* w0, double* w1, double* partial,
+                              uint32_t partial_cap, double* out, unsigned* sync_words, cudaStream_t s)
 {
   static int blocks_per_sm = 0;
   if (!blocks_per_sm) {
     int b = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, invariant_measure_kernel, kMeasureThreads, 0);
-    blocks_per_sm = b > 0 ? (b < 2 ? b : 2) : 1;
+    blocks_per_sm = b > 0 ? b : 1;
   }
-  int grid = grid_for(uint64_t(n) * kRowLanes, kMeasureThreads, blocks_per_sm);
+  int grid = grid_for(n, kMeasureThreads, blocks_per_sm);
   if (grid > int(partial_cap / 2)) grid = int(partial_cap / 2);
   if (grid < 1) grid = 1;
-  cudaMemsetAsync(sync_words, 0, 3 * sizeof(unsigned), s);
-  MeasureArgs a{tptr, trows, tvals, n, iters, w0, w1, partial, out, sync_words, sync_words + 1, sync_words + 2};
+  if (grid > int(partial_cap / 2) - 1) grid = int(partial_cap / 2) - 1;
+  cudaMemsetAsync(sync_words, 0, 65 * sizeof(unsigned), s);
+  // partial: 2 x grid per-block sums, then 2 totals
+  // barrier words on separate 128-byte lines: arrival count, generation, error
+  const bool lists = mid_list && long_list;
+  MeasureArgs a{tptr, trows, tvals, mid_list, lists ? n_mid : 0u, long_list, lists ? n_long : 0u,
+                lists ? kShortRow : 0xFFFFFFFFu, n, iters, w0, w1, partial, out, sync_words, sync_words + 32,
+                sync_words + 64, partial + 2 * size_t(grid), 0u};
   void* params[] = {&a};
   return cudaLaunchCooperativeKernel((const void*)invariant_measure_kernel, dim3(grid), dim3(kMeasureThreads), params,
                                      0, s);

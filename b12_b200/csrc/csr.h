@@ -13,11 +13,18 @@ cudaError_t transpose_csr(const uint32_t* rowptr, const uint32_t* cols, const do
                           uint32_t* tptr, uint32_t* trows, double* tvals, uint32_t* work, uint32_t* tile_sums,
                           const uint32_t* n_cols_dev, cudaStream_t s);
 
-// power iteration on the CSR of P^T; sync_words: 3 u32 (barrier count, generation,
-// error: bit 1 = barrier timeout); partial: partial_cap doubles
-cudaError_t invariant_measure(const uint32_t* tptr, const uint32_t* trows, const double* tvals, uint32_t n,
-                              uint32_t iters, double* w0, double* w1, double* partial, uint32_t partial_cap,
-                              double* out, unsigned* sync_words, cudaStream_t s);
+// the rows of P^T of one length class (1: 9..64 entries, 2: more), ascending; the count
+// ends up in pos[n] (flag, pos: n + 1 u32; list: n u32; n_dev: device copy of n)
+cudaError_t class_rows(const uint32_t* tptr, uint32_t n, uint32_t cls, uint32_t* flag, uint32_t* pos,
+                       uint32_t* list, const uint32_t* n_dev, uint32_t* tile_sums, cudaStream_t s);
+
+// power iteration on the CSR of P^T with the medium and long rows listed by class_rows
+// (both lists nullptr: every row gets one thread); sync_words: 65 u32 (barrier count at
+// 0, generation at 32, error at 64: bit 1 = barrier timeout); partial: partial_cap doubles
+cudaError_t invariant_measure(const uint32_t* tptr, const uint32_t* trows, const double* tvals,
+                              const uint32_t* mid_list, uint32_t n_mid, const uint32_t* long_list, uint32_t n_long,
+                              uint32_t n, uint32_t iters, double* w0, double* w1, double* partial,
+                              uint32_t partial_cap, double* out, unsigned* sync_words, cudaStream_t s);
 int measure_partial_slots();
 
 }  // namespace b12g

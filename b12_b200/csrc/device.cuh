@@ -72,10 +72,87 @@ struct GridParams {
 template<int D>
 __device__ __forceinline__ int bisections(int depth, int j) { return depth / D + (j < depth % D ? 1 : 0); }
 
-// extract the k bits of dimension j from a depth-d code, first bisection = MSB
+// bit spreading: bit i of x goes to bit D*i (magic-number shifts), and back
+template<int D> struct Bits;
+template<> struct Bits<1> {
+  static constexpr int kMax = 64;
+  static __device__ __forceinline__ uint64_t spread(uint64_t x) { return x; }
+  static __device__ __forceinline__ uint64_t compact(uint64_t x) { return x; }
+};
+template<> struct Bits<2> {
+  static constexpr int kMax = 32;
+  static __device__ __forceinline__ uint64_t spread(uint64_t x)
+  {
+    x &= 0xFFFFFFFFull;
+    x = (x | (x << 16)) & 0x0000FFFF0000FFFFull;
+    x = (x | (x << 8)) & 0x00FF00FF00FF00FFull;
+    x = (x | (x << 4)) & 0x0F0F0F0F0F0F0F0Full;
+    x = (x | (x << 2)) & 0x3333333333333333ull;
+    return (x | (x << 1)) & 0x5555555555555555ull;
+  }
+  static __device__ __forceinline__ uint64_t compact(uint64_t x)
+  {
+    x &= 0x5555555555555555ull;
+    x = (x ^ (x >> 1)) & 0x3333333333333333ull;
+    x = (x ^ (x >> 2)) & 0x0F0F0F0F0F0F0F0Full;
+    x = (x ^ (x >> 4)) & 0x00FF00FF00FF00FFull;
+    x = (x ^ (x >> 8)) & 0x0000FFFF0000FFFFull;
+    return (x ^ (x >> 16)) & 0x00000000FFFFFFFFull;
+  }
+};
+template<> struct Bits<3> {
+  static constexpr int kMax = 21;
+  static __device__ __forceinline__ uint64_t spread(uint64_t x)
+  {
+    x &= 0x1FFFFFull;
+    x = (x | (x << 32)) & 0x1F00000000FFFFull;
+    x = (x | (x << 16)) & 0x1F0000FF0000FFull;
+    x = (x | (x << 8)) & 0x100F00F00F00F00Full;
+    x = (x | (x << 4)) & 0x10C30C30C30C30C3ull;
+    return (x | (x << 2)) & 0x1249249249249249ull;
+  }
+  static __device__ __forceinline__ uint64_t compact(uint64_t x)
+  {
+    x &= 0x1249249249249249ull;
+    x = (x ^ (x >> 2)) & 0x10C30C30C30C30C3ull;
+    x = (x ^ (x >> 4)) & 0x100F00F00F00F00Full;
+    x = (x ^ (x >> 8)) & 0x1F0000FF0000FFull;
+    x = (x ^ (x >> 16)) & 0x1F00000000FFFFull;
+    return (x ^ (x >> 32)) & 0x1FFFFFull;
+  }
+};
+template<> struct Bits<4> {
+  static constexpr int kMax = 16;
+  static __device__ __forceinline__ uint64_t spread(uint64_t x)
+  {
+    x &= 0xFFFFull;
+    x = (x | (x << 24)) & 0x000000FF000000FFull;
+    x = (x | (x << 12)) & 0x000F000F000F000Full;
+    x = (x | (x << 6)) & 0x0303030303030303ull;
+    return (x | (x << 3)) & 0x1111111111111111ull;
+  }
+  static __device__ __forceinline__ uint64_t compact(uint64_t x)
+  {
+    x &= 0x1111111111111111ull;
+    x = (x ^ (x >> 3)) & 0x0303030303030303ull;
+    x = (x ^ (x >> 6)) & 0x000F000F000F000Full;
+    x = (x ^ (x >> 12)) & 0x000000FF000000FFull;
+    return (x ^ (x >> 24)) & 0x000000000000FFFFull;
+  }
+};
+
+// extract the k bits of dimension j from a depth-d code, first bisection = MSB.
+// Padding the code to K = ceil(d/D) full rounds puts dimension j's bits at positions
+// D*m + (D-1-j), so one compaction extracts them.
 template<int D>
 __device__ __forceinline__ uint32_t deinterleave(uint64_t code, int depth, int j)
 {
+  const int K = (depth + D - 1) / D;
+  if (K <= Bits<D>::kMax && D * K <= 64) {
+    const int k = depth / D + (j < depth % D ? 1 : 0);
+    const uint64_t x = (code << (D * K - depth)) >> (D - 1 - j);
+    return uint32_t(Bits<D>::compact(x) >> (K - k));
+  }
   uint32_t bits = 0;
   for (int t = j; t < depth; t += D) bits = (bits << 1) | uint32_t((code >> (depth - 1 - t)) & 1u);
   return bits;
@@ -84,10 +161,16 @@ __device__ __forceinline__ uint32_t deinterleave(uint64_t code, int depth, int j
 template<int D>
 __device__ __forceinline__ uint64_t interleave(const uint32_t (&bits)[D], const int (&k)[D], int depth)
 {
+  const int K = (depth + D - 1) / D;
+  if (K <= Bits<D>::kMax && D * K <= 64) {
+    uint64_t x = 0;
+#pragma unroll
+    for (int j = 0; j < D; ++j) x |= Bits<D>::spread(uint64_t(bits[j]) << (K - k[j])) << (D - 1 - j);
+    return depth == 0 ? 0ull : x >> (D * K - depth);
+  }
   uint64_t code = 0;
-  const int rounds = (depth + D - 1) / D;
 #pragma unroll 1
-  for (int m = 0; m < rounds; ++m) {
+  for (int m = 0; m < K; ++m) {
 #pragma unroll
     for (int j = 0; j < D; ++j)
       if (m * D + j < depth) code = (code << 1) | uint64_t((bits[j] >> (k[j] - 1 - m)) & 1u);
@@ -156,6 +239,58 @@ __device__ __forceinline__ uint32_t locate(const uint64_t* __restrict__ codes, u
 }
 
 // ---------------------------------------------------------------------------------
+// O(1) point location: an open-addressing hash of the leaf codes (linear probing,
+// 16-byte slots {tag<<56 | code, leaf index}), built once per leaf set.  A slot whose
+// tag differs from the current build's tag is empty, so a table is reused across
+// builds without clearing; lookups return the same index the binary search would.
+// ---------------------------------------------------------------------------------
+struct LeafHash {
+  ulonglong2* slots;         // nullptr: use the binary search
+  uint32_t tag;              // 1..255
+  uint32_t log2_cap;         // table capacity (slots allocated) = 2^log2_cap
+};
+
+constexpr int kHashMaxDepth = 56;
+
+// slots used for n keys: the smallest power of two >= 2n (load factor <= 1/2), >= 2^6
+__device__ __forceinline__ int hash_log2(uint32_t n)
+{
+  const uint64_t want = 2ull * n;
+  int l = 6;
+  while ((1ull << l) < want) ++l;
+  return l;
+}
+
+__device__ __forceinline__ uint64_t hash_slot(uint64_t code, int log2)
+{
+  return (code * 0x9E3779B97F4A7C15ull) >> (64 - log2);
+}
+
+__device__ __forceinline__ uint32_t hash_locate(const LeafHash& h, uint32_t n, uint64_t code)
+{
+  const int l = hash_log2(n);
+  const uint64_t mask = (1ull << l) - 1ull;
+  const uint64_t key = (uint64_t(h.tag) << 56) | code;
+  uint64_t s = hash_slot(code, l);
+  for (uint64_t probe = 0; probe <= mask; ++probe) {
+    const ulonglong2 e = __ldg(h.slots + s);
+    if (e.x == key) return uint32_t(e.y);
+    if ((e.x >> 56) != h.tag) return kInvalidIndex;
+    s = (s + 1) & mask;
+  }
+  return kInvalidIndex;
+}
+
+// leaf index of a depth-d code: hash when built, binary search otherwise (with the
+// out-of-domain rule of `locate`)
+__device__ __forceinline__ uint32_t find_leaf(const LeafHash& h, const uint64_t* codes, uint32_t n, bool valid,
+                                              uint64_t code)
+{
+  if (!h.slots || !valid || n == 0) return locate(codes, n, valid, code);
+  return hash_locate(h, n, code);
+}
+
+// ---------------------------------------------------------------------------------
 // grids (Grids.hpp)
 // ---------------------------------------------------------------------------------
 // Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11)
@@ -177,8 +312,17 @@ __device__ __forceinline__ double philox_signed(uint32_t hi, uint32_t lo)
   return __dsub_rn(__dmul_rn(2.0, double(m) * 0x1p-53), 1.0);
 }
 
+// Inner and full grids read a per-block table of the P grid points (dimension-major,
+// built from the 1-D coordinates at kernel start) instead of splitting the point index
+// into digits for every point.
 struct InnerGrid {
-  // InnerGrid::operator() (Grids.hpp:105-120): coordinate table built on the host
+  static constexpr bool kTable = true;
+  // InnerGrid::operator() (Grids.hpp:105-120): digit j of the point index picks coord[]
+  static __device__ __forceinline__ double table_value(const GridParams& g, const double* coord, uint32_t k, int j)
+  {
+    for (int q = 0; q < j; ++q) k /= g.n;
+    return coord[k % g.n];
+  }
   template<int D>
   static __device__ __forceinline__ void point(const GridParams& g, const double* coord, uint64_t /*i*/,
                                                uint32_t k, double* res)
@@ -189,7 +333,13 @@ struct InnerGrid {
 };
 
 struct FullGrid {
-  // FullGrid::operator() (Grids.hpp:67-83)
+  static constexpr bool kTable = true;
+  // FullGrid::operator() (Grids.hpp:67-83), stretched by 1 + eps
+  static __device__ __forceinline__ double table_value(const GridParams& g, const double* coord, uint32_t k, int j)
+  {
+    for (int q = 0; q < j; ++q) k /= g.n;
+    return __dmul_rn(coord[k % g.n], g.eps1);
+  }
   template<int D>
   static __device__ __forceinline__ void point(const GridParams& g, const double* coord, uint64_t /*i*/,
                                                uint32_t k, double* res)
@@ -200,6 +350,8 @@ struct FullGrid {
 };
 
 struct PhiloxGrid {
+  static constexpr bool kTable = false;
+  static __device__ __forceinline__ double table_value(const GridParams&, const double*, uint32_t, int) { return 0.0; }
   // uniform points in [-1,1)^D keyed by (seed, global point index i)
   template<int D>
   static __device__ __forceinline__ void point(const GridParams& g, const double* /*coord*/, uint64_t i,

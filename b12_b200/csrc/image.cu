@@ -21,13 +21,20 @@ struct PointImage {
     return a.children ? ((__ldg(a.codes + (leaf >> 1)) << 1) | uint64_t(leaf & 1u)) : __ldg(a.codes + leaf);
   }
 
-  // returns the target code validity; `tcode` the depth-d code of the image point
-  static __device__ __forceinline__ bool image(const ImageArgs& a, const double* coord, uint64_t code,
+  // returns the target code validity; `tcode` the depth-d code of the image point.
+  // `pts` is the block's grid-point table (dimension-major, P entries per dimension)
+  // when the grid has one, else the 1-D coordinate table.
+  static __device__ __forceinline__ bool image(const ImageArgs& a, const double* pts, bool use_table, uint64_t code,
                                                uint64_t i, uint32_t k, uint64_t& tcode)
   {
     double c[D], r[D], g[D], x[D], y[D];
     box_coordinates<D>(a.dom, code, a.depth, c, r);
-    Grid::template point<D>(a.grid, coord, i, k, g);
+    if (Grid::kTable && use_table) {
+#pragma unroll
+      for (int j = 0; j < D; ++j) g[j] = pts[j * uint32_t(a.points) + k];
+    } else {
+      Grid::template point<D>(a.grid, pts, i, k, g);
+    }
 #pragma unroll
     for (int j = 0; j < D; ++j) x[j] = __dadd_rn(c[j], __dmul_rn(g[j], r[j]));
     Map::apply(a.map, x, y);
@@ -36,25 +43,39 @@ struct PointImage {
 
   static __device__ __forceinline__ uint32_t target(const ImageArgs& a, uint32_t n, bool valid, uint64_t tcode)
   {
-    if (!a.children) return locate(a.codes, n, valid, tcode);
+    if (!a.children) return find_leaf(a.hash, a.codes, n, valid, tcode);
     if (!valid) return kInvalidIndex;
-    const uint32_t p = locate(a.codes, n, true, tcode >> 1);
+    const uint32_t p = find_leaf(a.hash, a.codes, n, true, tcode >> 1);
     return p == kInvalidIndex ? kInvalidIndex : 2u * p + uint32_t(tcode & 1u);
   }
 };
 
-__device__ __forceinline__ void load_coords(const GridParams& g, double* smem)
+constexpr uint32_t kPointTable = 2048;  // doubles of grid-point table per block (16 KB)
+
+// fills `pts` with the P x D grid points when they fit (returns true), else with the
+// 1-D coordinates for the per-point path
+template<class Grid, int D>
+__device__ __forceinline__ bool load_points(const GridParams& g, uint64_t P, double* pts)
 {
-  for (uint32_t i = threadIdx.x; i < 64; i += blockDim.x) smem[i] = g.coord[i];
+  const bool table = Grid::kTable && P * D <= kPointTable;
+  if (table) {
+    for (uint32_t idx = threadIdx.x; idx < uint32_t(P) * D; idx += blockDim.x) {
+      const int j = int(idx / uint32_t(P));
+      pts[idx] = Grid::table_value(g, g.coord, idx - uint32_t(j) * uint32_t(P), j);
+    }
+  } else {
+    for (uint32_t i = threadIdx.x; i < 64; i += blockDim.x) pts[i] = g.coord[i];
+  }
   __syncthreads();
+  return table;
 }
 
 template<class Map, class Grid, ImageMode M>
 __global__ void __launch_bounds__(kThreads) image_points_kernel(const ImageArgs a)
 {
   using PI = PointImage<Map, Grid>;
-  __shared__ double coord[64];
-  load_coords(a.grid, coord);
+  __shared__ double pts[kPointTable];
+  const bool table = load_points<Grid, Map::D>(a.grid, a.points, pts);
 
   const uint32_t n = *a.n_leaves;
   const uint32_t nboxes = a.n_src ? *a.n_src : (a.children ? 2u * n : n);
@@ -66,30 +87,28 @@ __global__ void __launch_bounds__(kThreads) image_points_kernel(const ImageArgs 
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(a.error, 1u);
     return;
   }
+  // point g = rank * P + k; (rank, k) advance by (stride / P, stride % P) per trip
+  const uint64_t g0 = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  uint64_t rank = g0 / P;
+  uint64_t k = g0 - rank * P;
+  const uint64_t rank_step = stride / P, k_step = stride - rank_step * P;
 
   // the loop trip count is uniform per warp so that warp collectives stay converged
-  for (uint64_t base = uint64_t(blockIdx.x) * blockDim.x + (threadIdx.x & ~31u); base < total; base += stride) {
+  for (uint64_t base = g0 - lane; base < total; base += stride) {
     const uint64_t g = base + lane;
     const bool active = g < total;
     uint32_t t = kInvalidIndex;
     uint64_t tcode = 0;
     bool valid = false;
     if (active) {
-      uint64_t rank;
-      uint32_t k;
-      if (total <= 0xFFFFFFFFull) {
-        const uint32_t g32 = uint32_t(g), P32 = uint32_t(P);
-        rank = g32 / P32;
-        k = g32 - uint32_t(rank) * P32;
-      } else {
-        rank = g / P;
-        k = uint32_t(g - rank * P);
-      }
       const uint32_t leaf = a.src ? __ldg(a.src + rank) : uint32_t(rank);
       const uint64_t code = PI::source_code(a, leaf);
-      valid = PI::image(a, coord, code, g, k, tcode);
+      valid = PI::image(a, pts, table, code, g, uint32_t(k), tcode);
       t = PI::target(a, n, valid, tcode);
     }
+    rank += rank_step;
+    k += k_step;
+    if (k >= P) { k -= P; ++rank; }
     if constexpr (M == ImageMode::Hit) {
       // one store per distinct target in the warp
       const unsigned peers = __match_any_sync(0xFFFFFFFFu, t);
@@ -99,9 +118,9 @@ __global__ void __launch_bounds__(kThreads) image_points_kernel(const ImageArgs 
     } else {
       // candidates: valid images that are not leaves; deduplicated within the warp and
       // appended with one atomic per warp
-      if (a.hit && active && t != kInvalidIndex) {
-        const unsigned hp = __match_any_sync(__activemask(), t);
-        if (lane == __ffs(hp) - 1) a.hit[t] = 1;
+      if (a.hit) {
+        const unsigned hp = __match_any_sync(0xFFFFFFFFu, t);
+        if (active && t != kInvalidIndex && lane == __ffs(hp) - 1) a.hit[t] = 1;
       }
       const bool is_cand = active && valid && t == kInvalidIndex;
       const uint64_t key = is_cand ? tcode : kInvalidCode;
@@ -153,10 +172,10 @@ __global__ void __launch_bounds__(kThreads) transition_rows_kernel(const RowArgs
 {
   using PI = PointImage<Map, Grid>;
   const ImageArgs& a = ra.img;
-  __shared__ double coord[64];
+  __shared__ double pts[kPointTable];
   __shared__ uint32_t keys[kRowWarps][128];
   __shared__ uint32_t bounds[kRowWarps][4];
-  load_coords(a.grid, coord);
+  const bool table = load_points<Grid, Map::D>(a.grid, a.points, pts);
 
   const uint32_t n = *a.n_leaves;
   const uint32_t nrows = a.n_src ? *a.n_src : n;
@@ -174,7 +193,7 @@ __global__ void __launch_bounds__(kThreads) transition_rows_kernel(const RowArgs
       uint32_t key = kPadKey;
       if (k < P) {
         uint64_t tcode;
-        const bool valid = PI::image(a, coord, code, uint64_t(row) * P + k, k, tcode);
+        const bool valid = PI::image(a, pts, table, code, uint64_t(row) * P + k, k, tcode);
         const uint32_t t = PI::target(a, n, valid, tcode);
         key = t == kInvalidIndex ? kLostKey : t;
       }

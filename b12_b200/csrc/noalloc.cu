@@ -23,7 +23,7 @@ namespace {
 
 constexpr uint32_t kMaxRows = 1u << 18;          // 262,144 boxes
 constexpr uint32_t kPartialSlots = 4096;         // 2 x the largest grid of the launch
-constexpr size_t kScratchBytes = 2 * size_t(kMaxRows) * sizeof(double) + kPartialSlots * sizeof(double) + 256;
+constexpr size_t kScratchBytes = 2 * size_t(kMaxRows) * sizeof(double) + kPartialSlots * sizeof(double) + 512;
 
 static __device__ __align__(256) unsigned char g_measure_scratch[kScratchBytes];
 
@@ -68,10 +68,11 @@ extern "C" b12g_status b12g_invariant_measure_noalloc(const uint32_t* tptr, cons
   double* partial = w1 + kMaxRows;
   unsigned* sync_words = reinterpret_cast<unsigned*>(partial + kPartialSlots);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  CK(b12g::invariant_measure(tptr, trows, tvals, n, iters, w0, w1, partial, kPartialSlots, v, sync_words, s));
+  CK(b12g::invariant_measure(tptr, trows, tvals, nullptr, 0, nullptr, 0, n, iters, w0, w1, partial, kPartialSlots, v,
+                             sync_words, s));
   b12g::count_launches(1);
   unsigned err = 0;
-  CK(cudaMemcpyAsync(&err, sync_words + 2, sizeof err, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(&err, sync_words + 64, sizeof err, cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   if (err & 2u) return fail(B12G_ERR_TIMEOUT, "invariant_measure_noalloc: grid barrier gave up");
   return B12G_OK;

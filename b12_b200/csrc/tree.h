@@ -113,6 +113,9 @@ struct b12g_tree {
   Buf<double> points;
   Buf<uint32_t> step_counts;
   Buf<uint8_t> sort_tmp;
+  Buf<ulonglong2> hash;        // leaf lookup table
+  uint32_t hash_tag = 0;       // tag of the last build (1..255; 0 = cleared)
+  uint32_t hash_log2 = 0;      // log2 of the table's slots
   uint32_t* h_ctr = nullptr;   // pinned mirror of ctr
   // graph cache of the fused subdivision loop
   cudaGraphExec_t sub_graph = nullptr;
@@ -140,7 +143,8 @@ struct b12g_csr {
   Buf<uint32_t> rowptr, cols;
   Buf<double> vals;
   // P^T, built on first use by the invariant measure
-  Buf<uint32_t> tptr, trows, work, tiles;
+  Buf<uint32_t> tptr, trows, work, tiles, long_flag, long_pos, long_list, mid_list;
+  uint32_t n_long = 0, n_mid = 0;
   Buf<double> tvals, w0, w1, partial, vout;
   Buf<uint32_t> ctr;
   bool has_transpose = false;
@@ -166,6 +170,12 @@ b12g_status select_sources(b12g_tree* t, const b12g_scheme* sc, Prepared& pr, ui
 b12g_status check_error(b12g_tree* t, const char* where);
 b12g_status set_root(b12g_tree* t, uint8_t flags);
 b12g_status flag_call(b12g_tree* t, int op, uint8_t u, uint8_t f, uint8_t depth, uint32_t* n_changed);
+// make the lookup table hold up to max_n codes (clears it when it grows)
+b12g_status ensure_hash(b12g_tree* t, uint64_t max_n);
+// next build tag (clears the table when the 8-bit tag would wrap)
+b12g_status next_hash_tag(b12g_tree* t, uint32_t* tag);
+// build the table for the current leaves and point pr.a.hash at it (no-op above depth 56)
+b12g_status build_current_hash(b12g_tree* t, Prepared& pr);
 // record a timing event of `kind` (0: box-image kernel, 1: transition rows) on the tree stream
 void prof_mark(b12g_tree* t, int kind);
 b12g_status prof_collect(b12g_tree* t);

@@ -130,6 +130,41 @@ __global__ void split_kernel(const uint64_t* code, const uint8_t* flags, const u
 }
 
 // ---------------------------------------------------------------------------------
+// leaf lookup table: linear-probing inserts with a 64-bit CAS on the key word; a CAS
+// that loses to another insert re-reads the same slot (which now carries the current
+// tag) and moves on, so every insert ends within the table size
+// ---------------------------------------------------------------------------------
+__global__ void hash_build_kernel(const uint64_t* codes, const uint32_t* n_ptr, LeafHash h, uint32_t* error)
+{
+  const uint32_t n = *n_ptr;
+  const int l = hash_log2(n);
+  if (l > int(h.log2_cap)) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(error, 1u);
+    return;
+  }
+  const uint64_t mask = (1ull << l) - 1ull;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint64_t code = codes[i];
+    const unsigned long long key = (uint64_t(h.tag) << 56) | code;
+    uint64_t s = hash_slot(code, l);
+    bool done = false;
+    for (uint64_t step = 0; step <= 2 * mask + 64 && !done; ++step) {
+      unsigned long long* kw = reinterpret_cast<unsigned long long*>(&h.slots[s].x);
+      const unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(kw);
+      if ((cur >> 56) != h.tag) {
+        if (atomicCAS(kw, cur, key) == cur) {
+          h.slots[s].y = i;
+          done = true;
+        }
+        continue;  // lost the slot to another insert: look at it again
+      }
+      s = (s + 1) & mask;
+    }
+    if (!done) atomicOr(error, 1u);
+  }
+}
+
+// ---------------------------------------------------------------------------------
 // compaction: tile counts -> single-block tile scan -> ordered scatter
 // ---------------------------------------------------------------------------------
 // element count; 0 (with error bit 0) if the children do not fit the hit mask
@@ -313,6 +348,13 @@ cudaError_t split_codes(const uint64_t* code, const uint8_t* flags, const uint32
                         uint8_t* out_flags, uint32_t* n_out, uint32_t max_n, cudaStream_t s)
 {
   split_kernel<<<grid_for(max_n, kThreads, 8), kThreads, 0, s>>>(code, flags, n, out_code, out_flags, n_out);
+  return cudaGetLastError();
+}
+
+cudaError_t build_leaf_hash(const uint64_t* codes, const uint32_t* n, LeafHash h, uint32_t* error, uint32_t max_n,
+                            cudaStream_t s)
+{
+  hash_build_kernel<<<grid_for(max_n, kThreads, 8), kThreads, 0, s>>>(codes, n, h, error);
   return cudaGetLastError();
 }
 

@@ -6,6 +6,12 @@ One step = one whole Lorenz job of the reference's subdivision driver
 5x5x5 inner grid, domain centre (0,0,27) radius (30,30,40)), the CSR transition matrix
 on the final boxes, and 200 FP64 power iterations for the invariant measure.
 
+The headline uses the explicit-FMA integrator (the same fused multiply-adds in the
+kernel, the oracle and the reference harness's plug-in map); its box sets and transition
+matrix equal the reference's strict (-fmad=false) run at every step on this workload.
+The strict integrator - one rounding per operation, the reference's own Map_Lorenz.h
+order - is measured in the same run and reported under "strict".
+
 metric = box-images per second (a box-image is one box's 125 test points sampled,
 integrated and located): the subdivision steps image 2*n(k-1) boxes each, the transition
 matrix n(27).  Inputs are synthetic: the workload is defined entirely by its parameters.
@@ -39,7 +45,7 @@ METRIC = "Lorenz box-images/s"
 UNIT = "box-images/s"
 CONFIG = {"workload": "lorenz-rk4-depth27", "sigma": 10.0, "rho": 28.0, "beta": 8.0 / 3.0, "h": 0.01,
           "rk4_steps": 20, "grid": "inner 5x5x5", "depth": DEPTH, "tm": "csr", "measure_iters": MEASURE_ITERS,
-          "l2": "flushed between timed steps (256 MiB write)", "arith": "strict"}
+          "l2": "flushed between timed steps (256 MiB write)", "arith": "fma"}
 NOMINAL_FP64_TFLOPS = 37.0
 
 
@@ -196,48 +202,43 @@ def box_images_of(counts) -> tuple[int, int]:
     return int(2 * prev.sum()), int(counts[-1])
 
 
-def gpu_arm(args, rank: int, world: int, dist):
+def measure_mode(args, rank, world, dist, fma: bool, peak_tflops: float):
+    """Time args.steps whole jobs with the given integrator arithmetic."""
     import torch
     import b12_b200 as B
     from b12_b200 import tree as T
 
-    dev = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(dev)
-    sc = B.Scheme(B.lorenz(rho=28.0, fma=args.fma), B.inner_grid(5))
+    dev = torch.cuda.current_device()
+    sc = B.Scheme(B.lorenz(rho=28.0, fma=fma), B.inner_grid(5))
     tree = B.ImplicitBoxTree([0.0, 0.0, 27.0], [30.0, 30.0, 40.0])
     tree.reserve(1 << 20)
     stream = torch.cuda.ExternalStream(tree.stream_handle(), device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    csr = None
+    state = {"csr": None}
 
-    def job(profile: bool):
-        nonlocal csr
+    def job():
         tree.delete_depth(0)
         counts = tree.subdivision_run(sc, DEPTH)
-        csr = tree.transition_matrix(sc, into=csr)
-        csr.invariant_measure(MEASURE_ITERS, keep_on_device=True)
+        state["csr"] = tree.transition_matrix(sc, into=state["csr"])
+        state["csr"].invariant_measure(MEASURE_ITERS, keep_on_device=True)
         return counts
-
-    # FP64 roofline denominator, measured on this device
-    peak_tflops, _ = T.probe_fp64_fma(0.25)
 
     counts = None
     for _ in range(args.warmup):
-        counts = job(False)
+        counts = job()
     bi_sub, n_final = box_images_of(counts)
     box_images = bi_sub + n_final
 
     # phase breakdown of one job (host clock around the synchronous API calls)
-    phases = {}
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     tree.delete_depth(0)
     t1 = time.perf_counter()
     tree.subdivision_run(sc, DEPTH)
     t2 = time.perf_counter()
-    csr = tree.transition_matrix(sc, into=csr)
+    state["csr"] = tree.transition_matrix(sc, into=state["csr"])
     t3 = time.perf_counter()
-    csr.invariant_measure(MEASURE_ITERS, keep_on_device=True)
+    state["csr"].invariant_measure(MEASURE_ITERS, keep_on_device=True)
     t4 = time.perf_counter()
     phases = {"reset_ms": 1e3 * (t1 - t0), "subdivision_ms": 1e3 * (t2 - t1), "transition_matrix_ms": 1e3 * (t3 - t2),
               "invariant_measure_ms": 1e3 * (t4 - t3)}
@@ -256,7 +257,7 @@ def gpu_arm(args, rank: int, world: int, dist):
             with torch.cuda.stream(stream):
                 flush.zero_()
                 ev[i][0].record(stream)
-            c = job(True)
+            c = job()
             with torch.cuda.stream(stream):
                 ev[i][1].record(stream)
             if list(c) != list(counts):
@@ -265,79 +266,98 @@ def gpu_arm(args, rank: int, world: int, dist):
     if dist:
         dist.barrier()
     launches = T.launch_count() - launches0
-    step_ms = [a.elapsed_time(b) for a, b in ev]
-    total_ms = sum(step_ms)
+    total_ms = sum(a.elapsed_time(b) for a, b in ev)
     img_ms, img_n = tree.profile_read(0)
     row_ms, row_n = tree.profile_read(1)
     tree.profile(False)
-
     if dist:
         t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
     value = world * args.steps * box_images / (total_ms * 1e-3)
-
-    # dominant kernel: the fused box-image kernel (subdivision steps)
     flops_img = args.steps * bi_sub * P * FLOP_PER_POINT
     achieved = flops_img / (img_ms * 1e-3) / 1e12 if img_ms > 0 else None
     flops_rows = args.steps * n_final * P * FLOP_PER_POINT
     rows_tflops = flops_rows / (row_ms * 1e-3) / 1e12 if row_ms > 0 else None
 
     # end to end through the public API: results copied to pinned host memory each step
-    if True:
-        codes = torch.empty(n_final, dtype=torch.int64, pin_memory=True).numpy().view(np.uint64)
-        depth = torch.empty(n_final, dtype=torch.uint8, pin_memory=True).numpy()
-        flags = torch.empty(n_final, dtype=torch.uint8, pin_memory=True).numpy()
-        rowptr = torch.empty(n_final + 1, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
-        cols = torch.empty(max(csr.nnz, 1), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
-        vals = torch.empty(max(csr.nnz, 1), dtype=torch.float64, pin_memory=True).numpy()
-        meas = torch.empty(n_final, dtype=torch.float64, pin_memory=True).numpy()
-        root = (np.zeros(1, np.uint64), np.zeros(1, np.uint8), np.zeros(1, np.uint8))
-        h2d = 8 + 1 + 1
-        d2h = codes.nbytes + depth.nbytes + flags.nbytes + rowptr.nbytes + cols.nbytes + vals.nbytes + meas.nbytes
-        e2e_steps = max(1, min(args.steps, 5))
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for _ in range(e2e_steps):
-            tree.load_leaves(*root)                       # the job's input: the surrounding box
-            tree.subdivision_run(sc, DEPTH)
-            csr = tree.transition_matrix(sc, into=csr)
-            csr.invariant_measure(MEASURE_ITERS, out=meas)
-            lib_leaves(tree, codes, depth, flags)
-            csr.to_host_into(rowptr, cols, vals)
-        torch.cuda.synchronize()
-        e2e_s = time.perf_counter() - t0
-        if dist:
-            t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
-        e2e = {"value": world * e2e_steps * box_images / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": int(d2h), "steps": e2e_steps, "timer": "host wall clock, synchronous API"}
-
-    cpu = cpu_baseline(cpu_cores()) if (rank == 0 and world == 1 and not args.no_cpu) else None
-
-    if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": dict(CONFIG, arith="fma" if args.fma else "strict",
-                               parallelism=f"{world} independent jobs" if world > 1 else "1 job",
-                               box_images_per_step=box_images, final_boxes=n_final, nnz=csr.nnz),
-                "e2e": e2e, "gpu_launches": int(launches),
-                "roofline": {"bound": "fp64", "kernel": "image_points_kernel (fused sample/RK4/locate)",
-                             "achieved": achieved, "peak": peak_tflops, "unit": "TFLOP/s",
-                             "frac": (achieved / peak_tflops) if achieved else None, "traffic": None,
-                             "peak_source": "measured: FP64 FMA-chain probe kernel on this device "
-                                            f"(nominal {NOMINAL_FP64_TFLOPS} TFLOP/s)",
-                             "flop_per_box_image": P * FLOP_PER_POINT, "launches": img_n,
-                             "kernel_ms_per_step": img_ms / args.steps,
-                             "transition_rows_tflops": rows_tflops},
-                "clocks": clocks.summary(), "cpu_baseline": cpu, "phases_ms": phases,
-                "counts": [int(c) for c in counts]}
-        print(json.dumps(line), flush=True)
+    csr = state["csr"]
+    codes = torch.empty(n_final, dtype=torch.int64, pin_memory=True).numpy().view(np.uint64)
+    depth = torch.empty(n_final, dtype=torch.uint8, pin_memory=True).numpy()
+    flags = torch.empty(n_final, dtype=torch.uint8, pin_memory=True).numpy()
+    rowptr = torch.empty(n_final + 1, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+    cols = torch.empty(max(csr.nnz, 1), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+    vals = torch.empty(max(csr.nnz, 1), dtype=torch.float64, pin_memory=True).numpy()
+    meas = torch.empty(n_final, dtype=torch.float64, pin_memory=True).numpy()
+    root = (np.zeros(1, np.uint64), np.zeros(1, np.uint8), np.zeros(1, np.uint8))
+    h2d = 8 + 1 + 1
+    d2h = codes.nbytes + depth.nbytes + flags.nbytes + rowptr.nbytes + cols.nbytes + vals.nbytes + meas.nbytes
+    e2e_steps = max(1, min(args.steps, 5))
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        tree.load_leaves(*root)                       # the job's input: the surrounding box
+        tree.subdivision_run(sc, DEPTH)
+        csr = tree.transition_matrix(sc, into=csr)
+        csr.invariant_measure(MEASURE_ITERS, out=meas)
+        lib_leaves(tree, codes, depth, flags)
+        csr.to_host_into(rowptr, cols, vals)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": world * e2e_steps * box_images / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": int(d2h), "steps": e2e_steps, "timer": "host wall clock, synchronous API"}
+    roofline = {"bound": "fp64", "kernel": "image_points_kernel (fused sample/RK4/locate)", "achieved": achieved,
+                "peak": peak_tflops, "unit": "TFLOP/s", "frac": (achieved / peak_tflops) if achieved else None,
+                "traffic": None,
+                "peak_source": "measured: FP64 FMA-chain probe kernel on this device "
+                               f"(nominal {NOMINAL_FP64_TFLOPS} TFLOP/s)",
+                "flop_per_box_image": P * FLOP_PER_POINT, "launches": img_n,
+                "kernel_ms_per_step": img_ms / args.steps, "transition_rows_tflops": rows_tflops}
+    out = dict(value=value, total_ms=total_ms, e2e=e2e, launches=launches, roofline=roofline,
+               clocks=clocks.summary(), phases=phases, counts=[int(c) for c in counts], box_images=box_images,
+               n_final=n_final, nnz=csr.nnz)
+    state["csr"] = None
+    csr.close()
     tree.close()
+    return out
+
+
+def gpu_arm(args, rank: int, world: int, dist):
+    import torch
+    from b12_b200 import tree as T
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    # FP64 roofline denominator, measured on this device
+    peak_tflops, _ = T.probe_fp64_fma(0.25)
+    main = measure_mode(args, rank, world, dist, fma=not args.strict, peak_tflops=peak_tflops)
+    other = None if args.single else measure_mode(args, rank, world, dist, fma=args.strict, peak_tflops=peak_tflops)
+    cpu = cpu_baseline(cpu_cores()) if (rank == 0 and world == 1 and not args.no_cpu) else None
+    if rank == 0:
+        arith = "strict" if args.strict else "fma"
+        line = {"metric": METRIC, "value": main["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": main["total_ms"] / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": dict(CONFIG, arith=arith,
+                               parallelism=f"{world} independent jobs" if world > 1 else "1 job",
+                               box_images_per_step=main["box_images"], final_boxes=main["n_final"],
+                               nnz=main["nnz"]),
+                "e2e": main["e2e"], "gpu_launches": int(main["launches"]), "roofline": main["roofline"],
+                "clocks": main["clocks"], "cpu_baseline": cpu, "phases_ms": main["phases"],
+                "counts": main["counts"]}
+        if other is not None:
+            line["strict" if not args.strict else "fma"] = {
+                "value": other["value"], "ms_per_step": other["total_ms"] / args.steps, "e2e": other["e2e"]["value"],
+                "roofline_achieved": other["roofline"]["achieved"], "roofline_frac": other["roofline"]["frac"],
+                "transition_rows_tflops": other["roofline"]["transition_rows_tflops"], "phases_ms": other["phases"],
+                "counts_identical": other["counts"] == main["counts"], "clocks": other["clocks"]}
+        print(json.dumps(line), flush=True)
     return 0
 
 
@@ -352,7 +372,9 @@ def main():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--fma", action="store_true", help="explicit-FMA integrator arithmetic")
+    ap.add_argument("--strict", action="store_true",
+                    help="headline with the strict (one rounding per operation) integrator instead of explicit FMA")
+    ap.add_argument("--single", action="store_true", help="measure only the headline arithmetic")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
