@@ -1,24 +1,292 @@
-// Insertion of new boxes (continuation).  Filled in with the radix sort.
+// Insertion of new boxes and the continuation driver.
+//
+// insertByPoints / insertByIterators (ImplicitBoxTree.hpp:1615-1946) at one depth d
+// equal to the tree's: every point (or mapped grid point) is located among the leaves;
+// a hit leaf gets flagsForHit, a point in no leaf contributes its depth-d code as a
+// candidate.  Candidates are radix-sorted, made unique and merged into the sorted
+// leaf array with flagsForInserted.  The reference's whole-tree re-sort and its two
+// HasSamePath scans (1875-1897) reduce to this merge because all leaves share a depth
+// and no candidate equals a leaf.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "sort.h"
 #include "tree.h"
 
+using namespace b12g;
 using namespace b12g::host;
+
+namespace {
+
+constexpr int kThreads = 256;
+
+// locate given points among the leaves: hit mask for found leaves, candidate codes for
+// points inside the domain but in no leaf
+template<int D>
+__global__ void locate_points_kernel(const double* pts, uint32_t n_pts, Domain dom, int depth,
+                                     const uint64_t* codes, const uint32_t* n_leaves, LeafHash hash, bool root_only,
+                                     uint8_t* hit, uint64_t* cand, uint32_t* cand_count, uint32_t cand_cap,
+                                     uint32_t* error)
+{
+  const uint32_t n = *n_leaves;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_pts; i += gridDim.x * blockDim.x) {
+    double p[D];
+#pragma unroll
+    for (int j = 0; j < D; ++j) p[j] = pts[size_t(i) * D + j];
+    uint64_t code = 0;
+    const bool valid = point_code<D>(dom, p, depth, code);
+    if (!valid) continue;
+    const uint32_t t = root_only ? kInvalidIndex : find_leaf(hash, codes, n, true, code);
+    if (t != kInvalidIndex) {
+      if (hit) hit[t] = 1;
+    } else {
+      const uint32_t pos = atomicAdd(cand_count, 1u);
+      if (pos < cand_cap) cand[pos] = code;
+      else atomicOr(error, 1u);
+    }
+  }
+}
+
+cudaError_t launch_locate_points(uint32_t dim, const double* pts, uint32_t n_pts, const Domain& dom, int depth,
+                                 const uint64_t* codes, const uint32_t* n_leaves, LeafHash hash, bool root_only,
+                                 uint8_t* hit, uint64_t* cand, uint32_t* cand_count, uint32_t cand_cap,
+                                 uint32_t* error, cudaStream_t s)
+{
+  const int grid = int(std::min<uint64_t>(std::max<uint64_t>((n_pts + kThreads - 1) / kThreads, 1), 1024));
+  switch (dim) {
+    case 1: locate_points_kernel<1><<<grid, kThreads, 0, s>>>(pts, n_pts, dom, depth, codes, n_leaves, hash, root_only, hit, cand, cand_count, cand_cap, error); break;
+    case 2: locate_points_kernel<2><<<grid, kThreads, 0, s>>>(pts, n_pts, dom, depth, codes, n_leaves, hash, root_only, hit, cand, cand_count, cand_cap, error); break;
+    case 3: locate_points_kernel<3><<<grid, kThreads, 0, s>>>(pts, n_pts, dom, depth, codes, n_leaves, hash, root_only, hit, cand, cand_count, cand_cap, error); break;
+    case 4: locate_points_kernel<4><<<grid, kThreads, 0, s>>>(pts, n_pts, dom, depth, codes, n_leaves, hash, root_only, hit, cand, cand_count, cand_cap, error); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+// candidates (count in C_CAND) -> sorted unique codes in t->cand2 (count in C_NNEW)
+b12g_status sort_unique_candidates(b12g_tree* t, uint32_t m, uint8_t depth, uint32_t* u)
+{
+  *u = 0;
+  if (m == 0) return set_ctr(t, C_NNEW, 0);
+  const uint64_t cells = sort_scratch_u32(m);
+  ST(t->cand2.ensure(m, "candidate sort"));
+  ST(t->sort_idx.ensure(2 * cells + 2 * (size_t(m) + 1) + compact_tiles(std::max<uint64_t>(cells, m + 1)) + 8,
+                        "candidate sort scratch"));
+  uint32_t* hist = t->sort_idx.p;
+  uint32_t* offsets = hist + cells;
+  uint32_t* flag = offsets + cells;
+  uint32_t* pos = flag + (m + 1);
+  uint32_t* tiles = pos + (m + 1);
+  uint64_t* sorted = nullptr;
+  const int bits = std::max(8, ((int(depth) + 7) / 8) * 8);
+  CK(radix_sort_u64(t->cand.p, t->cand2.p, t->ctr.p + C_CAND, m, bits, hist, offsets, tiles, t->ctr.p + C_TMP,
+                    &sorted, t->stream));
+  uint64_t* other = sorted == t->cand.p ? t->cand2.p : t->cand.p;
+  CK(unique_sorted_u64(sorted, t->ctr.p + C_CAND, m, other, t->ctr.p + C_NNEW, flag, pos, tiles, t->stream));
+  count_launches(1 + 5 * uint64_t(bits / 8) + 5);
+  ST(read_ctr(t, C_NNEW, 1));
+  *u = t->h_ctr[C_NNEW];
+  // the unique codes must end up in t->cand2 for merge_new
+  if (other != t->cand2.p)
+    CK(cudaMemcpyAsync(t->cand2.p, other, size_t(*u) * 8, cudaMemcpyDeviceToDevice, t->stream));
+  return B12G_OK;
+}
+
+// merge the u unique new codes of t->cand2 into the leaves with flags `ins`
+b12g_status merge_new(b12g_tree* t, uint32_t u, uint8_t ins)
+{
+  if (u == 0) return B12G_OK;
+  const uint64_t total = uint64_t(t->n) + u;
+  ST(reserve(t, total));
+  const int o = 1 - t->cur, no = 1 - t->ncur;
+  CK(merge_sorted(t->codes(), t->flg(), t->dn(), t->cand2.p, ins, t->ctr.p + C_NNEW, uint32_t(total), t->code[o].p,
+                  t->flags[o].p, t->ctr.p + no, t->stream));
+  count_launches(1);
+  ST(sync(t, "merge"));
+  t->cur = o;
+  t->ncur = no;
+  t->n = uint32_t(total);
+  return B12G_OK;
+}
+
+b12g_status ensure_candidates(b12g_tree* t, uint64_t m)
+{
+  if (m > 0xFFFFFFF0ull) return fail(B12G_ERR_CAPACITY, "more than 2^32 candidate boxes in one insert");
+  ST(t->cand.ensure(std::max<uint64_t>(m, 256), "insert candidates"));
+  return B12G_OK;
+}
+
+// hit flags of leaves that were hit (and not newly inserted)
+b12g_status apply_hit_flags(b12g_tree* t, uint8_t hit_flags)
+{
+  if (!hit_flags) return B12G_OK;
+  CK(apply_hits(t->flg(), t->hit.p, t->dn(), hit_flags, t->ctr.p + C_CHANGED, t->n, t->stream));
+  count_launches(1);
+  return B12G_OK;
+}
+
+b12g_status insert_points_impl(b12g_tree* t, const double* points, uint64_t n_points, uint8_t depth, uint8_t ins,
+                               uint8_t hit_flags, uint32_t* n_inserted)
+{
+  if (!t || (!points && n_points)) return fail(B12G_ERR_INVALID, "NULL argument");
+  if (n_points > 0xFFFFFFF0ull) return fail(B12G_ERR_CAPACITY, "too many points");
+  if (depth == B12G_LEAF_DEPTH) return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "insertion at the leaf depth -1");
+  if (depth > 64) return fail(B12G_ERR_INVALID, "depth above 64");
+  const bool root_only = t->n == 1 && t->depth == 0;
+  if (depth == 0) {
+    // the surrounding box always exists: only flagsForHit (ImplicitBoxTree.hpp:1625-1640)
+    if (hit_flags && n_points) {
+      // any point inside the domain hits the root
+      ST(ensure_candidates(t, n_points));
+      ST(set_ctr(t, C_CAND, 0));
+      ST(t->points.ensure(n_points * t->domain.dim, "points"));
+      CK(cudaMemcpyAsync(t->points.p, points, n_points * t->domain.dim * 8, cudaMemcpyHostToDevice, t->stream));
+      CK(launch_locate_points(t->domain.dim, t->points.p, uint32_t(n_points), t->dom, 0, t->codes(), t->dn(),
+                              LeafHash{nullptr, 0, 0}, true, nullptr, t->cand.p, t->ctr.p + C_CAND,
+                              uint32_t(t->cand.n), t->ctr.p + C_ERROR, t->stream));
+      ST(read_ctr(t, C_CAND, 1));
+      if (t->h_ctr[C_CAND] > 0) ST(flag_call(t, 0, 0, hit_flags, 0, nullptr));
+    }
+    if (n_inserted) *n_inserted = 0;
+    return B12G_OK;
+  }
+  if (!root_only && depth != t->depth)
+    return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "insertion at depth %u into a depth-%u tree", depth, t->depth);
+  uint32_t u = 0;
+  if (n_points) {
+    ST(ensure_candidates(t, n_points));
+    ST(set_ctr(t, C_CAND, 0));
+    ST(t->points.ensure(n_points * t->domain.dim, "points"));
+    CK(cudaMemcpyAsync(t->points.p, points, n_points * t->domain.dim * 8, cudaMemcpyHostToDevice, t->stream));
+    Prepared pr;
+    pr.a.hash = LeafHash{nullptr, 0, 0};
+    if (!root_only) ST(build_current_hash(t, pr));
+    CK(launch_locate_points(t->domain.dim, t->points.p, uint32_t(n_points), t->dom, depth, t->codes(), t->dn(),
+                            pr.a.hash, root_only, hit_flags ? t->hit.p : nullptr, t->cand.p, t->ctr.p + C_CAND,
+                            uint32_t(t->cand.n), t->ctr.p + C_ERROR, t->stream));
+    count_launches(1);
+    ST(read_ctr(t, C_CAND, 1));
+    ST(check_error(t, "insert_points"));
+    const uint32_t m = t->h_ctr[C_CAND];
+    if (!root_only) ST(apply_hit_flags(t, hit_flags));
+    ST(sort_unique_candidates(t, m, depth, &u));
+  }
+  if (root_only) {
+    // the surrounding box shares its path with every box and merges into the one new
+    // box, which keeps the union of both flags (ImplicitBoxTree.hpp:1878-1897)
+    if (u == 0) {
+      if (n_inserted) *n_inserted = 0;
+      return B12G_OK;
+    }
+    if (u > 1)
+      return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH,
+                  "inserting %u distinct boxes into the surrounding box alone (the reference merges them)", u);
+    uint8_t root_flags = 0;
+    CK(cudaMemcpyAsync(&root_flags, t->flg(), 1, cudaMemcpyDeviceToHost, t->stream));
+    ST(sync(t, "root flags"));
+    CK(cudaMemcpyAsync(t->codes(), t->cand2.p, 8, cudaMemcpyDeviceToDevice, t->stream));
+    CK(cudaMemsetAsync(t->flg(), uint8_t(ins | root_flags), 1, t->stream));
+    t->depth = depth;
+    ST(set_ctr(t, t->ncur, 1));
+    ST(sync(t, "insert into the surrounding box"));
+    if (n_inserted) *n_inserted = 1;
+    return B12G_OK;
+  }
+  ST(merge_new(t, u, ins));
+  if (n_inserted) *n_inserted = u;
+  return B12G_OK;
+}
+
+b12g_status insert_by_image_impl(b12g_tree* t, const b12g_scheme* sc, uint8_t depth, uint8_t ins, uint8_t hit_flags,
+                                 uint32_t* n_inserted)
+{
+  if (!t || !sc) return fail(B12G_ERR_INVALID, "NULL argument");
+  if (depth != t->depth || t->depth == 0)
+    return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "insertion of images at depth %u into a depth-%u tree", depth,
+                t->depth);
+  Prepared pr;
+  ST(prepare(t, sc, pr));
+  uint32_t n_src = 0;
+  ST(select_sources(t, sc, pr, n_src));
+  const uint64_t points = uint64_t(n_src) * pr.P;
+  if (points == 0) {
+    if (n_inserted) *n_inserted = 0;
+    return B12G_OK;
+  }
+  ST(build_current_hash(t, pr));
+  // room for every point to be a new box; grows (and the images are recomputed) on overflow
+  uint64_t cap = std::min<uint64_t>(points, std::max<uint64_t>(uint64_t(t->cand.n), uint64_t(1) << 20));
+  for (int attempt = 0; attempt < 8; ++attempt) {
+    ST(ensure_candidates(t, cap));
+    ST(set_ctr(t, C_CAND, 0));
+    pr.a.cand = t->cand.p;
+    pr.a.cand_count = t->ctr.p + C_CAND;
+    pr.a.cand_cap = uint32_t(std::min<size_t>(t->cand.n, 0xFFFFFFFFu));
+    pr.a.hit = hit_flags ? t->hit.p : nullptr;
+    prof_mark(t, 0);
+    CK(launch_image(sc->map.kind, sc->map.arith, sc->grid.kind, t->domain.dim, ImageMode::Insert, pr.a, points,
+                    t->stream));
+    prof_mark(t, 0);
+    count_launches(1);
+    ST(read_ctr(t, C_CAND, 1));
+    ST(prof_collect(t));
+    const uint32_t m = t->h_ctr[C_CAND];
+    ST(read_ctr(t, C_ERROR, 1));
+    if (t->h_ctr[C_ERROR] & 1u) {
+      ST(set_ctr(t, C_ERROR, 0));
+      cap = std::min<uint64_t>(points, std::max<uint64_t>(uint64_t(m), cap * 2));
+      continue;
+    }
+    ST(apply_hit_flags(t, hit_flags));
+    uint32_t u = 0;
+    ST(sort_unique_candidates(t, m, depth, &u));
+    ST(merge_new(t, u, ins));
+    if (n_inserted) *n_inserted = u;
+    return B12G_OK;
+  }
+  return fail(B12G_ERR_CAPACITY, "insert_by_image: candidate buffer retries exhausted");
+}
+
+}  // namespace
 
 extern "C" {
 
-b12g_status b12g_insert_points(b12g_tree* t, const double*, uint64_t, uint8_t, uint8_t, uint8_t, uint32_t*)
+b12g_status b12g_insert_points(b12g_tree* t, const double* points, uint64_t n_points, uint8_t depth,
+                               uint8_t flags_for_inserted, uint8_t flags_for_hit, uint32_t* n_inserted)
 {
-  return fail(B12G_ERR_INVALID, "insert_points: not built yet");
+  return insert_points_impl(t, points, n_points, depth, flags_for_inserted, flags_for_hit, n_inserted);
 }
 
-b12g_status b12g_insert_by_image(b12g_tree* t, const b12g_scheme*, uint8_t, uint8_t, uint8_t, uint32_t*)
+b12g_status b12g_insert_by_image(b12g_tree* t, const b12g_scheme* sc, uint8_t depth, uint8_t flags_for_inserted,
+                                 uint8_t flags_for_hit, uint32_t* n_inserted)
 {
-  return fail(B12G_ERR_INVALID, "insert_by_image: not built yet");
+  return insert_by_image_impl(t, sc, depth, flags_for_inserted, flags_for_hit, n_inserted);
 }
 
-b12g_status b12g_continuation_run(b12g_tree*, const b12g_scheme*, const double*, uint64_t, uint8_t, uint32_t,
-                                  uint32_t*, uint32_t*)
+// continuation.m:13-44 at one depth
+b12g_status b12g_continuation_run(b12g_tree* t, const b12g_scheme* sc, const double* x0, uint64_t n_x0,
+                                  uint8_t depth, uint32_t max_sweeps, uint32_t* counts, uint32_t* n_sweeps)
 {
-  return fail(B12G_ERR_INVALID, "continuation_run: not built yet");
+  if (!t || !sc || !x0) return fail(B12G_ERR_INVALID, "NULL argument");
+  ST(set_root(t, B12G_NONE));                                               // deleteDepth(0)
+  ST(insert_points_impl(t, x0, n_x0, depth, B12G_INS, B12G_NONE, nullptr));  // insert(points, d, INS)
+  b12g_scheme s = *sc;
+  s.depth = depth;
+  s.flags_to_check = B12G_EXPD;                                             // {grid, map, d, EXPD}
+  uint32_t nb0 = 0, nb1 = t->depth == depth ? t->n : 0;
+  uint32_t k = 0;
+  while (nb1 > nb0 && k < max_sweeps) {
+    ST(flag_call(t, 2, B12G_INS, B12G_EXPD, depth, nullptr));              // changeFlags('all', INS, EXPD, d)
+    ST(insert_by_image_impl(t, &s, depth, B12G_INS, B12G_NONE, nullptr));   // insert(scheme, d, INS, NONE)
+    ST(flag_call(t, 1, 0, B12G_EXPD, B12G_LEAF_DEPTH, nullptr));           // unsetFlags('all', EXPD)
+    nb0 = nb1;
+    nb1 = t->n;
+    if (counts) counts[k] = nb1;
+    ++k;
+  }
+  if (n_sweeps) *n_sweeps = k;
+  return B12G_OK;
 }
 
-}
+}  // extern "C"

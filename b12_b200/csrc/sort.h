@@ -1,0 +1,28 @@
+// Radix sort and sorted-set operations on 64-bit box codes (sort.cu).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace b12g {
+
+// u32 cells of the digit table (hist and offsets each) for up to max_n keys
+uint64_t sort_scratch_u32(uint64_t max_n);
+
+// sort the low `bits` bits of *n == max_n keys; the result is in keys or alt
+// (*sorted tells which).  hist, offsets: sort_scratch_u32(max_n) u32 each; scan_tiles:
+// compact_tiles(sort_scratch_u32(max_n)) + 2 u32; count_tmp: 1 u32.
+cudaError_t radix_sort_u64(uint64_t* keys, uint64_t* alt, const uint32_t* n, uint32_t max_n, int bits,
+                           uint32_t* hist, uint32_t* offsets, uint32_t* scan_tiles, uint32_t* count_tmp,
+                           uint64_t** sorted, cudaStream_t s);
+
+// distinct values of a sorted array, in order; flag and pos: max_n + 1 u32
+cudaError_t unique_sorted_u64(const uint64_t* keys, const uint32_t* n, uint32_t max_n, uint64_t* out, uint32_t* n_out,
+                              uint32_t* flag, uint32_t* pos, uint32_t* scan_tiles, cudaStream_t s);
+
+// merge two sorted arrays with no common value; entries of b get flags fb
+cudaError_t merge_sorted(const uint64_t* a, const uint8_t* fa, const uint32_t* na, const uint64_t* b, uint8_t fb,
+                         const uint32_t* nb, uint32_t max_total, uint64_t* out, uint8_t* fout, uint32_t* n_out,
+                         cudaStream_t s);
+
+}  // namespace b12g

@@ -606,21 +606,28 @@ static void merge_new(orc_tree* t, const uint64_t* nc, uint64_t m, uint32_t dept
   free(c); free(d); free(f);
 }
 
-uint32_t orc_insert_points(orc_tree* t, const double* pts, uint64_t n_points, uint32_t depth, uint8_t ins)
+uint32_t orc_insert_points(orc_tree* t, const double* pts, uint64_t n_points, uint32_t depth, uint8_t ins,
+                           uint8_t hit)
 {
-  /* only the start of a continuation is restated: the tree holds just the surrounding
-   * box, which merges into the new boxes (its path is shared by every box) */
+  /* insertByPoints (ImplicitBoxTree.hpp:1927-1946) at depth `depth` into a tree whose
+   * leaves are all at that depth, or into the surrounding box alone, which merges
+   * into the (single) new box (its path is shared by every box) */
   const uint32_t D = t->dom.dim;
+  const int root_only = t->n == 1 && t->depth[0] == 0;
   uint64_t* nc = (uint64_t*)malloc((n_points ? n_points : 1) * 8);
   uint64_t m = 0;
   for (uint64_t p = 0; p < n_points; ++p) {
     uint64_t c64;
-    if (orc_point_code64(&t->dom, pts + p * D, &c64)) nc[m++] = srs(c64, 64 - (int)depth);
+    if (!orc_point_code64(&t->dom, pts + p * D, &c64)) continue;
+    if (!root_only) {
+      const uint32_t f = orc_search(t, c64, 1);
+      if (f != ORC_INVALID) { t->flags[f] |= hit; continue; }
+    }
+    nc[m++] = srs(c64, 64 - (int)depth);
   }
   qsort(nc, m, 8, cmp_u64);
   uint64_t u = 0;
   for (uint64_t k = 0; k < m; ++k) if (u == 0 || nc[k] != nc[u - 1]) nc[u++] = nc[k];
-  const int root_only = t->n == 1 && t->depth[0] == 0;
   uint8_t root_flags = root_only ? t->flags[0] : 0;
   if (root_only && u > 0) t->n = 0;
   merge_new(t, nc, u, depth, ins);

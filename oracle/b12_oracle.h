@@ -95,7 +95,8 @@ uint32_t orc_set_flags_by_image(orc_tree* t, const orc_map* m, const orc_grid* g
 /* continuation insert at uniform depth d: sources = leaves with flags_to_check */
 uint32_t orc_insert_by_image(orc_tree* t, const orc_map* m, const orc_grid* g, uint8_t flags_to_check,
                              uint8_t ins, uint8_t hit);
-uint32_t orc_insert_points(orc_tree* t, const double* pts, uint64_t n_points, uint32_t depth, uint8_t ins);
+uint32_t orc_insert_points(orc_tree* t, const double* pts, uint64_t n_points, uint32_t depth, uint8_t ins,
+                           uint8_t hit);
 void orc_delete_depth0(orc_tree* t);
 
 /* transition matrix on the leaves, row-major CSR; returns nnz.  Pass NULL arrays to

@@ -76,7 +76,7 @@ def lib():
             "orc_search_by_image": (None, [P(OrcTree), P(OrcMap), P(OrcGrid), P(u32), u64, P(u32)]),
             "orc_set_flags_by_image": (u32, [P(OrcTree), P(OrcMap), P(OrcGrid), u8]),
             "orc_insert_by_image": (u32, [P(OrcTree), P(OrcMap), P(OrcGrid), u8, u8, u8]),
-            "orc_insert_points": (u32, [P(OrcTree), P(dbl), u64, u32, u8]),
+            "orc_insert_points": (u32, [P(OrcTree), P(dbl), u64, u32, u8, u8]),
             "orc_delete_depth0": (None, [P(OrcTree)]),
             "orc_transition_matrix": (u64, [P(OrcTree), P(OrcMap), P(OrcGrid), C.c_int, C.c_int,
                                             P(u32), P(u32), P(dbl), P(u32)]),
@@ -200,10 +200,10 @@ class Oracle:
         return self.L.orc_insert_by_image(C.byref(self.tree), C.byref(self.map), C.byref(self.grid),
                                           check, ins, hit)
 
-    def insert_points(self, pts, depth, ins=2):
+    def insert_points(self, pts, depth, ins=2, hit=0):
         pts = np.ascontiguousarray(pts, dtype=np.float64)
         return self.L.orc_insert_points(C.byref(self.tree), _ptr(pts, C.c_double),
-                                        pts.size // self.spec["dim"], depth, ins)
+                                        pts.size // self.spec["dim"], depth, ins, hit)
 
     def delete_depth0(self): self.L.orc_delete_depth0(C.byref(self.tree))
 

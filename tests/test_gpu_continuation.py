@@ -1,0 +1,105 @@
+"""GPU parity of the unstable-manifold continuation (continuation.m:13-44) and of box
+insertion (insertByPoints / insertByIterators) against the reference's golden runs
+and the oracle: leaf codes, flags and per-sweep counts bit-exact."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from workloads import domain, oracle_spec, scheme, sha
+
+pytestmark = pytest.mark.gpu
+
+B = pytest.importorskip("b12_b200")
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _device():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+def make_tree(spec):
+    c, r = domain(spec)
+    return B.ImplicitBoxTree(c, r)
+
+
+@pytest.mark.parametrize("name", ["coupled_duffing_cont_d8", "coupled_duffing_cont_d12"])
+def test_continuation_run_matches_reference(golden, name):
+    meta, _ = golden(name)
+    spec = meta["spec"]
+    t = make_tree(spec)
+    counts = t.continuation_run(scheme(spec), np.zeros(4), spec["depth"])
+    ref = [s for s in meta["steps"] if s["step"] > 0]
+    assert list(counts) == [s["n"] for s in ref]
+    codes, depth, flags = t.leaves()
+    assert sha(codes) == ref[-1]["codes_sha256"]
+    assert sha(flags) == ref[-1]["flags_sha256"]
+    assert (depth == spec["depth"]).all()
+
+
+def test_continuation_step_api_matches_reference_each_sweep(golden):
+    meta, _ = golden("coupled_duffing_cont_d8")
+    spec = meta["spec"]
+    t = make_tree(spec)
+    sc = scheme(spec, depth=8, flags_to_check=B.EXPD)
+    assert t.delete_depth(0) == 1
+    assert t.insert_points(np.zeros(4), 8, B.INS, B.NONE) == 1
+    for st in meta["steps"]:
+        if st["step"] > 0:
+            t.change_flags(B.INS, B.EXPD, 8)
+            t.insert_by_image(sc, 8, B.INS, B.NONE)
+            t.unset_flags(B.EXPD)
+        codes, _, flags = t.leaves()
+        assert len(codes) == st["n"], st["step"]
+        assert sha(codes) == st["codes_sha256"] and sha(flags) == st["flags_sha256"], st["step"]
+
+
+def test_continuation_depth16_matches_oracle():
+    spec = dict(map="coupled_duffing", points=64, seed=0)
+    t = make_tree(spec)
+    counts = t.continuation_run(scheme(spec), np.zeros(4), 16)
+    o, oc = O.continuation(oracle_spec(spec), 16, np.zeros(4))
+    assert list(counts) == oc
+    for x, y in zip(t.leaves(), o.leaves()):
+        np.testing.assert_array_equal(x, y)
+
+
+def test_insert_by_image_with_hit_flags_matches_oracle():
+    spec = dict(map="henon", a=1.4, b=0.3, grid=4)
+    t = make_tree(spec)
+    o = O.Oracle(oracle_spec(spec))
+    t.subdivision_run(scheme(spec), 12)
+    o.subdivision(12)
+    # keep a sparse subset of the attractor, flag a part of it, and insert its images
+    codes, depth, _ = o.leaves()
+    keep = np.arange(len(codes)) % 3 == 0
+    flags = np.where(np.arange(keep.sum()) % 2 == 0, B.EXPD, B.NONE).astype(np.uint8)
+    t.load_leaves(codes[keep], depth[keep], flags)
+    o.load(codes[keep], depth[keep], flags)
+    sc = scheme(spec, depth=12, flags_to_check=B.EXPD)
+    n_new = t.insert_by_image(sc, 12, B.INS, B.HIT)
+    assert n_new == o.insert_by_image(B.EXPD, B.INS, B.HIT)
+    for x, y in zip(t.leaves(), o.leaves()):
+        np.testing.assert_array_equal(x, y)
+
+
+def test_insert_points_into_a_tree_of_one_depth():
+    spec = dict(map="lorenz", rho=28.0, grid=3)
+    t = make_tree(spec)
+    o = O.Oracle(oracle_spec(spec))
+    t.subdivision_run(scheme(spec), 9)
+    o.subdivision(9)
+    rng = np.random.default_rng(5)
+    pts = rng.uniform([-35, -35, -15], [35, 35, 70], size=(2000, 3))   # some outside the domain
+    assert t.insert_points(pts, 9, B.INS, B.HIT) == o.insert_points(pts, 9, 2, 1)
+    for x, y in zip(t.leaves(), o.leaves()):
+        np.testing.assert_array_equal(x, y)
+
+
+def test_insert_many_distinct_boxes_into_root_is_refused():
+    t = B.ImplicitBoxTree([0.0, 0.0], [1.0, 1.0])
+    with pytest.raises(B.B12gError) as e:
+        t.insert_points(np.array([[0.5, 0.5], [-0.5, -0.5]]), 4)
+    assert e.value.status == 5
+    assert t.count() == 1 and t.depth() == 0

@@ -101,3 +101,28 @@ def test_philox_known_answer():
         c = (C.c_uint32 * 4)(*ctr)
         L.orc_philox4x32_10(c, key[0], key[1])
         assert tuple(c) == expect
+
+
+@pytest.mark.parametrize("name", ["coupled_duffing_cont_d8", "coupled_duffing_cont_d12"])
+def test_continuation_matches_reference(golden, name):
+    meta, arrays = golden(name)
+    spec = meta["spec"]
+    o, counts = O.continuation(oracle_spec(spec), spec["depth"], np.zeros(4))
+    ref = [s for s in meta["steps"] if s["step"] > 0]
+    assert counts == [s["n"] for s in ref]
+    codes, depth, flags = o.leaves()
+    assert sha(codes) == ref[-1]["codes_sha256"] and sha(flags) == ref[-1]["flags_sha256"]
+
+
+def test_continuation_each_sweep_matches_reference(golden):
+    meta, arrays = golden("coupled_duffing_cont_d8")
+    o = O.Oracle(oracle_spec(meta["spec"]))
+    o.delete_depth0()
+    o.insert_points(np.zeros(4), 8, 2)
+    for st in meta["steps"]:
+        if st["step"] > 0:
+            o.change_flags(2, 4)
+            o.insert_by_image(4, 2, 0)
+            o.unset_flags(4)
+        codes, depth, flags = o.leaves()
+        assert len(codes) == st["n"] and sha(codes) == st["codes_sha256"] and sha(flags) == st["flags_sha256"]
