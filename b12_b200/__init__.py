@@ -7,11 +7,11 @@ ImplicitBoxTree interface used by the tests and the benchmark.
 from ._lib import (ALL, ARITH_FMA, ARITH_STRICT, B12gError, ENTR, EQU, EXPD, EXTR, GRID_FULL, GRID_INNER,
                    GRID_PHILOX, HIT, INS, INVALID_INDEX, LEAF_DEPTH, MAP_COUPLED_DUFFING, MAP_FORCED_DUFFING,
                    MAP_HENON, MAP_LORENZ, NONE, SD)
-from .tree import (CsrMatrix, GridSpec, ImplicitBoxTree, MapSpec, Scheme, coupled_duffing, forced_duffing,
+from .tree import (Batch, CsrMatrix, GridSpec, ImplicitBoxTree, MapSpec, Scheme, coupled_duffing, forced_duffing,
                    full_grid, henon, inner_grid, lorenz, philox_grid)
 
 __all__ = [
-    "ImplicitBoxTree", "CsrMatrix", "Scheme", "MapSpec", "GridSpec", "henon", "lorenz", "coupled_duffing",
+    "ImplicitBoxTree", "Batch", "CsrMatrix", "Scheme", "MapSpec", "GridSpec", "henon", "lorenz", "coupled_duffing",
     "forced_duffing", "inner_grid", "full_grid", "philox_grid", "B12gError", "NONE", "HIT", "INS", "EXPD", "SD",
     "EQU", "ENTR", "EXTR", "ALL", "LEAF_DEPTH", "INVALID_INDEX", "MAP_HENON", "MAP_LORENZ", "MAP_COUPLED_DUFFING",
     "MAP_FORCED_DUFFING", "GRID_INNER", "GRID_FULL", "GRID_PHILOX", "ARITH_STRICT", "ARITH_FMA",

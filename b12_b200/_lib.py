@@ -92,6 +92,19 @@ _SIGS = {
     "b12g_subdivision_run": (C.c_int, [C.c_void_p, C.POINTER(Scheme), C.c_uint32, C.c_void_p]),
     "b12g_continuation_run": (C.c_int, [C.c_void_p, C.POINTER(Scheme), C.c_void_p, C.c_uint64, C.c_uint8,
                                         C.c_uint32, C.c_void_p, C.POINTER(C.c_uint32)]),
+    "b12g_batch_create": (C.c_int, [C.POINTER(Domain), C.POINTER(Scheme), C.c_uint32, C.c_void_p, C.c_void_p,
+                                    C.POINTER(C.c_void_p)]),
+    "b12g_batch_destroy": (C.c_int, [C.c_void_p]),
+    "b12g_batch_run": (C.c_int, [C.c_void_p]),
+    "b12g_batch_counts": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p]),
+    "b12g_batch_leaves": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32),
+                                    C.POINTER(C.c_uint8)]),
+    "b12g_batch_transition_matrices": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "b12g_batch_csr": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                 C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]),
+    "b12g_batch_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
+                                  C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    "b12g_batch_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "b12g_tree_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "b12g_profile_enable": (C.c_int, [C.c_void_p, C.c_int]),
     "b12g_profile_read": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_double), C.POINTER(C.c_uint64), C.c_int]),

@@ -414,6 +414,45 @@ struct LorenzMap {
   }
 };
 
+// W independent Lorenz states integrated in one loop: the same operations per state as
+// apply(), interleaved so that one thread keeps W dependency chains in flight
+template<class A, int W>
+__device__ __forceinline__ void lorenz_apply_multi(const MapParams& m, const double (&x0)[W][3], double (&res)[W][3])
+{
+  double x[W][3], k[W][3], a[W][3];
+#pragma unroll
+  for (int w = 0; w < W; ++w)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) x[w][j] = x0[w][j];
+#pragma unroll 1
+  for (uint32_t s = 0; s < m.steps; ++s) {
+#pragma unroll
+    for (int w = 0; w < W; ++w) LorenzMap<A>::rhs(m, x[w], k[w]);
+#pragma unroll
+    for (int w = 0; w < W; ++w)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) { res[w][j] = A::madd(m.h6, k[w][j], x[w][j]); a[w][j] = A::madd(m.h2, k[w][j], x[w][j]); }
+#pragma unroll
+    for (int w = 0; w < W; ++w) LorenzMap<A>::rhs(m, a[w], k[w]);
+#pragma unroll
+    for (int w = 0; w < W; ++w)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) { res[w][j] = A::madd(m.h3, k[w][j], res[w][j]); a[w][j] = A::madd(m.h2, k[w][j], x[w][j]); }
+#pragma unroll
+    for (int w = 0; w < W; ++w) LorenzMap<A>::rhs(m, a[w], k[w]);
+#pragma unroll
+    for (int w = 0; w < W; ++w)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) { res[w][j] = A::madd(m.h3, k[w][j], res[w][j]); a[w][j] = A::madd(m.h, k[w][j], x[w][j]); }
+#pragma unroll
+    for (int w = 0; w < W; ++w) LorenzMap<A>::rhs(m, a[w], k[w]);
+#pragma unroll
+    for (int w = 0; w < W; ++w)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) { res[w][j] = A::madd(m.h6, k[w][j], res[w][j]); x[w][j] = res[w][j]; }
+  }
+}
+
 // LorenzRHS (Map_Lorenz.h:10-24): (sigma (y-x), rho x - y - x z, -beta z + x y)
 template<>
 __device__ __forceinline__ void LorenzMap<Strict>::rhs(const MapParams& m, const double* x, double* r)

@@ -4,6 +4,7 @@
 // ComputeSearchIndexFunctor (ImplicitBoxTree.hpp:2394-2432), evaluated once per point
 // instead of twice and without the point stream ever being stored.
 #include "kernels.h"
+#include "rows.cuh"
 
 namespace b12g {
 
@@ -147,26 +148,6 @@ __global__ void __launch_bounds__(kThreads) image_points_kernel(const ImageArgs 
 // ---------------------------------------------------------------------------------
 constexpr int kRowWarps = kThreads / 32;
 
-__device__ __forceinline__ void warp_bitonic_128(uint32_t* s, int lane)
-{
-#pragma unroll 1
-  for (int k = 2; k <= 128; k <<= 1) {
-#pragma unroll 1
-    for (int j = k >> 1; j > 0; j >>= 1) {
-#pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        const int c = lane + 32 * q;                           // comparator 0..63
-        const int i = ((c & ~(j - 1)) << 1) | (c & (j - 1));    // insert a zero bit at log2(j)
-        const int l = i | j;
-        const bool up = (i & k) == 0;
-        const uint32_t x = s[i], y = s[l];
-        if ((x > y) == up) { s[i] = y; s[l] = x; }
-      }
-      __syncwarp();
-    }
-  }
-}
-
 template<class Map, class Grid>
 __global__ void __launch_bounds__(kThreads) transition_rows_kernel(const RowArgs ra)
 {
@@ -199,56 +180,8 @@ __global__ void __launch_bounds__(kThreads) transition_rows_kernel(const RowArgs
       }
       s[lane + 32 * q] = key;
     }
-    if (lane < 4) bounds[w][lane] = 0;
-    __syncwarp();
-    warp_bitonic_128(s, lane);
-
-    // run boundaries: position p starts a run if p == 0 or s[p] != s[p-1]
-    uint32_t nib = 0;
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      const int p = lane * 4 + r;
-      if (p == 0 || s[p] != s[p - 1]) nib |= 1u << r;
-    }
-    atomicOr(&bounds[w][lane >> 3], nib << ((lane & 7) * 4));
-    __syncwarp();
-
-    const uint32_t ws[4] = {bounds[w][0], bounds[w][1], bounds[w][2], bounds[w][3]};
-    uint32_t cols[4], cnts[4], emit = 0;
-    bool take[4];
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      const int p = lane * 4 + r;
-      const uint32_t key = s[p];
-      take[r] = ((nib >> r) & 1u) && key != kPadKey && (key != kLostKey || ra.keep_lost);
-      // the run ends at the next boundary after p (or at P, where the padding starts)
-      int end = int(P);
-      bool found = false;
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int first = q * 32, from = p + 1;
-        if (found || from >= first + 32) continue;
-        const uint32_t m = from > first ? ws[q] & (0xFFFFFFFFu << (from - first)) : ws[q];
-        if (m) { end = min(int(P), first + __ffs(m) - 1); found = true; }
-      }
-      cols[r] = key == kLostKey ? ra.lost_col : key;
-      cnts[r] = uint32_t(end - p);
-      emit += take[r] ? 1u : 0u;
-    }
-    // warp exclusive scan of emit counts
-    uint32_t off = emit;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-      const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, off, d);
-      if (lane >= d) off += v;
-    }
-    const uint32_t total = __shfl_sync(0xFFFFFFFFu, off, 31);
-    off -= emit;
-    uint32_t* sc = ra.stage_col + size_t(row) * P;
-    uint32_t* sn = ra.stage_cnt + size_t(row) * P;
-#pragma unroll
-    for (int r = 0; r < 4; ++r)
-      if (take[r]) { sc[off] = cols[r]; sn[off] = cnts[r]; ++off; }
+    const uint32_t total = row_emit(s, bounds[w], lane, P, ra.keep_lost, ra.lost_col,
+                                    ra.stage_col + size_t(row) * P, ra.stage_cnt + size_t(row) * P);
     if (lane == 0) ra.row_count[row] = total;
     __syncwarp();
   }

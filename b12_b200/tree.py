@@ -344,3 +344,86 @@ class ImplicitBoxTree:
     def transitionMatrixForLeaves(self, grid: GridSpec, map_: MapSpec, use_absolute_values: bool = False,
                                   use_invalid_nr_boxes: bool = False) -> CsrMatrix:
         return self.transition_matrix(Scheme(map_, grid), use_absolute_values, use_invalid_nr_boxes)
+
+
+# ----------------------------------------------------------------------------- batches
+class Batch:
+    """Many independent subdivision jobs (same domain, map kind, grid) advanced together."""
+
+    def __init__(self, center, radius, scheme: Scheme, params, depths):
+        params = np.asarray(params, dtype=np.float64)
+        if params.ndim != 2:
+            raise ValueError("params must be n x k")
+        n = params.shape[0]
+        p6 = np.zeros((n, 6), dtype=np.float64)
+        p6[:, : params.shape[1]] = params
+        self._params = np.ascontiguousarray(p6)
+        self._depths = np.ascontiguousarray(np.asarray(depths, dtype=np.uint8))
+        if len(self._depths) != n:
+            raise ValueError("one depth per instance")
+        d = L.Domain()
+        d.dim = len(center)
+        for j in range(d.dim):
+            d.center[j] = float(center[j])
+            d.radius[j] = float(radius[j])
+        self.n = n
+        self.dim = d.dim
+        s = scheme.to_c()
+        self._h = C.c_void_p()
+        check(lib().b12g_batch_create(C.byref(d), C.byref(s), n, self._params.ctypes.data, self._depths.ctypes.data,
+                                      C.byref(self._h)), "batch_create")
+
+    def close(self):
+        if self._h:
+            lib().b12g_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self) -> None:
+        check(lib().b12g_batch_run(self._h), "batch_run")
+
+    def counts(self, i: int) -> np.ndarray:
+        c = np.zeros(int(self._depths[i]), dtype=np.uint32)
+        check(lib().b12g_batch_counts(self._h, i, c.ctypes.data), "batch_counts")
+        return c
+
+    def leaves(self, i: int):
+        n, d = C.c_uint32(), C.c_uint8()
+        check(lib().b12g_batch_leaves(self._h, i, None, None, C.byref(n), C.byref(d)), "batch_leaves")
+        codes = np.zeros(n.value, dtype=np.uint64)
+        flags = np.zeros(n.value, dtype=np.uint8)
+        check(lib().b12g_batch_leaves(self._h, i, codes.ctypes.data, flags.ctypes.data, C.byref(n), C.byref(d)),
+              "batch_leaves")
+        return codes, np.full(n.value, d.value, dtype=np.uint8), flags
+
+    def transition_matrices(self, absolute: bool = False, invalid_column: bool = False) -> None:
+        check(lib().b12g_batch_transition_matrices(self._h, int(absolute), int(invalid_column)),
+              "batch_transition_matrices")
+
+    def csr(self, i: int):
+        rows, nnz = C.c_uint32(), C.c_uint64()
+        check(lib().b12g_batch_csr(self._h, i, None, None, None, C.byref(rows), C.byref(nnz)), "batch_csr")
+        rowptr = np.zeros(rows.value + 1, dtype=np.uint32)
+        cols = np.zeros(max(nnz.value, 1), dtype=np.uint32)
+        vals = np.zeros(max(nnz.value, 1), dtype=np.float64)
+        check(lib().b12g_batch_csr(self._h, i, rowptr.ctypes.data, cols.ctypes.data, vals.ctypes.data,
+                                   C.byref(rows), C.byref(nnz)), "batch_csr")
+        return rowptr, cols[: nnz.value], vals[: nnz.value]
+
+    def info(self) -> dict:
+        bi, fb, nnz = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        th, ppt, ch = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        check(lib().b12g_batch_info(self._h, C.byref(bi), C.byref(fb), C.byref(nnz), C.byref(th), C.byref(ppt),
+                                    C.byref(ch)), "batch_info")
+        return dict(box_images=bi.value, final_boxes=fb.value, nnz=nnz.value, threads=th.value,
+                    points_per_thread=ppt.value, chunk=ch.value)
+
+    def stream_handle(self) -> int:
+        p = C.c_void_p()
+        check(lib().b12g_batch_stream(self._h, C.byref(p)), "batch_stream")
+        return p.value or 0

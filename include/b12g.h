@@ -214,6 +214,35 @@ b12g_status b12g_subdivision_run(b12g_tree* tree, const b12g_scheme* scheme, uin
 b12g_status b12g_continuation_run(b12g_tree* tree, const b12g_scheme* scheme, const double* x0, uint64_t n_x0,
                                   uint8_t depth, uint32_t max_sweeps, uint32_t* counts, uint32_t* n_sweeps);
 
+/* ---- batches of independent subdivision jobs --------------------------------------------
+ * Many instances of the subdivision loop (subdivision.m:18-45) with one domain, map
+ * kind, grid and arithmetic but per-instance map parameters and depths, advanced in
+ * lockstep on one GPU: one persistent launch per subdivision step serves every
+ * instance still subdividing, fed by a device work queue of point chunks; the steps
+ * run as one CUDA graph; the launch shape is autotuned on the first run.  The reference
+ * runs such scans one ImplicitBoxTree at a time.  Inner and full grids only. */
+typedef struct b12g_batch b12g_batch;
+/* params: n x 6 map parameters (b12g_map.p per instance); depths: n target depths 1..32 */
+b12g_status b12g_batch_create(const b12g_domain* domain, const b12g_scheme* scheme, uint32_t n,
+                              const double* params, const uint8_t* depths, b12g_batch** batch);
+b12g_status b12g_batch_destroy(b12g_batch* batch);
+/* run every instance's subdivision loop from the surrounding box */
+b12g_status b12g_batch_run(b12g_batch* batch);
+/* leaf counts of instance i after each of its steps (depth_i entries) */
+b12g_status b12g_batch_counts(b12g_batch* batch, uint32_t i, uint32_t* counts);
+/* final leaves of instance i (codes/flags may be NULL to query *n and *depth) */
+b12g_status b12g_batch_leaves(b12g_batch* batch, uint32_t i, uint64_t* codes, uint8_t* flags, uint32_t* n,
+                              uint8_t* depth);
+/* every instance's transition matrix (transitionMatrixForLeaves), resident on the device */
+b12g_status b12g_batch_transition_matrices(b12g_batch* batch, int absolute, int invalid_column);
+/* instance i's CSR (host arrays, any may be NULL to query sizes) */
+b12g_status b12g_batch_csr(b12g_batch* batch, uint32_t i, uint32_t* rowptr, uint32_t* cols, double* vals,
+                           uint32_t* n_rows, uint64_t* nnz);
+/* box-images of the last run, final boxes, nonzeros, and the autotuned launch shape */
+b12g_status b12g_batch_info(b12g_batch* batch, uint64_t* box_images, uint64_t* final_boxes, uint64_t* nnz,
+                            uint32_t* threads, uint32_t* points_per_thread, uint32_t* chunk);
+b12g_status b12g_batch_stream(b12g_batch* batch, void** stream);
+
 /* ---- measurement hooks (no counterpart in the reference) ---------------------------------- */
 /* the CUDA stream (cudaStream_t) every kernel of this tree runs on */
 b12g_status b12g_tree_stream(b12g_tree* tree, void** stream);

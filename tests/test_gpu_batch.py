@@ -1,0 +1,91 @@
+"""GPU: the batched subdivision (many instances, one persistent launch per step) gives
+every instance exactly the single-tree result - leaf codes, flags, per-step counts and
+transition matrices bit-exact - and the reference's golden runs."""
+import numpy as np
+import pytest
+
+from workloads import csr_digests, sha
+
+pytestmark = pytest.mark.gpu
+
+B = pytest.importorskip("b12_b200")
+from b12_b200.workloads import LORENZ_CENTER, LORENZ_RADIUS, lorenz_scan  # noqa: E402
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _device():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+def single(center, radius, mp, grid, depth):
+    t = B.ImplicitBoxTree(center, radius)
+    sc = B.Scheme(mp, grid)
+    counts = t.subdivision_run(sc, depth)
+    m = t.transition_matrix(sc)
+    return counts, t.leaves(), m.to_host()
+
+
+@pytest.mark.parametrize("fma", [False, True])
+def test_lorenz_batch_matches_single_trees(fma):
+    rho, _ = lorenz_scan(12, 0)
+    depths = [8, 14, 11, 9, 12, 14, 10, 13, 9, 12, 8, 11]
+    params = [(10.0, r, 8.0 / 3.0) for r in rho]
+    grid = B.inner_grid(5)
+    b = B.Batch(LORENZ_CENTER, LORENZ_RADIUS, B.Scheme(B.lorenz(fma=fma), grid), params, depths)
+    b.run()
+    b.transition_matrices()
+    for i in range(12):
+        counts, leaves, csr = single(LORENZ_CENTER, LORENZ_RADIUS, B.lorenz(rho=rho[i], fma=fma), grid, depths[i])
+        np.testing.assert_array_equal(b.counts(i), counts)
+        for x, y in zip(b.leaves(i), leaves):
+            np.testing.assert_array_equal(x, y)
+        for x, y in zip(b.csr(i), csr):
+            np.testing.assert_array_equal(x, y)
+
+
+def test_batch_replays_identically_and_reports_tuning():
+    rho, depth = lorenz_scan(40, 3)
+    depth = [min(d, 16) for d in depth]
+    b = B.Batch(LORENZ_CENTER, LORENZ_RADIUS, B.Scheme(B.lorenz(fma=True), B.inner_grid(5)),
+                [(10.0, r, 8.0 / 3.0) for r in rho], depth)
+    b.run()
+    first = [b.leaves(i)[0].copy() for i in range(40)]
+    b.run()
+    for i in range(40):
+        np.testing.assert_array_equal(b.leaves(i)[0], first[i])
+    info = b.info()
+    assert info["threads"] in (128, 256, 512) and info["points_per_thread"] in (1, 2)
+    assert info["final_boxes"] == sum(len(f) for f in first)
+
+
+def test_batch_members_match_reference_goldens(golden):
+    metas = [golden("lorenz_rho15_d18")[0], golden("lorenz_rho35_d18")[0], golden("lorenz_d15")[0]]
+    params = [(10.0, m["spec"]["rho"], 8.0 / 3.0) for m in metas]
+    depths = [len(m["steps"]) for m in metas]
+    b = B.Batch(LORENZ_CENTER, LORENZ_RADIUS, B.Scheme(B.lorenz(), B.inner_grid(5)), params, depths)
+    b.run()
+    b.transition_matrices()
+    for i, m in enumerate(metas):
+        assert list(b.counts(i)) == [s["n"] for s in m["steps"]]
+        codes, _, flags = b.leaves(i)
+        assert sha(codes) == m["steps"][-1]["codes_sha256"] and sha(flags) == m["steps"][-1]["flags_sha256"]
+        d = csr_digests(*b.csr(i))
+        for k in ("nnz", "rowptr_sha256", "cols_sha256", "vals_sha256"):
+            assert d[k] == m["tm"][k], (i, k)
+
+
+def test_henon_batch_matches_single_trees():
+    a_vals = [1.0, 1.1, 1.2, 1.3, 1.4, 1.05]
+    depths = [14, 12, 16, 10, 15, 13]
+    grid = B.inner_grid(4)
+    b = B.Batch((0.0, 0.0), (1.5, 0.45), B.Scheme(B.henon(), grid), [(a, 0.3) for a in a_vals], depths)
+    b.run()
+    b.transition_matrices()
+    for i, a in enumerate(a_vals):
+        counts, leaves, csr = single((0.0, 0.0), (1.5, 0.45), B.henon(a, 0.3), grid, depths[i])
+        np.testing.assert_array_equal(b.counts(i), counts)
+        np.testing.assert_array_equal(b.leaves(i)[0], leaves[0])
+        for x, y in zip(b.csr(i), csr):
+            np.testing.assert_array_equal(x, y)
