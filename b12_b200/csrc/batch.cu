@@ -75,14 +75,14 @@ __device__ __forceinline__ uint32_t find_instance(const uint32_t* off_s, uint32_
 __device__ __forceinline__ uint64_t inst_key(uint32_t inst, uint64_t code) { return (uint64_t(inst) << 32) | code; }
 
 __global__ void batch_hash_build_kernel(const uint64_t* codes, const uint32_t* off, uint32_t n_inst, LeafHash h,
-                                        uint32_t* error)
+                                        uint32_t code_cap, uint32_t* error)
 {
   __shared__ uint32_t off_s[kMaxInstances + 1];
   for (uint32_t i = threadIdx.x; i <= n_inst; i += blockDim.x) off_s[i] = off[i];
   __syncthreads();
   const uint32_t n = off_s[n_inst];
   const int l = hash_log2(n);
-  if (l > int(h.log2_cap)) {
+  if (n > code_cap || l > int(h.log2_cap)) {
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(error, 1u);
     return;
   }
@@ -234,11 +234,17 @@ __global__ void __launch_bounds__(512) batch_image_kernel(const BatchArgs a)
 
 
 // survivors per instance (children with a hit), one block per instance
-__global__ void inst_count_kernel(const uint8_t* hit, const uint32_t* off, uint32_t* cnt)
+__global__ void inst_count_kernel(const uint8_t* hit, const uint32_t* off, uint32_t* cnt, uint64_t hit_cap,
+                                  uint32_t* error)
 {
   __shared__ uint32_t red[32];
   const uint32_t i = blockIdx.x;
   const uint64_t b = 2ull * off[i], e = 2ull * off[i + 1];
+  if (e > hit_cap || b > e) {
+    // capacity exceeded upstream: report it and leave this instance's count at zero
+    if (threadIdx.x == 0) { cnt[i] = 0; atomicOr(error, 1u); }
+    return;
+  }
   uint32_t c = 0;
   for (uint64_t x = b + threadIdx.x; x < e; x += blockDim.x) c += hit[x] ? 1u : 0u;
 #pragma unroll
@@ -256,7 +262,8 @@ __global__ void inst_count_kernel(const uint8_t* hit, const uint32_t* off, uint3
 // the instances [a_next, n_inst) are finished: they get consecutive regions of the
 // final arena starting at *fin_base (fin_lo, fin_len per sorted position)
 __global__ void inst_offsets_kernel(const uint32_t* cnt, uint32_t n_inst, uint32_t a_next, uint32_t* new_off,
-                                    uint32_t* step_counts, uint32_t* fin_lo, uint32_t* fin_len, uint32_t* fin_base)
+                                    uint32_t* step_counts, uint32_t* fin_lo, uint32_t* fin_len, uint32_t* fin_base,
+                                    uint32_t code_cap, uint32_t* error)
 {
   __shared__ uint32_t part[1024];
   const uint32_t per = (n_inst + blockDim.x - 1) / blockDim.x;
@@ -269,6 +276,7 @@ __global__ void inst_offsets_kernel(const uint32_t* cnt, uint32_t n_inst, uint32
     uint32_t run = 0;
     for (uint32_t t = 0; t < blockDim.x; ++t) { const uint32_t v = part[t]; part[t] = run; run += v; }
     new_off[n_inst] = run;
+    if (run > code_cap) atomicOr(error, 1u);
   }
   __syncthreads();
   uint32_t run = part[threadIdx.x];
@@ -289,9 +297,9 @@ __global__ void inst_offsets_kernel(const uint32_t* cnt, uint32_t n_inst, uint32
 
 __global__ void copy_finished_kernel(const uint64_t* code, const uint8_t* flags, const uint32_t* new_off,
                                      uint32_t a_next, uint32_t n_inst, const uint32_t* fin_lo, uint64_t* fin_code,
-                                     uint8_t* fin_flags, uint32_t fin_cap, uint32_t* error)
+                                     uint8_t* fin_flags, uint32_t fin_cap, uint32_t code_cap, uint32_t* error)
 {
-  const uint32_t b = new_off[a_next], e = new_off[n_inst];
+  const uint32_t b = new_off[a_next], e = min(new_off[n_inst], code_cap);
   const uint32_t dst = fin_lo[a_next];
   for (uint32_t i = b + blockIdx.x * blockDim.x + threadIdx.x; i < e; i += gridDim.x * blockDim.x) {
     const uint32_t d = dst + (i - b);
@@ -537,6 +545,7 @@ b12g_status batch_reset(b12g_batch* b)
   CK(cudaMemsetAsync(b->flags[0].p, B12G_SD, b->N, b->stream));
   CK(cudaMemsetAsync(b->ctr.p, 0, B_COUNT * 4, b->stream));
   CK(cudaMemsetAsync(b->fin_len.p, 0, b->N * 4, b->stream));
+  CK(cudaMemsetAsync(b->hit.p, 0, b->hit.n, b->stream));
   CK(cudaMemsetAsync(b->fin_lo.p, 0, b->N * 4, b->stream));
   CK(cudaMemsetAsync(b->hash.p, 0, b->hash.n * sizeof(ulonglong2), b->stream));
   CK(cudaStreamSynchronize(b->stream));
@@ -549,8 +558,8 @@ cudaError_t build_step_hash(b12g_batch* b, uint32_t k)
   const uint32_t A = b->active[k];
   const int in = (k - 1) & 1;
   const LeafHash h{b->hash.p, k, b->hash_log2};
-  batch_hash_build_kernel<<<device_sm_count() * 4, 256, 0, b->stream>>>(b->code[in].p, b->off[in].p, A, h,
-                                                                       b->ctr.p + B_ERROR);
+  batch_hash_build_kernel<<<device_sm_count() * 4, 256, 0, b->stream>>>(
+      b->code[in].p, b->off[in].p, A, h, uint32_t(std::min<uint64_t>(b->cap, 0xFFFFFFFFu)), b->ctr.p + B_ERROR);
   return cudaGetLastError();
 }
 
@@ -584,7 +593,8 @@ cudaError_t enqueue_step(b12g_batch* b, uint32_t k, const Tuning& tu, bool with_
   a.error = b->ctr.p + B_ERROR;
   cudaError_t e = launch_batch_image(b->scheme.map.kind, b->scheme.map.arith, b->scheme.grid.kind, tu, a, b->stream);
   if (e != cudaSuccess) return e;
-  if (A > 0) inst_count_kernel<<<A, 256, 0, b->stream>>>(b->hit.p, b->off[in].p, b->cnt.p);
+  if (A > 0) inst_count_kernel<<<A, 256, 0, b->stream>>>(b->hit.p, b->off[in].p, b->cnt.p, b->hit.n,
+                                                         b->ctr.p + B_ERROR);
   // all active instances' children, in instance order, compacted by the hit mask
   CompactArgs ca{};
   ca.code = b->code[in].p;
@@ -602,11 +612,11 @@ cudaError_t enqueue_step(b12g_batch* b, uint32_t k, const Tuning& tu, bool with_
   if (e != cudaSuccess) return e;
   inst_offsets_kernel<<<1, 1024, 0, b->stream>>>(b->cnt.p, A, a_next, b->off[out].p,
                                                  b->step_counts.p + size_t(k - 1) * b->N, b->fin_lo.p,
-                                                 b->fin_len.p, b->ctr.p + B_FINBASE);
+                                                 b->fin_len.p, b->ctr.p + B_FINBASE, capu, b->ctr.p + B_ERROR);
   if (a_next < A) {
     copy_finished_kernel<<<device_sm_count() * 2, 256, 0, b->stream>>>(
         b->code[out].p, b->flags[out].p, b->off[out].p, a_next, A, b->fin_lo.p, b->fin_code.p, b->fin_flags.p,
-        uint32_t(std::min<uint64_t>(b->fin_cap, 0xFFFFFFFFu)), b->ctr.p + B_ERROR);
+        uint32_t(std::min<uint64_t>(b->fin_cap, 0xFFFFFFFFu)), capu, b->ctr.p + B_ERROR);
   }
   return cudaGetLastError();
 }
@@ -800,7 +810,7 @@ b12g_status b12g_batch_create(const b12g_domain* domain, const b12g_scheme* sche
       b->mp.table = tp;
     }
   }
-  if (st == B12G_OK) st = batch_reserve(b, std::max<uint64_t>(1ull << 20, 4ull * n));
+  if (st == B12G_OK) st = batch_reserve(b, std::max<uint64_t>(1ull << 22, 4ull * n));
   {
     std::lock_guard<std::mutex> lock(g_tune_mu);
     auto it = g_tuned.find(tune_key(b->device, scheme->map.kind, scheme->map.arith, scheme->grid.kind));
@@ -931,8 +941,9 @@ b12g_status b12g_batch_transition_matrices(b12g_batch* b, int absolute, int inva
   }
   CK(cudaMemsetAsync(b->hash.p, 0, b->hash.n * sizeof(ulonglong2), b->stream));
   const LeafHash h{b->hash.p, 1, b->hash_log2};
-  batch_hash_build_kernel<<<device_sm_count() * 4, 256, 0, b->stream>>>(b->fin_code.p, b->arena_off.p, b->N, h,
-                                                                       b->ctr.p + B_ERROR);
+  batch_hash_build_kernel<<<device_sm_count() * 4, 256, 0, b->stream>>>(
+      b->fin_code.p, b->arena_off.p, b->N, h, uint32_t(std::min<uint64_t>(b->fin_cap, 0xFFFFFFFFu)),
+      b->ctr.p + B_ERROR);
   BatchRowArgs ra{};
   ra.dom = b->dom;
   ra.map = b->mp;
