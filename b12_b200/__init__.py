@@ -9,9 +9,10 @@ from ._lib import (ALL, ARITH_FMA, ARITH_STRICT, B12gError, ENTR, EQU, EXPD, EXT
                    MAP_HENON, MAP_LORENZ, NONE, SD)
 from .tree import (Batch, CsrMatrix, GridSpec, ImplicitBoxTree, MapSpec, Scheme, coupled_duffing, forced_duffing,
                    full_grid, henon, inner_grid, lorenz, philox_grid)
+from .server import JobServer
 
 __all__ = [
-    "ImplicitBoxTree", "Batch", "CsrMatrix", "Scheme", "MapSpec", "GridSpec", "henon", "lorenz", "coupled_duffing",
+    "ImplicitBoxTree", "Batch", "JobServer", "CsrMatrix", "Scheme", "MapSpec", "GridSpec", "henon", "lorenz", "coupled_duffing",
     "forced_duffing", "inner_grid", "full_grid", "philox_grid", "B12gError", "NONE", "HIT", "INS", "EXPD", "SD",
     "EQU", "ENTR", "EXTR", "ALL", "LEAF_DEPTH", "INVALID_INDEX", "MAP_HENON", "MAP_LORENZ", "MAP_COUPLED_DUFFING",
     "MAP_FORCED_DUFFING", "GRID_INNER", "GRID_FULL", "GRID_PHILOX", "ARITH_STRICT", "ARITH_FMA",

@@ -48,6 +48,18 @@ class Scheme(C.Structure):
                 ("pad", C.c_uint8 * 6)]
 
 
+class Job(C.Structure):
+    _fields_ = [("domain", Domain), ("map", Map), ("grid", Grid), ("depth", C.c_uint32), ("pad", C.c_uint32)]
+
+
+class JobInfo(C.Structure):
+    _fields_ = [("state", C.c_uint32), ("depth", C.c_uint32), ("n_boxes", C.c_uint32), ("pad", C.c_uint32),
+                ("nnz", C.c_uint64), ("t_submit", C.c_double), ("t_start", C.c_double), ("t_done", C.c_double)]
+
+
+JOB_WAITING, JOB_RUNNING, JOB_DONE, JOB_FAILED = 0, 1, 2, 3
+
+
 class B12gError(RuntimeError):
     def __init__(self, status: int, where: str, message: str):
         super().__init__(f"{where}: {STATUS_NAMES.get(status, status)}: {message}")
@@ -105,6 +117,17 @@ _SIGS = {
     "b12g_batch_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
                                   C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     "b12g_batch_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "b12g_server_create": (C.c_int, [C.c_uint64, C.POINTER(C.c_void_p)]),
+    "b12g_server_destroy": (C.c_int, [C.c_void_p]),
+    "b12g_server_submit": (C.c_int, [C.c_void_p, C.POINTER(Job), C.POINTER(C.c_uint64)]),
+    "b12g_server_poll": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32), C.c_double]),
+    "b12g_server_job": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(JobInfo)]),
+    "b12g_server_result": (C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_void_p]),
+    "b12g_server_release": (C.c_int, [C.c_void_p, C.c_uint64]),
+    "b12g_server_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
+                                    C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint32),
+                                    C.POINTER(C.c_uint32)]),
     "b12g_tree_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "b12g_profile_enable": (C.c_int, [C.c_void_p, C.c_int]),
     "b12g_profile_read": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_double), C.POINTER(C.c_uint64), C.c_int]),

@@ -23,6 +23,7 @@
 #include <mutex>
 #include <vector>
 
+#include "batch.h"
 #include "rows.cuh"
 #include "tree.h"
 
@@ -31,34 +32,6 @@ using namespace b12g::host;
 
 namespace {
 
-constexpr uint32_t kMaxInstances = 4096;
-constexpr int kTune = 6;            // candidate (threads, points per thread) shapes
-
-struct Tuning {
-  uint32_t threads = 256;
-  uint32_t ppt = 1;                 // test points per thread
-  uint32_t chunk = 8192;            // points per work-queue item
-};
-
-// ------------------------------------------------------------------------ device side
-struct BatchArgs {
-  Domain dom;
-  MapParams map;                    // h, steps, table; p[] per instance from `params`
-  GridParams grid;
-  uint64_t points;                  // per box
-  const double* params;             // instance x 6
-  const uint8_t* depths;            // instance -> target depth (row kernel)
-  uint32_t n_inst;                  // instances in this launch (active prefix)
-  const uint32_t* off;              // n_inst + 1 parent offsets
-  const uint64_t* codes;            // parents
-  int depth;                        // depth of the children (subdivision step)
-  LeafHash hash;
-  uint8_t* hit;
-  uint32_t hit_cap;
-  uint32_t* queue;                  // work-queue head (zeroed before the launch)
-  uint32_t chunk;
-  uint32_t* error;
-};
 
 __device__ __forceinline__ uint32_t find_instance(const uint32_t* off_s, uint32_t n_inst, uint64_t x)
 {
@@ -140,14 +113,16 @@ struct BatchPoint {
   {
     double x[W][D], y[W][D];
     uint32_t inst[W];
+    int dep[W];
     MapParams mp[W];
 #pragma unroll
     for (int w = 0; w < W; ++w) {
       inst[w] = act[w] ? find_instance(off_s, a.n_inst, child[w] >> 1) : 0u;
+      dep[w] = a.inst_depth ? int(a.inst_depth[inst[w]]) : a.depth;
       const uint64_t c = child[w];
       const uint64_t code = act[w] ? ((a.codes[c >> 1] << 1) | (c & 1u)) : 0ull;
       double cc[D], r[D];
-      box_coordinates<D>(a.dom, code, a.depth, cc, r);
+      box_coordinates<D>(a.dom, code, dep[w], cc, r);
 #pragma unroll
       for (int j = 0; j < D; ++j) x[w][j] = __dadd_rn(cc[j], __dmul_rn(pts[j * uint32_t(a.points) + k[w]], r[j]));
       mp[w] = a.map;
@@ -173,7 +148,7 @@ struct BatchPoint {
 #pragma unroll
     for (int w = 0; w < W; ++w) {
       uint64_t tcode = 0;
-      const bool valid = act[w] && point_code<D>(a.dom, y[w], a.depth, tcode);
+      const bool valid = act[w] && point_code<D>(a.dom, y[w], dep[w], tcode);
       uint32_t t = kInvalidIndex;
       if (valid) {
         const uint32_t p = hash_locate(a.hash, off_s[a.n_inst], inst_key(inst[w], tcode >> 1));
@@ -308,26 +283,6 @@ __global__ void copy_finished_kernel(const uint64_t* code, const uint8_t* flags,
   }
 }
 
-// transition rows of the finished leaves of all instances: warp per row, targets found
-// by (instance, code); column = target index within its instance
-struct BatchRowArgs {
-  Domain dom;
-  MapParams map;
-  GridParams grid;
-  uint64_t points;
-  const double* params;
-  const uint8_t* depths;
-  uint32_t n_inst;
-  const uint32_t* off;            // arena-order region offsets (n_inst + 1)
-  const uint32_t* inst_of;        // arena index -> sorted position (params, depth)
-  const uint64_t* codes;          // final arena
-  LeafHash hash;
-  int keep_lost;
-  uint32_t* stage_col;
-  uint32_t* stage_cnt;
-  uint32_t* row_count;
-};
-
 template<class Map, class Grid>
 __global__ void __launch_bounds__(256) batch_rows_kernel(const BatchRowArgs a)
 {
@@ -408,6 +363,10 @@ int batch_grid(const void* kernel, int threads)
   return device_sm_count() * (b > 0 ? b : 1);
 }
 
+}  // namespace
+
+namespace b12g {
+
 cudaError_t launch_batch_image(uint32_t map_kind, uint32_t arith, uint32_t grid_kind, const Tuning& tu,
                                const BatchArgs& a, cudaStream_t s)
 {
@@ -437,6 +396,29 @@ cudaError_t launch_batch_rows(uint32_t map_kind, uint32_t arith, uint32_t grid_k
     return cudaGetLastError();
   });
 }
+
+bool batch_supported(uint32_t map_kind, uint32_t arith, uint32_t grid_kind)
+{
+  return batch_dispatch(map_kind, arith, grid_kind, [](auto, auto) { return cudaSuccess; }) == cudaSuccess;
+}
+
+cudaError_t launch_batch_hash(const uint64_t* codes, const uint32_t* off, uint32_t n_inst, LeafHash h,
+                              uint32_t code_cap, uint32_t* error, cudaStream_t s)
+{
+  batch_hash_build_kernel<<<device_sm_count() * 4, 256, 0, s>>>(codes, off, n_inst, h, code_cap, error);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_inst_count(const uint8_t* hit, const uint32_t* off, uint32_t n_inst, uint32_t* cnt,
+                              uint64_t hit_cap, uint32_t* error, cudaStream_t s)
+{
+  if (n_inst > 0) inst_count_kernel<<<n_inst, 256, 0, s>>>(hit, off, cnt, hit_cap, error);
+  return cudaGetLastError();
+}
+
+}  // namespace b12g
+
+namespace {
 
 // autotuning results, per (device, map, arith, grid)
 std::mutex g_tune_mu;

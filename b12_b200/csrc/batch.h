@@ -1,0 +1,73 @@
+// Batched box-image kernels shared by the batch (batch.cu) and the job server (serve.cu).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "kernels.h"
+
+namespace b12g {
+
+constexpr uint32_t kMaxInstances = 4096;
+
+struct Tuning {
+  uint32_t threads = 256;
+  uint32_t ppt = 1;                 // test points per thread
+  uint32_t chunk = 8192;            // points per work-queue item
+};
+
+// ------------------------------------------------------------------------ device side
+struct BatchArgs {
+  Domain dom;
+  MapParams map;                    // h, steps, table; p[] per instance from `params`
+  GridParams grid;
+  uint64_t points;                  // per box
+  const double* params;             // instance x 6
+  const uint8_t* depths;            // instance -> target depth (row kernel)
+  uint32_t n_inst;                  // instances in this launch (active prefix)
+  const uint32_t* off;              // n_inst + 1 parent offsets
+  const uint64_t* codes;            // parents
+  int depth;                        // depth of the children (subdivision step)
+  const uint8_t* inst_depth;        // per-instance children depth (nullptr: `depth` for all)
+  LeafHash hash;
+  uint8_t* hit;
+  uint32_t hit_cap;
+  uint32_t* queue;                  // work-queue head (zeroed before the launch)
+  uint32_t chunk;
+  uint32_t* error;
+};
+
+// transition rows of the finished leaves of all instances: warp per row, targets found
+// by (instance, code); column = target index within its instance
+struct BatchRowArgs {
+  Domain dom;
+  MapParams map;
+  GridParams grid;
+  uint64_t points;
+  const double* params;
+  const uint8_t* depths;
+  uint32_t n_inst;
+  const uint32_t* off;            // arena-order region offsets (n_inst + 1)
+  const uint32_t* inst_of;        // arena index -> sorted position (params, depth)
+  const uint64_t* codes;          // final arena
+  LeafHash hash;
+  int keep_lost;
+  uint32_t* stage_col;
+  uint32_t* stage_cnt;
+  uint32_t* row_count;
+};
+
+// launches (batch.cu)
+bool batch_supported(uint32_t map_kind, uint32_t arith, uint32_t grid_kind);
+cudaError_t launch_batch_image(uint32_t map_kind, uint32_t arith, uint32_t grid_kind, const Tuning& tu,
+                               const BatchArgs& a, cudaStream_t s);
+cudaError_t launch_batch_rows(uint32_t map_kind, uint32_t arith, uint32_t grid_kind, const BatchRowArgs& a,
+                              uint32_t max_rows, cudaStream_t s);
+// lookup table over (instance, code) of n_inst concatenated code segments
+cudaError_t launch_batch_hash(const uint64_t* codes, const uint32_t* off, uint32_t n_inst, LeafHash h,
+                              uint32_t code_cap, uint32_t* error, cudaStream_t s);
+// survivors per instance from the hit mask of the instances' (implicit) children
+cudaError_t launch_inst_count(const uint8_t* hit, const uint32_t* off, uint32_t n_inst, uint32_t* cnt,
+                              uint64_t hit_cap, uint32_t* error, cudaStream_t s);
+
+}  // namespace b12g

@@ -243,6 +243,52 @@ b12g_status b12g_batch_info(b12g_batch* batch, uint64_t* box_images, uint64_t* f
                             uint32_t* threads, uint32_t* points_per_thread, uint32_t* chunk);
 b12g_status b12g_batch_stream(b12g_batch* batch, void** stream);
 
+/* ---- job server: continuous batching of subdivision jobs ---------------------------------
+ * No counterpart in the reference, which runs one ImplicitBoxTree per process.  A job is
+ * `depth` steps of the subdivision loop (subdivision.m:18-45) from the surrounding box,
+ * followed by transitionMatrixForLeaves (relative transition probabilities, points
+ * leaving the leaves dropped).  Jobs of one family (domain, map kind, arithmetic,
+ * integrator step and steps, grid) share an engine: a host thread and CUDA stream that
+ * advances every job it holds by one subdivision step per tick in one batched launch
+ * sequence; a job submitted while others run joins at the next tick, and leaves at the
+ * end of its last step with its leaves and CSR resident on the device until released.
+ * Families run concurrently.  Admission is by projected HBM footprint against the
+ * server's cap (first come, first served within a family).  Inner and full grids with up
+ * to 128 points per box. */
+typedef struct b12g_server b12g_server;
+typedef struct {
+  b12g_domain domain;
+  b12g_map map;          /* p[] is the job's own parameter set */
+  b12g_grid grid;
+  uint32_t depth;        /* subdivision steps, 1..32 */
+  uint32_t pad;
+} b12g_job;
+enum { B12G_JOB_WAITING = 0, B12G_JOB_RUNNING = 1, B12G_JOB_DONE = 2, B12G_JOB_FAILED = 3 };
+typedef struct {
+  uint32_t state;
+  uint32_t depth;
+  uint32_t n_boxes;      /* final leaves (done jobs) */
+  uint32_t pad;
+  uint64_t nnz;
+  double t_submit, t_start, t_done;   /* seconds on the server's steady clock */
+} b12g_job_info;
+/* hbm_cap_bytes: admission cap (0: 80% of the free device memory at creation) */
+b12g_status b12g_server_create(uint64_t hbm_cap_bytes, b12g_server** server);
+/* stops the engines after their current tick and frees every result */
+b12g_status b12g_server_destroy(b12g_server* server);
+b12g_status b12g_server_submit(b12g_server* server, const b12g_job* job, uint64_t* id);
+/* ids of jobs finished (or failed) since the last poll, waiting up to wait_seconds for one */
+b12g_status b12g_server_poll(b12g_server* server, uint64_t* ids, uint32_t max, uint32_t* n, double wait_seconds);
+b12g_status b12g_server_job(b12g_server* server, uint64_t id, b12g_job_info* info);
+/* a done job's leaf counts after each step (depth entries), final leaves (n_boxes codes at
+ * the job's depth) and CSR; any pointer may be NULL */
+b12g_status b12g_server_result(b12g_server* server, uint64_t id, uint64_t* codes, uint32_t* counts,
+                               uint32_t* rowptr, uint32_t* cols, double* vals);
+/* free a done or failed job's resident result and its admission reservation */
+b12g_status b12g_server_release(b12g_server* server, uint64_t id);
+b12g_status b12g_server_stats(b12g_server* server, uint64_t* ticks, uint64_t* box_images, uint64_t* in_use_bytes,
+                              uint64_t* cap_bytes, uint32_t* waiting, uint32_t* running);
+
 /* ---- measurement hooks (no counterpart in the reference) ---------------------------------- */
 /* the CUDA stream (cudaStream_t) every kernel of this tree runs on */
 b12g_status b12g_tree_stream(b12g_tree* tree, void** stream);
