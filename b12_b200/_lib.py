@@ -128,6 +128,8 @@ _SIGS = {
     "b12g_server_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
                                     C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint32),
                                     C.POINTER(C.c_uint32)]),
+    "b12g_server_engine_stats": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64),
+                                           C.POINTER(C.c_uint64), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "b12g_tree_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "b12g_profile_enable": (C.c_int, [C.c_void_p, C.c_int]),
     "b12g_profile_read": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_double), C.POINTER(C.c_uint64), C.c_int]),

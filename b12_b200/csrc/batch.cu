@@ -102,6 +102,15 @@ template<class A> struct Multi<LorenzMap<A>> {
   }
 };
 
+template<> struct Multi<ForcedDuffingMap> {
+  static constexpr bool kOk = true;
+  template<int W, int D>
+  static __device__ __forceinline__ void apply(const MapParams& m, const double (&x)[W][D], double (&y)[W][D])
+  {
+    duffing_apply_multi<W>(m, x, y);
+  }
+};
+
 // the image of child point (child c of the concatenated children, grid index k)
 template<class Map, class Grid, int W>
 struct BatchPoint {
@@ -373,7 +382,15 @@ cudaError_t launch_batch_image(uint32_t map_kind, uint32_t arith, uint32_t grid_
   return batch_dispatch(map_kind, arith, grid_kind, [&](auto map, auto grid) -> cudaError_t {
     using Map = decltype(map);
     using Grid = decltype(grid);
-    if (tu.ppt == 2) {
+    if constexpr (Map::D <= 2) {
+      // four points per thread only for the two-dimensional maps (register budget)
+      if (tu.ppt == 4) {
+        const void* k = (const void*)batch_image_kernel<Map, Grid, 4>;
+        batch_image_kernel<Map, Grid, 4><<<batch_grid(k, int(tu.threads)), tu.threads, 0, s>>>(a);
+        return cudaGetLastError();
+      }
+    }
+    if (tu.ppt >= 2) {
       const void* k = (const void*)batch_image_kernel<Map, Grid, 2>;
       batch_image_kernel<Map, Grid, 2><<<batch_grid(k, int(tu.threads)), tu.threads, 0, s>>>(a);
     } else {
@@ -428,6 +445,28 @@ uint64_t tune_key(int dev, uint32_t map, uint32_t arith, uint32_t grid)
 {
   return (uint64_t(dev) << 48) | (uint64_t(map) << 32) | (uint64_t(arith) << 16) | grid;
 }
+
+}  // namespace
+
+namespace b12g {
+
+Tuning batch_tuning(int device, uint32_t map_kind, uint32_t arith, uint32_t grid_kind, uint32_t dim)
+{
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tuned.find(tune_key(device, map_kind, arith, grid_kind));
+    if (it != g_tuned.end()) return it->second;
+  }
+  // the shapes the tuner picks on B200 for these maps: the two-dimensional maps keep four
+  // points per thread in flight, Lorenz one
+  Tuning t{};
+  if (dim <= 2 && map_kind == B12G_MAP_FORCED_DUFFING) t.ppt = 4;
+  return t;
+}
+
+}  // namespace b12g
+
+namespace {
 
 }  // namespace
 
@@ -612,9 +651,12 @@ uint64_t step_kernels(const b12g_batch* b, uint32_t k)
 // time every candidate shape on the batch's own steps (first run) and keep the fastest
 b12g_status autotune(b12g_batch* b)
 {
-  const Tuning cands[] = {{256, 1, 8192}, {256, 2, 8192}, {128, 1, 8192}, {512, 1, 16384}, {256, 1, 32768},
-                          {256, 2, 32768}};
-  std::vector<double> total(sizeof cands / sizeof cands[0], 0.0);
+  const Tuning all[] = {{256, 1, 8192}, {256, 2, 8192}, {128, 1, 8192}, {512, 1, 16384}, {256, 1, 32768},
+                        {256, 2, 32768}, {256, 4, 8192}, {128, 4, 8192}};
+  std::vector<Tuning> cands;
+  for (const Tuning& t : all)
+    if (t.ppt < 4 || b->domain.dim <= 2) cands.push_back(t);   // 4 points per thread: 2-D maps only
+  std::vector<double> total(cands.size(), 0.0);
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
@@ -793,6 +835,8 @@ b12g_status b12g_batch_create(const b12g_domain* domain, const b12g_scheme* sche
     }
   }
   if (st == B12G_OK) st = batch_reserve(b, std::max<uint64_t>(1ull << 22, 4ull * n));
+  // start from the family's usual shape; the first run tunes it unless this process has
+  b->tuning = batch_tuning(b->device, scheme->map.kind, scheme->map.arith, scheme->grid.kind, domain->dim);
   {
     std::lock_guard<std::mutex> lock(g_tune_mu);
     auto it = g_tuned.find(tune_key(b->device, scheme->map.kind, scheme->map.arith, scheme->grid.kind));

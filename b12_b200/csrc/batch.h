@@ -57,6 +57,10 @@ struct BatchRowArgs {
   uint32_t* row_count;
 };
 
+// the image kernel's launch shape for a map family: the autotuned one when a batch of
+// this process has tuned it on `device`, else the shape the tuner settles on for it
+Tuning batch_tuning(int device, uint32_t map_kind, uint32_t arith, uint32_t grid_kind, uint32_t dim);
+
 // launches (batch.cu)
 bool batch_supported(uint32_t map_kind, uint32_t arith, uint32_t grid_kind);
 cudaError_t launch_batch_image(uint32_t map_kind, uint32_t arith, uint32_t grid_kind, const Tuning& tu,

@@ -527,4 +527,55 @@ struct ForcedDuffingMap {
   }
 };
 
+// ForcedDuffingMap::apply for W points sharing the map parameters, interleaved so that one
+// thread keeps W dependency chains in flight; every point's operations and their order
+// are those of apply()
+template<int W>
+__device__ __forceinline__ void duffing_apply_multi(const MapParams& m, const double (&x0)[W][2], double (&res)[W][2])
+{
+  double x[W][2], k[W][2], a[W][2];
+#pragma unroll
+  for (int w = 0; w < W; ++w) { x[w][0] = x0[w][0]; x[w][1] = x0[w][1]; }
+#pragma unroll 1
+  for (uint32_t s = 0; s < m.steps; ++s) {
+    const double c0 = __ldg(m.table + 2 * s), c1 = __ldg(m.table + 2 * s + 1), c2 = __ldg(m.table + 2 * s + 2);
+#pragma unroll
+    for (int w = 0; w < W; ++w) ForcedDuffingMap::rhs(m, c0, x[w], k[w]);
+#pragma unroll
+    for (int w = 0; w < W; ++w)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        res[w][j] = Strict::madd(m.h6, k[w][j], x[w][j]);
+        a[w][j] = Strict::madd(m.h2, k[w][j], x[w][j]);
+      }
+#pragma unroll
+    for (int w = 0; w < W; ++w) ForcedDuffingMap::rhs(m, c1, a[w], k[w]);
+#pragma unroll
+    for (int w = 0; w < W; ++w)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        res[w][j] = Strict::madd(m.h3, k[w][j], res[w][j]);
+        a[w][j] = Strict::madd(m.h2, k[w][j], x[w][j]);
+      }
+#pragma unroll
+    for (int w = 0; w < W; ++w) ForcedDuffingMap::rhs(m, c1, a[w], k[w]);
+#pragma unroll
+    for (int w = 0; w < W; ++w)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        res[w][j] = Strict::madd(m.h3, k[w][j], res[w][j]);
+        a[w][j] = Strict::madd(m.h, k[w][j], x[w][j]);
+      }
+#pragma unroll
+    for (int w = 0; w < W; ++w) ForcedDuffingMap::rhs(m, c2, a[w], k[w]);
+#pragma unroll
+    for (int w = 0; w < W; ++w)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        res[w][j] = Strict::madd(m.h6, k[w][j], res[w][j]);
+        x[w][j] = res[w][j];
+      }
+  }
+}
+
 }  // namespace b12g

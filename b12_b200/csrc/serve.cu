@@ -37,6 +37,7 @@ using namespace b12g::host;
 namespace {
 
 constexpr uint32_t kMaxSlots = 2048;            // jobs per engine at once
+constexpr uint64_t kInitialLeaves = 1u << 19;
 
 double now_s()
 {
@@ -50,7 +51,7 @@ uint64_t projected_boxes(const b12g_job& j)
   double c = 4.0;
   if (j.map.kind == B12G_MAP_HENON) c = 2.5;
   else if (j.map.kind == B12G_MAP_LORENZ) c = 1.6;
-  else if (j.map.kind == B12G_MAP_FORCED_DUFFING) c = 8.0;
+  else if (j.map.kind == B12G_MAP_FORCED_DUFFING) c = 2.0;
   const double est = c * std::pow(1.6, double(j.depth));
   const double cap = std::ldexp(1.0, std::min<int>(int(j.depth), 62));
   return uint64_t(std::max(1.0, std::min(est, cap)));
@@ -78,7 +79,8 @@ struct Job {
   uint64_t reserved = 0;          // admitted bytes
   uint32_t depth_done = 0;        // subdivision steps done
   std::vector<uint32_t> counts;   // leaves after each step
-  // resident results
+  // resident result: one block from the server's pool holding codes, vals, rowptr, cols
+  void* mem = nullptr;
   uint64_t* codes = nullptr;
   uint32_t* rowptr = nullptr;
   uint32_t* cols = nullptr;
@@ -119,9 +121,14 @@ struct Engine {
   double* hp = nullptr;              // parameters
   uint8_t* hd = nullptr;             // depths and finishing marks
   uint64_t boxes = 0;                // parents after the last tick
+  // counters written by the engine thread
+  std::atomic<uint64_t> ticks{0}, jobs_done{0};
+  std::atomic<double> tick_seconds{0.0}, finish_seconds{0.0};
 };
 
 struct Server {
+  cudaMemPool_t pool = nullptr;    // results (kept across synchronisations)
+  cudaStream_t release_stream = nullptr;
   std::mutex mu;
   std::condition_variable cv;
   bool stop = false;
@@ -166,28 +173,80 @@ __global__ void append_roots_kernel(uint32_t* off, uint32_t A, uint32_t n_new, u
   }
 }
 
-// new offsets (all slots) and the split into continuing slots (packed, keep_off) and
-// finished slots (fin_off), both in slot order
-__global__ void split_offsets_kernel(const uint32_t* cnt, const uint8_t* finishing, uint32_t A, uint32_t* new_off,
-                                     uint32_t* keep_off, uint32_t* fin_off, uint32_t* ctr)
+// exclusive scan over one block of kSplitThreads threads of four counters at once
+constexpr uint32_t kSplitThreads = kMaxSlots / 2;
+
+__device__ uint4 block_exclusive_scan4(uint4 v, uint4* total)
 {
-  if (threadIdx.x != 0) return;
-  uint32_t all = 0, keep = 0, fin = 0, nf = 0;
-  for (uint32_t i = 0; i < A; ++i) {
-    new_off[i] = all;
-    if (finishing[i]) {
-      fin_off[nf++] = fin;
-      fin += cnt[i];
-    } else {
-      keep_off[i] = keep;
-      keep += cnt[i];
-    }
-    all += cnt[i];
+  __shared__ uint4 warp_sums[kSplitThreads / 32];
+  const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  uint4 inc = v;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t x = __shfl_up_sync(0xFFFFFFFFu, inc.x, d), y = __shfl_up_sync(0xFFFFFFFFu, inc.y, d);
+    const uint32_t z = __shfl_up_sync(0xFFFFFFFFu, inc.z, d), q = __shfl_up_sync(0xFFFFFFFFu, inc.w, d);
+    if (lane >= uint32_t(d)) { inc.x += x; inc.y += y; inc.z += z; inc.w += q; }
   }
-  new_off[A] = all;
-  fin_off[nf] = fin;
-  ctr[E_KEEP] = keep;
-  ctr[E_FIN] = fin;
+  if (lane == 31) warp_sums[w] = inc;
+  __syncthreads();
+  if (w == 0) {
+    uint4 s = lane < kSplitThreads / 32 ? warp_sums[lane] : make_uint4(0, 0, 0, 0);
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t x = __shfl_up_sync(0xFFFFFFFFu, s.x, d), y = __shfl_up_sync(0xFFFFFFFFu, s.y, d);
+      const uint32_t z = __shfl_up_sync(0xFFFFFFFFu, s.z, d), q = __shfl_up_sync(0xFFFFFFFFu, s.w, d);
+      if (lane >= uint32_t(d)) { s.x += x; s.y += y; s.z += z; s.w += q; }
+    }
+    if (lane < kSplitThreads / 32) warp_sums[lane] = s;   // inclusive warp prefixes
+  }
+  __syncthreads();
+  const uint4 before = w ? warp_sums[w - 1] : make_uint4(0, 0, 0, 0);
+  *total = warp_sums[kSplitThreads / 32 - 1];
+  return make_uint4(before.x + inc.x - v.x, before.y + inc.y - v.y, before.z + inc.z - v.z, before.w + inc.w - v.w);
+}
+
+// one block of kSplitThreads threads, two slots each: the survivors' offsets for all
+// slots (new_off), for the continuing slots (keep_off, and packed into `off` as the
+// parent offsets of the next tick) and for the finished slots (fin_off, in finish order)
+__global__ void __launch_bounds__(kSplitThreads) split_offsets_kernel(const uint32_t* cnt, const uint8_t* finishing,
+                                                                      uint32_t A, uint32_t* new_off,
+                                                                      uint32_t* keep_off, uint32_t* fin_off,
+                                                                      uint32_t* off, uint32_t* ctr)
+{
+  uint32_t c[2] = {0, 0}, f[2] = {0, 0};
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const uint32_t i = 2 * threadIdx.x + k;
+    if (i < A) { c[k] = cnt[i]; f[k] = finishing[i] ? 1u : 0u; }
+  }
+  // (all survivors, continuing survivors, finished survivors, finished slots)
+  const uint4 mine = make_uint4(c[0] + c[1], (1 - f[0]) * c[0] + (1 - f[1]) * c[1], f[0] * c[0] + f[1] * c[1],
+                                f[0] + f[1]);
+  uint4 total;
+  uint4 p = block_exclusive_scan4(mine, &total);
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const uint32_t i = 2 * threadIdx.x + k;
+    if (i >= A) break;
+    new_off[i] = p.x;
+    if (f[k]) {
+      fin_off[p.w] = p.z;
+    } else {
+      keep_off[i] = p.y;
+      off[i - p.w] = p.y;            // rank among the continuing slots
+    }
+    p.x += c[k];
+    p.y += (1 - f[k]) * c[k];
+    p.z += f[k] * c[k];
+    p.w += f[k];
+  }
+  if (threadIdx.x == 0) {
+    new_off[A] = total.x;
+    fin_off[total.w] = total.z;
+    off[A - total.w] = total.y;
+    ctr[E_KEEP] = total.y;
+    ctr[E_FIN] = total.z;
+  }
 }
 
 // move every survivor to the packed parents of the continuing slots or to the arena
@@ -222,17 +281,6 @@ __global__ void split_copy_kernel(const uint64_t* survivors, const uint8_t* surv
   }
 }
 
-// offsets of the continuing slots, packed in slot order
-__global__ void keep_offsets_kernel(const uint32_t* keep_off, const uint8_t* finishing, uint32_t A,
-                                    const uint32_t* ctr, uint32_t* off)
-{
-  if (threadIdx.x != 0) return;
-  uint32_t k = 0;
-  for (uint32_t i = 0; i < A; ++i)
-    if (!finishing[i]) off[k++] = keep_off[i];
-  off[k] = ctr[E_KEEP];
-}
-
 // first nonzero of each finished job's rows: row0[q] = rowptr[fin_off[q]], q <= nf
 __global__ void row_starts_kernel(const uint32_t* rowptr, const uint32_t* fin_off, uint32_t nf, uint32_t* row0)
 {
@@ -257,6 +305,8 @@ __global__ void extract_kernel(const uint32_t* rowptr, const uint32_t* cols, con
 }
 
 // ---------------------------------------------------------------------------- engine
+b12g_status engine_reserve(Engine* e, uint64_t parents);
+
 b12g_status engine_init(Engine* e, const b12g_job& key)
 {
   e->key = key;
@@ -286,6 +336,7 @@ b12g_status engine_init(Engine* e, const b12g_job& key)
   if (st != B12G_OK) return st;
   if (e->P > kMaxRowPoints)
     return fail(B12G_ERR_CAPACITY, "served jobs take up to %u grid points per box", kMaxRowPoints);
+  e->tuning = batch_tuning(e->srv->device, key.map.kind, key.map.arith, key.grid.kind, key.domain.dim);
   CK(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
   CK(cudaMallocHost(&e->h, kHostWords * 4));
   CK(cudaMallocHost(&e->hp, size_t(kMaxSlots) * 6 * 8));
@@ -305,9 +356,17 @@ b12g_status engine_init(Engine* e, const b12g_job& key)
   ST(e->fin_depth.ensure(kMaxSlots, "engine depths"));
   CK(cudaMemsetAsync(e->off.p, 0, (kMaxSlots + 1) * 4, e->stream));
   CK(cudaMemsetAsync(e->ctr.p, 0, E_COUNT * 4, e->stream));
+  // working set for half a million leaves in flight before the first growth
+  ST(engine_reserve(e, kInitialLeaves));
+  ST(e->stage_col.ensure(kInitialLeaves * e->P, "row staging"));
+  ST(e->stage_cnt.ensure(kInitialLeaves * e->P, "row staging"));
   CK(cudaStreamSynchronize(e->stream));
   return B12G_OK;
 }
+
+// grow-only buffers of an engine double when they grow: every reallocation frees the old
+// buffer, which waits for the whole device
+size_t grow(size_t have, size_t need) { return need <= have ? need : std::max(need, 2 * have); }
 
 b12g_status engine_hash_capacity(Engine* e, uint64_t keys)
 {
@@ -329,15 +388,15 @@ b12g_status engine_reserve(Engine* e, uint64_t parents)
   const uint64_t need = std::max<uint64_t>(parents, 1024);
   if (need > 0x3FFFFFF0ull) return fail(B12G_ERR_CAPACITY, "engine above 2^30 leaves");
   // the live parents (and their flags) survive a reallocation
-  ST(e->parents.grow_keep(2 * need, e->boxes, e->stream, "engine parents"));
-  ST(e->flags_a.grow_keep(2 * need, e->boxes, e->stream, "engine flags"));
-  ST(e->children.ensure(2 * need, "engine survivors"));
-  ST(e->flags_b.ensure(2 * need, "engine survivor flags"));
+  ST(e->parents.grow_keep(grow(e->parents.n, 2 * need), e->boxes, e->stream, "engine parents"));
+  ST(e->flags_a.grow_keep(grow(e->flags_a.n, 2 * need), e->boxes, e->stream, "engine flags"));
+  ST(e->children.ensure(grow(e->children.n, 2 * need), "engine survivors"));
+  ST(e->flags_b.ensure(grow(e->flags_b.n, 2 * need), "engine survivor flags"));
   if (e->hit.n < 2 * need) {
-    ST(e->hit.ensure(2 * need, "engine hit mask"));
+    ST(e->hit.ensure(grow(e->hit.n, 2 * need), "engine hit mask"));
     CK(cudaMemsetAsync(e->hit.p, 0, e->hit.n, e->stream));
   }
-  ST(e->arena.ensure(2 * need, "engine arena"));
+  ST(e->arena.ensure(grow(e->arena.n, 2 * need), "engine arena"));
   const size_t most = std::max<size_t>(e->hit.n, 2 * need) + 1;
   ST(e->tiles_a.ensure(compact_tiles(most) + 2, "engine tiles"));
   ST(e->tiles_b.ensure(compact_tiles(most) + 2, "engine tiles"));
@@ -367,6 +426,7 @@ void fail_job_locked(Server* s, Job* j, const std::string& why)
 b12g_status engine_finish(Engine* e, const std::vector<uint32_t>& fin, uint32_t rows)
 {
   Server* s = e->srv;
+  const double t_begin = now_s();
   const uint32_t nf = uint32_t(fin.size());
   if (nf == 0) return B12G_OK;
   // the finished jobs' parameters and depths, in finish order
@@ -380,8 +440,8 @@ b12g_status engine_finish(Engine* e, const std::vector<uint32_t>& fin, uint32_t 
   CK(cudaMemcpyAsync(e->fin_depth.p, e->hd, nf, cudaMemcpyHostToDevice, e->stream));
   CK(cudaMemcpyAsync(e->fin_slot.p, e->h + kHostScratch, nf * 4, cudaMemcpyHostToDevice, e->stream));
   const uint64_t stage = std::max<uint64_t>(uint64_t(rows) * e->P, 1);
-  ST(e->stage_col.ensure(stage, "row staging"));
-  ST(e->stage_cnt.ensure(stage, "row staging"));
+  ST(e->stage_col.ensure(grow(e->stage_col.n, stage), "row staging"));
+  ST(e->stage_cnt.ensure(grow(e->stage_cnt.n, stage), "row staging"));
   ST(e->row_count.ensure(rows + 1, "row counts"));
   ST(e->rowptr.ensure(rows + 1, "row pointers"));
   ST(e->tiles_a.ensure(compact_tiles(rows + 1) + 2, "tiles"));
@@ -414,8 +474,8 @@ b12g_status engine_finish(Engine* e, const std::vector<uint32_t>& fin, uint32_t 
   CK(cudaMemcpyAsync(h_nnz, e->rowptr.p + rows, 4, cudaMemcpyDeviceToHost, e->stream));
   CK(cudaStreamSynchronize(e->stream));
   const uint32_t nnz = *h_nnz;
-  ST(e->cols_all.ensure(std::max<uint32_t>(nnz, 1), "columns"));
-  ST(e->vals_all.ensure(std::max<uint32_t>(nnz, 1), "values"));
+  ST(e->cols_all.ensure(grow(e->cols_all.n, std::max<uint32_t>(nnz, 1)), "columns"));
+  ST(e->vals_all.ensure(grow(e->vals_all.n, std::max<uint32_t>(nnz, 1)), "values"));
   CK(gather_rows(e->stage_col.p, e->stage_cnt.p, uint32_t(e->P), e->row_count.p, e->rowptr.p, e->fin_off.p + nf,
                  e->cols_all.p, e->vals_all.p, 0, double(e->P), rows, e->stream));
   row_starts_kernel<<<(nf + 256) / 256, 256, 0, e->stream>>>(e->rowptr.p, e->fin_off.p, nf, e->row0.p);
@@ -434,11 +494,16 @@ b12g_status engine_finish(Engine* e, const std::vector<uint32_t>& fin, uint32_t 
     j->n_boxes = n;
     j->nnz = z;
     if (n == 0) continue;  // every box was removed: the result is the surrounding box
-    cudaError_t ce = cudaMallocAsync(&j->codes, size_t(n) * 8, e->stream);
-    if (ce == cudaSuccess) ce = cudaMallocAsync(&j->rowptr, size_t(n + 1) * 4, e->stream);
-    if (ce == cudaSuccess) ce = cudaMallocAsync(&j->cols, std::max<size_t>(z, 1) * 4, e->stream);
-    if (ce == cudaSuccess) ce = cudaMallocAsync(&j->vals, std::max<size_t>(z, 1) * 8, e->stream);
-    if (ce != cudaSuccess) {
+    const size_t b_codes = size_t(n) * 8, b_vals = z * 8, b_rowptr = size_t(n + 1) * 4;
+    const size_t bytes = b_codes + b_vals + b_rowptr + z * 4;
+    const cudaError_t ce = cudaMallocFromPoolAsync(&j->mem, bytes, s->pool, e->stream);
+    if (ce == cudaSuccess) {
+      uint8_t* m = static_cast<uint8_t*>(j->mem);
+      j->codes = reinterpret_cast<uint64_t*>(m);
+      j->vals = reinterpret_cast<double*>(m + b_codes);
+      j->rowptr = reinterpret_cast<uint32_t*>(m + b_codes + b_vals);
+      j->cols = reinterpret_cast<uint32_t*>(m + b_codes + b_vals + b_rowptr);
+    } else {
       cudaGetLastError();
       failed[q] = "out of device memory for the job's result";
       continue;
@@ -451,6 +516,8 @@ b12g_status engine_finish(Engine* e, const std::vector<uint32_t>& fin, uint32_t 
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(e->stream));
   const double t = now_s();
+  e->finish_seconds = e->finish_seconds + (t - t_begin);
+  e->jobs_done += nf;
   std::lock_guard<std::mutex> lock(s->mu);
   for (uint32_t q = 0; q < nf; ++q) {
     Job* j = e->slots[fin[q]];
@@ -474,6 +541,7 @@ b12g_status engine_tick(Engine* e, const std::vector<Job*>& joining)
   const uint32_t J = uint32_t(joining.size());
   const uint32_t A = A0 + J;
   if (A == 0) return B12G_OK;
+  const double t_begin = now_s();
   const uint64_t parents = e->boxes + J;
   ST(engine_reserve(e, parents));
   if (J) {
@@ -541,14 +609,13 @@ b12g_status engine_tick(Engine* e, const std::vector<Job*>& joining)
   ca.error = e->ctr.p + E_ERROR;
   CK(compact(ca, {e->tiles_a.p, e->tiles_b.p}, uint32_t(parents), e->stream));
   // 4. continuing jobs packed back into the parents, finished ones into the arena
-  split_offsets_kernel<<<1, 32, 0, e->stream>>>(e->cnt.p, e->depth_child.p + kMaxSlots, A, e->new_off.p,
-                                                e->keep_off.p, e->fin_off.p, e->ctr.p);
+  split_offsets_kernel<<<1, kSplitThreads, 0, e->stream>>>(e->cnt.p, e->depth_child.p + kMaxSlots, A, e->new_off.p,
+                                                           e->keep_off.p, e->fin_off.p, e->off.p, e->ctr.p);
   split_copy_kernel<<<device_sm_count() * 2, 256, 0, e->stream>>>(
       e->children.p, e->flags_b.p, e->new_off.p, A, e->depth_child.p + kMaxSlots, e->keep_off.p, e->fin_off.p,
       e->fin_rank.p, e->parents.p, e->flags_a.p, e->arena.p, capu,
       uint32_t(std::min<size_t>(e->arena.n, 0xFFFFFFFFu)), e->ctr.p + E_ERROR);
-  keep_offsets_kernel<<<1, 32, 0, e->stream>>>(e->keep_off.p, e->depth_child.p + kMaxSlots, A, e->ctr.p, e->off.p);
-  count_launches(9);
+  count_launches(8);
   CK(cudaGetLastError());
   // this step's counts and the counters
   CK(cudaMemcpyAsync(e->h + kHostCounts, e->cnt.p, size_t(A) * 4, cudaMemcpyDeviceToHost, e->stream));
@@ -571,6 +638,8 @@ b12g_status engine_tick(Engine* e, const std::vector<Job*>& joining)
   e->slots.swap(rest);
   e->boxes = keep_total;
   s->ticks += 1;
+  e->ticks += 1;
+  e->tick_seconds = e->tick_seconds + (now_s() - t_begin);
   return B12G_OK;
 }
 
@@ -621,12 +690,10 @@ void engine_loop(Engine* e)
   }
 }
 
-void free_job_memory(Job* j)
+void free_job_memory(Server* s, Job* j)
 {
-  if (j->codes) cudaFree(j->codes);
-  if (j->rowptr) cudaFree(j->rowptr);
-  if (j->cols) cudaFree(j->cols);
-  if (j->vals) cudaFree(j->vals);
+  if (j->mem) cudaFreeAsync(j->mem, s->release_stream);
+  j->mem = nullptr;
   j->codes = nullptr;
   j->rowptr = nullptr;
   j->cols = nullptr;
@@ -671,6 +738,19 @@ b12g_status b12g_server_create(uint64_t hbm_cap_bytes, b12g_server** out)
   size_t free_b = 0, total_b = 0;
   CK(cudaMemGetInfo(&free_b, &total_b));
   sv->s.cap_bytes = hbm_cap_bytes ? hbm_cap_bytes : uint64_t(double(free_b) * 0.8);
+  // results come from a pool of the server's own that keeps freed memory for reuse
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = sv->s.device;
+  cudaError_t ce = cudaMemPoolCreate(&sv->s.pool, &props);
+  uint64_t keep = ~0ull;
+  if (ce == cudaSuccess) ce = cudaMemPoolSetAttribute(sv->s.pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&sv->s.release_stream, cudaStreamNonBlocking);
+  if (ce != cudaSuccess) {
+    b12g_server_destroy(sv);
+    return cuda_fail(ce, "server memory pool");
+  }
   *out = sv;
   return B12G_OK;
 }
@@ -801,7 +881,7 @@ b12g_status b12g_server_release(b12g_server* sv, uint64_t id)
     s.in_use -= std::min(s.in_use, j->reserved);
     s.cv.notify_all();
   }
-  free_job_memory(j.get());
+  free_job_memory(&s, j.get());
   return B12G_OK;
 }
 
@@ -825,6 +905,22 @@ b12g_status b12g_server_stats(b12g_server* sv, uint64_t* ticks, uint64_t* box_im
   return B12G_OK;
 }
 
+b12g_status b12g_server_engine_stats(b12g_server* sv, uint32_t i, uint32_t* map_kind, uint64_t* ticks,
+                                     uint64_t* jobs_done, double* tick_seconds, double* finish_seconds)
+{
+  if (!sv) return fail(B12G_ERR_INVALID, "NULL server");
+  Server& s = sv->s;
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (i >= s.engines.size()) return fail(B12G_ERR_INVALID, "engine %u of %zu", i, s.engines.size());
+  const Engine* e = s.engines[i].get();
+  if (map_kind) *map_kind = e->key.map.kind;
+  if (ticks) *ticks = e->ticks;
+  if (jobs_done) *jobs_done = e->jobs_done;
+  if (tick_seconds) *tick_seconds = e->tick_seconds;
+  if (finish_seconds) *finish_seconds = e->finish_seconds;
+  return B12G_OK;
+}
+
 b12g_status b12g_server_destroy(b12g_server* sv)
 {
   if (!sv) return B12G_OK;
@@ -837,7 +933,12 @@ b12g_status b12g_server_destroy(b12g_server* sv)
   for (auto& e : s.engines)
     if (e->thread.joinable()) e->thread.join();
   for (auto& e : s.engines) engine_release(e.get());
-  for (auto& kv : s.jobs) free_job_memory(kv.second.get());
+  for (auto& kv : s.jobs) free_job_memory(&s, kv.second.get());
+  if (s.release_stream) {
+    cudaStreamSynchronize(s.release_stream);
+    cudaStreamDestroy(s.release_stream);
+  }
+  if (s.pool) cudaMemPoolDestroy(s.pool);
   delete sv;
   return B12G_OK;
 }

@@ -85,6 +85,12 @@ class JobServer:
                                        cols.ctypes.data, vals.ctypes.data), "server_result")
         return dict(codes=codes[:n], counts=counts, rowptr=rowptr[: n + 1], cols=cols[:z], vals=vals[:z])
 
+    def counts(self, jid: int) -> np.ndarray:
+        """Leaf counts after each step of a done job."""
+        counts = np.zeros(self.info(jid)["depth"], dtype=np.uint32)
+        check(lib().b12g_server_result(self._h, jid, None, counts.ctypes.data, None, None, None), "server_result")
+        return counts
+
     def release(self, jid: int) -> None:
         check(lib().b12g_server_release(self._h, jid), "server_release")
 
@@ -95,6 +101,19 @@ class JobServer:
                                       C.byref(r)), "server_stats")
         return dict(ticks=t.value, box_images=b.value, in_use_bytes=u.value, cap_bytes=c.value, waiting=w.value,
                     running=r.value)
+
+    def engine_stats(self) -> list[dict]:
+        """Per engine (family): map kind, ticks, finished jobs, host seconds in ticks and in finishing."""
+        out = []
+        while True:
+            k, t, d = C.c_uint32(), C.c_uint64(), C.c_uint64()
+            ts, fs = C.c_double(), C.c_double()
+            st = lib().b12g_server_engine_stats(self._h, len(out), C.byref(k), C.byref(t), C.byref(d), C.byref(ts),
+                                                C.byref(fs))
+            if st != L.OK:
+                return out
+            out.append(dict(map_kind=k.value, ticks=t.value, jobs_done=d.value, tick_seconds=ts.value,
+                            finish_seconds=fs.value))
 
     def wait_all(self, ids, timeout: float = 600.0) -> list[int]:
         """Block until every job in `ids` has finished (done or failed); returns them in finish order."""
@@ -109,3 +128,58 @@ class JobServer:
                     left.discard(jid)
                     order.append(jid)
         return order
+
+
+def stream_job_args(job: dict):
+    """(center, radius, map, grid, depth) of a served-stream job (b12_b200.workloads.job_stream):
+    Henon and forced Duffing with 4x4 inner grids, Lorenz (explicit FMA integrator) with a
+    5x5x5 inner grid."""
+    from . import tree as T
+    from . import workloads as W
+    fam, p, d = job["family"], job["params"], job["depth"]
+    if fam == "henon":
+        return W.HENON_CENTER, W.HENON_RADIUS, T.henon(p[0], p[1]), T.inner_grid(4), d
+    if fam == "lorenz":
+        return W.LORENZ_CENTER, W.LORENZ_RADIUS, T.lorenz(p[0], p[1], p[2], fma=True), T.inner_grid(5), d
+    if fam == "forced_duffing":
+        return W.FORCED_CENTER, W.FORCED_RADIUS, T.forced_duffing(200, *p), T.inner_grid(4), d
+    raise ValueError(fam)
+
+
+def replay(server: JobServer, stream: list, on_done=None, timeout: float = 3600.0) -> dict:
+    """Submit every job of `stream` at its arrival time (seconds after the start) and wait
+    for all of them.  Returns per-job latency (finish minus scheduled arrival, seconds),
+    the time from the first arrival to the last finish, and the largest submission lag.
+    `on_done(job, jid)` is called for every finished job (e.g. to read and release it)."""
+    n = len(stream)
+    t0 = time.monotonic()
+    ids = {}
+    latency = [0.0] * n
+    lag = 0.0
+    i = 0
+    finished = 0
+    t_first = None
+    t_last = 0.0
+    while finished < n:
+        now = time.monotonic() - t0
+        if now > timeout:
+            raise TimeoutError(f"{n - finished} jobs unfinished")
+        while i < n and stream[i]["arrival"] <= now:
+            jid = server.submit(*stream_job_args(stream[i]))
+            ids[jid] = i
+            lag = max(lag, time.monotonic() - t0 - stream[i]["arrival"])
+            if t_first is None:
+                t_first = stream[i]["arrival"]
+            i += 1
+        wait = min(0.01, stream[i]["arrival"] - now) if i < n else 0.01
+        for jid in server.poll(wait=max(wait, 0.0)):
+            k = ids[jid]
+            inf = server.info(jid)
+            if inf["state"] != L.JOB_DONE:
+                server.result(jid)  # raises with the job's error
+            latency[k] = inf["t_done"] - (t0 + stream[k]["arrival"])
+            t_last = max(t_last, inf["t_done"] - t0)
+            finished += 1
+            if on_done is not None:
+                on_done(stream[k], jid)
+    return dict(latency=latency, span=t_last - (t_first or 0.0), submit_lag=lag)

@@ -339,6 +339,7 @@ def gpu_arm(args, rank: int, world: int, dist):
     main = measure_mode(args, rank, world, dist, fma=not args.strict, peak_tflops=peak_tflops)
     other = None if args.single else measure_mode(args, rank, world, dist, fma=args.strict, peak_tflops=peak_tflops)
     cpu = cpu_baseline(cpu_cores()) if (rank == 0 and world == 1 and not args.no_cpu) else None
+    serving = serve_mode(args) if (rank == 0 and world == 1 and args.serve_jobs > 0) else None
     if rank == 0:
         arith = "strict" if args.strict else "fma"
         line = {"metric": METRIC, "value": main["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -357,8 +358,129 @@ def gpu_arm(args, rank: int, world: int, dist):
                 "roofline_achieved": other["roofline"]["achieved"], "roofline_frac": other["roofline"]["frac"],
                 "transition_rows_tflops": other["roofline"]["transition_rows_tflops"], "phases_ms": other["phases"],
                 "counts_identical": other["counts"] == main["counts"], "clocks": other["clocks"]}
+        if serving is not None:
+            line["serving"] = serving
         print(json.dumps(line), flush=True)
     return 0
+
+
+# ------------------------------------------------------------------------------ serving
+SERVE_RATES = (500.0, 1000.0, 2000.0)
+SERVE_TIMEOUT = 300.0            # seconds per replayed stream before the bench gives up
+SERVE_DIGEST_EVERY = 10          # full-result digests on every 10th job; counts and nnz on all
+SERVE_CAP = 150 * 10**9
+
+
+def _job_digest(codes, counts, rowptr, cols, vals) -> str:
+    import hashlib
+    h = hashlib.sha256()
+    for a in (codes, counts, rowptr, cols, vals):
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
+
+
+def fifo_latencies(arrivals, service):
+    """Latencies of a single server taking jobs one at a time in arrival order."""
+    t, out = 0.0, []
+    for a, s in zip(arrivals, service):
+        t = max(t, a) + s
+        out.append(t - a)
+    return out
+
+
+def _pct(x, q):
+    return float(np.percentile(np.asarray(x), q)) * 1e3
+
+
+def serve_mode(args):
+    """The served stream (Henon / Lorenz / forced Duffing jobs, Poisson arrivals) through the
+    job server against the plain path: one ImplicitBoxTree per job, one job at a time
+    (subdivision_run, then transition_matrix), on the same GPU and the same jobs."""
+    from b12_b200 import tree as T
+    from b12_b200.server import JobServer, replay, stream_job_args
+    from b12_b200.workloads import job_stream
+
+    n = args.serve_jobs
+    base = job_stream(n, 1.0, 0)          # family, parameters, depth of every job (seed 0)
+    fams = [j["family"] for j in base]
+
+    def plain_job(job):
+        c, r, mp, g, d = stream_job_args(job)
+        t = T.ImplicitBoxTree(c, r)
+        sc = T.Scheme(mp, g)
+        counts = t.subdivision_run(sc, d)
+        return t, counts, t.transition_matrix(sc)
+
+    # plain path: warm-up on other jobs, then every job timed on its own
+    for job in job_stream(6, 1.0, 1):
+        t, _, m = plain_job(job)
+        m.close()
+        t.close()
+    service, plain_digest, plain_shape = [], {}, []
+    for k, job in enumerate(base):
+        t0 = time.perf_counter()
+        t, counts, m = plain_job(job)
+        service.append(time.perf_counter() - t0)
+        plain_shape.append((tuple(int(c) for c in counts), int(m.nnz)))
+        if k % SERVE_DIGEST_EVERY == 0:
+            rowptr, cols, vals = m.to_host()
+            plain_digest[k] = _job_digest(t.leaves()[0], np.asarray(counts, np.uint32), rowptr, cols, vals)
+        m.close()
+        t.close()
+    plain_rate = n / sum(service)
+
+    out = {"workload": f"served stream of {n} jobs (seed 0): Henon a~U[1.0,1.4] depth 14-22, Lorenz "
+                       "rho~U[15,35] depth 18-27, forced Duffing depth 16-22, uniform family mix",
+           "jobs": n, "hbm_cap_bytes": SERVE_CAP,
+           "plain": {"jobs_per_s": plain_rate, "service_ms_mean": 1e3 * sum(service) / n,
+                     "per_family_ms": {f: 1e3 * float(np.mean([s for s, g in zip(service, fams) if g == f]))
+                                       for f in sorted(set(fams))}}}
+    with JobServer(SERVE_CAP) as srv:
+        # warm-up on a burst of other jobs: engines created, buffers and the result pool grown
+        warm = [dict(j, arrival=0.0) for j in job_stream(min(n, 1000), 1.0, 1)]
+        replay(srv, warm, lambda job, jid: srv.release(jid), timeout=SERVE_TIMEOUT)
+        # saturated: every job submitted at once; each result checked against the plain path
+        # and released as it arrives (a resident result counts against the admission cap)
+        sat = [dict(j, arrival=0.0) for j in base]
+        check = {"shape": 0, "digest": 0}
+
+        def check_and_release(job, jid):
+            k = job["id"]
+            inf = srv.info(jid)
+            if k in plain_digest:
+                r = srv.result(jid)
+                check["digest"] += _job_digest(r["codes"], r["counts"], r["rowptr"], r["cols"],
+                                               r["vals"]) == plain_digest[k]
+                counts = r["counts"]
+            else:
+                counts = srv.counts(jid)
+            check["shape"] += (tuple(int(c) for c in counts), int(inf["nnz"])) == plain_shape[k]
+            srv.release(jid)
+
+        res = replay(srv, sat, check_and_release, timeout=SERVE_TIMEOUT)
+        same_shape, same = check["shape"], check["digest"]
+        out["served_saturated"] = {"jobs_per_s": n / res["span"], "span_s": res["span"],
+                                   "p50_ms": _pct(res["latency"], 50), "p99_ms": _pct(res["latency"], 99)}
+        out["identical_to_plain"] = {"step_counts_and_nnz": f"{same_shape}/{n}",
+                                     "full_result_sha256": f"{same}/{len(plain_digest)}"}
+        out["jobs_per_s_vs_plain"] = (n / res["span"]) / plain_rate
+        sweep = []
+        for rate in SERVE_RATES:
+            st = job_stream(n, rate, 0)
+            res = replay(srv, st, lambda job, jid: srv.release(jid), timeout=SERVE_TIMEOUT)
+            arr = [j["arrival"] for j in st]
+            pl = fifo_latencies(arr, service)
+            plain_span = max(a + x for a, x in zip(arr, pl)) - arr[0]
+            sweep.append({"offered_jobs_per_s": rate,
+                          "served": {"jobs_per_s": n / res["span"],
+                                     "p50_ms": _pct(res["latency"], 50), "p99_ms": _pct(res["latency"], 99),
+                                     "submit_lag_ms": 1e3 * res["submit_lag"]},
+                          "plain": {"jobs_per_s": n / plain_span, "p50_ms": _pct(pl, 50), "p99_ms": _pct(pl, 99)}})
+        out["rate_sweep"] = sweep
+        out["ticks"] = srv.stats()["ticks"]
+    out["latency"] = ("finish minus scheduled arrival; plain-path latencies are its measured per-job times "
+                      "queued first come, first served at the same arrivals")
+    return out
 
 
 def lib_leaves(tree, codes, depth, flags):
@@ -376,6 +498,8 @@ def main():
                     help="headline with the strict (one rounding per operation) integrator instead of explicit FMA")
     ap.add_argument("--single", action="store_true", help="measure only the headline arithmetic")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--serve-jobs", type=int, default=10000,
+                    help="jobs of the served stream measured against the plain path at 1 GPU (0: skip)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

@@ -253,7 +253,9 @@ b12g_status b12g_batch_stream(b12g_batch* batch, void** stream);
  * sequence; a job submitted while others run joins at the next tick, and leaves at the
  * end of its last step with its leaves and CSR resident on the device until released.
  * Families run concurrently.  Admission is by projected HBM footprint against the
- * server's cap (first come, first served within a family).  Inner and full grids with up
+ * server's cap (first come, first served within a family); a job's reservation lasts
+ * until its result is released, so a client that holds results while waiting for later
+ * jobs can stall admission once the cap is reached.  Inner and full grids with up
  * to 128 points per box. */
 typedef struct b12g_server b12g_server;
 typedef struct {
@@ -288,6 +290,10 @@ b12g_status b12g_server_result(b12g_server* server, uint64_t id, uint64_t* codes
 b12g_status b12g_server_release(b12g_server* server, uint64_t id);
 b12g_status b12g_server_stats(b12g_server* server, uint64_t* ticks, uint64_t* box_images, uint64_t* in_use_bytes,
                               uint64_t* cap_bytes, uint32_t* waiting, uint32_t* running);
+/* engine i (in order of creation): its map kind, ticks, finished jobs, and host seconds
+ * spent in ticks (finishing included) and in finishing jobs; B12G_ERR_INVALID past the last */
+b12g_status b12g_server_engine_stats(b12g_server* server, uint32_t i, uint32_t* map_kind, uint64_t* ticks,
+                                     uint64_t* jobs_done, double* tick_seconds, double* finish_seconds);
 
 /* ---- measurement hooks (no counterpart in the reference) ---------------------------------- */
 /* the CUDA stream (cudaStream_t) every kernel of this tree runs on */

@@ -89,3 +89,28 @@ def test_henon_batch_matches_single_trees():
         np.testing.assert_array_equal(b.leaves(i)[0], leaves[0])
         for x, y in zip(b.csr(i), csr):
             np.testing.assert_array_equal(x, y)
+
+
+def test_forced_duffing_batch_matches_single_trees_and_reference(golden):
+    # the two-dimensional maps run several points per thread, interleaved: every point's
+    # operations stay those of the single-point integrator
+    from b12_b200.workloads import FORCED_CENTER, FORCED_RADIUS
+    meta = golden("forced_duffing_d16")[0]
+    params = [(0.25, -1.0, 1.0, 0.3), (0.2, -1.0, 1.0, 0.3), (0.25, -1.0, 1.0, 0.35), (0.3, -1.0, 1.0, 0.25)]
+    depths = [len(meta["steps"]), 12, 14, 11]
+    grid = B.inner_grid(4)
+    b = B.Batch(FORCED_CENTER, FORCED_RADIUS, B.Scheme(B.forced_duffing(), grid), params, depths)
+    b.run()
+    b.transition_matrices()
+    assert list(b.counts(0)) == [s["n"] for s in meta["steps"]]
+    codes, _, flags = b.leaves(0)
+    assert sha(codes) == meta["steps"][-1]["codes_sha256"] and sha(flags) == meta["steps"][-1]["flags_sha256"]
+    d = csr_digests(*b.csr(0))
+    for k in ("nnz", "rowptr_sha256", "cols_sha256", "vals_sha256"):
+        assert d[k] == meta["tm"][k], k
+    for i in range(1, 4):
+        counts, leaves, csr = single(FORCED_CENTER, FORCED_RADIUS, B.forced_duffing(200, *params[i]), grid, depths[i])
+        np.testing.assert_array_equal(b.counts(i), counts)
+        np.testing.assert_array_equal(b.leaves(i)[0], leaves[0])
+        for x, y in zip(b.csr(i), csr):
+            np.testing.assert_array_equal(x, y)
