@@ -207,6 +207,7 @@ def measure_mode(args, rank, world, dist, fma: bool, peak_tflops: float):
     import torch
     import b12_b200 as B
     from b12_b200 import tree as T
+    from b12_b200.ranks import throughput
 
     dev = torch.cuda.current_device()
     sc = B.Scheme(B.lorenz(rho=28.0, fma=fma), B.inner_grid(5))
@@ -270,11 +271,9 @@ def measure_mode(args, rank, world, dist, fma: bool, peak_tflops: float):
     img_ms, img_n = tree.profile_read(0)
     row_ms, row_n = tree.profile_read(1)
     tree.profile(False)
-    if dist:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * args.steps * box_images / (total_ms * 1e-3)
+    # all ranks' box-images over the slowest rank's device time
+    value, _, slowest_s = throughput(dist, args.steps * box_images, total_ms * 1e-3, dev)
+    total_ms = 1e3 * slowest_s
     flops_img = args.steps * bi_sub * P * FLOP_PER_POINT
     achieved = flops_img / (img_ms * 1e-3) / 1e12 if img_ms > 0 else None
     flops_rows = args.steps * n_final * P * FLOP_PER_POINT
@@ -306,11 +305,8 @@ def measure_mode(args, rank, world, dist, fma: bool, peak_tflops: float):
         csr.to_host_into(rowptr, cols, vals)
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = {"value": world * e2e_steps * box_images / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
+    e2e_value, _, e2e_s = throughput(dist, e2e_steps * box_images, e2e_s, dev)
+    e2e = {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": int(d2h), "steps": e2e_steps, "timer": "host wall clock, synchronous API"}
     roofline = {"bound": "fp64", "kernel": "image_points_kernel (fused sample/RK4/locate)", "achieved": achieved,
                 "peak": peak_tflops, "unit": "TFLOP/s", "frac": (achieved / peak_tflops) if achieved else None,
