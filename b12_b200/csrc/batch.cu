@@ -115,13 +115,14 @@ template<> struct Multi<ForcedDuffingMap> {
 template<class Map, class Grid, int W>
 struct BatchPoint {
   static constexpr int D = Map::D;
-  // W points: child[w], k[w]; returns their children-level targets (global child index)
+  // W points: child[w], k[w]; returns their children-level targets (global child index,
+  // kInvalidIndex when the image box is no child of a leaf, kOutsideIndex when the image
+  // left the domain) and their instances
   static __device__ __forceinline__ void run(const BatchArgs& a, const uint32_t* off_s, const double* pts,
                                              const uint64_t (&child)[W], const uint32_t (&k)[W],
-                                             const bool (&act)[W], uint32_t (&target)[W])
+                                             const bool (&act)[W], uint32_t (&target)[W], uint32_t (&inst)[W])
   {
     double x[W][D], y[W][D];
-    uint32_t inst[W];
     int dep[W];
     MapParams mp[W];
 #pragma unroll
@@ -157,11 +158,11 @@ struct BatchPoint {
 #pragma unroll
     for (int w = 0; w < W; ++w) {
       uint64_t tcode = 0;
-      const bool valid = act[w] && point_code<D>(a.dom, y[w], dep[w], tcode);
-      uint32_t t = kInvalidIndex;
-      if (valid) {
+      const bool inside = act[w] && point_code<D>(a.dom, y[w], dep[w], tcode);
+      uint32_t t = act[w] ? kOutsideIndex : kInvalidIndex;
+      if (inside) {
         const uint32_t p = hash_locate(a.hash, off_s[a.n_inst], inst_key(inst[w], tcode >> 1));
-        if (p != kInvalidIndex) t = 2u * p + uint32_t(tcode & 1u);
+        t = p != kInvalidIndex ? 2u * p + uint32_t(tcode & 1u) : kInvalidIndex;
       }
       target[w] = t;
     }
@@ -206,11 +207,22 @@ __global__ void __launch_bounds__(512) batch_image_kernel(const BatchArgs a)
         child[w] = act[w] ? g / P : 0;
         k[w] = act[w] ? uint32_t(g - child[w] * P) : 0u;
       }
-      BatchPoint<Map, Grid, W>::run(a, off_s, pts, child, k, act, target);
+      uint32_t inst[W];
+      BatchPoint<Map, Grid, W>::run(a, off_s, pts, child, k, act, target, inst);
 #pragma unroll
       for (int w = 0; w < W; ++w) {
         const unsigned peers = __match_any_sync(0xFFFFFFFFu, target[w]);
-        if (act[w] && target[w] != kInvalidIndex && lane == __ffs(peers) - 1) a.hit[target[w]] = 1;
+        if (act[w] && target[w] < kOutsideIndex && lane == __ffs(peers) - 1) a.hit[target[w]] = 1;
+      }
+      if (a.targets) {
+        // the instances finishing in this step keep every point's target for their
+        // transition matrix
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+          if (!act[w]) continue;
+          const uint64_t tb = a.tgt_base[inst[w]];
+          if (tb != ~0ull) a.targets[tb + (child[w] - 2ull * off_s[inst[w]]) * P + k[w]] = target[w];
+        }
       }
     }
   }
@@ -332,6 +344,8 @@ __global__ void __launch_bounds__(256) batch_rows_kernel(const BatchRowArgs a)
         if (point_code<D>(a.dom, y, depth, tcode)) {
           const uint32_t g = hash_locate(a.hash, nrows, inst_key(inst, tcode));
           if (g != kInvalidIndex) t = g - off_s[inst];
+        } else if (a.codes[off_s[inst] + n_i - 1] == 0) {
+          t = n_i - 1;   // a point outside the domain is found in a last leaf of code 0
         }
         key = t == kInvalidIndex ? kLostKey : t;
       }
@@ -340,6 +354,49 @@ __global__ void __launch_bounds__(256) batch_rows_kernel(const BatchRowArgs a)
     const uint32_t total = row_emit(s, bounds[w], lane, P, a.keep_lost, n_i + 1, a.stage_col + size_t(row) * P,
                                     a.stage_cnt + size_t(row) * P);
     if (lane == 0) a.row_count[row] = total;
+    __syncwarp();
+  }
+}
+
+// transition rows from stored targets: a warp per child of a finishing instance; the
+// child is a row when it survived (its rank advances), a target is a column when its
+// child survived, and its column is its rank within the instance
+__global__ void __launch_bounds__(256) target_rows_kernel(const TargetRowArgs a)
+{
+  __shared__ uint32_t off_s[kMaxInstances + 1];
+  __shared__ uint32_t keys[8][128];
+  __shared__ uint32_t bounds[8][4];
+  for (uint32_t i = threadIdx.x; i <= a.n_inst; i += blockDim.x) off_s[i] = a.child_off[i];
+  __syncthreads();
+  const uint32_t total = off_s[a.n_inst];
+  const uint32_t P = a.points;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  uint32_t* s = keys[w];
+  for (uint32_t j = blockIdx.x * 8 + w; j < total; j += gridDim.x * 8) {
+    const uint32_t q = find_instance(off_s, a.n_inst, j);
+    const uint32_t cb = a.child_base[q];
+    const uint32_t c = cb + (j - off_s[q]);
+    const uint32_t r0 = a.rank[cb];
+    const uint32_t rc = a.rank[c];
+    if (a.rank[c + 1] == rc) continue;            // not a survivor: no row (warp-uniform)
+    const uint32_t n_i = a.rank[cb + (off_s[q + 1] - off_s[q])] - r0;
+    const uint32_t row = a.row_off[q] + (rc - r0);
+    // a point outside the domain is found in a last leaf of code 0
+    const bool zero_leaf = a.arena[a.row_off[q] + n_i - 1] == 0;
+#pragma unroll 1
+    for (int u = 0; u < 4; ++u) {
+      const uint32_t k = uint32_t(lane) + 32u * u;
+      uint32_t key = kPadKey;
+      if (k < P) {
+        const uint32_t t = a.targets[size_t(j) * P + k];
+        if (t < kOutsideIndex) key = a.rank[t + 1] != a.rank[t] ? a.rank[t] - r0 : kLostKey;
+        else key = (t == kOutsideIndex && zero_leaf) ? n_i - 1 : kLostKey;
+      }
+      s[lane + 32 * u] = key;
+    }
+    const uint32_t cnt = row_emit(s, bounds[w], lane, P, a.keep_lost, n_i + 1, a.stage_col + size_t(row) * P,
+                                  a.stage_cnt + size_t(row) * P);
+    if (lane == 0) a.row_count[row] = cnt;
     __syncwarp();
   }
 }
@@ -412,6 +469,15 @@ cudaError_t launch_batch_rows(uint32_t map_kind, uint32_t arith, uint32_t grid_k
     batch_rows_kernel<Map, Grid><<<g, 256, 0, s>>>(a);
     return cudaGetLastError();
   });
+}
+
+cudaError_t launch_target_rows(const TargetRowArgs& a, uint32_t max_children, cudaStream_t s)
+{
+  if (max_children == 0) return cudaSuccess;
+  const int g = std::max(1, std::min<int>(batch_grid((const void*)target_rows_kernel, 256),
+                                          int((uint64_t(max_children) + 7) / 8)));
+  target_rows_kernel<<<g, 256, 0, s>>>(a);
+  return cudaGetLastError();
 }
 
 bool batch_supported(uint32_t map_kind, uint32_t arith, uint32_t grid_kind)

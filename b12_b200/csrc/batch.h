@@ -35,6 +35,28 @@ struct BatchArgs {
   uint32_t* queue;                  // work-queue head (zeroed before the launch)
   uint32_t chunk;
   uint32_t* error;
+  // optional: every point's target (global child index, kInvalidIndex when its box is
+  // not a child of a leaf, kOutsideIndex when it left the domain) for the instances with
+  // tgt_base[i] != ~0: targets[tgt_base[i] + (child - 2 off[i]) * points + k]
+  uint32_t* targets;
+  const uint64_t* tgt_base;
+};
+
+// transition rows of the instances finishing in a step, from the targets their last
+// step stored and the ranks of that step's compaction (no map evaluation)
+struct TargetRowArgs {
+  uint32_t n_inst;                  // finishing instances
+  const uint32_t* child_off;        // n_inst + 1: prefix of their children counts
+  const uint32_t* child_base;       // n_inst: global index of each one's first child
+  const uint32_t* row_off;          // n_inst: each one's first row (arena position)
+  const uint32_t* rank;             // the step's compaction ranks (children + 1 entries)
+  const uint32_t* targets;          // child_off[n_inst] x points
+  const uint64_t* arena;            // final leaves (for the single-leaf rule)
+  uint32_t points;
+  int keep_lost;
+  uint32_t* stage_col;
+  uint32_t* stage_cnt;
+  uint32_t* row_count;
 };
 
 // transition rows of the finished leaves of all instances: warp per row, targets found
@@ -70,6 +92,7 @@ cudaError_t launch_batch_rows(uint32_t map_kind, uint32_t arith, uint32_t grid_k
 // lookup table over (instance, code) of n_inst concatenated code segments
 cudaError_t launch_batch_hash(const uint64_t* codes, const uint32_t* off, uint32_t n_inst, LeafHash h,
                               uint32_t code_cap, uint32_t* error, cudaStream_t s);
+cudaError_t launch_target_rows(const TargetRowArgs& a, uint32_t max_children, cudaStream_t s);
 // survivors per instance from the hit mask of the instances' (implicit) children
 cudaError_t launch_inst_count(const uint8_t* hit, const uint32_t* off, uint32_t n_inst, uint32_t* cnt,
                               uint64_t hit_cap, uint32_t* error, cudaStream_t s);

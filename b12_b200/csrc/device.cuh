@@ -14,6 +14,7 @@
 namespace b12g {
 
 constexpr uint32_t kInvalidIndex = 0xFFFFFFFFu;
+constexpr uint32_t kOutsideIndex = 0xFFFFFFFEu;   // stored image target: point left the domain
 constexpr uint64_t kInvalidCode = ~uint64_t(0);
 
 // ---------------------------------------------------------------------------------

@@ -104,6 +104,7 @@ struct CompactArgs {
   uint32_t* out_index;       // non-null: write the kept indices instead of code/flags
   uint32_t* n_out;
   uint32_t* n_out2;          // optional second copy of the new count
+  uint32_t* out_rank;        // optional: out_rank[i] = kept elements before input i (n + 1 entries)
   uint32_t out_cap;
   uint32_t* error;
 };

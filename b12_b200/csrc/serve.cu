@@ -115,11 +115,15 @@ struct Engine {
   Buf<uint64_t> arena;               // finished jobs' leaves, contiguous
   Buf<uint32_t> stage_col, stage_cnt, row_count, rowptr, cols_all;
   Buf<double> vals_all;
+  // the finishing jobs' last-step image targets and that step's compaction ranks
+  Buf<uint32_t> targets, rank, fin_child;       // fin_child: child offsets (nf + 1), child bases (nf)
+  Buf<uint64_t> tgt_base;                        // per slot: targets offset, ~0 when not finishing
   double* table = nullptr;           // forcing table (forced Duffing)
   // pinned host mirrors
   uint32_t* h = nullptr;             // counts, counters, ranks
   double* hp = nullptr;              // parameters
   uint8_t* hd = nullptr;             // depths and finishing marks
+  uint64_t* ht = nullptr;            // targets offsets
   uint64_t boxes = 0;                // parents after the last tick
   // counters written by the engine thread
   std::atomic<uint64_t> ticks{0}, jobs_done{0};
@@ -159,7 +163,9 @@ constexpr size_t kHostCounts = 0;                    // A counts
 constexpr size_t kHostCtr = 2 * kMaxSlots;           // E_COUNT counters
 constexpr size_t kHostRank = 3 * kMaxSlots;          // A finish ranks
 constexpr size_t kHostScratch = 5 * kMaxSlots;       // finish bookkeeping (2 x (kMaxSlots + 1))
-constexpr size_t kHostWords = 8 * kMaxSlots;
+constexpr size_t kHostFinChildren = 8 * kMaxSlots;  // finishing jobs' children this tick
+constexpr size_t kHostFinStage = 9 * kMaxSlots;     // their child offsets and bases (2 nf + 1)
+constexpr size_t kHostWords = 11 * kMaxSlots + 16;
 
 // ---------------------------------------------------------------------------- kernels
 // append n_new surrounding boxes (code 0, flags SD) after the A current slots
@@ -341,6 +347,9 @@ b12g_status engine_init(Engine* e, const b12g_job& key)
   CK(cudaMallocHost(&e->h, kHostWords * 4));
   CK(cudaMallocHost(&e->hp, size_t(kMaxSlots) * 6 * 8));
   CK(cudaMallocHost(&e->hd, 2 * size_t(kMaxSlots)));
+  CK(cudaMallocHost(&e->ht, size_t(kMaxSlots) * 8));
+  ST(e->tgt_base.ensure(kMaxSlots, "engine targets offsets"));
+  ST(e->fin_child.ensure(2 * kMaxSlots + 1, "engine finishing children"));
   ST(e->off.ensure(kMaxSlots + 1, "engine offsets"));
   ST(e->new_off.ensure(kMaxSlots + 1, "engine offsets"));
   ST(e->keep_off.ensure(kMaxSlots + 1, "engine offsets"));
@@ -423,7 +432,8 @@ void fail_job_locked(Server* s, Job* j, const std::string& why)
 }
 
 // the finished slots of this tick: transition matrices and resident results
-b12g_status engine_finish(Engine* e, const std::vector<uint32_t>& fin, uint32_t rows)
+// stored: the tick kept the finishing jobs' image targets and compaction ranks
+b12g_status engine_finish(Engine* e, const std::vector<uint32_t>& fin, uint32_t rows, bool stored)
 {
   Server* s = e->srv;
   const double t_begin = now_s();
@@ -436,15 +446,34 @@ b12g_status engine_finish(Engine* e, const std::vector<uint32_t>& fin, uint32_t 
     e->hd[q] = uint8_t(j->spec.depth);
     e->h[kHostScratch + q] = q;
   }
-  CK(cudaMemcpyAsync(e->fin_params.p, e->hp, size_t(nf) * 6 * 8, cudaMemcpyHostToDevice, e->stream));
-  CK(cudaMemcpyAsync(e->fin_depth.p, e->hd, nf, cudaMemcpyHostToDevice, e->stream));
-  CK(cudaMemcpyAsync(e->fin_slot.p, e->h + kHostScratch, nf * 4, cudaMemcpyHostToDevice, e->stream));
+  if (!stored) {
+    CK(cudaMemcpyAsync(e->fin_params.p, e->hp, size_t(nf) * 6 * 8, cudaMemcpyHostToDevice, e->stream));
+    CK(cudaMemcpyAsync(e->fin_depth.p, e->hd, nf, cudaMemcpyHostToDevice, e->stream));
+    CK(cudaMemcpyAsync(e->fin_slot.p, e->h + kHostScratch, nf * 4, cudaMemcpyHostToDevice, e->stream));
+  }
   const uint64_t stage = std::max<uint64_t>(uint64_t(rows) * e->P, 1);
   ST(e->stage_col.ensure(grow(e->stage_col.n, stage), "row staging"));
   ST(e->stage_cnt.ensure(grow(e->stage_cnt.n, stage), "row staging"));
   ST(e->row_count.ensure(rows + 1, "row counts"));
   ST(e->rowptr.ensure(rows + 1, "row pointers"));
   ST(e->tiles_a.ensure(compact_tiles(rows + 1) + 2, "tiles"));
+  if (stored) {
+    // rows from the targets the last step kept: no map evaluation
+    TargetRowArgs ta{};
+    ta.n_inst = nf;
+    ta.child_off = e->fin_child.p;
+    ta.child_base = e->fin_child.p + (nf + 1);
+    ta.row_off = e->fin_off.p;
+    ta.rank = e->rank.p;
+    ta.targets = e->targets.p;
+    ta.arena = e->arena.p;
+    ta.points = uint32_t(e->P);
+    ta.keep_lost = 0;
+    ta.stage_col = e->stage_col.p;
+    ta.stage_cnt = e->stage_cnt.p;
+    ta.row_count = e->row_count.p;
+    CK(launch_target_rows(ta, e->h[kHostFinChildren], e->stream));
+  } else {
   // lookup over the finished leaves keyed by (finish rank, code)
   ST(engine_hash_capacity(e, rows));
   uint32_t tag = 0;
@@ -469,6 +498,7 @@ b12g_status engine_finish(Engine* e, const std::vector<uint32_t>& fin, uint32_t 
   ra.stage_cnt = e->stage_cnt.p;
   ra.row_count = e->row_count.p;
   CK(launch_batch_rows(e->key.map.kind, e->key.map.arith, e->key.grid.kind, ra, rows, e->stream));
+  }
   CK(exclusive_scan_u32(e->row_count.p, e->rowptr.p, e->fin_off.p + nf, e->tiles_a.p, rows, e->stream));
   uint32_t* h_nnz = e->h + kHostScratch;
   CK(cudaMemcpyAsync(h_nnz, e->rowptr.p + rows, 4, cudaMemcpyDeviceToHost, e->stream));
@@ -479,7 +509,7 @@ b12g_status engine_finish(Engine* e, const std::vector<uint32_t>& fin, uint32_t 
   CK(gather_rows(e->stage_col.p, e->stage_cnt.p, uint32_t(e->P), e->row_count.p, e->rowptr.p, e->fin_off.p + nf,
                  e->cols_all.p, e->vals_all.p, 0, double(e->P), rows, e->stream));
   row_starts_kernel<<<(nf + 256) / 256, 256, 0, e->stream>>>(e->rowptr.p, e->fin_off.p, nf, e->row0.p);
-  count_launches(7);
+  count_launches(stored ? 6 : 7);
   // per finished job: its first row and first nonzero
   uint32_t* h_foff = e->h + kHostScratch;
   uint32_t* h_e0 = e->h + kHostScratch + (kMaxSlots + 1);
@@ -568,6 +598,43 @@ b12g_status engine_tick(Engine* e, const std::vector<Job*>& joining)
   CK(cudaMemcpyAsync(e->depth_child.p, e->hd, A, cudaMemcpyHostToDevice, e->stream));
   CK(cudaMemcpyAsync(e->depth_child.p + kMaxSlots, e->hd + kMaxSlots, A, cudaMemcpyHostToDevice, e->stream));
   CK(cudaMemcpyAsync(e->fin_rank.p, e->h + kHostRank, size_t(A) * 4, cudaMemcpyHostToDevice, e->stream));
+  // the finishing jobs keep every image target of this step and the compaction's ranks,
+  // from which their transition matrices follow without evaluating the map again.
+  // Slot i's children start at twice the parents of the slots before it.
+  const uint32_t nf = uint32_t(fin.size());
+  bool store = nf > 0;
+  uint64_t fin_children = 0;
+  if (store) {
+    uint32_t* child_off = e->h + kHostFinStage;
+    uint32_t* child_base = child_off + (nf + 1);
+    uint64_t before = 0;
+    uint32_t q = 0;
+    for (uint32_t i = 0; i < A; ++i) {
+      const Job* j = e->slots[i];
+      const uint64_t p = j->counts.empty() ? 1u : j->counts.back();
+      if (e->hd[kMaxSlots + i]) {
+        child_off[q] = uint32_t(fin_children);
+        child_base[q] = uint32_t(2 * before);
+        e->ht[i] = fin_children * e->P;
+        fin_children += 2 * p;
+        ++q;
+      } else {
+        e->ht[i] = ~0ull;
+      }
+      before += p;
+    }
+    child_off[nf] = uint32_t(fin_children);
+    // the host's view of the layout must be the device's; else recompute the rows
+    store = before == parents && fin_children < 0x7FFFFFFFull &&
+            e->targets.ensure(grow(e->targets.n, std::max<uint64_t>(fin_children * e->P, 1)), "targets") ==
+                B12G_OK &&
+            e->rank.ensure(grow(e->rank.n, 2 * parents + 1), "ranks") == B12G_OK;
+    if (store) {
+      CK(cudaMemcpyAsync(e->tgt_base.p, e->ht, size_t(A) * 8, cudaMemcpyHostToDevice, e->stream));
+      CK(cudaMemcpyAsync(e->fin_child.p, child_off, size_t(2 * nf + 1) * 4, cudaMemcpyHostToDevice, e->stream));
+    }
+  }
+  e->h[kHostFinChildren] = uint32_t(fin_children);
   const uint32_t capu = uint32_t(std::min<size_t>(e->parents.n, 0xFFFFFFFFu));
   // 1. lookup table over (slot, parent code)
   uint32_t tag = 0;
@@ -592,6 +659,8 @@ b12g_status engine_tick(Engine* e, const std::vector<Job*>& joining)
   a.queue = e->ctr.p + E_QUEUE;
   a.chunk = e->tuning.chunk;
   a.error = e->ctr.p + E_ERROR;
+  a.targets = store ? e->targets.p : nullptr;
+  a.tgt_base = store ? e->tgt_base.p : nullptr;
   CK(launch_batch_image(e->key.map.kind, e->key.map.arith, e->key.grid.kind, e->tuning, a, e->stream));
   // 3. survivors per job, then one ordered compaction of all children
   CK(launch_inst_count(e->hit.p, e->off.p, A, e->cnt.p, e->hit.n, e->ctr.p + E_ERROR, e->stream));
@@ -607,6 +676,7 @@ b12g_status engine_tick(Engine* e, const std::vector<Job*>& joining)
   ca.n_out = e->ctr.p + E_TOTAL;
   ca.out_cap = uint32_t(std::min<size_t>(e->children.n, 0xFFFFFFFFu));
   ca.error = e->ctr.p + E_ERROR;
+  ca.out_rank = store ? e->rank.p : nullptr;
   CK(compact(ca, {e->tiles_a.p, e->tiles_b.p}, uint32_t(parents), e->stream));
   // 4. continuing jobs packed back into the parents, finished ones into the arena
   split_offsets_kernel<<<1, kSplitThreads, 0, e->stream>>>(e->cnt.p, e->depth_child.p + kMaxSlots, A, e->new_off.p,
@@ -634,7 +704,7 @@ b12g_status engine_tick(Engine* e, const std::vector<Job*>& joining)
     if (!e->hd[kMaxSlots + i]) rest.push_back(j);
   }
   s->box_images += images;
-  ST(engine_finish(e, fin, fin_total));
+  ST(engine_finish(e, fin, fin_total, store));
   e->slots.swap(rest);
   e->boxes = keep_total;
   s->ticks += 1;
@@ -707,6 +777,8 @@ void engine_release(Engine* e)
   if (e->h) cudaFreeHost(e->h);
   if (e->hp) cudaFreeHost(e->hp);
   if (e->hd) cudaFreeHost(e->hd);
+  if (e->ht) cudaFreeHost(e->ht);
+  e->targets.release(); e->rank.release(); e->fin_child.release(); e->tgt_base.release();
   e->parents.release(); e->children.release(); e->flags_a.release(); e->flags_b.release(); e->hit.release();
   e->off.release(); e->new_off.release(); e->cnt.release(); e->ctr.release(); e->tiles_a.release();
   e->tiles_b.release(); e->keep_off.release(); e->fin_off.release(); e->fin_slot.release(); e->fin_rank.release();

@@ -215,6 +215,7 @@ __global__ void compact_scan_kernel(const CompactArgs a, const uint32_t* tile_co
   if (threadIdx.x == 0) {
     if (carry > a.out_cap || (a.children && 2ull * *a.n > a.hit_cap)) atomicOr(a.error, 1u);
     if (carry > a.out_cap) carry = a.out_cap;
+    if (a.out_rank) a.out_rank[n] = carry;
     *a.n_out = carry;
     if (a.n_out2) *a.n_out2 = carry;
   }
@@ -246,6 +247,7 @@ __global__ void compact_scatter_kernel(const CompactArgs a, const uint32_t* tile
           }
         }
       }
+      if (a.out_rank && i < n) a.out_rank[i] = off + ex;
       if (a.children && i < n) a.hit[i] = 0;
       off += total;
     }
