@@ -1,0 +1,120 @@
+"""Single workloads sized for an ncu capture of one kernel family on one GPU.
+
+    python -m b12_b200.profile_cases <case> [options]
+
+image     a Lorenz tree subdivided to --depth - 1 (default 23), then one subdivide and
+          one set_flags_by_image with the strict and one with the explicit-FMA integrator:
+          two launches of the fused box-image kernel over the same 2n boxes.
+compact   64 Lorenz instances (rho = 28, explicit FMA) batched to depth 27: the last
+          steps compact ~20 M children (code 8 B + flags 1 B + hit 1 B each), well
+          beyond the 126 MB L2, so the compaction's DRAM traffic is meaningful.
+sort      the coupled-Duffing continuation at depth 24 (64 Philox points per box):
+          each sweep radix-sorts 64 candidate codes per expanded box.
+measure   one Lorenz job to --depth (default 27), its transition matrix and 200 power
+          iterations; depth 32 gives ~2.6 M boxes, a matrix of ~0.25 GB (HBM-bound SpMV).
+serve     a burst of --jobs served-stream jobs through the job server.
+
+Every case prints one line of sizes; none writes files.
+"""
+from __future__ import annotations
+
+import argparse
+import time
+
+import numpy as np
+
+
+def case_image(args):
+    import b12_b200 as B
+    from b12_b200.workloads import LORENZ_CENTER, LORENZ_RADIUS
+    t = B.ImplicitBoxTree(LORENZ_CENTER, LORENZ_RADIUS)
+    strict = B.Scheme(B.lorenz(), B.inner_grid(5))
+    fma = B.Scheme(B.lorenz(fma=True), B.inner_grid(5))
+    t.subdivision_run(strict, args.depth - 1)
+    t.subdivide(B.SD)
+    n = t.count()
+    a = t.set_flags_by_image(strict, B.HIT)
+    t.unset_flags(B.HIT)
+    b = t.set_flags_by_image(fma, B.HIT)
+    print(f"image: {n} boxes at depth {args.depth}, {n * 125} points per launch, hits {a} / {b}")
+    t.close()
+
+
+def case_compact(args):
+    import b12_b200 as B
+    from b12_b200.workloads import LORENZ_CENTER, LORENZ_RADIUS
+    n = args.instances
+    b = B.Batch(LORENZ_CENTER, LORENZ_RADIUS, B.Scheme(B.lorenz(fma=True), B.inner_grid(5)),
+                [(10.0, 28.0, 8.0 / 3.0)] * n, [args.depth] * n)
+    b.run()                       # first run: autotunes the launch shape
+    # the second run (one CUDA graph, 27 steps) inside a profiler range: capture it with
+    # ncu --profile-from-start off
+    import torch
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    t0 = time.perf_counter()
+    b.run()
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    info = b.info()
+    print(f"compact: {n} instances depth {args.depth}: {info['final_boxes']} final boxes, "
+          f"{info['box_images']} box-images, {time.perf_counter() - t0:.3f} s (second run)")
+    b.close()
+
+
+def case_sort(args):
+    import b12_b200 as B
+    t = B.ImplicitBoxTree((0.0,) * 4, (2.0,) * 4)
+    t.reserve(16 << 20)
+    sc = B.Scheme(B.coupled_duffing(), B.philox_grid(64, 0))
+    t0 = time.perf_counter()
+    sweeps = t.continuation_run(sc, np.zeros(4), args.depth)
+    # sweep s sorts 64 candidates per box inserted by sweep s - 1
+    grown = np.diff(np.concatenate([[0, 1], sweeps.astype(np.int64)]))[:-1]
+    big = int(np.argmax(grown))
+    print(f"sort: continuation depth {args.depth}: {int(sweeps[-1])} boxes in {len(sweeps)} sweeps, "
+          f"{time.perf_counter() - t0:.3f} s; largest sort: sweep {big} ({64 * int(grown[big])} candidates)")
+    t.close()
+
+
+def case_measure(args):
+    import b12_b200 as B
+    from b12_b200.workloads import LORENZ_CENTER, LORENZ_RADIUS
+    t = B.ImplicitBoxTree(LORENZ_CENTER, LORENZ_RADIUS)
+    sc = B.Scheme(B.lorenz(fma=True), B.inner_grid(5))
+    counts = t.subdivision_run(sc, args.depth)
+    m = t.transition_matrix(sc)
+    t.close()                     # the matrix owns its memory; only it stays on the device
+    t0 = time.perf_counter()
+    v = m.invariant_measure(200)
+    print(f"measure: depth {args.depth}: {int(counts[-1])} boxes, {m.nnz} nonzeros, sum {v.sum():.15f}, "
+          f"{1e3 * (time.perf_counter() - t0):.2f} ms")
+    m.close()
+
+
+def case_serve(args):
+    from b12_b200.server import JobServer, replay
+    from b12_b200.workloads import job_stream
+    with JobServer(150 * 10**9) as srv:
+        warm = [dict(j, arrival=0.0) for j in job_stream(60, 1.0, 1)]
+        replay(srv, warm, lambda job, jid: srv.release(jid))
+        burst = [dict(j, arrival=0.0) for j in job_stream(args.jobs, 1.0, 0)]
+        res = replay(srv, burst, lambda job, jid: srv.release(jid))
+        print(f"serve: {args.jobs} jobs in {res['span']:.3f} s, {srv.stats()['ticks']} ticks")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("case", choices=["image", "compact", "sort", "measure", "serve"])
+    ap.add_argument("--depth", type=int, default=None)
+    ap.add_argument("--instances", type=int, default=64)
+    ap.add_argument("--jobs", type=int, default=300)
+    args = ap.parse_args()
+    if args.depth is None:
+        args.depth = {"image": 23, "compact": 27, "sort": 24, "measure": 27, "serve": 0}[args.case]
+    {"image": case_image, "compact": case_compact, "sort": case_sort, "measure": case_measure,
+     "serve": case_serve}[args.case](args)
+
+
+if __name__ == "__main__":
+    main()

@@ -335,6 +335,7 @@ def gpu_arm(args, rank: int, world: int, dist):
     main = measure_mode(args, rank, world, dist, fma=not args.strict, peak_tflops=peak_tflops)
     other = None if args.single else measure_mode(args, rank, world, dist, fma=args.strict, peak_tflops=peak_tflops)
     cpu = cpu_baseline(cpu_cores()) if (rank == 0 and world == 1 and not args.no_cpu) else None
+    configs = configs_mode(args, peak_tflops) if (rank == 0 and world == 1 and not args.no_configs) else None
     serving = serve_mode(args) if (rank == 0 and world == 1 and args.serve_jobs > 0) else None
     if rank == 0:
         arith = "strict" if args.strict else "fma"
@@ -354,10 +355,85 @@ def gpu_arm(args, rank: int, world: int, dist):
                 "roofline_achieved": other["roofline"]["achieved"], "roofline_frac": other["roofline"]["frac"],
                 "transition_rows_tflops": other["roofline"]["transition_rows_tflops"], "phases_ms": other["phases"],
                 "counts_identical": other["counts"] == main["counts"], "clocks": other["clocks"]}
+        if configs is not None:
+            line["configs"] = configs
         if serving is not None:
             line["serving"] = serving
         print(json.dumps(line), flush=True)
     return 0
+
+
+# ------------------------------------------------------------------------------ other configurations
+def _timed(fn, reps: int):
+    """Best-of-`reps` host wall time of a synchronous call (after one untimed call)."""
+    fn()
+    best = float("inf")
+    out = None
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        out = fn()
+        best = min(best, time.perf_counter() - t0)
+    return best, out
+
+
+def configs_mode(args, peak_tflops: float):
+    """The Henon validity workload, the coupled-Duffing continuation and the 512-instance
+    Lorenz scan, each timed on its own after a warm-up call."""
+    import b12_b200 as B
+    from b12_b200.workloads import LORENZ_CENTER, LORENZ_RADIUS, lorenz_scan
+
+    out = {}
+    # Henon a=1.4 b=0.3, 20 steps, 4x4 inner grid, CSR
+    sc = B.Scheme(B.henon(1.4, 0.3), B.inner_grid(4))
+    t = B.ImplicitBoxTree((0.0, 0.0), (1.5, 0.45))
+
+    def henon():
+        t.delete_depth(0)
+        c = t.subdivision_run(sc, 20)
+        m = t.transition_matrix(sc)
+        nnz = m.nnz
+        m.close()
+        return c, nnz
+
+    sec, (c, nnz) = _timed(henon, 5)
+    bi, nf = box_images_of(c)
+    out["henon_d20"] = {"boxes": nf, "nnz": nnz, "ms_per_job": 1e3 * sec, "box_images_per_s": (bi + nf) / sec}
+    t.close()
+
+    # coupled Duffing, unstable-manifold continuation at depth 24 from the box of the origin,
+    # 64 Philox points per box (seed 0), Stormer-Verlet h=0.05 x 10
+    sc = B.Scheme(B.coupled_duffing(), B.philox_grid(64, 0))
+    t = B.ImplicitBoxTree((0.0,) * 4, (2.0,) * 4)
+    t.reserve(16 << 20)
+    sec, sweeps = _timed(lambda: t.continuation_run(sc, np.zeros(4), 24), 2)
+    n = int(sweeps[-1])
+    flop = 64 * 280
+    out["coupled_duffing_continuation_d24"] = {
+        "boxes": n, "sweeps": len(sweeps), "seconds": sec, "box_images": n,
+        "box_images_per_s": n / sec, "tflops": n * flop / sec / 1e12, "flop_per_box_image": flop,
+        "note": "every box is imaged once, in the sweep after it was inserted"}
+    t.close()
+
+    # 512 Lorenz instances, rho ~ U[15,35], depth 18-27 (SplitMix64 seed 0): batched
+    rho, depth = lorenz_scan(512, 0)
+    params = [(10.0, r, 8.0 / 3.0) for r in rho]
+    b = B.Batch(LORENZ_CENTER, LORENZ_RADIUS, B.Scheme(B.lorenz(fma=True), B.inner_grid(5)), params, depth)
+    b.run()                       # first run: autotunes the launch shape
+    b.transition_matrices()
+    run_s, _ = _timed(b.run, 2)
+    tm_s, _ = _timed(b.transition_matrices, 2)
+    info = b.info()
+    bi, nf = info["box_images"], info["final_boxes"]
+    flop = P * FLOP_PER_POINT
+    out["lorenz_batch_512"] = {
+        "instances": 512, "box_images": bi, "final_boxes": nf, "nnz": info["nnz"],
+        "subdivision_s": run_s, "transition_matrices_s": tm_s,
+        "box_images_per_s": (bi + nf) / (run_s + tm_s),
+        "subdivision_tflops": bi * flop / run_s / 1e12, "subdivision_frac_of_fp64_peak": bi * flop / run_s / 1e12 /
+        peak_tflops, "launch_shape": {k: info[k] for k in ("threads", "points_per_thread", "chunk")},
+        "frac_note": "whole batched run (every kernel of the 27 steps) against the measured FP64 peak"}
+    b.close()
+    return out
 
 
 # ------------------------------------------------------------------------------ serving
@@ -494,6 +570,8 @@ def main():
                     help="headline with the strict (one rounding per operation) integrator instead of explicit FMA")
     ap.add_argument("--single", action="store_true", help="measure only the headline arithmetic")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the Henon, coupled-Duffing continuation and 512-instance batch measurements")
     ap.add_argument("--serve-jobs", type=int, default=10000,
                     help="jobs of the served stream measured against the plain path at 1 GPU (0: skip)")
     args = ap.parse_args()

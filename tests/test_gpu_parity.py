@@ -227,3 +227,22 @@ def test_capacity_retry_in_fused_run():
     oc, _ = o.subdivision(21)
     np.testing.assert_array_equal(counts, oc)
     np.testing.assert_array_equal(t.leaves()[0], o.leaves()[0])
+
+
+def test_invariant_measure_lorenz_depth27_against_oracle(capsys):
+    # the benchmark's job: Lorenz depth 27 (explicit-FMA integrator), its transition
+    # matrix and 200 power iterations; L1 distance to the oracle's FP64 power iteration
+    spec = dict(map="lorenz", rho=28.0, fma=True, grid=5)
+    t = make_tree(spec)
+    sc = scheme(spec)
+    counts = t.subdivision_run(sc, 27)
+    assert counts[-1] == 249450
+    m = t.transition_matrix(sc)
+    rowptr, cols, vals = m.to_host()
+    assert len(vals) == 1615474
+    v = m.invariant_measure(200)
+    ref = O.invariant_measure(rowptr, cols, vals, 200)
+    l1 = float(np.abs(v - ref).sum())
+    with capsys.disabled():
+        print(f"\nLorenz d27 invariant measure: L1 to the oracle = {l1:.3e} (n = {len(v)})")
+    assert l1 < MEASURE_L1, l1
