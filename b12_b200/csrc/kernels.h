@@ -105,6 +105,7 @@ struct CompactArgs {
   uint32_t* n_out;
   uint32_t* n_out2;          // optional second copy of the new count
   uint32_t* out_rank;        // optional: out_rank[i] = kept elements before input i (n + 1 entries)
+  int vec;                   // set by compact(): the mask and rank arrays take 16-byte accesses
   uint32_t out_cap;
   uint32_t* error;
 };

@@ -175,82 +175,162 @@ __device__ __forceinline__ uint32_t compact_n(const CompactArgs& a)
   return c <= a.hit_cap ? uint32_t(c) : 0u;
 }
 
-__device__ __forceinline__ bool compact_keep(const CompactArgs& a, uint32_t i)
+// Each thread owns a run of 16 consecutive elements (kItems), so a tile of kCompactTile
+// elements is one pass of the block: the keep bits of a run come from one 16-byte load
+// of the hit mask (children) or of the flags, and the block needs one scan per tile.
+static_assert(kItems == 16, "a thread's run is one 16-byte vector of mask bytes");
+
+// keep bits of the run starting at `base` (bit j: element base + j)
+__device__ __forceinline__ uint32_t run_mask(const CompactArgs& a, uint32_t base, uint32_t n, bool vec)
 {
-  return a.children ? a.hit[i] != 0 : has_all(a.flags[i], a.keep_flags);
+  const uint8_t* src = a.children ? a.hit : a.flags;
+  uint32_t m = 0;
+  if (vec && base + 16 <= n) {
+    const uint4 v = *reinterpret_cast<const uint4*>(src + base);
+    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const uint8_t byte = uint8_t(w[j >> 2] >> (8 * (j & 3)));
+      const bool keep = a.children ? byte != 0 : has_all(byte, a.keep_flags);
+      m |= uint32_t(keep) << j;
+    }
+  } else {
+    for (int j = 0; j < 16; ++j) {
+      const uint32_t i = base + j;
+      if (i >= n) break;
+      const bool keep = a.children ? src[i] != 0 : has_all(src[i], a.keep_flags);
+      m |= uint32_t(keep) << j;
+    }
+  }
+  return m;
 }
 
-__global__ void compact_count_kernel(const CompactArgs a, uint32_t* tile_counts)
+__global__ void __launch_bounds__(kThreads) compact_count_kernel(const CompactArgs a, uint32_t* tile_counts)
 {
   __shared__ uint32_t red[32];
   const uint32_t n = compact_n(a);
   const uint32_t tiles = (n + kCompactTile - 1) / kCompactTile;
+  const bool vec = a.vec != 0;
   for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
-    uint32_t c = 0;
-#pragma unroll 4
-    for (int k = 0; k < kItems; ++k) {
-      const uint32_t i = t * kCompactTile + k * kThreads + threadIdx.x;
-      if (i < n && compact_keep(a, i)) ++c;
-    }
-    c = block_sum(c, red);
-    if (threadIdx.x == 0) tile_counts[t] = c;
+    const uint32_t base = t * kCompactTile + threadIdx.x * kItems;
+    const uint32_t c = __popc(run_mask(a, base, n, vec));
+    const uint32_t total = block_sum(c, red);
+    if (threadIdx.x == 0) tile_counts[t] = total;
   }
 }
 
-// one block: exclusive scan of the tile counts; total -> *n_out
+// one block: exclusive scan of the tile counts; total -> *n_out.  Each thread sums a
+// contiguous group of tiles first, so the block scans once.
 __global__ void compact_scan_kernel(const CompactArgs a, const uint32_t* tile_counts, uint32_t* tile_offsets)
 {
   __shared__ uint32_t red[32];
   const uint32_t n = compact_n(a);
   const uint32_t tiles = (n + kCompactTile - 1) / kCompactTile;
-  uint32_t carry = 0;
-  for (uint32_t base = 0; base < tiles; base += blockDim.x) {
-    const uint32_t t = base + threadIdx.x;
-    const uint32_t v = t < tiles ? tile_counts[t] : 0u;
-    uint32_t total;
-    const uint32_t ex = block_exclusive(v, red, &total);
-    if (t < tiles) tile_offsets[t] = carry + ex;
-    carry += total;
+  const uint32_t per = (tiles + blockDim.x - 1) / blockDim.x;
+  const uint32_t first = threadIdx.x * per, last = min(tiles, first + per);
+  uint32_t mine = 0;
+  for (uint32_t t = first; t < last; ++t) mine += tile_counts[t];
+  uint32_t carry;
+  uint32_t off = block_exclusive(mine, red, &carry);
+  for (uint32_t t = first; t < last; ++t) {
+    const uint32_t v = tile_counts[t];
+    tile_offsets[t] = off;
+    off += v;
   }
   if (threadIdx.x == 0) {
     if (carry > a.out_cap || (a.children && 2ull * *a.n > a.hit_cap)) atomicOr(a.error, 1u);
-    if (carry > a.out_cap) carry = a.out_cap;
     if (a.out_rank) a.out_rank[n] = carry;
+    if (carry > a.out_cap) carry = a.out_cap;
     *a.n_out = carry;
     if (a.n_out2) *a.n_out2 = carry;
   }
 }
 
-__global__ void compact_scatter_kernel(const CompactArgs a, const uint32_t* tile_offsets)
+// survivors of a tile staged in shared memory in order, then written out coalesced
+__global__ void __launch_bounds__(kThreads) compact_scatter_kernel(const CompactArgs a, const uint32_t* tile_offsets)
 {
   __shared__ uint32_t red[32];
+  __shared__ uint64_t s_code[kCompactTile];     // codes, or kept indices in out_index mode
+  __shared__ uint8_t s_flags[kCompactTile];
   const uint32_t n = compact_n(a);
   const uint32_t tiles = (n + kCompactTile - 1) / kCompactTile;
+  const bool vec = a.vec != 0;
   for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
-    uint32_t off = tile_offsets[t];
-    for (int k = 0; k < kItems; ++k) {
-      const uint32_t i = t * kCompactTile + k * kThreads + threadIdx.x;
-      const bool keep = i < n && compact_keep(a, i);
-      uint32_t total;
-      const uint32_t ex = block_exclusive(keep ? 1u : 0u, red, &total);
-      if (keep) {
-        const uint32_t pos = off + ex;
-        if (pos < a.out_cap) {
-          if (a.out_index) {
-            a.out_index[pos] = i;
-          } else if (a.children) {
-            a.out_code[pos] = (a.code[i >> 1] << 1) | uint64_t(i & 1u);
-            a.out_flags[pos] = a.flags[i >> 1] & uint8_t(~a.clear_flags);
-          } else {
-            a.out_code[pos] = a.code[i];
-            a.out_flags[pos] = a.flags[i] & uint8_t(~a.clear_flags);
-          }
-        }
+    const uint32_t base = t * kCompactTile + threadIdx.x * kItems;
+    const uint32_t m = run_mask(a, base, n, vec);
+    uint32_t total;
+    uint32_t at = block_exclusive(__popc(m), red, &total);
+    const uint32_t off = tile_offsets[t];
+    if (a.out_rank) {
+      // rank of element base + j: survivors before it
+      uint32_t r[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) r[j] = off + at + __popc(m & ((1u << j) - 1u));
+      if (base + 16 <= n && vec) {
+        uint4* dst = reinterpret_cast<uint4*>(a.out_rank + base);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) dst[q] = make_uint4(r[4 * q], r[4 * q + 1], r[4 * q + 2], r[4 * q + 3]);
+      } else {
+        for (int j = 0; j < 16 && base + j < n; ++j) a.out_rank[base + j] = r[j];
       }
-      if (a.out_rank && i < n) a.out_rank[i] = off + ex;
-      if (a.children && i < n) a.hit[i] = 0;
-      off += total;
     }
+    if (a.children) {
+      // the mask is consumed: clear it for the next step
+      if (base + 16 <= n && vec) *reinterpret_cast<uint4*>(a.hit + base) = make_uint4(0, 0, 0, 0);
+      else
+        for (int j = 0; j < 16 && base + j < n; ++j) a.hit[base + j] = 0;
+    }
+    // stage this run's survivors at their tile positions
+    uint32_t mm = m;
+    if (a.children && !a.out_index && vec && m && base + 16 <= n) {
+      // the run's 8 parents: 64 bytes of codes and 8 of flags in four + one vector loads
+      const uint4* pc = reinterpret_cast<const uint4*>(a.code + (base >> 1));
+      uint64_t pcode[8];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const uint4 v = pc[q];
+        pcode[2 * q] = (uint64_t(v.y) << 32) | v.x;
+        pcode[2 * q + 1] = (uint64_t(v.w) << 32) | v.z;
+      }
+      const uint2 fv = *reinterpret_cast<const uint2*>(a.flags + (base >> 1));
+      const uint8_t keep_mask = uint8_t(~a.clear_flags);
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        if (!((m >> j) & 1u)) continue;
+        const uint32_t fw = (j >> 1) < 4 ? fv.x : fv.y;
+        s_code[at] = (pcode[j >> 1] << 1) | uint64_t(j & 1);
+        s_flags[at] = uint8_t(fw >> (8 * ((j >> 1) & 3))) & keep_mask;
+        ++at;
+      }
+      mm = 0;
+    }
+    while (mm) {
+      const int j = __ffs(mm) - 1;
+      const uint32_t i = base + j;
+      if (a.out_index) {
+        s_code[at] = i;
+      } else if (a.children) {
+        s_code[at] = (a.code[i >> 1] << 1) | uint64_t(i & 1u);
+        s_flags[at] = a.flags[i >> 1] & uint8_t(~a.clear_flags);
+      } else {
+        s_code[at] = a.code[i];
+        s_flags[at] = a.flags[i] & uint8_t(~a.clear_flags);
+      }
+      ++at;
+      mm &= mm - 1;
+    }
+    __syncthreads();
+    for (uint32_t x = threadIdx.x; x < total; x += kThreads) {
+      const uint32_t pos = off + x;
+      if (pos >= a.out_cap) break;
+      if (a.out_index) {
+        a.out_index[pos] = uint32_t(s_code[x]);
+      } else {
+        a.out_code[pos] = s_code[x];
+        a.out_flags[pos] = s_flags[x];
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -360,8 +440,13 @@ cudaError_t build_leaf_hash(const uint64_t* codes, const uint32_t* n, LeafHash h
   return cudaGetLastError();
 }
 
-cudaError_t compact(const CompactArgs& a, const CompactScratch& sc, uint32_t max_in, cudaStream_t s)
+cudaError_t compact(const CompactArgs& args, const CompactScratch& sc, uint32_t max_in, cudaStream_t s)
 {
+  CompactArgs a = args;
+  // 16-byte runs of the mask and of the ranks need 16-byte aligned arrays
+  const uintptr_t mask = uintptr_t(a.children ? static_cast<const void*>(a.hit) : a.flags);
+  a.vec = (mask % 16 == 0 && uintptr_t(a.out_rank) % 16 == 0 && uintptr_t(a.code) % 16 == 0 &&
+           uintptr_t(a.flags) % 8 == 0) ? 1 : 0;
   const uint64_t elems = a.children ? 2ull * max_in : uint64_t(max_in);
   const int g = grid_for(elems, kCompactTile, 4);
   compact_count_kernel<<<g, kThreads, 0, s>>>(a, sc.tile_counts);
