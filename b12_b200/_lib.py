@@ -117,6 +117,17 @@ _SIGS = {
     "b12g_batch_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
                                   C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     "b12g_batch_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "b12g_tree_save_json": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "b12g_tree_load_json": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
+    "b12g_csr_save_json": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "b12g_csr_load_json": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
+    "b12g_json_write_leaves": (C.c_int, [C.c_char_p, C.POINTER(Domain), C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.c_uint64]),
+    "b12g_json_read_leaves": (C.c_int, [C.c_char_p, C.POINTER(Domain), C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.POINTER(C.c_uint64)]),
+    "b12g_json_write_coo": (C.c_int, [C.c_char_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "b12g_json_read_coo": (C.c_int, [C.c_char_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.c_void_p,
+                                     C.c_void_p, C.c_void_p, C.POINTER(C.c_uint64)]),
     "b12g_server_create": (C.c_int, [C.c_uint64, C.POINTER(C.c_void_p)]),
     "b12g_server_destroy": (C.c_int, [C.c_void_p]),
     "b12g_server_submit": (C.c_int, [C.c_void_p, C.POINTER(Job), C.POINTER(C.c_uint64)]),

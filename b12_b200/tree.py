@@ -144,6 +144,17 @@ class CsrMatrix:
     def to_host_into(self, rowptr, cols, vals):
         check(lib().b12g_csr_copy(self._h, rowptr.ctypes.data, cols.ctypes.data, vals.ctypes.data), "csr_copy")
 
+    def save(self, path: str) -> None:
+        """CooMatrix::save (CooMatrix.hpp:473-525): the reference's JSON file."""
+        check(lib().b12g_csr_save_json(self._h, str(path).encode()), "csr_save_json")
+
+    @classmethod
+    def load(cls, path: str) -> "CsrMatrix":
+        """CooMatrix(fileName) (CooMatrix.hpp:236-291): a matrix from the reference's JSON file."""
+        h = C.c_void_p()
+        check(lib().b12g_csr_load_json(str(path).encode(), C.byref(h)), "csr_load_json")
+        return cls(h)
+
     def close(self):
         if self._h:
             lib().b12g_csr_destroy(self._h)
@@ -154,6 +165,55 @@ class CsrMatrix:
             self.close()
         except Exception:
             pass
+
+
+# ----------------------------------------------------------------------------- JSON files (host arrays)
+def json_write_leaves(path, center, radius, codes, depths, flags) -> None:
+    """Write leaves in the reference's tree JSON format (no device involved)."""
+    d = L.Domain()
+    d.dim = len(center)
+    for j in range(d.dim):
+        d.center[j], d.radius[j] = float(center[j]), float(radius[j])
+    codes = np.ascontiguousarray(codes, dtype=np.uint64)
+    depths = np.ascontiguousarray(depths, dtype=np.uint8)
+    flags = np.ascontiguousarray(flags, dtype=np.uint8)
+    check(lib().b12g_json_write_leaves(str(path).encode(), C.byref(d), codes.ctypes.data, depths.ctypes.data,
+                                       flags.ctypes.data, len(codes)), "json_write_leaves")
+
+
+def json_read_leaves(path):
+    """(center, radius, codes, depths, flags) of a tree JSON file (no device involved)."""
+    d = L.Domain()
+    n = C.c_uint64(0)
+    check(lib().b12g_json_read_leaves(str(path).encode(), C.byref(d), None, None, None, C.byref(n)), "json_read_leaves")
+    codes = np.zeros(n.value, dtype=np.uint64)
+    depths = np.zeros(n.value, dtype=np.uint8)
+    flags = np.zeros(n.value, dtype=np.uint8)
+    check(lib().b12g_json_read_leaves(str(path).encode(), C.byref(d), codes.ctypes.data, depths.ctypes.data,
+                                      flags.ctypes.data, C.byref(n)), "json_read_leaves")
+    return list(d.center[: d.dim]), list(d.radius[: d.dim]), codes, depths, flags
+
+
+def json_write_coo(path, n_rows, n_cols, rowptr, cols, vals) -> None:
+    """Write CSR arrays in the reference's CooMatrix JSON format (no device involved)."""
+    rowptr = np.ascontiguousarray(rowptr, dtype=np.uint32)
+    cols = np.ascontiguousarray(cols, dtype=np.uint32)
+    vals = np.ascontiguousarray(vals, dtype=np.float64)
+    check(lib().b12g_json_write_coo(str(path).encode(), n_rows, n_cols, rowptr.ctypes.data, cols.ctypes.data,
+                                    vals.ctypes.data), "json_write_coo")
+
+
+def json_read_coo(path):
+    """(n_rows, n_cols, rowptr, cols, vals) of a CooMatrix JSON file (no device involved)."""
+    r, c, z = C.c_uint32(), C.c_uint32(), C.c_uint64()
+    check(lib().b12g_json_read_coo(str(path).encode(), C.byref(r), C.byref(c), None, None, None, C.byref(z)),
+          "json_read_coo")
+    rowptr = np.zeros(r.value + 1, dtype=np.uint32)
+    cols = np.zeros(max(z.value, 1), dtype=np.uint32)
+    vals = np.zeros(max(z.value, 1), dtype=np.float64)
+    check(lib().b12g_json_read_coo(str(path).encode(), C.byref(r), C.byref(c), rowptr.ctypes.data, cols.ctypes.data,
+                                   vals.ctypes.data, C.byref(z)), "json_read_coo")
+    return r.value, c.value, rowptr, cols[: z.value], vals[: z.value]
 
 
 def launch_count() -> int:
@@ -191,6 +251,24 @@ class ImplicitBoxTree:
         if self._h:
             lib().b12g_tree_destroy(self._h)
             self._h = None
+
+    def save(self, path: str) -> None:
+        """ImplicitBoxTree::save (ImplicitBoxTree.hpp:435-528): the reference's JSON file."""
+        check(lib().b12g_tree_save_json(self._h, str(path).encode()), "tree_save_json")
+
+    @classmethod
+    def load(cls, path: str) -> "ImplicitBoxTree":
+        """ImplicitBoxTree(fileName) (ImplicitBoxTree.hpp:144-359): a tree from the reference's JSON file."""
+        h = C.c_void_p()
+        check(lib().b12g_tree_load_json(str(path).encode(), C.byref(h)), "tree_load_json")
+        t = cls.__new__(cls)
+        d = L.Domain()
+        n = C.c_uint64(0)
+        check(lib().b12g_json_read_leaves(str(path).encode(), C.byref(d), None, None, None, C.byref(n)),
+              "json_read_leaves")
+        t.dim = d.dim
+        t._h = h
+        return t
 
     def __del__(self):
         try:

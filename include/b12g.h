@@ -214,6 +214,31 @@ b12g_status b12g_subdivision_run(b12g_tree* tree, const b12g_scheme* scheme, uin
 b12g_status b12g_continuation_run(b12g_tree* tree, const b12g_scheme* scheme, const double* x0, uint64_t n_x0,
                                   uint8_t depth, uint32_t max_sweeps, uint32_t* counts, uint32_t* n_sweeps);
 
+/* ---- JSON files in the reference's format ----------------------------------------------
+ * Trees as written by ImplicitBoxTree::save (ImplicitBoxTree.hpp:435-528) and read by
+ * ImplicitBoxTree(fileName) (ImplicitBoxTree.hpp:144-359, JSON files only): center,
+ * radius, sdScheme, nLeaves, bitPatternVector, depthVector, flagsVector, nHostBufferBytes.
+ * Matrices as written by CooMatrix::save (CooMatrix.hpp:473-525) and read by
+ * CooMatrix(fileName) (CooMatrix.hpp:236-291): nRows, nColumns, nnz and the row-major
+ * triples.  Files written here are byte for byte what the reference writes for the same
+ * tree or matrix; ".json" is appended to a path without it, as the reference does.
+ * Loading needs the default subdivision scheme and, for a tree, one leaf depth. */
+b12g_status b12g_tree_save_json(b12g_tree* tree, const char* path);
+b12g_status b12g_tree_load_json(const char* path, b12g_tree** tree);
+b12g_status b12g_csr_save_json(const b12g_csr* matrix, const char* path);
+b12g_status b12g_csr_load_json(const char* path, b12g_csr** matrix);
+/* the same files from and to host arrays (no device involved): *n is the capacity of the
+ * arrays on entry (any array may be NULL to query the count) and the leaf count on return */
+b12g_status b12g_json_write_leaves(const char* path, const b12g_domain* domain, const uint64_t* codes,
+                                   const uint8_t* depths, const uint8_t* flags, uint64_t n);
+b12g_status b12g_json_read_leaves(const char* path, b12g_domain* domain, uint64_t* codes, uint8_t* depths,
+                                  uint8_t* flags, uint64_t* n);
+/* CSR arrays (rowptr: n_rows + 1 entries); reading fills rowptr, cols, vals when not NULL */
+b12g_status b12g_json_write_coo(const char* path, uint32_t n_rows, uint32_t n_cols, const uint32_t* rowptr,
+                                const uint32_t* cols, const double* vals);
+b12g_status b12g_json_read_coo(const char* path, uint32_t* n_rows, uint32_t* n_cols, uint32_t* rowptr,
+                               uint32_t* cols, double* vals, uint64_t* nnz);
+
 /* ---- batches of independent subdivision jobs --------------------------------------------
  * Many instances of the subdivision loop (subdivision.m:18-45) with one domain, map
  * kind, grid and arithmetic but per-instance map parameters and depths, advanced in

@@ -34,6 +34,8 @@ struct RunOpts
   std::string out;            // dump directory ("" = no dumps)
   int dumpFrom = 0;           // dump leaves of steps >= dumpFrom
   int tm = 1;                 // 0: none, 1: relative, 2: absolute, 3: relative + invalid column
+  std::string save;           // save the final tree and matrix as JSON (save(): ImplicitBoxTree.hpp:435-528,
+                              // CooMatrix.hpp:473-525) to SAVE_tree.json / SAVE_tm.json
 };
 
 inline RunOpts parseOpts(int argc, char** argv)
@@ -44,6 +46,7 @@ inline RunOpts parseOpts(int argc, char** argv)
   o.out = arg(argc, argv, "--out", "");
   o.dumpFrom = std::atoi(arg(argc, argv, "--dump-from", "0"));
   o.tm = std::atoi(arg(argc, argv, "--tm", "1"));
+  o.save = arg(argc, argv, "--save", "");
   return o;
 }
 
@@ -79,6 +82,7 @@ int runSubdivision(const std::vector<double>& c, const std::vector<double>& r,
   }
   auto t1 = clk::now();
   js << "], \"subdivision_s\": " << secs(t0, t1) << ", \"box_images\": " << boxImages;
+  if (!o.save.empty()) ibt.save(o.save + "_tree.json");
   if (o.tm) {
     const bool absolute = (o.tm == 2), invalid = (o.tm == 3);
     auto P = ibt.template transitionMatrixForLeaves<double>(grid, map, absolute, true, invalid);
@@ -86,6 +90,7 @@ int runSubdivision(const std::vector<double>& c, const std::vector<double>& r,
     js << ", \"tm_s\": " << secs(t1, t2) << ", \"nnz\": " << P.values_.size()
        << ", \"tm_box_images\": " << ibt.count(getLeafDepth());
     if (!o.out.empty()) dumpCoo(P, o.out + "/tm.bin");
+    if (!o.save.empty()) P.save(o.save + "_tm.json");
   }
   js << "}";
   std::cout << js.str() << std::endl;

@@ -44,6 +44,13 @@ WORKLOADS = {
                          dict(map="lorenz", rho=35.0, grid=5, steps=18)),
     "forced_duffing_d16": ("ref_forced", ["--steps", "16", "--tm", "1"],
                            dict(map="forced_duffing", grid=4, steps=16)),
+    # files written by the reference's ImplicitBoxTree::save and CooMatrix::save (JSON)
+    "henon_d8_files": ("ref_henon", ["--steps", "8", "--tm", "1", "--buf", "4294967296"],
+                       dict(map="henon", a=1.4, b=0.3, grid=4, steps=8, save=True)),
+    "henon_d10_lost_files": ("ref_henon", ["--steps", "10", "--tm", "3", "--buf", "4294967296"],
+                             dict(map="henon", a=1.4, b=0.3, grid=4, steps=10, invalid=True, save=True)),
+    "lorenz_d9_files": ("ref_lorenz", ["--steps", "9", "--tm", "1", "--buf", "4294967296"],
+                        dict(map="lorenz", rho=28.0, grid=5, steps=9, save=True)),
     "coupled_duffing_cont_d8": ("ref_duffing", ["--steps", "8"], dict(map="coupled_duffing", points=64, seed=0,
                                                                           depth=8)),
     "coupled_duffing_cont_d12": ("ref_duffing", ["--steps", "12"], dict(map="coupled_duffing", points=64, seed=0,
@@ -92,6 +99,8 @@ def generate(name: str) -> None:
         cmd = [exe, "--out", tmp] + args
         if "--buf" not in args:
             cmd += ["--buf", str(64 << 20)]
+        if spec.get("save"):
+            cmd += ["--save", os.path.join(tmp, "saved")]
         res = subprocess.run(cmd, check=True, capture_output=True, text=True)
         timing = json.loads(res.stdout.strip().splitlines()[-1])
         out = dict(workload=name, spec=spec, reference_cmd=" ".join([binary] + args), timing=timing, steps=[])
@@ -118,6 +127,13 @@ def generate(name: str) -> None:
                 arrays["tm_rowptr"] = rowptr
                 arrays["tm_cols"] = cols
                 arrays["tm_vals"] = vals
+        if spec.get("save"):
+            # the reference's own JSON files, byte for byte
+            os.makedirs(os.path.join(HERE, "files"), exist_ok=True)
+            for part in ("tree", "tm"):
+                src = os.path.join(tmp, f"saved_{part}.json")
+                with open(src, "rb") as fi, open(os.path.join(HERE, "files", f"{name}_{part}.json"), "wb") as fo:
+                    fo.write(fi.read())
     with open(os.path.join(HERE, f"{name}.json"), "w") as f:
         json.dump(out, f, indent=1)
     if arrays:
