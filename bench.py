@@ -47,6 +47,7 @@ CONFIG = {"workload": "lorenz-rk4-depth27", "sigma": 10.0, "rho": 28.0, "beta": 
           "rk4_steps": 20, "grid": "inner 5x5x5", "depth": DEPTH, "tm": "csr", "measure_iters": MEASURE_ITERS,
           "l2": "flushed between timed steps (256 MiB write)", "arith": "fma"}
 NOMINAL_FP64_TFLOPS = 37.0
+IMAGE_DRAM_BYTES_PER_BOX = 2.346752e6 / 47304   # ncu: DRAM bytes of one image launch / its boxes
 
 
 def log(*a):
@@ -310,7 +311,9 @@ def measure_mode(args, rank, world, dist, fma: bool, peak_tflops: float):
            "d2h_bytes_per_step": int(d2h), "steps": e2e_steps, "timer": "host wall clock, synchronous API"}
     roofline = {"bound": "fp64", "kernel": "image_points_kernel (fused sample/RK4/locate)", "achieved": achieved,
                 "peak": peak_tflops, "unit": "TFLOP/s", "frac": (achieved / peak_tflops) if achieved else None,
-                "traffic": None,
+                "traffic": IMAGE_DRAM_BYTES_PER_BOX * bi_sub / img_n * args.steps if img_n else None,
+                "traffic_source": "ncu (profiles/image_points_kernel_lorenz_depth23.md): 2.35 MB of DRAM reads "
+                                  "and writes in one launch over 47,304 boxes, scaled to this job's boxes per launch",
                 "peak_source": "measured: FP64 FMA-chain probe kernel on this device "
                                f"(nominal {NOMINAL_FP64_TFLOPS} TFLOP/s)",
                 "flop_per_box_image": P * FLOP_PER_POINT, "launches": img_n,
