@@ -670,12 +670,18 @@ b12g_status b12g_csr_destroy(b12g_csr* m)
   return B12G_OK;
 }
 
-b12g_status b12g_invariant_measure(b12g_csr* m, uint32_t iters, double* v)
+}  // extern "C"
+
+namespace b12g {
+namespace host {
+
+// P^T of a matrix (rows ascending per column, the lost column dropped) and its rows
+// split by length class, built once per matrix
+b12g_status ensure_transpose(b12g_csr* m)
 {
-  if (!m) return fail(B12G_ERR_INVALID, "NULL matrix");
   const uint32_t n = m->n_rows;
-  if (n == 0) return B12G_OK;
   cudaStream_t s = m->stream;
+  if (n == 0) return B12G_OK;
   if (!m->has_transpose) {
     ST(m->tptr.ensure(n + 1, "transpose"));
     ST(m->trows.ensure(std::max<uint64_t>(m->nnz, 1), "transpose"));
@@ -702,6 +708,21 @@ b12g_status b12g_invariant_measure(b12g_csr* m, uint32_t iters, double* v)
     count_launches(16);
     m->has_transpose = true;
   }
+  return B12G_OK;
+}
+
+}  // namespace host
+}  // namespace b12g
+
+extern "C" {
+
+b12g_status b12g_invariant_measure(b12g_csr* m, uint32_t iters, double* v)
+{
+  if (!m) return fail(B12G_ERR_INVALID, "NULL matrix");
+  const uint32_t n = m->n_rows;
+  if (n == 0) return B12G_OK;
+  cudaStream_t s = m->stream;
+  ST(ensure_transpose(m));
   ST(m->w0.ensure(n, "measure"));
   ST(m->w1.ensure(n, "measure"));
   ST(m->vout.ensure(n, "measure"));

@@ -179,6 +179,8 @@ b12g_status build_current_hash(b12g_tree* t, Prepared& pr);
 // record a timing event of `kind` (0: box-image kernel, 1: transition rows) on the tree stream
 void prof_mark(b12g_tree* t, int kind);
 b12g_status prof_collect(b12g_tree* t);
+// P^T of a matrix and its row classes, built on first use (api.cu)
+b12g_status ensure_transpose(b12g_csr* m);
 
 }  // namespace host
 }  // namespace b12g

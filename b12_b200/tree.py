@@ -144,6 +144,13 @@ class CsrMatrix:
     def to_host_into(self, rowptr, cols, vals):
         check(lib().b12g_csr_copy(self._h, rowptr.ctypes.data, cols.ctypes.data, vals.ctypes.data), "csr_copy")
 
+    def strong_components(self):
+        """(labels, count): every row's strongly connected component, labelled by its largest row."""
+        comp = np.zeros(self.n_rows, dtype=np.uint32)
+        k = C.c_uint32()
+        check(lib().b12g_csr_strong_components(self._h, comp.ctypes.data, C.byref(k)), "csr_strong_components")
+        return comp, k.value
+
     def save(self, path: str) -> None:
         """CooMatrix::save (CooMatrix.hpp:473-525): the reference's JSON file."""
         check(lib().b12g_csr_save_json(self._h, str(path).encode()), "csr_save_json")
@@ -387,6 +394,34 @@ class ImplicitBoxTree:
         return ms.value, n.value
 
     # ---- fused drivers
+    def set_flags_by_components(self, matrix: "CsrMatrix", flags: int, min_size: int = 2) -> int:
+        """chainRecurrentSet.m:29-37: flag the leaves in strongly connected components of at least min_size."""
+        k = C.c_uint32()
+        check(lib().b12g_set_flags_by_components(self._h, matrix._h, min_size, flags, C.byref(k)),
+              "set_flags_by_components")
+        return k.value
+
+    def set_flags_by_measure(self, matrix: "CsrMatrix", threshold: float, flags: int) -> int:
+        """subdivisionByNim.m:56-62: flag the leaves whose invariant measure is at least `threshold`."""
+        k = C.c_uint32()
+        check(lib().b12g_set_flags_by_measure(self._h, matrix._h, float(threshold), flags, C.byref(k)),
+              "set_flags_by_measure")
+        return k.value
+
+    def chain_recurrent_run(self, scheme: Scheme, steps: int) -> np.ndarray:
+        """chainRecurrentSet.m:18-44 on the GPU; leaf counts after each step."""
+        counts = np.zeros(max(steps, 1), dtype=np.uint32)
+        s = scheme.to_c()
+        check(lib().b12g_chain_recurrent_run(self._h, C.byref(s), steps, counts.ctypes.data), "chain_recurrent_run")
+        return counts[:steps]
+
+    def nim_run(self, scheme: Scheme, steps: int, power_iterations: int = 200) -> np.ndarray:
+        """subdivisionByNim.m:22-66 with the FP64 power iteration; leaf counts after each step."""
+        counts = np.zeros(max(steps, 1), dtype=np.uint32)
+        s = scheme.to_c()
+        check(lib().b12g_nim_run(self._h, C.byref(s), steps, power_iterations, counts.ctypes.data), "nim_run")
+        return counts[:steps]
+
     def subdivision_run(self, scheme: Scheme, steps: int) -> np.ndarray:
         counts = np.zeros(max(steps, 1), dtype=np.uint32)
         s = scheme.to_c()

@@ -214,6 +214,28 @@ b12g_status b12g_subdivision_run(b12g_tree* tree, const b12g_scheme* scheme, uin
 b12g_status b12g_continuation_run(b12g_tree* tree, const b12g_scheme* scheme, const double* x0, uint64_t n_x0,
                                   uint8_t depth, uint32_t max_sweeps, uint32_t* counts, uint32_t* n_sweeps);
 
+/* ---- selection steps that consume a transition matrix ------------------------------------
+ * The Matlab drivers chainRecurrentSet.m:18-44 (keep the boxes of strongly connected
+ * components of P's graph with at least two boxes; graphconncomp(P') there) and
+ * subdivisionByNim.m:22-66 (keep the boxes whose invariant measure is at least 1e-9 / n;
+ * an eigensolver there, the FP64 power iteration here). */
+/* component label of every row's box: the largest box index of its strongly connected
+ * component (self-loops join nothing; the lost column is ignored); comp: host, n_rows entries */
+b12g_status b12g_csr_strong_components(b12g_csr* matrix, uint32_t* comp, uint32_t* n_components);
+/* setFlags(stencil, flags) with the stencil "in a component of at least min_size boxes"
+ * (chainRecurrentSet.m:29-37); the matrix's rows are the tree's leaves */
+b12g_status b12g_set_flags_by_components(b12g_tree* tree, b12g_csr* matrix, uint32_t min_size, uint8_t flags,
+                                         uint32_t* n_flagged);
+/* setFlags(stencil, flags) with the stencil "measure >= threshold" on the matrix's last
+ * invariant measure (subdivisionByNim.m:56-62 uses threshold 1e-9 / n) */
+b12g_status b12g_set_flags_by_measure(b12g_tree* tree, b12g_csr* matrix, double threshold, uint8_t flags,
+                                      uint32_t* n_flagged);
+/* the two drivers: setFlags(SD); steps x {subdivide(SD); transition matrix; select with
+ * HIT; remove(HIT); unsetFlags(HIT)}; counts: leaves after each step (may be NULL) */
+b12g_status b12g_chain_recurrent_run(b12g_tree* tree, const b12g_scheme* scheme, uint32_t steps, uint32_t* counts);
+b12g_status b12g_nim_run(b12g_tree* tree, const b12g_scheme* scheme, uint32_t steps, uint32_t power_iterations,
+                         uint32_t* counts);
+
 /* ---- JSON files in the reference's format ----------------------------------------------
  * Trees as written by ImplicitBoxTree::save (ImplicitBoxTree.hpp:435-528) and read by
  * ImplicitBoxTree(fileName) (ImplicitBoxTree.hpp:144-359, JSON files only): center,

@@ -362,6 +362,16 @@ uint32_t orc_set_flags(orc_tree* t, uint8_t flags)
   return c;
 }
 
+/* setFlags(stencil, flags) with a logical vector over the leaves, as the Matlab drivers
+ * call it (chainRecurrentSet.m:37, subdivisionByNim.m:62); returns the leaves flagged */
+uint32_t orc_set_flags_mask(orc_tree* t, const uint8_t* mask, uint8_t flags)
+{
+  uint32_t c = 0;
+  for (uint64_t i = 0; i < t->n; ++i)
+    if (mask[i]) { t->flags[i] |= flags; ++c; }
+  return c;
+}
+
 /* unsetFlags / unsetFlagsByStencil on the leaves (ImplicitBoxTree.hpp:3336-3360) */
 uint32_t orc_unset_flags(orc_tree* t, uint8_t flags)
 {
@@ -669,4 +679,54 @@ uint32_t orc_insert_by_image(orc_tree* t, const orc_map* m, const orc_grid* g, u
   merge_new(t, cand, u, depth, ins);
   free(cand); free(tgt); free(src);
   return (uint32_t)u;
+}
+
+/* ------------------------------------------------------------------------------
+ * strongly connected components of the graph of a transition matrix (row = source,
+ * column = target; columns >= n, the lost column, ignored) - what graphconncomp(P')
+ * gives chainRecurrentSet.m:29.  Tarjan's algorithm with an explicit stack; each
+ * component is labelled by its largest vertex.
+ * ---------------------------------------------------------------------------- */
+void orc_strong_components(uint32_t n, const uint32_t* rowptr, const uint32_t* cols, uint32_t* comp)
+{
+  const uint32_t NONE = 0xFFFFFFFFu;
+  uint32_t* index = (uint32_t*)malloc((size_t)n * 4);
+  uint32_t* low = (uint32_t*)malloc((size_t)n * 4);
+  uint8_t* on = (uint8_t*)calloc(n, 1);
+  uint32_t* stack = (uint32_t*)malloc((size_t)n * 4);
+  uint32_t* call_v = (uint32_t*)malloc((size_t)n * 4);
+  uint32_t* call_e = (uint32_t*)malloc((size_t)n * 4);
+  uint32_t sp = 0, next = 0;
+  for (uint32_t v = 0; v < n; ++v) index[v] = NONE;
+  for (uint32_t r = 0; r < n; ++r) {
+    if (index[r] != NONE) continue;
+    uint32_t depth = 0;
+    call_v[0] = r; call_e[0] = rowptr[r];
+    index[r] = low[r] = next++; stack[sp++] = r; on[r] = 1;
+    while (1) {
+      const uint32_t v = call_v[depth];
+      if (call_e[depth] < rowptr[v + 1]) {
+        const uint32_t w = cols[call_e[depth]++];
+        if (w >= n) continue;
+        if (index[w] == NONE) {
+          ++depth;
+          call_v[depth] = w; call_e[depth] = rowptr[w];
+          index[w] = low[w] = next++; stack[sp++] = w; on[w] = 1;
+        } else if (on[w] && index[w] < low[v]) {
+          low[v] = index[w];
+        }
+        continue;
+      }
+      if (low[v] == index[v]) {
+        /* v is the root of a component: pop it, label by its largest vertex */
+        uint32_t top = sp, label = 0;
+        do { --top; if (stack[top] > label) label = stack[top]; } while (stack[top] != v);
+        while (sp > top) { const uint32_t x = stack[--sp]; on[x] = 0; comp[x] = label; }
+      }
+      if (depth == 0) break;
+      --depth;
+      { const uint32_t u = call_v[depth]; if (low[v] < low[u]) low[u] = low[v]; }
+    }
+  }
+  free(index); free(low); free(on); free(stack); free(call_v); free(call_e);
 }

@@ -82,6 +82,7 @@ void orc_tree_init(orc_tree* t, const orc_domain* d);     /* surrounding box (0,
 void orc_tree_free(orc_tree* t);
 void orc_tree_load(orc_tree* t, const uint64_t* code, const uint8_t* depth, const uint8_t* flags, uint64_t n);
 uint32_t orc_set_flags(orc_tree* t, uint8_t flags);
+uint32_t orc_set_flags_mask(orc_tree* t, const uint8_t* mask, uint8_t flags);
 uint32_t orc_unset_flags(orc_tree* t, uint8_t flags);
 uint32_t orc_change_flags(orc_tree* t, uint8_t to_unset, uint8_t to_set);
 uint32_t orc_subdivide(orc_tree* t, uint8_t flags);
@@ -106,6 +107,7 @@ uint64_t orc_transition_matrix(const orc_tree* t, const orc_map* m, const orc_gr
                                uint32_t* rowptr, uint32_t* cols, double* vals, uint32_t* n_cols);
 
 /* v <- P^T v, L1-normalised, `iters` times from the uniform vector */
+void orc_strong_components(uint32_t n, const uint32_t* rowptr, const uint32_t* cols, uint32_t* comp);
 void orc_invariant_measure(uint32_t n, const uint32_t* rowptr, const uint32_t* cols, const double* vals,
                            uint32_t iters, double* v);
 

@@ -68,6 +68,8 @@ def lib():
             "orc_tree_free": (None, [P(OrcTree)]),
             "orc_tree_load": (None, [P(OrcTree), P(u64), P(u8), P(u8), u64]),
             "orc_set_flags": (u32, [P(OrcTree), u8]),
+            "orc_set_flags_mask": (u32, [P(OrcTree), P(u8), u8]),
+            "orc_strong_components": (None, [u32, P(u32), P(u32), P(u32)]),
             "orc_unset_flags": (u32, [P(OrcTree), u8]),
             "orc_change_flags": (u32, [P(OrcTree), u8, u8]),
             "orc_subdivide": (u32, [P(OrcTree), u8]),
@@ -189,6 +191,11 @@ class Oracle:
     # -- reference operations
     def set_flags(self, f): return self.L.orc_set_flags(C.byref(self.tree), f)
     def unset_flags(self, f): return self.L.orc_unset_flags(C.byref(self.tree), f)
+
+    def set_flags_mask(self, mask, f):
+        m = np.ascontiguousarray(mask, dtype=np.uint8)
+        assert len(m) == self.n
+        return self.L.orc_set_flags_mask(C.byref(self.tree), _ptr(m, C.c_uint8), f)
     def change_flags(self, u, s): return self.L.orc_change_flags(C.byref(self.tree), u, s)
     def subdivide(self, f=8): return self.L.orc_subdivide(C.byref(self.tree), f)
     def remove(self, f): return self.L.orc_remove(C.byref(self.tree), f)
@@ -264,6 +271,51 @@ def invariant_measure(rowptr, cols, vals, iters=200):
     lib().orc_invariant_measure(n, _ptr(rowptr, C.c_uint32), _ptr(cols, C.c_uint32), _ptr(vals, C.c_double),
                                 iters, _ptr(v, C.c_double))
     return v
+
+
+def strong_components(rowptr, cols):
+    """Component label (largest vertex of the component) of every row's box."""
+    n = len(rowptr) - 1
+    rowptr = np.ascontiguousarray(rowptr, dtype=np.uint32)
+    cols = np.ascontiguousarray(cols, dtype=np.uint32)
+    comp = np.zeros(n, dtype=np.uint32)
+    lib().orc_strong_components(n, _ptr(rowptr, C.c_uint32), _ptr(cols, C.c_uint32), _ptr(comp, C.c_uint32))
+    return comp
+
+
+def chain_recurrent(spec: dict, steps: int):
+    """chainRecurrentSet.m:18-44: subdivide, transition matrix, keep the boxes of strongly
+    connected components with more than one box; returns the oracle and per-step counts."""
+    o = Oracle(spec)
+    o.set_flags(8)
+    counts = []
+    for _ in range(steps):
+        o.subdivide(8)
+        rowptr, cols, _, _ = o.transition_matrix()
+        comp = strong_components(rowptr, cols)
+        sizes = np.bincount(comp, minlength=len(comp))
+        o.set_flags_mask(sizes[comp] > 1, 1)
+        o.remove(1)
+        o.unset_flags(1)
+        counts.append(o.n)
+    return o, counts
+
+
+def nim_selection(spec: dict, steps: int, iters: int = 200):
+    """subdivisionByNim.m:22-66 with the FP64 power iteration for the eigenvector: keep the
+    boxes whose measure is at least 1e-9 / n; returns the oracle and per-step counts."""
+    o = Oracle(spec)
+    o.set_flags(8)
+    counts = []
+    for _ in range(steps):
+        o.subdivide(8)
+        rowptr, cols, vals, _ = o.transition_matrix()
+        v = invariant_measure(rowptr, cols, vals, iters)
+        o.set_flags_mask(v >= 1e-9 / len(v), 1)
+        o.remove(1)
+        o.unset_flags(1)
+        counts.append(o.n)
+    return o, counts
 
 
 def continuation(spec: dict, depth: int, x0, max_sweeps: int = 10_000):
