@@ -123,6 +123,8 @@ _SIGS = {
     "b12g_set_flags_by_measure": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_uint8, C.POINTER(C.c_uint32)]),
     "b12g_chain_recurrent_run": (C.c_int, [C.c_void_p, C.POINTER(Scheme), C.c_uint32, C.c_void_p]),
     "b12g_nim_run": (C.c_int, [C.c_void_p, C.POINTER(Scheme), C.c_uint32, C.c_uint32, C.c_void_p]),
+    "b12g_set_flags_by_self_hit": (C.c_int, [C.c_void_p, C.POINTER(Scheme), C.c_uint8, C.POINTER(C.c_uint32)]),
+    "b12g_fixed_boxes_run": (C.c_int, [C.c_void_p, C.POINTER(Scheme), C.c_uint32, C.c_void_p]),
     "b12g_tree_save_json": (C.c_int, [C.c_void_p, C.c_char_p]),
     "b12g_tree_load_json": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
     "b12g_csr_save_json": (C.c_int, [C.c_void_p, C.c_char_p]),

@@ -1,5 +1,5 @@
-// Strongly connected components of a transition graph, and the two selection steps that
-// consume a transition matrix:
+// Strongly connected components of a transition graph, the two selection steps that
+// consume a transition matrix, and the fixed-box selection of fixedBoxes.m:
 //   chain recurrent set: keep the boxes of strongly connected components with at least
 //     two boxes (chainRecurrentSet.m:18-44, graphconncomp on P')
 //   natural invariant measure: keep the boxes whose measure is at least 1e-9 / n
@@ -139,6 +139,22 @@ __global__ void flag_components_kernel(uint32_t n, const uint32_t* comp, const u
       flags[v] |= f;
       ++k;
     }
+  if (k) atomicAdd(count, k);
+}
+
+// a leaf one of whose own test points lands in it again (fixedBoxes.m:15-17)
+__global__ void flag_self_hit_kernel(uint32_t n, const uint32_t* target, uint32_t P, uint8_t* flags, uint8_t f,
+                                     uint32_t* count)
+{
+  uint32_t k = 0;
+  for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < n; b += gridDim.x * blockDim.x) {
+    bool self = false;
+    for (uint32_t q = 0; q < P && !self; ++q) self = target[size_t(b) * P + q] == b;
+    if (self) {
+      flags[b] |= f;
+      ++k;
+    }
+  }
   if (k) atomicAdd(count, k);
 }
 
@@ -295,6 +311,45 @@ b12g_status b12g_set_flags_by_measure(b12g_tree* t, b12g_csr* m, double threshol
   CK(cudaStreamSynchronize(s));
   word.release();
   if (n_flagged) *n_flagged = k;
+  return B12G_OK;
+}
+
+b12g_status b12g_set_flags_by_self_hit(b12g_tree* t, const b12g_scheme* sc, uint8_t flags, uint32_t* n_flagged)
+{
+  if (!t || !sc) return fail(B12G_ERR_INVALID, "NULL argument");
+  if (sc->flags_to_check != 0 || (sc->depth != B12G_LEAF_DEPTH && sc->depth != t->depth))
+    return fail(B12G_ERR_INVALID, "the self-hit selection images every leaf");
+  Prepared pr;
+  ST(prepare(t, sc, pr));
+  uint32_t n_src = 0;
+  ST(select_sources(t, sc, pr, n_src));
+  const uint64_t np = uint64_t(n_src) * pr.P;
+  ST(t->out.ensure(std::max<uint64_t>(np, 1), "search output"));
+  ST(build_current_hash(t, pr));
+  pr.a.out = t->out.p;
+  CK(launch_image(sc->map.kind, sc->map.arith, sc->grid.kind, t->domain.dim, ImageMode::Search, pr.a, np, t->stream));
+  ST(set_ctr(t, C_TMP, 0));
+  flag_self_hit_kernel<<<grid_for_n(n_src), kThreads, 0, t->stream>>>(n_src, t->out.p, uint32_t(pr.P), t->flg(), flags,
+                                                                     t->ctr.p + C_TMP);
+  count_launches(2);
+  ST(read_ctr(t, C_TMP, 1));
+  if (n_flagged) *n_flagged = t->h_ctr[C_TMP];
+  return B12G_OK;
+}
+
+b12g_status b12g_fixed_boxes_run(b12g_tree* t, const b12g_scheme* sc, uint32_t steps, uint32_t* counts)
+{
+  if (!t || !sc) return fail(B12G_ERR_INVALID, "NULL argument");
+  uint32_t k = 0;
+  ST(b12g_delete_depth(t, 0, &k));
+  ST(b12g_set_flags(t, B12G_SD, B12G_LEAF_DEPTH, &k));
+  for (uint32_t i = 0; i < steps; ++i) {
+    ST(b12g_subdivide(t, B12G_SD, &k));
+    ST(b12g_set_flags_by_self_hit(t, sc, B12G_HIT, &k));
+    ST(b12g_remove(t, B12G_HIT, &k));
+    ST(b12g_unset_flags(t, B12G_HIT, B12G_LEAF_DEPTH, &k));
+    if (counts) ST(b12g_count(t, B12G_LEAF_DEPTH, counts + i));
+  }
   return B12G_OK;
 }
 

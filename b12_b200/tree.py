@@ -422,6 +422,20 @@ class ImplicitBoxTree:
         check(lib().b12g_nim_run(self._h, C.byref(s), steps, power_iterations, counts.ctypes.data), "nim_run")
         return counts[:steps]
 
+    def set_flags_by_self_hit(self, scheme: Scheme, flags: int) -> int:
+        """fixedBoxes.m:15-17: flag the leaves one of whose own test points lands in them again."""
+        k = C.c_uint32()
+        s = scheme.to_c()
+        check(lib().b12g_set_flags_by_self_hit(self._h, C.byref(s), flags, C.byref(k)), "set_flags_by_self_hit")
+        return k.value
+
+    def fixed_boxes_run(self, scheme: Scheme, steps: int) -> np.ndarray:
+        """fixedBoxes.m:10-22 on the GPU; leaf counts after each step."""
+        counts = np.zeros(max(steps, 1), dtype=np.uint32)
+        s = scheme.to_c()
+        check(lib().b12g_fixed_boxes_run(self._h, C.byref(s), steps, counts.ctypes.data), "fixed_boxes_run")
+        return counts[:steps]
+
     def subdivision_run(self, scheme: Scheme, steps: int) -> np.ndarray:
         counts = np.zeros(max(steps, 1), dtype=np.uint32)
         s = scheme.to_c()

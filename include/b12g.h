@@ -233,6 +233,13 @@ b12g_status b12g_set_flags_by_measure(b12g_tree* tree, b12g_csr* matrix, double 
 /* the two drivers: setFlags(SD); steps x {subdivide(SD); transition matrix; select with
  * HIT; remove(HIT); unsetFlags(HIT)}; counts: leaves after each step (may be NULL) */
 b12g_status b12g_chain_recurrent_run(b12g_tree* tree, const b12g_scheme* scheme, uint32_t steps, uint32_t* counts);
+/* fixedBoxes.m:15-17: flag every leaf one of whose own test points lands in it again
+ * (search(scheme), then any(s == box index) per box) */
+b12g_status b12g_set_flags_by_self_hit(b12g_tree* tree, const b12g_scheme* scheme, uint8_t flags,
+                                       uint32_t* n_flagged);
+/* fixedBoxes.m:10-22: deleteDepth(0); setFlags(SD); steps x {subdivide(SD); self-hit
+ * selection with HIT; remove(HIT); unsetFlags(HIT)} */
+b12g_status b12g_fixed_boxes_run(b12g_tree* tree, const b12g_scheme* scheme, uint32_t steps, uint32_t* counts);
 b12g_status b12g_nim_run(b12g_tree* tree, const b12g_scheme* scheme, uint32_t steps, uint32_t power_iterations,
                          uint32_t* counts);
 

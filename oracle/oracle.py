@@ -318,6 +318,24 @@ def nim_selection(spec: dict, steps: int, iters: int = 200):
     return o, counts
 
 
+def fixed_boxes(spec: dict, steps: int):
+    """fixedBoxes.m:10-22: keep the boxes one of whose own test points lands in them
+    again; returns the oracle and per-step counts."""
+    o = Oracle(spec)
+    o.delete_depth0()
+    o.set_flags(8)
+    counts = []
+    P = o.points_per_box()
+    for _ in range(steps):
+        o.subdivide(8)
+        s = o.search_by_image().reshape(-1, P)
+        o.set_flags_mask((s == np.arange(len(s), dtype=s.dtype)[:, None]).any(axis=1), 1)
+        o.remove(1)
+        o.unset_flags(1)
+        counts.append(o.n)
+    return o, counts
+
+
 def continuation(spec: dict, depth: int, x0, max_sweeps: int = 10_000):
     """continuation.m:13-44 at one depth; returns the oracle and per-sweep counts."""
     o = Oracle(spec)

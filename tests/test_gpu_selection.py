@@ -1,6 +1,6 @@
-"""GPU: strongly connected components of transition graphs and the two selection drivers
-that use a transition matrix (chain recurrent set, natural invariant measure) against the
-oracle: Tarjan's algorithm and the same loops on the CPU."""
+"""GPU: strongly connected components of transition graphs, the two selection drivers
+that use a transition matrix (chain recurrent set, natural invariant measure) and the
+fixed-box driver, against the oracle: Tarjan's algorithm and the same loops on the CPU."""
 import numpy as np
 import pytest
 
@@ -77,6 +77,18 @@ def test_nim_run_matches_oracle():
     t = B.ImplicitBoxTree(c, r)
     counts = t.nim_run(scheme(spec), 14, 200)
     o, ocounts = O.nim_selection(oracle_spec(spec), 14, 200)
+    assert list(counts) == ocounts
+    for x, y in zip(t.leaves(), o.leaves()):
+        np.testing.assert_array_equal(x, y)
+
+
+@pytest.mark.parametrize("spec,steps", [(dict(map="henon"), 16), (dict(map="lorenz", rho=28.0, grid=5), 14),
+                                        (dict(map="forced_duffing", grid=4), 12)])
+def test_fixed_boxes_run_matches_oracle(spec, steps):
+    c, r = domain(spec)
+    t = B.ImplicitBoxTree(c, r)
+    counts = t.fixed_boxes_run(scheme(spec), steps)
+    o, ocounts = O.fixed_boxes(oracle_spec(spec), steps)
     assert list(counts) == ocounts
     for x, y in zip(t.leaves(), o.leaves()):
         np.testing.assert_array_equal(x, y)
