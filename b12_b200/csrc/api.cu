@@ -76,6 +76,7 @@ b12g_status reserve(b12g_tree* t, uint64_t n_boxes)
   for (int b = 0; b < 2; ++b) {
     ST(t->code[b].grow_keep(n_boxes, b == t->cur ? keep : 0, t->stream, "leaf codes"));
     ST(t->flags[b].grow_keep(n_boxes, b == t->cur ? keep : 0, t->stream, "leaf flags"));
+    if (t->mixed) ST(t->dep[b].grow_keep(n_boxes, b == t->cur ? keep : 0, t->stream, "leaf depths"));
   }
   if (t->hit.n < n_boxes) {
     ST(t->hit.ensure(n_boxes, "hit mask"));
@@ -205,6 +206,7 @@ b12g_status set_root(b12g_tree* t, uint8_t flags)
   CK(cudaMemsetAsync(t->flg(), flags, 1, t->stream));
   t->n = 1;
   t->depth = 0;
+  t->mixed = false;
   ST(set_ctr(t, t->ncur, 1));
   return sync(t, "set root");
 }
@@ -212,6 +214,8 @@ b12g_status set_root(b12g_tree* t, uint8_t flags)
 b12g_status flag_call(b12g_tree* t, int op, uint8_t u, uint8_t f, uint8_t depth, uint32_t* n_changed)
 {
   if (!t) return fail(B12G_ERR_INVALID, "NULL tree");
+  if (t->mixed && depth != 0 && depth != B12G_LEAF_DEPTH)
+    return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "flags of a tree of mixed depths change at depth 0 or 255");
   if (depth != 0) ST(check_depth(t, depth));
   ST(set_ctr(t, C_CHANGED, 0));
   CK(flag_op(t->flg(), t->dn(), op, u, f, t->ctr.p + C_CHANGED, t->n, t->stream));
@@ -368,7 +372,8 @@ b12g_status b12g_tree_destroy(b12g_tree* t)
     for (cudaEvent_t e : t->prof_events[k]) cudaEventDestroy(e);
     for (cudaEvent_t e : t->graph_prof[k]) cudaEventDestroy(e);
   }
-  for (int b = 0; b < 2; ++b) { t->code[b].release(); t->flags[b].release(); }
+  for (int b = 0; b < 2; ++b) { t->code[b].release(); t->flags[b].release(); t->dep[b].release(); }
+  t->cmp.release(); t->hash.release(); t->points.release();
   t->hit.release(); t->ctr.release(); t->tiles_a.release(); t->tiles_b.release();
   t->src.release(); t->out.release(); t->stage_col.release(); t->stage_cnt.release();
   t->row_count.release(); t->rowptr.release(); t->cand.release(); t->cand2.release();
@@ -389,6 +394,7 @@ b12g_status b12g_tree_reserve(b12g_tree* t, uint64_t n_boxes)
 b12g_status b12g_count(b12g_tree* t, uint8_t depth, uint32_t* count)
 {
   if (!t || !count) return fail(B12G_ERR_INVALID, "NULL argument");
+  if (t->mixed) return mixed_count(t, depth, count);
   // count(depth) (ImplicitBoxTree.hpp:1061-1095) for a uniform-depth tree
   if (depth == 0) *count = 1;
   else if (depth == B12G_LEAF_DEPTH || depth == t->depth) *count = t->n;
@@ -407,6 +413,7 @@ b12g_status b12g_depth(b12g_tree* t, uint8_t* depth)
 b12g_status b12g_leaves(b12g_tree* t, uint64_t* codes, uint8_t* depths, uint8_t* flags)
 {
   if (!t) return fail(B12G_ERR_INVALID, "NULL tree");
+  if (t->mixed) return mixed_leaves(t, codes, depths, flags);
   if (codes) CK(cudaMemcpyAsync(codes, t->codes(), size_t(t->n) * 8, cudaMemcpyDeviceToHost, t->stream));
   if (flags) CK(cudaMemcpyAsync(flags, t->flg(), t->n, cudaMemcpyDeviceToHost, t->stream));
   ST(sync(t, "leaves"));
@@ -421,8 +428,9 @@ b12g_status b12g_load_leaves(b12g_tree* t, const uint64_t* codes, const uint8_t*
   if (n == 0) return set_root(t, B12G_NONE);
   const uint8_t d = depths[0];
   if (d > 64) return fail(B12G_ERR_INVALID, "depth %u above the maximal depth 64", d);
+  for (uint32_t i = 1; i < n; ++i)
+    if (depths[i] != d) return mixed_load(t, codes, depths, flags, n);
   for (uint32_t i = 0; i < n; ++i) {
-    if (depths[i] != d) return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "leaves of mixed depth");
     if (d < 64 && (codes[i] >> d) != 0) return fail(B12G_ERR_INVALID, "code %u has bits above its depth", i);
     if (i && codes[i] <= codes[i - 1]) return fail(B12G_ERR_INVALID, "codes must be sorted and unique");
   }
@@ -431,6 +439,7 @@ b12g_status b12g_load_leaves(b12g_tree* t, const uint64_t* codes, const uint8_t*
   CK(cudaMemcpyAsync(t->flg(), flags, n, cudaMemcpyHostToDevice, t->stream));
   t->n = n;
   t->depth = d;
+  t->mixed = false;
   ST(set_ctr(t, t->ncur, n));
   return sync(t, "load leaves");
 }
@@ -455,18 +464,21 @@ b12g_status b12g_change_flags(b12g_tree* t, uint8_t to_unset, uint8_t to_set, ui
 b12g_status b12g_subdivide(b12g_tree* t, uint8_t flags, uint32_t* n_subdivided)
 {
   if (!t) return fail(B12G_ERR_INVALID, "NULL tree");
-  // IsSubdividableFunctor (Functors.hpp:332-335): all flags set and depth < 64
+  if (t->mixed) return mixed_subdivide(t, flags, n_subdivided);
+  // subdivide (ImplicitBoxTree.hpp:2884-2929) returns the number of leaves with all
+  // flags set; IsSubdividableFunctor (Functors.hpp:332-335) splits those below depth 64
   uint32_t m = 0;
-  if (t->depth < 64) {
-    ST(set_ctr(t, C_TMP, 0));
-    CK(count_flags(t->flg(), t->dn(), flags, t->ctr.p + C_TMP, t->n, t->stream));
-    count_launches(1);
-    ST(read_ctr(t, C_TMP, 1));
-    m = t->h_ctr[C_TMP];
+  ST(set_ctr(t, C_TMP, 0));
+  CK(count_flags(t->flg(), t->dn(), flags, t->ctr.p + C_TMP, t->n, t->stream));
+  count_launches(1);
+  ST(read_ctr(t, C_TMP, 1));
+  m = t->h_ctr[C_TMP];
+  if (m != 0 && m != t->n && t->depth < 64) {
+    // some leaves split: the tree's leaves get two depths
+    ST(mixed_enter(t));
+    return mixed_subdivide(t, flags, n_subdivided);
   }
-  if (m != 0 && m != t->n)
-    return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "subdividing %u of %u leaves would mix depths", m, t->n);
-  if (m == t->n) {
+  if (m == t->n && t->depth < 64) {
     ST(reserve(t, 2ull * t->n));
     const int o = 1 - t->cur, no = 1 - t->ncur;
     CK(split_codes(t->codes(), t->flg(), t->dn(), t->code[o].p, t->flags[o].p, t->ctr.p + no, t->n, t->stream));
@@ -484,6 +496,7 @@ b12g_status b12g_subdivide(b12g_tree* t, uint8_t flags, uint32_t* n_subdivided)
 b12g_status b12g_remove(b12g_tree* t, uint8_t flags, uint32_t* n_removed)
 {
   if (!t) return fail(B12G_ERR_INVALID, "NULL tree");
+  if (t->mixed) return mixed_remove(t, flags, n_removed);
   const int o = 1 - t->cur, no = 1 - t->ncur;
   CompactArgs ca{};
   ca.code = t->codes();
@@ -519,7 +532,7 @@ b12g_status b12g_delete_depth(b12g_tree* t, uint8_t depth, uint32_t* n_deleted)
   } else if (depth == B12G_LEAF_DEPTH || depth > t->depth) {
     c = 0;
   } else {
-    return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "deleteDepth(%u) of a depth-%u tree", depth, t->depth);
+    return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "deleteDepth(%u) of a tree of depth %u", depth, t->depth);
   }
   if (n_deleted) *n_deleted = c;
   return B12G_OK;
@@ -530,6 +543,7 @@ b12g_status b12g_set_flags_by_image(b12g_tree* t, const b12g_scheme* sc, uint8_t
                                     uint32_t* n_changed)
 {
   if (!t) return fail(B12G_ERR_INVALID, "NULL tree");
+  if (t->mixed) return mixed_set_flags_by_image(t, sc, flags, depth, n_changed);
   ST(check_depth(t, depth));
   Prepared pr;
   ST(prepare(t, sc, pr));
@@ -555,6 +569,18 @@ b12g_status b12g_search_by_image(b12g_tree* t, const b12g_scheme* sc, uint8_t de
                                  uint64_t* n_points)
 {
   if (!t) return fail(B12G_ERR_INVALID, "NULL tree");
+  if (t->mixed) {
+    if (depth != B12G_LEAF_DEPTH)
+      return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "a tree of mixed depths is searched at its leaves (255)");
+    uint64_t np = 0;
+    ST(mixed_search(t, sc, &np));
+    if (n_points) *n_points = np;
+    if (!out) return sync(t, "search_by_image");
+    if (capacity < np) return fail(B12G_ERR_CAPACITY, "output holds %llu of %llu points", (unsigned long long)capacity,
+                                   (unsigned long long)np);
+    CK(cudaMemcpyAsync(out, t->out.p, np * 4, cudaMemcpyDeviceToHost, t->stream));
+    return sync(t, "search_by_image");
+  }
   ST(check_depth(t, depth));
   Prepared pr;
   ST(prepare(t, sc, pr));
@@ -591,20 +617,26 @@ b12g_status b12g_transition_matrix(b12g_tree* t, const b12g_scheme* sc, int abso
   ST(t->stage_cnt.ensure(stage, "row staging"));
   ST(t->row_count.ensure(n + 1, "row counts"));
   ST(t->rowptr.ensure(n + 1, "row pointers"));
-  ST(build_current_hash(t, pr));
-  RowArgs ra{};
-  ra.img = pr.a;
-  ra.stage_col = t->stage_col.p;
-  ra.stage_cnt = t->stage_cnt.p;
-  ra.row_count = t->row_count.p;
-  ra.keep_lost = invalid_column ? 1 : 0;
-  ra.lost_col = n + 1;  // ImplicitBoxTree.hpp:3075-3090: nColumns += 1, lost entries get index nColumns
-  prof_mark(t, 1);
-  CK(launch_rows(sc->map.kind, sc->map.arith, sc->grid.kind, t->domain.dim, ra, n, t->stream));
-  prof_mark(t, 1);
+  if (t->mixed) {
+    prof_mark(t, 1);
+    ST(mixed_rows(t, sc, invalid_column));
+    prof_mark(t, 1);
+  } else {
+    ST(build_current_hash(t, pr));
+    RowArgs ra{};
+    ra.img = pr.a;
+    ra.stage_col = t->stage_col.p;
+    ra.stage_cnt = t->stage_cnt.p;
+    ra.row_count = t->row_count.p;
+    ra.keep_lost = invalid_column ? 1 : 0;
+    ra.lost_col = n + 1;  // ImplicitBoxTree.hpp:3075-3090: nColumns += 1, lost entries get index nColumns
+    prof_mark(t, 1);
+    CK(launch_rows(sc->map.kind, sc->map.arith, sc->grid.kind, t->domain.dim, ra, n, t->stream));
+    prof_mark(t, 1);
+  }
   CK(exclusive_scan_u32(t->row_count.p, t->rowptr.p, t->dn(), t->tiles_a.p, n, t->stream));
   CK(cudaMemcpyAsync(t->h_ctr + C_NNZ, t->rowptr.p + n, 4, cudaMemcpyDeviceToHost, t->stream));
-  count_launches(4);
+  count_launches(t->mixed ? 3 : 4);   // mixed_rows counts its own launches
   ST(sync(t, "transition rows"));
   ST(prof_collect(t));
   const uint32_t nnz32 = t->h_ctr[C_NNZ];
@@ -758,6 +790,18 @@ b12g_status b12g_subdivision_run(b12g_tree* t, const b12g_scheme* sc, uint32_t s
   if (int(t->depth) + int(steps) > 64) return fail(B12G_ERR_INVALID, "depth would exceed 64");
   // setFlags(SD) on every leaf (subdivision.m:16, B12_doc.tex:266)
   ST(flag_call(t, 0, 0, B12G_SD, B12G_LEAF_DEPTH, nullptr));
+  if (t->mixed) {
+    // leaves of several depths: the steps of subdivision.m:18-45 one call at a time
+    uint32_t k = 0;
+    for (uint32_t s = 0; s < steps; ++s) {
+      ST(b12g_subdivide(t, B12G_SD, &k));
+      ST(b12g_set_flags_by_image(t, sc, B12G_HIT, B12G_LEAF_DEPTH, &k));
+      ST(b12g_remove(t, B12G_HIT, &k));
+      ST(b12g_unset_flags(t, B12G_HIT, B12G_LEAF_DEPTH, &k));
+      if (counts) counts[s] = t->n;
+    }
+    return B12G_OK;
+  }
 
   // keep the initial state so that a capacity overflow can be retried with more room
   const uint32_t n0 = t->n;

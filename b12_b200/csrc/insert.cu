@@ -131,6 +131,7 @@ b12g_status insert_points_impl(b12g_tree* t, const double* points, uint64_t n_po
 {
   if (!t || (!points && n_points)) return fail(B12G_ERR_INVALID, "NULL argument");
   if (n_points > 0xFFFFFFF0ull) return fail(B12G_ERR_CAPACITY, "too many points");
+  if (t->mixed) return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "insertion into a tree of mixed depths");
   if (depth == B12G_LEAF_DEPTH) return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "insertion at the leaf depth -1");
   if (depth > 64) return fail(B12G_ERR_INVALID, "depth above 64");
   const bool root_only = t->n == 1 && t->depth == 0;
@@ -202,6 +203,7 @@ b12g_status insert_by_image_impl(b12g_tree* t, const b12g_scheme* sc, uint8_t de
                                  uint32_t* n_inserted)
 {
   if (!t || !sc) return fail(B12G_ERR_INVALID, "NULL argument");
+  if (t->mixed) return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "insertion into a tree of mixed depths");
   if (depth != t->depth || t->depth == 0)
     return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "insertion of images at depth %u into a depth-%u tree", depth,
                 t->depth);

@@ -329,9 +329,6 @@ b12g_status b12g_tree_load_json(const char* path, b12g_tree** out)
   ST(read_tree(path, f));
   const uint64_t n = f.codes.size();
   if (n == 0 || n > 0xFFFFFFFEull) return fail(B12G_ERR_INVALID, "%s: %llu leaves", path, (unsigned long long)n);
-  for (uint64_t i = 1; i < n; ++i)
-    if (f.depths[i] != f.depths[0])
-      return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "%s: leaves of different depths", path);
   std::vector<uint64_t> codes(f.codes);
   std::vector<uint8_t> depths(n), flags(n);
   for (uint64_t i = 0; i < n; ++i) {

@@ -319,6 +319,18 @@ b12g_status b12g_set_flags_by_self_hit(b12g_tree* t, const b12g_scheme* sc, uint
   if (!t || !sc) return fail(B12G_ERR_INVALID, "NULL argument");
   if (sc->flags_to_check != 0 || (sc->depth != B12G_LEAF_DEPTH && sc->depth != t->depth))
     return fail(B12G_ERR_INVALID, "the self-hit selection images every leaf");
+  if (t->mixed) {
+    uint64_t np = 0;
+    ST(mixed_search(t, sc, &np));
+    const uint32_t P = t->n ? uint32_t(np / t->n) : 0u;
+    ST(set_ctr(t, C_TMP, 0));
+    flag_self_hit_kernel<<<grid_for_n(t->n), kThreads, 0, t->stream>>>(t->n, t->out.p, P, t->flg(), flags,
+                                                                      t->ctr.p + C_TMP);
+    count_launches(1);
+    ST(read_ctr(t, C_TMP, 1));
+    if (n_flagged) *n_flagged = t->h_ctr[C_TMP];
+    return B12G_OK;
+  }
   Prepared pr;
   ST(prepare(t, sc, pr));
   uint32_t n_src = 0;

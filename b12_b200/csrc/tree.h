@@ -113,6 +113,10 @@ struct b12g_tree {
   Buf<double> points;
   Buf<uint32_t> step_counts;
   Buf<uint8_t> sort_tmp;
+  // leaves of different depths: per-leaf depths (with code/flags) and comparable patterns
+  bool mixed = false;
+  Buf<uint8_t> dep[2];
+  Buf<uint64_t> cmp;
   Buf<ulonglong2> hash;        // leaf lookup table
   uint32_t hash_tag = 0;       // tag of the last build (1..255; 0 = cleared)
   uint32_t hash_log2 = 0;      // log2 of the table's slots
@@ -181,6 +185,21 @@ void prof_mark(b12g_tree* t, int kind);
 b12g_status prof_collect(b12g_tree* t);
 // P^T of a matrix and its row classes, built on first use (api.cu)
 b12g_status ensure_transpose(b12g_csr* m);
+
+// trees of mixed leaf depths (mixed.cu); t->mixed selects them, t->depth is the deepest leaf
+b12g_status mixed_enter(b12g_tree* t);
+b12g_status mixed_settle(b12g_tree* t);
+b12g_status mixed_load(b12g_tree* t, const uint64_t* codes, const uint8_t* depths, const uint8_t* flags, uint32_t n);
+b12g_status mixed_count(b12g_tree* t, uint8_t depth, uint32_t* count);
+b12g_status mixed_leaves(b12g_tree* t, uint64_t* codes, uint8_t* depths, uint8_t* flags);
+b12g_status mixed_subdivide(b12g_tree* t, uint8_t flags, uint32_t* n_subdivided);
+b12g_status mixed_remove(b12g_tree* t, uint8_t flags, uint32_t* n_removed);
+b12g_status mixed_set_flags_by_image(b12g_tree* t, const b12g_scheme* sc, uint8_t flags, uint8_t depth,
+                                     uint32_t* n_changed);
+// target leaf of every point of the scheme's source leaves into t->out; *n_points of them
+b12g_status mixed_search(b12g_tree* t, const b12g_scheme* sc, uint64_t* n_points);
+// transition rows of every leaf into t->stage_col / stage_cnt / row_count
+b12g_status mixed_rows(b12g_tree* t, const b12g_scheme* sc, int invalid_column);
 
 }  // namespace host
 }  // namespace b12g

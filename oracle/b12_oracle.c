@@ -419,8 +419,12 @@ static void sort_tree(orc_tree* t)
  * 234-239); flags are inherited; the result is re-sorted */
 uint32_t orc_subdivide(orc_tree* t, uint8_t flags)
 {
-  uint64_t n = t->n, m = 0;
-  for (uint64_t i = 0; i < n; ++i) m += flags_set(t->flags[i], flags) && t->depth[i] < 64;
+  /* returns countIfFlags(flags) over the leaves; leaves at depth 64 stay whole */
+  uint64_t n = t->n, m = 0, flagged = 0;
+  for (uint64_t i = 0; i < n; ++i) {
+    flagged += flags_set(t->flags[i], flags);
+    m += flags_set(t->flags[i], flags) && t->depth[i] < 64;
+  }
   tree_reserve(t, n + m);
   uint64_t k = n;
   for (uint64_t i = 0; i < n; ++i) {
@@ -435,7 +439,7 @@ uint32_t orc_subdivide(orc_tree* t, uint8_t flags)
   }
   t->n = n + m;
   sort_tree(t);
-  return (uint32_t)m;
+  return (uint32_t)flagged;
 }
 
 /* remove (ImplicitBoxTree.hpp:2344-2371): keep leaves that have all `flags` set */

@@ -36,6 +36,7 @@ struct RunOpts
   int tm = 1;                 // 0: none, 1: relative, 2: absolute, 3: relative + invalid column
   std::string save;           // save the final tree and matrix as JSON (save(): ImplicitBoxTree.hpp:435-528,
                               // CooMatrix.hpp:473-525) to SAVE_tree.json / SAVE_tm.json
+  int mixed = 0;              // steps of selective refinement after the uniform steps (mixed leaf depths)
 };
 
 inline RunOpts parseOpts(int argc, char** argv)
@@ -47,7 +48,50 @@ inline RunOpts parseOpts(int argc, char** argv)
   o.dumpFrom = std::atoi(arg(argc, argv, "--dump-from", "0"));
   o.tm = std::atoi(arg(argc, argv, "--tm", "1"));
   o.save = arg(argc, argv, "--save", "");
+  o.mixed = std::atoi(arg(argc, argv, "--mixed", "0"));
   return o;
+}
+
+// Selective refinement: SD stays only on the leaves in the lower half of the first
+// coordinate (the first bisection bit is 0), set through setFlagsByStencil; then
+// o.mixed steps of subdivide(SD) + image selection run on a tree whose leaves have
+// different depths.  mixed_00.bin holds the flagged starting tree, mixed_KK.bin the
+// tree after step KK.
+template<class Tree, class Grid, class Map>
+void runMixed(Tree& ibt, Grid grid, Map map, const RunOpts& o, std::ostringstream& js, uint64_t& boxImages)
+{
+  using namespace b12;
+  ibt.unsetFlags(Flag::SD, getLeafDepth());
+  const uint64_t n = ibt.size();
+  ThrustSystem<OMP>::Vector<bool> lower(n);
+  uint64_t i = 0;
+  for (auto it = ibt.begin(); it != ibt.end(); ++it, ++i) {
+    auto b = *it;
+    const uint64_t code = thrust::get<0>(b);
+    const int depth = thrust::get<1>(b);
+    lower[i] = depth > 0 && (code >> (depth - 1)) == 0;
+  }
+  ibt.setFlagsByStencil(lower.begin(), Flag::SD, getLeafDepth());
+  if (!o.out.empty()) dumpLeaves(ibt, o.out + "/mixed_00.bin");
+  js << ", \"mixed\": [";
+  for (int k = 1; k <= o.mixed; ++k) {
+    auto a = clk::now();
+    ibt.subdivide(Flag::SD);
+    boxImages += ibt.count(getLeafDepth());
+    auto itPair = ibt.makePointIteratorPairOverLeaves(grid, map);
+    ibt.setFlagsByIterators(itPair, Flag::HIT, getLeafDepth());
+    ibt.remove(Flag::HIT);
+    ibt.unsetFlags(Flag::HIT, getLeafDepth());
+    auto b = clk::now();
+    js << (k > 1 ? ", " : "") << "[" << k << ", " << ibt.count(getLeafDepth()) << ", " << int(ibt.depth()) << ", "
+       << secs(a, b) << "]";
+    if (!o.out.empty()) {
+      char fn[64];
+      std::snprintf(fn, sizeof fn, "/mixed_%02d.bin", k);
+      dumpLeaves(ibt, o.out + fn);
+    }
+  }
+  js << "]";
 }
 
 template<b12::Dimension DIM, class Grid, class Map>
@@ -80,8 +124,10 @@ int runSubdivision(const std::vector<double>& c, const std::vector<double>& r,
       dumpLeaves(ibt, o.out + fn);
     }
   }
+  js << "]";
+  if (o.mixed > 0) runMixed(ibt, grid, map, o, js, boxImages);
   auto t1 = clk::now();
-  js << "], \"subdivision_s\": " << secs(t0, t1) << ", \"box_images\": " << boxImages;
+  js << ", \"subdivision_s\": " << secs(t0, t1) << ", \"box_images\": " << boxImages;
   if (!o.save.empty()) ibt.save(o.save + "_tree.json");
   if (o.tm) {
     const bool absolute = (o.tm == 2), invalid = (o.tm == 3);

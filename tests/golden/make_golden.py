@@ -51,6 +51,15 @@ WORKLOADS = {
                              dict(map="henon", a=1.4, b=0.3, grid=4, steps=10, invalid=True, save=True)),
     "lorenz_d9_files": ("ref_lorenz", ["--steps", "9", "--tm", "1", "--buf", "4294967296"],
                         dict(map="lorenz", rho=28.0, grid=5, steps=9, save=True)),
+    # selective refinement after uniform steps: trees whose leaves have different depths
+    "henon_d14_mixed8": ("ref_henon", ["--steps", "14", "--mixed", "8", "--tm", "1"],
+                         dict(map="henon", a=1.4, b=0.3, grid=4, steps=14, mixed=8)),
+    "lorenz_d15_mixed6_lost": ("ref_lorenz", ["--steps", "15", "--mixed", "6", "--tm", "3"],
+                               dict(map="lorenz", rho=28.0, grid=5, steps=15, mixed=6, invalid=True)),
+    "forced_duffing_d12_mixed5": ("ref_forced", ["--steps", "12", "--mixed", "5", "--tm", "2"],
+                                  dict(map="forced_duffing", grid=4, steps=12, mixed=5, absolute=True)),
+    "henon_d8_mixed4_files": ("ref_henon", ["--steps", "8", "--mixed", "4", "--tm", "1", "--buf", "4294967296"],
+                              dict(map="henon", a=1.4, b=0.3, grid=4, steps=8, mixed=4, save=True)),
     "coupled_duffing_cont_d8": ("ref_duffing", ["--steps", "8"], dict(map="coupled_duffing", points=64, seed=0,
                                                                           depth=8)),
     "coupled_duffing_cont_d12": ("ref_duffing", ["--steps", "12"], dict(map="coupled_duffing", points=64, seed=0,
@@ -108,6 +117,17 @@ def generate(name: str) -> None:
         is_cont = binary == "ref_duffing"
         prefix = "cont_" if is_cont else "leaves_"
         files = sorted(f for f in os.listdir(tmp) if f.startswith(prefix))
+        # selective refinement (--mixed K): mixed_00 is the flagged start, mixed_KK step KK
+        for fn in sorted(f for f in os.listdir(tmp) if f.startswith("mixed_")):
+            k = int(fn[len("mixed_"):-4])
+            codes, depth, flags = read_leaves(os.path.join(tmp, fn))
+            out.setdefault("mixed", []).append(dict(step=k, n=int(len(codes)), max_depth=int(depth.max()),
+                                                    min_depth=int(depth.min()), codes_sha256=sha(codes),
+                                                    depth_sha256=sha(depth), flags_sha256=sha(flags)))
+            if k == 0 or len(codes) <= FULL_LIMIT:
+                arrays[f"mixed_codes_{k:02d}"] = codes
+                arrays[f"mixed_depth_{k:02d}"] = depth
+                arrays[f"mixed_flags_{k:02d}"] = flags
         for fn in files:
             k = int(fn[len(prefix):-4])
             codes, depth, flags = read_leaves(os.path.join(tmp, fn))

@@ -60,14 +60,30 @@ def test_loaded_matrix_gives_the_same_measure():
     np.testing.assert_array_equal(loaded.invariant_measure(200), m.invariant_measure(200))
 
 
-def test_mixed_depth_file_is_refused(tmp_path):
+def test_mixed_depth_files_round_trip_byte_for_byte(tmp_path):
+    """A tree whose leaves have different depths (written by the reference's save) loads,
+    saves back to the same bytes, and gives the reference's transition-matrix file."""
+    t = B.ImplicitBoxTree.load(os.path.join(FILES, "henon_d8_mixed4_files_tree.json"))
+    codes, depths, flags = t.leaves()
+    assert depths.min() == 8 and depths.max() == 12 and t.depth() == 12
+    t.save(tmp_path / "tree")
+    t.transition_matrix(B.Scheme(B.henon(), B.inner_grid(4))).save(tmp_path / "tm.json")
+    for part in ("tree", "tm"):
+        with open(os.path.join(FILES, f"henon_d8_mixed4_files_{part}.json"), "rb") as f:
+            want = f.read()
+        with open(tmp_path / f"{part}.json", "rb") as f:
+            assert f.read() == want, part
+
+
+def test_nested_leaves_are_refused(tmp_path):
     from b12_b200 import tree as T
     c, r, codes, depths, flags = T.json_read_leaves(os.path.join(FILES, "henon_d8_files_tree.json"))
-    # the first two leaves (codes 0 and 1 at depth 8) merged into their parent at depth 7
-    codes = np.concatenate([[0], codes[2:]]).astype(np.uint64)
-    depths = np.concatenate([[7], depths[2:]]).astype(np.uint8)
-    flags = np.concatenate([[flags[0]], flags[2:]]).astype(np.uint8)
-    T.json_write_leaves(tmp_path / "mixed.json", c, r, codes, depths, flags)
+    # a depth-7 box in front of its own depth-8 half: the leaves overlap
+    parent = codes[0] >> np.uint64(1)
+    codes = np.concatenate([[parent], codes]).astype(np.uint64)
+    depths = np.concatenate([[7], depths]).astype(np.uint8)
+    flags = np.concatenate([[flags[0]], flags]).astype(np.uint8)
+    T.json_write_leaves(tmp_path / "nested.json", c, r, codes, depths, flags)
     with pytest.raises(B.B12gError) as e:
-        B.ImplicitBoxTree.load(tmp_path / "mixed.json")
-    assert e.value.status == B._lib.ERR_MIXED_DEPTH
+        B.ImplicitBoxTree.load(tmp_path / "nested.json")
+    assert e.value.status == B._lib.ERR_INVALID

@@ -1,0 +1,218 @@
+"""GPU: trees whose leaves have different depths, through the C ABI, against the
+reference's selective-refinement runs (tests/golden, `--mixed K`) and the oracle.
+
+The start state is the reference's uniform tree with SD kept on the leaves in the lower
+half of the first coordinate; subdivide(SD) then gives the tree two depths, and every
+further step deepens the flagged part only.  Leaves (codes, depths, flags), counts and
+transition matrices must be bit-exact."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from workloads import csr_digests, domain, oracle_spec, scheme, sha
+
+pytestmark = pytest.mark.gpu
+
+B = pytest.importorskip("b12_b200")
+
+CASES = ["henon_d14_mixed8", "lorenz_d15_mixed6_lost", "forced_duffing_d12_mixed5", "henon_d8_mixed4_files"]
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _device():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+def start(meta, arrays):
+    spec = meta["spec"]
+    c, r = domain(spec)
+    t = B.ImplicitBoxTree(c, r)
+    t.load_leaves(arrays["mixed_codes_00"], arrays["mixed_depth_00"], arrays["mixed_flags_00"])
+    return t
+
+
+def step(t, sc):
+    k = t.subdivide(B.SD)
+    t.set_flags_by_image(sc, B.HIT)
+    t.remove(B.HIT)
+    t.unset_flags(B.HIT)
+    return k
+
+
+def check_leaves(t, st, arrays):
+    codes, depth, flags = t.leaves()
+    k = st["step"]
+    assert t.count() == st["n"], f"step {k}"
+    assert t.depth() == st["max_depth"], f"step {k}"
+    assert sha(codes) == st["codes_sha256"], f"step {k} codes"
+    assert sha(depth) == st["depth_sha256"], f"step {k} depths"
+    assert sha(flags) == st["flags_sha256"], f"step {k} flags"
+    if f"mixed_codes_{k:02d}" in arrays:
+        np.testing.assert_array_equal(depth, arrays[f"mixed_depth_{k:02d}"])
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_selective_refinement_matches_reference(golden, name):
+    meta, arrays = golden(name)
+    spec = meta["spec"]
+    t = start(meta, arrays)
+    o = O.Oracle(oracle_spec(spec))
+    o.load(arrays["mixed_codes_00"], arrays["mixed_depth_00"], arrays["mixed_flags_00"])
+    sc = scheme(spec)
+    for st in meta["mixed"][1:]:
+        assert step(t, sc) == o.subdivide(8)
+        o.set_flags_by_image(1)
+        o.remove(1)
+        o.unset_flags(1)
+        check_leaves(t, st, arrays)
+    m = t.transition_matrix(sc, absolute=spec.get("absolute", False), invalid_column=spec.get("invalid", False))
+    rowptr, cols, vals = m.to_host()
+    d = csr_digests(rowptr, cols, vals)
+    tm = meta["tm"]
+    assert m.n_cols == tm["n_cols"]
+    for key in ("nnz", "rowptr_sha256", "cols_sha256", "vals_sha256"):
+        assert d[key] == tm[key], key
+
+
+def test_return_values_of_each_call_match_oracle(golden):
+    meta, arrays = golden("henon_d14_mixed8")
+    spec = meta["spec"]
+    t = start(meta, arrays)
+    o = O.Oracle(oracle_spec(spec))
+    o.load(arrays["mixed_codes_00"], arrays["mixed_depth_00"], arrays["mixed_flags_00"])
+    sc = scheme(spec)
+    for _ in range(4):
+        assert t.subdivide(B.SD) == o.subdivide(8)
+        assert t.set_flags_by_image(sc, B.HIT) == o.set_flags_by_image(1)
+        assert t.remove(B.HIT) == o.remove(1)
+        assert t.unset_flags(B.HIT) == o.unset_flags(1)
+        assert t.set_flags(B.EXPD) == o.set_flags(4)
+        assert t.change_flags(B.EXPD, B.INS) == o.change_flags(4, 2)
+        assert t.unset_flags(B.INS) == o.unset_flags(2)
+    for x, y in zip(t.leaves(), o.leaves()):
+        np.testing.assert_array_equal(x, y)
+
+
+@pytest.mark.parametrize("name", ["henon_d14_mixed8", "lorenz_d15_mixed6_lost"])
+def test_search_by_image_matches_oracle(golden, name):
+    meta, arrays = golden(name)
+    spec = meta["spec"]
+    t = start(meta, arrays)
+    sc = scheme(spec)
+    for _ in range(3):
+        step(t, sc)
+    codes, depth, flags = t.leaves()
+    o = O.Oracle(oracle_spec(spec))
+    o.load(codes, depth, flags)
+    np.testing.assert_array_equal(t.search_by_image(sc), o.search_by_image())
+    # sources filtered by flags: every third leaf carries EXPD
+    mask = np.zeros(len(codes), dtype=np.uint8)
+    mask[::3] = 1
+    o.set_flags_mask(mask, 4)
+    t.load_leaves(codes, depth, flags | (mask * 4).astype(np.uint8))
+    src = np.nonzero(mask)[0].astype(np.uint32)
+    np.testing.assert_array_equal(t.search_by_image(B.Scheme(sc.map, sc.grid, 255, B.EXPD)), o.search_by_image(src))
+
+
+def count_reference(codes, depth, d):
+    """count(d) (ImplicitBoxTree.hpp:1061-1095): leaves that start a new depth-d box."""
+    keep = depth >= d
+    pre = np.where(keep, codes >> (depth.astype(np.uint64) - np.uint64(d)) * keep, 0)
+    fresh = keep.copy()
+    fresh[1:] &= ~(keep[:-1] & (pre[1:] == pre[:-1]))
+    return int(fresh.sum())
+
+
+def test_count_at_inner_depths(golden):
+    meta, arrays = golden("henon_d14_mixed8")
+    t = start(meta, arrays)
+    sc = scheme(meta["spec"])
+    for _ in range(5):
+        step(t, sc)
+    codes, depth, flags = t.leaves()
+    assert t.count(0) == 1 and t.count() == len(codes)
+    for d in range(1, int(depth.max()) + 3):
+        assert t.count(d) == count_reference(codes, depth, d), d
+
+
+def test_subdivision_run_on_a_mixed_tree_matches_oracle(golden):
+    meta, arrays = golden("forced_duffing_d12_mixed5")
+    spec = meta["spec"]
+    t = start(meta, arrays)
+    sc = scheme(spec)
+    step(t, sc)
+    codes, depth, flags = t.leaves()
+    assert depth.min() != depth.max()
+    o = O.Oracle(oracle_spec(spec))
+    o.load(codes, depth, flags)
+    want, _ = o.subdivision(3)
+    np.testing.assert_array_equal(t.subdivision_run(sc, 3), want)
+    for x, y in zip(t.leaves(), o.leaves()):
+        np.testing.assert_array_equal(x, y)
+
+
+def test_self_hit_selection_on_a_mixed_tree(golden):
+    meta, arrays = golden("henon_d14_mixed8")
+    spec = meta["spec"]
+    t = start(meta, arrays)
+    sc = scheme(spec)
+    for _ in range(2):
+        step(t, sc)
+    codes, depth, flags = t.leaves()
+    o = O.Oracle(oracle_spec(spec))
+    o.load(codes, depth, flags)
+    tgt = o.search_by_image().reshape(len(codes), -1)
+    want = (tgt == np.arange(len(codes))[:, None]).any(axis=1)
+    assert t.set_flags_by_self_hit(sc, B.HIT) == int(want.sum())
+    np.testing.assert_array_equal(t.leaves()[2] & B.HIT != 0, want)
+
+
+def test_mixed_tree_returns_to_one_depth(golden):
+    meta, arrays = golden("henon_d8_mixed4_files")
+    t = start(meta, arrays)
+    sc = scheme(meta["spec"])
+    step(t, sc)
+    codes, depth, flags = t.leaves()
+    assert depth.min() == 8 and depth.max() == 9
+    # subdividing every leaf but the depth-8 ones joins the depths again
+    t.unset_flags(B.SD)
+    t.load_leaves(codes, depth, (flags & ~np.uint8(B.SD)) | np.where(depth == 8, B.SD, 0).astype(np.uint8))
+    assert t.subdivide(B.SD) == int((depth == 8).sum())
+    c2, d2, _ = t.leaves()
+    assert (d2 == 9).all() and t.depth() == 9
+    o = O.Oracle(oracle_spec(meta["spec"]))
+    o.load(codes, depth, (flags & ~np.uint8(8)) | np.where(depth == 8, 8, 0).astype(np.uint8))
+    o.subdivide(8)
+    np.testing.assert_array_equal(c2, o.leaves()[0])
+    # a uniform tree again: the fused loop takes over and matches the oracle
+    want, _ = o.subdivision(2)
+    np.testing.assert_array_equal(t.subdivision_run(sc, 2), want)
+    np.testing.assert_array_equal(t.leaves()[0], o.leaves()[0])
+
+
+def test_removing_every_leaf_leaves_the_surrounding_box(golden):
+    meta, arrays = golden("henon_d8_mixed4_files")
+    t = start(meta, arrays)
+    step(t, scheme(meta["spec"]))
+    t.unset_flags(B.HIT)
+    assert t.remove(B.HIT) == meta["mixed"][1]["n"]
+    codes, depth, flags = t.leaves()
+    assert list(codes) == [0] and list(depth) == [0] and t.depth() == 0
+
+
+def test_unsupported_calls_refuse_and_leave_the_tree(golden):
+    meta, arrays = golden("henon_d8_mixed4_files")
+    t = start(meta, arrays)
+    sc = scheme(meta["spec"])
+    step(t, sc)
+    before = [a.copy() for a in t.leaves()]
+    for call in (lambda: t.set_flags(B.EXPD, 5), lambda: t.set_flags_by_image(sc, B.HIT, 9),
+                 lambda: t.insert_by_image(B.Scheme(sc.map, sc.grid, 9, B.INS), 9),
+                 lambda: t.insert_points(np.zeros((1, 2)), 9), lambda: t.search_by_image(sc, 9)):
+        with pytest.raises(B.B12gError) as e:
+            call()
+        assert e.value.status == B._lib.ERR_MIXED_DEPTH
+    for x, y in zip(t.leaves(), before):
+        np.testing.assert_array_equal(x, y)

@@ -1,0 +1,71 @@
+"""CPU: the oracle on trees whose leaves have different depths, against the reference.
+
+The reference run (tests/golden/make_golden.py, `--mixed K`) refines uniformly to depth
+d, keeps SD only on the leaves in the lower half of the first coordinate, and then runs
+K steps of subdivide(SD) + image selection, so that the leaves span depths d..d+K.  Each
+step's leaves (codes, depths, flags) and the final transition matrix pin the oracle's
+ordering (isStrictlyPreceding), search (lower_bound + ComputeSearchIndexFunctor) and
+subdivision on mixed trees.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from workloads import csr_digests, oracle_spec, sha
+
+MIXED_CASES = ["henon_d14_mixed8", "lorenz_d15_mixed6_lost", "forced_duffing_d12_mixed5", "henon_d8_mixed4_files"]
+
+
+def mixed_start(meta, arrays):
+    return arrays["mixed_codes_00"], arrays["mixed_depth_00"], arrays["mixed_flags_00"]
+
+
+@pytest.mark.parametrize("name", MIXED_CASES)
+def test_start_state_is_the_uniform_run_with_a_lower_half_stencil(golden, name):
+    meta, arrays = golden(name)
+    codes, depth, flags = mixed_start(meta, arrays)
+    d = meta["steps"][-1]["depth"]
+    assert (depth == d).all() and len(codes) == meta["steps"][-1]["n"]
+    assert sha(codes) == meta["steps"][-1]["codes_sha256"]
+    lower = (codes >> np.uint64(d - 1)) == 0
+    assert np.array_equal(flags & 8 != 0, lower)
+
+
+@pytest.mark.parametrize("name", MIXED_CASES)
+def test_mixed_steps_match_reference(golden, name):
+    meta, arrays = golden(name)
+    o = O.Oracle(oracle_spec(meta["spec"]))
+    o.load(*mixed_start(meta, arrays))
+    for st in meta["mixed"][1:]:
+        o.subdivide(8)
+        o.set_flags_by_image(1)
+        o.remove(1)
+        o.unset_flags(1)
+        codes, depth, flags = o.leaves()
+        k = st["step"]
+        assert len(codes) == st["n"], f"step {k}"
+        assert sha(codes) == st["codes_sha256"], f"step {k} codes"
+        assert sha(depth) == st["depth_sha256"], f"step {k} depths"
+        assert sha(flags) == st["flags_sha256"], f"step {k} flags"
+        assert int(depth.min()) == st["min_depth"] and int(depth.max()) == st["max_depth"]
+    spec = meta["spec"]
+    rowptr, cols, vals, ncols = o.transition_matrix(absolute=spec.get("absolute", False),
+                                                    invalid=spec.get("invalid", False))
+    d = csr_digests(rowptr, cols, vals)
+    tm = meta["tm"]
+    assert ncols == tm["n_cols"]
+    for key in ("nnz", "rowptr_sha256", "cols_sha256", "vals_sha256"):
+        assert d[key] == tm[key], key
+
+
+def test_mixed_search_candidates_follow_the_reference_rule():
+    # a point on the path of the leaf before the lower bound, at the lower bound, or of neither
+    spec = O.henon_spec()
+    o = O.Oracle(spec)
+    # leaves: 0 (depth 1), 10 (depth 2), 11 (depth 2) - the left half and the right quarters
+    o.load(np.array([0, 2, 3], dtype=np.uint64), np.array([1, 2, 2], dtype=np.uint8), np.zeros(3, np.uint8))
+    for x, want in (((-1.0, 0.0), 0), ((0.2, -0.2), 1), ((0.2, 0.2), 2), ((1.4, 0.44), 2)):
+        c, ok = o.point_code64(np.array(x))
+        assert ok
+        assert o.L.orc_search(O.C.byref(o.tree), c, 1) == want, x
+    assert o.L.orc_search(O.C.byref(o.tree), 0, 0) == 0xFFFFFFFF  # invalid point: the last code is not 0
