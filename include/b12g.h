@@ -17,8 +17,13 @@
  *     "leaves" (getLeafDepth), 254 "unsubdividable" (not supported here).
  *   - Leaf index results use 0xFFFFFFFF for "not found" (getInvalidNrBoxes).
  *   - Flags are the reference's 8-bit flags (Flags.h:10-23).
- *   - All leaves of a tree share one depth.  Operations whose reference result would
- *     mix depths return B12G_ERR_UNSUPPORTED_MIXED_DEPTH and leave the tree unchanged.
+ *   - Leaves may have different depths, as in the reference (kept in the order of
+ *     isStrictlyPreceding, Box.hpp:124-135).  A tree whose leaves share one depth runs
+ *     the fused single-depth kernels; subdividing some of its leaves, or loading leaves
+ *     of several depths, switches it to per-leaf depths until one depth is left.  On a
+ *     tree of mixed depths, flags change at depth 0 or 255, schemes map the leaves
+ *     (depth 255) and insertion is not offered; those calls return
+ *     B12G_ERR_UNSUPPORTED_MIXED_DEPTH and leave the tree unchanged.
  *   - Host pointers are plain host memory (pinned or pageable); the library owns all
  *     device memory of a tree and of a CSR matrix.
  */
@@ -131,7 +136,8 @@ b12g_status b12g_depth(b12g_tree* tree, uint8_t* depth);
 /* the leaves in tree order: codes, depths, flags (host arrays of count(255) entries;
  * any pointer may be NULL).  Mirrors getBitPatternVector/getDepthVector/getFlagsVector. */
 b12g_status b12g_leaves(b12g_tree* tree, uint64_t* codes, uint8_t* depths, uint8_t* flags);
-/* replace the leaves (sorted, unique, one depth) - the load half of save/load */
+/* replace the leaves (in tree order, none inside another; depths may differ) - the load
+ * half of save/load */
 b12g_status b12g_load_leaves(b12g_tree* tree, const uint64_t* codes, const uint8_t* depths,
                              const uint8_t* flags, uint32_t n);
 
@@ -145,7 +151,8 @@ b12g_status b12g_change_flags(b12g_tree* tree, uint8_t to_unset, uint8_t to_set,
                               uint32_t* n_changed);
 
 /* ---- structure ------------------------------------------------------------------ */
-/* subdivide(flags) (ImplicitBoxTree.hpp:2884-2930) */
+/* subdivide(flags) (ImplicitBoxTree.hpp:2884-2930): returns the leaves with all flags set;
+ * those below depth 64 become their two halves */
 b12g_status b12g_subdivide(b12g_tree* tree, uint8_t flags, uint32_t* n_subdivided);
 /* remove(flags): drop leaves that do NOT have all `flags` (ImplicitBoxTree.hpp:2344-2371) */
 b12g_status b12g_remove(b12g_tree* tree, uint8_t flags, uint32_t* n_removed);
@@ -251,7 +258,7 @@ b12g_status b12g_nim_run(b12g_tree* tree, const b12g_scheme* scheme, uint32_t st
  * CooMatrix(fileName) (CooMatrix.hpp:236-291): nRows, nColumns, nnz and the row-major
  * triples.  Files written here are byte for byte what the reference writes for the same
  * tree or matrix; ".json" is appended to a path without it, as the reference does.
- * Loading needs the default subdivision scheme and, for a tree, one leaf depth. */
+ * Loading needs the default subdivision scheme. */
 b12g_status b12g_tree_save_json(b12g_tree* tree, const char* path);
 b12g_status b12g_tree_load_json(const char* path, b12g_tree** tree);
 b12g_status b12g_csr_save_json(const b12g_csr* matrix, const char* path);

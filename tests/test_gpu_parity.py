@@ -203,7 +203,7 @@ def test_remove_everything_leaves_the_root():
     assert t.depth() == 0
 
 
-def test_mixed_depth_is_refused_and_tree_unchanged():
+def test_subdividing_one_leaf_gives_two_depths():
     spec = dict(map="henon", a=1.4, b=0.3, grid=4)
     t = make_tree(spec)
     t.subdivision_run(scheme(spec), 4)
@@ -211,10 +211,18 @@ def test_mixed_depth_is_refused_and_tree_unchanged():
     flags = flags.copy()
     flags[0] |= B.INS
     t.load_leaves(codes, depth, flags)
+    o = O.Oracle(oracle_spec(spec))
+    o.load(codes, depth, flags)
+    assert t.subdivide(B.INS) == o.subdivide(2) == 1
+    for x, y in zip(t.leaves(), o.leaves()):
+        np.testing.assert_array_equal(x, y)
+    assert t.count() == len(codes) + 1 and t.depth() == depth[0] + 1 and t.count(int(depth[0])) == len(codes)
+    # inner-depth flag changes of a tree of mixed depths are refused and change nothing
+    before = [a.copy() for a in t.leaves()]
     with pytest.raises(B.B12gError) as e:
-        t.subdivide(B.INS)
+        t.set_flags(B.EXPD, int(depth[0]))
     assert e.value.status == 5
-    for x, y in zip(t.leaves(), (codes, depth, flags)):
+    for x, y in zip(t.leaves(), before):
         np.testing.assert_array_equal(x, y)
 
 
