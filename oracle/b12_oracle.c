@@ -686,6 +686,292 @@ uint32_t orc_insert_by_image(orc_tree* t, const orc_map* m, const orc_grid* g, u
 }
 
 /* ------------------------------------------------------------------------------
+ * trees of mixed depths: unsubdivide and the general insert
+ * ---------------------------------------------------------------------------- */
+typedef struct { uint64_t c; uint32_t d; uint8_t f; } obox;
+
+static inline int box_same(obox a, obox b)
+{
+  return (is_invalid_depth(a.d) && is_invalid_depth(b.d)) || (a.c == b.c && a.d == b.d);
+}
+static inline int box_same_path(obox a, obox b) { return same_path(a.c, a.d, b.c, b.d); }
+
+/* decrementDepthBy (Box.hpp:151-158) */
+static inline obox decrement_by(obox b, uint32_t k)
+{
+  if (k > b.d) k = b.d;
+  b.c = srs(b.c, (int)k);
+  b.d -= k;
+  return b;
+}
+
+/* IsUnsubdividableFunctor (Functors.hpp:343-364) on leaf i with its neighbours */
+static int unsubdividable(const orc_tree* t, uint64_t i, uint8_t flags)
+{
+  const uint64_t n = t->n;
+  const obox b = {t->code[i], t->depth[i], t->flags[i]};
+  if (!(flags_set(b.f, flags) && b.d > 0)) return 0;
+  const uint64_t j = (b.c & 1u) ? (i > 0 ? i - 1 : 0) : (i + 1 < n ? i + 1 : n - 1);
+  const obox nb = {t->code[j], t->depth[j], t->flags[j]};
+  const obox parent = decrement_by(b, 1);
+  return box_same(parent, decrement_by(nb, 1)) ? flags_set(nb.f, flags) : !box_same_path(parent, nb);
+}
+
+/* unsubdivide (ImplicitBoxTree.hpp:3414-3460): leaves with `flags` whose sibling is a
+ * leaf with them too, or whose sibling's region holds no leaf, become their parents;
+ * two halves merge into one parent with the AND of their flags.  Returns the number of
+ * parents made. */
+uint32_t orc_unsubdivide(orc_tree* t, uint8_t flags)
+{
+  const uint64_t n = t->n;
+  uint8_t* mask = (uint8_t*)malloc(n ? n : 1);
+  uint64_t res = 0;
+  for (uint64_t i = 0; i < n; ++i) res += (mask[i] = (uint8_t)unsubdividable(t, i, flags));
+  for (uint64_t i = 0; i < n; ++i)
+    if (mask[i]) { t->code[i] >>= 1; t->depth[i] -= 1; }
+  /* reverse inclusive_scan_by_key of the flags over runs of equal boxes (AND) */
+  for (uint64_t i = n; i-- > 1;) {
+    const obox a = {t->code[i - 1], t->depth[i - 1], 0}, b = {t->code[i], t->depth[i], 0};
+    if (box_same(b, a)) t->flags[i - 1] &= t->flags[i];
+  }
+  /* unique(IsSameBox): the first of each run stays */
+  uint64_t k = 0;
+  obox prev = {0, 0, 0};
+  for (uint64_t i = 0; i < n; ++i) {
+    const obox b = {t->code[i], t->depth[i], t->flags[i]};
+    const int dup = i > 0 && box_same(prev, b);
+    prev = b;
+    if (dup) continue;
+    t->code[k] = b.c; t->depth[k] = (uint8_t)b.d; t->flags[k] = b.f; ++k;
+  }
+  res -= n - k;
+  t->n = k;
+  free(mask);
+  return (uint32_t)res;
+}
+
+/* computeDepthOfMutualAncestor (Box.hpp:209-223) */
+static inline uint32_t mutual_ancestor(obox a, obox b)
+{
+  const uint64_t x = sls(a.c, 64 - (int)a.d) ^ sls(b.c, 64 - (int)b.d);
+  const uint32_t lz = x ? (uint32_t)__builtin_clzll(x) : 64u;
+  const uint32_t m = a.d < b.d ? a.d : b.d;
+  return lz < m ? lz : m;
+}
+
+/* changeDepthTo (Box.hpp:180-198) for depths 0..64 */
+static inline obox change_depth_to(obox b, uint32_t depth)
+{
+  if (depth < b.d) {
+    b.c = srs(b.c, (int)(b.d - depth));
+    b.d = depth;
+  } else if (depth > b.d && depth != ORC_LEAF_DEPTH) {
+    if (depth > 64) depth = 64;
+    b.c = sls(b.c, (int)(depth - b.d));
+    b.d = depth;
+  }
+  return b;
+}
+
+static int cmp_obox(const void* x, const void* y)
+{
+  const obox* a = (const obox*)x;
+  const obox* b = (const obox*)y;
+  if (strictly_preceding(a->c, a->d, b->c, b->d)) return -1;
+  if (strictly_preceding(b->c, b->d, a->c, a->d)) return 1;
+  return 0;
+}
+
+/* a stable sort in tree order (qsort is not stable: sort (box, position) pairs) */
+typedef struct { obox b; uint64_t pos; } opos;
+static int cmp_opos(const void* x, const void* y)
+{
+  const opos* a = (const opos*)x;
+  const opos* b = (const opos*)y;
+  const int c = cmp_obox(&a->b, &b->b);
+  return c ? c : (a->pos < b->pos ? -1 : (a->pos > b->pos));
+}
+static void stable_sort_boxes(obox* v, uint64_t n)
+{
+  opos* w = (opos*)malloc((n ? n : 1) * sizeof(opos));
+  for (uint64_t i = 0; i < n; ++i) { w[i].b = v[i]; w[i].pos = i; }
+  qsort(w, n, sizeof(opos), cmp_opos);
+  for (uint64_t i = 0; i < n; ++i) v[i] = w[i].b;
+  free(w);
+}
+
+/* a depth-d box exists that contains the depth-64 point box p (a leaf of depth >= d
+ * with p's depth-d prefix): the first leaf whose comparable pattern is not below the
+ * box's first address is inside it exactly when such a leaf exists */
+static int inner_box_exists(const orc_tree* t, uint64_t p64, uint32_t d)
+{
+  const uint64_t q = srs(p64, 64 - (int)d), first = sls(q, 64 - (int)d);
+  uint64_t lo = 0, hi = t->n;
+  while (lo < hi) {
+    const uint64_t mid = lo + (hi - lo) / 2;
+    if (comparable(t->code[mid], t->depth[mid]) < first) lo = mid + 1;
+    else hi = mid;
+  }
+  if (lo >= t->n || t->depth[lo] < d) return 0;
+  return srs(t->code[lo], (int)(t->depth[lo] - d)) == q;
+}
+
+/* insertByIterators (ImplicitBoxTree.hpp:1615-1910) for any tree, given the depth-64
+ * point boxes (valid[k] = 0: the point left the domain).  depth 255 inserts at the
+ * leaf depth (each new box the coarsest one that does not meet its neighbours,
+ * AdaptDepthOfFirstBoxFunctor, Functors.hpp:381-389); new boxes are merged into the
+ * leaves by the reference's two HasSamePath scans and unique (1875-1897).  Flags for
+ * hit boxes at an inner depth are not restated: *unsupported is set instead.
+ * Returns the number of distinct new boxes. */
+uint32_t orc_insert_boxes(orc_tree* t, const uint64_t* c64, const uint8_t* valid, uint64_t np, uint32_t depth,
+                          uint8_t ins, uint8_t hit, int* unsupported)
+{
+  *unsupported = 0;
+  const uint64_t n = t->n;
+  if (depth == 0) {
+    int any = 0;
+    for (uint64_t k = 0; k < np; ++k) any |= valid[k] != 0;
+    if (hit && any) for (uint64_t i = 0; i < n; ++i) t->flags[i] |= hit;
+    return 0;
+  }
+  if (!(depth == ORC_LEAF_DEPTH || depth <= 64)) return 0;
+  uint32_t maxd = 0, uniform = 1;
+  for (uint64_t i = 0; i < n; ++i) {
+    if (t->depth[i] > maxd) maxd = t->depth[i];
+    uniform &= t->depth[i] == t->depth[0];
+  }
+  const int leaf_search = depth == ORC_LEAF_DEPTH || (uniform && depth == t->depth[0]);
+  const int inner_search = !leaf_search && depth <= maxd;
+  if (inner_search && hit) { *unsupported = 1; return 0; }
+  obox* nb = (obox*)malloc((np ? np : 1) * sizeof(obox));
+  uint32_t* hits = (uint32_t*)malloc((np ? np : 1) * 4);
+  uint64_t m = 0, nh = 0;
+  for (uint64_t k = 0; k < np; ++k) {
+    const obox p = valid[k] ? (obox){c64[k], 64u, ins} : (obox){INVALID_CODE, ORC_LEAF_DEPTH, 0};
+    int to_insert;
+    if (leaf_search) {
+      const uint32_t s = orc_search(t, p.c, valid[k]);
+      if (depth == ORC_LEAF_DEPTH)
+        to_insert = s == ORC_INVALID ? valid[k] != 0 : t->depth[s] < 64;
+      else
+        to_insert = s == ORC_INVALID && valid[k];
+      if (!to_insert && s != ORC_INVALID) hits[nh++] = s;
+    } else if (inner_search) {
+      to_insert = valid[k] && !inner_box_exists(t, p.c, depth);
+    } else {
+      to_insert = valid[k] != 0;
+    }
+    if (!to_insert) continue;
+    obox b = p;
+    if (depth == ORC_LEAF_DEPTH) {
+      /* lower bound of the point box among the leaves; its two neighbours */
+      uint64_t lo = 0, hi = n;
+      while (lo < hi) {
+        const uint64_t mid = lo + (hi - lo) / 2;
+        if (strictly_preceding(t->code[mid], t->depth[mid], p.c, p.d)) lo = mid + 1;
+        else hi = mid;
+      }
+      const uint64_t ia = lo > 0 ? lo - 1 : 0, ib = lo < n - 1 ? lo : n - 1;
+      const obox a = {t->code[ia], t->depth[ia], 0}, c = {t->code[ib], t->depth[ib], 0};
+      const uint32_t x = mutual_ancestor(p, a), y = mutual_ancestor(p, c);
+      b = change_depth_to(p, (x > y ? x : y) + 1);
+    } else if (depth < b.d) {
+      b.c = srs(b.c, (int)(b.d - depth));
+      b.d = depth;
+    }
+    b.f = (uint8_t)(b.f | ins);
+    nb[m++] = b;
+  }
+  for (uint64_t k = 0; k < nh; ++k) t->flags[hits[k]] |= hit;
+  /* distinct new boxes in tree order */
+  stable_sort_boxes(nb, m);
+  uint64_t u = 0;
+  for (uint64_t k = 0; k < m; ++k) if (u == 0 || !box_same(nb[u - 1], nb[k])) nb[u++] = nb[k];
+  if (u > 0) {
+    const uint64_t total = n + u;
+    obox* all = (obox*)malloc(total * sizeof(obox));
+    for (uint64_t i = 0; i < n; ++i) all[i] = (obox){t->code[i], t->depth[i], t->flags[i]};
+    for (uint64_t k = 0; k < u; ++k) all[n + k] = nb[k];
+    stable_sort_boxes(all, total);
+    /* forward inclusive_scan_by_key: segments of adjacent boxes on one path (original keys) */
+    obox* f = (obox*)malloc(total * sizeof(obox));
+    for (uint64_t i = 0; i < total; ++i) {
+      if (i > 0 && box_same_path(all[i - 1], all[i])) {
+        f[i].c = f[i - 1].c > all[i].c ? f[i - 1].c : all[i].c;
+        f[i].d = f[i - 1].d > all[i].d ? f[i - 1].d : all[i].d;
+        f[i].f = (uint8_t)(f[i - 1].f | all[i].f);
+      } else {
+        f[i] = all[i];
+      }
+    }
+    /* reverse scan, keyed by the forward scan's output */
+    obox* r = all;
+    for (uint64_t i = total; i-- > 0;) {
+      if (i + 1 < total && box_same_path(f[i + 1], f[i])) {
+        r[i].c = r[i + 1].c > f[i].c ? r[i + 1].c : f[i].c;
+        r[i].d = r[i + 1].d > f[i].d ? r[i + 1].d : f[i].d;
+        r[i].f = (uint8_t)(r[i + 1].f | f[i].f);
+      } else {
+        r[i] = f[i];
+      }
+    }
+    /* unique(HasSamePath) with adjacent comparisons */
+    tree_reserve(t, total);
+    uint64_t k = 0;
+    for (uint64_t i = 0; i < total; ++i) {
+      if (i > 0 && box_same_path(r[i - 1], r[i])) continue;
+      t->code[k] = r[i].c; t->depth[k] = (uint8_t)r[i].d; t->flags[k] = r[i].f; ++k;
+    }
+    t->n = k;
+    free(f);
+    free(all);
+  }
+  free(nb);
+  free(hits);
+  return (uint32_t)u;
+}
+
+/* insertByPoints (ImplicitBoxTree.hpp:1927-1946) through the general insert */
+uint32_t orc_insert_points_general(orc_tree* t, const double* pts, uint64_t n_points, uint32_t depth, uint8_t ins,
+                                   uint8_t hit, int* unsupported)
+{
+  const uint32_t D = t->dom.dim;
+  uint64_t* c = (uint64_t*)malloc((n_points ? n_points : 1) * 8);
+  uint8_t* v = (uint8_t*)malloc(n_points ? n_points : 1);
+  for (uint64_t k = 0; k < n_points; ++k) v[k] = (uint8_t)orc_point_code64(&t->dom, pts + k * D, c + k);
+  const uint32_t r = orc_insert_boxes(t, c, v, n_points, depth, ins, hit, unsupported);
+  free(c); free(v);
+  return r;
+}
+
+/* insertByIterators(makePointIteratorPairByFlags(255, flags_to_check, grid, map), ...)
+ * through the general insert: the images of the leaves with flags_to_check */
+uint32_t orc_insert_by_image_general(orc_tree* t, const orc_map* m, const orc_grid* g, uint8_t flags_to_check,
+                                     uint32_t depth, uint8_t ins, uint8_t hit, int* unsupported)
+{
+  const uint64_t n = t->n, P = points_per_box(g, t->dom.dim);
+  const uint32_t D = t->dom.dim;
+  uint64_t ns = 0;
+  uint32_t* src = (uint32_t*)malloc((n ? n : 1) * 4);
+  for (uint64_t i = 0; i < n; ++i) if (flags_set(t->flags[i], flags_to_check)) src[ns++] = (uint32_t)i;
+  const uint64_t total = ns * P;
+  uint64_t* c = (uint64_t*)malloc((total ? total : 1) * 8);
+  uint8_t* v = (uint8_t*)malloc(total ? total : 1);
+  for (uint64_t i = 0; i < total; ++i) {
+    const uint32_t b = src[i / P];
+    double ctr[ORC_MAX_DIM], r[ORC_MAX_DIM], gp[ORC_MAX_DIM], y[ORC_MAX_DIM];
+    orc_box_coordinates(&t->dom, t->code[b], t->depth[b], ctr, r);
+    orc_grid_point(g, D, i, gp);
+    for (uint32_t j = 0; j < D; ++j) ctr[j] += gp[j] * r[j];
+    orc_map_apply(m, ctr, y);
+    v[i] = (uint8_t)orc_point_code64(&t->dom, y, c + i);
+  }
+  const uint32_t res = orc_insert_boxes(t, c, v, total, depth, ins, hit, unsupported);
+  free(c); free(v); free(src);
+  return res;
+}
+
+/* ------------------------------------------------------------------------------
  * strongly connected components of the graph of a transition matrix (row = source,
  * column = target; columns >= n, the lost column, ignored) - what graphconncomp(P')
  * gives chainRecurrentSet.m:29.  Tarjan's algorithm with an explicit stack; each

@@ -100,6 +100,16 @@ uint32_t orc_insert_points(orc_tree* t, const double* pts, uint64_t n_points, ui
                            uint8_t hit);
 void orc_delete_depth0(orc_tree* t);
 
+/* trees of mixed depths: unsubdivide, and insertByIterators for any tree and depth
+ * (255 = leaf depth); *unsupported is set for flags on hit boxes at an inner depth */
+uint32_t orc_unsubdivide(orc_tree* t, uint8_t flags);
+uint32_t orc_insert_boxes(orc_tree* t, const uint64_t* code64, const uint8_t* valid, uint64_t n_points,
+                          uint32_t depth, uint8_t ins, uint8_t hit, int* unsupported);
+uint32_t orc_insert_points_general(orc_tree* t, const double* pts, uint64_t n_points, uint32_t depth, uint8_t ins,
+                                   uint8_t hit, int* unsupported);
+uint32_t orc_insert_by_image_general(orc_tree* t, const orc_map* m, const orc_grid* g, uint8_t flags_to_check,
+                                     uint32_t depth, uint8_t ins, uint8_t hit, int* unsupported);
+
 /* transition matrix on the leaves, row-major CSR; returns nnz.  Pass NULL arrays to
  * query nnz only.  absolute: values are counts; invalid: lost points go to column
  * n+1 as in the reference (nColumns becomes n+1). */

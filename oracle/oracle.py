@@ -80,6 +80,10 @@ def lib():
             "orc_insert_by_image": (u32, [P(OrcTree), P(OrcMap), P(OrcGrid), u8, u8, u8]),
             "orc_insert_points": (u32, [P(OrcTree), P(dbl), u64, u32, u8, u8]),
             "orc_delete_depth0": (None, [P(OrcTree)]),
+            "orc_unsubdivide": (u32, [P(OrcTree), u8]),
+            "orc_insert_points_general": (u32, [P(OrcTree), P(dbl), u64, u32, u8, u8, P(C.c_int)]),
+            "orc_insert_by_image_general": (u32, [P(OrcTree), P(OrcMap), P(OrcGrid), u8, u32, u8, u8,
+                                                  P(C.c_int)]),
             "orc_transition_matrix": (u64, [P(OrcTree), P(OrcMap), P(OrcGrid), C.c_int, C.c_int,
                                             P(u32), P(u32), P(dbl), P(u32)]),
             "orc_invariant_measure": (None, [u32, P(u32), P(u32), P(dbl), u32, P(dbl)]),
@@ -213,6 +217,22 @@ class Oracle:
                                         pts.size // self.spec["dim"], depth, ins, hit)
 
     def delete_depth0(self): self.L.orc_delete_depth0(C.byref(self.tree))
+
+    def unsubdivide(self, f): return self.L.orc_unsubdivide(C.byref(self.tree), f)
+
+    def insert_points_general(self, pts, depth, ins=2, hit=0):
+        """insertByPoints for any tree and depth (255: leaf depth); None if not restated"""
+        pts = np.ascontiguousarray(pts, dtype=np.float64)
+        uns = C.c_int()
+        r = self.L.orc_insert_points_general(C.byref(self.tree), _ptr(pts, C.c_double), pts.size // self.spec["dim"],
+                                             depth, ins, hit, C.byref(uns))
+        return None if uns.value else r
+
+    def insert_by_image_general(self, check, depth, ins=2, hit=0):
+        uns = C.c_int()
+        r = self.L.orc_insert_by_image_general(C.byref(self.tree), C.byref(self.map), C.byref(self.grid), check,
+                                               depth, ins, hit, C.byref(uns))
+        return None if uns.value else r
 
     def points_per_box(self) -> int:
         return int(self.L.orc_grid_points_per_box(C.byref(self.grid), self.spec["dim"]))

@@ -37,6 +37,7 @@ struct RunOpts
   std::string save;           // save the final tree and matrix as JSON (save(): ImplicitBoxTree.hpp:435-528,
                               // CooMatrix.hpp:473-525) to SAVE_tree.json / SAVE_tm.json
   int mixed = 0;              // steps of selective refinement after the uniform steps (mixed leaf depths)
+  int edits = 0;              // 1: unsubdivide / insert edits of the mixed tree afterwards (runEdits)
 };
 
 inline RunOpts parseOpts(int argc, char** argv)
@@ -49,7 +50,94 @@ inline RunOpts parseOpts(int argc, char** argv)
   o.tm = std::atoi(arg(argc, argv, "--tm", "1"));
   o.save = arg(argc, argv, "--save", "");
   o.mixed = std::atoi(arg(argc, argv, "--mixed", "0"));
+  o.edits = std::atoi(arg(argc, argv, "--edits", "0"));
   return o;
+}
+
+// n points uniform in the domain from SplitMix64 (seed), u = (x >> 11) * 2^-53 per
+// coordinate in order; written to PATH as u64 n, u32 dim, f64 points[n][dim]
+inline std::vector<double> domainPoints(const std::vector<double>& c, const std::vector<double>& r, uint64_t n,
+                                        uint64_t seed, const std::string& path)
+{
+  const uint32_t dim = uint32_t(c.size());
+  std::vector<double> p(n * dim);
+  uint64_t s = seed;
+  for (uint64_t k = 0; k < n * dim; ++k) {
+    s += 0x9E3779B97F4A7C15ull;
+    uint64_t z = s;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    const double u = double(z >> 11) * (1.0 / 9007199254740992.0);
+    const uint32_t j = uint32_t(k % dim);
+    p[k] = (c[j] - r[j]) + 2.0 * r[j] * u;
+  }
+  if (!path.empty()) {
+    FILE* f = openOut(path);
+    std::fwrite(&n, 8, 1, f);
+    std::fwrite(&dim, 4, 1, f);
+    std::fwrite(p.data(), 8, p.size(), f);
+    std::fclose(f);
+  }
+  return p;
+}
+
+// Edits of a tree of mixed depths, each dumped to edit_KK.bin and its return value
+// recorded: unsubdivide (ImplicitBoxTree.hpp:3414-3460) twice, insertByPoints
+// (1927-1946) at the leaf depth with flags for hit leaves, deeper than every leaf, and
+// at an inner depth, then insertByIterators of the images of the INS leaves at the leaf
+// depth, and one image selection step.  Before that, points inserted into a fresh tree
+// (the surrounding box alone) at depth 6 go to root_insert.bin.
+template<class Tree, class Grid, class Map>
+void runEdits(Tree& ibt, const std::vector<double>& c, const std::vector<double>& r, Grid grid, Map map,
+              const RunOpts& o, std::ostringstream& js)
+{
+  using namespace b12;
+  using Vec = ThrustSystem<OMP>::Vector<double>;
+  const std::string dir = o.out;
+  auto pts = [&](uint64_t n, uint64_t seed, const char* name) {
+    std::vector<double> p = domainPoints(c, r, n, seed, dir.empty() ? "" : dir + "/" + name);
+    return Vec(p.begin(), p.end());
+  };
+  auto dump = [&](int k) {
+    if (dir.empty()) return;
+    char fn[64];
+    std::snprintf(fn, sizeof fn, "/edit_%02d.bin", k);
+    dumpLeaves(ibt, dir + fn);
+  };
+  {
+    ThrustSystem<OMP>::Vector<double> center(c.begin(), c.end()), radius(r.begin(), r.end());
+    Tree fresh(center, radius);
+    fresh.setFlags(Flag::SD, 0);
+    fresh.insertByPoints(pts(40, 7, "points_root.bin"), 6, Flag::INS, Flag::HIT);
+    if (!dir.empty()) dumpLeaves(fresh, dir + "/root_insert.bin");
+  }
+  js << ", \"edits\": [";
+  NrBoxes v = ibt.unsubdivide(Flag::SD);
+  js << v;
+  dump(1);
+  v = ibt.unsubdivide(Flag::SD);
+  js << ", " << v;
+  dump(2);
+  const int maxd = int(ibt.depth());
+  ibt.insertByPoints(pts(300, 1, "points_3.bin"), getLeafDepth(), Flag::INS, Flag::HIT);
+  js << ", " << ibt.count(getLeafDepth());
+  dump(3);
+  ibt.insertByPoints(pts(300, 2, "points_4.bin"), Depth(maxd + 2), Flag::INS, Flag::NONE);
+  js << ", " << ibt.count(getLeafDepth());
+  dump(4);
+  ibt.insertByPoints(pts(300, 3, "points_5.bin"), Depth(maxd - 1), Flag::EXPD, Flag::NONE);
+  js << ", " << ibt.count(getLeafDepth());
+  dump(5);
+  ibt.insertByIterators(ibt.makePointIteratorPairByFlags(getLeafDepth(), Flag::INS, grid, map), getLeafDepth(),
+                        Flag::EXPD, Flag::NONE);
+  js << ", " << ibt.count(getLeafDepth());
+  dump(6);
+  ibt.setFlagsByIterators(ibt.makePointIteratorPairOverLeaves(grid, map), Flag::HIT, getLeafDepth());
+  ibt.remove(Flag::HIT);
+  ibt.unsetFlags(Flag::HIT, getLeafDepth());
+  js << ", " << ibt.count(getLeafDepth()) << "], \"edit_max_depth\": " << maxd;
+  dump(7);
 }
 
 // Selective refinement: SD stays only on the leaves in the lower half of the first
@@ -126,6 +214,7 @@ int runSubdivision(const std::vector<double>& c, const std::vector<double>& r,
   }
   js << "]";
   if (o.mixed > 0) runMixed(ibt, grid, map, o, js, boxImages);
+  if (o.edits > 0) runEdits(ibt, c, r, grid, map, o, js);
   auto t1 = clk::now();
   js << ", \"subdivision_s\": " << secs(t0, t1) << ", \"box_images\": " << boxImages;
   if (!o.save.empty()) ibt.save(o.save + "_tree.json");

@@ -60,6 +60,14 @@ WORKLOADS = {
                                   dict(map="forced_duffing", grid=4, steps=12, mixed=5, absolute=True)),
     "henon_d8_mixed4_files": ("ref_henon", ["--steps", "8", "--mixed", "4", "--tm", "1", "--buf", "4294967296"],
                               dict(map="henon", a=1.4, b=0.3, grid=4, steps=8, mixed=4, save=True)),
+    # then unsubdivide twice, insert points at the leaf depth, deeper and at an inner
+    # depth, insert the images of the inserted leaves at the leaf depth, select once
+    "henon_d12_mixed6_edits": ("ref_henon", ["--steps", "12", "--mixed", "6", "--edits", "1", "--tm", "1"],
+                               dict(map="henon", a=1.4, b=0.3, grid=4, steps=12, mixed=6, edits=True)),
+    "lorenz_d12_mixed4_edits": ("ref_lorenz", ["--steps", "12", "--mixed", "4", "--edits", "1", "--tm", "3"],
+                                dict(map="lorenz", rho=28.0, grid=5, steps=12, mixed=4, edits=True, invalid=True)),
+    "forced_duffing_d10_mixed3_edits": ("ref_forced", ["--steps", "10", "--mixed", "3", "--edits", "1", "--tm", "1"],
+                                        dict(map="forced_duffing", grid=4, steps=10, mixed=3, edits=True)),
     "coupled_duffing_cont_d8": ("ref_duffing", ["--steps", "8"], dict(map="coupled_duffing", points=64, seed=0,
                                                                           depth=8)),
     "coupled_duffing_cont_d12": ("ref_duffing", ["--steps", "12"], dict(map="coupled_duffing", points=64, seed=0,
@@ -80,6 +88,13 @@ def read_leaves(path):
         depth = np.frombuffer(f.read(n), dtype=np.uint8).copy()
         flags = np.frombuffer(f.read(n), dtype=np.uint8).copy()
     return codes, depth, flags
+
+
+def read_points(path):
+    with open(path, "rb") as f:
+        n = int(np.frombuffer(f.read(8), dtype="<u8")[0])
+        dim = int(np.frombuffer(f.read(4), dtype="<u4")[0])
+        return np.frombuffer(f.read(8 * n * dim), dtype="<f8").reshape(n, dim).copy()
 
 
 def read_coo(path):
@@ -128,6 +143,17 @@ def generate(name: str) -> None:
                 arrays[f"mixed_codes_{k:02d}"] = codes
                 arrays[f"mixed_depth_{k:02d}"] = depth
                 arrays[f"mixed_flags_{k:02d}"] = flags
+        # edits (--edits 1): unsubdivide and inserts on the mixed tree, and the points used
+        for fn in sorted(f for f in os.listdir(tmp) if f.startswith("edit_") or f == "root_insert.bin"):
+            key = "root" if fn == "root_insert.bin" else f"{int(fn[len('edit_'):-4]):02d}"
+            codes, depth, flags = read_leaves(os.path.join(tmp, fn))
+            out.setdefault("edits", []).append(dict(step=key, n=int(len(codes)), codes_sha256=sha(codes),
+                                                    depth_sha256=sha(depth), flags_sha256=sha(flags)))
+            arrays[f"edit_codes_{key}"] = codes
+            arrays[f"edit_depth_{key}"] = depth
+            arrays[f"edit_flags_{key}"] = flags
+        for fn in sorted(f for f in os.listdir(tmp) if f.startswith("points_")):
+            arrays[fn[:-4]] = read_points(os.path.join(tmp, fn))
         for fn in files:
             k = int(fn[len(prefix):-4])
             codes, depth, flags = read_leaves(os.path.join(tmp, fn))

@@ -69,3 +69,55 @@ def test_mixed_search_candidates_follow_the_reference_rule():
         assert ok
         assert o.L.orc_search(O.C.byref(o.tree), c, 1) == want, x
     assert o.L.orc_search(O.C.byref(o.tree), 0, 0) == 0xFFFFFFFF  # invalid point: the last code is not 0
+
+
+EDIT_CASES = ["henon_d12_mixed6_edits", "lorenz_d12_mixed4_edits", "forced_duffing_d10_mixed3_edits"]
+
+
+def edit_sequence(o, meta, arrays):
+    """The reference run's edits (oracle/ref/runner.h, runEdits), yielding after each."""
+    maxd = meta["timing"]["edit_max_depth"]
+    yield "01", o.unsubdivide(8)
+    yield "02", o.unsubdivide(8)
+    yield "03", o.insert_points_general(arrays["points_3"], 255, 2, 1)
+    yield "04", o.insert_points_general(arrays["points_4"], maxd + 2, 2, 0)
+    yield "05", o.insert_points_general(arrays["points_5"], maxd - 1, 4, 0)
+    yield "06", o.insert_by_image_general(2, 255, 4, 0)
+    o.set_flags_by_image(1)
+    o.remove(1)
+    o.unset_flags(1)
+    yield "07", None
+
+
+@pytest.mark.parametrize("name", EDIT_CASES)
+def test_unsubdivide_and_insert_match_reference(golden, name):
+    meta, arrays = golden(name)
+    spec = meta["spec"]
+    last = meta["mixed"][-1]["step"]
+    o = O.Oracle(oracle_spec(spec))
+    o.load(arrays[f"mixed_codes_{last:02d}"], arrays[f"mixed_depth_{last:02d}"], arrays[f"mixed_flags_{last:02d}"])
+    want = {e["step"]: e for e in meta["edits"]}
+    counts = meta["timing"]["edits"]
+    for k, (key, ret) in enumerate(edit_sequence(o, meta, arrays)):
+        codes, depth, flags = o.leaves()
+        e = want[key]
+        assert len(codes) == e["n"], key
+        assert sha(codes) == e["codes_sha256"], f"{key} codes"
+        assert sha(depth) == e["depth_sha256"], f"{key} depths"
+        assert sha(flags) == e["flags_sha256"], f"{key} flags"
+        if key in ("01", "02"):
+            assert ret == counts[k], key          # unsubdivide's return value
+        else:
+            assert len(codes) == counts[k], key   # the run records the leaf count
+
+
+@pytest.mark.parametrize("name", EDIT_CASES)
+def test_insert_into_the_surrounding_box_alone(golden, name):
+    # several new boxes merge with the surrounding box, which shares every path
+    meta, arrays = golden(name)
+    o = O.Oracle(oracle_spec(meta["spec"]))
+    o.set_flags(8)
+    o.insert_points_general(arrays["points_root"], 6, 2, 1)
+    codes, depth, flags = o.leaves()
+    e = {x["step"]: x for x in meta["edits"]}["root"]
+    assert sha(codes) == e["codes_sha256"] and sha(depth) == e["depth_sha256"] and sha(flags) == e["flags_sha256"]
