@@ -85,6 +85,7 @@ _SIGS = {
     "b12g_subdivide": (C.c_int, [C.c_void_p, C.c_uint8, C.POINTER(C.c_uint32)]),
     "b12g_remove": (C.c_int, [C.c_void_p, C.c_uint8, C.POINTER(C.c_uint32)]),
     "b12g_delete_depth": (C.c_int, [C.c_void_p, C.c_uint8, C.POINTER(C.c_uint32)]),
+    "b12g_unsubdivide": (C.c_int, [C.c_void_p, C.c_uint8, C.POINTER(C.c_uint32)]),
     "b12g_set_flags_by_image": (C.c_int, [C.c_void_p, C.POINTER(Scheme), C.c_uint8, C.c_uint8,
                                           C.POINTER(C.c_uint32)]),
     "b12g_search_by_image": (C.c_int, [C.c_void_p, C.POINTER(Scheme), C.c_uint8, C.c_void_p, C.c_uint64,

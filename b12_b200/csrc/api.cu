@@ -374,6 +374,9 @@ b12g_status b12g_tree_destroy(b12g_tree* t)
   }
   for (int b = 0; b < 2; ++b) { t->code[b].release(); t->flags[b].release(); t->dep[b].release(); }
   t->cmp.release(); t->hash.release(); t->points.release();
+  t->pvalid.release(); t->ins_dep.release(); t->ins_dep2.release(); t->scan_dep.release(); t->scan_flags.release();
+  t->ins_code.release(); t->scan_code.release(); t->ins_pos.release(); t->ins_head.release();
+  for (int b = 0; b < 2; ++b) { t->ins_key[b].release(); t->ins_idx[b].release(); }
   t->hit.release(); t->ctr.release(); t->tiles_a.release(); t->tiles_b.release();
   t->src.release(); t->out.release(); t->stage_col.release(); t->stage_cnt.release();
   t->row_count.release(); t->rowptr.release(); t->cand.release(); t->cand2.release();
@@ -520,6 +523,12 @@ b12g_status b12g_remove(b12g_tree* t, uint8_t flags, uint32_t* n_removed)
   if (kept == 0) ST(set_root(t, B12G_NONE));  // insertSurroundingBoxIfEmpty
   if (n_removed) *n_removed = removed;
   return B12G_OK;
+}
+
+b12g_status b12g_unsubdivide(b12g_tree* t, uint8_t flags, uint32_t* n_parents)
+{
+  if (!t) return fail(B12G_ERR_INVALID, "NULL tree");
+  return mixed_unsubdivide(t, flags, n_parents);
 }
 
 b12g_status b12g_delete_depth(b12g_tree* t, uint8_t depth, uint32_t* n_deleted)

@@ -131,10 +131,7 @@ b12g_status insert_points_impl(b12g_tree* t, const double* points, uint64_t n_po
 {
   if (!t || (!points && n_points)) return fail(B12G_ERR_INVALID, "NULL argument");
   if (n_points > 0xFFFFFFF0ull) return fail(B12G_ERR_CAPACITY, "too many points");
-  if (t->mixed) return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "insertion into a tree of mixed depths");
-  if (depth == B12G_LEAF_DEPTH) return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "insertion at the leaf depth -1");
-  if (depth > 64) return fail(B12G_ERR_INVALID, "depth above 64");
-  const bool root_only = t->n == 1 && t->depth == 0;
+  if (depth > 64 && depth != B12G_LEAF_DEPTH) return fail(B12G_ERR_INVALID, "depth above 64");
   if (depth == 0) {
     // the surrounding box always exists: only flagsForHit (ImplicitBoxTree.hpp:1625-1640)
     if (hit_flags && n_points) {
@@ -152,8 +149,12 @@ b12g_status insert_points_impl(b12g_tree* t, const double* points, uint64_t n_po
     if (n_inserted) *n_inserted = 0;
     return B12G_OK;
   }
-  if (!root_only && depth != t->depth)
-    return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "insertion at depth %u into a depth-%u tree", depth, t->depth);
+  const bool root_only = t->n == 1 && t->depth == 0;
+  if (t->mixed || depth == B12G_LEAF_DEPTH || (root_only && t->domain.dim >= 2) || (!root_only && depth != t->depth)) {
+    // new boxes may nest in or around leaves: the reference's general insert
+    ST(mixed_point_boxes(t, points, n_points));
+    return mixed_insert_boxes(t, n_points, depth, ins, hit_flags, n_inserted);
+  }
   uint32_t u = 0;
   if (n_points) {
     ST(ensure_candidates(t, n_points));
@@ -203,10 +204,17 @@ b12g_status insert_by_image_impl(b12g_tree* t, const b12g_scheme* sc, uint8_t de
                                  uint32_t* n_inserted)
 {
   if (!t || !sc) return fail(B12G_ERR_INVALID, "NULL argument");
-  if (t->mixed) return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "insertion into a tree of mixed depths");
-  if (depth != t->depth || t->depth == 0)
-    return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "insertion of images at depth %u into a depth-%u tree", depth,
-                t->depth);
+  if (depth == 0) return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "insertion of images at depth 0");
+  if (depth > 64 && depth != B12G_LEAF_DEPTH) return fail(B12G_ERR_INVALID, "depth above 64");
+  if (t->mixed || depth == B12G_LEAF_DEPTH || depth != t->depth || t->depth == 0) {
+    // new boxes may nest in or around leaves: the reference's general insert of the
+    // images of the scheme's source leaves (sources at the leaf depth)
+    b12g_scheme s = *sc;
+    if (!t->mixed && s.depth == t->depth) s.depth = B12G_LEAF_DEPTH;
+    uint64_t np = 0;
+    ST(mixed_image_boxes(t, &s, &np));
+    return mixed_insert_boxes(t, np, depth, ins, hit_flags, n_inserted);
+  }
   Prepared pr;
   ST(prepare(t, sc, pr));
   uint32_t n_src = 0;

@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "rows.cuh"
+#include "sort.h"
 #include "tree.h"
 
 using namespace b12g;
@@ -171,6 +172,349 @@ __global__ void apply_hits_kernel(uint8_t* flags, uint8_t* hit, uint32_t n, uint
   if (c) atomicAdd(changed, c);
 }
 
+// ---------------------------------------------------------------------------- boxes
+// A box as the reference's Box<N> (code, depth, flags); depth above 64 is the invalid box.
+struct Bx {
+  uint64_t c;
+  uint32_t d;
+  uint32_t f;
+};
+
+__device__ __forceinline__ uint64_t srs(uint64_t b, int i) { return i <= 0 ? b : (i >= 64 ? 0ull : b >> i); }
+__device__ __forceinline__ uint64_t sls(uint64_t b, int i) { return i <= 0 ? b : (i >= 64 ? 0ull : b << i); }
+
+__device__ __forceinline__ Bx load_box(const uint64_t* code, const uint8_t* dep, const uint8_t* flags, uint32_t i)
+{
+  return Bx{code[i], dep[i], flags ? flags[i] : 0u};
+}
+
+// hasSamePath (Box.hpp:75-83)
+__device__ __forceinline__ bool same_path(const Bx& a, const Bx& b)
+{
+  const int diff = int(a.d) - int(b.d);
+  return (a.d > 64 && b.d > 64) || srs(a.c, diff) == srs(b.c, -diff);
+}
+
+// isSameBox (Box.hpp:113-120)
+__device__ __forceinline__ bool same_box(const Bx& a, const Bx& b)
+{
+  return (a.d > 64 && b.d > 64) || (a.c == b.c && a.d == b.d);
+}
+
+// isStrictlyPreceding (Box.hpp:124-135)
+__device__ __forceinline__ bool precedes(const Bx& a, const Bx& b)
+{
+  if (a.d > 64) return false;
+  if (b.d > 64) return true;
+  const uint64_t ka = comparable(a.c, a.d), kb = comparable(b.c, b.d);
+  return ka < kb || (ka == kb && b.d < a.d);
+}
+
+// ComputeMaxBitPatternMaxDepthOrFlagsFunctor (Functors.hpp:396-401)
+__device__ __forceinline__ Bx combine(const Bx& a, const Bx& b)
+{
+  return Bx{a.c > b.c ? a.c : b.c, a.d > b.d ? a.d : b.d, a.f | b.f};
+}
+
+// decrementDepthBy(box, 1) (Box.hpp:151-158)
+__device__ __forceinline__ Bx parent_of(Bx b)
+{
+  if (b.d > 0) {
+    b.c = srs(b.c, 1);
+    b.d -= 1;
+  }
+  return b;
+}
+
+// computeDepthOfMutualAncestor (Box.hpp:209-223)
+__device__ __forceinline__ uint32_t mutual_ancestor(const Bx& a, const Bx& b)
+{
+  const uint64_t x = sls(a.c, 64 - int(a.d)) ^ sls(b.c, 64 - int(b.d));
+  const uint32_t lz = uint32_t(__clzll(x));    // 64 for x == 0
+  const uint32_t m = a.d < b.d ? a.d : b.d;
+  return lz < m ? lz : m;
+}
+
+// changeDepthTo (Box.hpp:180-198) for target depths 0..64
+__device__ __forceinline__ Bx change_depth_to(Bx b, uint32_t depth)
+{
+  if (depth < b.d) {
+    b.c = srs(b.c, int(b.d - depth));
+    b.d = depth;
+  } else if (depth > b.d) {
+    if (depth > 64) depth = 64;
+    b.c = sls(b.c, int(depth - b.d));
+    b.d = depth;
+  }
+  return b;
+}
+
+// first leaf whose comparable pattern is not below `key`
+__device__ __forceinline__ uint32_t lower_bound_cmp(const uint64_t* __restrict__ cmp, uint32_t n, uint64_t key)
+{
+  uint32_t lo = 0, len = n;
+  while (len > 0) {
+    const uint32_t half = len >> 1;
+    if (__ldg(cmp + lo + half) < key) {
+      lo += half + 1;
+      len -= half + 1;
+    } else {
+      len = half;
+    }
+  }
+  return lo;
+}
+
+// unsubdivide, IsUnsubdividableFunctor (Functors.hpp:343-364): marks and their number
+__global__ void unsub_mark_kernel(const uint64_t* code, const uint8_t* dep, const uint8_t* flags, uint32_t n, uint8_t f,
+                                  uint32_t* mark, uint32_t* count)
+{
+  uint32_t c = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const Bx b = load_box(code, dep, flags, i);
+    bool res = uint8_t(b.f & f) == f && b.d > 0;
+    if (res) {
+      const uint32_t j = (b.c & 1ull) ? (i > 0 ? i - 1 : 0) : (i + 1 < n ? i + 1 : n - 1);
+      const Bx nb = load_box(code, dep, flags, j);
+      const Bx p = parent_of(b);
+      res = same_box(p, parent_of(nb)) ? uint8_t(nb.f & f) == f : !same_path(p, nb);
+    }
+    mark[i] = res ? 1u : 0u;
+    c += res;
+  }
+  if (c) atomicAdd(count, c);
+}
+
+// the marked leaves become their parents; two equal parents keep the first with the AND
+// of both flags (the reverse inclusive_scan_by_key and unique of unsubdivide,
+// ImplicitBoxTree.hpp:3430-3452; equal boxes come at most in pairs, as leaves are disjoint)
+__global__ void unsub_apply_kernel(const uint64_t* code, const uint8_t* dep, const uint8_t* flags, uint32_t n,
+                                   const uint32_t* mark, uint64_t* out_code, uint8_t* out_dep, uint8_t* out_flags,
+                                   uint32_t* keep)
+{
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    Bx b = load_box(code, dep, flags, i);
+    if (mark[i]) b = parent_of(b);
+    uint32_t f = b.f;
+    if (i + 1 < n) {
+      Bx nx = load_box(code, dep, flags, i + 1);
+      if (mark[i + 1]) nx = parent_of(nx);
+      if (same_box(nx, b)) f &= nx.f;
+    }
+    bool first = true;
+    if (i > 0) {
+      Bx pv = load_box(code, dep, nullptr, i - 1);
+      if (mark[i - 1]) pv = parent_of(pv);
+      first = !same_box(pv, b);
+    }
+    out_code[i] = b.c;
+    out_dep[i] = uint8_t(b.d);
+    out_flags[i] = uint8_t(f);
+    keep[i] = first ? 1u : 0u;
+  }
+}
+
+// insertByIterators (ImplicitBoxTree.hpp:1615-1910): the new box of every point box
+struct InsertArgs {
+  const uint64_t* p64;         // depth-64 point codes
+  const uint8_t* valid;        // 0: the point left the domain (the invalid box)
+  uint64_t np;
+  const uint64_t* code;        // leaves
+  const uint8_t* dep;
+  const uint64_t* cmp;
+  uint32_t n;
+  uint32_t depth;              // insertion depth; 255: the leaf depth
+  int mode;                    // 0: leaf depth, 2: below an existing depth, 3: deeper than every leaf
+  uint8_t* hit;                // marks of leaves hit (leaf depth, when flags for hit are given)
+  uint64_t* out_code;          // new boxes (appended)
+  uint8_t* out_dep;
+  uint32_t* count;
+  uint32_t cap;
+  uint32_t* error;
+};
+
+__global__ void insert_boxes_kernel(const InsertArgs a)
+{
+  for (uint64_t k = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; k < a.np; k += uint64_t(gridDim.x) * blockDim.x) {
+    const bool valid = a.valid[k] != 0;
+    const Bx p = valid ? Bx{a.p64[k], 64u, 0u} : Bx{~0ull, 255u, 0u};
+    bool to_insert;
+    uint32_t lo = 0;
+    if (a.mode == 0) {
+      // searchByIterators at the leaf depth, then the leaf-depth rule (1672-1702):
+      // a point in no leaf is inserted if valid, one in a leaf if that leaf is above depth 64
+      lo = valid ? lower_bound_cmp(a.cmp, a.n, p.c) : a.n;
+      const uint32_t ia = lo > 0 ? lo - 1 : 0, ib = lo < a.n - 1 ? lo : a.n - 1;
+      uint32_t s = kInvalidIndex;
+      if (same_path(p, load_box(a.code, a.dep, nullptr, ia))) s = lo > 0 ? lo - 1 : 0;
+      else if (same_path(p, load_box(a.code, a.dep, nullptr, ib))) s = lo;
+      to_insert = s == kInvalidIndex ? valid : a.dep[s] < 64;
+      if (!to_insert && s != kInvalidIndex && a.hit) a.hit[s] = 1;
+    } else if (a.mode == 2) {
+      // a depth-d box exists around the point when the first leaf at or after the box's
+      // first address lies inside it
+      bool found = false;
+      if (valid) {
+        const int sh = 64 - int(a.depth);
+        const uint64_t q = srs(p.c, sh);
+        const uint32_t j = lower_bound_cmp(a.cmp, a.n, sls(q, sh));
+        found = j < a.n && a.dep[j] >= a.depth && srs(a.code[j], int(a.dep[j]) - int(a.depth)) == q;
+      }
+      to_insert = valid && !found;
+    } else {
+      to_insert = valid;
+    }
+    if (!to_insert) continue;
+    Bx b;
+    if (a.mode == 0) {
+      // AdaptDepthOfFirstBoxFunctor (Functors.hpp:381-389): one below the deepest common
+      // ancestor with the two neighbours at the lower bound
+      const uint32_t ia = lo > 0 ? lo - 1 : 0, ib = lo < a.n - 1 ? lo : a.n - 1;
+      const uint32_t x = mutual_ancestor(p, load_box(a.code, a.dep, nullptr, ia));
+      const uint32_t y = mutual_ancestor(p, load_box(a.code, a.dep, nullptr, ib));
+      b = change_depth_to(p, (x > y ? x : y) + 1);
+    } else {
+      b = change_depth_to(p, a.depth);     // decrementDepthTo(depth)
+    }
+    const uint32_t slot = atomicAdd(a.count, 1u);
+    if (slot < a.cap) {
+      a.out_code[slot] = b.c;
+      a.out_dep[slot] = uint8_t(b.d);
+    } else {
+      atomicOr(a.error, 1u);
+    }
+  }
+}
+
+// sort keys of the new boxes: deeper first (pass 1), then the comparable pattern
+__global__ void depth_key_kernel(const uint8_t* dep, uint32_t m, uint64_t* key, uint32_t* idx)
+{
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x) {
+    key[j] = 255u - dep[j];
+    idx[j] = j;
+  }
+}
+
+__global__ void pattern_key_kernel(const uint64_t* code, const uint8_t* dep, const uint32_t* idx, uint32_t m,
+                                   uint64_t* key)
+{
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x)
+    key[j] = comparable(code[idx[j]], dep[idx[j]]);
+}
+
+// distinct new boxes in order: heads of runs of equal boxes (unique with IsSameBoxFunctor)
+__global__ void new_heads_kernel(const uint64_t* code, const uint8_t* dep, const uint32_t* idx, uint32_t m,
+                                 uint32_t* head)
+{
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x)
+    head[j] = (j == 0 || code[idx[j]] != code[idx[j - 1]] || dep[idx[j]] != dep[idx[j - 1]]) ? 1u : 0u;
+}
+
+__global__ void new_scatter_kernel(const uint64_t* code, const uint8_t* dep, const uint32_t* idx, uint32_t m,
+                                   const uint32_t* pos, uint64_t* ucode, uint8_t* udep)
+{
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x)
+    if (pos[j + 1] != pos[j]) {
+      ucode[pos[j]] = code[idx[j]];
+      udep[pos[j]] = dep[idx[j]];
+    }
+}
+
+// sortBoxes of the leaves and the new boxes together (stable: a leaf before an equal
+// new box): the merge of two sorted lists by rank
+__global__ void merge_boxes_kernel(const uint64_t* code, const uint8_t* dep, const uint8_t* flags, uint32_t n,
+                                   const uint64_t* ucode, const uint8_t* udep, uint8_t ins, uint32_t u,
+                                   uint64_t* out_code, uint8_t* out_dep, uint8_t* out_flags)
+{
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n + u; i += gridDim.x * blockDim.x) {
+    if (i < n) {
+      const Bx b = load_box(code, dep, flags, i);
+      // new boxes strictly before the leaf
+      uint32_t lo = 0, len = u;
+      while (len > 0) {
+        const uint32_t half = len >> 1;
+        if (precedes(Bx{ucode[lo + half], udep[lo + half], 0u}, b)) { lo += half + 1; len -= half + 1; }
+        else len = half;
+      }
+      out_code[i + lo] = b.c;
+      out_dep[i + lo] = uint8_t(b.d);
+      out_flags[i + lo] = uint8_t(b.f);
+    } else {
+      const uint32_t j = i - n;
+      const Bx b{ucode[j], udep[j], ins};
+      // leaves not strictly after the new box
+      uint32_t lo = 0, len = n;
+      while (len > 0) {
+        const uint32_t half = len >> 1;
+        if (!precedes(b, load_box(code, dep, nullptr, lo + half))) { lo += half + 1; len -= half + 1; }
+        else len = half;
+      }
+      out_code[j + lo] = b.c;
+      out_dep[j + lo] = uint8_t(b.d);
+      out_flags[j + lo] = ins;
+    }
+  }
+}
+
+// forward inclusive_scan_by_key (ImplicitBoxTree.hpp:1878-1884): runs of adjacent boxes
+// on one path, each run walked by the thread of its first box
+__global__ void forward_scan_kernel(const uint64_t* code, const uint8_t* dep, const uint8_t* flags, uint32_t total,
+                                    uint64_t* fc, uint8_t* fd, uint8_t* ff)
+{
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+    Bx acc = load_box(code, dep, flags, i);
+    if (i > 0 && same_path(load_box(code, dep, nullptr, i - 1), acc)) continue;
+    fc[i] = acc.c; fd[i] = uint8_t(acc.d); ff[i] = uint8_t(acc.f);
+    Bx prev = acc;
+    for (uint32_t j = i + 1; j < total; ++j) {
+      const Bx b = load_box(code, dep, flags, j);
+      if (!same_path(prev, b)) break;
+      acc = combine(acc, b);
+      fc[j] = acc.c; fd[j] = uint8_t(acc.d); ff[j] = uint8_t(acc.f);
+      prev = b;
+    }
+  }
+}
+
+// reverse scan keyed by the forward scan's output (1886-1892), from each run's last box
+__global__ void reverse_scan_kernel(const uint64_t* fc, const uint8_t* fd, const uint8_t* ff, uint32_t total,
+                                    uint64_t* rc, uint8_t* rd, uint8_t* rf)
+{
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+    Bx acc = load_box(fc, fd, ff, i);
+    if (i + 1 < total && same_path(load_box(fc, fd, nullptr, i + 1), acc)) continue;
+    rc[i] = acc.c; rd[i] = uint8_t(acc.d); rf[i] = uint8_t(acc.f);
+    Bx prev = acc;
+    for (uint32_t j = i; j-- > 0;) {
+      const Bx b = load_box(fc, fd, ff, j);
+      if (!same_path(prev, b)) break;
+      acc = combine(acc, b);
+      rc[j] = acc.c; rd[j] = uint8_t(acc.d); rf[j] = uint8_t(acc.f);
+      prev = b;
+    }
+  }
+}
+
+// unique(HasSamePathFunctor) (1894-1897): a box stays unless it shares a path with the one before
+__global__ void path_heads_kernel(const uint64_t* code, const uint8_t* dep, uint32_t total, uint32_t* keep)
+{
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x)
+    keep[i] = (i == 0 || !same_path(load_box(code, dep, nullptr, i - 1), load_box(code, dep, nullptr, i))) ? 1u : 0u;
+}
+
+template<int D>
+__global__ void point_codes_kernel(const double* pts, uint64_t np, Domain dom, uint64_t* p64, uint8_t* valid)
+{
+  for (uint64_t k = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; k < np; k += uint64_t(gridDim.x) * blockDim.x) {
+    double p[D];
+#pragma unroll
+    for (int j = 0; j < D; ++j) p[j] = pts[k * D + j];
+    uint64_t c = 0;
+    valid[k] = point_code<D>(dom, p, 64, c) ? 1 : 0;
+    p64[k] = c;
+  }
+}
+
 // ---------------------------------------------------------------------------- images
 struct MixedArgs {
   Domain dom;
@@ -185,6 +529,8 @@ struct MixedArgs {
   uint32_t n_src;
   uint8_t* hit;                // Hit: marks of the leaves hit
   uint32_t* out;               // Search: leaf index of every point
+  uint64_t* p64_out;           // Codes: depth-64 code of every image point
+  uint8_t* valid_out;          //        1 if it lies in the domain
   // transition rows
   uint32_t* stage_col;
   uint32_t* stage_cnt;
@@ -209,10 +555,11 @@ __device__ __forceinline__ bool load_table(const GridParams& g, uint64_t P, doub
   return table;
 }
 
-// the leaf the image of point k of source leaf `leaf` lands in (point index g)
+// the depth-64 code of the image of point k of source leaf `leaf` (point index g);
+// false if the image left the domain
 template<class Map, class Grid>
-__device__ __forceinline__ uint32_t image_of(const MixedArgs& a, const double* pts, bool table, uint32_t leaf,
-                                             uint32_t k, uint64_t g)
+__device__ __forceinline__ bool image_code(const MixedArgs& a, const double* pts, bool table, uint32_t leaf,
+                                           uint32_t k, uint64_t g, uint64_t& p64)
 {
   constexpr int D = Map::D;
   double c[D], r[D], gp[D], x[D], y[D];
@@ -226,12 +573,23 @@ __device__ __forceinline__ uint32_t image_of(const MixedArgs& a, const double* p
 #pragma unroll
   for (int j = 0; j < D; ++j) x[j] = __dadd_rn(c[j], __dmul_rn(gp[j], r[j]));
   Map::apply(a.map, x, y);
-  uint64_t p64 = 0;
-  const bool valid = point_code<D>(a.dom, y, 64, p64);
+  p64 = 0;
+  return point_code<D>(a.dom, y, 64, p64);
+}
+
+// the leaf the image of point k of source leaf `leaf` lands in (point index g)
+template<class Map, class Grid>
+__device__ __forceinline__ uint32_t image_of(const MixedArgs& a, const double* pts, bool table, uint32_t leaf,
+                                             uint32_t k, uint64_t g)
+{
+  uint64_t p64;
+  const bool valid = image_code<Map, Grid>(a, pts, table, leaf, k, g, p64);
   return locate_mixed(a.cmp, a.code, a.dep, a.n, valid, p64);
 }
 
-template<class Map, class Grid, bool kSearch>
+// kMode 0: hit marks of the leaves hit; 1: leaf index of every point; 2: the points'
+// depth-64 codes and validity (the point boxes of an insertion)
+template<class Map, class Grid, int kMode>
 __global__ void __launch_bounds__(kThreads) mixed_image_kernel(const MixedArgs a)
 {
   __shared__ double pts[kTable];
@@ -242,9 +600,15 @@ __global__ void __launch_bounds__(kThreads) mixed_image_kernel(const MixedArgs a
     const uint64_t rank = g / P;
     const uint32_t k = uint32_t(g - rank * P);
     const uint32_t leaf = a.src ? __ldg(a.src + rank) : uint32_t(rank);
-    const uint32_t t = image_of<Map, Grid>(a, pts, table, leaf, k, g);
-    if constexpr (kSearch) a.out[g] = t;
-    else if (t != kInvalidIndex) a.hit[t] = 1;
+    if constexpr (kMode == 2) {
+      uint64_t p64;
+      a.valid_out[g] = image_code<Map, Grid>(a, pts, table, leaf, k, g, p64) ? 1 : 0;
+      a.p64_out[g] = p64;
+    } else {
+      const uint32_t t = image_of<Map, Grid>(a, pts, table, leaf, k, g);
+      if constexpr (kMode == 1) a.out[g] = t;
+      else if (t != kInvalidIndex) a.hit[t] = 1;
+    }
   }
 }
 
@@ -526,7 +890,7 @@ b12g_status mixed_set_flags_by_image(b12g_tree* t, const b12g_scheme* sc, uint8_
   }
   a.hit = t->hit.p;
   CK(dispatch(sc->map.kind, sc->map.arith, sc->grid.kind, t->domain.dim, [&](auto map, auto grid) -> cudaError_t {
-    mixed_image_kernel<decltype(map), decltype(grid), false>
+    mixed_image_kernel<decltype(map), decltype(grid), 0>
         <<<grid_for_n(uint64_t(a.n_src) * a.points), kThreads, 0, t->stream>>>(a);
     return cudaGetLastError();
   }));
@@ -549,7 +913,7 @@ b12g_status mixed_search(b12g_tree* t, const b12g_scheme* sc, uint64_t* n_points
   ST(t->out.ensure(std::max<uint64_t>(np, 1), "search output"));
   a.out = t->out.p;
   CK(dispatch(sc->map.kind, sc->map.arith, sc->grid.kind, t->domain.dim, [&](auto map, auto grid) -> cudaError_t {
-    mixed_image_kernel<decltype(map), decltype(grid), true><<<grid_for_n(np), kThreads, 0, t->stream>>>(a);
+    mixed_image_kernel<decltype(map), decltype(grid), 1><<<grid_for_n(np), kThreads, 0, t->stream>>>(a);
     return cudaGetLastError();
   }));
   count_launches(1);
@@ -578,6 +942,196 @@ b12g_status mixed_rows(b12g_tree* t, const b12g_scheme* sc, int invalid_column)
     return cudaGetLastError();
   }));
   count_launches(1);
+  return B12G_OK;
+}
+
+// unsubdivide (ImplicitBoxTree.hpp:3414-3460); returns the number of parents made
+b12g_status mixed_unsubdivide(b12g_tree* t, uint8_t flags, uint32_t* n_parents)
+{
+  ST(mixed_enter(t));
+  const uint32_t n = t->n;
+  ST(t->out.ensure(std::max<uint32_t>(n, 1), "unsubdivide marks"));
+  ST(t->row_count.ensure(uint64_t(n) + 1, "keep marks"));
+  ST(t->rowptr.ensure(uint64_t(n) + 1, "keep positions"));
+  ST(set_ctr(t, C_CAND, 0));
+  const int o = 1 - t->cur;
+  unsub_mark_kernel<<<grid_for_n(n), kThreads, 0, t->stream>>>(t->codes(), dep_cur(t), t->flg(), n, flags, t->out.p,
+                                                                t->ctr.p + C_CAND);
+  unsub_apply_kernel<<<grid_for_n(n), kThreads, 0, t->stream>>>(t->codes(), dep_cur(t), t->flg(), n, t->out.p,
+                                                                 t->code[o].p, t->dep[o].p, t->flags[o].p,
+                                                                 t->row_count.p);
+  count_launches(2);
+  uint32_t kept = 0;
+  ST(scan_marks(t, t->row_count.p, t->rowptr.p, n, &kept));
+  keep_scatter_kernel<<<grid_for_n(n), kThreads, 0, t->stream>>>(t->code[o].p, t->flags[o].p, t->dep[o].p, n,
+                                                                   t->rowptr.p, t->codes(), t->flg(), dep_cur(t),
+                                                                   nullptr);
+  count_launches(1);
+  ST(read_ctr(t, C_CAND, 1));
+  const uint32_t marked = t->h_ctr[C_CAND];
+  t->n = kept;
+  ST(set_ctr(t, t->ncur, kept));
+  ST(sync(t, "unsubdivide"));
+  if (n_parents) *n_parents = marked - (n - kept);
+  return mixed_settle(t);
+}
+
+// insertByIterators (ImplicitBoxTree.hpp:1615-1910) for the np point boxes held in
+// t->cand (depth-64 codes) and t->pvalid, at `depth` (255: the leaf depth), for trees of
+// any depths; the caller handles depth 0.  *n_inserted gets the distinct new boxes.
+b12g_status mixed_insert_boxes(b12g_tree* t, uint64_t np, uint8_t depth, uint8_t ins, uint8_t hit,
+                               uint32_t* n_inserted)
+{
+  if (depth > 64 && depth != B12G_LEAF_DEPTH) return fail(B12G_ERR_INVALID, "insertion depth %u", depth);
+  if (np > 0xFFFFFFF0ull) return fail(B12G_ERR_CAPACITY, "too many points in one insertion");
+  const int mode = depth == B12G_LEAF_DEPTH ? 0 : (depth <= t->depth ? 2 : 3);
+  if (mode == 2 && hit)
+    return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "flags for boxes hit at the inner depth %u", depth);
+  if (n_inserted) *n_inserted = 0;
+  ST(mixed_enter(t));
+  ST(refresh_comparable(t));
+  const uint32_t m_cap = uint32_t(std::max<uint64_t>(np, 1));
+  ST(t->ins_code.ensure(m_cap, "new boxes"));
+  ST(t->ins_dep.ensure(m_cap, "new box depths"));
+  ST(set_ctr(t, C_CAND, 0));
+  InsertArgs a{};
+  a.p64 = t->cand.p;
+  a.valid = t->pvalid.p;
+  a.np = np;
+  a.code = t->codes();
+  a.dep = dep_cur(t);
+  a.cmp = t->cmp.p;
+  a.n = t->n;
+  a.depth = depth;
+  a.mode = mode;
+  a.hit = (mode == 0 && hit) ? t->hit.p : nullptr;
+  a.out_code = t->ins_code.p;
+  a.out_dep = t->ins_dep.p;
+  a.count = t->ctr.p + C_CAND;
+  a.cap = m_cap;
+  a.error = t->ctr.p + C_ERROR;
+  if (np) insert_boxes_kernel<<<grid_for_n(np), kThreads, 0, t->stream>>>(a);
+  count_launches(1);
+  if (a.hit) {
+    ST(set_ctr(t, C_CHANGED, 0));
+    apply_hits_kernel<<<grid_for_n(t->n), kThreads, 0, t->stream>>>(t->flg(), t->hit.p, t->n, hit,
+                                                                     t->ctr.p + C_CHANGED);
+    count_launches(1);
+  }
+  ST(read_ctr(t, C_CAND, 1));
+  ST(check_error(t, "insert"));
+  const uint32_t m = t->h_ctr[C_CAND];
+  if (m == 0) return mixed_settle(t);
+
+  // the new boxes in tree order (deeper first among equal patterns), then distinct
+  for (int q = 0; q < 2; ++q) {
+    ST(t->ins_key[q].ensure(m, "new box keys"));
+    ST(t->ins_idx[q].ensure(m, "new box order"));
+  }
+  ST(t->ins_pos.ensure(uint64_t(m) + 1, "new box heads"));
+  ST(t->ins_head.ensure(uint64_t(m) + 1, "new box heads"));
+  const uint64_t cells = sort_scratch_u32(m);
+  ST(t->sort_idx.ensure(2 * cells + compact_tiles(cells) + 8, "new box sort"));
+  uint32_t* hist = t->sort_idx.p;
+  uint32_t* offsets = hist + cells;
+  uint32_t* tiles = offsets + cells;
+  depth_key_kernel<<<grid_for_n(m), kThreads, 0, t->stream>>>(t->ins_dep.p, m, t->ins_key[0].p, t->ins_idx[0].p);
+  uint64_t* keys = nullptr;
+  uint32_t* order = nullptr;
+  CK(radix_sort_u64_values(t->ins_key[0].p, t->ins_key[1].p, t->ins_idx[0].p, t->ins_idx[1].p, t->ctr.p + C_CAND, m,
+                           8, hist, offsets, tiles, t->ctr.p + C_TMP, &keys, &order, t->stream));
+  uint32_t* order_alt = order == t->ins_idx[0].p ? t->ins_idx[1].p : t->ins_idx[0].p;
+  pattern_key_kernel<<<grid_for_n(m), kThreads, 0, t->stream>>>(t->ins_code.p, t->ins_dep.p, order, m,
+                                                                 t->ins_key[0].p);
+  CK(radix_sort_u64_values(t->ins_key[0].p, t->ins_key[1].p, order, order_alt, t->ctr.p + C_CAND, m, 64, hist,
+                           offsets, tiles, t->ctr.p + C_TMP, &keys, &order, t->stream));
+  count_launches(2 + (1 + 5 * 1) + (1 + 5 * 8));   // key kernels; per sort one set-up, 5 launches a digit
+  new_heads_kernel<<<grid_for_n(m), kThreads, 0, t->stream>>>(t->ins_code.p, t->ins_dep.p, order, m, t->ins_head.p);
+  count_launches(1);
+  uint32_t u = 0;
+  ST(scan_marks(t, t->ins_head.p, t->ins_pos.p, m, &u));
+  uint64_t* ucode = keys == t->ins_key[0].p ? t->ins_key[1].p : t->ins_key[0].p;
+  ST(t->ins_dep2.ensure(std::max<uint32_t>(u, 1), "distinct new boxes"));
+  uint8_t* udep = t->ins_dep2.p;
+  new_scatter_kernel<<<grid_for_n(m), kThreads, 0, t->stream>>>(t->ins_code.p, t->ins_dep.p, order, m,
+                                                                 t->ins_pos.p, ucode, udep);
+  count_launches(1);
+
+  // sortBoxes of leaves + new boxes, the two HasSamePath scans and unique (1862-1897)
+  const uint32_t n = t->n;
+  const uint64_t total = uint64_t(n) + u;
+  ST(reserve(t, total));
+  ST(t->scan_code.ensure(total, "merge scan"));
+  ST(t->scan_dep.ensure(total, "merge scan"));
+  ST(t->scan_flags.ensure(total, "merge scan"));
+  ST(t->row_count.ensure(total + 1, "keep marks"));
+  ST(t->rowptr.ensure(total + 1, "keep positions"));
+  const int o = 1 - t->cur;
+  merge_boxes_kernel<<<grid_for_n(total), kThreads, 0, t->stream>>>(t->codes(), dep_cur(t), t->flg(), n, ucode, udep,
+                                                                     ins, u, t->code[o].p, t->dep[o].p,
+                                                                     t->flags[o].p);
+  forward_scan_kernel<<<grid_for_n(total), kThreads, 0, t->stream>>>(t->code[o].p, t->dep[o].p, t->flags[o].p,
+                                                                      uint32_t(total), t->scan_code.p,
+                                                                      t->scan_dep.p, t->scan_flags.p);
+  reverse_scan_kernel<<<grid_for_n(total), kThreads, 0, t->stream>>>(t->scan_code.p, t->scan_dep.p, t->scan_flags.p,
+                                                                      uint32_t(total), t->code[o].p, t->dep[o].p,
+                                                                      t->flags[o].p);
+  path_heads_kernel<<<grid_for_n(total), kThreads, 0, t->stream>>>(t->code[o].p, t->dep[o].p, uint32_t(total),
+                                                                    t->row_count.p);
+  count_launches(4);
+  uint32_t kept = 0;
+  ST(scan_marks(t, t->row_count.p, t->rowptr.p, uint32_t(total), &kept));
+  keep_scatter_kernel<<<grid_for_n(total), kThreads, 0, t->stream>>>(t->code[o].p, t->flags[o].p, t->dep[o].p,
+                                                                       uint32_t(total), t->rowptr.p, t->codes(),
+                                                                       t->flg(), dep_cur(t), nullptr);
+  count_launches(1);
+  t->n = kept;
+  ST(set_ctr(t, t->ncur, kept));
+  ST(sync(t, "insert"));
+  if (n_inserted) *n_inserted = u;
+  return mixed_settle(t);
+}
+
+// the point boxes of n_points host points (row-major, dim doubles each) into t->cand / t->pvalid
+b12g_status mixed_point_boxes(b12g_tree* t, const double* points, uint64_t n_points)
+{
+  const uint32_t D = t->domain.dim;
+  if (D < 2) return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "insertion at other depths needs dimension 2 to 4");
+  ST(t->cand.ensure(std::max<uint64_t>(n_points, 256), "point boxes"));
+  ST(t->pvalid.ensure(std::max<uint64_t>(n_points, 1), "point boxes"));
+  if (n_points == 0) return B12G_OK;
+  ST(t->points.ensure(n_points * D, "points"));
+  CK(cudaMemcpyAsync(t->points.p, points, n_points * D * 8, cudaMemcpyHostToDevice, t->stream));
+  const int g = grid_for_n(n_points);
+  switch (D) {
+    case 2: point_codes_kernel<2><<<g, kThreads, 0, t->stream>>>(t->points.p, n_points, t->dom, t->cand.p, t->pvalid.p); break;
+    case 3: point_codes_kernel<3><<<g, kThreads, 0, t->stream>>>(t->points.p, n_points, t->dom, t->cand.p, t->pvalid.p); break;
+    default: point_codes_kernel<4><<<g, kThreads, 0, t->stream>>>(t->points.p, n_points, t->dom, t->cand.p, t->pvalid.p); break;
+  }
+  CK(cudaGetLastError());
+  count_launches(1);
+  return B12G_OK;
+}
+
+// the point boxes of the images of the scheme's source leaves into t->cand / t->pvalid
+b12g_status mixed_image_boxes(b12g_tree* t, const b12g_scheme* sc, uint64_t* n_points)
+{
+  ST(mixed_enter(t));
+  MixedArgs a;
+  ST(mixed_args(t, sc, a));
+  ST(mixed_sources(t, sc, &a.src, &a.n_src));
+  const uint64_t np = uint64_t(a.n_src) * a.points;
+  ST(t->cand.ensure(std::max<uint64_t>(np, 256), "point boxes"));
+  ST(t->pvalid.ensure(std::max<uint64_t>(np, 1), "point boxes"));
+  a.p64_out = t->cand.p;
+  a.valid_out = t->pvalid.p;
+  if (np)
+    CK(dispatch(sc->map.kind, sc->map.arith, sc->grid.kind, t->domain.dim, [&](auto map, auto grid) -> cudaError_t {
+      mixed_image_kernel<decltype(map), decltype(grid), 2><<<grid_for_n(np), kThreads, 0, t->stream>>>(a);
+      return cudaGetLastError();
+    }));
+  count_launches(1);
+  *n_points = np;
   return B12G_OK;
 }
 

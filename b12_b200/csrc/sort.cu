@@ -7,6 +7,8 @@
 // key order, then a prefix over the tile's warps).  This replaces the reference's
 // thrust::sort / sort_by_key on codes (helpFunctions.hpp:40-98 via sortBoxes, used by
 // insertByIterators at ImplicitBoxTree.hpp:1832-1875).
+#include <utility>
+
 #include "kernels.h"
 #include "sort.h"
 
@@ -50,8 +52,11 @@ __global__ void __launch_bounds__(kThreads) digit_hist_kernel(const uint64_t* ke
   }
 }
 
-__global__ void __launch_bounds__(kThreads) digit_scatter_kernel(const uint64_t* keys, const uint32_t* n_ptr,
-                                                                 int shift, const uint32_t* offsets, uint64_t* out)
+template<bool kValues>
+__global__ void __launch_bounds__(kThreads) digit_scatter_kernel(const uint64_t* keys, const uint32_t* vals,
+                                                                 const uint32_t* n_ptr, int shift,
+                                                                 const uint32_t* offsets, uint64_t* out,
+                                                                 uint32_t* vout)
 {
   __shared__ uint32_t wcount[kWarps][kBins];     // per-warp running digit counts
   __shared__ uint32_t wbase[kWarps][kBins];      // exclusive prefix over warps, + tile offset
@@ -62,12 +67,14 @@ __global__ void __launch_bounds__(kThreads) digit_scatter_kernel(const uint64_t*
     for (int i = threadIdx.x; i < kWarps * kBins; i += kThreads) (&wcount[0][0])[i] = 0;
     __syncthreads();
     uint64_t key[kRounds];
+    uint32_t val[kValues ? kRounds : 1];
     uint32_t rank[kRounds];
 #pragma unroll
     for (int r = 0; r < kRounds; ++r) {
       const uint32_t i = t * kTile + tile_index(w, r, lane);
       const bool valid = i < n;
       key[r] = valid ? keys[i] : 0ull;
+      if constexpr (kValues) val[r] = valid ? vals[i] : 0u;
       const uint32_t d = valid ? uint32_t((key[r] >> shift) & 0xFFu) : 0xFFFFFFFFu;
       const unsigned peers = __match_any_sync(0xFFFFFFFFu, d);
       const uint32_t before = valid ? wcount[w][d] : 0u;
@@ -89,7 +96,11 @@ __global__ void __launch_bounds__(kThreads) digit_scatter_kernel(const uint64_t*
 #pragma unroll
     for (int r = 0; r < kRounds; ++r) {
       const uint32_t i = t * kTile + tile_index(w, r, lane);
-      if (i < n) out[wbase[w][(key[r] >> shift) & 0xFFu] + rank[r]] = key[r];
+      if (i < n) {
+        const uint32_t p = wbase[w][(key[r] >> shift) & 0xFFu] + rank[r];
+        out[p] = key[r];
+        if constexpr (kValues) vout[p] = val[r];
+      }
     }
     __syncthreads();
   }
@@ -170,12 +181,36 @@ cudaError_t radix_sort_u64(uint64_t* keys, uint64_t* alt, const uint32_t* n, uin
     digit_hist_kernel<<<g, kThreads, 0, s>>>(src, n, shift, hist);
     cudaError_t e = exclusive_scan_u32(hist, offsets, count_tmp, scan_tiles, uint32_t(tiles) * kBins, s);
     if (e != cudaSuccess) return e;
-    digit_scatter_kernel<<<g, kThreads, 0, s>>>(src, n, shift, offsets, dst);
+    digit_scatter_kernel<false><<<g, kThreads, 0, s>>>(src, nullptr, n, shift, offsets, dst, nullptr);
     uint64_t* t = src;
     src = dst;
     dst = t;
   }
   *sorted = src;
+  return cudaGetLastError();
+}
+
+cudaError_t radix_sort_u64_values(uint64_t* keys, uint64_t* alt, uint32_t* vals, uint32_t* valt, const uint32_t* n,
+                                  uint32_t max_n, int bits, uint32_t* hist, uint32_t* offsets, uint32_t* scan_tiles,
+                                  uint32_t* count_tmp, uint64_t** sorted, uint32_t** sorted_vals, cudaStream_t s)
+{
+  const uint32_t tiles = (max_n + kTile - 1) / kTile;
+  set_u32_kernel<<<1, 1, 0, s>>>(count_tmp, tiles * kBins);
+  const int g = grid_for(uint64_t(tiles) * kTile, kTile, 4);
+  uint64_t* src = keys;
+  uint64_t* dst = alt;
+  uint32_t* vsrc = vals;
+  uint32_t* vdst = valt;
+  for (int shift = 0; shift < bits; shift += 8) {
+    digit_hist_kernel<<<g, kThreads, 0, s>>>(src, n, shift, hist);
+    cudaError_t e = exclusive_scan_u32(hist, offsets, count_tmp, scan_tiles, uint32_t(tiles) * kBins, s);
+    if (e != cudaSuccess) return e;
+    digit_scatter_kernel<true><<<g, kThreads, 0, s>>>(src, vsrc, n, shift, offsets, dst, vdst);
+    std::swap(src, dst);
+    std::swap(vsrc, vdst);
+  }
+  *sorted = src;
+  *sorted_vals = vsrc;
   return cudaGetLastError();
 }
 

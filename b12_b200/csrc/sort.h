@@ -16,6 +16,12 @@ cudaError_t radix_sort_u64(uint64_t* keys, uint64_t* alt, const uint32_t* n, uin
                            uint32_t* hist, uint32_t* offsets, uint32_t* scan_tiles, uint32_t* count_tmp,
                            uint64_t** sorted, cudaStream_t s);
 
+// the same with a u32 value per key moved along (stable); *sorted_vals tells where the
+// values ended up (vals or valt)
+cudaError_t radix_sort_u64_values(uint64_t* keys, uint64_t* alt, uint32_t* vals, uint32_t* valt, const uint32_t* n,
+                                  uint32_t max_n, int bits, uint32_t* hist, uint32_t* offsets, uint32_t* scan_tiles,
+                                  uint32_t* count_tmp, uint64_t** sorted, uint32_t** sorted_vals, cudaStream_t s);
+
 // distinct values of a sorted array, in order; flag and pos: max_n + 1 u32
 cudaError_t unique_sorted_u64(const uint64_t* keys, const uint32_t* n, uint32_t max_n, uint64_t* out, uint32_t* n_out,
                               uint32_t* flag, uint32_t* pos, uint32_t* scan_tiles, cudaStream_t s);

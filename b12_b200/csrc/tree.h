@@ -117,6 +117,10 @@ struct b12g_tree {
   bool mixed = false;
   Buf<uint8_t> dep[2];
   Buf<uint64_t> cmp;
+  // insertion into such trees: point-box validity, new boxes, their sort, the merge scans
+  Buf<uint8_t> pvalid, ins_dep, ins_dep2, scan_dep, scan_flags;
+  Buf<uint64_t> ins_code, ins_key[2], scan_code;
+  Buf<uint32_t> ins_idx[2], ins_pos, ins_head;
   Buf<ulonglong2> hash;        // leaf lookup table
   uint32_t hash_tag = 0;       // tag of the last build (1..255; 0 = cleared)
   uint32_t hash_log2 = 0;      // log2 of the table's slots
@@ -200,6 +204,15 @@ b12g_status mixed_set_flags_by_image(b12g_tree* t, const b12g_scheme* sc, uint8_
 b12g_status mixed_search(b12g_tree* t, const b12g_scheme* sc, uint64_t* n_points);
 // transition rows of every leaf into t->stage_col / stage_cnt / row_count
 b12g_status mixed_rows(b12g_tree* t, const b12g_scheme* sc, int invalid_column);
+// unsubdivide(flags); *n_parents = the parents made
+b12g_status mixed_unsubdivide(b12g_tree* t, uint8_t flags, uint32_t* n_parents);
+// the general insert of the point boxes in t->cand / t->pvalid (np of them) at depth
+// (255: leaf depth; not 0); *n_inserted = distinct new boxes
+b12g_status mixed_insert_boxes(b12g_tree* t, uint64_t np, uint8_t depth, uint8_t ins, uint8_t hit,
+                               uint32_t* n_inserted);
+// point boxes of host points, or of the images of a scheme's source leaves
+b12g_status mixed_point_boxes(b12g_tree* t, const double* points, uint64_t n_points);
+b12g_status mixed_image_boxes(b12g_tree* t, const b12g_scheme* sc, uint64_t* n_points);
 
 }  // namespace host
 }  // namespace b12g

@@ -343,6 +343,9 @@ class ImplicitBoxTree:
     def delete_depth(self, depth: int) -> int:
         return self._n("b12g_delete_depth", depth)
 
+    def unsubdivide(self, flags: int = L.SD) -> int:
+        return self._n("b12g_unsubdivide", flags)
+
     # ---- box images
     def set_flags_by_image(self, scheme: Scheme, flags: int, depth: int = LEAF) -> int:
         s = scheme.to_c()

@@ -156,6 +156,10 @@ b12g_status b12g_change_flags(b12g_tree* tree, uint8_t to_unset, uint8_t to_set,
 b12g_status b12g_subdivide(b12g_tree* tree, uint8_t flags, uint32_t* n_subdivided);
 /* remove(flags): drop leaves that do NOT have all `flags` (ImplicitBoxTree.hpp:2344-2371) */
 b12g_status b12g_remove(b12g_tree* tree, uint8_t flags, uint32_t* n_removed);
+/* unsubdivide(flags) (ImplicitBoxTree.hpp:3414-3460): a leaf with all flags becomes its
+ * parent when its sibling is a leaf with them too (the two merge, flags ANDed) or when
+ * its sibling's region holds no leaf; returns the number of parents made */
+b12g_status b12g_unsubdivide(b12g_tree* tree, uint8_t flags, uint32_t* n_parents);
 /* deleteDepth(depth) (ImplicitBoxTree.hpp:1217-1228); depth 0 and 255 supported */
 b12g_status b12g_delete_depth(b12g_tree* tree, uint8_t depth, uint32_t* n_deleted);
 
@@ -170,7 +174,11 @@ b12g_status b12g_set_flags_by_image(b12g_tree* tree, const b12g_scheme* scheme, 
 b12g_status b12g_search_by_image(b12g_tree* tree, const b12g_scheme* scheme, uint8_t depth,
                                  uint32_t* out, uint64_t capacity, uint64_t* n_points);
 /* insertByPoints(points, depth, ins, hit) (ImplicitBoxTree.hpp:1927-1946); points are
- * n_points x dim doubles, row-major */
+ * n_points x dim doubles, row-major.  depth 255 inserts at the leaf depth (each new box
+ * the coarsest one that meets neither neighbour; a point in a leaf above depth 64 splits
+ * it); a depth other than the leaves' merges new and old boxes on one path into the
+ * deepest, flags ORed, as the reference does.  *n_inserted = distinct new boxes.
+ * Flags for hit boxes at a depth inside the tree (not its leaf depth) are not offered. */
 b12g_status b12g_insert_points(b12g_tree* tree, const double* points, uint64_t n_points, uint8_t depth,
                                uint8_t flags_for_inserted, uint8_t flags_for_hit, uint32_t* n_inserted);
 /* insertByIterators(makePointIteratorPairByFlags(scheme), depth, ins, hit)

@@ -210,9 +210,126 @@ def test_unsupported_calls_refuse_and_leave_the_tree(golden):
     before = [a.copy() for a in t.leaves()]
     for call in (lambda: t.set_flags(B.EXPD, 5), lambda: t.set_flags_by_image(sc, B.HIT, 9),
                  lambda: t.insert_by_image(B.Scheme(sc.map, sc.grid, 9, B.INS), 9),
-                 lambda: t.insert_points(np.zeros((1, 2)), 9), lambda: t.search_by_image(sc, 9)):
+                 lambda: t.search_by_image(sc, 9)):
         with pytest.raises(B.B12gError) as e:
             call()
         assert e.value.status == B._lib.ERR_MIXED_DEPTH
+    for x, y in zip(t.leaves(), before):
+        np.testing.assert_array_equal(x, y)
+
+
+# ---------------------------------------------------------------- unsubdivide and insertion
+EDIT_CASES = ["henon_d12_mixed6_edits", "lorenz_d12_mixed4_edits", "forced_duffing_d10_mixed3_edits"]
+
+
+def check_edit(t, e, key):
+    codes, depth, flags = t.leaves()
+    assert t.count() == e["n"], key
+    assert sha(codes) == e["codes_sha256"], f"{key} codes"
+    assert sha(depth) == e["depth_sha256"], f"{key} depths"
+    assert sha(flags) == e["flags_sha256"], f"{key} flags"
+    assert t.depth() == int(depth.max())
+
+
+@pytest.mark.parametrize("name", EDIT_CASES)
+def test_unsubdivide_and_insert_match_reference(golden, name):
+    """The reference run's edits of a mixed tree (oracle/ref/runner.h, runEdits) call by
+    call, leaves after each against the reference, return values against the oracle."""
+    meta, arrays = golden(name)
+    spec = meta["spec"]
+    last = meta["mixed"][-1]["step"]
+    start_leaves = (arrays[f"mixed_codes_{last:02d}"], arrays[f"mixed_depth_{last:02d}"],
+                    arrays[f"mixed_flags_{last:02d}"])
+    c, r = domain(spec)
+    t = B.ImplicitBoxTree(c, r)
+    t.load_leaves(*start_leaves)
+    o = O.Oracle(oracle_spec(spec))
+    o.load(*start_leaves)
+    sc = scheme(spec)
+    want = {e["step"]: e for e in meta["edits"]}
+    maxd = meta["timing"]["edit_max_depth"]
+    assert t.unsubdivide(B.SD) == o.unsubdivide(8) == meta["timing"]["edits"][0]
+    check_edit(t, want["01"], "01")
+    assert t.unsubdivide(B.SD) == o.unsubdivide(8) == meta["timing"]["edits"][1]
+    check_edit(t, want["02"], "02")
+    assert t.depth() == maxd
+    assert t.insert_points(arrays["points_3"], 255, B.INS, B.HIT) == o.insert_points_general(arrays["points_3"], 255, 2, 1)
+    check_edit(t, want["03"], "03")
+    assert t.insert_points(arrays["points_4"], maxd + 2, B.INS) == o.insert_points_general(arrays["points_4"], maxd + 2, 2)
+    check_edit(t, want["04"], "04")
+    assert t.insert_points(arrays["points_5"], maxd - 1, B.EXPD) == o.insert_points_general(arrays["points_5"], maxd - 1, 4)
+    check_edit(t, want["05"], "05")
+    src = B.Scheme(sc.map, sc.grid, 255, B.INS)
+    assert t.insert_by_image(src, 255, B.EXPD) == o.insert_by_image_general(2, 255, 4)
+    check_edit(t, want["06"], "06")
+    step(t, sc)
+    check_edit(t, want["07"], "07")
+    m = t.transition_matrix(sc, invalid_column=spec.get("invalid", False))
+    d = csr_digests(*m.to_host())
+    for key in ("nnz", "rowptr_sha256", "cols_sha256", "vals_sha256"):
+        assert d[key] == meta["tm"][key], key
+
+
+@pytest.mark.parametrize("name", EDIT_CASES)
+def test_points_into_the_surrounding_box_alone(golden, name):
+    meta, arrays = golden(name)
+    c, r = domain(meta["spec"])
+    t = B.ImplicitBoxTree(c, r)
+    t.set_flags(B.SD, 0)
+    t.insert_points(arrays["points_root"], 6, B.INS, B.HIT)
+    check_edit(t, {x["step"]: x for x in meta["edits"]}["root"], "root")
+
+
+@pytest.mark.parametrize("depth_of", [lambda d: 255, lambda d: d + 3, lambda d: d - 2])
+def test_insert_into_a_one_depth_tree_at_another_depth(golden, depth_of):
+    meta, arrays = golden("henon_d12_mixed6_edits")
+    spec = meta["spec"]
+    c, r = domain(spec)
+    t = B.ImplicitBoxTree(c, r)
+    t.subdivision_run(scheme(spec), 10)
+    o = O.Oracle(oracle_spec(spec))
+    o.subdivision(10)
+    depth = depth_of(10)
+    hit = B.HIT if depth == 255 else 0
+    assert t.insert_points(arrays["points_3"], depth, B.INS, hit) == o.insert_points_general(arrays["points_3"], depth,
+                                                                                           2, hit)
+    for x, y in zip(t.leaves(), o.leaves()):
+        np.testing.assert_array_equal(x, y)
+    # and then a step of the image selection on whatever depths resulted
+    step(t, scheme(spec))
+    o.subdivide(8)
+    o.set_flags_by_image(1)
+    o.remove(1)
+    o.unset_flags(1)
+    for x, y in zip(t.leaves(), o.leaves()):
+        np.testing.assert_array_equal(x, y)
+
+
+def test_unsubdivide_of_a_one_depth_tree(golden):
+    meta, arrays = golden("henon_d12_mixed6_edits")
+    spec = meta["spec"]
+    c, r = domain(spec)
+    t = B.ImplicitBoxTree(c, r)
+    t.subdivision_run(scheme(spec), 12)
+    o = O.Oracle(oracle_spec(spec))
+    o.subdivision(12)
+    codes, depth, flags = t.leaves()
+    mask = (np.arange(len(codes)) % 3 == 0).astype(np.uint8)
+    t.load_leaves(codes, depth, (flags & ~np.uint8(B.SD)) | (mask * B.SD).astype(np.uint8))
+    o.load(codes, depth, (flags & ~np.uint8(8)) | (mask * 8).astype(np.uint8))
+    for _ in range(3):
+        assert t.unsubdivide(B.SD) == o.unsubdivide(8)
+        for x, y in zip(t.leaves(), o.leaves()):
+            np.testing.assert_array_equal(x, y)
+
+
+def test_inner_depth_hit_flags_are_refused(golden):
+    meta, arrays = golden("henon_d8_mixed4_files")
+    t = start(meta, arrays)
+    step(t, scheme(meta["spec"]))
+    before = [a.copy() for a in t.leaves()]
+    with pytest.raises(B.B12gError) as e:
+        t.insert_points(np.zeros((3, 2)), 8, B.INS, B.HIT)
+    assert e.value.status == B._lib.ERR_MIXED_DEPTH
     for x, y in zip(t.leaves(), before):
         np.testing.assert_array_equal(x, y)
