@@ -97,9 +97,16 @@ def test_insert_points_into_a_tree_of_one_depth():
         np.testing.assert_array_equal(x, y)
 
 
-def test_insert_many_distinct_boxes_into_root_is_refused():
+def test_insert_many_distinct_boxes_into_root_merges_like_the_reference():
+    # the surrounding box shares every path: it merges with the new boxes next to it in
+    # tree order (the reference's two HasSamePath scans), so its flags reach some of them
     t = B.ImplicitBoxTree([0.0, 0.0], [1.0, 1.0])
-    with pytest.raises(B.B12gError) as e:
-        t.insert_points(np.array([[0.5, 0.5], [-0.5, -0.5]]), 4)
-    assert e.value.status == 5
-    assert t.count() == 1 and t.depth() == 0
+    t.set_flags(B.SD, 0)
+    pts = np.array([[0.5, 0.5], [-0.5, -0.5], [0.5, -0.5], [-0.9, 0.9]])
+    assert t.insert_points(pts, 4, B.INS) == 4
+    o = O.Oracle(dict(O.henon_spec(), center=np.zeros(2), radius=np.ones(2)))
+    o.set_flags(8)
+    assert o.insert_points_general(pts, 4, 2, 0) == 4
+    for x, y in zip(t.leaves(), o.leaves()):
+        np.testing.assert_array_equal(x, y)
+    assert t.count() == 4 and t.depth() == 4

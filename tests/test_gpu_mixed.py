@@ -262,7 +262,9 @@ def test_unsubdivide_and_insert_match_reference(golden, name):
     src = B.Scheme(sc.map, sc.grid, 255, B.INS)
     assert t.insert_by_image(src, 255, B.EXPD) == o.insert_by_image_general(2, 255, 4)
     check_edit(t, want["06"], "06")
-    step(t, sc)
+    t.set_flags_by_image(sc, B.HIT)
+    t.remove(B.HIT)
+    t.unset_flags(B.HIT)
     check_edit(t, want["07"], "07")
     m = t.transition_matrix(sc, invalid_column=spec.get("invalid", False))
     d = csr_digests(*m.to_host())
