@@ -373,7 +373,7 @@ b12g_status b12g_tree_destroy(b12g_tree* t)
     for (cudaEvent_t e : t->graph_prof[k]) cudaEventDestroy(e);
   }
   for (int b = 0; b < 2; ++b) { t->code[b].release(); t->flags[b].release(); t->dep[b].release(); }
-  t->cmp.release(); t->hash.release(); t->points.release();
+  t->cmp.release(); t->cmp_tab.release(); t->hash.release(); t->points.release();
   t->pvalid.release(); t->ins_dep.release(); t->ins_dep2.release(); t->scan_dep.release(); t->scan_flags.release();
   t->ins_code.release(); t->scan_code.release(); t->ins_pos.release(); t->ins_head.release();
   for (int b = 0; b < 2; ++b) { t->ins_key[b].release(); t->ins_idx[b].release(); }

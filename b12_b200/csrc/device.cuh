@@ -213,6 +213,16 @@ __device__ __forceinline__ bool point_code(const Domain& dom, const double* p, i
     const double s = floor(u * pow2(k[j]));
     bits[j] = uint32_t((unsigned long long)s & ((1ull << k[j]) - 1ull));
   }
+  if constexpr (D == 3) {
+    if (depth == 64) {
+      // 22 + 21 + 21 bits: the first 63 bisections are 21 full rounds, the 64th is the
+      // last bit of dimension 0
+      const uint32_t top[3] = {bits[0] >> 1, bits[1], bits[2]};
+      const int k21[3] = {21, 21, 21};
+      code = (interleave<3>(top, k21, 63) << 1) | uint64_t(bits[0] & 1u);
+      return true;
+    }
+  }
   code = interleave<D>(bits, k, depth);
   return true;
 }

@@ -52,32 +52,75 @@ __device__ __forceinline__ bool on_path(uint64_t p64, uint64_t code, uint32_t de
   return (shift >= 64 ? 0ull : (p64 >> shift)) == code;
 }
 
-// search of one point among the leaves (ImplicitBoxTree.hpp:2394-2432, leaf branch)
-__device__ __forceinline__ uint32_t locate_mixed(const uint64_t* __restrict__ cmp, const uint64_t* __restrict__ code,
-                                                 const uint8_t* __restrict__ dep, uint32_t n, bool valid,
-                                                 uint64_t p64)
+// The leaves' comparable patterns with a prefix table: tab[v] is the first leaf whose
+// pattern is at least v << (64 - bits), tab[2^bits] = n, so the lower bound of a key lies
+// between tab[v] and tab[v + 1] for v = key >> (64 - bits).
+struct CmpIndex {
+  const uint64_t* cmp;
+  const uint32_t* tab;
+  uint32_t n;
+  uint32_t bits;               // 1..24
+};
+
+// first leaf whose comparable pattern is not below `key`
+__device__ __forceinline__ uint32_t lower_bound_idx(const CmpIndex& ix, uint64_t key)
 {
-  if (n == 0) return kInvalidIndex;
-  if (!valid) {
-    // the invalid box shares its path with a last leaf of code 0
-    return __ldg(code + n - 1) == 0 ? n - 1 : kInvalidIndex;
-  }
-  // lower bound: first leaf that does not strictly precede the depth-64 point box
-  uint32_t lo = 0, len = n;
+  const uint32_t v = uint32_t(key >> (64 - ix.bits));
+  uint32_t lo = __ldg(ix.tab + v);
+  uint32_t len = __ldg(ix.tab + v + 1) - lo;
   while (len > 0) {
     const uint32_t half = len >> 1;
-    if (__ldg(cmp + lo + half) < p64) {
+    if (__ldg(ix.cmp + lo + half) < key) {
       lo += half + 1;
       len -= half + 1;
     } else {
       len = half;
     }
   }
+  return lo;
+}
+
+// search of one point among the leaves (ImplicitBoxTree.hpp:2394-2432, leaf branch)
+__device__ __forceinline__ uint32_t locate_mixed(const CmpIndex& ix, const uint64_t* __restrict__ code,
+                                                 const uint8_t* __restrict__ dep, bool valid, uint64_t p64)
+{
+  const uint32_t n = ix.n;
+  if (n == 0) return kInvalidIndex;
+  if (!valid) {
+    // the invalid box shares its path with a last leaf of code 0
+    return __ldg(code + n - 1) == 0 ? n - 1 : kInvalidIndex;
+  }
+  // lower bound: first leaf that does not strictly precede the depth-64 point box
+  const uint32_t lo = lower_bound_idx(ix, p64);
   const uint32_t a = lo > 0 ? lo - 1 : 0;
   const uint32_t b = lo < n - 1 ? lo : n - 1;
   if (on_path(p64, __ldg(code + a), __ldg(dep + a))) return lo > 0 ? lo - 1 : 0;
   if (on_path(p64, __ldg(code + b), __ldg(dep + b))) return lo;
   return kInvalidIndex;
+}
+
+// the prefix table of CmpIndex, 2^bits + 1 entries
+__global__ void cmp_table_kernel(const uint64_t* cmp, uint32_t n, uint32_t bits, uint32_t* tab)
+{
+  const uint32_t entries = (1u << bits) + 1u;
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < entries; v += gridDim.x * blockDim.x) {
+    if (v == entries - 1) {
+      tab[v] = n;
+      continue;
+    }
+    const uint64_t key = uint64_t(v) << (64 - bits);
+    uint32_t lo = 0, len = n;
+    while (len > 0) {
+      const uint32_t half = len >> 1;
+      if (cmp[lo + half] < key) {
+        lo += half + 1;
+        len -= half + 1;
+      } else {
+        len = half;
+      }
+    }
+    tab[v] = lo;
+  }
 }
 
 __global__ void comparable_kernel(const uint64_t* code, const uint8_t* dep, uint32_t n, uint64_t* cmp)
@@ -249,22 +292,6 @@ __device__ __forceinline__ Bx change_depth_to(Bx b, uint32_t depth)
   return b;
 }
 
-// first leaf whose comparable pattern is not below `key`
-__device__ __forceinline__ uint32_t lower_bound_cmp(const uint64_t* __restrict__ cmp, uint32_t n, uint64_t key)
-{
-  uint32_t lo = 0, len = n;
-  while (len > 0) {
-    const uint32_t half = len >> 1;
-    if (__ldg(cmp + lo + half) < key) {
-      lo += half + 1;
-      len -= half + 1;
-    } else {
-      len = half;
-    }
-  }
-  return lo;
-}
-
 // unsubdivide, IsUnsubdividableFunctor (Functors.hpp:343-364): marks and their number
 __global__ void unsub_mark_kernel(const uint64_t* code, const uint8_t* dep, const uint8_t* flags, uint32_t n, uint8_t f,
                                   uint32_t* mark, uint32_t* count)
@@ -322,6 +349,8 @@ struct InsertArgs {
   const uint64_t* code;        // leaves
   const uint8_t* dep;
   const uint64_t* cmp;
+  const uint32_t* tab;         // prefix table of cmp (CmpIndex)
+  uint32_t tab_bits;
   uint32_t n;
   uint32_t depth;              // insertion depth; 255: the leaf depth
   int mode;                    // 0: leaf depth, 2: below an existing depth, 3: deeper than every leaf
@@ -343,7 +372,7 @@ __global__ void insert_boxes_kernel(const InsertArgs a)
     if (a.mode == 0) {
       // searchByIterators at the leaf depth, then the leaf-depth rule (1672-1702):
       // a point in no leaf is inserted if valid, one in a leaf if that leaf is above depth 64
-      lo = valid ? lower_bound_cmp(a.cmp, a.n, p.c) : a.n;
+      lo = valid ? lower_bound_idx(CmpIndex{a.cmp, a.tab, a.n, a.tab_bits}, p.c) : a.n;
       const uint32_t ia = lo > 0 ? lo - 1 : 0, ib = lo < a.n - 1 ? lo : a.n - 1;
       uint32_t s = kInvalidIndex;
       if (same_path(p, load_box(a.code, a.dep, nullptr, ia))) s = lo > 0 ? lo - 1 : 0;
@@ -357,7 +386,7 @@ __global__ void insert_boxes_kernel(const InsertArgs a)
       if (valid) {
         const int sh = 64 - int(a.depth);
         const uint64_t q = srs(p.c, sh);
-        const uint32_t j = lower_bound_cmp(a.cmp, a.n, sls(q, sh));
+        const uint32_t j = lower_bound_idx(CmpIndex{a.cmp, a.tab, a.n, a.tab_bits}, sls(q, sh));
         found = j < a.n && a.dep[j] >= a.depth && srs(a.code[j], int(a.dep[j]) - int(a.depth)) == q;
       }
       to_insert = valid && !found;
@@ -524,6 +553,8 @@ struct MixedArgs {
   const uint64_t* code;
   const uint8_t* dep;
   const uint64_t* cmp;
+  const uint32_t* tab;         // prefix table of cmp (CmpIndex)
+  uint32_t tab_bits;
   uint32_t n;                  // leaves
   const uint32_t* src;         // source leaves (nullptr: every leaf)
   uint32_t n_src;
@@ -584,7 +615,7 @@ __device__ __forceinline__ uint32_t image_of(const MixedArgs& a, const double* p
 {
   uint64_t p64;
   const bool valid = image_code<Map, Grid>(a, pts, table, leaf, k, g, p64);
-  return locate_mixed(a.cmp, a.code, a.dep, a.n, valid, p64);
+  return locate_mixed(CmpIndex{a.cmp, a.tab, a.n, a.tab_bits}, a.code, a.dep, valid, p64);
 }
 
 // kMode 0: hit marks of the leaves hit; 1: leaf index of every point; 2: the points'
@@ -694,7 +725,14 @@ b12g_status refresh_comparable(b12g_tree* t)
 {
   ST(t->cmp.ensure(std::max<uint32_t>(t->n, 1), "comparable patterns"));
   comparable_kernel<<<grid_for_n(t->n), kThreads, 0, t->stream>>>(t->codes(), dep_cur(t), t->n, t->cmp.p);
-  count_launches(1);
+  // about two table entries per leaf, 4 .. 22 bits
+  uint32_t bits = 4;
+  while (bits < 22 && (1ull << bits) < 2ull * t->n) ++bits;
+  t->cmp_bits = bits;
+  ST(t->cmp_tab.ensure((size_t(1) << bits) + 1, "pattern prefix table"));
+  cmp_table_kernel<<<grid_for_n((uint64_t(1) << bits) + 1), kThreads, 0, t->stream>>>(t->cmp.p, t->n, bits,
+                                                                                       t->cmp_tab.p);
+  count_launches(2);
   return B12G_OK;
 }
 
@@ -736,6 +774,8 @@ b12g_status mixed_args(b12g_tree* t, const b12g_scheme* sc, MixedArgs& a)
   a.n = t->n;
   ST(refresh_comparable(t));
   a.cmp = t->cmp.p;
+  a.tab = t->cmp_tab.p;
+  a.tab_bits = t->cmp_bits;
   return B12G_OK;
 }
 
@@ -1001,6 +1041,8 @@ b12g_status mixed_insert_boxes(b12g_tree* t, uint64_t np, uint8_t depth, uint8_t
   a.code = t->codes();
   a.dep = dep_cur(t);
   a.cmp = t->cmp.p;
+  a.tab = t->cmp_tab.p;
+  a.tab_bits = t->cmp_bits;
   a.n = t->n;
   a.depth = depth;
   a.mode = mode;

@@ -117,6 +117,8 @@ struct b12g_tree {
   bool mixed = false;
   Buf<uint8_t> dep[2];
   Buf<uint64_t> cmp;
+  Buf<uint32_t> cmp_tab;       // prefix table over cmp: first leaf per top-bits value
+  uint32_t cmp_bits = 1;
   // insertion into such trees: point-box validity, new boxes, their sort, the merge scans
   Buf<uint8_t> pvalid, ins_dep, ins_dep2, scan_dep, scan_flags;
   Buf<uint64_t> ins_code, ins_key[2], scan_code;

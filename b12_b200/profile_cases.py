@@ -13,6 +13,9 @@ sort      the coupled-Duffing continuation at depth 24 (64 Philox points per box
 measure   one Lorenz job to --depth (default 27), its transition matrix and 200 power
           iterations; depth 32 gives ~2.6 M boxes, a matrix of ~0.25 GB (HBM-bound SpMV).
 serve     a burst of --jobs served-stream jobs through the job server.
+mixed     a Lorenz tree (explicit FMA) refined to --depth (default 21), SD kept on the
+          lower half in x, four selective steps (leaves of depths d..d+4), then one more
+          subdivide and set_flags_by_image: the per-leaf-depth image kernel over the tree.
 
 Every case prints one line of sizes; none writes files.
 """
@@ -106,18 +109,39 @@ def case_serve(args):
         print(f"serve: {args.jobs} jobs in {res['span']:.3f} s, {srv.stats()['ticks']} ticks")
 
 
+def case_mixed(args):
+    import b12_b200 as B
+    from b12_b200.workloads import LORENZ_CENTER, LORENZ_RADIUS
+    t = B.ImplicitBoxTree(LORENZ_CENTER, LORENZ_RADIUS)
+    sc = B.Scheme(B.lorenz(fma=True), B.inner_grid(5))
+    t.subdivision_run(sc, args.depth)
+    codes, depth, flags = t.leaves()
+    lower = (codes >> np.uint64(args.depth - 1)) == 0
+    t.load_leaves(codes, depth, ((flags & ~np.uint8(B.SD)) | np.where(lower, B.SD, 0)).astype(np.uint8))
+    for _ in range(5):
+        t.subdivide(B.SD)
+        n = t.count()
+        hits = t.set_flags_by_image(sc, B.HIT)
+        t.remove(B.HIT)
+        t.unset_flags(B.HIT)
+    d = t.leaves()[1]
+    print(f"mixed: last image launch over {n} boxes ({n * 125} points), {hits} hit; depths {d.min()}-{d.max()}")
+    t.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["image", "compact", "sort", "measure", "serve"])
+    ap.add_argument("case", choices=["image", "compact", "sort", "measure", "serve", "mixed"])
     ap.add_argument("--depth", type=int, default=None)
     ap.add_argument("--instances", type=int, default=64)
     ap.add_argument("--jobs", type=int, default=300)
     ap.add_argument("--repeat", type=int, default=1, help="measure: timed calls after the first")
     args = ap.parse_args()
     if args.depth is None:
-        args.depth = {"image": 23, "compact": 27, "sort": 24, "measure": 27, "serve": 0}[args.case]
+        args.depth = {"image": 23, "compact": 27, "sort": 24, "measure": 27, "serve": 0,
+                      "mixed": 21}[args.case]
     {"image": case_image, "compact": case_compact, "sort": case_sort, "measure": case_measure,
-     "serve": case_serve}[args.case](args)
+     "serve": case_serve, "mixed": case_mixed}[args.case](args)
 
 
 if __name__ == "__main__":

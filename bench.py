@@ -417,6 +417,42 @@ def configs_mode(args, peak_tflops: float):
         "note": "every box is imaged once, in the sweep after it was inserted"}
     t.close()
 
+    # selective refinement (leaves of several depths): Lorenz (explicit FMA) refined to
+    # depth 21, SD kept on the leaves of the lower half in x, then 6 steps that subdivide
+    # and select only those, and the CSR of the final tree (depths 21-27)
+    sc = B.Scheme(B.lorenz(fma=True), B.inner_grid(5))
+    t = B.ImplicitBoxTree(LORENZ_CENTER, LORENZ_RADIUS)
+    t.subdivision_run(sc, 21)
+    codes, depth, flags = t.leaves()
+    lower = (codes >> np.uint64(20)) == 0
+    start = (codes, depth, ((flags & ~np.uint8(B.SD)) | np.where(lower, B.SD, 0)).astype(np.uint8))
+
+    def selective():
+        t.load_leaves(*start)
+        imaged = 0
+        for _ in range(6):
+            t.subdivide(B.SD)
+            imaged += t.count()
+            t.set_flags_by_image(sc, B.HIT)
+            t.remove(B.HIT)
+            t.unset_flags(B.HIT)
+        m = t.transition_matrix(sc)
+        nnz = m.nnz
+        m.close()
+        d = t.leaves()[1]
+        return imaged, t.count(), nnz, int(d.min()), int(d.max())
+
+    sec, (imaged, nf, nnz, dmin, dmax) = _timed(selective, 3)
+    flop = P * FLOP_PER_POINT
+    out["lorenz_selective_d21_plus6"] = {
+        "start_boxes": int(len(codes)), "final_boxes": nf, "depths": [dmin, dmax], "nnz": nnz,
+        "box_images": imaged + nf, "seconds": sec, "box_images_per_s": (imaged + nf) / sec,
+        "tflops": (imaged + nf) * flop / sec / 1e12,
+        "frac_of_fp64_peak": (imaged + nf) * flop / sec / 1e12 / peak_tflops,
+        "note": "per-leaf-depth kernels (binary search over comparable patterns); includes the "
+                "reload of the depth-21 start leaves from the host and every host round trip"}
+    t.close()
+
     # 512 Lorenz instances, rho ~ U[15,35], depth 18-27 (SplitMix64 seed 0): batched
     rho, depth = lorenz_scan(512, 0)
     params = [(10.0, r, 8.0 / 3.0) for r in rho]
