@@ -550,9 +550,14 @@ def serve_mode(args):
         # warm-up on a burst of other jobs: engines created, buffers and the result pool grown
         warm = [dict(j, arrival=0.0) for j in job_stream(min(n, 1000), 1.0, 1)]
         replay(srv, warm, lambda job, jid: srv.release(jid), timeout=SERVE_TIMEOUT)
-        # saturated: every job submitted at once; each result checked against the plain path
-        # and released as it arrives (a resident result counts against the admission cap)
+        # saturated: every job submitted at once and released as it finishes (a resident
+        # result counts against the admission cap), as the plain path frees each tree; the
+        # results stay on the device in both, so neither timing reads them back
         sat = [dict(j, arrival=0.0) for j in base]
+        res = replay(srv, sat, lambda job, jid: srv.release(jid), timeout=SERVE_TIMEOUT)
+        out["served_saturated"] = {"jobs_per_s": n / res["span"], "span_s": res["span"],
+                                   "p50_ms": _pct(res["latency"], 50), "p99_ms": _pct(res["latency"], 99)}
+        # the same burst again, untimed: every result read and checked against the plain path
         check = {"shape": 0, "digest": 0}
 
         def check_and_release(job, jid):
@@ -568,13 +573,12 @@ def serve_mode(args):
             check["shape"] += (tuple(int(c) for c in counts), int(inf["nnz"])) == plain_shape[k]
             srv.release(jid)
 
-        res = replay(srv, sat, check_and_release, timeout=SERVE_TIMEOUT)
+        replay(srv, sat, check_and_release, timeout=SERVE_TIMEOUT)
         same_shape, same = check["shape"], check["digest"]
-        out["served_saturated"] = {"jobs_per_s": n / res["span"], "span_s": res["span"],
-                                   "p50_ms": _pct(res["latency"], 50), "p99_ms": _pct(res["latency"], 99)}
         out["identical_to_plain"] = {"step_counts_and_nnz": f"{same_shape}/{n}",
-                                     "full_result_sha256": f"{same}/{len(plain_digest)}"}
-        out["jobs_per_s_vs_plain"] = (n / res["span"]) / plain_rate
+                                     "full_result_sha256": f"{same}/{len(plain_digest)}",
+                                     "pass": "a second, untimed saturated burst whose results are read back"}
+        out["jobs_per_s_vs_plain"] = out["served_saturated"]["jobs_per_s"] / plain_rate
         sweep = []
         for rate in SERVE_RATES:
             st = job_stream(n, rate, 0)
