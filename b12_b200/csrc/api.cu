@@ -214,9 +214,12 @@ b12g_status set_root(b12g_tree* t, uint8_t flags)
 b12g_status flag_call(b12g_tree* t, int op, uint8_t u, uint8_t f, uint8_t depth, uint32_t* n_changed)
 {
   if (!t) return fail(B12G_ERR_INVALID, "NULL tree");
-  if (t->mixed && depth != 0 && depth != B12G_LEAF_DEPTH)
-    return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "flags of a tree of mixed depths change at depth 0 or 255");
-  if (depth != 0) ST(check_depth(t, depth));
+  if (depth != 0 && depth != B12G_LEAF_DEPTH && (t->mixed || depth != t->depth)) {
+    // the boxes at a depth that is not every leaf's own: all leaves of each box change
+    if (depth == 254) return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "flags at the unsubdividable depth 254");
+    if (depth > 64) return fail(B12G_ERR_INVALID, "depth %u above the maximal depth 64", depth);
+    return mixed_flags_at_depth(t, op, u, f, depth, n_changed);
+  }
   ST(set_ctr(t, C_CHANGED, 0));
   CK(flag_op(t->flg(), t->dn(), op, u, f, t->ctr.p + C_CHANGED, t->n, t->stream));
   count_launches(1);

@@ -154,6 +154,62 @@ __global__ void new_box_kernel(const uint64_t* code, const uint8_t* dep, uint32_
   if (c) atomicAdd(count, c);
 }
 
+// ---- flags of the boxes at an inner depth d: a box is a run of leaves at least d deep
+// with one d-prefix; head[i] marks the run's first leaf, and after a scan pos[i + 1] - 1
+// is the box of leaf i
+__global__ void box_head_kernel(const uint64_t* code, const uint8_t* dep, uint32_t n, uint32_t d, uint32_t* head)
+{
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    bool fresh = false;
+    if (dep[i] >= d) {
+      fresh = i == 0 || dep[i - 1] < d;
+      if (!fresh) fresh = (code[i - 1] >> (dep[i - 1] - d)) != (code[i] >> (dep[i] - d));
+    }
+    head[i] = fresh ? 1u : 0u;
+  }
+}
+
+// every box's AND and OR of its leaves' flags (box_and starts all ones, box_or zero)
+__global__ void box_combine_kernel(const uint8_t* flags, const uint8_t* dep, uint32_t n, uint32_t d,
+                                   const uint32_t* pos, uint32_t* box_and, uint32_t* box_or)
+{
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (dep[i] < d) continue;
+    const uint32_t b = pos[i + 1] - 1;
+    atomicAnd(box_and + b, uint32_t(flags[i]));
+    atomicOr(box_or + b, uint32_t(flags[i]));
+  }
+}
+
+// op 0: setFlags (boxes whose AND lacked f), 1: unsetFlags (boxes whose OR had any of f),
+// 2: changeFlags (boxes whose AND has all of u: their leaves change); counts those boxes
+__device__ __forceinline__ bool box_selected(int op, uint32_t all, uint32_t any, uint8_t u, uint8_t f)
+{
+  if (op == 0) return (all & f) != f;
+  if (op == 1) return (any & f) != 0;
+  return (all & u) == u;
+}
+
+__global__ void box_apply_kernel(uint8_t* flags, const uint8_t* dep, uint32_t n, uint32_t d, const uint32_t* pos,
+                                 const uint32_t* box_and, const uint32_t* box_or, uint32_t n_boxes, int op, uint8_t u,
+                                 uint8_t f, uint32_t* count)
+{
+  uint32_t c = 0;
+  for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < n_boxes; b += gridDim.x * blockDim.x)
+    c += box_selected(op, box_and[b], box_or[b], u, f);
+  if (c) atomicAdd(count, c);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (dep[i] < d) continue;
+    const uint8_t x = flags[i];
+    if (op == 0) flags[i] = x | f;
+    else if (op == 1) flags[i] = x & uint8_t(~f);
+    else {
+      const uint32_t b = pos[i + 1] - 1;
+      if (box_selected(2, box_and[b], box_or[b], u, f)) flags[i] = uint8_t(x & uint8_t(~u)) | f;
+    }
+  }
+}
+
 // subdivide: a flagged leaf below depth 64 becomes its two halves in place (order kept)
 __global__ void split_count_kernel(const uint8_t* flags, const uint8_t* dep, uint32_t n, uint8_t f, uint32_t* cnt)
 {
@@ -833,6 +889,41 @@ b12g_status mixed_load(b12g_tree* t, const uint64_t* codes, const uint8_t* depth
   t->mixed = true;
   ST(set_ctr(t, t->ncur, n));
   ST(sync(t, "load leaves"));
+  return mixed_settle(t);
+}
+
+// setFlags / unsetFlags / changeFlags (op 0 / 1 / 2) at a depth inside the tree: every
+// leaf of a box at that depth changes (setFlagsByStencil, unsetFlagsByStencil,
+// changeFlagsByStencil with a true stencil, ImplicitBoxTree.hpp:914-1058, 2805-2882,
+// 3336-3411); *n_changed counts boxes as countIfFlags does (1104-1200).  A depth below
+// no leaf changes nothing.
+b12g_status mixed_flags_at_depth(b12g_tree* t, int op, uint8_t u, uint8_t f, uint8_t depth, uint32_t* n_changed)
+{
+  if (n_changed) *n_changed = 0;
+  if (depth == 0 || depth > 64) return fail(B12G_ERR_INVALID, "inner depth %u", depth);
+  if (depth > t->depth) return B12G_OK;
+  ST(mixed_enter(t));
+  const uint32_t n = t->n;
+  ST(t->row_count.ensure(uint64_t(n) + 1, "box heads"));
+  ST(t->rowptr.ensure(uint64_t(n) + 1, "box positions"));
+  ST(t->src.ensure(std::max<uint32_t>(n, 1), "box flags"));
+  ST(t->out.ensure(std::max<uint32_t>(n, 1), "box flags"));
+  box_head_kernel<<<grid_for_n(n), kThreads, 0, t->stream>>>(t->codes(), dep_cur(t), n, depth, t->row_count.p);
+  count_launches(1);
+  uint32_t boxes = 0;
+  ST(scan_marks(t, t->row_count.p, t->rowptr.p, n, &boxes));
+  if (boxes) {
+    CK(cudaMemsetAsync(t->src.p, 0xFF, size_t(boxes) * 4, t->stream));
+    CK(cudaMemsetAsync(t->out.p, 0, size_t(boxes) * 4, t->stream));
+    ST(set_ctr(t, C_CHANGED, 0));
+    box_combine_kernel<<<grid_for_n(n), kThreads, 0, t->stream>>>(t->flg(), dep_cur(t), n, depth, t->rowptr.p,
+                                                                   t->src.p, t->out.p);
+    box_apply_kernel<<<grid_for_n(std::max(n, boxes)), kThreads, 0, t->stream>>>(
+        t->flg(), dep_cur(t), n, depth, t->rowptr.p, t->src.p, t->out.p, boxes, op, u, f, t->ctr.p + C_CHANGED);
+    count_launches(2);
+    ST(read_ctr(t, C_CHANGED, 1));
+    if (n_changed) *n_changed = t->h_ctr[C_CHANGED];
+  }
   return mixed_settle(t);
 }
 

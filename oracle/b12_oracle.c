@@ -750,6 +750,44 @@ uint32_t orc_unsubdivide(orc_tree* t, uint8_t flags)
   return (uint32_t)res;
 }
 
+/* setFlags / unsetFlags / changeFlags (op 0 / 1 / 2) at a depth that is neither the
+ * leaves' own nor 0 (setFlagsByStencil, unsetFlagsByStencil, changeFlagsByStencil with a
+ * true stencil, ImplicitBoxTree.hpp:914-1058, 2805-2882, 3336-3411; countIfFlags
+ * 1104-1200): a box at that depth is a run of leaves at least that deep with one prefix;
+ * its flags are its leaves' AND (set, change) or OR (unset).  Every leaf of the box
+ * changes (change: only the boxes whose AND has all of u); the count is of the boxes
+ * whose combined flags lacked f (set), had any of f (unset) or had all of u (change).
+ * Depths above the deepest leaf change nothing. */
+uint32_t orc_flags_at_depth(orc_tree* t, int op, uint8_t u, uint8_t f, uint32_t depth)
+{
+  const uint64_t n = t->n;
+  uint32_t count = 0;
+  uint64_t i = 0;
+  while (i < n) {
+    if (t->depth[i] < depth) { ++i; continue; }
+    const uint64_t pre = t->code[i] >> (t->depth[i] - depth);
+    uint64_t j = i;
+    uint8_t all = 0xFF, any = 0;
+    while (j < n && t->depth[j] >= depth && (t->code[j] >> (t->depth[j] - depth)) == pre) {
+      all &= t->flags[j];
+      any |= t->flags[j];
+      ++j;
+    }
+    int hit;
+    if (op == 0) hit = !flags_set(all, f);
+    else if (op == 1) hit = (any & f) != 0;
+    else hit = flags_set(all, u);
+    count += hit;
+    for (uint64_t k = i; k < j; ++k) {
+      if (op == 0) t->flags[k] |= f;
+      else if (op == 1) t->flags[k] &= (uint8_t)~f;
+      else if (hit) t->flags[k] = (uint8_t)((t->flags[k] & ~u) | f);
+    }
+    i = j;
+  }
+  return count;
+}
+
 /* computeDepthOfMutualAncestor (Box.hpp:209-223) */
 static inline uint32_t mutual_ancestor(obox a, obox b)
 {

@@ -103,6 +103,9 @@ void orc_delete_depth0(orc_tree* t);
 /* trees of mixed depths: unsubdivide, and insertByIterators for any tree and depth
  * (255 = leaf depth); *unsupported is set for flags on hit boxes at an inner depth */
 uint32_t orc_unsubdivide(orc_tree* t, uint8_t flags);
+/* set / unset / change (op 0 / 1 / 2) flags of the boxes at an inner depth; for change, u
+ * is unset and f set */
+uint32_t orc_flags_at_depth(orc_tree* t, int op, uint8_t u, uint8_t f, uint32_t depth);
 uint32_t orc_insert_boxes(orc_tree* t, const uint64_t* code64, const uint8_t* valid, uint64_t n_points,
                           uint32_t depth, uint8_t ins, uint8_t hit, int* unsupported);
 uint32_t orc_insert_points_general(orc_tree* t, const double* pts, uint64_t n_points, uint32_t depth, uint8_t ins,

@@ -81,6 +81,7 @@ def lib():
             "orc_insert_points": (u32, [P(OrcTree), P(dbl), u64, u32, u8, u8]),
             "orc_delete_depth0": (None, [P(OrcTree)]),
             "orc_unsubdivide": (u32, [P(OrcTree), u8]),
+            "orc_flags_at_depth": (u32, [P(OrcTree), C.c_int, u8, u8, u32]),
             "orc_insert_points_general": (u32, [P(OrcTree), P(dbl), u64, u32, u8, u8, P(C.c_int)]),
             "orc_insert_by_image_general": (u32, [P(OrcTree), P(OrcMap), P(OrcGrid), u8, u32, u8, u8,
                                                   P(C.c_int)]),
@@ -219,6 +220,10 @@ class Oracle:
     def delete_depth0(self): self.L.orc_delete_depth0(C.byref(self.tree))
 
     def unsubdivide(self, f): return self.L.orc_unsubdivide(C.byref(self.tree), f)
+
+    def flags_at_depth(self, op, u, f, depth):
+        """set (0) / unset (1) / change (2, u -> f) flags of the boxes at an inner depth"""
+        return self.L.orc_flags_at_depth(C.byref(self.tree), op, u, f, depth)
 
     def insert_points_general(self, pts, depth, ins=2, hit=0):
         """insertByPoints for any tree and depth (255: leaf depth); None if not restated"""

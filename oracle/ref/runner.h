@@ -136,8 +136,19 @@ void runEdits(Tree& ibt, const std::vector<double>& c, const std::vector<double>
   ibt.setFlagsByIterators(ibt.makePointIteratorPairOverLeaves(grid, map), Flag::HIT, getLeafDepth());
   ibt.remove(Flag::HIT);
   ibt.unsetFlags(Flag::HIT, getLeafDepth());
-  js << ", " << ibt.count(getLeafDepth()) << "], \"edit_max_depth\": " << maxd;
+  js << ", " << ibt.count(getLeafDepth());
   dump(7);
+  // flags of the boxes at inner depths (setFlags / changeFlags / unsetFlags with a depth
+  // below the deepest leaf: every leaf of such a box changes, ImplicitBoxTree.hpp:914-1058,
+  // 2805-2882, 3336-3411); the return values count the boxes
+  const int md = int(ibt.depth());
+  js << ", " << ibt.setFlags(Flag::EXPD, Depth(md - 2));
+  dump(8);
+  js << ", " << ibt.changeFlags(Flag::EXPD, Flag::INS, Depth(md - 3));
+  dump(9);
+  js << ", " << ibt.unsetFlags(Flag::INS, Depth(md - 1));
+  dump(10);
+  js << "], \"edit_max_depth\": " << maxd << ", \"edit_flag_depth\": " << md;
 }
 
 // Selective refinement: SD stays only on the leaves in the lower half of the first

@@ -208,7 +208,7 @@ def test_unsupported_calls_refuse_and_leave_the_tree(golden):
     sc = scheme(meta["spec"])
     step(t, sc)
     before = [a.copy() for a in t.leaves()]
-    for call in (lambda: t.set_flags(B.EXPD, 5), lambda: t.set_flags_by_image(sc, B.HIT, 9),
+    for call in (lambda: t.set_flags(B.EXPD, 254), lambda: t.set_flags_by_image(sc, B.HIT, 9),
                  lambda: t.insert_by_image(B.Scheme(sc.map, sc.grid, 9, B.INS), 9),
                  lambda: t.search_by_image(sc, 9)):
         with pytest.raises(B.B12gError) as e:
@@ -266,6 +266,16 @@ def test_unsubdivide_and_insert_match_reference(golden, name):
     t.remove(B.HIT)
     t.unset_flags(B.HIT)
     check_edit(t, want["07"], "07")
+    # flags of the boxes at inner depths: every leaf of such a box changes
+    md = meta["timing"]["edit_flag_depth"]
+    counts = meta["timing"]["edits"]
+    assert t.depth() == md
+    assert t.set_flags(B.EXPD, md - 2) == counts[7]
+    check_edit(t, want["08"], "08")
+    assert t.change_flags(B.EXPD, B.INS, md - 3) == counts[8]
+    check_edit(t, want["09"], "09")
+    assert t.unset_flags(B.INS, md - 1) == counts[9]
+    check_edit(t, want["10"], "10")
     m = t.transition_matrix(sc, invalid_column=spec.get("invalid", False))
     d = csr_digests(*m.to_host())
     for key in ("nnz", "rowptr_sha256", "cols_sha256", "vals_sha256"):
@@ -335,3 +345,30 @@ def test_inner_depth_hit_flags_are_refused(golden):
     assert e.value.status == B._lib.ERR_MIXED_DEPTH
     for x, y in zip(t.leaves(), before):
         np.testing.assert_array_equal(x, y)
+
+
+@pytest.mark.parametrize("op", [0, 1, 2])
+def test_flags_at_an_inner_depth_of_a_one_depth_tree(golden, op):
+    meta, arrays = golden("henon_d12_mixed6_edits")
+    spec = meta["spec"]
+    c, r = domain(spec)
+    t = B.ImplicitBoxTree(c, r)
+    t.subdivision_run(scheme(spec), 12)
+    o = O.Oracle(oracle_spec(spec))
+    o.subdivision(12)
+    codes, depth, flags = t.leaves()
+    mask = ((codes * np.uint64(2654435761)) >> np.uint64(7)) % np.uint64(3) == 0   # some leaves carry EXPD
+    f2 = (flags | np.where(mask, B.EXPD, 0)).astype(np.uint8)
+    t.load_leaves(codes, depth, f2)
+    o.load(codes, depth, f2)
+    for d in (3, 9, 11, 13):
+        if op == 0:
+            got, want = t.set_flags(B.INS, d), o.flags_at_depth(0, 0, 2, d)
+        elif op == 1:
+            got, want = t.unset_flags(B.EXPD, d), o.flags_at_depth(1, 0, 4, d)
+        else:
+            got, want = t.change_flags(B.EXPD, B.HIT, d), o.flags_at_depth(2, 4, 1, d)
+        assert got == want, d
+        for x, y in zip(t.leaves(), o.leaves()):
+            np.testing.assert_array_equal(x, y)
+        assert t.depth() == 12

@@ -87,6 +87,10 @@ def edit_sequence(o, meta, arrays):
     o.remove(1)
     o.unset_flags(1)
     yield "07", None
+    md = meta["timing"]["edit_flag_depth"]
+    yield "08", o.flags_at_depth(0, 0, 4, md - 2)        # setFlags(EXPD, md - 2)
+    yield "09", o.flags_at_depth(2, 4, 2, md - 3)        # changeFlags(EXPD, INS, md - 3)
+    yield "10", o.flags_at_depth(1, 0, 2, md - 1)        # unsetFlags(INS, md - 1)
 
 
 @pytest.mark.parametrize("name", EDIT_CASES)
@@ -105,8 +109,8 @@ def test_unsubdivide_and_insert_match_reference(golden, name):
         assert sha(codes) == e["codes_sha256"], f"{key} codes"
         assert sha(depth) == e["depth_sha256"], f"{key} depths"
         assert sha(flags) == e["flags_sha256"], f"{key} flags"
-        if key in ("01", "02"):
-            assert ret == counts[k], key          # unsubdivide's return value
+        if key in ("01", "02", "08", "09", "10"):
+            assert ret == counts[k], key          # the call's own return value
         else:
             assert len(codes) == counts[k], key   # the run records the leaf count
 
