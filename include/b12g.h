@@ -20,10 +20,11 @@
  *   - Leaves may have different depths, as in the reference (kept in the order of
  *     isStrictlyPreceding, Box.hpp:124-135).  A tree whose leaves share one depth runs
  *     the fused single-depth kernels; subdividing some of its leaves, or loading leaves
- *     of several depths, switches it to per-leaf depths until one depth is left.  On a
- *     tree of mixed depths, flags change at depth 0 or 255, schemes map the leaves
- *     (depth 255) and insertion is not offered; those calls return
- *     B12G_ERR_UNSUPPORTED_MIXED_DEPTH and leave the tree unchanged.
+ *     of several depths, switches it to per-leaf depths until one depth is left.  Flags
+ *     at a depth inside the tree change every leaf of each box at that depth.  On a
+ *     tree of mixed depths schemes map the leaves (depth 255); the unsubdividable depth
+ *     254 is not offered; those calls return B12G_ERR_UNSUPPORTED_MIXED_DEPTH and leave
+ *     the tree unchanged.
  *   - Host pointers are plain host memory (pinned or pageable); the library owns all
  *     device memory of a tree and of a CSR matrix.
  */

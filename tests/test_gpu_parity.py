@@ -217,10 +217,14 @@ def test_subdividing_one_leaf_gives_two_depths():
     for x, y in zip(t.leaves(), o.leaves()):
         np.testing.assert_array_equal(x, y)
     assert t.count() == len(codes) + 1 and t.depth() == depth[0] + 1 and t.count(int(depth[0])) == len(codes)
-    # inner-depth flag changes of a tree of mixed depths are refused and change nothing
+    # the shallower depth is now an inner depth for the split box: its two halves are one box
+    assert t.set_flags(B.EXPD, int(depth[0])) == o.flags_at_depth(0, 0, 4, int(depth[0]))
+    for x, y in zip(t.leaves(), o.leaves()):
+        np.testing.assert_array_equal(x, y)
+    # the unsubdividable depth 254 stays refused and changes nothing
     before = [a.copy() for a in t.leaves()]
     with pytest.raises(B.B12gError) as e:
-        t.set_flags(B.EXPD, int(depth[0]))
+        t.set_flags(B.HIT, 254)
     assert e.value.status == 5
     for x, y in zip(t.leaves(), before):
         np.testing.assert_array_equal(x, y)
