@@ -555,7 +555,8 @@ b12g_status b12g_set_flags_by_image(b12g_tree* t, const b12g_scheme* sc, uint8_t
                                     uint32_t* n_changed)
 {
   if (!t) return fail(B12G_ERR_INVALID, "NULL tree");
-  if (t->mixed) return mixed_set_flags_by_image(t, sc, flags, depth, n_changed);
+  if (t->mixed || (depth != B12G_LEAF_DEPTH && depth != t->depth))
+    return mixed_set_flags_by_image(t, sc, flags, depth, n_changed);
   ST(check_depth(t, depth));
   Prepared pr;
   ST(prepare(t, sc, pr));
@@ -581,17 +582,19 @@ b12g_status b12g_search_by_image(b12g_tree* t, const b12g_scheme* sc, uint8_t de
                                  uint64_t* n_points)
 {
   if (!t) return fail(B12G_ERR_INVALID, "NULL tree");
-  if (t->mixed) {
-    if (depth != B12G_LEAF_DEPTH)
-      return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "a tree of mixed depths is searched at its leaves (255)");
+  if (t->mixed || (depth != B12G_LEAF_DEPTH && depth != t->depth)) {
+    // leaves of several depths, or a depth inside the tree: the index of each point's
+    // leaf, or of its box at that depth
     uint64_t np = 0;
-    ST(mixed_search(t, sc, &np));
+    if (depth == B12G_LEAF_DEPTH) ST(mixed_search(t, sc, &np));
+    else ST(mixed_image_at_depth(t, sc, depth, 0, true, &np, nullptr));
     if (n_points) *n_points = np;
-    if (!out) return sync(t, "search_by_image");
-    if (capacity < np) return fail(B12G_ERR_CAPACITY, "output holds %llu of %llu points", (unsigned long long)capacity,
-                                   (unsigned long long)np);
-    CK(cudaMemcpyAsync(out, t->out.p, np * 4, cudaMemcpyDeviceToHost, t->stream));
-    return sync(t, "search_by_image");
+    if (out && capacity < np)
+      return fail(B12G_ERR_CAPACITY, "output holds %llu of %llu points", (unsigned long long)capacity,
+                  (unsigned long long)np);
+    if (out) CK(cudaMemcpyAsync(out, t->out.p, np * 4, cudaMemcpyDeviceToHost, t->stream));
+    ST(sync(t, "search_by_image"));
+    return mixed_settle(t);
   }
   ST(check_depth(t, depth));
   Prepared pr;

@@ -210,6 +210,21 @@ __global__ void box_apply_kernel(uint8_t* flags, const uint8_t* dep, uint32_t n,
   }
 }
 
+// flags f on every leaf of the boxes marked hit; counts the marked boxes whose leaves did
+// not all have f (setFlagsBySearch below the leaves: a stencil over the boxes, then
+// setFlagsByStencil, ImplicitBoxTree.hpp:2776-2800, 2805-2882)
+__global__ void box_hit_apply_kernel(uint8_t* flags, const uint8_t* dep, uint32_t n, uint32_t d, const uint32_t* pos,
+                                     const uint32_t* box_and, const uint8_t* box_hit, uint32_t n_boxes, uint8_t f,
+                                     uint32_t* count)
+{
+  uint32_t c = 0;
+  for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < n_boxes; b += gridDim.x * blockDim.x)
+    c += box_hit[b] && (box_and[b] & f) != f;
+  if (c) atomicAdd(count, c);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    if (dep[i] >= d && box_hit[pos[i + 1] - 1]) flags[i] |= f;
+}
+
 // subdivide: a flagged leaf below depth 64 becomes its two halves in place (order kept)
 __global__ void split_count_kernel(const uint8_t* flags, const uint8_t* dep, uint32_t n, uint8_t f, uint32_t* cnt)
 {
@@ -397,6 +412,31 @@ __global__ void unsub_apply_kernel(const uint64_t* code, const uint8_t* dep, con
   }
 }
 
+// the box at the inner depth d around a point (searchByIterators below the leaves,
+// ImplicitBoxTree.hpp:2473-2566): it exists when the first leaf at or after the box's
+// first address lies inside it; its index is that leaf's box (pos: scan of the box heads
+// at d).  A point that left the domain is found in the last leaf's box when that leaf's
+// d-prefix is 0, as hasSamePath of the invalid box makes it.
+__device__ __forceinline__ uint32_t inner_box_of(const CmpIndex& ix, const uint64_t* __restrict__ code,
+                                                 const uint8_t* __restrict__ dep, const uint32_t* __restrict__ pos,
+                                                 uint32_t d, bool valid, uint64_t p64)
+{
+  const uint32_t n = ix.n;
+  if (n == 0) return kInvalidIndex;
+  uint32_t j;
+  bool in;
+  if (!valid) {
+    j = n - 1;
+    in = __ldg(dep + j) >= d && (__ldg(code + j) >> (__ldg(dep + j) - d)) == 0;
+  } else {
+    const int sh = 64 - int(d);
+    const uint64_t q = srs(p64, sh);
+    j = lower_bound_idx(ix, sls(q, sh));
+    in = j < n && __ldg(dep + j) >= d && srs(__ldg(code + j), int(__ldg(dep + j)) - int(d)) == q;
+  }
+  return in ? __ldg(pos + j + 1) - 1 : kInvalidIndex;
+}
+
 // insertByIterators (ImplicitBoxTree.hpp:1615-1910): the new box of every point box
 struct InsertArgs {
   const uint64_t* p64;         // depth-64 point codes
@@ -411,6 +451,8 @@ struct InsertArgs {
   uint32_t depth;              // insertion depth; 255: the leaf depth
   int mode;                    // 0: leaf depth, 2: below an existing depth, 3: deeper than every leaf
   uint8_t* hit;                // marks of leaves hit (leaf depth, when flags for hit are given)
+  const uint32_t* box_pos;     // inner depth: scan of the box heads
+  uint8_t* box_hit;            //              marks of the boxes hit (when flags for hit are given)
   uint64_t* out_code;          // new boxes (appended)
   uint8_t* out_dep;
   uint32_t* count;
@@ -436,16 +478,11 @@ __global__ void insert_boxes_kernel(const InsertArgs a)
       to_insert = s == kInvalidIndex ? valid : a.dep[s] < 64;
       if (!to_insert && s != kInvalidIndex && a.hit) a.hit[s] = 1;
     } else if (a.mode == 2) {
-      // a depth-d box exists around the point when the first leaf at or after the box's
-      // first address lies inside it
-      bool found = false;
-      if (valid) {
-        const int sh = 64 - int(a.depth);
-        const uint64_t q = srs(p.c, sh);
-        const uint32_t j = lower_bound_idx(CmpIndex{a.cmp, a.tab, a.n, a.tab_bits}, sls(q, sh));
-        found = j < a.n && a.dep[j] >= a.depth && srs(a.code[j], int(a.dep[j]) - int(a.depth)) == q;
-      }
-      to_insert = valid && !found;
+      // the box at the inner depth around the point; its leaves get the flags for hit
+      const uint32_t b = inner_box_of(CmpIndex{a.cmp, a.tab, a.n, a.tab_bits}, a.code, a.dep, a.box_pos, a.depth,
+                                      valid, p.c);
+      if (b != kInvalidIndex && a.box_hit) a.box_hit[b] = 1;
+      to_insert = valid && b == kInvalidIndex;
     } else {
       to_insert = valid;
     }
@@ -618,6 +655,9 @@ struct MixedArgs {
   uint32_t* out;               // Search: leaf index of every point
   uint64_t* p64_out;           // Codes: depth-64 code of every image point
   uint8_t* valid_out;          //        1 if it lies in the domain
+  const uint32_t* box_pos;     // inner depth: scan of the box heads (box of leaf j: box_pos[j + 1] - 1)
+  uint32_t inner_depth;
+  uint8_t* box_hit;            //              hit marks of the boxes
   // transition rows
   uint32_t* stage_col;
   uint32_t* stage_cnt;
@@ -675,7 +715,8 @@ __device__ __forceinline__ uint32_t image_of(const MixedArgs& a, const double* p
 }
 
 // kMode 0: hit marks of the leaves hit; 1: leaf index of every point; 2: the points'
-// depth-64 codes and validity (the point boxes of an insertion)
+// depth-64 codes and validity (the point boxes of an insertion); 3: hit marks of the
+// boxes at the inner depth a.inner_depth; 4: box index at that depth of every point
 template<class Map, class Grid, int kMode>
 __global__ void __launch_bounds__(kThreads) mixed_image_kernel(const MixedArgs a)
 {
@@ -691,6 +732,13 @@ __global__ void __launch_bounds__(kThreads) mixed_image_kernel(const MixedArgs a
       uint64_t p64;
       a.valid_out[g] = image_code<Map, Grid>(a, pts, table, leaf, k, g, p64) ? 1 : 0;
       a.p64_out[g] = p64;
+    } else if constexpr (kMode >= 3) {
+      uint64_t p64;
+      const bool valid = image_code<Map, Grid>(a, pts, table, leaf, k, g, p64);
+      const uint32_t b = inner_box_of(CmpIndex{a.cmp, a.tab, a.n, a.tab_bits}, a.code, a.dep, a.box_pos,
+                                      a.inner_depth, valid, p64);
+      if constexpr (kMode == 4) a.out[g] = b;
+      else if (b != kInvalidIndex) a.box_hit[b] = 1;
     } else {
       const uint32_t t = image_of<Map, Grid>(a, pts, table, leaf, k, g);
       if constexpr (kMode == 1) a.out[g] = t;
@@ -774,6 +822,31 @@ b12g_status scan_marks(b12g_tree* t, const uint32_t* marks, uint32_t* pos, uint3
   ST(sync(t, "scan"));
   count_launches(3);
   *total = t->h_ctr[C_TMP];
+  return B12G_OK;
+}
+
+// heads of the boxes at `depth` into t->row_count and their scan into t->rowptr (the box
+// of a leaf j at least that deep is rowptr[j + 1] - 1); *n_boxes
+b12g_status inner_boxes(b12g_tree* t, uint8_t depth, uint32_t* n_boxes)
+{
+  const uint32_t n = t->n;
+  ST(t->row_count.ensure(uint64_t(n) + 1, "box heads"));
+  ST(t->rowptr.ensure(uint64_t(n) + 1, "box positions"));
+  box_head_kernel<<<grid_for_n(n), kThreads, 0, t->stream>>>(t->codes(), dep_cur(t), n, depth, t->row_count.p);
+  count_launches(1);
+  return scan_marks(t, t->row_count.p, t->rowptr.p, n, n_boxes);
+}
+
+// every box's AND (into t->src) and OR (into t->out) of its leaves' flags
+b12g_status box_flags(b12g_tree* t, uint8_t depth, uint32_t n_boxes)
+{
+  ST(t->src.ensure(std::max<uint32_t>(n_boxes, 1), "box flags"));
+  ST(t->out.ensure(std::max<uint32_t>(n_boxes, 1), "box flags"));
+  CK(cudaMemsetAsync(t->src.p, 0xFF, size_t(n_boxes) * 4, t->stream));
+  CK(cudaMemsetAsync(t->out.p, 0, size_t(n_boxes) * 4, t->stream));
+  box_combine_kernel<<<grid_for_n(t->n), kThreads, 0, t->stream>>>(t->flg(), dep_cur(t), t->n, depth, t->rowptr.p,
+                                                                   t->src.p, t->out.p);
+  count_launches(1);
   return B12G_OK;
 }
 
@@ -904,26 +977,69 @@ b12g_status mixed_flags_at_depth(b12g_tree* t, int op, uint8_t u, uint8_t f, uin
   if (depth > t->depth) return B12G_OK;
   ST(mixed_enter(t));
   const uint32_t n = t->n;
-  ST(t->row_count.ensure(uint64_t(n) + 1, "box heads"));
-  ST(t->rowptr.ensure(uint64_t(n) + 1, "box positions"));
-  ST(t->src.ensure(std::max<uint32_t>(n, 1), "box flags"));
-  ST(t->out.ensure(std::max<uint32_t>(n, 1), "box flags"));
-  box_head_kernel<<<grid_for_n(n), kThreads, 0, t->stream>>>(t->codes(), dep_cur(t), n, depth, t->row_count.p);
-  count_launches(1);
   uint32_t boxes = 0;
-  ST(scan_marks(t, t->row_count.p, t->rowptr.p, n, &boxes));
+  ST(inner_boxes(t, depth, &boxes));
   if (boxes) {
-    CK(cudaMemsetAsync(t->src.p, 0xFF, size_t(boxes) * 4, t->stream));
-    CK(cudaMemsetAsync(t->out.p, 0, size_t(boxes) * 4, t->stream));
+    ST(box_flags(t, depth, boxes));
     ST(set_ctr(t, C_CHANGED, 0));
-    box_combine_kernel<<<grid_for_n(n), kThreads, 0, t->stream>>>(t->flg(), dep_cur(t), n, depth, t->rowptr.p,
-                                                                   t->src.p, t->out.p);
     box_apply_kernel<<<grid_for_n(std::max(n, boxes)), kThreads, 0, t->stream>>>(
         t->flg(), dep_cur(t), n, depth, t->rowptr.p, t->src.p, t->out.p, boxes, op, u, f, t->ctr.p + C_CHANGED);
-    count_launches(2);
+    count_launches(1);
     ST(read_ctr(t, C_CHANGED, 1));
     if (n_changed) *n_changed = t->h_ctr[C_CHANGED];
   }
+  return mixed_settle(t);
+}
+
+// flags f on every leaf of the boxes at `depth` marked in t->hit[0 .. n_boxes), which
+// are cleared after; *n_changed (if not null) = marked boxes whose leaves did not all have f
+b12g_status apply_box_hits(b12g_tree* t, uint8_t depth, uint32_t n_boxes, uint8_t f, uint32_t* n_changed)
+{
+  if (n_changed) *n_changed = 0;
+  if (!n_boxes) return B12G_OK;
+  ST(box_flags(t, depth, n_boxes));
+  ST(set_ctr(t, C_CHANGED, 0));
+  box_hit_apply_kernel<<<grid_for_n(std::max(t->n, n_boxes)), kThreads, 0, t->stream>>>(
+      t->flg(), dep_cur(t), t->n, depth, t->rowptr.p, t->src.p, t->hit.p, n_boxes, f, t->ctr.p + C_CHANGED);
+  CK(cudaMemsetAsync(t->hit.p, 0, n_boxes, t->stream));
+  count_launches(1);
+  ST(read_ctr(t, C_CHANGED, 1));
+  if (n_changed) *n_changed = t->h_ctr[C_CHANGED];
+  return B12G_OK;
+}
+
+// the images of the scheme's source leaves located at an inner depth: flags on the
+// boxes hit (setFlagsByIterators, ImplicitBoxTree.hpp:2691-2694), or with search set
+// each point's box index at that depth into t->out (searchByIterators, 2473-2566)
+b12g_status mixed_image_at_depth(b12g_tree* t, const b12g_scheme* sc, uint8_t depth, uint8_t flags, bool search,
+                                 uint64_t* n_points, uint32_t* n_changed)
+{
+  if (n_changed) *n_changed = 0;
+  if (depth == 0 || depth > 64) return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "image search at depth %u", depth);
+  ST(mixed_enter(t));
+  MixedArgs a;
+  ST(mixed_args(t, sc, a));
+  ST(mixed_sources(t, sc, &a.src, &a.n_src));
+  const uint64_t np = uint64_t(a.n_src) * a.points;
+  if (n_points) *n_points = np;
+  uint32_t boxes = 0;
+  ST(inner_boxes(t, depth, &boxes));   // no box below the deepest leaf: every search fails
+  a.box_pos = t->rowptr.p;
+  a.inner_depth = depth;
+  a.box_hit = t->hit.p;
+  if (search) {
+    ST(t->out.ensure(std::max<uint64_t>(np, 1), "search output"));
+    a.out = t->out.p;
+  }
+  if (np)
+    CK(dispatch(sc->map.kind, sc->map.arith, sc->grid.kind, t->domain.dim, [&](auto map, auto grid) -> cudaError_t {
+      if (search) mixed_image_kernel<decltype(map), decltype(grid), 4><<<grid_for_n(np), kThreads, 0, t->stream>>>(a);
+      else mixed_image_kernel<decltype(map), decltype(grid), 3><<<grid_for_n(np), kThreads, 0, t->stream>>>(a);
+      return cudaGetLastError();
+    }));
+  count_launches(1);
+  if (!search) ST(apply_box_hits(t, depth, boxes, flags, n_changed));
+  if (search) return B12G_OK;       // t->out is read by the caller before the layout may change
   return mixed_settle(t);
 }
 
@@ -1009,8 +1125,7 @@ b12g_status mixed_remove(b12g_tree* t, uint8_t flags, uint32_t* n_removed)
 b12g_status mixed_set_flags_by_image(b12g_tree* t, const b12g_scheme* sc, uint8_t flags, uint8_t depth,
                                      uint32_t* n_changed)
 {
-  if (depth != B12G_LEAF_DEPTH)
-    return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "images flag the leaves (depth 255) of a tree of mixed depths");
+  if (depth != B12G_LEAF_DEPTH) return mixed_image_at_depth(t, sc, depth, flags, false, nullptr, n_changed);
   MixedArgs a;
   ST(mixed_args(t, sc, a));
   ST(mixed_sources(t, sc, &a.src, &a.n_src));
@@ -1116,8 +1231,6 @@ b12g_status mixed_insert_boxes(b12g_tree* t, uint64_t np, uint8_t depth, uint8_t
   if (depth > 64 && depth != B12G_LEAF_DEPTH) return fail(B12G_ERR_INVALID, "insertion depth %u", depth);
   if (np > 0xFFFFFFF0ull) return fail(B12G_ERR_CAPACITY, "too many points in one insertion");
   const int mode = depth == B12G_LEAF_DEPTH ? 0 : (depth <= t->depth ? 2 : 3);
-  if (mode == 2 && hit)
-    return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "flags for boxes hit at the inner depth %u", depth);
   if (n_inserted) *n_inserted = 0;
   ST(mixed_enter(t));
   ST(refresh_comparable(t));
@@ -1143,6 +1256,12 @@ b12g_status mixed_insert_boxes(b12g_tree* t, uint64_t np, uint8_t depth, uint8_t
   a.count = t->ctr.p + C_CAND;
   a.cap = m_cap;
   a.error = t->ctr.p + C_ERROR;
+  uint32_t inner = 0;   // boxes at an inner insertion depth, for the flags of the boxes hit
+  if (mode == 2) {
+    ST(inner_boxes(t, depth, &inner));
+    a.box_pos = t->rowptr.p;
+    a.box_hit = hit ? t->hit.p : nullptr;
+  }
   if (np) insert_boxes_kernel<<<grid_for_n(np), kThreads, 0, t->stream>>>(a);
   count_launches(1);
   if (a.hit) {
@@ -1151,6 +1270,7 @@ b12g_status mixed_insert_boxes(b12g_tree* t, uint64_t np, uint8_t depth, uint8_t
                                                                      t->ctr.p + C_CHANGED);
     count_launches(1);
   }
+  if (a.box_hit) ST(apply_box_hits(t, depth, inner, hit, nullptr));
   ST(read_ctr(t, C_CAND, 1));
   ST(check_error(t, "insert"));
   const uint32_t m = t->h_ctr[C_CAND];

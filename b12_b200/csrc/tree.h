@@ -199,6 +199,11 @@ b12g_status mixed_load(b12g_tree* t, const uint64_t* codes, const uint8_t* depth
 b12g_status mixed_count(b12g_tree* t, uint8_t depth, uint32_t* count);
 // set / unset / change (op 0 / 1 / 2) flags of the boxes at a depth inside the tree
 b12g_status mixed_flags_at_depth(b12g_tree* t, int op, uint8_t u, uint8_t f, uint8_t depth, uint32_t* n_changed);
+// images of the scheme's source leaves located at an inner depth: flags on the boxes hit,
+// or (search) each point's box index at that depth into t->out; settles the tree's
+// layout unless searching (the caller reads t->out first, then settles)
+b12g_status mixed_image_at_depth(b12g_tree* t, const b12g_scheme* sc, uint8_t depth, uint8_t flags, bool search,
+                                 uint64_t* n_points, uint32_t* n_changed);
 b12g_status mixed_leaves(b12g_tree* t, uint64_t* codes, uint8_t* depths, uint8_t* flags);
 b12g_status mixed_subdivide(b12g_tree* t, uint8_t flags, uint32_t* n_subdivided);
 b12g_status mixed_remove(b12g_tree* t, uint8_t flags, uint32_t* n_removed);

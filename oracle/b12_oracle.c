@@ -788,6 +788,91 @@ uint32_t orc_flags_at_depth(orc_tree* t, int op, uint8_t u, uint8_t f, uint32_t 
   return count;
 }
 
+/* the index of every leaf's box at depth d (initializeIndicesInDepth,
+ * ImplicitBoxTree.hpp:1399-1470): boxes counted in tree order; ORC_INVALID for leaves
+ * shallower than d.  Caller frees. */
+static uint32_t* boxes_at_depth(const orc_tree* t, uint32_t d, uint64_t* n_boxes)
+{
+  uint32_t* box = (uint32_t*)malloc((t->n ? t->n : 1) * 4);
+  uint64_t b = 0;
+  for (uint64_t i = 0; i < t->n; ++i) {
+    if (t->depth[i] < d) { box[i] = ORC_INVALID; continue; }
+    int fresh = i == 0 || t->depth[i - 1] < d;
+    if (!fresh) fresh = (t->code[i - 1] >> (t->depth[i - 1] - d)) != (t->code[i] >> (t->depth[i] - d));
+    if (fresh) ++b;
+    box[i] = (uint32_t)(b - 1);
+  }
+  *n_boxes = b;
+  return box;
+}
+
+/* searchByIterators at an inner depth d (ImplicitBoxTree.hpp:2473-2566): the lower
+ * bound of the point box among the leaves, its two neighbours taken to depth d
+ * (decrementDepthTo) when at least that deep, ComputeSearchIndexFunctor, then the
+ * box index at depth d of the leaf found */
+static uint32_t search_at_depth(const orc_tree* t, const uint32_t* box, uint64_t code64, int valid, uint32_t d)
+{
+  const uint64_t n = t->n;
+  if (n == 0) return ORC_INVALID;
+  const uint32_t pd = valid ? 64u : ORC_LEAF_DEPTH;
+  const uint64_t pc = valid ? code64 : INVALID_CODE;
+  uint64_t lo = 0, hi = n;
+  while (lo < hi) {
+    const uint64_t mid = lo + (hi - lo) / 2;
+    if (strictly_preceding(t->code[mid], t->depth[mid], pc, pd)) lo = mid + 1;
+    else hi = mid;
+  }
+  const uint64_t ia = lo > 0 ? lo - 1 : 0, ib = lo < n - 1 ? lo : n - 1;
+  uint64_t found = ORC_INVALID;
+  for (int c = 0; c < 2 && found == ORC_INVALID; ++c) {
+    const uint64_t j = c == 0 ? ia : ib;
+    if (t->depth[j] < d) continue;                        /* hasAtLeastDepth */
+    const uint64_t cd = t->code[j] >> (t->depth[j] - d);  /* decrementDepthTo(d) */
+    if (pd >= d && same_path(pc, pd, cd, d)) found = c == 0 ? (lo > 0 ? lo - 1 : 0) : lo;
+  }
+  return found == ORC_INVALID ? ORC_INVALID : box[found];
+}
+
+/* flags on the boxes at depth d hit by the images of every leaf (setFlagsByIterators
+ * with makePointIteratorPairOverLeaves at an inner depth, ImplicitBoxTree.hpp:2691-2694
+ * via setFlagsBySearch 2776-2800): every leaf of a hit box gets the flags; returns the
+ * hit boxes whose leaves did not all have them.  out (if not NULL) gets each point's
+ * box index instead, and nothing changes. */
+uint32_t orc_image_at_depth(orc_tree* t, const orc_map* m, const orc_grid* g, uint32_t d, uint8_t flags,
+                            uint32_t* out)
+{
+  const uint64_t n = t->n, P = points_per_box(g, t->dom.dim);
+  const uint32_t D = t->dom.dim;
+  uint64_t nb = 0;
+  uint32_t* box = boxes_at_depth(t, d, &nb);
+  uint8_t* hit = (uint8_t*)calloc(nb ? nb : 1, 1);
+  for (uint64_t i = 0; i < n * P; ++i) {
+    const uint64_t b = i / P;
+    double c[ORC_MAX_DIM], r[ORC_MAX_DIM], gp[ORC_MAX_DIM], y[ORC_MAX_DIM];
+    orc_box_coordinates(&t->dom, t->code[b], t->depth[b], c, r);
+    orc_grid_point(g, D, i, gp);
+    for (uint32_t j = 0; j < D; ++j) c[j] += gp[j] * r[j];
+    orc_map_apply(m, c, y);
+    uint64_t c64;
+    const int valid = orc_point_code64(&t->dom, y, &c64);
+    const uint32_t s = search_at_depth(t, box, c64, valid, d);
+    if (out) out[i] = s;
+    else if (s != ORC_INVALID) hit[s] = 1;
+  }
+  uint32_t count = 0;
+  if (!out) {
+    uint8_t* all = (uint8_t*)malloc(nb ? nb : 1);
+    memset(all, 0xFF, nb ? nb : 1);
+    for (uint64_t i = 0; i < n; ++i) if (box[i] != ORC_INVALID) all[box[i]] &= t->flags[i];
+    for (uint64_t b = 0; b < nb; ++b) count += hit[b] && !flags_set(all[b], flags);
+    for (uint64_t i = 0; i < n; ++i) if (box[i] != ORC_INVALID && hit[box[i]]) t->flags[i] |= flags;
+    free(all);
+  }
+  free(hit);
+  free(box);
+  return count;
+}
+
 /* computeDepthOfMutualAncestor (Box.hpp:209-223) */
 static inline uint32_t mutual_ancestor(obox a, obox b)
 {
@@ -838,28 +923,12 @@ static void stable_sort_boxes(obox* v, uint64_t n)
   free(w);
 }
 
-/* a depth-d box exists that contains the depth-64 point box p (a leaf of depth >= d
- * with p's depth-d prefix): the first leaf whose comparable pattern is not below the
- * box's first address is inside it exactly when such a leaf exists */
-static int inner_box_exists(const orc_tree* t, uint64_t p64, uint32_t d)
-{
-  const uint64_t q = srs(p64, 64 - (int)d), first = sls(q, 64 - (int)d);
-  uint64_t lo = 0, hi = t->n;
-  while (lo < hi) {
-    const uint64_t mid = lo + (hi - lo) / 2;
-    if (comparable(t->code[mid], t->depth[mid]) < first) lo = mid + 1;
-    else hi = mid;
-  }
-  if (lo >= t->n || t->depth[lo] < d) return 0;
-  return srs(t->code[lo], (int)(t->depth[lo] - d)) == q;
-}
-
 /* insertByIterators (ImplicitBoxTree.hpp:1615-1910) for any tree, given the depth-64
  * point boxes (valid[k] = 0: the point left the domain).  depth 255 inserts at the
  * leaf depth (each new box the coarsest one that does not meet its neighbours,
  * AdaptDepthOfFirstBoxFunctor, Functors.hpp:381-389); new boxes are merged into the
- * leaves by the reference's two HasSamePath scans and unique (1875-1897).  Flags for
- * hit boxes at an inner depth are not restated: *unsupported is set instead.
+ * leaves by the reference's two HasSamePath scans and unique (1875-1897).  At an inner
+ * depth, flags for hit boxes go to every leaf of the box hit.  *unsupported stays 0.
  * Returns the number of distinct new boxes. */
 uint32_t orc_insert_boxes(orc_tree* t, const uint64_t* c64, const uint8_t* valid, uint64_t np, uint32_t depth,
                           uint8_t ins, uint8_t hit, int* unsupported)
@@ -880,7 +949,9 @@ uint32_t orc_insert_boxes(orc_tree* t, const uint64_t* c64, const uint8_t* valid
   }
   const int leaf_search = depth == ORC_LEAF_DEPTH || (uniform && depth == t->depth[0]);
   const int inner_search = !leaf_search && depth <= maxd;
-  if (inner_search && hit) { *unsupported = 1; return 0; }
+  uint64_t n_boxes = 0;
+  uint32_t* box = inner_search ? boxes_at_depth(t, depth, &n_boxes) : NULL;
+  uint8_t* box_hit = inner_search ? (uint8_t*)calloc(n_boxes ? n_boxes : 1, 1) : NULL;
   obox* nb = (obox*)malloc((np ? np : 1) * sizeof(obox));
   uint32_t* hits = (uint32_t*)malloc((np ? np : 1) * 4);
   uint64_t m = 0, nh = 0;
@@ -895,7 +966,10 @@ uint32_t orc_insert_boxes(orc_tree* t, const uint64_t* c64, const uint8_t* valid
         to_insert = s == ORC_INVALID && valid[k];
       if (!to_insert && s != ORC_INVALID) hits[nh++] = s;
     } else if (inner_search) {
-      to_insert = valid[k] && !inner_box_exists(t, p.c, depth);
+      /* the box at `depth` around the point (setFlagsBySearch marks it for hit flags) */
+      const uint32_t s = search_at_depth(t, box, p.c, valid[k], depth);
+      if (s != ORC_INVALID) box_hit[s] = 1;
+      to_insert = valid[k] && s == ORC_INVALID;
     } else {
       to_insert = valid[k] != 0;
     }
@@ -921,6 +995,13 @@ uint32_t orc_insert_boxes(orc_tree* t, const uint64_t* c64, const uint8_t* valid
     nb[m++] = b;
   }
   for (uint64_t k = 0; k < nh; ++k) t->flags[hits[k]] |= hit;
+  if (inner_search) {
+    /* setFlagsByStencil at the inner depth: every leaf of a hit box */
+    if (hit)
+      for (uint64_t i = 0; i < n; ++i) if (box[i] != ORC_INVALID && box_hit[box[i]]) t->flags[i] |= hit;
+    free(box);
+    free(box_hit);
+  }
   /* distinct new boxes in tree order */
   stable_sort_boxes(nb, m);
   uint64_t u = 0;

@@ -101,11 +101,15 @@ uint32_t orc_insert_points(orc_tree* t, const double* pts, uint64_t n_points, ui
 void orc_delete_depth0(orc_tree* t);
 
 /* trees of mixed depths: unsubdivide, and insertByIterators for any tree and depth
- * (255 = leaf depth); *unsupported is set for flags on hit boxes at an inner depth */
+ * (255 = leaf depth) */
 uint32_t orc_unsubdivide(orc_tree* t, uint8_t flags);
 /* set / unset / change (op 0 / 1 / 2) flags of the boxes at an inner depth; for change, u
  * is unset and f set */
 uint32_t orc_flags_at_depth(orc_tree* t, int op, uint8_t u, uint8_t f, uint32_t depth);
+/* images of every leaf located at an inner depth d: flags on the boxes hit (returns the
+ * hit boxes that lacked them), or with out != NULL each point's box index at d */
+uint32_t orc_image_at_depth(orc_tree* t, const orc_map* m, const orc_grid* g, uint32_t d, uint8_t flags,
+                            uint32_t* out);
 uint32_t orc_insert_boxes(orc_tree* t, const uint64_t* code64, const uint8_t* valid, uint64_t n_points,
                           uint32_t depth, uint8_t ins, uint8_t hit, int* unsupported);
 uint32_t orc_insert_points_general(orc_tree* t, const double* pts, uint64_t n_points, uint32_t depth, uint8_t ins,

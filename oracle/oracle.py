@@ -82,6 +82,7 @@ def lib():
             "orc_delete_depth0": (None, [P(OrcTree)]),
             "orc_unsubdivide": (u32, [P(OrcTree), u8]),
             "orc_flags_at_depth": (u32, [P(OrcTree), C.c_int, u8, u8, u32]),
+            "orc_image_at_depth": (u32, [P(OrcTree), P(OrcMap), P(OrcGrid), u32, u8, P(u32)]),
             "orc_insert_points_general": (u32, [P(OrcTree), P(dbl), u64, u32, u8, u8, P(C.c_int)]),
             "orc_insert_by_image_general": (u32, [P(OrcTree), P(OrcMap), P(OrcGrid), u8, u32, u8, u8,
                                                   P(C.c_int)]),
@@ -220,6 +221,17 @@ class Oracle:
     def delete_depth0(self): self.L.orc_delete_depth0(C.byref(self.tree))
 
     def unsubdivide(self, f): return self.L.orc_unsubdivide(C.byref(self.tree), f)
+
+    def image_flags_at_depth(self, depth, f):
+        """flags on the boxes at an inner depth hit by the images of every leaf"""
+        return self.L.orc_image_at_depth(C.byref(self.tree), C.byref(self.map), C.byref(self.grid), depth, f, None)
+
+    def image_search_at_depth(self, depth):
+        """each image point's box index at an inner depth (0xFFFFFFFF: none)"""
+        out = np.zeros(self.n * self.points_per_box(), dtype=np.uint32)
+        self.L.orc_image_at_depth(C.byref(self.tree), C.byref(self.map), C.byref(self.grid), depth, 0,
+                                  _ptr(out, C.c_uint32))
+        return out
 
     def flags_at_depth(self, op, u, f, depth):
         """set (0) / unset (1) / change (2, u -> f) flags of the boxes at an inner depth"""

@@ -148,6 +148,26 @@ void runEdits(Tree& ibt, const std::vector<double>& c, const std::vector<double>
   dump(9);
   js << ", " << ibt.unsetFlags(Flag::INS, Depth(md - 1));
   dump(10);
+  // images located at inner depths: flags on the boxes hit (setFlagsByIterators,
+  // 2691-2694), the boxes' indices at that depth (searchByIterators, 2375-2572), and
+  // flags for hit boxes of an insertion at an inner depth (1700-1712)
+  js << ", " << ibt.setFlagsByIterators(ibt.makePointIteratorPairOverLeaves(grid, map), Flag::HIT, Depth(md - 2));
+  dump(11);
+  {
+    auto s = ibt.searchByIterators(ibt.makePointIteratorPairOverLeaves(grid, map), Depth(md - 3));
+    std::vector<uint32_t> h(s.begin(), s.end());
+    if (!dir.empty()) {
+      FILE* f = openOut(dir + "/search_12.bin");
+      const uint64_t n = h.size();
+      std::fwrite(&n, 8, 1, f);
+      std::fwrite(h.data(), 4, n, f);
+      std::fclose(f);
+    }
+    js << ", " << h.size();
+  }
+  ibt.insertByPoints(pts(300, 4, "points_13.bin"), Depth(md - 1), Flag::INS, Flag::EXPD);
+  js << ", " << ibt.count(getLeafDepth());
+  dump(13);
   js << "], \"edit_max_depth\": " << maxd << ", \"edit_flag_depth\": " << md;
 }
 

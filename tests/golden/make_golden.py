@@ -154,6 +154,13 @@ def generate(name: str) -> None:
             arrays[f"edit_flags_{key}"] = flags
         for fn in sorted(f for f in os.listdir(tmp) if f.startswith("points_")):
             arrays[fn[:-4]] = read_points(os.path.join(tmp, fn))
+        # box indices of a search at an inner depth (u64 n, then u32 indices)
+        for fn in sorted(f for f in os.listdir(tmp) if f.startswith("search_")):
+            with open(os.path.join(tmp, fn), "rb") as f:
+                ns = int(np.frombuffer(f.read(8), dtype="<u8")[0])
+                idx = np.frombuffer(f.read(4 * ns), dtype="<u4").copy()
+            out.setdefault("searches", {})[fn[:-4]] = dict(n=ns, sha256=sha(idx))
+            arrays[fn[:-4]] = idx
         for fn in files:
             k = int(fn[len(prefix):-4])
             codes, depth, flags = read_leaves(os.path.join(tmp, fn))

@@ -208,9 +208,8 @@ def test_unsupported_calls_refuse_and_leave_the_tree(golden):
     sc = scheme(meta["spec"])
     step(t, sc)
     before = [a.copy() for a in t.leaves()]
-    for call in (lambda: t.set_flags(B.EXPD, 254), lambda: t.set_flags_by_image(sc, B.HIT, 9),
-                 lambda: t.insert_by_image(B.Scheme(sc.map, sc.grid, 9, B.INS), 9),
-                 lambda: t.search_by_image(sc, 9)):
+    for call in (lambda: t.set_flags(B.EXPD, 254), lambda: t.set_flags_by_image(sc, B.HIT, 0),
+                 lambda: t.insert_by_image(B.Scheme(sc.map, sc.grid, 9, B.INS), 9)):
         with pytest.raises(B.B12gError) as e:
             call()
         assert e.value.status == B._lib.ERR_MIXED_DEPTH
@@ -276,6 +275,12 @@ def test_unsubdivide_and_insert_match_reference(golden, name):
     check_edit(t, want["09"], "09")
     assert t.unset_flags(B.INS, md - 1) == counts[9]
     check_edit(t, want["10"], "10")
+    # images located at inner depths: flags on the boxes hit, box indices, insertion hits
+    assert t.set_flags_by_image(sc, B.HIT, md - 2) == counts[10]
+    check_edit(t, want["11"], "11")
+    np.testing.assert_array_equal(t.search_by_image(sc, md - 3), arrays["search_12"])
+    t.insert_points(arrays["points_13"], md - 1, B.INS, B.EXPD)
+    check_edit(t, want["13"], "13")
     m = t.transition_matrix(sc, invalid_column=spec.get("invalid", False))
     d = csr_digests(*m.to_host())
     for key in ("nnz", "rowptr_sha256", "cols_sha256", "vals_sha256"):
@@ -335,16 +340,20 @@ def test_unsubdivide_of_a_one_depth_tree(golden):
             np.testing.assert_array_equal(x, y)
 
 
-def test_inner_depth_hit_flags_are_refused(golden):
-    meta, arrays = golden("henon_d8_mixed4_files")
-    t = start(meta, arrays)
-    step(t, scheme(meta["spec"]))
-    before = [a.copy() for a in t.leaves()]
-    with pytest.raises(B.B12gError) as e:
-        t.insert_points(np.zeros((3, 2)), 8, B.INS, B.HIT)
-    assert e.value.status == B._lib.ERR_MIXED_DEPTH
-    for x, y in zip(t.leaves(), before):
-        np.testing.assert_array_equal(x, y)
+def test_insertion_hits_at_an_inner_depth_match_oracle(golden):
+    meta, arrays = golden("henon_d12_mixed6_edits")
+    spec = meta["spec"]
+    last = meta["mixed"][-1]["step"]
+    leaves = (arrays[f"mixed_codes_{last:02d}"], arrays[f"mixed_depth_{last:02d}"], arrays[f"mixed_flags_{last:02d}"])
+    c, r = domain(spec)
+    t = B.ImplicitBoxTree(c, r)
+    t.load_leaves(*leaves)
+    o = O.Oracle(oracle_spec(spec))
+    o.load(*leaves)
+    for d, pts in ((14, arrays["points_3"]), (17, arrays["points_4"]), (12, arrays["points_5"])):
+        assert t.insert_points(pts, d, B.INS, B.HIT) == o.insert_points_general(pts, d, 2, 1)
+        for x, y in zip(t.leaves(), o.leaves()):
+            np.testing.assert_array_equal(x, y)
 
 
 @pytest.mark.parametrize("op", [0, 1, 2])

@@ -91,6 +91,9 @@ def edit_sequence(o, meta, arrays):
     yield "08", o.flags_at_depth(0, 0, 4, md - 2)        # setFlags(EXPD, md - 2)
     yield "09", o.flags_at_depth(2, 4, 2, md - 3)        # changeFlags(EXPD, INS, md - 3)
     yield "10", o.flags_at_depth(1, 0, 2, md - 1)        # unsetFlags(INS, md - 1)
+    yield "11", o.image_flags_at_depth(md - 2, 1)       # setFlagsByIterators(leaves, HIT, md - 2)
+    yield "search", o.image_search_at_depth(md - 3)     # searchByIterators(leaves, md - 3)
+    yield "13", o.insert_points_general(arrays["points_13"], md - 1, 2, 4)   # insert(pts, md - 1, INS, EXPD)
 
 
 @pytest.mark.parametrize("name", EDIT_CASES)
@@ -103,13 +106,17 @@ def test_unsubdivide_and_insert_match_reference(golden, name):
     want = {e["step"]: e for e in meta["edits"]}
     counts = meta["timing"]["edits"]
     for k, (key, ret) in enumerate(edit_sequence(o, meta, arrays)):
+        if key == "search":
+            np.testing.assert_array_equal(ret, arrays["search_12"])
+            assert len(ret) == counts[k]
+            continue
         codes, depth, flags = o.leaves()
         e = want[key]
         assert len(codes) == e["n"], key
         assert sha(codes) == e["codes_sha256"], f"{key} codes"
         assert sha(depth) == e["depth_sha256"], f"{key} depths"
         assert sha(flags) == e["flags_sha256"], f"{key} flags"
-        if key in ("01", "02", "08", "09", "10"):
+        if key in ("01", "02", "08", "09", "10", "11"):
             assert ret == counts[k], key          # the call's own return value
         else:
             assert len(codes) == counts[k], key   # the run records the leaf count
