@@ -20,11 +20,12 @@
  *   - Leaves may have different depths, as in the reference (kept in the order of
  *     isStrictlyPreceding, Box.hpp:124-135).  A tree whose leaves share one depth runs
  *     the fused single-depth kernels; subdividing some of its leaves, or loading leaves
- *     of several depths, switches it to per-leaf depths until one depth is left.  Flags
- *     at a depth inside the tree change every leaf of each box at that depth.  On a
- *     tree of mixed depths schemes map the leaves (depth 255); the unsubdividable depth
- *     254 is not offered; those calls return B12G_ERR_UNSUPPORTED_MIXED_DEPTH and leave
- *     the tree unchanged.
+ *     of several depths, switches it to per-leaf depths until one depth is left.  At a
+ *     depth inside the tree, flags (and image flags, insertion hit flags) change every
+ *     leaf of each box at that depth, and searches return the box's index among the
+ *     boxes at that depth.  On a tree of mixed depths schemes map the leaves (source
+ *     depth 255); the unsubdividable depth 254 is not offered; those calls return
+ *     B12G_ERR_UNSUPPORTED_MIXED_DEPTH and leave the tree unchanged.
  *   - Host pointers are plain host memory (pinned or pageable); the library owns all
  *     device memory of a tree and of a CSR matrix.
  */
@@ -178,8 +179,7 @@ b12g_status b12g_search_by_image(b12g_tree* tree, const b12g_scheme* scheme, uin
  * n_points x dim doubles, row-major.  depth 255 inserts at the leaf depth (each new box
  * the coarsest one that meets neither neighbour; a point in a leaf above depth 64 splits
  * it); a depth other than the leaves' merges new and old boxes on one path into the
- * deepest, flags ORed, as the reference does.  *n_inserted = distinct new boxes.
- * Flags for hit boxes at a depth inside the tree (not its leaf depth) are not offered. */
+ * deepest, flags ORed, as the reference does.  *n_inserted = distinct new boxes. */
 b12g_status b12g_insert_points(b12g_tree* tree, const double* points, uint64_t n_points, uint8_t depth,
                                uint8_t flags_for_inserted, uint8_t flags_for_hit, uint32_t* n_inserted);
 /* insertByIterators(makePointIteratorPairByFlags(scheme), depth, ins, hit)
