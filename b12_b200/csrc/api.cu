@@ -380,6 +380,7 @@ b12g_status b12g_tree_destroy(b12g_tree* t)
   t->pvalid.release(); t->ins_dep.release(); t->ins_dep2.release(); t->scan_dep.release(); t->scan_flags.release();
   t->ins_code.release(); t->scan_code.release(); t->ins_pos.release(); t->ins_head.release();
   for (int b = 0; b < 2; ++b) { t->ins_key[b].release(); t->ins_idx[b].release(); }
+  t->isrc_head.release(); t->isrc_pos.release(); t->isrc_and.release(); t->isrc.release();
   t->hit.release(); t->ctr.release(); t->tiles_a.release(); t->tiles_b.release();
   t->src.release(); t->out.release(); t->stage_col.release(); t->stage_cnt.release();
   t->row_count.release(); t->rowptr.release(); t->cand.release(); t->cand2.release();
@@ -555,7 +556,8 @@ b12g_status b12g_set_flags_by_image(b12g_tree* t, const b12g_scheme* sc, uint8_t
                                     uint32_t* n_changed)
 {
   if (!t) return fail(B12G_ERR_INVALID, "NULL tree");
-  if (t->mixed || (depth != B12G_LEAF_DEPTH && depth != t->depth))
+  if (t->mixed || (depth != B12G_LEAF_DEPTH && depth != t->depth) ||
+      (sc && sc->depth != B12G_LEAF_DEPTH && sc->depth != t->depth))
     return mixed_set_flags_by_image(t, sc, flags, depth, n_changed);
   ST(check_depth(t, depth));
   Prepared pr;
@@ -582,9 +584,10 @@ b12g_status b12g_search_by_image(b12g_tree* t, const b12g_scheme* sc, uint8_t de
                                  uint64_t* n_points)
 {
   if (!t) return fail(B12G_ERR_INVALID, "NULL tree");
-  if (t->mixed || (depth != B12G_LEAF_DEPTH && depth != t->depth)) {
-    // leaves of several depths, or a depth inside the tree: the index of each point's
-    // leaf, or of its box at that depth
+  if (t->mixed || (depth != B12G_LEAF_DEPTH && depth != t->depth) ||
+      (sc && sc->depth != B12G_LEAF_DEPTH && sc->depth != t->depth)) {
+    // leaves of several depths, or a depth inside the tree (of the sources or the
+    // targets): the index of each point's leaf, or of its box at that depth
     uint64_t np = 0;
     if (depth == B12G_LEAF_DEPTH) ST(mixed_search(t, sc, &np));
     else ST(mixed_image_at_depth(t, sc, depth, 0, true, &np, nullptr));

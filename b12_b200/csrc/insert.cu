@@ -206,7 +206,8 @@ b12g_status insert_by_image_impl(b12g_tree* t, const b12g_scheme* sc, uint8_t de
   if (!t || !sc) return fail(B12G_ERR_INVALID, "NULL argument");
   if (depth == 0) return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "insertion of images at depth 0");
   if (depth > 64 && depth != B12G_LEAF_DEPTH) return fail(B12G_ERR_INVALID, "depth above 64");
-  if (t->mixed || depth == B12G_LEAF_DEPTH || depth != t->depth || t->depth == 0) {
+  if (t->mixed || depth == B12G_LEAF_DEPTH || depth != t->depth || t->depth == 0 ||
+      (sc->depth != B12G_LEAF_DEPTH && sc->depth != t->depth)) {
     // new boxes may nest in or around leaves: the reference's general insert of the
     // images of the scheme's source leaves (sources at the leaf depth)
     b12g_scheme s = *sc;

@@ -225,6 +225,22 @@ __global__ void box_hit_apply_kernel(uint8_t* flags, const uint8_t* dep, uint32_
     if (dep[i] >= d && box_hit[pos[i + 1] - 1]) flags[i] |= f;
 }
 
+// every box's AND of its leaves' flags (box_and starts all ones)
+__global__ void box_and_kernel(const uint8_t* flags, const uint8_t* dep, uint32_t n, uint32_t d, const uint32_t* pos,
+                               uint32_t* box_and)
+{
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    if (dep[i] >= d) atomicAnd(box_and + (pos[i + 1] - 1), uint32_t(flags[i]));
+}
+
+// the sources of a scheme at an inner depth (initializeLeafIndicesFromDepth,
+// ImplicitBoxTree.hpp:1476-1611): the first leaf of every box whose leaves all have f
+__global__ void source_select_kernel(uint32_t* head, const uint32_t* pos, const uint32_t* box_and, uint32_t n, uint8_t f)
+{
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    if (head[i]) head[i] = (box_and[pos[i + 1] - 1] & f) == f ? 1u : 0u;
+}
+
 // subdivide: a flagged leaf below depth 64 becomes its two halves in place (order kept)
 __global__ void split_count_kernel(const uint8_t* flags, const uint8_t* dep, uint32_t n, uint8_t f, uint32_t* cnt)
 {
@@ -651,6 +667,7 @@ struct MixedArgs {
   uint32_t n;                  // leaves
   const uint32_t* src;         // source leaves (nullptr: every leaf)
   uint32_t n_src;
+  uint32_t src_depth;          // 0: each source is its leaf; d: the leaf's box at depth d
   uint8_t* hit;                // Hit: marks of the leaves hit
   uint32_t* out;               // Search: leaf index of every point
   uint64_t* p64_out;           // Codes: depth-64 code of every image point
@@ -690,7 +707,14 @@ __device__ __forceinline__ bool image_code(const MixedArgs& a, const double* pts
 {
   constexpr int D = Map::D;
   double c[D], r[D], gp[D], x[D], y[D];
-  box_coordinates<D>(a.dom, __ldg(a.code + leaf), int(__ldg(a.dep + leaf)), c, r);
+  uint64_t code = __ldg(a.code + leaf);
+  int depth = int(__ldg(a.dep + leaf));
+  if (a.src_depth) {
+    // a box of an inner depth, by its first leaf
+    code >>= depth - int(a.src_depth);
+    depth = int(a.src_depth);
+  }
+  box_coordinates<D>(a.dom, code, depth, c, r);
   if (Grid::kTable && table) {
 #pragma unroll
     for (int j = 0; j < D; ++j) gp[j] = pts[j * uint32_t(a.points) + k];
@@ -866,31 +890,62 @@ b12g_status refresh_comparable(b12g_tree* t)
 }
 
 // the scheme's source leaves: every leaf with all the scheme's flags
-b12g_status mixed_sources(b12g_tree* t, const b12g_scheme* sc, const uint32_t** src, uint32_t* n_src)
+// the scheme's sources into a.src / a.n_src / a.src_depth: every leaf with all the
+// scheme's flags, or at an inner source depth the boxes whose leaves all have them
+b12g_status mixed_sources(b12g_tree* t, const b12g_scheme* sc, MixedArgs& a)
 {
-  if (sc->flags_to_check == 0) {
-    *src = nullptr;
-    *n_src = t->n;
+  const uint32_t n = t->n;
+  a.src_depth = 0;
+  if (sc->depth != B12G_LEAF_DEPTH) {
+    const uint32_t d = sc->depth;
+    if (d == 0 || d > 64)
+      return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "scheme source depth %u (inner depths 1..64 and 255)", d);
+    a.src_depth = d;
+    a.src = nullptr;
+    a.n_src = 0;
+    if (d > t->depth) return B12G_OK;      // no box that deep: no sources
+    ST(t->isrc_head.ensure(uint64_t(n) + 1, "inner sources"));
+    ST(t->isrc_pos.ensure(uint64_t(n) + 1, "inner sources"));
+    ST(t->isrc_and.ensure(std::max<uint32_t>(n, 1), "inner sources"));
+    ST(t->isrc.ensure(std::max<uint32_t>(n, 1), "inner sources"));
+    box_head_kernel<<<grid_for_n(n), kThreads, 0, t->stream>>>(t->codes(), dep_cur(t), n, d, t->isrc_head.p);
+    uint32_t boxes = 0;
+    ST(scan_marks(t, t->isrc_head.p, t->isrc_pos.p, n, &boxes));
+    CK(cudaMemsetAsync(t->isrc_and.p, 0xFF, size_t(std::max<uint32_t>(boxes, 1)) * 4, t->stream));
+    box_and_kernel<<<grid_for_n(n), kThreads, 0, t->stream>>>(t->flg(), dep_cur(t), n, d, t->isrc_pos.p,
+                                                               t->isrc_and.p);
+    source_select_kernel<<<grid_for_n(n), kThreads, 0, t->stream>>>(t->isrc_head.p, t->isrc_pos.p, t->isrc_and.p, n,
+                                                                     sc->flags_to_check);
+    uint32_t total = 0;
+    ST(scan_marks(t, t->isrc_head.p, t->isrc_pos.p, n, &total));
+    keep_scatter_kernel<<<grid_for_n(n), kThreads, 0, t->stream>>>(nullptr, nullptr, nullptr, n, t->isrc_pos.p,
+                                                                     nullptr, nullptr, nullptr, t->isrc.p);
+    count_launches(4);
+    a.src = t->isrc.p;
+    a.n_src = total;
     return B12G_OK;
   }
-  ST(t->row_count.ensure(uint64_t(t->n) + 1, "source marks"));
-  ST(t->rowptr.ensure(uint64_t(t->n) + 1, "source positions"));
-  ST(t->src.ensure(std::max<uint32_t>(t->n, 1), "source list"));
-  keep_kernel<<<grid_for_n(t->n), kThreads, 0, t->stream>>>(t->flg(), t->n, sc->flags_to_check, t->row_count.p);
+  if (sc->flags_to_check == 0) {
+    a.src = nullptr;
+    a.n_src = n;
+    return B12G_OK;
+  }
+  ST(t->row_count.ensure(uint64_t(n) + 1, "source marks"));
+  ST(t->rowptr.ensure(uint64_t(n) + 1, "source positions"));
+  ST(t->src.ensure(std::max<uint32_t>(n, 1), "source list"));
+  keep_kernel<<<grid_for_n(n), kThreads, 0, t->stream>>>(t->flg(), n, sc->flags_to_check, t->row_count.p);
   uint32_t total = 0;
-  ST(scan_marks(t, t->row_count.p, t->rowptr.p, t->n, &total));
-  keep_scatter_kernel<<<grid_for_n(t->n), kThreads, 0, t->stream>>>(nullptr, nullptr, nullptr, t->n, t->rowptr.p,
-                                                                     nullptr, nullptr, nullptr, t->src.p);
+  ST(scan_marks(t, t->row_count.p, t->rowptr.p, n, &total));
+  keep_scatter_kernel<<<grid_for_n(n), kThreads, 0, t->stream>>>(nullptr, nullptr, nullptr, n, t->rowptr.p,
+                                                                   nullptr, nullptr, nullptr, t->src.p);
   count_launches(2);
-  *src = t->src.p;
-  *n_src = total;
+  a.src = t->src.p;
+  a.n_src = total;
   return B12G_OK;
 }
 
 b12g_status mixed_args(b12g_tree* t, const b12g_scheme* sc, MixedArgs& a)
 {
-  if (sc && sc->depth != B12G_LEAF_DEPTH)
-    return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "the scheme of a tree of mixed depths maps its leaves (depth 255)");
   Prepared pr;
   ST(prepare(t, sc, pr));
   a = MixedArgs{};
@@ -1019,7 +1074,7 @@ b12g_status mixed_image_at_depth(b12g_tree* t, const b12g_scheme* sc, uint8_t de
   ST(mixed_enter(t));
   MixedArgs a;
   ST(mixed_args(t, sc, a));
-  ST(mixed_sources(t, sc, &a.src, &a.n_src));
+  ST(mixed_sources(t, sc, a));
   const uint64_t np = uint64_t(a.n_src) * a.points;
   if (n_points) *n_points = np;
   uint32_t boxes = 0;
@@ -1128,7 +1183,7 @@ b12g_status mixed_set_flags_by_image(b12g_tree* t, const b12g_scheme* sc, uint8_
   if (depth != B12G_LEAF_DEPTH) return mixed_image_at_depth(t, sc, depth, flags, false, nullptr, n_changed);
   MixedArgs a;
   ST(mixed_args(t, sc, a));
-  ST(mixed_sources(t, sc, &a.src, &a.n_src));
+  ST(mixed_sources(t, sc, a));
   if (t->hit.n < t->n) {
     // the hit marks are all clear between calls (apply_hits clears what it reads)
     ST(t->hit.ensure(t->n, "hit marks"));
@@ -1154,7 +1209,7 @@ b12g_status mixed_search(b12g_tree* t, const b12g_scheme* sc, uint64_t* n_points
 {
   MixedArgs a;
   ST(mixed_args(t, sc, a));
-  ST(mixed_sources(t, sc, &a.src, &a.n_src));
+  ST(mixed_sources(t, sc, a));
   const uint64_t np = uint64_t(a.n_src) * a.points;
   ST(t->out.ensure(std::max<uint64_t>(np, 1), "search output"));
   a.out = t->out.p;
@@ -1372,7 +1427,7 @@ b12g_status mixed_image_boxes(b12g_tree* t, const b12g_scheme* sc, uint64_t* n_p
   ST(mixed_enter(t));
   MixedArgs a;
   ST(mixed_args(t, sc, a));
-  ST(mixed_sources(t, sc, &a.src, &a.n_src));
+  ST(mixed_sources(t, sc, a));
   const uint64_t np = uint64_t(a.n_src) * a.points;
   ST(t->cand.ensure(std::max<uint64_t>(np, 256), "point boxes"));
   ST(t->pvalid.ensure(std::max<uint64_t>(np, 1), "point boxes"));

@@ -123,6 +123,7 @@ struct b12g_tree {
   Buf<uint8_t> pvalid, ins_dep, ins_dep2, scan_dep, scan_flags;
   Buf<uint64_t> ins_code, ins_key[2], scan_code;
   Buf<uint32_t> ins_idx[2], ins_pos, ins_head;
+  Buf<uint32_t> isrc_head, isrc_pos, isrc_and, isrc;   // scheme sources at an inner depth
   Buf<ulonglong2> hash;        // leaf lookup table
   uint32_t hash_tag = 0;       // tag of the last build (1..255; 0 = cleared)
   uint32_t hash_log2 = 0;      // log2 of the table's slots

@@ -833,44 +833,91 @@ static uint32_t search_at_depth(const orc_tree* t, const uint32_t* box, uint64_t
   return found == ORC_INVALID ? ORC_INVALID : box[found];
 }
 
-/* flags on the boxes at depth d hit by the images of every leaf (setFlagsByIterators
- * with makePointIteratorPairOverLeaves at an inner depth, ImplicitBoxTree.hpp:2691-2694
- * via setFlagsBySearch 2776-2800): every leaf of a hit box gets the flags; returns the
- * hit boxes whose leaves did not all have them.  out (if not NULL) gets each point's
- * box index instead, and nothing changes. */
-uint32_t orc_image_at_depth(orc_tree* t, const orc_map* m, const orc_grid* g, uint32_t d, uint8_t flags,
-                            uint32_t* out)
+/* the sources of a scheme (initializeLeafIndicesFromDepth, ImplicitBoxTree.hpp:1476-1611):
+ * at the leaf depth (255) the leaves with all of flags_to_check; at an inner depth d the
+ * boxes at d whose leaves all have them, each as its first leaf taken to depth d
+ * (DecrementDepthToFunctor in makePointIteratorPairByFlags, 2303-2341) */
+static uint64_t scheme_sources(const orc_tree* t, uint32_t src_depth, uint8_t flags_to_check, uint64_t* code,
+                               uint32_t* depth)
+{
+  uint64_t ns = 0;
+  if (src_depth == ORC_LEAF_DEPTH) {
+    for (uint64_t i = 0; i < t->n; ++i)
+      if (flags_set(t->flags[i], flags_to_check)) { code[ns] = t->code[i]; depth[ns] = t->depth[i]; ++ns; }
+    return ns;
+  }
+  uint64_t i = 0;
+  while (i < t->n) {
+    if (t->depth[i] < src_depth) { ++i; continue; }
+    const uint64_t pre = t->code[i] >> (t->depth[i] - src_depth);
+    uint64_t j = i;
+    uint8_t all = 0xFF;
+    while (j < t->n && t->depth[j] >= src_depth && (t->code[j] >> (t->depth[j] - src_depth)) == pre) all &= t->flags[j++];
+    if (flags_set(all, flags_to_check)) { code[ns] = pre; depth[ns] = src_depth; ++ns; }
+    i = j;
+  }
+  return ns;
+}
+
+/* the images of a scheme's sources located among the leaves (target 255: leaf index,
+ * searchByIterators 2394-2432) or at an inner depth (the box index, 2473-2566).  With
+ * out == NULL the hit leaves / every leaf of the hit boxes get `flags`
+ * (setFlagsByIterators 2691-2694 via setFlagsBySearch 2717-2800), and the return value
+ * counts the hit leaves / boxes that lacked them; with out != NULL each point's index is
+ * written and nothing changes.  *n_points gets the number of points. */
+uint32_t orc_image_search(orc_tree* t, const orc_map* m, const orc_grid* g, uint32_t src_depth, uint8_t flags_to_check,
+                          uint32_t target, uint8_t flags, uint32_t* out, uint64_t* n_points)
 {
   const uint64_t n = t->n, P = points_per_box(g, t->dom.dim);
   const uint32_t D = t->dom.dim;
+  uint64_t* scode = (uint64_t*)malloc((n ? n : 1) * 8);
+  uint32_t* sdep = (uint32_t*)malloc((n ? n : 1) * 4);
+  const uint64_t ns = scheme_sources(t, src_depth, flags_to_check, scode, sdep);
+  if (n_points) *n_points = ns * P;
   uint64_t nb = 0;
-  uint32_t* box = boxes_at_depth(t, d, &nb);
-  uint8_t* hit = (uint8_t*)calloc(nb ? nb : 1, 1);
-  for (uint64_t i = 0; i < n * P; ++i) {
+  uint32_t* box = target == ORC_LEAF_DEPTH ? NULL : boxes_at_depth(t, target, &nb);
+  const uint64_t nt = target == ORC_LEAF_DEPTH ? n : nb;
+  uint8_t* hit = (uint8_t*)calloc(nt ? nt : 1, 1);
+  for (uint64_t i = 0; i < ns * P; ++i) {
     const uint64_t b = i / P;
     double c[ORC_MAX_DIM], r[ORC_MAX_DIM], gp[ORC_MAX_DIM], y[ORC_MAX_DIM];
-    orc_box_coordinates(&t->dom, t->code[b], t->depth[b], c, r);
+    orc_box_coordinates(&t->dom, scode[b], sdep[b], c, r);
     orc_grid_point(g, D, i, gp);
     for (uint32_t j = 0; j < D; ++j) c[j] += gp[j] * r[j];
     orc_map_apply(m, c, y);
     uint64_t c64;
     const int valid = orc_point_code64(&t->dom, y, &c64);
-    const uint32_t s = search_at_depth(t, box, c64, valid, d);
+    const uint32_t s = target == ORC_LEAF_DEPTH ? orc_search(t, c64, valid) : search_at_depth(t, box, c64, valid, target);
     if (out) out[i] = s;
     else if (s != ORC_INVALID) hit[s] = 1;
   }
   uint32_t count = 0;
   if (!out) {
-    uint8_t* all = (uint8_t*)malloc(nb ? nb : 1);
-    memset(all, 0xFF, nb ? nb : 1);
-    for (uint64_t i = 0; i < n; ++i) if (box[i] != ORC_INVALID) all[box[i]] &= t->flags[i];
-    for (uint64_t b = 0; b < nb; ++b) count += hit[b] && !flags_set(all[b], flags);
-    for (uint64_t i = 0; i < n; ++i) if (box[i] != ORC_INVALID && hit[box[i]]) t->flags[i] |= flags;
-    free(all);
+    if (target == ORC_LEAF_DEPTH) {
+      for (uint64_t i = 0; i < n; ++i)
+        if (hit[i]) { count += !flags_set(t->flags[i], flags); t->flags[i] |= flags; }
+    } else {
+      uint8_t* all = (uint8_t*)malloc(nb ? nb : 1);
+      memset(all, 0xFF, nb ? nb : 1);
+      for (uint64_t i = 0; i < n; ++i) if (box[i] != ORC_INVALID) all[box[i]] &= t->flags[i];
+      for (uint64_t b = 0; b < nb; ++b) count += hit[b] && !flags_set(all[b], flags);
+      for (uint64_t i = 0; i < n; ++i) if (box[i] != ORC_INVALID && hit[box[i]]) t->flags[i] |= flags;
+      free(all);
+    }
   }
   free(hit);
   free(box);
+  free(scode);
+  free(sdep);
   return count;
+}
+
+/* images of every leaf located at an inner depth d (orc_image_search with the leaves as
+ * sources) */
+uint32_t orc_image_at_depth(orc_tree* t, const orc_map* m, const orc_grid* g, uint32_t d, uint8_t flags,
+                            uint32_t* out)
+{
+  return orc_image_search(t, m, g, ORC_LEAF_DEPTH, 0, d, flags, out, NULL);
 }
 
 /* computeDepthOfMutualAncestor (Box.hpp:209-223) */

@@ -110,6 +110,11 @@ uint32_t orc_flags_at_depth(orc_tree* t, int op, uint8_t u, uint8_t f, uint32_t 
  * hit boxes that lacked them), or with out != NULL each point's box index at d */
 uint32_t orc_image_at_depth(orc_tree* t, const orc_map* m, const orc_grid* g, uint32_t d, uint8_t flags,
                             uint32_t* out);
+/* the images of a scheme's sources (leaves with flags_to_check at src_depth 255, or the
+ * boxes of an inner src_depth whose leaves all have them) located at `target` (255: the
+ * leaves, else an inner depth): flags on what is hit, or each point's index into out */
+uint32_t orc_image_search(orc_tree* t, const orc_map* m, const orc_grid* g, uint32_t src_depth, uint8_t flags_to_check,
+                          uint32_t target, uint8_t flags, uint32_t* out, uint64_t* n_points);
 uint32_t orc_insert_boxes(orc_tree* t, const uint64_t* code64, const uint8_t* valid, uint64_t n_points,
                           uint32_t depth, uint8_t ins, uint8_t hit, int* unsupported);
 uint32_t orc_insert_points_general(orc_tree* t, const double* pts, uint64_t n_points, uint32_t depth, uint8_t ins,

@@ -83,6 +83,7 @@ def lib():
             "orc_unsubdivide": (u32, [P(OrcTree), u8]),
             "orc_flags_at_depth": (u32, [P(OrcTree), C.c_int, u8, u8, u32]),
             "orc_image_at_depth": (u32, [P(OrcTree), P(OrcMap), P(OrcGrid), u32, u8, P(u32)]),
+            "orc_image_search": (u32, [P(OrcTree), P(OrcMap), P(OrcGrid), u32, u8, u32, u8, P(u32), P(u64)]),
             "orc_insert_points_general": (u32, [P(OrcTree), P(dbl), u64, u32, u8, u8, P(C.c_int)]),
             "orc_insert_by_image_general": (u32, [P(OrcTree), P(OrcMap), P(OrcGrid), u8, u32, u8, u8,
                                                   P(C.c_int)]),
@@ -232,6 +233,22 @@ class Oracle:
         self.L.orc_image_at_depth(C.byref(self.tree), C.byref(self.map), C.byref(self.grid), depth, 0,
                                   _ptr(out, C.c_uint32))
         return out
+
+    def image_flags(self, src_depth, check, target, f):
+        """flags on what the images of a scheme's sources hit (sources at src_depth with
+        all of `check`; target 255 = leaves, else an inner depth); returns the count"""
+        return self.L.orc_image_search(C.byref(self.tree), C.byref(self.map), C.byref(self.grid), src_depth, check,
+                                       target, f, None, None)
+
+    def image_search(self, src_depth, check, target):
+        """each image point's leaf (target 255) or box index at an inner target depth"""
+        npts = C.c_uint64()
+        self.L.orc_image_search(C.byref(self.tree), C.byref(self.map), C.byref(self.grid), src_depth, check, target, 0,
+                                None, C.byref(npts))
+        out = np.zeros(max(npts.value, 1), dtype=np.uint32)
+        self.L.orc_image_search(C.byref(self.tree), C.byref(self.map), C.byref(self.grid), src_depth, check, target, 0,
+                                _ptr(out, C.c_uint32), None)
+        return out[:npts.value]
 
     def flags_at_depth(self, op, u, f, depth):
         """set (0) / unset (1) / change (2, u -> f) flags of the boxes at an inner depth"""

@@ -168,6 +168,23 @@ void runEdits(Tree& ibt, const std::vector<double>& c, const std::vector<double>
   ibt.insertByPoints(pts(300, 4, "points_13.bin"), Depth(md - 1), Flag::INS, Flag::EXPD);
   js << ", " << ibt.count(getLeafDepth());
   dump(13);
+  // images of the boxes of an inner depth (makePointIteratorPairByFlags / OverDepth below
+  // the leaves, 2267-2341, sources from initializeLeafIndicesFromDepth 1476-1611)
+  js << ", " << ibt.setFlagsByIterators(ibt.makePointIteratorPairByFlags(Depth(md - 3), Flag::EXPD, grid, map),
+                                        Flag::ENTR, getLeafDepth());
+  dump(14);
+  {
+    auto s = ibt.searchByIterators(ibt.makePointIteratorPairOverDepth(Depth(md - 2), grid, map), getLeafDepth());
+    std::vector<uint32_t> h(s.begin(), s.end());
+    if (!dir.empty()) {
+      FILE* f = openOut(dir + "/search_15.bin");
+      const uint64_t n = h.size();
+      std::fwrite(&n, 8, 1, f);
+      std::fwrite(h.data(), 4, n, f);
+      std::fclose(f);
+    }
+    js << ", " << h.size();
+  }
   js << "], \"edit_max_depth\": " << maxd << ", \"edit_flag_depth\": " << md;
 }
 

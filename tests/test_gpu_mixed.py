@@ -281,6 +281,10 @@ def test_unsubdivide_and_insert_match_reference(golden, name):
     np.testing.assert_array_equal(t.search_by_image(sc, md - 3), arrays["search_12"])
     t.insert_points(arrays["points_13"], md - 1, B.INS, B.EXPD)
     check_edit(t, want["13"], "13")
+    # images of the boxes of an inner depth (sources: boxes whose leaves all carry EXPD)
+    assert t.set_flags_by_image(B.Scheme(sc.map, sc.grid, md - 3, B.EXPD), B.ENTR) == counts[13]
+    check_edit(t, want["14"], "14")
+    np.testing.assert_array_equal(t.search_by_image(B.Scheme(sc.map, sc.grid, md - 2, 0)), arrays["search_15"])
     m = t.transition_matrix(sc, invalid_column=spec.get("invalid", False))
     d = csr_digests(*m.to_host())
     for key in ("nnz", "rowptr_sha256", "cols_sha256", "vals_sha256"):

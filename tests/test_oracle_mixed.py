@@ -94,6 +94,8 @@ def edit_sequence(o, meta, arrays):
     yield "11", o.image_flags_at_depth(md - 2, 1)       # setFlagsByIterators(leaves, HIT, md - 2)
     yield "search", o.image_search_at_depth(md - 3)     # searchByIterators(leaves, md - 3)
     yield "13", o.insert_points_general(arrays["points_13"], md - 1, 2, 4)   # insert(pts, md - 1, INS, EXPD)
+    yield "14", o.image_flags(md - 3, 4, 255, 0x20)      # setFlagsByIterators(ByFlags(md - 3, EXPD), ENTR)
+    yield "search15", o.image_search(md - 2, 0, 255)    # searchByIterators(OverDepth(md - 2), leaves)
 
 
 @pytest.mark.parametrize("name", EDIT_CASES)
@@ -106,8 +108,8 @@ def test_unsubdivide_and_insert_match_reference(golden, name):
     want = {e["step"]: e for e in meta["edits"]}
     counts = meta["timing"]["edits"]
     for k, (key, ret) in enumerate(edit_sequence(o, meta, arrays)):
-        if key == "search":
-            np.testing.assert_array_equal(ret, arrays["search_12"])
+        if key in ("search", "search15"):
+            np.testing.assert_array_equal(ret, arrays["search_12" if key == "search" else "search_15"])
             assert len(ret) == counts[k]
             continue
         codes, depth, flags = o.leaves()
@@ -116,7 +118,7 @@ def test_unsubdivide_and_insert_match_reference(golden, name):
         assert sha(codes) == e["codes_sha256"], f"{key} codes"
         assert sha(depth) == e["depth_sha256"], f"{key} depths"
         assert sha(flags) == e["flags_sha256"], f"{key} flags"
-        if key in ("01", "02", "08", "09", "10", "11"):
+        if key in ("01", "02", "08", "09", "10", "11", "14"):
             assert ret == counts[k], key          # the call's own return value
         else:
             assert len(codes) == counts[k], key   # the run records the leaf count
