@@ -23,8 +23,9 @@
  *     of several depths, switches it to per-leaf depths until one depth is left.  At a
  *     depth inside the tree, flags (and image flags, insertion hit flags) change every
  *     leaf of each box at that depth, and searches return the box's index among the
- *     boxes at that depth.  On a tree of mixed depths schemes map the leaves (source
- *     depth 255); the unsubdividable depth 254 is not offered; those calls return
+ *     boxes at that depth.  A scheme's source depth may be 255 (the leaves) or a depth
+ *     inside the tree (its boxes whose leaves all carry the scheme's flags).  Source
+ *     depth 0 and the unsubdividable depth 254 are not offered; those calls return
  *     B12G_ERR_UNSUPPORTED_MIXED_DEPTH and leave the tree unchanged.
  *   - Host pointers are plain host memory (pinned or pageable); the library owns all
  *     device memory of a tree and of a CSR matrix.

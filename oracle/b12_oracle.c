@@ -1112,29 +1112,35 @@ uint32_t orc_insert_points_general(orc_tree* t, const double* pts, uint64_t n_po
 
 /* insertByIterators(makePointIteratorPairByFlags(255, flags_to_check, grid, map), ...)
  * through the general insert: the images of the leaves with flags_to_check */
-uint32_t orc_insert_by_image_general(orc_tree* t, const orc_map* m, const orc_grid* g, uint8_t flags_to_check,
-                                     uint32_t depth, uint8_t ins, uint8_t hit, int* unsupported)
+uint32_t orc_insert_by_image_src(orc_tree* t, const orc_map* m, const orc_grid* g, uint32_t src_depth,
+                                 uint8_t flags_to_check, uint32_t depth, uint8_t ins, uint8_t hit, int* unsupported)
 {
   const uint64_t n = t->n, P = points_per_box(g, t->dom.dim);
   const uint32_t D = t->dom.dim;
-  uint64_t ns = 0;
-  uint32_t* src = (uint32_t*)malloc((n ? n : 1) * 4);
-  for (uint64_t i = 0; i < n; ++i) if (flags_set(t->flags[i], flags_to_check)) src[ns++] = (uint32_t)i;
+  uint64_t* scode = (uint64_t*)malloc((n ? n : 1) * 8);
+  uint32_t* sdep = (uint32_t*)malloc((n ? n : 1) * 4);
+  const uint64_t ns = scheme_sources(t, src_depth, flags_to_check, scode, sdep);
   const uint64_t total = ns * P;
   uint64_t* c = (uint64_t*)malloc((total ? total : 1) * 8);
   uint8_t* v = (uint8_t*)malloc(total ? total : 1);
   for (uint64_t i = 0; i < total; ++i) {
-    const uint32_t b = src[i / P];
+    const uint64_t b = i / P;
     double ctr[ORC_MAX_DIM], r[ORC_MAX_DIM], gp[ORC_MAX_DIM], y[ORC_MAX_DIM];
-    orc_box_coordinates(&t->dom, t->code[b], t->depth[b], ctr, r);
+    orc_box_coordinates(&t->dom, scode[b], sdep[b], ctr, r);
     orc_grid_point(g, D, i, gp);
     for (uint32_t j = 0; j < D; ++j) ctr[j] += gp[j] * r[j];
     orc_map_apply(m, ctr, y);
     v[i] = (uint8_t)orc_point_code64(&t->dom, y, c + i);
   }
   const uint32_t res = orc_insert_boxes(t, c, v, total, depth, ins, hit, unsupported);
-  free(c); free(v); free(src);
+  free(c); free(v); free(scode); free(sdep);
   return res;
+}
+
+uint32_t orc_insert_by_image_general(orc_tree* t, const orc_map* m, const orc_grid* g, uint8_t flags_to_check,
+                                     uint32_t depth, uint8_t ins, uint8_t hit, int* unsupported)
+{
+  return orc_insert_by_image_src(t, m, g, ORC_LEAF_DEPTH, flags_to_check, depth, ins, hit, unsupported);
 }
 
 /* ------------------------------------------------------------------------------

@@ -121,6 +121,10 @@ uint32_t orc_insert_points_general(orc_tree* t, const double* pts, uint64_t n_po
                                    uint8_t hit, int* unsupported);
 uint32_t orc_insert_by_image_general(orc_tree* t, const orc_map* m, const orc_grid* g, uint8_t flags_to_check,
                                      uint32_t depth, uint8_t ins, uint8_t hit, int* unsupported);
+/* the same with the scheme's sources at src_depth (255: leaves; else the boxes of that
+ * inner depth whose leaves all have flags_to_check) */
+uint32_t orc_insert_by_image_src(orc_tree* t, const orc_map* m, const orc_grid* g, uint32_t src_depth,
+                                 uint8_t flags_to_check, uint32_t depth, uint8_t ins, uint8_t hit, int* unsupported);
 
 /* transition matrix on the leaves, row-major CSR; returns nnz.  Pass NULL arrays to
  * query nnz only.  absolute: values are counts; invalid: lost points go to column

@@ -83,6 +83,7 @@ def lib():
             "orc_unsubdivide": (u32, [P(OrcTree), u8]),
             "orc_flags_at_depth": (u32, [P(OrcTree), C.c_int, u8, u8, u32]),
             "orc_image_at_depth": (u32, [P(OrcTree), P(OrcMap), P(OrcGrid), u32, u8, P(u32)]),
+            "orc_insert_by_image_src": (u32, [P(OrcTree), P(OrcMap), P(OrcGrid), u32, u8, u32, u8, u8, P(C.c_int)]),
             "orc_image_search": (u32, [P(OrcTree), P(OrcMap), P(OrcGrid), u32, u8, u32, u8, P(u32), P(u64)]),
             "orc_insert_points_general": (u32, [P(OrcTree), P(dbl), u64, u32, u8, u8, P(C.c_int)]),
             "orc_insert_by_image_general": (u32, [P(OrcTree), P(OrcMap), P(OrcGrid), u8, u32, u8, u8,
@@ -261,6 +262,11 @@ class Oracle:
         r = self.L.orc_insert_points_general(C.byref(self.tree), _ptr(pts, C.c_double), pts.size // self.spec["dim"],
                                              depth, ins, hit, C.byref(uns))
         return None if uns.value else r
+
+    def insert_by_image_src(self, src_depth, check, depth, ins=2, hit=0):
+        uns = C.c_int()
+        return self.L.orc_insert_by_image_src(C.byref(self.tree), C.byref(self.map), C.byref(self.grid), src_depth,
+                                              check, depth, ins, hit, C.byref(uns))
 
     def insert_by_image_general(self, check, depth, ins=2, hit=0):
         uns = C.c_int()

@@ -209,7 +209,7 @@ def test_unsupported_calls_refuse_and_leave_the_tree(golden):
     step(t, sc)
     before = [a.copy() for a in t.leaves()]
     for call in (lambda: t.set_flags(B.EXPD, 254), lambda: t.set_flags_by_image(sc, B.HIT, 0),
-                 lambda: t.insert_by_image(B.Scheme(sc.map, sc.grid, 9, B.INS), 9)):
+                 lambda: t.insert_by_image(B.Scheme(sc.map, sc.grid, 0, B.INS), 9)):
         with pytest.raises(B.B12gError) as e:
             call()
         assert e.value.status == B._lib.ERR_MIXED_DEPTH
@@ -385,3 +385,21 @@ def test_flags_at_an_inner_depth_of_a_one_depth_tree(golden, op):
         for x, y in zip(t.leaves(), o.leaves()):
             np.testing.assert_array_equal(x, y)
         assert t.depth() == 12
+
+
+@pytest.mark.parametrize("src_depth,depth", [(13, 255), (15, 17), (12, 14)])
+def test_insertion_of_images_of_inner_boxes_matches_oracle(golden, src_depth, depth):
+    meta, arrays = golden("henon_d12_mixed6_edits")
+    spec = meta["spec"]
+    last = meta["mixed"][-1]["step"]
+    leaves = (arrays[f"mixed_codes_{last:02d}"], arrays[f"mixed_depth_{last:02d}"], arrays[f"mixed_flags_{last:02d}"])
+    c, r = domain(spec)
+    t = B.ImplicitBoxTree(c, r)
+    t.load_leaves(*leaves)
+    o = O.Oracle(oracle_spec(spec))
+    o.load(*leaves)
+    sc = scheme(spec)
+    got = t.insert_by_image(B.Scheme(sc.map, sc.grid, src_depth, B.SD), depth, B.INS, B.HIT)
+    assert got == o.insert_by_image_src(src_depth, 8, depth, 2, 1)
+    for x, y in zip(t.leaves(), o.leaves()):
+        np.testing.assert_array_equal(x, y)
