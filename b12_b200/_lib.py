@@ -95,6 +95,14 @@ _SIGS = {
     "b12g_insert_by_image": (C.c_int, [C.c_void_p, C.POINTER(Scheme), C.c_uint8, C.c_uint8, C.c_uint8,
                                        C.POINTER(C.c_uint32)]),
     "b12g_transition_matrix": (C.c_int, [C.c_void_p, C.POINTER(Scheme), C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "b12g_image_point_boxes": (C.c_int, [C.c_void_p, C.POINTER(Scheme), C.c_void_p, C.c_void_p, C.c_uint64,
+                                         C.POINTER(C.c_uint64)]),
+    "b12g_search_point_boxes": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p]),
+    "b12g_set_flags_by_point_boxes": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint8,
+                                                C.POINTER(C.c_uint32)]),
+    "b12g_transition_rows": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_int, C.c_int,
+                                       C.POINTER(C.c_void_p)]),
+    "b12g_load_leaves_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]),
     "b12g_csr_shape": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]),
     "b12g_csr_copy": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "b12g_csr_destroy": (C.c_int, [C.c_void_p]),

@@ -421,10 +421,18 @@ b12g_status b12g_leaves(b12g_tree* t, uint64_t* codes, uint8_t* depths, uint8_t*
 {
   if (!t) return fail(B12G_ERR_INVALID, "NULL tree");
   if (t->mixed) return mixed_leaves(t, codes, depths, flags);
-  if (codes) CK(cudaMemcpyAsync(codes, t->codes(), size_t(t->n) * 8, cudaMemcpyDeviceToHost, t->stream));
-  if (flags) CK(cudaMemcpyAsync(flags, t->flg(), t->n, cudaMemcpyDeviceToHost, t->stream));
+  // host or device buffers (unified addressing tells the copies which)
+  if (codes) CK(cudaMemcpyAsync(codes, t->codes(), size_t(t->n) * 8, cudaMemcpyDefault, t->stream));
+  if (flags) CK(cudaMemcpyAsync(flags, t->flg(), t->n, cudaMemcpyDefault, t->stream));
+  cudaPointerAttributes pa{};
+  bool dev_depths = false;
+  if (depths) {
+    if (cudaPointerGetAttributes(&pa, depths) == cudaSuccess) dev_depths = pa.type == cudaMemoryTypeDevice;
+    else cudaGetLastError();  // a pointer CUDA does not know is host memory
+  }
+  if (dev_depths) CK(cudaMemsetAsync(depths, t->depth, t->n, t->stream));
   ST(sync(t, "leaves"));
-  if (depths) std::memset(depths, t->depth, t->n);
+  if (depths && !dev_depths) std::memset(depths, t->depth, t->n);
   return B12G_OK;
 }
 
@@ -652,18 +660,34 @@ b12g_status b12g_transition_matrix(b12g_tree* t, const b12g_scheme* sc, int abso
     CK(launch_rows(sc->map.kind, sc->map.arith, sc->grid.kind, t->domain.dim, ra, n, t->stream));
     prof_mark(t, 1);
   }
+  if (!t->mixed) count_launches(1);    // mixed_rows counts its own launches
+  ST(finish_rows(t, uint32_t(pr.P), n, absolute, invalid_column, out));
+  return prof_collect(t);
+}
+
+}  // extern "C"
+
+namespace b12g {
+namespace host {
+
+// The CSR of the rows staged for the tree's n leaves (stage_col / stage_cnt / row_count,
+// P slots a row): row pointers by a scan, then every row's runs gathered.  Columns index
+// n_cols boxes; lost points, kept in column n_cols + 1, make nColumns n_cols + 1 only when
+// some row has one (ImplicitBoxTree.hpp:3075-3090).  An existing matrix in *out is
+// refilled in place (its buffers only grow).
+b12g_status finish_rows(b12g_tree* t, uint32_t P, uint32_t n_cols, int absolute, int invalid_column, b12g_csr** out)
+{
+  const uint32_t n = t->n;
   CK(exclusive_scan_u32(t->row_count.p, t->rowptr.p, t->dn(), t->tiles_a.p, n, t->stream));
   CK(cudaMemcpyAsync(t->h_ctr + C_NNZ, t->rowptr.p + n, 4, cudaMemcpyDeviceToHost, t->stream));
-  count_launches(t->mixed ? 3 : 4);   // mixed_rows counts its own launches
+  count_launches(3);
   ST(sync(t, "transition rows"));
-  ST(prof_collect(t));
   const uint32_t nnz32 = t->h_ctr[C_NNZ];
-  // an existing matrix passed in *out is refilled in place (its buffers only grow)
   const bool fresh = *out == nullptr;
   b12g_csr* m = fresh ? new b12g_csr() : *out;
   m->device = t->device;
   m->n_rows = n;
-  m->n_cols = invalid_column ? n + 1 : n;
+  m->n_cols = n_cols;
   m->nnz = nnz32;
   m->has_transpose = false;
   b12g_status st = B12G_OK;
@@ -673,12 +697,22 @@ b12g_status b12g_transition_matrix(b12g_tree* t, const b12g_scheme* sc, int abso
   if (st == B12G_OK) st = m->cols.ensure(std::max<uint64_t>(m->nnz, 1), "cols");
   if (st == B12G_OK) st = m->vals.ensure(std::max<uint64_t>(m->nnz, 1), "vals");
   if (st == B12G_OK) st = m->ctr.ensure(256, "csr counters");
+  const bool find_lost = invalid_column && nnz32 != 0;
+  if (st == B12G_OK && find_lost) st = set_ctr(t, C_TMP, 0);
   if (st == B12G_OK) {
     cudaMemcpyAsync(m->rowptr.p, t->rowptr.p, size_t(n + 1) * 4, cudaMemcpyDeviceToDevice, t->stream);
-    gather_rows(t->stage_col.p, t->stage_cnt.p, uint32_t(pr.P), t->row_count.p, t->rowptr.p, t->dn(), m->cols.p,
-                m->vals.p, absolute, double(pr.P), n, t->stream);
+    gather_rows(t->stage_col.p, t->stage_cnt.p, P, t->row_count.p, t->rowptr.p, t->dn(), m->cols.p, m->vals.p,
+                absolute, double(P), n, t->stream);
     count_launches(1);
+    if (find_lost) {
+      value_present(m->cols.p, nnz32, n_cols + 1, t->ctr.p + C_TMP, t->stream);
+      count_launches(1);
+    }
     st = sync(t, "gather rows");
+  }
+  if (st == B12G_OK && find_lost) {
+    st = read_ctr(t, C_TMP, 1);
+    if (st == B12G_OK && t->h_ctr[C_TMP] != 0) m->n_cols = n_cols + 1;
   }
   if (st != B12G_OK) {
     if (fresh) b12g_csr_destroy(m);
@@ -687,6 +721,11 @@ b12g_status b12g_transition_matrix(b12g_tree* t, const b12g_scheme* sc, int abso
   *out = m;
   return B12G_OK;
 }
+
+}  // namespace host
+}  // namespace b12g
+
+extern "C" {
 
 b12g_status b12g_csr_shape(const b12g_csr* m, uint32_t* n_rows, uint32_t* n_cols, uint64_t* nnz)
 {

@@ -121,4 +121,8 @@ cudaError_t gather_rows(const uint32_t* stage_col, const uint32_t* stage_cnt, ui
                         uint32_t* cols, double* vals, int absolute, double points, uint32_t max_rows,
                         cudaStream_t s);
 
+// partition.cu -----------------------------------------------------------------------
+// *found = 1 when some of the n values equals x (found is not cleared)
+cudaError_t value_present(const uint32_t* v, uint64_t n, uint32_t x, uint32_t* found, cudaStream_t s);
+
 }  // namespace b12g

@@ -826,6 +826,41 @@ cudaError_t dispatch(uint32_t map_kind, uint32_t arith, uint32_t grid_kind, uint
   }
 }
 
+// the leaf of each of n point boxes given by the caller (the search of
+// searchByIterators / setFlagsByIterators, ImplicitBoxTree.hpp:2394-2432): its index into
+// `index`, or (index null) a hit mark on it
+__global__ void point_box_kernel(const CmpIndex ix, const uint64_t* __restrict__ code,
+                                 const uint8_t* __restrict__ dep, const uint64_t* __restrict__ p64,
+                                 const uint8_t* __restrict__ valid, uint64_t n, uint32_t* index, uint8_t* hit)
+{
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+    const uint32_t t = locate_mixed(ix, code, dep, __ldg(valid + i) != 0, __ldg(p64 + i));
+    if (index) index[i] = t;
+    else if (t != kInvalidIndex) hit[t] = 1;
+  }
+}
+
+// counts the leaves that break the tree's invariants: a depth above 64, bits above the
+// depth, or a leaf that does not strictly precede the next one or contains it
+__global__ void leaf_order_kernel(const uint64_t* code, const uint8_t* dep, uint32_t n, uint32_t* bad)
+{
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t d = dep[i];
+    bool ok = d <= 64 && (d == 64 || (code[i] >> d) == 0);
+    if (ok && i + 1 < n) {
+      const uint32_t e = dep[i + 1];
+      if (e > 64) {
+        ok = false;
+      } else {
+        const uint32_t m = d < e ? d : e;
+        const bool nested = m == 0 || (srs(code[i], d - m) == srs(code[i + 1], e - m));
+        ok = comparable(code[i], d) < comparable(code[i + 1], e) && !nested;
+      }
+    }
+    if (!ok) atomicAdd(bad, 1u);
+  }
+}
+
 // ---------------------------------------------------------------------------- host helpers
 uint8_t* dep_cur(b12g_tree* t) { return t->dep[t->cur].p; }
 
@@ -1118,9 +1153,9 @@ b12g_status mixed_count(b12g_tree* t, uint8_t depth, uint32_t* count)
 
 b12g_status mixed_leaves(b12g_tree* t, uint64_t* codes, uint8_t* depths, uint8_t* flags)
 {
-  if (codes) CK(cudaMemcpyAsync(codes, t->codes(), size_t(t->n) * 8, cudaMemcpyDeviceToHost, t->stream));
-  if (flags) CK(cudaMemcpyAsync(flags, t->flg(), t->n, cudaMemcpyDeviceToHost, t->stream));
-  if (depths) CK(cudaMemcpyAsync(depths, dep_cur(t), t->n, cudaMemcpyDeviceToHost, t->stream));
+  if (codes) CK(cudaMemcpyAsync(codes, t->codes(), size_t(t->n) * 8, cudaMemcpyDefault, t->stream));
+  if (flags) CK(cudaMemcpyAsync(flags, t->flg(), t->n, cudaMemcpyDefault, t->stream));
+  if (depths) CK(cudaMemcpyAsync(depths, dep_cur(t), t->n, cudaMemcpyDefault, t->stream));
   return sync(t, "leaves");
 }
 
@@ -1441,6 +1476,100 @@ b12g_status mixed_image_boxes(b12g_tree* t, const b12g_scheme* sc, uint64_t* n_p
   count_launches(1);
   *n_points = np;
   return B12G_OK;
+}
+
+// the point boxes of the images of the scheme's sources into the caller's device buffers
+// (codes, validity), source-major; CAPACITY with *n_points set when they do not fit
+b12g_status mixed_image_point_boxes(b12g_tree* t, const b12g_scheme* sc, uint64_t* codes, uint8_t* valid,
+                                    uint64_t capacity, uint64_t* n_points)
+{
+  ST(mixed_enter(t));
+  MixedArgs a;
+  ST(mixed_args(t, sc, a));
+  ST(mixed_sources(t, sc, a));
+  const uint64_t np = uint64_t(a.n_src) * a.points;
+  *n_points = np;
+  if (np > capacity) {
+    ST(mixed_settle(t));
+    return fail(B12G_ERR_CAPACITY, "%llu image points, room for %llu", (unsigned long long)np,
+                (unsigned long long)capacity);
+  }
+  if (np && (!codes || !valid)) {
+    ST(mixed_settle(t));
+    return fail(B12G_ERR_INVALID, "NULL output buffer");
+  }
+  a.p64_out = codes;
+  a.valid_out = valid;
+  if (np) {
+    CK(dispatch(sc->map.kind, sc->map.arith, sc->grid.kind, t->domain.dim, [&](auto map, auto grid) -> cudaError_t {
+      mixed_image_kernel<decltype(map), decltype(grid), 2><<<grid_for_n(np), kThreads, 0, t->stream>>>(a);
+      return cudaGetLastError();
+    }));
+    count_launches(1);
+  }
+  ST(sync(t, "image point boxes"));
+  return mixed_settle(t);
+}
+
+// the leaf of each given point box into index (device), or, with index null, `flags` set
+// on every leaf that holds one; *n_changed counts the leaves whose flags changed
+b12g_status mixed_point_box_search(b12g_tree* t, const uint64_t* codes, const uint8_t* valid, uint64_t n,
+                                   uint32_t* index, uint8_t flags, uint32_t* n_changed)
+{
+  if (n_changed) *n_changed = 0;
+  if (n && (!codes || !valid)) return fail(B12G_ERR_INVALID, "NULL point boxes");
+  ST(mixed_enter(t));
+  ST(refresh_comparable(t));
+  const CmpIndex ix{t->cmp.p, t->cmp_tab.p, t->n, t->cmp_bits};
+  if (!index && t->hit.n < t->n) {
+    // the hit marks are all clear between calls (apply_hits clears what it reads)
+    ST(t->hit.ensure(t->n, "hit marks"));
+    CK(cudaMemsetAsync(t->hit.p, 0, t->hit.n, t->stream));
+  }
+  if (n) {
+    point_box_kernel<<<grid_for_n(n), kThreads, 0, t->stream>>>(ix, t->codes(), dep_cur(t), codes, valid, n, index,
+                                                                 t->hit.p);
+    CK(cudaGetLastError());
+    count_launches(1);
+  }
+  if (!index) {
+    ST(set_ctr(t, C_CHANGED, 0));
+    apply_hits_kernel<<<grid_for_n(t->n), kThreads, 0, t->stream>>>(t->flg(), t->hit.p, t->n, flags,
+                                                                     t->ctr.p + C_CHANGED);
+    count_launches(1);
+    ST(read_ctr(t, C_CHANGED, 1));
+    if (n_changed) *n_changed = t->h_ctr[C_CHANGED];
+  } else {
+    ST(sync(t, "search point boxes"));
+  }
+  return mixed_settle(t);
+}
+
+// leaves from device memory; the same checks as a load from the host, made on the device
+b12g_status mixed_load_device(b12g_tree* t, const uint64_t* codes, const uint8_t* depths, const uint8_t* flags,
+                              uint32_t n)
+{
+  if (n == 0) return set_root(t, B12G_NONE);
+  ST(reserve(t, n));
+  ST(ensure_dep(t, std::max<uint64_t>(t->code[0].n, n)));
+  CK(cudaMemcpyAsync(t->codes(), codes, size_t(n) * 8, cudaMemcpyDeviceToDevice, t->stream));
+  CK(cudaMemcpyAsync(t->flg(), flags, n, cudaMemcpyDeviceToDevice, t->stream));
+  CK(cudaMemcpyAsync(dep_cur(t), depths, n, cudaMemcpyDeviceToDevice, t->stream));
+  ST(set_ctr(t, C_TMP, 0));
+  leaf_order_kernel<<<grid_for_n(n), kThreads, 0, t->stream>>>(t->codes(), dep_cur(t), n, t->ctr.p + C_TMP);
+  CK(cudaGetLastError());
+  count_launches(1);
+  ST(read_ctr(t, C_TMP, 1));
+  if (t->h_ctr[C_TMP] != 0) {
+    const uint32_t bad = t->h_ctr[C_TMP];
+    ST(set_root(t, B12G_NONE));
+    return fail(B12G_ERR_INVALID, "%u leaves out of order, nested or deeper than 64", bad);
+  }
+  t->n = n;
+  t->mixed = true;
+  ST(set_ctr(t, t->ncur, n));
+  ST(sync(t, "load leaves"));
+  return mixed_settle(t);
 }
 
 }  // namespace host

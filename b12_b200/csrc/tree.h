@@ -192,6 +192,8 @@ void prof_mark(b12g_tree* t, int kind);
 b12g_status prof_collect(b12g_tree* t);
 // P^T of a matrix and its row classes, built on first use (api.cu)
 b12g_status ensure_transpose(b12g_csr* m);
+// the CSR of the rows staged in stage_col / stage_cnt / row_count for the tree's leaves (api.cu)
+b12g_status finish_rows(b12g_tree* t, uint32_t P, uint32_t n_cols, int absolute, int invalid_column, b12g_csr** out);
 
 // trees of mixed leaf depths (mixed.cu); t->mixed selects them, t->depth is the deepest leaf
 b12g_status mixed_enter(b12g_tree* t);
@@ -223,6 +225,15 @@ b12g_status mixed_insert_boxes(b12g_tree* t, uint64_t np, uint8_t depth, uint8_t
 // point boxes of host points, or of the images of a scheme's source leaves
 b12g_status mixed_point_boxes(b12g_tree* t, const double* points, uint64_t n_points);
 b12g_status mixed_image_boxes(b12g_tree* t, const b12g_scheme* sc, uint64_t* n_points);
+// point boxes in the caller's device buffers (range-partitioned trees): the images of the
+// scheme's sources, the leaf of each given point box, or flags set on the leaves hit
+b12g_status mixed_image_point_boxes(b12g_tree* t, const b12g_scheme* sc, uint64_t* codes, uint8_t* valid,
+                                    uint64_t capacity, uint64_t* n_points);
+b12g_status mixed_point_box_search(b12g_tree* t, const uint64_t* codes, const uint8_t* valid, uint64_t n,
+                                   uint32_t* index, uint8_t flags, uint32_t* n_changed);
+// leaves from device memory, checked for order and nesting on the device
+b12g_status mixed_load_device(b12g_tree* t, const uint64_t* codes, const uint8_t* depths, const uint8_t* flags,
+                              uint32_t n);
 
 }  // namespace host
 }  // namespace b12g

@@ -382,6 +382,75 @@ class ImplicitBoxTree:
             return into
         return CsrMatrix(h)
 
+    # ---- device buffers of a range-partitioned tree (torch tensors on this tree's GPU)
+    # Every call waits for torch's current stream first (the tensors, or the memory torch
+    # just handed out for them, may still be in use by work queued there, a collective
+    # among it) and returns after its own work, queued on the tree's stream, has finished.
+    @staticmethod
+    def _ready(*tensors):
+        import torch
+        for x in tensors:
+            if x is not None and x.is_cuda:
+                torch.cuda.current_stream(x.device).synchronize()
+                return
+
+    def image_point_boxes(self, scheme: Scheme, device):
+        """(codes, valid): the depth-64 point boxes of the images of the scheme's sources,
+        source-major, as int64 (the code's bits) and uint8 tensors on `device`."""
+        import torch
+        room = self.count() * scheme.grid.points_per_box(self.dim)
+        codes = torch.empty(max(room, 1), dtype=torch.int64, device=device)
+        valid = torch.empty(max(room, 1), dtype=torch.uint8, device=device)
+        n = C.c_uint64()
+        s = scheme.to_c()
+        self._ready(codes)
+        check(lib().b12g_image_point_boxes(self._h, C.byref(s), codes.data_ptr(), valid.data_ptr(), room,
+                                           C.byref(n)), "image_point_boxes")
+        return codes[: n.value], valid[: n.value]
+
+    def search_point_boxes(self, codes, valid):
+        """searchByIterators over point boxes: an int64 tensor of leaf indices (-1: none)."""
+        import torch
+        n = codes.numel()
+        out = torch.empty(max(n, 1), dtype=torch.int32, device=codes.device)
+        self._ready(codes, valid)
+        check(lib().b12g_search_point_boxes(self._h, codes.data_ptr(), valid.data_ptr(), n, out.data_ptr()),
+              "search_point_boxes")
+        return out[:n].to(torch.int64)   # B12G_INVALID_INDEX reads as -1 in int32
+
+    def set_flags_by_point_boxes(self, codes, valid, flags: int) -> int:
+        self._ready(codes, valid)
+        return self._n("b12g_set_flags_by_point_boxes", codes.data_ptr(), valid.data_ptr(), codes.numel(), flags)
+
+    def transition_rows(self, targets, points_per_row: int, n_columns: int, absolute: bool = False,
+                        invalid_column: bool = False) -> CsrMatrix:
+        """Rows of this tree's leaves from global targets (int32/int64 tensor, -1 for lost points)."""
+        import torch
+        t = targets.to(torch.int32).contiguous()
+        self._ready(t)
+        h = C.c_void_p()
+        check(lib().b12g_transition_rows(self._h, t.data_ptr(), points_per_row, n_columns, int(absolute),
+                                         int(invalid_column), C.byref(h)), "transition_rows")
+        return CsrMatrix(h)
+
+    def leaves_device(self, device):
+        """(codes int64, depths uint8, flags uint8) tensors of the leaves on `device`."""
+        import torch
+        n = self.count()
+        codes = torch.empty(n, dtype=torch.int64, device=device)
+        depth = torch.empty(n, dtype=torch.uint8, device=device)
+        flags = torch.empty(n, dtype=torch.uint8, device=device)
+        self._ready(codes)
+        check(lib().b12g_leaves(self._h, codes.data_ptr(), depth.data_ptr(), flags.data_ptr()), "leaves")
+        return codes, depth, flags
+
+    def load_leaves_device(self, codes, depth, flags):
+        """b12g_load_leaves from device tensors (checked on the device)."""
+        c, d, f = codes.contiguous(), depth.contiguous(), flags.contiguous()
+        self._ready(c, d, f)
+        check(lib().b12g_load_leaves_device(self._h, c.data_ptr(), d.data_ptr(), f.data_ptr(), c.numel()),
+              "load_leaves_device")
+
     # ---- measurement hooks
     def stream_handle(self) -> int:
         p = C.c_void_p()

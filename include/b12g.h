@@ -188,9 +188,44 @@ b12g_status b12g_insert_points(b12g_tree* tree, const double* points, uint64_t n
 b12g_status b12g_insert_by_image(b12g_tree* tree, const b12g_scheme* scheme, uint8_t depth,
                                  uint8_t flags_for_inserted, uint8_t flags_for_hit, uint32_t* n_inserted);
 
+/* ---- range-partitioned trees ---------------------------------------------------------
+ * One tree split over ranks, each holding a contiguous run of the leaves in the
+ * reference's order.  A subdivision step sends every image point box to the rank whose
+ * code range holds it; the reference is single-device, so these entries have no direct
+ * counterpart: each is the named reference step restricted to the leaves of one rank.
+ * Every pointer here is DEVICE memory (the buffers the collectives move); a point box is
+ * a depth-64 code with a validity byte (0: the point left the domain, the reference's
+ * invalid box (~0, 255)). */
+/* the point boxes of the images of the scheme's sources (GridPointsFunctor +
+ * PointToBox of makePointIteratorPairByFlags, ImplicitBoxTree.hpp:2624-2681),
+ * source-major; CAPACITY with *n_points set when capacity is too small */
+b12g_status b12g_image_point_boxes(b12g_tree* tree, const b12g_scheme* scheme, uint64_t* codes, uint8_t* valid,
+                                   uint64_t capacity, uint64_t* n_points);
+/* searchByIterators over n point boxes at the leaf depth (ImplicitBoxTree.hpp:2394-2432):
+ * the leaf holding each, or B12G_INVALID_INDEX */
+b12g_status b12g_search_point_boxes(b12g_tree* tree, const uint64_t* codes, const uint8_t* valid, uint64_t n,
+                                    uint32_t* index);
+/* setFlagsByIterators over n point boxes at the leaf depth (ImplicitBoxTree.hpp:2167-2196,
+ * 2717-2775); *n_changed = leaves whose flags changed */
+b12g_status b12g_set_flags_by_point_boxes(b12g_tree* tree, const uint64_t* codes, const uint8_t* valid, uint64_t n,
+                                          uint8_t flags, uint32_t* n_changed);
+/* the run-length step of transitionMatrixForLeaves (ImplicitBoxTree.hpp:2934-3090) for the
+ * tree's leaves as rows: targets holds points_per_row column indices a row (< n_columns,
+ * or B12G_INVALID_INDEX for a lost point), row-major; columns and the lost column follow
+ * b12g_transition_matrix with n = n_columns */
+b12g_status b12g_transition_rows(b12g_tree* tree, const uint32_t* targets, uint32_t points_per_row,
+                                 uint32_t n_columns, int absolute, int invalid_column, b12g_csr** csr);
+/* b12g_load_leaves from device buffers, with the same checks made on the device (a
+ * failed check leaves the surrounding box); b12g_leaves copies into host or device
+ * buffers alike */
+b12g_status b12g_load_leaves_device(b12g_tree* tree, const uint64_t* codes, const uint8_t* depths,
+                                    const uint8_t* flags, uint32_t n);
+
 /* ---- transition matrix (ImplicitBoxTree.hpp:2934-3193, CooMatrix.hpp:14-56) ---------- */
 /* transitionMatrixForLeaves<double>(grid, map, absolute, rowMajor=true, invalid):
  * row = source leaf, column = target leaf, value = count (absolute) or count / P.
+ * With `invalid_column`, lost points go to column n + 1 and the matrix has n + 1 columns
+ * if any point was lost, n otherwise (ImplicitBoxTree.hpp:3075-3090).
  * The result is a row-major CSR that stays on the device.  *csr must be NULL (a new
  * matrix is created) or a matrix from an earlier call, which is refilled in place. */
 b12g_status b12g_transition_matrix(b12g_tree* tree, const b12g_scheme* scheme, int absolute,

@@ -522,7 +522,8 @@ uint64_t orc_subdivision(orc_tree* t, const orc_map* m, const orc_grid* g, uint3
 /* ------------------------------------------------------------------------------
  * transition matrix (ImplicitBoxTree.hpp:2934-3159): row = source leaf, column =
  * target leaf, value = count (absolute) or count / P; row-major, columns ascending;
- * lost points dropped, or sent to column n+1 with nColumns = n+1 (invalid)
+ * lost points dropped, or sent to column n+1 with nColumns = n+1 (invalid, and only
+ * when some point was lost: nColumns stays n otherwise)
  * ---------------------------------------------------------------------------- */
 static int cmp_u32(const void* a, const void* b)
 {
@@ -530,15 +531,15 @@ static int cmp_u32(const void* a, const void* b)
   return x < y ? -1 : (x > y);
 }
 
-uint64_t orc_transition_matrix(const orc_tree* t, const orc_map* m, const orc_grid* g, int absolute, int invalid,
-                               uint32_t* rowptr, uint32_t* cols, double* vals, uint32_t* n_cols)
+/* the run-length step of transitionMatrixForLeaves for n_rows rows of P targets each
+ * (columns < n_cols, ORC_INVALID for a lost point); tgt is sorted row by row in place */
+uint64_t orc_transition_rows(uint32_t* tgt, uint64_t n, uint64_t P, uint32_t n_cols, int absolute, int invalid,
+                             uint32_t* rowptr, uint32_t* cols, double* vals, uint32_t* out_n_cols)
 {
-  const uint64_t n = t->n, P = points_per_box(g, t->dom.dim);
-  uint32_t* src = (uint32_t*)malloc(n * 4);
-  for (uint64_t i = 0; i < n; ++i) src[i] = (uint32_t)i;
-  uint32_t* tgt = (uint32_t*)malloc(n * P * 4);
-  orc_search_by_image(t, m, g, src, n, tgt);
-  const uint32_t nc = invalid ? (uint32_t)n + 1 : (uint32_t)n;
+  /* the lost column exists only when some point was lost (ImplicitBoxTree.hpp:3075-3090) */
+  int lost = 0;
+  for (uint64_t i = 0; i < n * P && !lost; ++i) lost = tgt[i] == ORC_INVALID;
+  const uint32_t nc = invalid && lost ? n_cols + 1 : n_cols;
   uint64_t nnz = 0;
   if (rowptr) rowptr[0] = 0;
   for (uint64_t r = 0; r < n; ++r) {
@@ -559,9 +560,67 @@ uint64_t orc_transition_matrix(const orc_tree* t, const orc_map* m, const orc_gr
     }
     if (rowptr) rowptr[r + 1] = (uint32_t)nnz;
   }
-  if (n_cols) *n_cols = nc;
+  if (out_n_cols) *out_n_cols = nc;
+  return nnz;
+}
+
+uint64_t orc_transition_matrix(const orc_tree* t, const orc_map* m, const orc_grid* g, int absolute, int invalid,
+                               uint32_t* rowptr, uint32_t* cols, double* vals, uint32_t* n_cols)
+{
+  const uint64_t n = t->n, P = points_per_box(g, t->dom.dim);
+  uint32_t* src = (uint32_t*)malloc(n * 4);
+  for (uint64_t i = 0; i < n; ++i) src[i] = (uint32_t)i;
+  uint32_t* tgt = (uint32_t*)malloc(n * P * 4);
+  orc_search_by_image(t, m, g, src, n, tgt);
+  const uint64_t nnz = orc_transition_rows(tgt, n, P, (uint32_t)n, absolute, invalid, rowptr, cols, vals, n_cols);
   free(tgt); free(src);
   return nnz;
+}
+
+/* ------------------------------------------------------------------------------
+ * point boxes of a range-partitioned tree: the steps above restricted to given point
+ * boxes (depth-64 codes with a validity byte)
+ * ---------------------------------------------------------------------------- */
+/* GridPointsFunctor + PointToBox of every leaf (ImplicitBoxTree.hpp:2624-2681), leaf-major */
+void orc_image_point_boxes(const orc_tree* t, const orc_map* m, const orc_grid* g, uint64_t* codes, uint8_t* valid)
+{
+  const uint64_t n = t->n, P = points_per_box(g, t->dom.dim);
+  const uint32_t D = t->dom.dim;
+  const int64_t total = (int64_t)(n * P);
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < total; ++i) {
+    const uint64_t b = (uint64_t)i / P;
+    double c[ORC_MAX_DIM], r[ORC_MAX_DIM], gp[ORC_MAX_DIM], y[ORC_MAX_DIM];
+    orc_box_coordinates(&t->dom, t->code[b], t->depth[b], c, r);
+    orc_grid_point(g, D, (uint64_t)i, gp);
+    for (uint32_t j = 0; j < D; ++j) c[j] += gp[j] * r[j];
+    orc_map_apply(m, c, y);
+    valid[i] = (uint8_t)orc_point_code64(&t->dom, y, codes + i);
+  }
+}
+
+/* searchByIterators over point boxes (ImplicitBoxTree.hpp:2394-2432) */
+void orc_search_point_boxes(const orc_tree* t, const uint64_t* codes, const uint8_t* valid, uint64_t n,
+                            uint32_t* out)
+{
+  for (uint64_t i = 0; i < n; ++i) out[i] = orc_search(t, codes[i], valid[i]);
+}
+
+/* setFlagsByIterators over point boxes (ImplicitBoxTree.hpp:2167-2196); returns the
+ * leaves whose flags changed */
+uint32_t orc_set_flags_by_point_boxes(orc_tree* t, const uint64_t* codes, const uint8_t* valid, uint64_t n,
+                                      uint8_t flags)
+{
+  uint8_t* hit = (uint8_t*)calloc(t->n ? t->n : 1, 1);
+  for (uint64_t i = 0; i < n; ++i) {
+    const uint32_t b = orc_search(t, codes[i], valid[i]);
+    if (b != ORC_INVALID) hit[b] = 1;
+  }
+  uint32_t c = 0;
+  for (uint64_t i = 0; i < t->n; ++i)
+    if (hit[i]) { c += !flags_set(t->flags[i], flags); t->flags[i] |= flags; }
+  free(hit);
+  return c;
 }
 
 /* ------------------------------------------------------------------------------

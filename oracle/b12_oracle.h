@@ -89,6 +89,14 @@ uint32_t orc_subdivide(orc_tree* t, uint8_t flags);
 uint32_t orc_remove(orc_tree* t, uint8_t flags);
 /* search of a depth-64 point box among the leaves; ORC_INVALID if no leaf contains it */
 uint32_t orc_search(const orc_tree* t, uint64_t code64, int valid);
+/* point boxes of a range-partitioned tree */
+void orc_image_point_boxes(const orc_tree* t, const orc_map* m, const orc_grid* g, uint64_t* codes, uint8_t* valid);
+void orc_search_point_boxes(const orc_tree* t, const uint64_t* codes, const uint8_t* valid, uint64_t n,
+                            uint32_t* out);
+uint32_t orc_set_flags_by_point_boxes(orc_tree* t, const uint64_t* codes, const uint8_t* valid, uint64_t n,
+                                      uint8_t flags);
+uint64_t orc_transition_rows(uint32_t* tgt, uint64_t n, uint64_t P, uint32_t n_cols, int absolute, int invalid,
+                             uint32_t* rowptr, uint32_t* cols, double* vals, uint32_t* out_n_cols);
 /* per-point target leaf index of the image of grid point i of source leaf src[k] */
 void orc_search_by_image(const orc_tree* t, const orc_map* m, const orc_grid* g,
                          const uint32_t* src, uint64_t n_src, uint32_t* out);

@@ -91,6 +91,10 @@ def lib():
             "orc_transition_matrix": (u64, [P(OrcTree), P(OrcMap), P(OrcGrid), C.c_int, C.c_int,
                                             P(u32), P(u32), P(dbl), P(u32)]),
             "orc_invariant_measure": (None, [u32, P(u32), P(u32), P(dbl), u32, P(dbl)]),
+            "orc_image_point_boxes": (None, [P(OrcTree), P(OrcMap), P(OrcGrid), P(u64), P(u8)]),
+            "orc_search_point_boxes": (None, [P(OrcTree), P(u64), P(u8), u64, P(u32)]),
+            "orc_set_flags_by_point_boxes": (u32, [P(OrcTree), P(u64), P(u8), u64, u8]),
+            "orc_transition_rows": (u64, [P(u32), u64, u64, u32, C.c_int, C.c_int, P(u32), P(u32), P(dbl), P(u32)]),
             "orc_subdivision": (u64, [P(OrcTree), P(OrcMap), P(OrcGrid), u32, P(u32)]),
             "orc_num_threads": (C.c_int, []),
         }
@@ -302,6 +306,46 @@ class Oracle:
         self.L.orc_transition_matrix(t, m, g, int(absolute), int(invalid), _ptr(rowptr, C.c_uint32),
                                      _ptr(cols, C.c_uint32), _ptr(vals, C.c_double), C.byref(ncols))
         return rowptr, cols[:nnz], vals[:nnz], int(ncols.value)
+
+    # -- point boxes of a range-partitioned tree
+    def image_point_boxes(self):
+        """the point boxes (depth-64 codes, validity) of the images of every leaf, leaf-major"""
+        total = self.n * self.points_per_box()
+        codes = np.zeros(max(total, 1), dtype=np.uint64)
+        valid = np.zeros(max(total, 1), dtype=np.uint8)
+        self.L.orc_image_point_boxes(C.byref(self.tree), C.byref(self.map), C.byref(self.grid),
+                                     _ptr(codes, C.c_uint64), _ptr(valid, C.c_uint8))
+        return codes[:total], valid[:total]
+
+    def search_point_boxes(self, codes, valid):
+        codes = np.ascontiguousarray(codes, dtype=np.uint64)
+        valid = np.ascontiguousarray(valid, dtype=np.uint8)
+        out = np.zeros(max(len(codes), 1), dtype=np.uint32)
+        self.L.orc_search_point_boxes(C.byref(self.tree), _ptr(codes, C.c_uint64), _ptr(valid, C.c_uint8),
+                                      len(codes), _ptr(out, C.c_uint32))
+        return out[:len(codes)]
+
+    def set_flags_by_point_boxes(self, codes, valid, flags):
+        codes = np.ascontiguousarray(codes, dtype=np.uint64)
+        valid = np.ascontiguousarray(valid, dtype=np.uint8)
+        return self.L.orc_set_flags_by_point_boxes(C.byref(self.tree), _ptr(codes, C.c_uint64),
+                                                   _ptr(valid, C.c_uint8), len(codes), flags)
+
+    @staticmethod
+    def transition_rows(targets, P, n_cols, absolute=False, invalid=False):
+        """(rowptr, cols, vals, n_cols) of rows of P targets each (ORC_INVALID: lost)"""
+        tgt = np.array(targets, dtype=np.uint32).reshape(-1)
+        n = len(tgt) // P
+        L = lib()
+        nnz = L.orc_transition_rows(_ptr(tgt.copy(), C.c_uint32), n, P, n_cols, int(absolute), int(invalid),
+                                    None, None, None, None)
+        rowptr = np.zeros(n + 1, dtype=np.uint32)
+        cols = np.zeros(max(nnz, 1), dtype=np.uint32)
+        vals = np.zeros(max(nnz, 1), dtype=np.float64)
+        nc = C.c_uint32()
+        L.orc_transition_rows(_ptr(tgt, C.c_uint32), n, P, n_cols, int(absolute), int(invalid),
+                              _ptr(rowptr, C.c_uint32), _ptr(cols, C.c_uint32), _ptr(vals, C.c_double), C.byref(nc))
+        return rowptr, cols[:nnz], vals[:nnz], int(nc.value)
 
     # -- geometry
     def point_code64(self, p):

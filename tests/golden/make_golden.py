@@ -29,6 +29,8 @@ WORKLOADS = {
     "henon_d20": ("ref_henon", ["--steps", "20", "--tm", "1"], dict(map="henon", a=1.4, b=0.3, grid=4, steps=20)),
     "henon_d12_abs": ("ref_henon", ["--steps", "12", "--tm", "2"],
                       dict(map="henon", a=1.4, b=0.3, grid=4, steps=12, absolute=True)),
+    "lorenz_rho15_d4_invalid_column_unused": ("ref_lorenz", ["--steps", "4", "--tm", "3", "--rho", "15"],
+                                               dict(map="lorenz", rho=15.0, grid=5, steps=4, invalid=True)),
     "henon_d12_lost": ("ref_henon", ["--steps", "12", "--tm", "3", "--grid", "6"],
                        dict(map="henon", a=1.4, b=0.3, grid=6, steps=12, invalid=True)),
     "henon_a1.0_d16": ("ref_henon", ["--steps", "16", "--tm", "1", "--a", "1.0"],

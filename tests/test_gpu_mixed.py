@@ -403,3 +403,49 @@ def test_insertion_of_images_of_inner_boxes_matches_oracle(golden, src_depth, de
     assert got == o.insert_by_image_src(src_depth, 8, depth, 2, 1)
     for x, y in zip(t.leaves(), o.leaves()):
         np.testing.assert_array_equal(x, y)
+
+
+def comparable(code, depth):
+    """getComparableBitPattern (Box.hpp:67-73) of a depth <= 64 box"""
+    s = 64 - depth
+    high = (code << s) & ((1 << 64) - 1) if s < 64 else 0
+    return high | (((1 << (s - 1)) - 1) if s >= 2 else 0)
+
+
+def deepest_leaves(o, points, depths):
+    """leaves around the given points at the given depths (<= 64), in tree order"""
+    boxes = []
+    for p, d in zip(points, depths):
+        c, ok = o.point_code64(np.asarray(p, dtype=np.float64))
+        assert ok
+        boxes.append((c >> (64 - d) if d < 64 else c, d))
+    boxes.sort(key=lambda b: (comparable(*b), -b[1]))
+    codes = np.array([b[0] for b in boxes], dtype=np.uint64)
+    depth = np.array([b[1] for b in boxes], dtype=np.uint8)
+    return codes, depth
+
+
+def test_leaves_at_the_maximal_depth():
+    """Depth-64 leaves stay whole under subdivide (which still counts them), and a point
+    inside one at the leaf depth is not inserted but flags it as hit."""
+    o = O.Oracle(O.henon_spec())
+    codes, depth = deepest_leaves(o, [(-1.0, 0.1), (0.5, -0.2), (1.2, 0.3)], [64, 63, 64])
+    flags = np.full(len(codes), 8, dtype=np.uint8)
+    t = B.ImplicitBoxTree([0.0, 0.0], [1.5, 0.45])
+    t.load_leaves(codes, depth, flags)
+    o.load(codes, depth, flags)
+    assert t.subdivide(B.SD) == o.subdivide(8) == 3
+    for x, y in zip(t.leaves(), o.leaves()):
+        np.testing.assert_array_equal(x, y)
+    assert t.count() == 4 and t.depth() == 64
+    # one point inside the first depth-64 leaf, one elsewhere
+    pts = np.array([[-1.0, 0.1], [0.0, 0.0]])
+    assert t.insert_points(pts, 255, B.INS, B.HIT) == o.insert_points_general(pts, 255, 2, 1)
+    for x, y in zip(t.leaves(), o.leaves()):
+        np.testing.assert_array_equal(x, y)
+    # a uniform tree at depth 64: subdivide counts the flagged leaves and splits none
+    u_codes, u_depth = deepest_leaves(o, [(-1.0, 0.1), (1.2, 0.3)], [64, 64])
+    t.load_leaves(u_codes, u_depth, np.full(2, 8, dtype=np.uint8))
+    assert t.subdivide(B.SD) == 2
+    np.testing.assert_array_equal(t.leaves()[0], u_codes)
+    assert t.depth() == 64

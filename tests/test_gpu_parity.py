@@ -107,7 +107,8 @@ def test_fused_and_step_api_agree():
 # ------------------------------------------------------------------ transition matrix
 @pytest.mark.parametrize("name,absolute,invalid", [
     ("henon_d20", False, False), ("henon_d12_abs", True, False), ("henon_d12_lost", False, True),
-    ("lorenz_d15", False, False), ("forced_duffing_d16", False, False), ("lorenz_rho15_d18", False, False)])
+    ("lorenz_d15", False, False), ("forced_duffing_d16", False, False), ("lorenz_rho15_d18", False, False),
+    ("lorenz_rho15_d4_invalid_column_unused", False, True)])
 def test_transition_matrix_matches_reference(golden, name, absolute, invalid):
     meta, arrays = golden(name)
     spec = meta["spec"]

@@ -1,0 +1,177 @@
+"""GPU: the entry points of a range-partitioned tree through the C ABI against the oracle,
+and the partitioned subdivision and transition matrix (ranks emulated in one process on
+one GPU, their collectives answered on the host between launches) against one tree.
+
+Point boxes, leaf indices, flags, rows, leaf counts and matrices must be bit-exact."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from workloads import domain, oracle_spec, scheme, sha
+
+pytestmark = pytest.mark.gpu
+
+B = pytest.importorskip("b12_b200")
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _device():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+def _tree(spec):
+    c, r = domain(spec)
+    return B.ImplicitBoxTree(c, r)
+
+
+def _grown(name, golden, steps=None):
+    meta, _ = golden(name)
+    spec = meta["spec"]
+    t = _tree(spec)
+    sc = scheme(spec)
+    k = len(meta["steps"]) if steps is None else steps
+    t.subdivision_run(sc, k)
+    o = O.Oracle(oracle_spec(spec))
+    o.load(*t.leaves())
+    return meta, spec, t, sc, o
+
+
+@pytest.mark.parametrize("name", ["henon_d12_lost", "lorenz_d15"])
+def test_point_box_entries_match_oracle(golden, name):
+    import torch
+    _, spec, t, sc, o = _grown(name, golden)
+    codes, valid = t.image_point_boxes(sc, "cuda")
+    oc, ov = o.image_point_boxes()
+    np.testing.assert_array_equal(codes.cpu().numpy().view(np.uint64), oc)
+    np.testing.assert_array_equal(valid.cpu().numpy(), ov)
+    assert (ov == 0).any() or name == "lorenz_d15"
+    # search and flags over the same point boxes
+    idx = t.search_point_boxes(codes, valid).cpu().numpy()
+    want = o.search_point_boxes(oc, ov).astype(np.int64)
+    want[want == 0xFFFFFFFF] = -1
+    np.testing.assert_array_equal(idx, want)
+    half = codes.numel() // 2
+    assert t.set_flags_by_point_boxes(codes[:half], valid[:half], B.EQU) == \
+        o.set_flags_by_point_boxes(oc[:half], ov[:half], 0x10)
+    for x, y in zip(t.leaves(), o.leaves()):
+        np.testing.assert_array_equal(x, y)
+    # rows from the targets equal the tree's own matrix
+    P = sc.grid.points_per_box(t.dim)
+    for invalid in (False, True):
+        m = t.transition_rows(torch.from_numpy(want).cuda(), P, t.count(), False, invalid)
+        ref = t.transition_matrix(sc, invalid_column=invalid)
+        for x, y in zip(m.to_host(), ref.to_host()):
+            np.testing.assert_array_equal(x, y)
+        assert m.n_cols == ref.n_cols
+        m.close()
+        ref.close()
+
+
+def test_point_boxes_of_a_tree_of_several_depths(golden):
+    meta, arrays = golden("henon_d14_mixed8")
+    spec = meta["spec"]
+    t = _tree(spec)
+    t.load_leaves(arrays["mixed_codes_00"], arrays["mixed_depth_00"], arrays["mixed_flags_00"])
+    t.subdivide(B.SD)
+    o = O.Oracle(oracle_spec(spec))
+    o.load(*t.leaves())
+    assert len(set(t.leaves()[1].tolist())) == 2
+    sc = scheme(spec)
+    codes, valid = t.image_point_boxes(sc, "cuda")
+    oc, ov = o.image_point_boxes()
+    np.testing.assert_array_equal(codes.cpu().numpy().view(np.uint64), oc)
+    idx = t.search_point_boxes(codes, valid).cpu().numpy()
+    want = o.search_point_boxes(oc, ov).astype(np.int64)
+    want[want == 0xFFFFFFFF] = -1
+    np.testing.assert_array_equal(idx, want)
+    assert len(set(t.leaves()[1].tolist())) == 2      # still a tree of two depths
+
+
+def test_leaves_through_device_buffers(golden):
+    import torch
+    _, spec, t, sc, o = _grown("henon_d12_lost", golden)
+    c, d, f = t.leaves_device("cuda")
+    u = _tree(spec)
+    u.load_leaves_device(c, d, f)
+    for x, y in zip(u.leaves(), t.leaves()):
+        np.testing.assert_array_equal(x, y)
+    # out of order: refused on the device, the tree is its surrounding box
+    with pytest.raises(B.B12gError):
+        u.load_leaves_device(torch.flip(c, [0]).contiguous(), d, f)
+    assert u.count() == 1 and u.depth() == 0
+    # a run of two depths keeps them
+    codes, depth, flags = t.leaves()
+    depth = depth.copy()
+    codes = codes.copy()
+    codes[0] >>= np.uint64(1)
+    depth[0] -= 1
+    ok = codes[0] != codes[1] >> np.uint64(1)
+    if ok:
+        u.load_leaves_device(torch.from_numpy(codes.view(np.int64)).cuda(), torch.from_numpy(depth).cuda(),
+                             torch.from_numpy(flags).cuda())
+        for x, y in zip(u.leaves(), (codes, depth, flags)):
+            np.testing.assert_array_equal(x, y)
+
+
+def _partitioned(spec, world, leaves=None):
+    from b12_b200.partition import DeviceRun, PartitionedTree, split_leaves
+    if leaves is None:
+        leaves = (np.zeros(1, np.uint64), np.zeros(1, np.uint8), np.zeros(1, np.uint8))
+    runs = []
+    for part in split_leaves(*leaves, world):
+        r = DeviceRun(_tree(spec), "cuda")
+        if len(part[0]):
+            r.tree.load_leaves(*part)
+        else:
+            r.empty = True
+        runs.append(r)
+    return runs, [PartitionedTree(r, i, world) for i, r in enumerate(runs)]
+
+
+def _concat(runs):
+    parts = [r.host_leaves() for r in runs]
+    return tuple(np.concatenate([p[k] for p in parts]) for k in range(3))
+
+
+@pytest.mark.parametrize("name,world", [("henon_d20", 2), ("lorenz_d15", 3), ("forced_duffing_d16", 4)])
+def test_partitioned_subdivision_matches_reference(golden, name, world):
+    from b12_b200.partition import drive_lockstep
+    meta, _ = golden(name)
+    spec = meta["spec"]
+    steps = len(meta["steps"])
+    runs, trees = _partitioned(spec, world)
+    counts = drive_lockstep([t.subdivision(scheme(spec), steps) for t in trees])
+    assert counts[0] == [s["n"] for s in meta["steps"]]
+    codes, depth, flags = _concat(runs)
+    assert sha(codes) == meta["steps"][-1]["codes_sha256"]
+    assert sha(flags) == meta["steps"][-1]["flags_sha256"]
+    assert max(r.n for r in runs) <= 1.05 * len(codes) / world + 1
+
+
+@pytest.mark.parametrize("name,absolute,invalid", [
+    ("henon_d20", False, False), ("henon_d12_lost", False, True), ("lorenz_d15", False, False),
+    ("lorenz_rho15_d4_invalid_column_unused", False, True)])
+def test_partitioned_transition_matrix_matches_reference(golden, name, absolute, invalid):
+    from b12_b200.partition import drive_lockstep
+    from workloads import csr_digests
+    meta, _ = golden(name)
+    spec = meta["spec"]
+    t = _tree(spec)
+    t.subdivision_run(scheme(spec), len(meta["steps"]))
+    for world in (2, 3):
+        runs, trees = _partitioned(spec, world, t.leaves())
+        blocks = drive_lockstep([p.transition_matrix(scheme(spec), absolute, invalid) for p in trees])
+        rowptr, cols, vals, base = [np.zeros(1, np.uint64)], [], [], 0
+        for b in blocks:
+            rp, c, v = b.rows.to_host()
+            rowptr.append(rp[1:].astype(np.uint64) + base)
+            base += int(rp[-1])
+            cols.append(c)
+            vals.append(v)
+            b.rows.close()
+        d = csr_digests(np.concatenate(rowptr).astype(np.uint32), np.concatenate(cols), np.concatenate(vals))
+        for k in ("nnz", "rowptr_sha256", "cols_sha256", "vals_sha256"):
+            assert d[k] == meta["tm"][k], k
+        assert blocks[0].n_cols == meta["tm"]["n_cols"]

@@ -31,7 +31,8 @@ def test_subdivision_matches_reference(golden, name):
 
 @pytest.mark.parametrize("name,absolute,invalid", [
     ("henon_d20", False, False), ("henon_d12_abs", True, False), ("henon_d12_lost", False, True),
-    ("lorenz_d15", False, False), ("forced_duffing_d16", False, False)])
+    ("lorenz_d15", False, False), ("forced_duffing_d16", False, False),
+    ("lorenz_rho15_d4_invalid_column_unused", False, True)])
 def test_transition_matrix_matches_reference(golden, name, absolute, invalid):
     meta, arrays = golden(name)
     o = O.Oracle(oracle_spec(meta["spec"]))
