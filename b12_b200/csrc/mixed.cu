@@ -754,8 +754,9 @@ __global__ void __launch_bounds__(kThreads) mixed_image_kernel(const MixedArgs a
     const uint32_t leaf = a.src ? __ldg(a.src + rank) : uint32_t(rank);
     if constexpr (kMode == 2) {
       uint64_t p64;
-      a.valid_out[g] = image_code<Map, Grid>(a, pts, table, leaf, k, g, p64) ? 1 : 0;
-      a.p64_out[g] = p64;
+      const bool valid = image_code<Map, Grid>(a, pts, table, leaf, k, g, p64);
+      a.valid_out[g] = valid ? 1 : 0;
+      a.p64_out[g] = valid ? p64 : ~0ull;   // the invalid box (~0, 255) of PointToBox
     } else if constexpr (kMode >= 3) {
       uint64_t p64;
       const bool valid = image_code<Map, Grid>(a, pts, table, leaf, k, g, p64);
@@ -913,6 +914,7 @@ b12g_status refresh_comparable(b12g_tree* t)
 {
   ST(t->cmp.ensure(std::max<uint32_t>(t->n, 1), "comparable patterns"));
   comparable_kernel<<<grid_for_n(t->n), kThreads, 0, t->stream>>>(t->codes(), dep_cur(t), t->n, t->cmp.p);
+  LAUNCHED("comparable patterns");
   // about two table entries per leaf, 4 .. 22 bits
   uint32_t bits = 4;
   while (bits < 22 && (1ull << bits) < 2ull * t->n) ++bits;
@@ -920,6 +922,7 @@ b12g_status refresh_comparable(b12g_tree* t)
   ST(t->cmp_tab.ensure((size_t(1) << bits) + 1, "pattern prefix table"));
   cmp_table_kernel<<<grid_for_n((uint64_t(1) << bits) + 1), kThreads, 0, t->stream>>>(t->cmp.p, t->n, bits,
                                                                                        t->cmp_tab.p);
+  LAUNCHED("pattern prefix table");
   count_launches(2);
   return B12G_OK;
 }
@@ -1019,6 +1022,7 @@ b12g_status mixed_settle(b12g_tree* t)
   ST(set_ctr(t, C_TMP, 255));
   ST(set_ctr(t, C_TMP + 1, 0));
   depth_range_kernel<<<grid_for_n(t->n), kThreads, 0, t->stream>>>(dep_cur(t), t->n, t->ctr.p + C_TMP);
+  LAUNCHED("depth range");
   count_launches(1);
   ST(read_ctr(t, C_TMP, 2));
   if (t->h_ctr[C_TMP] == t->h_ctr[C_TMP + 1]) {
@@ -1536,6 +1540,7 @@ b12g_status mixed_point_box_search(b12g_tree* t, const uint64_t* codes, const ui
     ST(set_ctr(t, C_CHANGED, 0));
     apply_hits_kernel<<<grid_for_n(t->n), kThreads, 0, t->stream>>>(t->flg(), t->hit.p, t->n, flags,
                                                                      t->ctr.p + C_CHANGED);
+    LAUNCHED("apply hits");
     count_launches(1);
     ST(read_ctr(t, C_CHANGED, 1));
     if (n_changed) *n_changed = t->h_ctr[C_CHANGED];

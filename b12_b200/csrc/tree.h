@@ -20,6 +20,13 @@ b12g_status cuda_fail(cudaError_t e, const char* where);
     if (e_ != cudaSuccess) return ::b12g::host::cuda_fail(e_, #call); \
   } while (0)
 
+// the launch just queued (or an earlier one) failed: report it with `where`
+#define LAUNCHED(where)                                            \
+  do {                                                             \
+    cudaError_t e_ = cudaGetLastError();                           \
+    if (e_ != cudaSuccess) return ::b12g::host::cuda_fail(e_, where); \
+  } while (0)
+
 #define ST(call)                                                   \
   do {                                                             \
     b12g_status s_ = (call);                                       \
@@ -58,9 +65,12 @@ struct Buf {
     b12g_status st = ensure(count, what);
     if (st != B12G_OK) { p = old; n = oldn; return st; }
     if (old) {
-      if (keep) cudaMemcpyAsync(p, old, keep * sizeof(T), cudaMemcpyDeviceToDevice, s);
-      cudaStreamSynchronize(s);
+      // the old buffer holds oldn elements, whatever the caller counts as kept
+      keep = std::min(keep, oldn);
+      cudaError_t e = keep ? cudaMemcpyAsync(p, old, keep * sizeof(T), cudaMemcpyDeviceToDevice, s) : cudaSuccess;
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
       cudaFree(old);
+      if (e != cudaSuccess) return ::b12g::host::cuda_fail(e, what);
     }
     return B12G_OK;
   }
