@@ -38,7 +38,7 @@ __global__ void value_present_kernel(const uint32_t* __restrict__ v, uint64_t n,
 
 // a warp per row: the row's P <= 128 targets (column indices, or B12G_INVALID_INDEX for
 // points that left the domain) sorted and run-length counted, as for a whole tree
-__global__ void __launch_bounds__(kThreads) target_rows_kernel(const uint32_t* __restrict__ targets, uint32_t n,
+__global__ void __launch_bounds__(kThreads) partition_rows_kernel(const uint32_t* __restrict__ targets, uint32_t n,
                                                                uint32_t P, int keep_lost, uint32_t lost_col,
                                                                uint32_t* stage_col, uint32_t* stage_cnt,
                                                                uint32_t* row_count)
@@ -116,7 +116,7 @@ b12g_status b12g_transition_rows(b12g_tree* t, const uint32_t* targets, uint32_t
   ST(t->stage_cnt.ensure(stage, "row staging"));
   ST(t->row_count.ensure(uint64_t(n) + 1, "row counts"));
   ST(t->rowptr.ensure(uint64_t(n) + 1, "row pointers"));
-  target_rows_kernel<<<grid_for(n, kThreads / 32), kThreads, 0, t->stream>>>(
+  partition_rows_kernel<<<grid_for(n, kThreads / 32), kThreads, 0, t->stream>>>(
       targets, n, P, invalid_column ? 1 : 0, n_columns + 1, t->stage_col.p, t->stage_cnt.p, t->row_count.p);
   CK(cudaGetLastError());
   count_launches(1);
