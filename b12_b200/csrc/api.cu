@@ -89,6 +89,28 @@ b12g_status reserve(b12g_tree* t, uint64_t n_boxes)
   return B12G_OK;
 }
 
+// order-sensitive 64-bit checksum of the leaf codes
+b12g_status leaf_sum(b12g_tree* t, unsigned long long* sum)
+{
+  ST(t->csum.ensure(1, "checksum"));
+  CK(cudaMemsetAsync(t->csum.p, 0, sizeof(unsigned long long), t->stream));
+  CK(leaf_checksum(t->codes(), t->n, t->csum.p, t->stream));
+  count_launches(1);
+  CK(cudaMemcpyAsync(sum, t->csum.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, t->stream));
+  return sync(t, "checksum");
+}
+
+// the stored targets of the last subdivision step describe the current leaves under
+// this scheme: same scheme bytes, same leaf count and depth, same codes (checksum)
+bool stored_rows_fit(b12g_tree* t, const b12g_scheme* sc, const Prepared& pr)
+{
+  if (!t->tgt_ok || t->mixed || t->n != t->tgt_n || t->depth != t->tgt_depth || pr.P != t->tgt_points) return false;
+  if (std::memcmp(sc, &t->tgt_scheme, sizeof(b12g_scheme)) != 0) return false;
+  unsigned long long sum = 0;
+  if (leaf_sum(t, &sum) != B12G_OK) return false;
+  return sum == t->tgt_sum;
+}
+
 b12g_status prepare(b12g_tree* t, const b12g_scheme* sc, Prepared& pr)
 {
   if (!sc) return fail(B12G_ERR_INVALID, "scheme is NULL");
@@ -385,6 +407,7 @@ b12g_status b12g_tree_destroy(b12g_tree* t)
   t->src.release(); t->out.release(); t->stage_col.release(); t->stage_cnt.release();
   t->row_count.release(); t->rowptr.release(); t->cand.release(); t->cand2.release();
   t->sort_idx.release(); t->table.release(); t->step_counts.release(); t->sort_tmp.release();
+  t->last_tgt.release(); t->last_rank.release(); t->csum.release();
   if (t->h_ctr) cudaFreeHost(t->h_ctr);
   if (t->stream) cudaStreamDestroy(t->stream);
   delete t;
@@ -647,6 +670,22 @@ b12g_status b12g_transition_matrix(b12g_tree* t, const b12g_scheme* sc, int abso
     prof_mark(t, 1);
     ST(mixed_rows(t, sc, invalid_column));
     prof_mark(t, 1);
+  } else if (stored_rows_fit(t, sc, pr)) {
+    // the targets the last subdivision step stored, for these very leaves and scheme
+    StoredRowArgs ra{};
+    ra.targets = t->last_tgt.p;
+    ra.rank = t->last_rank.p;
+    ra.codes = t->codes();
+    ra.n_children = t->tgt_children;
+    ra.n_leaves = n;
+    ra.points = uint32_t(pr.P);
+    ra.stage_col = t->stage_col.p;
+    ra.stage_cnt = t->stage_cnt.p;
+    ra.row_count = t->row_count.p;
+    ra.keep_lost = invalid_column ? 1 : 0;
+    prof_mark(t, 1);
+    CK(launch_stored_rows(ra, t->stream));
+    prof_mark(t, 1);
   } else {
     ST(build_current_hash(t, pr));
     RowArgs ra{};
@@ -871,18 +910,33 @@ b12g_status b12g_subdivision_run(b12g_tree* t, const b12g_scheme* sc, uint32_t s
   ST(t->step_counts.ensure(steps + 1, "step counts"));
 
   uint64_t cap = std::max<uint64_t>(t->code[0].n, std::max<uint64_t>(4ull * n0, 1ull << 16));
+  t->tgt_ok = false;
   for (int attempt = 0; attempt < 12; ++attempt) {
     ST(reserve(t, cap));
     const bool use_hash = int(d0) + int(steps) - 1 <= kHashMaxDepth;
     if (use_hash) ST(ensure_hash(t, cap));
     Prepared pr;
     ST(prepare(t, sc, pr));
+    // The last step keeps every point's target and the compaction ranks for the
+    // transition matrix of the result.  The buffer is sized by the previous run of this
+    // tree (a tree's first run stores nothing and allocates nothing); a last step with
+    // more points than it holds only marks the stored targets unusable.
+    const uint64_t tgt_entries = t->tgt_want;
+    const bool store = tgt_entries > 0 && pr.P <= kMaxRowPoints && tgt_entries * 4 <= (8ull << 30);
+    if (store) {
+      ST(t->last_tgt.ensure(tgt_entries, "stored targets"));
+      ST(t->last_rank.ensure(2ull * cap + 1, "stored ranks"));
+    }
+    uint32_t* const store_tgt = store ? t->last_tgt.p : nullptr;
+    uint32_t* const store_rank = store ? t->last_rank.p : nullptr;
+    const uint64_t store_cap = store ? t->last_tgt.n : 0;
     // key of the captured graph: every pointer and parameter the launches bake in
-    std::vector<uint8_t> key(sizeof(b12g_scheme) + 64);
+    std::vector<uint8_t> key(sizeof(b12g_scheme) + 80);
     std::memcpy(key.data(), sc, sizeof(b12g_scheme));
-    uint64_t extra[8] = {steps, cap, uint64_t(t->cur) | uint64_t(t->ncur) << 1 | uint64_t(t->profile) << 2, uint64_t(d0),
-                         uint64_t(uintptr_t(t->code[0].p)), uint64_t(uintptr_t(t->hit.p)), uint64_t(uintptr_t(t->table.p)),
-                         uint64_t(uintptr_t(t->code[1].p)) ^ (uint64_t(uintptr_t(t->hash.p)) << 1)};
+    uint64_t extra[10] = {steps, cap, uint64_t(t->cur) | uint64_t(t->ncur) << 1 | uint64_t(t->profile) << 2, uint64_t(d0),
+                          uint64_t(uintptr_t(t->code[0].p)), uint64_t(uintptr_t(t->hit.p)), uint64_t(uintptr_t(t->table.p)),
+                          uint64_t(uintptr_t(t->code[1].p)) ^ (uint64_t(uintptr_t(t->hash.p)) << 1),
+                          uint64_t(uintptr_t(store_tgt)) ^ (store_cap << 1), uint64_t(uintptr_t(store_rank))};
     std::memcpy(key.data() + sizeof(b12g_scheme), extra, sizeof extra);
 
     if (!t->sub_graph || key != t->sub_key) {
@@ -913,6 +967,10 @@ b12g_status b12g_subdivision_run(b12g_tree* t, const b12g_scheme* sc, uint32_t s
         a.depth = int(d0) + int(s) + 1;
         a.children = 1;
         a.hit_cap = uint32_t(std::min<size_t>(t->hit.n, 0xFFFFFFFFu));
+        const bool last = s + 1 == steps;
+        a.targets = last ? store_tgt : nullptr;
+        a.targets_cap = store_cap;
+        a.targets_over = t->ctr.p + C_TGT;
         prof_mark(t, 0);
         err = launch_image(sc->map.kind, sc->map.arith, sc->grid.kind, t->domain.dim, ImageMode::Hit, a,
                            2ull * cap * pr.P, t->stream);
@@ -931,6 +989,7 @@ b12g_status b12g_subdivision_run(b12g_tree* t, const b12g_scheme* sc, uint32_t s
         ca.n_out2 = t->step_counts.p + s;
         ca.out_cap = uint32_t(std::min<size_t>(t->code[o].n, 0xFFFFFFFFu));
         ca.error = t->ctr.p + C_ERROR;
+        ca.out_rank = last ? store_rank : nullptr;
         err = compact(ca, {t->tiles_a.p, t->tiles_b.p}, uint32_t(std::min<uint64_t>(cap, 0xFFFFFFFFu)), t->stream);
         cur = o;
         ncur = no;
@@ -950,12 +1009,14 @@ b12g_status b12g_subdivision_run(b12g_tree* t, const b12g_scheme* sc, uint32_t s
         t->prof_used[k] = 0;
       }
     }
+    ST(set_ctr(t, C_TGT, 0));
     CK(cudaGraphLaunch(t->sub_graph, t->stream));
     count_launches(t->sub_graph_kernels);
     if (use_hash) t->hash_tag = steps;
     std::vector<uint32_t> hc(steps);
     CK(cudaMemcpyAsync(hc.data(), t->step_counts.p, steps * 4, cudaMemcpyDeviceToHost, t->stream));
     CK(cudaMemcpyAsync(t->h_ctr + C_ERROR, t->ctr.p + C_ERROR, 4, cudaMemcpyDeviceToHost, t->stream));
+    CK(cudaMemcpyAsync(t->h_ctr + C_TGT, t->ctr.p + C_TGT, 4, cudaMemcpyDeviceToHost, t->stream));
     ST(sync(t, "subdivision run"));
     if (t->profile)
       for (int k = 0; k < 2; ++k)
@@ -989,6 +1050,17 @@ b12g_status b12g_subdivision_run(b12g_tree* t, const b12g_scheme* sc, uint32_t s
     } else {
       t->n = final_n;
       t->depth = uint8_t(d0 + steps);
+      const uint64_t children = 2ull * (steps >= 2 ? hc[steps - 2] : n0);
+      t->tgt_want = std::max<uint64_t>(t->tgt_want, (children + children / 8 + 1) * pr.P);
+      if (store && t->h_ctr[C_TGT] == 0) {
+        t->tgt_children = uint32_t(children);
+        t->tgt_n = final_n;
+        t->tgt_depth = t->depth;
+        t->tgt_points = uint32_t(pr.P);
+        t->tgt_scheme = *sc;
+        ST(leaf_sum(t, &t->tgt_sum));
+        t->tgt_ok = true;
+      }
     }
     if (counts) std::memcpy(counts, hc.data(), steps * 4);
     return B12G_OK;

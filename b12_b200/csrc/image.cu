@@ -114,6 +114,10 @@ __global__ void __launch_bounds__(kThreads) image_points_kernel(const ImageArgs 
       // one store per distinct target in the warp
       const unsigned peers = __match_any_sync(0xFFFFFFFFu, t);
       if (active && t != kInvalidIndex && lane == __ffs(peers) - 1) a.hit[t] = 1;
+      if (a.targets && active) {
+        if (g < a.targets_cap) a.targets[g] = valid ? t : kOutsideIndex;
+        else *a.targets_over = 1;
+      }
     } else if constexpr (M == ImageMode::Search) {
       if (active) a.out[g] = t;
     } else {
@@ -253,7 +257,73 @@ cudaError_t dispatch(uint32_t map_kind, uint32_t arith, uint32_t grid_kind, uint
   }
 }
 
+// a warp per child of the step that stored the targets: the child is a row when it
+// survived (its rank advances); a target is a column when its child survived, at the
+// child's rank; a point that left the domain is found in a last leaf of code 0
+__global__ void __launch_bounds__(kThreads) stored_rows_kernel(const StoredRowArgs a)
+{
+  __shared__ uint32_t keys[kRowWarps][128];
+  __shared__ uint32_t bounds[kRowWarps][4];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  uint32_t* s = keys[w];
+  const uint32_t P = a.points, n = a.n_leaves;
+  const bool zero_leaf = n > 0 && __ldg(a.codes + n - 1) == 0;
+  for (uint32_t c = blockIdx.x * kRowWarps + w; c < a.n_children; c += gridDim.x * kRowWarps) {
+    const uint32_t row = __ldg(a.rank + c);
+    if (__ldg(a.rank + c + 1) == row) continue;        // removed: no row (warp-uniform)
+#pragma unroll 1
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t k = uint32_t(lane) + 32u * q;
+      uint32_t key = kPadKey;
+      if (k < P) {
+        const uint32_t t = __ldg(a.targets + size_t(c) * P + k);
+        if (t < kOutsideIndex) key = __ldg(a.rank + t + 1) != __ldg(a.rank + t) ? __ldg(a.rank + t) : kLostKey;
+        else key = (t == kOutsideIndex && zero_leaf) ? n - 1 : kLostKey;
+      }
+      s[lane + 32 * q] = key;
+    }
+    const uint32_t total = row_emit(s, bounds[w], lane, P, a.keep_lost, n + 1, a.stage_col + size_t(row) * P,
+                                    a.stage_cnt + size_t(row) * P);
+    if (lane == 0) a.row_count[row] = total;
+    __syncwarp();
+  }
+}
+
+__device__ __forceinline__ uint64_t mix64(uint64_t z)
+{
+  // SplitMix64's finaliser (Steele, Lea, Flood 2014)
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+__global__ void leaf_checksum_kernel(const uint64_t* __restrict__ codes, uint32_t n, unsigned long long* sum)
+{
+  uint64_t acc = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    acc += mix64(__ldg(codes + i) ^ (uint64_t(i) * 0x9E3779B97F4A7C15ull));
+  for (int d = 16; d > 0; d >>= 1) acc += __shfl_down_sync(0xFFFFFFFFu, acc, d);
+  if ((threadIdx.x & 31) == 0 && acc) atomicAdd(sum, (unsigned long long)acc);
+}
+
 }  // namespace
+
+cudaError_t launch_stored_rows(const StoredRowArgs& a, cudaStream_t s)
+{
+  if (a.n_children == 0) return cudaSuccess;
+  const uint64_t want = (uint64_t(a.n_children) + kRowWarps - 1) / kRowWarps;
+  const uint64_t cap = uint64_t(device_sm_count()) * 8;
+  stored_rows_kernel<<<unsigned(want < cap ? want : cap), kThreads, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t leaf_checksum(const uint64_t* codes, uint32_t n, unsigned long long* sum, cudaStream_t s)
+{
+  const uint64_t want = (uint64_t(n) + kThreads * 8 - 1) / (kThreads * 8);
+  const uint64_t cap = uint64_t(device_sm_count()) * 4;
+  leaf_checksum_kernel<<<unsigned(want < 1 ? 1 : (want < cap ? want : cap)), kThreads, 0, s>>>(codes, n, sum);
+  return cudaGetLastError();
+}
 
 bool image_supported(uint32_t map_kind, uint32_t arith, uint32_t grid_kind, uint32_t dim)
 {

@@ -31,6 +31,10 @@ struct ImageArgs {
   // outputs
   uint8_t* hit;
   uint32_t hit_cap;          // entries of `hit`; more boxes than this sets error bit 0
+  uint32_t* targets;         // Hit mode, optional: every point's target box (kInvalidIndex:
+                             // in no box; kOutsideIndex: it left the domain)
+  uint64_t targets_cap;      // entries of `targets`; a point beyond sets *targets_over
+  uint32_t* targets_over;
   uint32_t* out;
   uint64_t* cand;            // insert candidates (depth-d codes)
   uint32_t* cand_count;
@@ -51,6 +55,25 @@ struct RowArgs {
   int keep_lost;             // 1: lost points form a column `lost_col`
   uint32_t lost_col;
 };
+
+// Transition rows from the targets a subdivision step stored (child indices of that
+// step's boxes) and its compaction ranks (rank[c] = survivors before child c, 2n + 1
+// entries): a row per surviving child, a column per surviving target.
+struct StoredRowArgs {
+  const uint32_t* targets;   // children x points
+  const uint32_t* rank;
+  const uint64_t* codes;     // the survivors (the tree's leaves)
+  uint32_t n_children;
+  uint32_t n_leaves;
+  uint32_t points;
+  uint32_t* stage_col;
+  uint32_t* stage_cnt;
+  uint32_t* row_count;
+  int keep_lost;
+};
+cudaError_t launch_stored_rows(const StoredRowArgs& a, cudaStream_t s);
+// 64-bit checksum of n leaf codes (order-sensitive) added into *sum
+cudaError_t leaf_checksum(const uint64_t* codes, uint32_t n, unsigned long long* sum, cudaStream_t s);
 
 // launch helpers (image.cu); return cudaSuccess or the launch error
 cudaError_t launch_image(uint32_t map_kind, uint32_t arith, uint32_t grid_kind, uint32_t dim, ImageMode mode,

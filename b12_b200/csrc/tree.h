@@ -95,6 +95,7 @@ enum : int {
   C_NCOLS = 8,
   C_SYNC = 9,      // 3 words for the grid barrier
   C_NNEW = 12,
+  C_TGT = 13,      // the stored image targets overflowed their buffer
   C_COUNT = 16
 };
 
@@ -149,6 +150,16 @@ struct b12g_tree {
   double prof_ms[2] = {0.0, 0.0};
   uint64_t prof_launches[2] = {0, 0};
   std::vector<cudaEvent_t> graph_prof[2];    // events baked into the captured loop
+  // the last step of the fused loop stores its image targets and compaction ranks; the
+  // transition matrix of the same leaves and scheme is assembled from them
+  Buf<uint32_t> last_tgt, last_rank;
+  Buf<unsigned long long> csum;
+  bool tgt_ok = false;
+  uint64_t tgt_want = 0;       // entries the next run's last step needs (from this run)
+  uint32_t tgt_children = 0, tgt_n = 0, tgt_points = 0;
+  uint8_t tgt_depth = 0;
+  b12g_scheme tgt_scheme{};
+  unsigned long long tgt_sum = 0;
 
   uint64_t* codes() { return code[cur].p; }
   uint8_t* flg() { return flags[cur].p; }
@@ -186,6 +197,8 @@ b12g_status read_ctr(b12g_tree* t, int first, int count);
 b12g_status set_ctr(b12g_tree* t, int slot, uint32_t v);
 b12g_status reserve(b12g_tree* t, uint64_t n_boxes);
 b12g_status prepare(b12g_tree* t, const b12g_scheme* sc, Prepared& pr);
+b12g_status leaf_sum(b12g_tree* t, unsigned long long* sum);
+bool stored_rows_fit(b12g_tree* t, const b12g_scheme* sc, const Prepared& pr);
 b12g_status check_depth(b12g_tree* t, uint8_t depth);
 b12g_status select_sources(b12g_tree* t, const b12g_scheme* sc, Prepared& pr, uint32_t& n_src);
 b12g_status check_error(b12g_tree* t, const char* where);

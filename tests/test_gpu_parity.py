@@ -127,6 +127,52 @@ def test_transition_matrix_matches_reference(golden, name, absolute, invalid):
     assert d["vals_sha256"] == meta["tm"]["vals_sha256"]
 
 
+def test_matrix_from_stored_targets_and_after_changes(golden):
+    """From a tree's second fused run on, the matrix right after subdivision_run is
+    assembled from the targets its last step stored; once the leaves or the scheme differ
+    it is recomputed.  Every matrix must be the oracle's."""
+    meta, _ = golden("henon_d12_lost")
+    spec = meta["spec"]
+    t = make_tree(spec)
+    sc = scheme(spec)
+    t.subdivision_run(sc, len(meta["steps"]))       # first run: nothing stored
+    t.transition_matrix(sc).close()
+    t.delete_depth(0)
+    t.subdivision_run(sc, len(meta["steps"]))       # second run: targets stored
+    o = O.Oracle(oracle_spec(spec))
+
+    def check(m, sc_spec, absolute=False, invalid=False):
+        o = O.Oracle(oracle_spec(sc_spec))
+        o.load(*t.leaves())
+        want = o.transition_matrix(absolute=absolute, invalid=invalid)
+        got = m.to_host()
+        for x, y in zip(got, want[:3]):
+            np.testing.assert_array_equal(x, y)
+        assert m.n_cols == want[3]
+        m.close()
+
+    for absolute, invalid in ((False, False), (True, False), (False, True)):
+        check(t.transition_matrix(sc, absolute=absolute, invalid_column=invalid), spec, absolute, invalid)
+    t.set_flags(B.EQU)                                # flags only: the same leaves
+    check(t.transition_matrix(sc, invalid_column=True), spec, invalid=True)
+    other = dict(spec, grid=3)                        # another scheme over the same leaves
+    check(t.transition_matrix(scheme(other)), other)
+    check(t.transition_matrix(sc), spec)              # and back to the stored one
+    t.subdivide(B.SD)                                 # new leaves
+    check(t.transition_matrix(sc, invalid_column=True), spec, invalid=True)
+    # one step: the stored children are the children of the loaded leaves
+    t2 = make_tree(spec)
+    t2.subdivision_run(sc, 9)
+    codes, depth, flags = t2.leaves()
+    t.load_leaves(codes, depth, flags)
+    t.subdivision_run(sc, 1)
+    o.load(codes, depth, flags)
+    o.subdivision(1)
+    for x, y in zip(t.leaves(), o.leaves()):
+        np.testing.assert_array_equal(x, y)
+    check(t.transition_matrix(sc, invalid_column=True), spec, invalid=True)
+
+
 def test_invariant_measure_against_oracle():
     spec = dict(map="henon", a=1.4, b=0.3, grid=4)
     t = make_tree(spec)
