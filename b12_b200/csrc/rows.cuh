@@ -30,8 +30,8 @@ __device__ __forceinline__ void warp_bitonic_128(uint32_t* s, int lane)
 // The warp's 128 keys are in s (targets, kLostKey for points that left the domain,
 // kPadKey beyond P).  Sorts them, writes the runs to col/cnt (at most P entries) and
 // returns their number.  bounds: 4 words of the warp's shared memory.
-__device__ __forceinline__ uint32_t row_emit(uint32_t* s, uint32_t* bounds, int lane, uint32_t P, int keep_lost,
-                                             uint32_t lost_col, uint32_t* col, uint32_t* cnt)
+__device__ __forceinline__ uint32_t row_emit_sorted(uint32_t* s, uint32_t* bounds, int lane, uint32_t P,
+                                                    int keep_lost, uint32_t lost_col, uint32_t* col, uint32_t* cnt)
 {
     if (lane < 4) bounds[lane] = 0;
     __syncwarp();
@@ -83,6 +83,44 @@ __device__ __forceinline__ uint32_t row_emit(uint32_t* s, uint32_t* bounds, int 
       if (take[r]) { col[off] = cols[r]; cnt[off] = cnts[r]; ++off; }
     __syncwarp();
     return total;
+}
+
+// The same runs, found by taking the warp's smallest remaining key and its count until
+// none is left: a box's points fall into a few boxes (about 6.5 on average for Lorenz at
+// depth 27), so this usually ends after a few rounds.  A row with more than kMinRounds
+// distinct keys sorts the rest with row_emit_sorted.  Same arguments and results.
+constexpr int kMinRounds = 16;
+
+__device__ __forceinline__ uint32_t row_emit(uint32_t* s, uint32_t* bounds, int lane, uint32_t P, int keep_lost,
+                                             uint32_t lost_col, uint32_t* col, uint32_t* cnt)
+{
+  __syncwarp();
+  uint32_t k0 = s[lane], k1 = s[lane + 32], k2 = s[lane + 64], k3 = s[lane + 96];
+  const uint32_t stop = keep_lost ? kPadKey : kLostKey;
+  uint32_t total = 0;
+#pragma unroll 1
+  for (int round = 0; round < kMinRounds; ++round) {
+    const uint32_t m = __reduce_min_sync(0xFFFFFFFFu, min(min(k0, k1), min(k2, k3)));
+    if (m >= stop) return total;
+    const uint32_t c = uint32_t(k0 == m) + uint32_t(k1 == m) + uint32_t(k2 == m) + uint32_t(k3 == m);
+    const uint32_t count = __reduce_add_sync(0xFFFFFFFFu, c);
+    if (lane == 0) {
+      col[total] = m == kLostKey ? lost_col : m;
+      cnt[total] = count;
+    }
+    ++total;
+    k0 = k0 == m ? kPadKey : k0;
+    k1 = k1 == m ? kPadKey : k1;
+    k2 = k2 == m ? kPadKey : k2;
+    k3 = k3 == m ? kPadKey : k3;
+  }
+  // many distinct keys: sort what is left (the keys taken are padding now)
+  s[lane] = k0;
+  s[lane + 32] = k1;
+  s[lane + 64] = k2;
+  s[lane + 96] = k3;
+  __syncwarp();
+  return total + row_emit_sorted(s, bounds, lane, P, keep_lost, lost_col, col + total, cnt + total);
 }
 
 }  // namespace b12g
