@@ -164,28 +164,50 @@ class PartitionedTree:
         return self.table
 
     def _owners(self, codes, valid):
-        """The rank that owns each point box (int64 tensor)."""
+        """The rank that owns each point box (int16 tensor), or an int when one rank owns all."""
         import torch
         n = self.table[:, 0]
         ranks = torch.nonzero(n > 0).flatten()
+        if ranks.numel() == 1:
+            return int(ranks[0])
         starts = self.table[ranks, 1].to(codes.device)
-        ranks = ranks.to(codes.device)
+        ranks = ranks.to(device=codes.device, dtype=torch.int16)
         pos = torch.searchsorted(starts, codes ^ _SIGN, right=True) - 1
         owner = ranks[pos.clamp_(min=0)]
         return torch.where(valid != 0, owner, ranks[-1])
 
     def _route(self, owner, *fields):
+        """Per destination rank, the fields of the point boxes it owns (in their order)."""
         import torch
-        order = torch.argsort(owner, stable=True)
-        splits = torch.bincount(owner, minlength=self.world).tolist()
-        return order, [list(f[order].split(splits)) for f in fields]
+        if isinstance(owner, int):
+            # one rank owns every point box: no permutation
+            empty = [f[:0] for f in fields]
+            parts = [[f if d == owner else e for d in range(self.world)] for f, e in zip(fields, empty)]
+            return None, parts
+        # a stable partition by owner: each point box's slot is its owner's offset plus
+        # the number of earlier point boxes with the same owner
+        splits = torch.bincount(owner.to(torch.int32), minlength=self.world).tolist()
+        slot = torch.empty(owner.shape, dtype=torch.int64, device=owner.device)
+        base = 0
+        for d in range(self.world):
+            if splits[d] == 0:
+                continue
+            mine = owner == d
+            slot = torch.where(mine, torch.cumsum(mine, 0) - 1 + base, slot)
+            base += splits[d]
+        parts = []
+        for f in fields:
+            g = torch.empty_like(f)
+            g[slot] = f
+            parts.append(list(g.split(splits)))
+        return slot, parts
 
     def _exchange_point_boxes(self, codes, valid):
         import torch
-        order, (c_parts, v_parts) = self._route(self._owners(codes, valid), codes, valid)
+        slot, (c_parts, v_parts) = self._route(self._owners(codes, valid), codes, valid)
         rc = yield ("alltoall", c_parts)
         rv = yield ("alltoall", v_parts)
-        return order, [x.numel() for x in rc], torch.cat(rc), torch.cat(rv)
+        return slot, [x.numel() for x in rc], torch.cat(rc), torch.cat(rv)
 
     def _rebalance(self):
         """Even the runs out when the largest exceeds `balance` times the mean and the
@@ -262,12 +284,13 @@ class PartitionedTree:
         total, offset = sum(n), sum(n[: self.rank])
         P = self.run.points_per_box(scheme)
         codes, valid = self.run.image_point_boxes(scheme)
-        order, sizes, rc, rv = yield from self._exchange_point_boxes(codes, valid)
+        slot, sizes, rc, rv = yield from self._exchange_point_boxes(codes, valid)
         idx = self.run.search_point_boxes(rc, rv)
         glob = torch.where(idx >= 0, idx + offset, torch.full_like(idx, -1))
         back = yield ("alltoall", list(glob.split(sizes)))
-        targets = torch.empty_like(codes)
-        targets[order] = torch.cat(back)
+        targets = torch.cat(back)
+        if slot is not None:
+            targets = targets[slot]
         lost = torch.tensor([int(bool((targets < 0).any().item())) if targets.numel() else 0],
                             dtype=torch.int64, device=self.run.device)
         any_lost = bool((yield ("allgather", lost)).sum().item())
