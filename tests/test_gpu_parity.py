@@ -173,6 +173,31 @@ def test_matrix_from_stored_targets_and_after_changes(golden):
     check(t.transition_matrix(sc, invalid_column=True), spec, invalid=True)
 
 
+def test_stored_targets_find_outside_points_in_a_last_leaf_of_code_0():
+    """A run that ends with the single leaf of code 0 while 12 of its 16 image points leave
+    the domain: those points are found in that leaf (hasSamePath of the invalid box), in
+    the recomputed matrix and in the one built from stored targets alike."""
+    a, b, center, radius = 5.8223, -0.912, [1.5308, 0.2375], [1.4846, 0.5467]
+    spec = O.henon_spec(a, b, 4)
+    spec["center"], spec["radius"] = center, radius
+    o = O.Oracle(spec)
+    o.subdivision(2)
+    codes, depth, _ = o.leaves()
+    assert list(codes) == [0] and list(depth) == [2]
+    assert (o.image_point_boxes()[1] == 0).sum() == 12
+    want = o.transition_matrix(invalid=True)
+    t = B.ImplicitBoxTree(center, radius)
+    sc = B.Scheme(B.henon(a, b), B.inner_grid(4))
+    for run in range(2):                       # the second run stores its targets
+        t.delete_depth(0)
+        assert list(t.subdivision_run(sc, 2)) == [1, 1]
+        m = t.transition_matrix(sc, invalid_column=True)
+        for x, y in zip(m.to_host(), want[:3]):
+            np.testing.assert_array_equal(x, y)
+        assert m.n_cols == want[3] == 1
+        m.close()
+
+
 def test_invariant_measure_against_oracle():
     spec = dict(map="henon", a=1.4, b=0.3, grid=4)
     t = make_tree(spec)
