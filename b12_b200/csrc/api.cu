@@ -857,13 +857,15 @@ b12g_status b12g_invariant_measure(b12g_csr* m, uint32_t iters, double* v)
   const int slots = measure_partial_slots();
   ST(m->partial.ensure(slots, "measure"));
   CK(invariant_measure(m->tptr.p, m->trows.p, m->tvals.p, m->mid_list.p, m->n_mid, m->long_list.p, m->n_long, n,
-                       iters, m->w0.p, m->w1.p, m->partial.p, uint32_t(slots), m->vout.p, m->ctr.p + 64, s));
+                       iters, m->w0.p, m->w1.p, m->partial.p, uint32_t(slots), m->vout.p, m->ctr.p + 64, s,
+                       m->nnz));
   count_launches(1);
   if (v) CK(cudaMemcpyAsync(v, m->vout.p, size_t(n) * 8, cudaMemcpyDeviceToHost, s));
   uint32_t err = 0;
   CK(cudaMemcpyAsync(&err, m->ctr.p + 64 + 64, 4, cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   if (err & 2u) return fail(B12G_ERR_TIMEOUT, "invariant measure: grid barrier gave up");
+  if (err & 4u) return fail(B12G_ERR_CAPACITY, "invariant measure: a block's rows exceed its shared memory");
   return B12G_OK;
 }
 

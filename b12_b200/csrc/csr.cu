@@ -262,6 +262,169 @@ __global__ void __launch_bounds__(kMeasureThreads) invariant_measure_kernel(Meas
   for (uint32_t j = tid; j < n; j += nthreads) a.out[j] = a.iters ? __dmul_rn(__ldcg(wl + j), inv) : v0;
 }
 
+// Grid barrier that also reduces, on a counter that only grows: every block publishes its
+// partial sum and arrives; once the counter reaches (round + 1) x blocks every block adds
+// all partials itself, in the same fixed order (lane-strided, then a fixed shuffle tree),
+// so no block waits for a last arriver to publish the total.  Polls are bounded.
+__device__ bool barrier_allsum(const MeasureArgs& a, const double* part, uint32_t round, double* total)
+{
+  __shared__ int ok;
+  __shared__ double bcast;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ok = 1;
+    __threadfence();
+    atomicAdd(a.bar_count, 1u);
+    const unsigned target = (round + 1u) * gridDim.x;
+    volatile unsigned* vc = a.bar_count;
+    unsigned long long polls = 0;
+    while (*vc < target) {
+      if (++polls > kBarrierPolls) { atomicOr(a.error, 2u); ok = 0; break; }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double x = 0.0;
+    for (uint32_t i = threadIdx.x; i < gridDim.x; i += 32) x = __dadd_rn(x, __ldcg(part + i));
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) x = __dadd_rn(x, __shfl_xor_sync(0xFFFFFFFFu, x, d));
+    if (threadIdx.x == 0) bcast = x;
+  }
+  __syncthreads();
+  *total = bcast;
+  return ok && !(*(volatile unsigned*)a.error & 2u);
+}
+
+// The same iteration with the matrix held on chip.  Block b owns the rows of P^T whose
+// first entry lies in [b * per, (b + 1) * per) (per = nnz / blocks, rounded up), keeps
+// their entries (source, value, row) in shared memory for all iterations, and gives each
+// thread a run of at most kSmemChunk consecutive entries: one round of gathers of the
+// previous iterate per iteration, whatever the row lengths.  A row split over several
+// threads is summed by the thread holding its first entry, adding the other threads'
+// parts in thread order, so the result does not depend on scheduling.
+constexpr int kSmemChunk = 13;
+constexpr uint32_t kSmemEntries = uint32_t(kSmemChunk) * kMeasureThreads;
+constexpr size_t kSmemMeasureBytes = size_t(kSmemEntries) * (8 + 4 + 4) + size_t(kMeasureThreads) * (8 + 4);
+
+__device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t* a, uint32_t n, uint32_t x)
+{
+  uint32_t lo = 0, len = n;
+  while (len > 0) {
+    const uint32_t half = len >> 1;
+    if (__ldg(a + lo + half) < x) { lo += half + 1; len -= half + 1; }
+    else len = half;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(kMeasureThreads, 1) invariant_measure_smem_kernel(MeasureArgs a, uint32_t nnz)
+{
+  extern __shared__ __align__(16) unsigned char smem[];
+  double* s_val = reinterpret_cast<double*>(smem);
+  uint32_t* s_src = reinterpret_cast<uint32_t*>(s_val + kSmemEntries);
+  uint32_t* s_row = s_src + kSmemEntries;
+  double* s_head = reinterpret_cast<double*>(s_row + kSmemEntries);
+  uint32_t* s_head_end = reinterpret_cast<uint32_t*>(s_head + kMeasureThreads);
+  __shared__ double red[kMeasureThreads / 32];
+  __shared__ uint32_t s_range[2];
+  const uint32_t n = a.n;
+  const uint32_t t = threadIdx.x, lane = t & 31;
+  const uint32_t per = (nnz + gridDim.x - 1) / gridDim.x;
+  if (t == 0) {
+    // lower bounds over the n + 1 row starts, at most n (a block past the last entry gets no rows)
+    s_range[0] = min(lower_bound_u32(a.tptr, n + 1, blockIdx.x * per), n);
+    s_range[1] = blockIdx.x + 1 == gridDim.x ? n : min(lower_bound_u32(a.tptr, n + 1, (blockIdx.x + 1) * per), n);
+  }
+  __syncthreads();
+  const uint32_t r0 = s_range[0], r1 = max(s_range[0], s_range[1]);
+  const uint32_t e0 = __ldg(a.tptr + r0), e1 = __ldg(a.tptr + r1);
+  uint32_t nloc = e1 - e0;
+  if (nloc > kSmemEntries) {
+    // more entries than the host planned for: flag it and take part in the barriers only
+    if (t == 0) atomicOr(a.error, 4u);
+    nloc = 0;
+  }
+  for (uint32_t k = t; k < nloc; k += blockDim.x) {
+    s_src[k] = __ldg(a.trows + e0 + k);
+    s_val[k] = __ldg(a.tvals + e0 + k);
+  }
+  for (uint32_t r = r0 + t; r < r1; r += blockDim.x) {
+    const uint32_t b = __ldg(a.tptr + r), e = __ldg(a.tptr + r + 1);
+    if (b == e) { a.w0[r] = 0.0; a.w1[r] = 0.0; }   // no entries: 0 in every iterate
+    if (nloc) for (uint32_t k = b; k < e; ++k) s_row[k - e0] = r;
+  }
+  __syncthreads();
+  // this thread's run of entries and whether its first row began in an earlier run
+  const uint32_t chunk = (nloc + blockDim.x - 1) / blockDim.x;
+  const uint32_t k0 = min(t * chunk, nloc), k1 = min(k0 + chunk, nloc);
+  const bool head_open = k0 < k1 && k0 > 0 && s_row[k0 - 1] == s_row[k0];
+  const bool tail_open = k0 < k1 && k1 < nloc && s_row[k1] == s_row[k1 - 1];
+  const double v0 = __ddiv_rn(1.0, double(n));
+  double inv = 1.0;
+  for (uint32_t it = 0; it < a.iters; ++it) {
+    const double* wp = (it & 1u) ? a.w0 : a.w1;
+    double* wc = (it & 1u) ? a.w1 : a.w0;
+    double local = 0.0;
+    double v[kSmemChunk];
+#pragma unroll
+    for (int q = 0; q < kSmemChunk; ++q) {
+      const uint32_t k = k0 + q;
+      v[q] = k < k1 ? iterate_value(wp, s_src[k], it, v0, inv) : 0.0;
+    }
+    // walk the run: a row that ends inside it is written here unless it began earlier
+    uint32_t row = k0 < k1 ? s_row[k0] : 0u;
+    double acc = 0.0, tail = 0.0;
+    bool first = true;
+#pragma unroll
+    for (int q = 0; q < kSmemChunk; ++q) {
+      const uint32_t k = k0 + q;
+      if (k < k1) {
+        const uint32_t r = s_row[k];
+        if (r != row) {
+          if (first && head_open) { s_head[t] = acc; s_head_end[t] = 1u; }
+          else { __stcg(wc + row, acc); local = __dadd_rn(local, fabs(acc)); }
+          first = false;
+          row = r;
+          acc = 0.0;
+        }
+        acc = __fma_rn(s_val[k], v[q], acc);
+      }
+    }
+    if (k0 < k1) {
+      if (first && head_open) { s_head[t] = acc; s_head_end[t] = tail_open ? 0u : 1u; }
+      else if (tail_open) tail = acc;
+      else { __stcg(wc + row, acc); local = __dadd_rn(local, fabs(acc)); }
+    }
+    __syncthreads();
+    if (k0 < k1 && tail_open && !(first && head_open)) {
+      // this run holds the row's first entry: add the later runs' parts in order
+      double sum = tail;
+      for (uint32_t j = t + 1; j < blockDim.x; ++j) {
+        sum = __dadd_rn(sum, s_head[j]);
+        if (s_head_end[j]) break;
+      }
+      __stcg(wc + row, sum);
+      local = __dadd_rn(local, fabs(sum));
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) local = __dadd_rn(local, __shfl_xor_sync(0xFFFFFFFFu, local, d));
+    if (lane == 0) red[t >> 5] = local;
+    __syncthreads();
+    if (t == 0) {
+      double sum = 0.0;
+      for (int i = 0; i < kMeasureThreads / 32; ++i) sum = __dadd_rn(sum, red[i]);
+      __stcg(a.partial + (it & 1u) * gridDim.x + blockIdx.x, sum);
+    }
+    double s_it;
+    if (!barrier_allsum(a, a.partial + (it & 1u) * gridDim.x, it, &s_it)) return;
+    inv = __ddiv_rn(1.0, s_it);
+  }
+  const double* wl = (a.iters & 1u) ? a.w0 : a.w1;
+  const uint32_t tid = blockIdx.x * blockDim.x + t, nthreads = gridDim.x * blockDim.x;
+  for (uint32_t j = tid; j < n; j += nthreads) a.out[j] = a.iters ? __dmul_rn(__ldcg(wl + j), inv) : v0;
+}
+
 // the rows of P^T of one length class (1: medium, 2: long), ascending (flag, scan, scatter)
 __device__ __forceinline__ uint32_t row_class(const uint32_t* tptr, uint32_t j)
 {
@@ -323,8 +486,30 @@ cudaError_t class_rows(const uint32_t* tptr, uint32_t n, uint32_t cls, uint32_t*
 cudaError_t invariant_measure(const uint32_t* tptr, const uint32_t* trows, const double* tvals,
                               const uint32_t* mid_list, uint32_t n_mid, const uint32_t* long_list, uint32_t n_long,
                               uint32_t n, uint32_t iters, double* w0, double* w1, double* partial,
-                              uint32_t partial_cap, double* out, unsigned* sync_words, cudaStream_t s)
+                              uint32_t partial_cap, double* out, unsigned* sync_words, cudaStream_t s, uint64_t nnz)
 {
+  // the matrix on chip: one block per SM, every block's rows within its shared memory
+  // (a row of P^T has at most kMidRow entries when there are no long rows)
+  static int smem_ok = -1;
+  if (smem_ok < 0) {
+    int b = 0;
+    smem_ok = cudaFuncSetAttribute(invariant_measure_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   int(kSmemMeasureBytes)) == cudaSuccess &&
+              cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, invariant_measure_smem_kernel, kMeasureThreads,
+                                                            kSmemMeasureBytes) == cudaSuccess && b >= 1;
+    cudaGetLastError();
+  }
+  const uint32_t blocks = uint32_t(device_sm_count());
+  if (smem_ok == 1 && mid_list && long_list && n_long == 0 && nnz > 0 &&
+      (nnz + blocks - 1) / blocks + kMidRow <= kSmemEntries && 2 * blocks + 2 <= partial_cap) {
+    cudaMemsetAsync(sync_words, 0, 65 * sizeof(unsigned), s);
+    MeasureArgs a{tptr, trows, tvals, mid_list, n_mid, long_list, 0u, kShortRow, n, iters, w0, w1, partial, out,
+                  sync_words, sync_words + 32, sync_words + 64, partial + 2 * size_t(blocks), 0u};
+    uint32_t nnz32 = uint32_t(nnz);
+    void* params[] = {&a, &nnz32};
+    return cudaLaunchCooperativeKernel((const void*)invariant_measure_smem_kernel, dim3(blocks),
+                                       dim3(kMeasureThreads), params, kSmemMeasureBytes, s);
+  }
   static int blocks_per_sm = 0;
   if (!blocks_per_sm) {
     int b = 0;

@@ -24,7 +24,8 @@ cudaError_t class_rows(const uint32_t* tptr, uint32_t n, uint32_t cls, uint32_t*
 cudaError_t invariant_measure(const uint32_t* tptr, const uint32_t* trows, const double* tvals,
                               const uint32_t* mid_list, uint32_t n_mid, const uint32_t* long_list, uint32_t n_long,
                               uint32_t n, uint32_t iters, double* w0, double* w1, double* partial,
-                              uint32_t partial_cap, double* out, unsigned* sync_words, cudaStream_t s);
+                              uint32_t partial_cap, double* out, unsigned* sync_words, cudaStream_t s,
+                              uint64_t nnz = 0);
 int measure_partial_slots();
 
 }  // namespace b12g
