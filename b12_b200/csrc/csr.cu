@@ -273,15 +273,17 @@ __device__ bool barrier_allsum(const MeasureArgs& a, const double* part, uint32_
   __syncthreads();
   if (threadIdx.x == 0) {
     ok = 1;
-    __threadfence();
-    atomicAdd(a.bar_count, 1u);
+    // arrive with release semantics (the block's stores, ordered by the block barrier,
+    // become visible first), then poll with acquire loads
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(a.bar_count) : "memory");
     const unsigned target = (round + 1u) * gridDim.x;
-    volatile unsigned* vc = a.bar_count;
     unsigned long long polls = 0;
-    while (*vc < target) {
+    unsigned seen;
+    for (;;) {
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(seen) : "l"(a.bar_count) : "memory");
+      if (seen >= target) break;
       if (++polls > kBarrierPolls) { atomicOr(a.error, 2u); ok = 0; break; }
     }
-    __threadfence();
   }
   __syncthreads();
   if (threadIdx.x < 32) {
