@@ -175,3 +175,33 @@ def test_partitioned_transition_matrix_matches_reference(golden, name, absolute,
         for k in ("nnz", "rowptr_sha256", "cols_sha256", "vals_sha256"):
             assert d[k] == meta["tm"][k], k
         assert blocks[0].n_cols == meta["tm"]["n_cols"]
+
+
+def test_partitioned_run_over_an_nccl_group_of_one(golden):
+    """The process-group driver with NCCL collectives (one rank on this GPU): the same
+    steps as the emulated ranks, through torch.distributed."""
+    import socket
+    import datetime
+    import torch.distributed as dist
+    from b12_b200.partition import ProcessGroupExchange, drive
+    from workloads import csr_digests
+    meta, _ = golden("lorenz_d15")
+    spec = meta["spec"]
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        runs, trees = _partitioned(spec, 1)
+        ex = ProcessGroupExchange(dist, "cuda")
+        counts = drive(trees[0].subdivision(scheme(spec), len(meta["steps"])), ex)
+        assert counts == [s["n"] for s in meta["steps"]]
+        assert sha(runs[0].host_leaves()[0]) == meta["steps"][-1]["codes_sha256"]
+        block = drive(trees[0].transition_matrix(scheme(spec)), ex)
+        d = csr_digests(*block.rows.to_host())
+        for k in ("nnz", "rowptr_sha256", "cols_sha256", "vals_sha256"):
+            assert d[k] == meta["tm"][k], k
+        block.rows.close()
+    finally:
+        dist.destroy_process_group()
