@@ -245,6 +245,7 @@ b12g_status flag_call(b12g_tree* t, int op, uint8_t u, uint8_t f, uint8_t depth,
   ST(set_ctr(t, C_CHANGED, 0));
   CK(flag_op(t->flg(), t->dn(), op, u, f, t->ctr.p + C_CHANGED, t->n, t->stream));
   count_launches(1);
+  if (!n_changed) return B12G_OK;   // nobody reads the count: no round trip (the stream keeps the order)
   ST(read_ctr(t, C_CHANGED, 1));
   uint32_t c = t->h_ctr[C_CHANGED];
   if (depth == 0 && t->depth != 0) {
