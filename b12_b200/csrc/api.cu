@@ -62,10 +62,22 @@ b12g_status read_ctr(b12g_tree* t, int first, int count)
   return sync(t, "read counters");
 }
 
+// A counter is set without staging the value in host memory: zero by a memset, any
+// other value by a one-thread kernel that takes it as a launch parameter.  A copy from
+// the pinned counter block would read that slot whenever the stream reaches it, so a
+// later host write of the slot (before a synchronisation) could change the value copied.
+__global__ void set_word_kernel(uint32_t* p, uint32_t v) { *p = v; }
+
 b12g_status set_ctr(b12g_tree* t, int slot, uint32_t v)
 {
   t->h_ctr[slot] = v;
-  CK(cudaMemcpyAsync(t->ctr.p + slot, t->h_ctr + slot, sizeof(uint32_t), cudaMemcpyHostToDevice, t->stream));
+  if (v == 0) {
+    CK(cudaMemsetAsync(t->ctr.p + slot, 0, sizeof(uint32_t), t->stream));
+  } else {
+    set_word_kernel<<<1, 1, 0, t->stream>>>(t->ctr.p + slot, v);
+    CK(cudaGetLastError());
+    count_launches(1);
+  }
   return B12G_OK;
 }
 
@@ -89,26 +101,31 @@ b12g_status reserve(b12g_tree* t, uint64_t n_boxes)
   return B12G_OK;
 }
 
-// order-sensitive 64-bit checksum of the leaf codes
-b12g_status leaf_sum(b12g_tree* t, unsigned long long* sum)
+// two schemes map and sample alike: field by field (the padding is not compared), the
+// doubles by their bits
+bool same_bits(double a, double b) { return std::memcmp(&a, &b, sizeof(double)) == 0; }
+
+bool same_scheme(const b12g_scheme& a, const b12g_scheme& b)
 {
-  ST(t->csum.ensure(1, "checksum"));
-  CK(cudaMemsetAsync(t->csum.p, 0, sizeof(unsigned long long), t->stream));
-  CK(leaf_checksum(t->codes(), t->n, t->csum.p, t->stream));
-  count_launches(1);
-  CK(cudaMemcpyAsync(sum, t->csum.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, t->stream));
-  return sync(t, "checksum");
+  if (a.map.kind != b.map.kind || a.map.arith != b.map.arith || a.map.steps != b.map.steps ||
+      !same_bits(a.map.h, b.map.h))
+    return false;
+  for (int i = 0; i < 6; ++i)
+    if (!same_bits(a.map.p[i], b.map.p[i])) return false;
+  return a.grid.kind == b.grid.kind && a.grid.n == b.grid.n && a.grid.points == b.grid.points &&
+         a.grid.seed == b.grid.seed && same_bits(a.grid.eps, b.grid.eps) && a.depth == b.depth &&
+         a.flags_to_check == b.flags_to_check;
 }
 
 // the stored targets of the last subdivision step describe the current leaves under
-// this scheme: same scheme bytes, same leaf count and depth, same codes (checksum)
+// this scheme: no change of the leaf set since they were stored (generation), and the
+// same scheme field by field
 bool stored_rows_fit(b12g_tree* t, const b12g_scheme* sc, const Prepared& pr)
 {
-  if (!t->tgt_ok || t->mixed || t->n != t->tgt_n || t->depth != t->tgt_depth || pr.P != t->tgt_points) return false;
-  if (std::memcmp(sc, &t->tgt_scheme, sizeof(b12g_scheme)) != 0) return false;
-  unsigned long long sum = 0;
-  if (leaf_sum(t, &sum) != B12G_OK) return false;
-  return sum == t->tgt_sum;
+  if (!t->tgt_ok || t->mixed || t->leaf_gen != t->tgt_gen || t->n != t->tgt_n || t->depth != t->tgt_depth ||
+      pr.P != t->tgt_points)
+    return false;
+  return same_scheme(*sc, t->tgt_scheme);
 }
 
 b12g_status prepare(b12g_tree* t, const b12g_scheme* sc, Prepared& pr)
@@ -227,6 +244,7 @@ b12g_status set_root(b12g_tree* t, uint8_t flags)
   CK(cudaMemcpyAsync(t->codes(), &zero, 8, cudaMemcpyHostToDevice, t->stream));
   CK(cudaMemsetAsync(t->flg(), flags, 1, t->stream));
   t->n = 1;
+  ++t->leaf_gen;
   t->depth = 0;
   t->mixed = false;
   ST(set_ctr(t, t->ncur, 1));
@@ -408,7 +426,7 @@ b12g_status b12g_tree_destroy(b12g_tree* t)
   t->src.release(); t->out.release(); t->stage_col.release(); t->stage_cnt.release();
   t->row_count.release(); t->rowptr.release(); t->cand.release(); t->cand2.release();
   t->sort_idx.release(); t->table.release(); t->step_counts.release(); t->sort_tmp.release();
-  t->last_tgt.release(); t->last_rank.release(); t->csum.release();
+  t->last_tgt.release(); t->last_rank.release();
   if (t->h_ctr) cudaFreeHost(t->h_ctr);
   if (t->stream) cudaStreamDestroy(t->stream);
   delete t;
@@ -477,6 +495,7 @@ b12g_status b12g_load_leaves(b12g_tree* t, const uint64_t* codes, const uint8_t*
   CK(cudaMemcpyAsync(t->codes(), codes, size_t(n) * 8, cudaMemcpyHostToDevice, t->stream));
   CK(cudaMemcpyAsync(t->flg(), flags, n, cudaMemcpyHostToDevice, t->stream));
   t->n = n;
+  ++t->leaf_gen;
   t->depth = d;
   t->mixed = false;
   ST(set_ctr(t, t->ncur, n));
@@ -524,6 +543,7 @@ b12g_status b12g_subdivide(b12g_tree* t, uint8_t flags, uint32_t* n_subdivided)
     count_launches(1);
     ST(sync(t, "subdivide"));
     t->cur = o;
+    ++t->leaf_gen;
     t->ncur = no;
     t->n *= 2;
     t->depth += 1;
@@ -554,8 +574,10 @@ b12g_status b12g_remove(b12g_tree* t, uint8_t flags, uint32_t* n_removed)
   const uint32_t kept = t->h_ctr[no];
   const uint32_t removed = t->n - kept;
   t->cur = o;
+  ++t->leaf_gen;
   t->ncur = no;
   t->n = kept;
+  ++t->leaf_gen;
   if (kept == 0) ST(set_root(t, B12G_NONE));  // insertSurroundingBoxIfEmpty
   if (n_removed) *n_removed = removed;
   return B12G_OK;
@@ -1035,6 +1057,7 @@ b12g_status b12g_subdivision_run(b12g_tree* t, const b12g_scheme* sc, uint32_t s
       ST(set_ctr(t, t->ncur, n0));
       ST(sync(t, "restore"));
       t->n = n0;
+      ++t->leaf_gen;
       t->depth = d0;
       continue;
     }
@@ -1052,6 +1075,7 @@ b12g_status b12g_subdivision_run(b12g_tree* t, const b12g_scheme* sc, uint32_t s
       final_n = 1;
     } else {
       t->n = final_n;
+      ++t->leaf_gen;
       t->depth = uint8_t(d0 + steps);
       const uint64_t children = 2ull * (steps >= 2 ? hc[steps - 2] : n0);
       t->tgt_want = std::max<uint64_t>(t->tgt_want, (children + children / 8 + 1) * pr.P);
@@ -1061,7 +1085,7 @@ b12g_status b12g_subdivision_run(b12g_tree* t, const b12g_scheme* sc, uint32_t s
         t->tgt_depth = t->depth;
         t->tgt_points = uint32_t(pr.P);
         t->tgt_scheme = *sc;
-        ST(leaf_sum(t, &t->tgt_sum));
+        t->tgt_gen = t->leaf_gen;
         t->tgt_ok = true;
       }
     }

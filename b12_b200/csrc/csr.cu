@@ -8,6 +8,8 @@
 //                        cooperative launch with a bounded grid barrier
 #include <cooperative_groups.h>
 
+#include <mutex>
+
 #include "kernels.h"
 #include "csr.h"
 
@@ -485,6 +487,47 @@ cudaError_t class_rows(const uint32_t* tptr, uint32_t n, uint32_t cls, uint32_t*
   return cudaGetLastError();
 }
 
+namespace {
+
+struct MeasureLaunch
+{
+  bool smem_ok;        // the shared-memory kernel may take kSmemMeasureBytes and fits one block per SM
+  int blocks_per_sm;   // resident blocks per SM of the L2 kernel
+};
+
+std::mutex g_measure_mu;
+int g_measure_ready[64] = {};
+MeasureLaunch g_measure_cfg[64];
+
+// Per device: cudaFuncSetAttribute applies to the device current when it runs, so the
+// opt-in to the large shared memory is made once on every device that launches the
+// kernel, with that device current, under a lock (server engines run on their own
+// host threads).
+MeasureLaunch measure_launch()
+{
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) { cudaGetLastError(); return {false, 1}; }
+  std::lock_guard<std::mutex> lock(g_measure_mu);
+  if (!g_measure_ready[dev]) {
+    int b = 0;
+    MeasureLaunch c;
+    c.smem_ok = cudaFuncSetAttribute(invariant_measure_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     int(kSmemMeasureBytes)) == cudaSuccess &&
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, invariant_measure_smem_kernel, kMeasureThreads,
+                                                              kSmemMeasureBytes) == cudaSuccess && b >= 1;
+    cudaGetLastError();
+    b = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, invariant_measure_kernel, kMeasureThreads, 0);
+    cudaGetLastError();
+    c.blocks_per_sm = b > 0 ? b : 1;
+    g_measure_cfg[dev] = c;
+    g_measure_ready[dev] = 1;
+  }
+  return g_measure_cfg[dev];
+}
+
+}  // namespace
+
 cudaError_t invariant_measure(const uint32_t* tptr, const uint32_t* trows, const double* tvals,
                               const uint32_t* mid_list, uint32_t n_mid, const uint32_t* long_list, uint32_t n_long,
                               uint32_t n, uint32_t iters, double* w0, double* w1, double* partial,
@@ -492,17 +535,9 @@ cudaError_t invariant_measure(const uint32_t* tptr, const uint32_t* trows, const
 {
   // the matrix on chip: one block per SM, every block's rows within its shared memory
   // (a row of P^T has at most kMidRow entries when there are no long rows)
-  static int smem_ok = -1;
-  if (smem_ok < 0) {
-    int b = 0;
-    smem_ok = cudaFuncSetAttribute(invariant_measure_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   int(kSmemMeasureBytes)) == cudaSuccess &&
-              cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, invariant_measure_smem_kernel, kMeasureThreads,
-                                                            kSmemMeasureBytes) == cudaSuccess && b >= 1;
-    cudaGetLastError();
-  }
+  const MeasureLaunch cfg = measure_launch();
   const uint32_t blocks = uint32_t(device_sm_count());
-  if (smem_ok == 1 && mid_list && long_list && n_long == 0 && nnz > 0 &&
+  if (cfg.smem_ok && mid_list && long_list && n_long == 0 && nnz > 0 &&
       (nnz + blocks - 1) / blocks + kMidRow <= kSmemEntries && 2 * blocks + 2 <= partial_cap) {
     cudaMemsetAsync(sync_words, 0, 65 * sizeof(unsigned), s);
     MeasureArgs a{tptr, trows, tvals, mid_list, n_mid, long_list, 0u, kShortRow, n, iters, w0, w1, partial, out,
@@ -512,13 +547,7 @@ cudaError_t invariant_measure(const uint32_t* tptr, const uint32_t* trows, const
     return cudaLaunchCooperativeKernel((const void*)invariant_measure_smem_kernel, dim3(blocks),
                                        dim3(kMeasureThreads), params, kSmemMeasureBytes, s);
   }
-  static int blocks_per_sm = 0;
-  if (!blocks_per_sm) {
-    int b = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, invariant_measure_kernel, kMeasureThreads, 0);
-    blocks_per_sm = b > 0 ? b : 1;
-  }
-  int grid = grid_for(n, kMeasureThreads, blocks_per_sm);
+  int grid = grid_for(n, kMeasureThreads, cfg.blocks_per_sm);
   if (grid > int(partial_cap / 2)) grid = int(partial_cap / 2);
   if (grid < 1) grid = 1;
   if (grid > int(partial_cap / 2) - 1) grid = int(partial_cap / 2) - 1;

@@ -289,23 +289,6 @@ __global__ void __launch_bounds__(kThreads) stored_rows_kernel(const StoredRowAr
   }
 }
 
-__device__ __forceinline__ uint64_t mix64(uint64_t z)
-{
-  // SplitMix64's finaliser (Steele, Lea, Flood 2014)
-  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-  return z ^ (z >> 31);
-}
-
-__global__ void leaf_checksum_kernel(const uint64_t* __restrict__ codes, uint32_t n, unsigned long long* sum)
-{
-  uint64_t acc = 0;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    acc += mix64(__ldg(codes + i) ^ (uint64_t(i) * 0x9E3779B97F4A7C15ull));
-  for (int d = 16; d > 0; d >>= 1) acc += __shfl_down_sync(0xFFFFFFFFu, acc, d);
-  if ((threadIdx.x & 31) == 0 && acc) atomicAdd(sum, (unsigned long long)acc);
-}
-
 }  // namespace
 
 cudaError_t launch_stored_rows(const StoredRowArgs& a, cudaStream_t s)
@@ -314,14 +297,6 @@ cudaError_t launch_stored_rows(const StoredRowArgs& a, cudaStream_t s)
   const uint64_t want = (uint64_t(a.n_children) + kRowWarps - 1) / kRowWarps;
   const uint64_t cap = uint64_t(device_sm_count()) * 8;
   stored_rows_kernel<<<unsigned(want < cap ? want : cap), kThreads, 0, s>>>(a);
-  return cudaGetLastError();
-}
-
-cudaError_t leaf_checksum(const uint64_t* codes, uint32_t n, unsigned long long* sum, cudaStream_t s)
-{
-  const uint64_t want = (uint64_t(n) + kThreads * 8 - 1) / (kThreads * 8);
-  const uint64_t cap = uint64_t(device_sm_count()) * 4;
-  leaf_checksum_kernel<<<unsigned(want < 1 ? 1 : (want < cap ? want : cap)), kThreads, 0, s>>>(codes, n, sum);
   return cudaGetLastError();
 }
 

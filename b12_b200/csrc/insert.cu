@@ -105,8 +105,10 @@ b12g_status merge_new(b12g_tree* t, uint32_t u, uint8_t ins)
   count_launches(1);
   ST(sync(t, "merge"));
   t->cur = o;
+  ++t->leaf_gen;
   t->ncur = no;
   t->n = uint32_t(total);
+  ++t->leaf_gen;
   return B12G_OK;
 }
 
@@ -190,6 +192,7 @@ b12g_status insert_points_impl(b12g_tree* t, const double* points, uint64_t n_po
     CK(cudaMemcpyAsync(t->codes(), t->cand2.p, 8, cudaMemcpyDeviceToDevice, t->stream));
     CK(cudaMemsetAsync(t->flg(), uint8_t(ins | root_flags), 1, t->stream));
     t->depth = depth;
+    ++t->leaf_gen;
     ST(set_ctr(t, t->ncur, 1));
     ST(sync(t, "insert into the surrounding box"));
     if (n_inserted) *n_inserted = 1;

@@ -72,8 +72,6 @@ struct StoredRowArgs {
   int keep_lost;
 };
 cudaError_t launch_stored_rows(const StoredRowArgs& a, cudaStream_t s);
-// 64-bit checksum of n leaf codes (order-sensitive) added into *sum
-cudaError_t leaf_checksum(const uint64_t* codes, uint32_t n, unsigned long long* sum, cudaStream_t s);
 
 // launch helpers (image.cu); return cudaSuccess or the launch error
 cudaError_t launch_image(uint32_t map_kind, uint32_t arith, uint32_t grid_kind, uint32_t dim, ImageMode mode,

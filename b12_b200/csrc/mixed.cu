@@ -1053,6 +1053,7 @@ b12g_status mixed_load(b12g_tree* t, const uint64_t* codes, const uint8_t* depth
   CK(cudaMemcpyAsync(t->flg(), flags, n, cudaMemcpyHostToDevice, t->stream));
   CK(cudaMemcpyAsync(dep_cur(t), depths, n, cudaMemcpyHostToDevice, t->stream));
   t->n = n;
+  ++t->leaf_gen;
   t->mixed = true;
   ST(set_ctr(t, t->ncur, n));
   ST(sync(t, "load leaves"));
@@ -1186,8 +1187,10 @@ b12g_status mixed_subdivide(b12g_tree* t, uint8_t flags, uint32_t* n_subdivided)
                                                                     t->code[o].p, t->flags[o].p, t->dep[o].p);
   count_launches(1);
   t->cur = o;
+  ++t->leaf_gen;
   t->ncur = no;
   t->n = total;
+  ++t->leaf_gen;
   ST(set_ctr(t, t->ncur, total));
   ST(sync(t, "subdivide"));
   return mixed_settle(t);
@@ -1207,8 +1210,10 @@ b12g_status mixed_remove(b12g_tree* t, uint8_t flags, uint32_t* n_removed)
                                                                    t->code[o].p, t->flags[o].p, t->dep[o].p, nullptr);
   count_launches(1);
   t->cur = o;
+  ++t->leaf_gen;
   t->ncur = no;
   t->n = kept;
+  ++t->leaf_gen;
   ST(set_ctr(t, t->ncur, kept));
   ST(sync(t, "remove"));
   if (n_removed) *n_removed = n - kept;
@@ -1310,6 +1315,7 @@ b12g_status mixed_unsubdivide(b12g_tree* t, uint8_t flags, uint32_t* n_parents)
   ST(read_ctr(t, C_CAND, 1));
   const uint32_t marked = t->h_ctr[C_CAND];
   t->n = kept;
+  ++t->leaf_gen;
   ST(set_ctr(t, t->ncur, kept));
   ST(sync(t, "unsubdivide"));
   if (n_parents) *n_parents = marked - (n - kept);
@@ -1433,6 +1439,7 @@ b12g_status mixed_insert_boxes(b12g_tree* t, uint64_t np, uint8_t depth, uint8_t
                                                                        t->flg(), dep_cur(t), nullptr);
   count_launches(1);
   t->n = kept;
+  ++t->leaf_gen;
   ST(set_ctr(t, t->ncur, kept));
   ST(sync(t, "insert"));
   if (n_inserted) *n_inserted = u;
@@ -1571,6 +1578,7 @@ b12g_status mixed_load_device(b12g_tree* t, const uint64_t* codes, const uint8_t
     return fail(B12G_ERR_INVALID, "%u leaves out of order, nested or deeper than 64", bad);
   }
   t->n = n;
+  ++t->leaf_gen;
   t->mixed = true;
   ST(set_ctr(t, t->ncur, n));
   ST(sync(t, "load leaves"));

@@ -13,7 +13,9 @@
 // loads the library holds it until the process exits).  All calls share the array, so
 // calls that overlap on the GPU (different streams, or different host threads at the
 // same time) race with each other; the barrier words that must start at zero are
-// cleared by every call.
+// cleared by every call.  Before the power iteration a check kernel reads the row
+// pointers and sources once; a matrix whose sources are not all below n is refused
+// with B12G_ERR_INVALID before any iterate is read.
 #include <mutex>
 
 #include "csr.h"
@@ -49,6 +51,21 @@ b12g_status scratch_address(unsigned char** out)
   return B12G_OK;
 }
 
+// The caller's P^T must index only its own n boxes: the iterates in the scratch array
+// are read at every source index, so a source >= n would read past them.  One pass
+// over the row pointers and sources sets bit 0 of *bad on the first violation
+// (tptr[0] != 0, a decreasing row pointer, a source >= n).
+__global__ void check_transpose_kernel(const uint32_t* tptr, const uint32_t* trows, uint32_t n, unsigned* bad)
+{
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
+  if (tid == 0 && tptr[0] != 0u) atomicOr(bad, 1u);
+  for (uint32_t j = tid; j < n; j += nthreads)
+    if (tptr[j] > tptr[j + 1]) atomicOr(bad, 1u);
+  const uint32_t nnz = tptr[n];
+  for (uint32_t k = tid; k < nnz; k += nthreads)
+    if (trows[k] >= n) atomicOr(bad, 1u);
+}
+
 }  // namespace
 
 using namespace b12g::host;
@@ -68,10 +85,18 @@ extern "C" b12g_status b12g_invariant_measure_noalloc(const uint32_t* tptr, cons
   double* partial = w1 + kMaxRows;
   unsigned* sync_words = reinterpret_cast<unsigned*>(partial + kPartialSlots);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // word 96 of the barrier block (past the 65 words the kernel uses): the check's result
+  unsigned* bad = sync_words + 96;
+  unsigned err = 0;
+  CK(cudaMemsetAsync(bad, 0, sizeof(unsigned), s));
+  check_transpose_kernel<<<b12g::device_sm_count() * 4, 256, 0, s>>>(tptr, trows, n, bad);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(&err, bad, sizeof err, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (err) return fail(B12G_ERR_INVALID, "invariant_measure_noalloc: tptr/trows do not describe a matrix of %u boxes", n);
   CK(b12g::invariant_measure(tptr, trows, tvals, nullptr, 0, nullptr, 0, n, iters, w0, w1, partial, kPartialSlots, v,
                              sync_words, s));
-  b12g::count_launches(1);
-  unsigned err = 0;
+  b12g::count_launches(2);
   CK(cudaMemcpyAsync(&err, sync_words + 64, sizeof err, cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   if (err & 2u) return fail(B12G_ERR_TIMEOUT, "invariant_measure_noalloc: grid barrier gave up");

@@ -152,14 +152,16 @@ struct b12g_tree {
   std::vector<cudaEvent_t> graph_prof[2];    // events baked into the captured loop
   // the last step of the fused loop stores its image targets and compaction ranks; the
   // transition matrix of the same leaves and scheme is assembled from them
+  // (valid while leaf_gen is the generation they were stored at: every change of the
+  // leaf set - count, codes, order, depths - increments leaf_gen)
   Buf<uint32_t> last_tgt, last_rank;
-  Buf<unsigned long long> csum;
+  uint64_t leaf_gen = 0;
   bool tgt_ok = false;
   uint64_t tgt_want = 0;       // entries the next run's last step needs (from this run)
   uint32_t tgt_children = 0, tgt_n = 0, tgt_points = 0;
   uint8_t tgt_depth = 0;
   b12g_scheme tgt_scheme{};
-  unsigned long long tgt_sum = 0;
+  uint64_t tgt_gen = 0;
 
   uint64_t* codes() { return code[cur].p; }
   uint8_t* flg() { return flags[cur].p; }

@@ -245,10 +245,14 @@ b12g_status b12g_csr_measure(const b12g_csr* csr, double* v);
  * the free HBM, or a latency-critical loop where cudaMalloc/cudaFree would synchronize
  * the device.  Same power iteration as b12g_invariant_measure, on the CSR of P^T given
  * as device arrays (tptr[n+1], trows[nnz], tvals[nnz]; sources ascending in each row),
- * result in the device array v[n].  Its scratch is one fixed __device__ array shared by
- * all calls: at most 262,144 boxes (B12G_ERR_CAPACITY above that), and calls that overlap
- * on the GPU race.  The first call on a device looks up the array's device address, so
- * make it before any stream capture.  Returns after the work on `stream` has finished. */
+ * result in the device array v[n].  Every row pointer must be non-decreasing from
+ * tptr[0] = 0 and every source below n; a matrix that breaks this is refused with
+ * B12G_ERR_INVALID (a check kernel reads tptr and trows once before the iteration).
+ * Its scratch is one fixed __device__ array shared by all calls: at most 262,144 boxes
+ * (B12G_ERR_CAPACITY above that), and calls that overlap on the GPU race.  The first
+ * call on a device looks up the array's device address.  The call waits for `stream`
+ * twice (after the check and after the iteration, to read their error words) and
+ * returns after the work on `stream` has finished. */
 b12g_status b12g_invariant_measure_noalloc(const uint32_t* tptr, const uint32_t* trows, const double* tvals,
                                            uint32_t n, uint32_t iters, double* v, void* stream);
 

@@ -74,7 +74,18 @@ WORKLOADS = {
                                                                           depth=8)),
     "coupled_duffing_cont_d12": ("ref_duffing", ["--steps", "12"], dict(map="coupled_duffing", points=64, seed=0,
                                                                             depth=12)),
+    # the configured continuation: depth 24, about 10^7 boxes (digests only)
+    "coupled_duffing_cont_d24": ("ref_duffing", ["--steps", "24", "--buf", "1073741824"],
+                                 dict(map="coupled_duffing", points=64, seed=0, depth=24)),
 }
+
+# members of the 512-instance Lorenz parameter scan (SplitMix64 seed 0, explicit-FMA map),
+# run one at a time by the reference: two of depth 27, one of depth 24 and one of depth 21
+for _i, _rho, _d in ((1, "15.528675431851955", 27), (14, "27.729680145646142", 27),
+                     (10, "32.109794817225435", 24), (2, "17.12693383134425", 21)):
+    WORKLOADS[f"lorenz_scan0_i{_i}_d{_d}_fma"] = (
+        "ref_lorenz", ["--steps", str(_d), "--tm", "1", "--fma", "1", "--rho", _rho, "--buf", "1073741824"],
+        dict(map="lorenz", rho=float(_rho), grid=5, steps=_d, fma=True, scan_seed=0, scan_index=_i))
 
 FULL_LIMIT = 20000  # store leaf arrays of steps with at most this many leaves
 

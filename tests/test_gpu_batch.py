@@ -114,3 +114,44 @@ def test_forced_duffing_batch_matches_single_trees_and_reference(golden):
         np.testing.assert_array_equal(b.leaves(i)[0], leaves[0])
         for x, y in zip(b.csr(i), csr):
             np.testing.assert_array_equal(x, y)
+
+
+def test_full_lorenz_scan_512_matches_single_trees_and_reference(golden):
+    """The configured batch: 512 Lorenz instances (rho ~ U[15,35], depth 18-27 from
+    SplitMix64 seed 0, explicit-FMA map, 125-point grid), one persistent launch per step.
+    Every instance equals its own single-tree run (per-step counts, leaf codes and flags,
+    CSR bit for bit), and four instances run one at a time by the reference (two of
+    depth 27, one of 24, one of 21) give the reference's digests."""
+    rho, depth = lorenz_scan(512, 0)
+    grid = B.inner_grid(5)
+    b = B.Batch(LORENZ_CENTER, LORENZ_RADIUS, B.Scheme(B.lorenz(fma=True), grid),
+                [(10.0, r, 8.0 / 3.0) for r in rho], depth)
+    b.run()
+    b.transition_matrices()
+    total = 0
+    tree = B.ImplicitBoxTree(LORENZ_CENTER, LORENZ_RADIUS)
+    for i in range(512):
+        sc = B.Scheme(B.lorenz(rho=rho[i], fma=True), grid)
+        tree.delete_depth(0)
+        counts = tree.subdivision_run(sc, depth[i])
+        np.testing.assert_array_equal(b.counts(i), counts, err_msg=str(i))
+        codes, _, flags = b.leaves(i)
+        scodes, _, sflags = tree.leaves()
+        assert sha(codes) == sha(scodes) and sha(flags) == sha(sflags), i
+        m = tree.transition_matrix(sc)
+        assert csr_digests(*b.csr(i)) == csr_digests(*m.to_host()), i
+        m.close()
+        total += len(codes)
+    assert total == b.info()["final_boxes"]
+    for name in ("lorenz_scan0_i1_d27_fma", "lorenz_scan0_i14_d27_fma", "lorenz_scan0_i10_d24_fma",
+                 "lorenz_scan0_i2_d21_fma"):
+        meta = golden(name)[0]
+        i = meta["spec"]["scan_index"]
+        assert meta["spec"]["rho"] == rho[i] and meta["spec"]["steps"] == depth[i]
+        assert list(b.counts(i)) == [s["n"] for s in meta["steps"]], name
+        codes, _, flags = b.leaves(i)
+        assert sha(codes) == meta["steps"][-1]["codes_sha256"], name
+        assert sha(flags) == meta["steps"][-1]["flags_sha256"], name
+        d = csr_digests(*b.csr(i))
+        for k in ("nnz", "rowptr_sha256", "cols_sha256", "vals_sha256"):
+            assert d[k] == meta["tm"][k], (name, k)

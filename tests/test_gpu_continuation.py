@@ -24,7 +24,7 @@ def make_tree(spec):
     return B.ImplicitBoxTree(c, r)
 
 
-@pytest.mark.parametrize("name", ["coupled_duffing_cont_d8", "coupled_duffing_cont_d12"])
+@pytest.mark.parametrize("name", ["coupled_duffing_cont_d8", "coupled_duffing_cont_d12", "coupled_duffing_cont_d24"])
 def test_continuation_run_matches_reference(golden, name):
     meta, _ = golden(name)
     spec = meta["spec"]
@@ -38,17 +38,21 @@ def test_continuation_run_matches_reference(golden, name):
     assert (depth == spec["depth"]).all()
 
 
-def test_continuation_step_api_matches_reference_each_sweep(golden):
-    meta, _ = golden("coupled_duffing_cont_d8")
+@pytest.mark.parametrize("name", ["coupled_duffing_cont_d8", "coupled_duffing_cont_d24"])
+def test_continuation_step_api_matches_reference_each_sweep(golden, name):
+    """Every sweep's leaf codes and flags, through the step-by-step API (at depth 24: 49
+    sweeps up to 9,910,846 boxes, the configured continuation)."""
+    meta, _ = golden(name)
     spec = meta["spec"]
+    d = spec["depth"]
     t = make_tree(spec)
-    sc = scheme(spec, depth=8, flags_to_check=B.EXPD)
+    sc = scheme(spec, depth=d, flags_to_check=B.EXPD)
     assert t.delete_depth(0) == 1
-    assert t.insert_points(np.zeros(4), 8, B.INS, B.NONE) == 1
+    assert t.insert_points(np.zeros(4), d, B.INS, B.NONE) == 1
     for st in meta["steps"]:
         if st["step"] > 0:
-            t.change_flags(B.INS, B.EXPD, 8)
-            t.insert_by_image(sc, 8, B.INS, B.NONE)
+            t.change_flags(B.INS, B.EXPD, d)
+            t.insert_by_image(sc, d, B.INS, B.NONE)
             t.unset_flags(B.EXPD)
         codes, _, flags = t.leaves()
         assert len(codes) == st["n"], st["step"]

@@ -214,6 +214,30 @@ def test_invariant_measure_against_oracle():
     np.testing.assert_array_equal(v, m.invariant_measure(200))
 
 
+def test_invariant_measure_on_a_second_device_after_the_first():
+    """The power iteration's launch set-up (shared-memory opt-in, occupancy) is made per
+    device: a measure on device 1 after one on device 0 runs and matches the oracle."""
+    import torch
+    if torch.cuda.device_count() < 2:
+        pytest.skip("needs two CUDA devices")
+    spec = dict(map="lorenz", rho=28.0, grid=5)
+    results = []
+    try:
+        for dev in (0, 1):
+            torch.cuda.set_device(dev)
+            t = make_tree(spec)
+            sc = scheme(spec)
+            t.subdivision_run(sc, 18)
+            m = t.transition_matrix(sc)
+            rowptr, cols, vals = m.to_host()
+            results.append((m.invariant_measure(200), O.invariant_measure(rowptr, cols, vals, 200)))
+    finally:
+        torch.cuda.set_device(0)
+    for v, ref in results:
+        assert np.abs(v - ref).sum() < MEASURE_L1
+    np.testing.assert_array_equal(results[0][0], results[1][0])
+
+
 # ------------------------------------------------------------------ search and flags
 @pytest.mark.parametrize("spec", [dict(map="henon", a=1.4, b=0.3, grid=4),
                                   dict(map="lorenz", rho=28.0, grid=3),

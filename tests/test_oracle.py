@@ -10,7 +10,8 @@ import pytest
 from oracle import oracle as O
 from workloads import csr_digests, oracle_spec, sha
 
-SUBDIVISION_CASES = ["henon_d20", "henon_a1.0_d16", "lorenz_d15", "forced_duffing_d16", "lorenz_rho15_d18"]
+SUBDIVISION_CASES = ["henon_d20", "henon_a1.0_d16", "lorenz_d15", "forced_duffing_d16", "lorenz_rho15_d18",
+                     "lorenz_scan0_i2_d21_fma"]
 
 
 @pytest.mark.parametrize("name", SUBDIVISION_CASES)
@@ -32,7 +33,7 @@ def test_subdivision_matches_reference(golden, name):
 @pytest.mark.parametrize("name,absolute,invalid", [
     ("henon_d20", False, False), ("henon_d12_abs", True, False), ("henon_d12_lost", False, True),
     ("lorenz_d15", False, False), ("forced_duffing_d16", False, False),
-    ("lorenz_rho15_d4_invalid_column_unused", False, True)])
+    ("lorenz_rho15_d4_invalid_column_unused", False, True), ("lorenz_scan0_i2_d21_fma", False, False)])
 def test_transition_matrix_matches_reference(golden, name, absolute, invalid):
     meta, arrays = golden(name)
     o = O.Oracle(oracle_spec(meta["spec"]))
