@@ -289,6 +289,7 @@ static uint32_t host_hash_log2(uint64_t n)
 b12g_status ensure_hash(b12g_tree* t, uint64_t max_n)
 {
   const uint32_t l = host_hash_log2(std::max<uint64_t>(max_n, 1));
+  ST(t->pk.ensure(std::max<uint64_t>(max_n, 1), "packed leaf keys"));
   if (t->hash.p && l <= t->hash_log2) return B12G_OK;
   t->hash.release();
   ST(t->hash.ensure(size_t(1) << l, "leaf lookup table"));
@@ -310,13 +311,13 @@ b12g_status next_hash_tag(b12g_tree* t, uint32_t* tag)
 
 b12g_status build_current_hash(b12g_tree* t, Prepared& pr)
 {
-  pr.a.hash = LeafHash{nullptr, 0, 0};
-  if (t->depth > kHashMaxDepth || t->n == 0) return B12G_OK;
+  pr.a.hash = LeafHash{nullptr, 0, 0, nullptr};
+  if (t->depth > kHashMaxDepth || t->n == 0 || t->domain.dim < 2) return B12G_OK;
   ST(ensure_hash(t, t->n));
   uint32_t tag = 0;
   ST(next_hash_tag(t, &tag));
-  const LeafHash h{t->hash.p, tag, t->hash_log2};
-  CK(build_leaf_hash(t->codes(), t->dn(), h, t->ctr.p + C_ERROR, t->n, t->stream));
+  const LeafHash h{t->hash.p, tag, t->hash_log2, t->pk.p};
+  CK(build_leaf_hash(t->codes(), t->dn(), int(t->depth), int(t->domain.dim), h, t->ctr.p + C_ERROR, t->n, t->stream));
   count_launches(1);
   pr.a.hash = h;
   return B12G_OK;
@@ -389,6 +390,9 @@ b12g_status b12g_tree_create(const b12g_domain* domain, b12g_tree** out)
     t->dom.r[j] = r;
     t->dom.lo[j] = c - r;
     t->dom.hi[j] = c + r;
+    // the point-code fast path multiplies by RN(1/r) (checked against the IEEE quotient
+    // per point); radii far from 1 keep the division alone
+    t->dom.inv_r[j] = (r >= 0x1p-500 && r <= 0x1p500) ? 1.0 / r : 0.0;
   }
   b12g_status st = B12G_OK;
   if (cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking) != cudaSuccess) st = cuda_fail(cudaGetLastError(), "stream");
@@ -938,7 +942,7 @@ b12g_status b12g_subdivision_run(b12g_tree* t, const b12g_scheme* sc, uint32_t s
   t->tgt_ok = false;
   for (int attempt = 0; attempt < 12; ++attempt) {
     ST(reserve(t, cap));
-    const bool use_hash = int(d0) + int(steps) - 1 <= kHashMaxDepth;
+    const bool use_hash = int(d0) + int(steps) - 1 <= kHashMaxDepth && t->domain.dim >= 2;
     if (use_hash) ST(ensure_hash(t, cap));
     Prepared pr;
     ST(prepare(t, sc, pr));
@@ -956,9 +960,9 @@ b12g_status b12g_subdivision_run(b12g_tree* t, const b12g_scheme* sc, uint32_t s
     uint32_t* const store_rank = store ? t->last_rank.p : nullptr;
     const uint64_t store_cap = store ? t->last_tgt.n : 0;
     // key of the captured graph: every pointer and parameter the launches bake in
-    std::vector<uint8_t> key(sizeof(b12g_scheme) + 80);
+    std::vector<uint8_t> key(sizeof(b12g_scheme) + 88);
     std::memcpy(key.data(), sc, sizeof(b12g_scheme));
-    uint64_t extra[10] = {steps, cap, uint64_t(t->cur) | uint64_t(t->ncur) << 1 | uint64_t(t->profile) << 2, uint64_t(d0),
+    uint64_t extra[11] = {uint64_t(uintptr_t(t->pk.p)), steps, cap, uint64_t(t->cur) | uint64_t(t->ncur) << 1 | uint64_t(t->profile) << 2, uint64_t(d0),
                           uint64_t(uintptr_t(t->code[0].p)), uint64_t(uintptr_t(t->hit.p)), uint64_t(uintptr_t(t->table.p)),
                           uint64_t(uintptr_t(t->code[1].p)) ^ (uint64_t(uintptr_t(t->hash.p)) << 1),
                           uint64_t(uintptr_t(store_tgt)) ^ (store_cap << 1), uint64_t(uintptr_t(store_rank))};
@@ -980,11 +984,11 @@ b12g_status b12g_subdivision_run(b12g_tree* t, const b12g_scheme* sc, uint32_t s
       for (uint32_t s = 0; s < steps && err == cudaSuccess; ++s) {
         const int o = 1 - cur, no = 1 - ncur;
         ImageArgs a = pr.a;
-        a.hash = LeafHash{nullptr, 0, 0};
+        a.hash = LeafHash{nullptr, 0, 0, nullptr};
         if (use_hash) {
-          a.hash = LeafHash{t->hash.p, s + 1, t->hash_log2};
-          err = build_leaf_hash(t->code[cur].p, t->ctr.p + ncur, a.hash, t->ctr.p + C_ERROR,
-                                uint32_t(std::min<uint64_t>(cap, 0xFFFFFFFFu)), t->stream);
+          a.hash = LeafHash{t->hash.p, s + 1, t->hash_log2, t->pk.p};
+          err = build_leaf_hash(t->code[cur].p, t->ctr.p + ncur, int(d0) + int(s), int(t->domain.dim), a.hash,
+                                t->ctr.p + C_ERROR, uint32_t(std::min<uint64_t>(cap, 0xFFFFFFFFu)), t->stream);
           if (err != cudaSuccess) break;
         }
         a.codes = t->code[cur].p;

@@ -47,6 +47,7 @@ struct Domain {
   double r[B12G_MAX_DIM];
   double lo[B12G_MAX_DIM];   // c - r, rounded as the reference does (isPointInBox)
   double hi[B12G_MAX_DIM];   // c + r
+  double inv_r[B12G_MAX_DIM];  // RN(1 / r) for the point-code fast path, 0 where it is not used
 };
 
 struct MapParams {
@@ -179,17 +180,44 @@ __device__ __forceinline__ uint64_t interleave(const uint32_t (&bits)[D], const 
   return code;
 }
 
+// centre and radius of dimension j of a box whose index in that dimension is `bits`
+// after k bisections
+__device__ __forceinline__ void box_axis(const Domain& dom, int j, uint32_t bits, int k, double& c, double& r)
+{
+  r = dom.r[j] * pow2(-k);
+  const double t = __dsub_rn(__dmul_rn(double(bits) * pow2(-k), 2.0), 1.0);
+  c = __dadd_rn(__dadd_rn(__dmul_rn(t, dom.r[j]), dom.c[j]), r);
+}
+
 // centre and radius of a box
 template<int D>
 __device__ __forceinline__ void box_coordinates(const Domain& dom, uint64_t code, int depth, double* c, double* r)
 {
 #pragma unroll
-  for (int j = 0; j < D; ++j) {
+  for (int j = 0; j < D; ++j) box_axis(dom, j, deinterleave<D>(code, depth, j), bisections<D>(depth, j), c[j], r[j]);
+}
+
+// The per-dimension indices of a depth-d box packed dimension 0 first: dimension j
+// takes bisections(d, j) bits, so a packed key holds d bits.  The single-tree leaf
+// lookup table is keyed by it (no bit interleaving on the lookup path); the order of
+// packed keys is not the tree order.
+template<int D>
+__device__ __forceinline__ uint64_t pack_bits(const uint32_t* bits, int depth)
+{
+  uint64_t p = 0;
+#pragma unroll
+  for (int j = 0; j < D; ++j) p = (p << bisections<D>(depth, j)) | uint64_t(bits[j]);
+  return p;
+}
+
+template<int D>
+__device__ __forceinline__ void unpack_bits(uint64_t p, int depth, uint32_t* bits)
+{
+#pragma unroll
+  for (int j = D - 1; j >= 0; --j) {
     const int k = bisections<D>(depth, j);
-    const uint32_t bits = deinterleave<D>(code, depth, j);
-    r[j] = dom.r[j] * pow2(-k);
-    const double t = __dsub_rn(__dmul_rn(double(bits) * pow2(-k), 2.0), 1.0);
-    c[j] = __dadd_rn(__dadd_rn(__dmul_rn(t, dom.r[j]), dom.c[j]), r[j]);
+    bits[j] = uint32_t(p & ((1ull << k) - 1ull));
+    p >>= k;
   }
 }
 
@@ -197,22 +225,56 @@ __device__ __forceinline__ void box_coordinates(const Domain& dom, uint64_t code
 // floor(u * 2^64bits) >> (64bits - k) == floor(u * 2^k) for u >= 0 and exact scaling,
 // so the code equals the reference's depth-64 code shifted to depth d, including the
 // u == 1.0 rounding case where the overflow bit is dropped.
+//
+// The index of p in dimension j after k bisections is floor(u 2^k) with
+// u = RN(RN(RN(x / r) + 1) / 2), x = RN(p - c).  Since the halving is exact this is
+// floor(RN(q + 1) 2^(k-1)) with q = RN(x / r), a non-decreasing function of q.  The fast
+// path replaces the division by qa = RN(x RN(1/r)): two roundings of relative size
+// 2^-53 each give |qa - x/r| <= 2^-52 |x/r| (1 + 2^-53), and |q - x/r| <= 2^-53 |x/r|,
+// so |q - qa| < 2^-50.9 for |x/r| <= 1 + 2^-50 (p inside the domain).  The two
+// roundings to RN(. + 1) in [0, 2] add at most 2^-52, so sa = RN(qa + 1) 2^(k-1) is
+// within 2^(k-51) of the exact s.  When sa is at least 2^(k-49) away from both
+// neighbouring integers, floor(s) = floor(sa); otherwise (probability about 2^(k-48))
+// the IEEE division decides, exactly as before.
+__device__ __forceinline__ uint32_t axis_index(const Domain& dom, int j, double pj, int k)
+{
+  const double x = __dsub_rn(pj, dom.c[j]);
+  const double y = dom.inv_r[j];
+  const unsigned long long mask = (1ull << k) - 1ull;
+  if (y != 0.0) {
+    const double sa = __dmul_rn(__dadd_rn(__dmul_rn(x, y), 1.0), pow2(k - 1));
+    const double fl = floor(sa);
+    const double f = __dsub_rn(sa, fl);
+    const double eps = pow2(k - 49);
+    if (f >= eps && f <= __dsub_rn(1.0, eps)) return uint32_t((unsigned long long)fl & mask);
+  }
+  const double u = __dmul_rn(__dadd_rn(__ddiv_rn(x, dom.r[j]), 1.0), 0.5);
+  const double s = floor(u * pow2(k));
+  return uint32_t((unsigned long long)s & mask);
+}
+
+// per-dimension indices of the depth-d box that contains p; false if p lies outside
+// the domain
 template<int D>
-__device__ __forceinline__ bool point_code(const Domain& dom, const double* p, int depth, uint64_t& code)
+__device__ __forceinline__ bool point_bits(const Domain& dom, const double* p, int depth, uint32_t* bits)
 {
   bool inside = true;
 #pragma unroll
   for (int j = 0; j < D; ++j) inside = inside && (dom.lo[j] <= p[j]) && (p[j] < dom.hi[j]);
   if (!inside) return false;
+#pragma unroll
+  for (int j = 0; j < D; ++j) bits[j] = axis_index(dom, j, p[j], bisections<D>(depth, j));
+  return true;
+}
+
+template<int D>
+__device__ __forceinline__ bool point_code(const Domain& dom, const double* p, int depth, uint64_t& code)
+{
   uint32_t bits[D];
+  if (!point_bits<D>(dom, p, depth, bits)) return false;
   int k[D];
 #pragma unroll
-  for (int j = 0; j < D; ++j) {
-    k[j] = bisections<D>(depth, j);
-    const double u = __dmul_rn(__dadd_rn(__ddiv_rn(__dsub_rn(p[j], dom.c[j]), dom.r[j]), 1.0), 0.5);
-    const double s = floor(u * pow2(k[j]));
-    bits[j] = uint32_t((unsigned long long)s & ((1ull << k[j]) - 1ull));
-  }
+  for (int j = 0; j < D; ++j) k[j] = bisections<D>(depth, j);
   if constexpr (D == 3) {
     if (depth == 64) {
       // 22 + 21 + 21 bits: the first 63 bisections are 21 full rounds, the 64th is the
@@ -259,6 +321,8 @@ struct LeafHash {
   ulonglong2* slots;         // nullptr: use the binary search
   uint32_t tag;              // 1..255
   uint32_t log2_cap;         // table capacity (slots allocated) = 2^log2_cap
+  uint64_t* pk;              // single-tree tables: every leaf's packed key (pack_bits), which
+                             // the image kernels read as their source box's indices
 };
 
 constexpr int kHashMaxDepth = 56;
@@ -292,13 +356,19 @@ __device__ __forceinline__ uint32_t hash_locate(const LeafHash& h, uint32_t n, u
   return kInvalidIndex;
 }
 
-// leaf index of a depth-d code: hash when built, binary search otherwise (with the
-// out-of-domain rule of `locate`)
-__device__ __forceinline__ uint32_t find_leaf(const LeafHash& h, const uint64_t* codes, uint32_t n, bool valid,
-                                              uint64_t code)
+// leaf index of the depth-d box with per-dimension indices `bits` (valid: inside the
+// domain) among the leaves of a single tree: the table of packed keys when built, the
+// binary search over the codes otherwise (with the out-of-domain rule of `locate`)
+template<int D>
+__device__ __forceinline__ uint32_t find_leaf_bits(const LeafHash& h, const uint64_t* codes, uint32_t n, bool valid,
+                                                   const uint32_t (&bits)[D], int depth)
 {
-  if (!h.slots || !valid || n == 0) return locate(codes, n, valid, code);
-  return hash_locate(h, n, code);
+  if (h.slots && valid && n > 0) return hash_locate(h, n, pack_bits<D>(bits, depth));
+  if (!valid || n == 0) return locate(codes, n, valid, 0);
+  int k[D];
+#pragma unroll
+  for (int j = 0; j < D; ++j) k[j] = bisections<D>(depth, j);
+  return locate(codes, n, true, interleave<D>(bits, k, depth));
 }
 
 // ---------------------------------------------------------------------------------

@@ -17,19 +17,37 @@ template<class Map, class Grid>
 struct PointImage {
   static constexpr int D = Map::D;
 
-  static __device__ __forceinline__ uint64_t source_code(const ImageArgs& a, uint32_t leaf)
+  // per-dimension indices of source box `leaf` at a.depth (in children mode: child
+  // leaf & 1 of leaf leaf >> 1): from the packed keys the lookup table was built from,
+  // else from the code
+  static __device__ __forceinline__ void source_bits(const ImageArgs& a, uint32_t leaf, uint32_t (&bits)[D])
   {
-    return a.children ? ((__ldg(a.codes + (leaf >> 1)) << 1) | uint64_t(leaf & 1u)) : __ldg(a.codes + leaf);
+    if (a.hash.pk) {
+      if (a.children) {
+        unpack_bits<D>(__ldg(a.hash.pk + (leaf >> 1)), a.depth - 1, bits);
+        const int jd = (a.depth - 1) % D;          // the last bisection splits dimension jd
+        bits[jd] = (bits[jd] << 1) | (leaf & 1u);
+      } else {
+        unpack_bits<D>(__ldg(a.hash.pk + leaf), a.depth, bits);
+      }
+      return;
+    }
+    const uint64_t code =
+        a.children ? ((__ldg(a.codes + (leaf >> 1)) << 1) | uint64_t(leaf & 1u)) : __ldg(a.codes + leaf);
+#pragma unroll
+    for (int j = 0; j < D; ++j) bits[j] = deinterleave<D>(code, a.depth, j);
   }
 
-  // returns the target code validity; `tcode` the depth-d code of the image point.
-  // `pts` is the block's grid-point table (dimension-major, P entries per dimension)
-  // when the grid has one, else the 1-D coordinate table.
-  static __device__ __forceinline__ bool image(const ImageArgs& a, const double* pts, bool use_table, uint64_t code,
-                                               uint64_t i, uint32_t k, uint64_t& tcode)
+  // returns whether the image point lies in the domain; `tbits` its box's per-dimension
+  // indices at a.depth.  `pts` is the block's grid-point table (dimension-major, P
+  // entries per dimension) when the grid has one, else the 1-D coordinate table.
+  static __device__ __forceinline__ bool image(const ImageArgs& a, const double* pts, bool use_table,
+                                               const uint32_t (&sbits)[D], uint64_t i, uint32_t k,
+                                               uint32_t (&tbits)[D])
   {
     double c[D], r[D], g[D], x[D], y[D];
-    box_coordinates<D>(a.dom, code, a.depth, c, r);
+#pragma unroll
+    for (int j = 0; j < D; ++j) box_axis(a.dom, j, sbits[j], bisections<D>(a.depth, j), c[j], r[j]);
     if (Grid::kTable && use_table) {
 #pragma unroll
       for (int j = 0; j < D; ++j) g[j] = pts[j * uint32_t(a.points) + k];
@@ -39,15 +57,29 @@ struct PointImage {
 #pragma unroll
     for (int j = 0; j < D; ++j) x[j] = __dadd_rn(c[j], __dmul_rn(g[j], r[j]));
     Map::apply(a.map, x, y);
-    return point_code<D>(a.dom, y, a.depth, tcode);
+    return point_bits<D>(a.dom, y, a.depth, tbits);
   }
 
-  static __device__ __forceinline__ uint32_t target(const ImageArgs& a, uint32_t n, bool valid, uint64_t tcode)
+  // the depth-d code of a box (candidates of Insert mode)
+  static __device__ __forceinline__ uint64_t code_of(const ImageArgs& a, const uint32_t (&bits)[D])
   {
-    if (!a.children) return find_leaf(a.hash, a.codes, n, valid, tcode);
+    int k[D];
+#pragma unroll
+    for (int j = 0; j < D; ++j) k[j] = bisections<D>(a.depth, j);
+    return interleave<D>(bits, k, a.depth);
+  }
+
+  static __device__ __forceinline__ uint32_t target(const ImageArgs& a, uint32_t n, bool valid,
+                                                    const uint32_t (&tbits)[D])
+  {
+    if (!a.children) return find_leaf_bits<D>(a.hash, a.codes, n, valid, tbits, a.depth);
     if (!valid) return kInvalidIndex;
-    const uint32_t p = find_leaf(a.hash, a.codes, n, true, tcode >> 1);
-    return p == kInvalidIndex ? kInvalidIndex : 2u * p + uint32_t(tcode & 1u);
+    const int jd = (a.depth - 1) % D;
+    uint32_t pbits[D];
+#pragma unroll
+    for (int j = 0; j < D; ++j) pbits[j] = j == jd ? tbits[j] >> 1 : tbits[j];
+    const uint32_t p = find_leaf_bits<D>(a.hash, a.codes, n, true, pbits, a.depth - 1);
+    return p == kInvalidIndex ? kInvalidIndex : 2u * p + (tbits[jd] & 1u);
   }
 };
 
@@ -99,13 +131,14 @@ __global__ void __launch_bounds__(kThreads) image_points_kernel(const ImageArgs 
     const uint64_t g = base + lane;
     const bool active = g < total;
     uint32_t t = kInvalidIndex;
-    uint64_t tcode = 0;
+    uint32_t tbits[Map::D];
     bool valid = false;
     if (active) {
       const uint32_t leaf = a.src ? __ldg(a.src + rank) : uint32_t(rank);
-      const uint64_t code = PI::source_code(a, leaf);
-      valid = PI::image(a, pts, table, code, g, uint32_t(k), tcode);
-      t = PI::target(a, n, valid, tcode);
+      uint32_t sbits[Map::D];
+      PI::source_bits(a, leaf, sbits);
+      valid = PI::image(a, pts, table, sbits, g, uint32_t(k), tbits);
+      t = PI::target(a, n, valid, tbits);
     }
     rank += rank_step;
     k += k_step;
@@ -128,6 +161,7 @@ __global__ void __launch_bounds__(kThreads) image_points_kernel(const ImageArgs 
         if (active && t != kInvalidIndex && lane == __ffs(hp) - 1) a.hit[t] = 1;
       }
       const bool is_cand = active && valid && t == kInvalidIndex;
+      const uint64_t tcode = is_cand ? PI::code_of(a, tbits) : 0ull;
       const uint64_t key = is_cand ? tcode : kInvalidCode;
       const unsigned peers = __match_any_sync(0xFFFFFFFFu, key);
       const bool leader = is_cand && lane == __ffs(peers) - 1;
@@ -171,15 +205,16 @@ __global__ void __launch_bounds__(kThreads) transition_rows_kernel(const RowArgs
 
   for (uint32_t row = blockIdx.x * kRowWarps + w; row < nrows; row += warps) {
     const uint32_t leaf = a.src ? __ldg(a.src + row) : row;
-    const uint64_t code = PI::source_code(a, leaf);
+    uint32_t sbits[Map::D];
+    PI::source_bits(a, leaf, sbits);
 #pragma unroll 1
     for (int q = 0; q < 4; ++q) {
       const uint32_t k = uint32_t(lane) + 32u * q;
       uint32_t key = kPadKey;
       if (k < P) {
-        uint64_t tcode;
-        const bool valid = PI::image(a, pts, table, code, uint64_t(row) * P + k, k, tcode);
-        const uint32_t t = PI::target(a, n, valid, tcode);
+        uint32_t tbits[Map::D];
+        const bool valid = PI::image(a, pts, table, sbits, uint64_t(row) * P + k, k, tbits);
+        const uint32_t t = PI::target(a, n, valid, tbits);
         key = t == kInvalidIndex ? kLostKey : t;
       }
       s[lane + 32 * q] = key;

@@ -34,15 +34,17 @@ __global__ void locate_points_kernel(const double* pts, uint32_t n_pts, Domain d
     double p[D];
 #pragma unroll
     for (int j = 0; j < D; ++j) p[j] = pts[size_t(i) * D + j];
-    uint64_t code = 0;
-    const bool valid = point_code<D>(dom, p, depth, code);
-    if (!valid) continue;
-    const uint32_t t = root_only ? kInvalidIndex : find_leaf(hash, codes, n, true, code);
+    uint32_t bits[D];
+    if (!point_bits<D>(dom, p, depth, bits)) continue;
+    const uint32_t t = root_only ? kInvalidIndex : find_leaf_bits<D>(hash, codes, n, true, bits, depth);
     if (t != kInvalidIndex) {
       if (hit) hit[t] = 1;
     } else {
+      int k[D];
+#pragma unroll
+      for (int j = 0; j < D; ++j) k[j] = bisections<D>(depth, j);
       const uint32_t pos = atomicAdd(cand_count, 1u);
-      if (pos < cand_cap) cand[pos] = code;
+      if (pos < cand_cap) cand[pos] = interleave<D>(bits, k, depth);
       else atomicOr(error, 1u);
     }
   }
@@ -71,20 +73,19 @@ b12g_status sort_unique_candidates(b12g_tree* t, uint32_t m, uint8_t depth, uint
   if (m == 0) return set_ctr(t, C_NNEW, 0);
   const uint64_t cells = sort_scratch_u32(m);
   ST(t->cand2.ensure(m, "candidate sort"));
-  ST(t->sort_idx.ensure(2 * cells + 2 * (size_t(m) + 1) + compact_tiles(std::max<uint64_t>(cells, m + 1)) + 8,
-                        "candidate sort scratch"));
-  uint32_t* hist = t->sort_idx.p;
-  uint32_t* offsets = hist + cells;
-  uint32_t* flag = offsets + cells;
+  ST(t->sort_idx.ensure(cells + 2 * (size_t(m) + 1) + compact_tiles(uint64_t(m) + 1) + 8, "candidate sort scratch"));
+  uint32_t* scratch = t->sort_idx.p;
+  uint32_t* flag = scratch + cells;
   uint32_t* pos = flag + (m + 1);
   uint32_t* tiles = pos + (m + 1);
   uint64_t* sorted = nullptr;
   const int bits = std::max(8, ((int(depth) + 7) / 8) * 8);
-  CK(radix_sort_u64(t->cand.p, t->cand2.p, t->ctr.p + C_CAND, m, bits, hist, offsets, tiles, t->ctr.p + C_TMP,
-                    &sorted, t->stream));
+  CK(radix_sort_u64(t->cand.p, t->cand2.p, t->ctr.p + C_CAND, m, bits, scratch, t->ctr.p + C_ERROR, &sorted,
+                    t->stream));
   uint64_t* other = sorted == t->cand.p ? t->cand2.p : t->cand.p;
   CK(unique_sorted_u64(sorted, t->ctr.p + C_CAND, m, other, t->ctr.p + C_NNEW, flag, pos, tiles, t->stream));
-  count_launches(1 + 5 * uint64_t(bits / 8) + 5);
+  count_launches(uint64_t(sort_launches(bits)) + 5);
+  ST(check_error(t, "candidate sort"));
   ST(read_ctr(t, C_NNEW, 1));
   *u = t->h_ctr[C_NNEW];
   // the unique codes must end up in t->cand2 for merge_new

@@ -83,10 +83,12 @@ bool image_supported(uint32_t map_kind, uint32_t arith, uint32_t grid_kind, uint
 
 // tree_ops.cu ---------------------------------------------------------------------
 int device_sm_count();
-// insert the n codes into the lookup table with tag h.tag; table slots = 2^h.log2_cap
-// must be >= the slots hash_log2(n) asks for (error bit 0 otherwise)
-cudaError_t build_leaf_hash(const uint64_t* codes, const uint32_t* n, LeafHash h, uint32_t* error, uint32_t max_n,
-                            cudaStream_t s);
+// insert the n leaves of one depth (dim 2..4, depth <= kHashMaxDepth) into the lookup
+// table with tag h.tag, keyed by their packed per-dimension indices (pack_bits), which
+// also go to h.pk[i]; table slots = 2^h.log2_cap must be >= the slots hash_log2(n) asks
+// for (error bit 0 otherwise)
+cudaError_t build_leaf_hash(const uint64_t* codes, const uint32_t* n, int depth, int dim, LeafHash h, uint32_t* error,
+                            uint32_t max_n, cudaStream_t s);
 // flags |= f on hit leaves (hit cleared); *changed += leaves that lacked f
 cudaError_t apply_hits(uint8_t* flags, uint8_t* hit, const uint32_t* n, uint8_t f, uint32_t* changed,
                        uint32_t max_n, cudaStream_t s);

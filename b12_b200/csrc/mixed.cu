@@ -1384,21 +1384,20 @@ b12g_status mixed_insert_boxes(b12g_tree* t, uint64_t np, uint8_t depth, uint8_t
   ST(t->ins_pos.ensure(uint64_t(m) + 1, "new box heads"));
   ST(t->ins_head.ensure(uint64_t(m) + 1, "new box heads"));
   const uint64_t cells = sort_scratch_u32(m);
-  ST(t->sort_idx.ensure(2 * cells + compact_tiles(cells) + 8, "new box sort"));
-  uint32_t* hist = t->sort_idx.p;
-  uint32_t* offsets = hist + cells;
-  uint32_t* tiles = offsets + cells;
+  ST(t->sort_idx.ensure(cells + 8, "new box sort"));
+  uint32_t* scratch = t->sort_idx.p;
   depth_key_kernel<<<grid_for_n(m), kThreads, 0, t->stream>>>(t->ins_dep.p, m, t->ins_key[0].p, t->ins_idx[0].p);
   uint64_t* keys = nullptr;
   uint32_t* order = nullptr;
   CK(radix_sort_u64_values(t->ins_key[0].p, t->ins_key[1].p, t->ins_idx[0].p, t->ins_idx[1].p, t->ctr.p + C_CAND, m,
-                           8, hist, offsets, tiles, t->ctr.p + C_TMP, &keys, &order, t->stream));
+                           8, scratch, t->ctr.p + C_ERROR, &keys, &order, t->stream));
   uint32_t* order_alt = order == t->ins_idx[0].p ? t->ins_idx[1].p : t->ins_idx[0].p;
   pattern_key_kernel<<<grid_for_n(m), kThreads, 0, t->stream>>>(t->ins_code.p, t->ins_dep.p, order, m,
                                                                  t->ins_key[0].p);
-  CK(radix_sort_u64_values(t->ins_key[0].p, t->ins_key[1].p, order, order_alt, t->ctr.p + C_CAND, m, 64, hist,
-                           offsets, tiles, t->ctr.p + C_TMP, &keys, &order, t->stream));
-  count_launches(2 + (1 + 5 * 1) + (1 + 5 * 8));   // key kernels; per sort one set-up, 5 launches a digit
+  CK(radix_sort_u64_values(t->ins_key[0].p, t->ins_key[1].p, order, order_alt, t->ctr.p + C_CAND, m, 64, scratch,
+                           t->ctr.p + C_ERROR, &keys, &order, t->stream));
+  count_launches(2 + sort_launches(8) + sort_launches(64));   // key kernels and the two sorts
+  ST(check_error(t, "new box sort"));
   new_heads_kernel<<<grid_for_n(m), kThreads, 0, t->stream>>>(t->ins_code.p, t->ins_dep.p, order, m, t->ins_head.p);
   count_launches(1);
   uint32_t u = 0;

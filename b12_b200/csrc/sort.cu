@@ -1,12 +1,19 @@
-// LSD radix sort of 64-bit keys (box codes), 8-bit digits, and the set operations the
-// continuation needs on sorted code arrays: unique and merge.
+// Onesweep LSD radix sort of 64-bit keys (box codes), 8-bit digits, and the set
+// operations the continuation needs on sorted code arrays: unique and merge.
 //
-// One pass over a digit = three steps: every 4096-key tile counts its digits
-// (histogram kernel), the digit-major table of tile counts is scanned, and every tile
-// scatters its keys, stably ranked within the tile (warp ballots on equal digits in
-// key order, then a prefix over the tile's warps).  This replaces the reference's
-// thrust::sort / sort_by_key on codes (helpFunctions.hpp:40-98 via sortBoxes, used by
-// insertByIterators at ImplicitBoxTree.hpp:1832-1875).
+// The sort follows the onesweep scheme of Adinets and Merrill ("Onesweep: A Faster
+// Least Significant Digit Radix Sort for GPUs", 2022): one histogram pass counts every
+// digit position of every key at once; then each digit takes ONE pass in which a tile
+// of 4096 keys (tile number drawn from an atomic counter, so that lower tiles are always
+// already running) ranks its keys stably in shared memory, publishes its per-digit
+// count, adds its predecessors' counts by decoupled look-back (a predecessor that has
+// already published its inclusive prefix ends the walk), and writes its keys out in
+// digit order from shared memory, so a warp's stores are runs of consecutive
+// addresses.  Every look-back wait is bounded: a tile that gives up sets bit 2 of the
+// caller's error word (the caller reports a timeout) and the result is not used.
+// This replaces the reference's thrust::sort / sort_by_key on codes
+// (helpFunctions.hpp:40-98 via sortBoxes, used by insertByIterators at
+// ImplicitBoxTree.hpp:1832-1875).
 #include <utility>
 
 #include "kernels.h"
@@ -21,6 +28,11 @@ constexpr int kWarps = kThreads / 32;
 constexpr int kRounds = 16;                       // keys per thread per tile
 constexpr uint32_t kTile = kThreads * kRounds;    // 4096
 constexpr int kBins = 256;
+constexpr int kMaxPasses = 8;
+constexpr uint64_t kAggregate = 1ull << 62;       // status word: tile count published
+constexpr uint64_t kInclusive = 2ull << 62;       // status word: inclusive prefix published
+constexpr uint64_t kFlagMask = 3ull << 62;
+constexpr uint32_t kLookbackPolls = 1u << 20;     // polls of one predecessor before giving up
 
 int grid_for(uint64_t work, int per_block, int blocks_per_sm)
 {
@@ -29,82 +41,255 @@ int grid_for(uint64_t work, int per_block, int blocks_per_sm)
   return int(want < 1 ? 1 : (want < cap ? want : cap));
 }
 
+// Scratch layout (u64 words): [status region 0: tiles x 256][status region 1: tiles x 256]
+// [histograms: kMaxPasses x 256 (u32 pairs)][tile counters: kMaxPasses (u32)]
+struct SortScratch
+{
+  uint64_t* status[2];
+  uint32_t* hist;       // kMaxPasses x kBins
+  uint32_t* counter;    // kMaxPasses
+};
+
+SortScratch carve(uint32_t* base, uint32_t tiles)
+{
+  SortScratch sc;
+  uint64_t* w = reinterpret_cast<uint64_t*>(base);
+  sc.status[0] = w;
+  sc.status[1] = w + size_t(tiles) * kBins;
+  sc.hist = reinterpret_cast<uint32_t*>(w + 2 * size_t(tiles) * kBins);
+  sc.counter = sc.hist + kMaxPasses * kBins;
+  return sc;
+}
+
+// every digit of every key, all passes at once (one read of the keys)
+__global__ void __launch_bounds__(kThreads) onesweep_hist_kernel(const uint64_t* __restrict__ keys,
+                                                                 const uint32_t* n_ptr, int passes, uint32_t* hist)
+{
+  __shared__ uint32_t h[kMaxPasses * kBins];
+  for (int i = threadIdx.x; i < passes * kBins; i += kThreads) h[i] = 0;
+  __syncthreads();
+  const uint32_t n = *n_ptr;
+  for (uint32_t i = blockIdx.x * kThreads + threadIdx.x; i < n; i += gridDim.x * kThreads) {
+    const uint64_t k = __ldg(keys + i);
+    for (int p = 0; p < passes; ++p) atomicAdd(&h[p * kBins + int((k >> (8 * p)) & 0xFFu)], 1u);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < passes * kBins; i += kThreads)
+    if (h[i]) atomicAdd(hist + i, h[i]);
+}
+
+// exclusive scan of one value per thread over the block (256 threads)
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* warp_sums)
+{
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d);
+    if (lane >= d) x += y;
+  }
+  if (lane == 31) warp_sums[w] = x;
+  __syncthreads();
+  uint32_t before = 0;
+  for (int q = 0; q < w; ++q) before += warp_sums[q];
+  __syncthreads();
+  return before + x - v;
+}
+
 // key index of (warp w, round r, lane) within a tile: each warp owns 512 consecutive keys
 __device__ __forceinline__ uint32_t tile_index(int w, int r, int lane) { return uint32_t(w * 512 + r * 32 + lane); }
 
-__global__ void __launch_bounds__(kThreads) digit_hist_kernel(const uint64_t* keys, const uint32_t* n_ptr, int shift,
-                                                              uint32_t* tile_hist)
+template<bool kValues>
+__global__ void __launch_bounds__(kThreads) onesweep_pass_kernel(const uint64_t* __restrict__ keys,
+                                                                 const uint32_t* __restrict__ vals,
+                                                                 const uint32_t* n_ptr, int pass, SortScratch sc,
+                                                                 uint64_t* out, uint32_t* vout, uint32_t* error)
 {
-  __shared__ uint32_t h[kBins];
+  static_assert(kBins == kThreads, "one thread per digit");
+  __shared__ uint32_t wcount[kWarps][kBins];   // per-warp digit counts, then per-warp digit bases in the tile
+  __shared__ uint32_t s_gofs[kBins];           // global position of the tile's first key of digit d, minus
+                                               // that key's staging index
+  __shared__ uint32_t warp_sums[kWarps];
+  __shared__ uint32_t s_tile;
+  __shared__ __align__(16) uint64_t s_key[kTile];   // the tile in digit order (then its values, as u32)
+  __shared__ uint8_t s_dig[kTile];                  // digit of each staged key
+
   const uint32_t n = *n_ptr;
   const uint32_t tiles = (n + kTile - 1) / kTile;
-  for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
-    for (int i = threadIdx.x; i < kBins; i += kThreads) h[i] = 0;
+  if (threadIdx.x == 0) s_tile = atomicAdd(sc.counter + pass, 1u);
+  for (int i = threadIdx.x; i < kWarps * kBins; i += kThreads) (&wcount[0][0])[i] = 0;
+  __syncthreads();
+  const uint32_t t = s_tile;
+  if (t >= tiles) return;
+  const int shift = 8 * pass;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const uint32_t first = t * kTile;
+  const uint32_t tile_n = min(kTile, n - first);
+
+  // 1. stable ranks within each warp's 512 keys
+  uint64_t key[kRounds];
+  uint32_t val[kValues ? kRounds : 1];
+  uint32_t rank[kRounds];
+#pragma unroll
+  for (int r = 0; r < kRounds; ++r) {             // all loads first: 16 in flight per thread
+    const uint32_t li = tile_index(w, r, lane);
+    key[r] = li < tile_n ? __ldcs(keys + first + li) : 0ull;
+    if constexpr (kValues) val[r] = li < tile_n ? __ldcs(vals + first + li) : 0u;
+  }
+#pragma unroll
+  for (int r = 0; r < kRounds; ++r) {
+    const bool valid = tile_index(w, r, lane) < tile_n;
+    const uint32_t d = valid ? uint32_t((key[r] >> shift) & 0xFFu) : 0xFFFFFFFFu;
+    const unsigned peers = __match_any_sync(0xFFFFFFFFu, d);
+    const uint32_t before = valid ? wcount[w][d] : 0u;
+    rank[r] = before + __popc(peers & ((1u << lane) - 1u));
+    __syncwarp();
+    if (valid && lane == 31 - __clz(peers)) wcount[w][d] = before + __popc(peers);
+    __syncwarp();
+  }
+  __syncthreads();
+
+  // 2. thread d owns digit d: the tile's count, published at once for the successors
+  const int d = threadIdx.x;
+  uint32_t cnt = 0;
+  for (int q = 0; q < kWarps; ++q) {
+    const uint32_t c = wcount[q][d];
+    wcount[q][d] = cnt;                  // the warp's first rank among the tile's keys of digit d
+    cnt += c;
+  }
+  uint64_t* status = sc.status[pass & 1] + size_t(t) * kBins;
+  {
+    const uint64_t word = (t == 0 ? kInclusive : kAggregate) | cnt;
+    __stcg(reinterpret_cast<unsigned long long*>(status + d), (unsigned long long)word);
+  }
+  // the other region is the next pass's: clear this tile's slots (the pass before, which
+  // used it, has finished)
+  __stcg(reinterpret_cast<unsigned long long*>(sc.status[(pass + 1) & 1] + size_t(t) * kBins + d), 0ull);
+  const uint32_t digit_base = block_exclusive_scan(sc.hist[pass * kBins + d], warp_sums);
+  const uint32_t tile_start = block_exclusive_scan(cnt, warp_sums);   // digit d's first staging index
+
+  // 3. decoupled look-back over the preceding tiles for digit d
+  uint32_t excl = 0;
+  if (t > 0) {
+    int64_t j = int64_t(t) - 1;
+    while (j >= 0) {
+      const volatile unsigned long long* src =
+          reinterpret_cast<const volatile unsigned long long*>(sc.status[pass & 1] + size_t(j) * kBins + d);
+      uint64_t v = *src;
+      uint32_t polls = 0;
+      while ((v & kFlagMask) == 0) {
+        if (++polls > kLookbackPolls) break;
+        v = *src;
+      }
+      if ((v & kFlagMask) == 0) { atomicOr(error, 2u); break; }
+      excl += uint32_t(v);
+      if ((v & kFlagMask) == kInclusive) break;
+      --j;
+    }
+    __threadfence();
+    __stcg(reinterpret_cast<unsigned long long*>(status + d), (unsigned long long)(kInclusive | (excl + cnt)));
+  }
+  s_gofs[d] = digit_base + excl - tile_start;
+  for (int q = 0; q < kWarps; ++q) wcount[q][d] += tile_start;
+  __syncthreads();
+
+  // 4. stage the tile in digit order, then write runs of consecutive addresses
+#pragma unroll
+  for (int r = 0; r < kRounds; ++r) {
+    const uint32_t li = tile_index(w, r, lane);
+    if (li < tile_n) {
+      const uint32_t dg = uint32_t((key[r] >> shift) & 0xFFu);
+      const uint32_t p = wcount[w][dg] + rank[r];
+      if (p < kTile) {
+        s_key[p] = key[r];
+        s_dig[p] = uint8_t(dg);
+      }
+    }
+  }
+  __syncthreads();
+  // (a position past n would mean inconsistent counts: recorded as a capacity error, not written)
+  for (uint32_t i = threadIdx.x; i < tile_n; i += kThreads) {
+    const uint32_t g = s_gofs[s_dig[i]] + i;
+    if (g < n) out[g] = s_key[i];
+    else atomicOr(error, 1u);
+  }
+  if constexpr (kValues) {
+    // the values take the same positions, staged in the keys' place
+    uint32_t* s_val = reinterpret_cast<uint32_t*>(s_key);
     __syncthreads();
+#pragma unroll
     for (int r = 0; r < kRounds; ++r) {
-      const uint32_t i = t * kTile + r * kThreads + threadIdx.x;
-      if (i < n) atomicAdd(&h[(keys[i] >> shift) & 0xFFu], 1u);
+      const uint32_t li = tile_index(w, r, lane);
+      if (li < tile_n) {
+        const uint32_t p = wcount[w][(key[r] >> shift) & 0xFFu] + rank[r];
+        if (p < kTile) s_val[p] = val[r];
+      }
     }
     __syncthreads();
-    // digit-major: all tiles of digit 0, then digit 1, ...
-    for (int d = threadIdx.x; d < kBins; d += kThreads) tile_hist[size_t(d) * tiles + t] = h[d];
-    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < tile_n; i += kThreads) {
+      const uint32_t g = s_gofs[s_dig[i]] + i;
+      if (g < n) vout[g] = s_val[i];
+    }
   }
 }
 
 template<bool kValues>
-__global__ void __launch_bounds__(kThreads) digit_scatter_kernel(const uint64_t* keys, const uint32_t* vals,
-                                                                 const uint32_t* n_ptr, int shift,
-                                                                 const uint32_t* offsets, uint64_t* out,
-                                                                 uint32_t* vout)
+cudaError_t onesweep(uint64_t* keys, uint64_t* alt, uint32_t* vals, uint32_t* valt, const uint32_t* n,
+                     uint32_t max_n, int bits, uint32_t* scratch, uint32_t* error, uint64_t** sorted,
+                     uint32_t** sorted_vals, cudaStream_t s)
 {
-  __shared__ uint32_t wcount[kWarps][kBins];     // per-warp running digit counts
-  __shared__ uint32_t wbase[kWarps][kBins];      // exclusive prefix over warps, + tile offset
-  const uint32_t n = *n_ptr;
-  const uint32_t tiles = (n + kTile - 1) / kTile;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
-    for (int i = threadIdx.x; i < kWarps * kBins; i += kThreads) (&wcount[0][0])[i] = 0;
-    __syncthreads();
-    uint64_t key[kRounds];
-    uint32_t val[kValues ? kRounds : 1];
-    uint32_t rank[kRounds];
-#pragma unroll
-    for (int r = 0; r < kRounds; ++r) {
-      const uint32_t i = t * kTile + tile_index(w, r, lane);
-      const bool valid = i < n;
-      key[r] = valid ? keys[i] : 0ull;
-      if constexpr (kValues) val[r] = valid ? vals[i] : 0u;
-      const uint32_t d = valid ? uint32_t((key[r] >> shift) & 0xFFu) : 0xFFFFFFFFu;
-      const unsigned peers = __match_any_sync(0xFFFFFFFFu, d);
-      const uint32_t before = valid ? wcount[w][d] : 0u;
-      rank[r] = before + __popc(peers & ((1u << lane) - 1u));
-      __syncwarp();
-      if (valid && lane == 31 - __clz(peers)) wcount[w][d] = before + __popc(peers);
-      __syncwarp();
-    }
-    __syncthreads();
-    // prefix over the tile's warps per digit, plus the global offset of this tile's digit
-    for (int d = threadIdx.x; d < kBins; d += kThreads) {
-      uint32_t run = offsets[size_t(d) * tiles + t];
-      for (int q = 0; q < kWarps; ++q) {
-        wbase[q][d] = run;
-        run += wcount[q][d];
-      }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int r = 0; r < kRounds; ++r) {
-      const uint32_t i = t * kTile + tile_index(w, r, lane);
-      if (i < n) {
-        const uint32_t p = wbase[w][(key[r] >> shift) & 0xFFu] + rank[r];
-        out[p] = key[r];
-        if constexpr (kValues) vout[p] = val[r];
-      }
-    }
-    __syncthreads();
+  const uint32_t tiles = (max_n + kTile - 1) / kTile;
+  const int passes = (bits + 7) / 8 < 1 ? 1 : ((bits + 7) / 8 > kMaxPasses ? kMaxPasses : (bits + 7) / 8);
+  const SortScratch sc = carve(scratch, tiles);
+  // status region 0 (the first pass's), histograms and tile counters start at zero
+  cudaError_t e = cudaMemsetAsync(sc.status[0], 0, size_t(tiles) * kBins * sizeof(uint64_t), s);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(sc.hist, 0, (kMaxPasses * kBins + kMaxPasses) * sizeof(uint32_t), s);
+  if (e != cudaSuccess) return e;
+  onesweep_hist_kernel<<<grid_for(max_n, kThreads * 16, 4), kThreads, 0, s>>>(keys, n, passes, sc.hist);
+  uint64_t* src = keys;
+  uint64_t* dst = alt;
+  uint32_t* vsrc = vals;
+  uint32_t* vdst = valt;
+  const unsigned grid = tiles < 1 ? 1u : tiles;
+  for (int p = 0; p < passes; ++p) {
+    onesweep_pass_kernel<kValues><<<grid, kThreads, 0, s>>>(src, vsrc, n, p, sc, dst, vdst, error);
+    std::swap(src, dst);
+    if constexpr (kValues) std::swap(vsrc, vdst);
   }
+  *sorted = src;
+  if (sorted_vals) *sorted_vals = vsrc;
+  return cudaGetLastError();
 }
+
+}  // namespace
+
+uint64_t sort_scratch_u32(uint64_t max_n)
+{
+  const uint64_t tiles = (max_n + kTile - 1) / kTile;
+  return 2 * (2 * tiles * kBins) + kMaxPasses * kBins + kMaxPasses + 4;
+}
+
+int sort_launches(int bits)
+{
+  const int passes = (bits + 7) / 8 < 1 ? 1 : ((bits + 7) / 8 > kMaxPasses ? kMaxPasses : (bits + 7) / 8);
+  return 1 + passes;
+}
+
+cudaError_t radix_sort_u64(uint64_t* keys, uint64_t* alt, const uint32_t* n, uint32_t max_n, int bits,
+                           uint32_t* scratch, uint32_t* error, uint64_t** sorted, cudaStream_t s)
+{
+  return onesweep<false>(keys, alt, nullptr, nullptr, n, max_n, bits, scratch, error, sorted, nullptr, s);
+}
+
+cudaError_t radix_sort_u64_values(uint64_t* keys, uint64_t* alt, uint32_t* vals, uint32_t* valt, const uint32_t* n,
+                                  uint32_t max_n, int bits, uint32_t* scratch, uint32_t* error, uint64_t** sorted,
+                                  uint32_t** sorted_vals, cudaStream_t s)
+{
+  return onesweep<true>(keys, alt, vals, valt, n, max_n, bits, scratch, error, sorted, sorted_vals, s);
+}
+
+namespace {
 
 // unique of a sorted array: flag heads, scan, scatter
 __global__ void head_flag_kernel(const uint64_t* keys, const uint32_t* n_ptr, uint32_t* flag)
@@ -156,63 +341,7 @@ __global__ void merge_kernel(const uint64_t* a, const uint8_t* fa, const uint32_
   if (blockIdx.x == 0 && threadIdx.x == 0) *n_out = na + nb;
 }
 
-__global__ void set_u32_kernel(uint32_t* p, uint32_t v) { *p = v; }
-
 }  // namespace
-
-uint64_t sort_scratch_u32(uint64_t max_n)
-{
-  const uint64_t tiles = (max_n + kTile - 1) / kTile;
-  return tiles * kBins + 1;
-}
-
-cudaError_t radix_sort_u64(uint64_t* keys, uint64_t* alt, const uint32_t* n, uint32_t max_n, int bits,
-                           uint32_t* hist, uint32_t* offsets, uint32_t* scan_tiles, uint32_t* count_tmp,
-                           uint64_t** sorted, cudaStream_t s)
-{
-  // *n must equal max_n: the digit-major table has 256 x tiles(max_n) cells, and
-  // count_tmp[0] tells the scan how many
-  const uint32_t tiles = (max_n + kTile - 1) / kTile;
-  set_u32_kernel<<<1, 1, 0, s>>>(count_tmp, tiles * kBins);
-  const int g = grid_for(uint64_t(tiles) * kTile, kTile, 4);
-  uint64_t* src = keys;
-  uint64_t* dst = alt;
-  for (int shift = 0; shift < bits; shift += 8) {
-    digit_hist_kernel<<<g, kThreads, 0, s>>>(src, n, shift, hist);
-    cudaError_t e = exclusive_scan_u32(hist, offsets, count_tmp, scan_tiles, uint32_t(tiles) * kBins, s);
-    if (e != cudaSuccess) return e;
-    digit_scatter_kernel<false><<<g, kThreads, 0, s>>>(src, nullptr, n, shift, offsets, dst, nullptr);
-    uint64_t* t = src;
-    src = dst;
-    dst = t;
-  }
-  *sorted = src;
-  return cudaGetLastError();
-}
-
-cudaError_t radix_sort_u64_values(uint64_t* keys, uint64_t* alt, uint32_t* vals, uint32_t* valt, const uint32_t* n,
-                                  uint32_t max_n, int bits, uint32_t* hist, uint32_t* offsets, uint32_t* scan_tiles,
-                                  uint32_t* count_tmp, uint64_t** sorted, uint32_t** sorted_vals, cudaStream_t s)
-{
-  const uint32_t tiles = (max_n + kTile - 1) / kTile;
-  set_u32_kernel<<<1, 1, 0, s>>>(count_tmp, tiles * kBins);
-  const int g = grid_for(uint64_t(tiles) * kTile, kTile, 4);
-  uint64_t* src = keys;
-  uint64_t* dst = alt;
-  uint32_t* vsrc = vals;
-  uint32_t* vdst = valt;
-  for (int shift = 0; shift < bits; shift += 8) {
-    digit_hist_kernel<<<g, kThreads, 0, s>>>(src, n, shift, hist);
-    cudaError_t e = exclusive_scan_u32(hist, offsets, count_tmp, scan_tiles, uint32_t(tiles) * kBins, s);
-    if (e != cudaSuccess) return e;
-    digit_scatter_kernel<true><<<g, kThreads, 0, s>>>(src, vsrc, n, shift, offsets, dst, vdst);
-    std::swap(src, dst);
-    std::swap(vsrc, vdst);
-  }
-  *sorted = src;
-  *sorted_vals = vsrc;
-  return cudaGetLastError();
-}
 
 cudaError_t unique_sorted_u64(const uint64_t* keys, const uint32_t* n, uint32_t max_n, uint64_t* out, uint32_t* n_out,
                               uint32_t* flag, uint32_t* pos, uint32_t* scan_tiles, cudaStream_t s)

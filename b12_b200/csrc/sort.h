@@ -6,21 +6,24 @@
 
 namespace b12g {
 
-// u32 cells of the digit table (hist and offsets each) for up to max_n keys
+// u32 cells of the sort's scratch (look-back status words, digit histograms, tile
+// counters) for up to max_n keys; the scratch must be 8-byte aligned
 uint64_t sort_scratch_u32(uint64_t max_n);
 
-// sort the low `bits` bits of *n == max_n keys; the result is in keys or alt
-// (*sorted tells which).  hist, offsets: sort_scratch_u32(max_n) u32 each; scan_tiles:
-// compact_tiles(sort_scratch_u32(max_n)) + 2 u32; count_tmp: 1 u32.
+// kernel launches of one sort of `bits` bits (the histogram pass + one pass a digit)
+int sort_launches(int bits);
+
+// onesweep sort of the low `bits` bits of *n <= max_n keys; the result is in keys or alt
+// (*sorted tells which).  scratch: sort_scratch_u32(max_n) u32.  A look-back that gives
+// up sets bit 2 of *error (the result is then not sorted).
 cudaError_t radix_sort_u64(uint64_t* keys, uint64_t* alt, const uint32_t* n, uint32_t max_n, int bits,
-                           uint32_t* hist, uint32_t* offsets, uint32_t* scan_tiles, uint32_t* count_tmp,
-                           uint64_t** sorted, cudaStream_t s);
+                           uint32_t* scratch, uint32_t* error, uint64_t** sorted, cudaStream_t s);
 
 // the same with a u32 value per key moved along (stable); *sorted_vals tells where the
 // values ended up (vals or valt)
 cudaError_t radix_sort_u64_values(uint64_t* keys, uint64_t* alt, uint32_t* vals, uint32_t* valt, const uint32_t* n,
-                                  uint32_t max_n, int bits, uint32_t* hist, uint32_t* offsets, uint32_t* scan_tiles,
-                                  uint32_t* count_tmp, uint64_t** sorted, uint32_t** sorted_vals, cudaStream_t s);
+                                  uint32_t max_n, int bits, uint32_t* scratch, uint32_t* error, uint64_t** sorted,
+                                  uint32_t** sorted_vals, cudaStream_t s);
 
 // distinct values of a sorted array, in order; flag and pos: max_n + 1 u32
 cudaError_t unique_sorted_u64(const uint64_t* keys, const uint32_t* n, uint32_t max_n, uint64_t* out, uint32_t* n_out,

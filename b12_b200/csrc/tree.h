@@ -136,6 +136,7 @@ struct b12g_tree {
   Buf<uint32_t> ins_idx[2], ins_pos, ins_head;
   Buf<uint32_t> isrc_head, isrc_pos, isrc_and, isrc;   // scheme sources at an inner depth
   Buf<ulonglong2> hash;        // leaf lookup table
+  Buf<uint64_t> pk;            // the leaves' packed per-dimension indices (the table's keys)
   uint32_t hash_tag = 0;       // tag of the last build (1..255; 0 = cleared)
   uint32_t hash_log2 = 0;      // log2 of the table's slots
   uint32_t* h_ctr = nullptr;   // pinned mirror of ctr

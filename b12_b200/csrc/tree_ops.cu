@@ -134,7 +134,11 @@ __global__ void split_kernel(const uint64_t* code, const uint8_t* flags, const u
 // that loses to another insert re-reads the same slot (which now carries the current
 // tag) and moves on, so every insert ends within the table size
 // ---------------------------------------------------------------------------------
-__global__ void hash_build_kernel(const uint64_t* codes, const uint32_t* n_ptr, LeafHash h, uint32_t* error)
+// The keys are the leaves' packed per-dimension indices (pack_bits at `depth`), also
+// written to h.pk for the image kernels.
+template<int D>
+__global__ void hash_build_kernel(const uint64_t* codes, const uint32_t* n_ptr, int depth, LeafHash h,
+                                  uint32_t* error)
 {
   const uint32_t n = *n_ptr;
   const int l = hash_log2(n);
@@ -145,8 +149,13 @@ __global__ void hash_build_kernel(const uint64_t* codes, const uint32_t* n_ptr, 
   const uint64_t mask = (1ull << l) - 1ull;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const uint64_t code = codes[i];
-    const unsigned long long key = (uint64_t(h.tag) << 56) | code;
-    uint64_t s = hash_slot(code, l);
+    uint32_t bits[D];
+#pragma unroll
+    for (int j = 0; j < D; ++j) bits[j] = deinterleave<D>(code, depth, j);
+    const uint64_t pk = pack_bits<D>(bits, depth);
+    h.pk[i] = pk;
+    const unsigned long long key = (uint64_t(h.tag) << 56) | pk;
+    uint64_t s = hash_slot(pk, l);
     bool done = false;
     for (uint64_t step = 0; step <= 2 * mask + 64 && !done; ++step) {
       unsigned long long* kw = reinterpret_cast<unsigned long long*>(&h.slots[s].x);
@@ -433,10 +442,16 @@ cudaError_t split_codes(const uint64_t* code, const uint8_t* flags, const uint32
   return cudaGetLastError();
 }
 
-cudaError_t build_leaf_hash(const uint64_t* codes, const uint32_t* n, LeafHash h, uint32_t* error, uint32_t max_n,
-                            cudaStream_t s)
+cudaError_t build_leaf_hash(const uint64_t* codes, const uint32_t* n, int depth, int dim, LeafHash h, uint32_t* error,
+                            uint32_t max_n, cudaStream_t s)
 {
-  hash_build_kernel<<<grid_for(max_n, kThreads, 8), kThreads, 0, s>>>(codes, n, h, error);
+  const int g = grid_for(max_n, kThreads, 8);
+  switch (dim) {
+    case 2: hash_build_kernel<2><<<g, kThreads, 0, s>>>(codes, n, depth, h, error); break;
+    case 3: hash_build_kernel<3><<<g, kThreads, 0, s>>>(codes, n, depth, h, error); break;
+    case 4: hash_build_kernel<4><<<g, kThreads, 0, s>>>(codes, n, depth, h, error); break;
+    default: return cudaErrorInvalidValue;
+  }
   return cudaGetLastError();
 }
 

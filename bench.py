@@ -12,9 +12,17 @@ matrix equal the reference's strict (-fmad=false) run at every step on this work
 The strict integrator - one rounding per operation, the reference's own Map_Lorenz.h
 order - is measured in the same run and reported under "strict".
 
-metric = box-images per second (a box-image is one box's 125 test points sampled,
-integrated and located): the subdivision steps image 2*n(k-1) boxes each, the transition
-matrix n(27).  Inputs are synthetic: the workload is defined entirely by its parameters.
+metric = box-images per second of whole-job time (a box-image is one box's 125 test
+points sampled, integrated and located): the subdivision steps image 2*n(k-1) boxes each.
+The transition matrix is assembled from the targets the last step stored, so its
+n(27) boxes are not imaged again and are not counted (the job's time includes it).
+Inputs are synthetic: the workload is defined entirely by its parameters.
+
+The reference arm (--impl reference) runs the reference's own Thrust code (OMP backend,
+all host cores) on a bounded sample of the same job: subdivision step 25 from the
+depth-24 tree the reference itself saved, then transitionMatrixForLeaves on the
+depth-25 tree, timed per round; its value is that step's box-images over the step's and
+the matrix's time.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -118,8 +126,8 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------------------ CPU arms
-def reference_binary():
-    exe = os.path.join(REPO, "oracle", "_ref", "ref_lorenz")
+def ref_exe(name: str):
+    exe = os.path.join(REPO, "oracle", "_ref", name)
     return exe if os.path.exists(exe) else None
 
 
@@ -130,68 +138,108 @@ def cpu_cores() -> int:
         return os.cpu_count() or 1
 
 
-def run_reference_sample(steps: int, buf: int, threads: int):
-    """The reference's own Thrust code (OMP backend) on the Lorenz subdivision loop."""
-    exe = reference_binary()
+def run_ref(name: str, args, threads: int) -> dict:
+    """One run of a reference harness binary; its JSON line (the harness times itself,
+    so process start-up and file writes are outside every figure)."""
     env = dict(os.environ, OMP_NUM_THREADS=str(threads))
-    res = subprocess.run([exe, "--steps", str(steps), "--buf", str(buf), "--tm", "0"], env=env, check=True,
-                         capture_output=True, text=True)
-    rec = json.loads(res.stdout.strip().splitlines()[-1])
-    return rec["box_images"], rec["subdivision_s"], rec
+    res = subprocess.run([ref_exe(name)] + [str(x) for x in args], env=env, check=True, capture_output=True,
+                         text=True)
+    return json.loads(res.stdout.strip().splitlines()[-1])
 
 
-def run_port_sample(steps: int):
-    """The oracle restatement (OpenMP C) on the same loop, when the reference build is absent."""
+REF_FROM_DEPTH = 24              # the reference arm's rounds start from the saved depth-24 tree
+REF_BUF = 1 << 30                # nHostBufferBytes for Lorenz (the reference's default is 4 GiB)
+REF_SMALL_BUF = 64 << 20         # for Henon and forced Duffing
+
+
+class ReferenceLorenz:
+    """The reference's Lorenz job on a bounded sample: the reference saves its own
+    depth-24 tree once (untimed); a round loads it, runs subdivision step 25 and
+    transitionMatrixForLeaves of the depth-25 tree."""
+
+    def __init__(self, threads: int):
+        import tempfile
+        self.threads = threads
+        self.dir = tempfile.mkdtemp(prefix="b12_ref_")
+        base = os.path.join(self.dir, "d24")
+        run_ref("ref_lorenz", ["--steps", REF_FROM_DEPTH, "--tm", 0, "--buf", REF_BUF, "--save", base], threads)
+        self.tree = base + "_tree.json"
+
+    def rounds(self, n: int) -> list:
+        rec = run_ref("ref_lorenz", ["--load", self.tree, "--steps", 1, "--tm", 1, "--buf", REF_BUF,
+                                     "--repeat", n], self.threads)
+        return rec["rounds"]          # [subdivision s, matrix s, box-images, leaves, nonzeros]
+
+    def close(self):
+        import shutil
+        shutil.rmtree(self.dir, ignore_errors=True)
+
+    def sample_text(self, r) -> str:
+        return (f"Lorenz subdivision step {REF_FROM_DEPTH + 1} from the depth-{REF_FROM_DEPTH} tree the reference "
+                f"saved ({r[2]} box-images, {r[0]:.2f} s) + transitionMatrixForLeaves on its {r[3]} boxes "
+                f"({r[4]} nonzeros, {r[1]:.2f} s); strict arithmetic (the reference's own Map_Lorenz.h); "
+                f"nHostBufferBytes {REF_BUF >> 20} MiB; Thrust OMP backend; the reference has no invariant measure")
+
+
+def run_port_sample():
+    """The oracle restatement (OpenMP C) on the same sample, when the reference build is absent:
+    step 25 from its own depth-24 tree, then the transition matrix."""
     from oracle import oracle as O
     o = O.Oracle(O.lorenz_spec())
+    o.subdivision(REF_FROM_DEPTH)
     t0 = time.perf_counter()
-    _, bi = o.subdivision(steps)
-    return bi, time.perf_counter() - t0, {}
-
-
-CPU_SAMPLE_STEPS = 24
-CPU_SAMPLE_BUF = 1 << 30
+    _, bi = o.subdivision(1)
+    t1 = time.perf_counter()
+    rowptr, _, _, _ = o.transition_matrix()
+    t2 = time.perf_counter()
+    return [t1 - t0, t2 - t1, bi, len(rowptr) - 1, int(rowptr[-1])]
 
 
 def cpu_baseline(threads: int):
-    if reference_binary():
-        bi, sec, _ = run_reference_sample(CPU_SAMPLE_STEPS, CPU_SAMPLE_BUF, threads)
+    if ref_exe("ref_lorenz"):
+        ref = ReferenceLorenz(threads)
+        try:
+            r = ref.rounds(2)[-1]
+            text = ref.sample_text(r)
+        finally:
+            ref.close()
         kind = "reference"
     else:
         from oracle import oracle as O
         threads = O.lib().orc_num_threads()
-        bi, sec, _ = run_port_sample(CPU_SAMPLE_STEPS)
+        r = run_port_sample()
         kind = "port"
-    return {"value": bi / sec, "unit": UNIT, "cores": threads, "kind": kind,
-            "sample": f"Lorenz subdivision steps 1-{CPU_SAMPLE_STEPS} ({bi} box-images, {sec:.2f} s"
-                      + (f", nHostBufferBytes {CPU_SAMPLE_BUF >> 20} MiB, OMP backend)" if kind == "reference"
-                         else ", OpenMP C restatement)")}
+        text = f"Lorenz step {REF_FROM_DEPTH + 1} + transition matrix, OpenMP C restatement"
+    return {"value": r[2] / (r[0] + r[1]), "unit": UNIT, "cores": threads, "kind": kind, "sample": text}
 
 
 def reference_arm(args, rank: int, world: int):
     if rank != 0:
         return 0
     threads = cpu_cores()
-    kind = "reference" if reference_binary() else "port"
-    samples = []
-    for i in range(args.warmup + args.steps):
-        if kind == "reference":
-            bi, sec, _ = run_reference_sample(CPU_SAMPLE_STEPS, CPU_SAMPLE_BUF, threads)
-        else:
-            bi, sec, _ = run_port_sample(CPU_SAMPLE_STEPS)
-        if i >= args.warmup:
-            samples.append((bi, sec))
-    tot_bi = sum(s[0] for s in samples)
-    tot_s = sum(s[1] for s in samples)
+    if ref_exe("ref_lorenz"):
+        kind = "reference"
+        ref = ReferenceLorenz(threads)
+        try:
+            rounds = ref.rounds(args.warmup + args.steps)[args.warmup:]
+            text = ref.sample_text(rounds[0])
+        finally:
+            ref.close()
+    else:
+        kind = "port"
+        rounds = [run_port_sample() for _ in range(args.warmup + args.steps)][args.warmup:]
+        text = f"Lorenz step {REF_FROM_DEPTH + 1} + transition matrix, OpenMP C restatement"
+    tot_bi = sum(r[2] for r in rounds)
+    tot_s = sum(r[0] + r[1] for r in rounds)
     value = tot_bi / tot_s
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * tot_s / len(samples), "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": 1e3 * tot_s / len(rounds), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": dict(CONFIG, sample=f"subdivision steps 1-{CPU_SAMPLE_STEPS} per step"),
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
-                             "sample": f"Lorenz subdivision steps 1-{CPU_SAMPLE_STEPS} per step, "
-                                       f"{tot_bi // len(samples)} box-images, nHostBufferBytes "
-                                       f"{CPU_SAMPLE_BUF >> 20} MiB, Thrust OMP backend"},
+            "config": dict(CONFIG, arith="strict", measure_iters=0,
+                           sample=f"per step: subdivision step {REF_FROM_DEPTH + 1} + transition matrix "
+                                  f"(the job's most expensive regime; steps 25-27 and the matrix are most of "
+                                  f"the reference's whole job)"),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": text},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -229,7 +277,7 @@ def measure_mode(args, rank, world, dist, fma: bool, peak_tflops: float):
     for _ in range(args.warmup):
         counts = job()
     bi_sub, n_final = box_images_of(counts)
-    box_images = bi_sub + n_final
+    box_images = bi_sub          # imaged boxes only: the matrix's rows come from stored targets
 
     # phase breakdown of one job (host clock around the synchronous API calls)
     torch.cuda.synchronize()
@@ -357,7 +405,7 @@ def gpu_arm(args, rank: int, world: int, dist):
                 "config": dict(CONFIG, arith=arith,
                                parallelism=f"{world} independent jobs" if world > 1 else "1 job",
                                box_images_per_step=main["box_images"], final_boxes=main["n_final"],
-                               nnz=main["nnz"]),
+                               matrix_boxes_not_counted=main["n_final"], nnz=main["nnz"]),
                 "e2e": main["e2e"], "gpu_launches": int(main["launches"]), "roofline": main["roofline"],
                 "clocks": main["clocks"], "cpu_baseline": cpu, "phases_ms": main["phases"],
                 "counts": main["counts"]}
@@ -390,10 +438,13 @@ def _timed(fn, reps: int):
 
 def configs_mode(args, peak_tflops: float):
     """The Henon validity workload, the coupled-Duffing continuation and the 512-instance
-    Lorenz scan, each timed on its own after a warm-up call."""
+    Lorenz scan, each timed on its own after a warm-up call, each beside the reference's
+    own code on a stated sample (all host cores)."""
     import b12_b200 as B
     from b12_b200.workloads import LORENZ_CENTER, LORENZ_RADIUS, lorenz_scan
 
+    threads = cpu_cores()
+    cpu = not args.no_cpu and all(ref_exe(x) for x in ("ref_henon", "ref_lorenz", "ref_duffing"))
     out = {}
     # Henon a=1.4 b=0.3, 20 steps, 4x4 inner grid, CSR
     sc = B.Scheme(B.henon(1.4, 0.3), B.inner_grid(4))
@@ -409,7 +460,17 @@ def configs_mode(args, peak_tflops: float):
 
     sec, (c, nnz) = _timed(henon, 5)
     bi, nf = box_images_of(c)
-    out["henon_d20"] = {"boxes": nf, "nnz": nnz, "ms_per_job": 1e3 * sec, "box_images_per_s": (bi + nf) / sec}
+    out["henon_d20"] = {"boxes": nf, "nnz": nnz, "ms_per_job": 1e3 * sec, "box_images_per_s": bi / sec,
+                        "note": "imaged boxes of the 20 steps per second of job time (the matrix comes from "
+                                "the last step's stored targets)"}
+    if cpu:
+        rec = run_ref("ref_henon", ["--steps", 20, "--tm", 1, "--buf", REF_SMALL_BUF], threads)
+        job_s = rec["subdivision_s"] + rec["tm_s"]
+        out["henon_d20"]["cpu_baseline"] = {
+            "value": rec["box_images"] / job_s, "unit": UNIT, "cores": threads, "kind": "reference",
+            "ms_per_job": 1e3 * job_s, "boxes": rec["steps"][-1][1], "nnz": rec["nnz"],
+            "sample": f"the whole job: 20 steps + transitionMatrixForLeaves, nHostBufferBytes {REF_SMALL_BUF >> 20} "
+                      "MiB, Thrust OMP backend"}
     t.close()
 
     # coupled Duffing, unstable-manifold continuation at depth 24 from the box of the origin,
@@ -424,6 +485,15 @@ def configs_mode(args, peak_tflops: float):
         "boxes": n, "sweeps": len(sweeps), "seconds": sec, "box_images": n,
         "box_images_per_s": n / sec, "tflops": n * flop / sec / 1e12, "flop_per_box_image": flop,
         "note": "every box is imaged once, in the sweep after it was inserted"}
+    if cpu:
+        sweeps_ref = 20
+        rec = run_ref("ref_duffing", ["--steps", 24, "--buf", REF_BUF, "--max-sweeps", sweeps_ref], threads)
+        out["coupled_duffing_continuation_d24"]["cpu_baseline"] = {
+            "value": rec["box_images"] / rec["continuation_s"], "unit": UNIT, "cores": threads, "kind": "reference",
+            "seconds": rec["continuation_s"], "box_images": rec["box_images"],
+            "boxes_after_sample": rec["sweeps"][-1][1],
+            "sample": f"sweeps 1-{sweeps_ref} of the same depth-24 continuation (of 49), nHostBufferBytes "
+                      f"{REF_BUF >> 20} MiB, Thrust OMP backend"}
     t.close()
 
     # selective refinement (leaves of several depths): Lorenz (explicit FMA) refined to
@@ -481,6 +551,22 @@ def configs_mode(args, peak_tflops: float):
         peak_tflops, "launch_shape": {k: info[k] for k in ("threads", "points_per_thread", "chunk")},
         "frac_note": "whole batched run (every kernel of the 27 steps) against the measured FP64 peak"}
     b.close()
+    if cpu:
+        # the reference runs one instance after another; sample: the first instances in
+        # scan order of depth <= 22 (deeper ones skipped, which favours the reference)
+        picked = [i for i in range(512) if depth[i] <= 22][:3]
+        bi_ref, sec_ref = 0, 0.0
+        for i in picked:
+            rec = run_ref("ref_lorenz", ["--steps", depth[i], "--tm", 1, "--rho", repr(rho[i]), "--buf", REF_BUF],
+                          threads)
+            bi_ref += rec["box_images"] + rec["tm_box_images"]
+            sec_ref += rec["subdivision_s"] + rec["tm_s"]
+        out["lorenz_batch_512"]["cpu_baseline"] = {
+            "value": bi_ref / sec_ref, "unit": UNIT, "cores": threads, "kind": "reference",
+            "seconds": sec_ref, "box_images": bi_ref,
+            "sample": f"instances {picked} of the scan (depths {[depth[i] for i in picked]}) run one at a time, "
+                      f"27-step loop to each depth + transitionMatrixForLeaves, strict arithmetic (the reference's "
+                      f"Map_Lorenz.h), nHostBufferBytes {REF_BUF >> 20} MiB, Thrust OMP backend"}
     return out
 
 
@@ -489,6 +575,37 @@ SERVE_RATES = (500.0, 1000.0, 2000.0)
 SERVE_TIMEOUT = 300.0            # seconds per replayed stream before the bench gives up
 SERVE_DIGEST_EVERY = 10          # full-result digests on every 10th job; counts and nnz on all
 SERVE_CAP = 150 * 10**9
+SERVE_FRESH_JOBS = 2000          # jobs of the fresh-tree plain path (a prefix of the stream)
+SERVE_CPU_SECONDS = 8.0          # reference sample: jobs in arrival order until this much CPU time
+
+
+def serve_cpu_baseline(base):
+    """The reference running served-stream jobs one at a time (its only way): jobs in
+    arrival order, Lorenz jobs deeper than 22 skipped (which favours the reference), until
+    SERVE_CPU_SECONDS of job time; each job is the subdivision loop + transitionMatrixForLeaves."""
+    threads = cpu_cores()
+    done, sec, fams = 0, 0.0, {}
+    for job in base:
+        fam, p, d = job["family"], job["params"], job["depth"]
+        if fam == "henon":
+            rec = run_ref("ref_henon", ["--steps", d, "--tm", 1, "--a", repr(p[0]), "--b", repr(p[1]),
+                                        "--buf", REF_SMALL_BUF], threads)
+        elif fam == "lorenz":
+            if d > 22:
+                continue
+            rec = run_ref("ref_lorenz", ["--steps", d, "--tm", 1, "--rho", repr(p[1]), "--buf", REF_BUF], threads)
+        else:
+            rec = run_ref("ref_forced", ["--steps", d, "--tm", 1, "--buf", REF_SMALL_BUF], threads)
+        sec += rec["subdivision_s"] + rec["tm_s"]
+        done += 1
+        fams[fam] = fams.get(fam, 0) + 1
+        if sec >= SERVE_CPU_SECONDS:
+            break
+    return {"value": done / sec, "unit": "jobs/s", "cores": threads, "kind": "reference", "jobs": done,
+            "seconds": sec, "sample": f"the first {done} jobs of the stream in arrival order ({fams}), Lorenz "
+                                      "jobs deeper than 22 skipped; one job at a time; Lorenz in strict arithmetic "
+                                      f"(the reference's Map_Lorenz.h); nHostBufferBytes {REF_SMALL_BUF >> 20} MiB "
+                                      f"(Henon, forced Duffing) / {REF_BUF >> 20} MiB (Lorenz); Thrust OMP backend"}
 
 
 def _job_digest(codes, counts, rowptr, cols, vals) -> str:
@@ -524,18 +641,36 @@ def serve_mode(args):
     base = job_stream(n, 1.0, 0)          # family, parameters, depth of every job (seed 0)
     fams = [j["family"] for j in base]
 
+    # the plain path: one job at a time through the single-tree API, one tree handle
+    # per family reused across jobs (delete_depth(0) resets it; the matrix is refilled in
+    # place), as the integration notes recommend
+    trees = {}
+
     def plain_job(job):
+        c, r, mp, g, d = stream_job_args(job)
+        ent = trees.get(job["family"])
+        if ent is None:
+            ent = trees[job["family"]] = [T.ImplicitBoxTree(c, r), None]
+        t = ent[0]
+        t.delete_depth(0)
+        sc = T.Scheme(mp, g)
+        counts = t.subdivision_run(sc, d)
+        ent[1] = t.transition_matrix(sc, into=ent[1])
+        return t, counts, ent[1]
+
+    def fresh_job(job):
         c, r, mp, g, d = stream_job_args(job)
         t = T.ImplicitBoxTree(c, r)
         sc = T.Scheme(mp, g)
-        counts = t.subdivision_run(sc, d)
-        return t, counts, t.transition_matrix(sc)
-
-    # plain path: warm-up on other jobs, then every job timed on its own
-    for job in job_stream(6, 1.0, 1):
-        t, _, m = plain_job(job)
+        t.subdivision_run(sc, d)
+        m = t.transition_matrix(sc)
         m.close()
         t.close()
+
+    # warm-up on other jobs, then every job timed on its own
+    for job in job_stream(6, 1.0, 1):
+        plain_job(job)
+        fresh_job(job)
     service, plain_digest, plain_shape = [], {}, []
     for k, job in enumerate(base):
         t0 = time.perf_counter()
@@ -545,16 +680,33 @@ def serve_mode(args):
         if k % SERVE_DIGEST_EVERY == 0:
             rowptr, cols, vals = m.to_host()
             plain_digest[k] = _job_digest(t.leaves()[0], np.asarray(counts, np.uint32), rowptr, cols, vals)
-        m.close()
+    for t, m in trees.values():
+        if m is not None:
+            m.close()
         t.close()
     plain_rate = n / sum(service)
+    # the same path with a new tree per job (allocations, graph instantiation), on a prefix
+    n_fresh = min(n, SERVE_FRESH_JOBS)
+    t0 = time.perf_counter()
+    for job in base[:n_fresh]:
+        fresh_job(job)
+    fresh_s = time.perf_counter() - t0
 
     out = {"workload": f"served stream of {n} jobs (seed 0): Henon a~U[1.0,1.4] depth 14-22, Lorenz "
                        "rho~U[15,35] depth 18-27, forced Duffing depth 16-22, uniform family mix",
            "jobs": n, "hbm_cap_bytes": SERVE_CAP,
            "plain": {"jobs_per_s": plain_rate, "service_ms_mean": 1e3 * sum(service) / n,
                      "per_family_ms": {f: 1e3 * float(np.mean([s for s, g in zip(service, fams) if g == f]))
-                                       for f in sorted(set(fams))}}}
+                                       for f in sorted(set(fams))},
+                     "path": "one job at a time, one reused tree handle per family (delete_depth(0) between "
+                             "jobs, matrix refilled in place)"},
+           "plain_fresh_tree": {"jobs_per_s": n_fresh / fresh_s, "jobs": n_fresh,
+                                "reused_handle_jobs_per_s_same_jobs": n_fresh / sum(service[:n_fresh]),
+                                "path": "a new ImplicitBoxTree per job (first jobs of the stream)"}}
+    if args.no_cpu or not all(ref_exe(x) for x in ("ref_henon", "ref_lorenz", "ref_forced")):
+        pass
+    else:
+        out["cpu_baseline"] = serve_cpu_baseline(base)
     with JobServer(SERVE_CAP) as srv:
         # warm-up on a burst of other jobs: engines created, buffers and the result pool grown
         warm = [dict(j, arrival=0.0) for j in job_stream(min(n, 1000), 1.0, 1)]
@@ -588,6 +740,8 @@ def serve_mode(args):
                                      "full_result_sha256": f"{same}/{len(plain_digest)}",
                                      "pass": "a second, untimed saturated burst whose results are read back"}
         out["jobs_per_s_vs_plain"] = out["served_saturated"]["jobs_per_s"] / plain_rate
+        out["jobs_per_s_vs_plain_fresh_tree"] = out["served_saturated"]["jobs_per_s"] / out["plain_fresh_tree"][
+            "jobs_per_s"]
         sweep = []
         for rate in SERVE_RATES:
             st = job_stream(n, rate, 0)

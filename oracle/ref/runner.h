@@ -38,6 +38,10 @@ struct RunOpts
                               // CooMatrix.hpp:473-525) to SAVE_tree.json / SAVE_tm.json
   int mixed = 0;              // steps of selective refinement after the uniform steps (mixed leaf depths)
   int edits = 0;              // 1: unsubdivide / insert edits of the mixed tree afterwards (runEdits)
+  std::string load;           // start from a tree the reference saved (ImplicitBoxTree(fileName),
+                              // ImplicitBoxTree.hpp:144-359) instead of the surrounding box (runFromFile)
+  int repeat = 1;             // runFromFile: load + steps + matrix this many times, each timed
+  int maxSweeps = 0;          // continuation: stop after this many sweeps (0 = until the count stops growing)
 };
 
 inline RunOpts parseOpts(int argc, char** argv)
@@ -51,6 +55,9 @@ inline RunOpts parseOpts(int argc, char** argv)
   o.save = arg(argc, argv, "--save", "");
   o.mixed = std::atoi(arg(argc, argv, "--mixed", "0"));
   o.edits = std::atoi(arg(argc, argv, "--edits", "0"));
+  o.load = arg(argc, argv, "--load", "");
+  o.repeat = std::atoi(arg(argc, argv, "--repeat", "1"));
+  o.maxSweeps = std::atoi(arg(argc, argv, "--max-sweeps", "0"));
   return o;
 }
 
@@ -280,6 +287,44 @@ int runSubdivision(const std::vector<double>& c, const std::vector<double>& r,
   return 0;
 }
 
+// The subdivision loop and the transition matrix from a tree the reference saved: each
+// of o.repeat rounds constructs the tree from the file (untimed), then times o.steps
+// steps (subdivide(SD), image flags, remove, unset) and transitionMatrixForLeaves.
+// One JSON line: per round [subdivision s, matrix s, box-images, leaves, nonzeros].
+template<b12::Dimension DIM, class Grid, class Map>
+int runFromFile(Grid grid, Map map, const RunOpts& o, const std::string& name)
+{
+  using namespace b12;
+  std::ostringstream js;
+  js << "{\"workload\": \"" << name << "\", \"buf\": " << o.buf << ", \"load\": \"" << o.load << "\", \"rounds\": [";
+  for (int rep = 0; rep < o.repeat; ++rep) {
+    ImplicitBoxTree<OMP, DIM, double, 64> ibt(o.load);
+    ibt.setNHostBufferBytes(o.buf);
+    uint64_t boxImages = 0;
+    auto t0 = clk::now();
+    for (int i = 1; i <= o.steps; ++i) {
+      ibt.subdivide(Flag::SD);
+      boxImages += ibt.count(getLeafDepth());
+      auto itPair = ibt.makePointIteratorPairOverLeaves(grid, map);
+      ibt.setFlagsByIterators(itPair, Flag::HIT, getLeafDepth());
+      ibt.remove(Flag::HIT);
+      ibt.unsetFlags(Flag::HIT, getLeafDepth());
+    }
+    auto t1 = clk::now();
+    uint64_t nnz = 0;
+    if (o.tm) {
+      auto P = ibt.template transitionMatrixForLeaves<double>(grid, map, o.tm == 2, true, o.tm == 3);
+      nnz = P.values_.size();
+    }
+    auto t2 = clk::now();
+    js << (rep ? ", " : "") << "[" << secs(t0, t1) << ", " << secs(t1, t2) << ", " << boxImages << ", "
+       << ibt.count(getLeafDepth()) << ", " << nnz << "]";
+  }
+  js << "]}";
+  std::cout << js.str() << std::endl;
+  return 0;
+}
+
 // Continuation of an unstable manifold at one depth (continuation.m:13-44).
 template<b12::Dimension DIM, class Grid, class Map>
 int runContinuation(const std::vector<double>& c, const std::vector<double>& r, const std::vector<double>& x0,
@@ -301,7 +346,7 @@ int runContinuation(const std::vector<double>& c, const std::vector<double>& r, 
   uint64_t boxImages = 0;
   int k = 0;
   if (!o.out.empty()) dumpLeaves(ibt, o.out + "/cont_00.bin");
-  while (nb1 > nb0) {
+  while (nb1 > nb0 && (o.maxSweeps <= 0 || k < o.maxSweeps)) {
     auto a = clk::now();
     boxImages += ibt.changeFlags(Flag::INS, Flag::EXPD, d);
     ibt.insertByIterators(ibt.makePointIteratorPairByFlags(d, Flag::EXPD, grid, map), d, Flag::INS, Flag::NONE);

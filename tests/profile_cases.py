@@ -1,6 +1,7 @@
-"""Single workloads sized for an ncu capture of one kernel family on one GPU.
+"""Single workloads sized for an ncu capture of one kernel family on one GPU (profiling
+infrastructure, not part of the library).
 
-    python -m b12_b200.profile_cases <case> [options]
+    python tests/profile_cases.py <case> [options]
 
 image     a Lorenz tree subdivided to --depth - 1 (default 23), then one subdivide and
           one set_flags_by_image with the strict and one with the explicit-FMA integrator:
@@ -22,7 +23,11 @@ Every case prints one line of sizes; none writes files.
 from __future__ import annotations
 
 import argparse
+import os
+import sys
 import time
+
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 
 import numpy as np
 
