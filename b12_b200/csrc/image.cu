@@ -26,7 +26,9 @@ struct PointImage {
       if (a.children) {
         unpack_bits<D>(__ldg(a.hash.pk + (leaf >> 1)), a.depth - 1, bits);
         const int jd = (a.depth - 1) % D;          // the last bisection splits dimension jd
-        bits[jd] = (bits[jd] << 1) | (leaf & 1u);
+#pragma unroll
+        for (int j = 0; j < D; ++j)                // (no dynamic index: the array stays in registers)
+          if (j == jd) bits[j] = (bits[j] << 1) | (leaf & 1u);
       } else {
         unpack_bits<D>(__ldg(a.hash.pk + leaf), a.depth, bits);
       }
@@ -75,11 +77,14 @@ struct PointImage {
     if (!a.children) return find_leaf_bits<D>(a.hash, a.codes, n, valid, tbits, a.depth);
     if (!valid) return kInvalidIndex;
     const int jd = (a.depth - 1) % D;
-    uint32_t pbits[D];
+    uint32_t pbits[D], child = 0;
 #pragma unroll
-    for (int j = 0; j < D; ++j) pbits[j] = j == jd ? tbits[j] >> 1 : tbits[j];
+    for (int j = 0; j < D; ++j) {
+      pbits[j] = j == jd ? tbits[j] >> 1 : tbits[j];
+      if (j == jd) child = tbits[j] & 1u;
+    }
     const uint32_t p = find_leaf_bits<D>(a.hash, a.codes, n, true, pbits, a.depth - 1);
-    return p == kInvalidIndex ? kInvalidIndex : 2u * p + (tbits[jd] & 1u);
+    return p == kInvalidIndex ? kInvalidIndex : 2u * p + child;
   }
 };
 
@@ -104,7 +109,7 @@ __device__ __forceinline__ bool load_points(const GridParams& g, uint64_t P, dou
 }
 
 template<class Map, class Grid, ImageMode M>
-__global__ void __launch_bounds__(kThreads) image_points_kernel(const ImageArgs a)
+__global__ void __launch_bounds__(kThreads, 6) image_points_kernel(const ImageArgs a)
 {
   using PI = PointImage<Map, Grid>;
   __shared__ double pts[kPointTable];
