@@ -107,6 +107,8 @@ _SIGS = {
     "b12g_csr_copy": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "b12g_csr_destroy": (C.c_int, [C.c_void_p]),
     "b12g_invariant_measure": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p]),
+    "b12g_invariant_measure_tol": (C.c_int, [C.c_void_p, C.c_double, C.c_uint32, C.c_uint32, C.c_void_p,
+                                             C.POINTER(C.c_uint32), C.POINTER(C.c_double)]),
     "b12g_csr_measure": (C.c_int, [C.c_void_p, C.c_void_p]),
     "b12g_invariant_measure_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32,
                                                  C.c_void_p, C.c_void_p]),
@@ -132,6 +134,7 @@ _SIGS = {
     "b12g_set_flags_by_measure": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_uint8, C.POINTER(C.c_uint32)]),
     "b12g_chain_recurrent_run": (C.c_int, [C.c_void_p, C.POINTER(Scheme), C.c_uint32, C.c_void_p]),
     "b12g_nim_run": (C.c_int, [C.c_void_p, C.POINTER(Scheme), C.c_uint32, C.c_uint32, C.c_void_p]),
+    "b12g_nim_run_tol": (C.c_int, [C.c_void_p, C.POINTER(Scheme), C.c_uint32, C.c_double, C.c_uint32, C.c_void_p]),
     "b12g_set_flags_by_self_hit": (C.c_int, [C.c_void_p, C.POINTER(Scheme), C.c_uint8, C.POINTER(C.c_uint32)]),
     "b12g_fixed_boxes_run": (C.c_int, [C.c_void_p, C.POINTER(Scheme), C.c_uint32, C.c_void_p]),
     "b12g_tree_save_json": (C.c_int, [C.c_void_p, C.c_char_p]),

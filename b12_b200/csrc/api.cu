@@ -818,7 +818,7 @@ b12g_status b12g_csr_destroy(b12g_csr* m)
   if (m->stream) cudaStreamSynchronize(m->stream);
   m->rowptr.release(); m->cols.release(); m->vals.release(); m->tptr.release(); m->trows.release();
   m->work.release(); m->tiles.release(); m->tvals.release(); m->w0.release(); m->w1.release();
-  m->partial.release(); m->vout.release(); m->ctr.release();
+  m->partial.release(); m->vout.release(); m->ctr.release(); m->vstart.release(); m->change.release();
   m->long_flag.release(); m->long_pos.release(); m->long_list.release(); m->mid_list.release();
   if (m->stream) cudaStreamDestroy(m->stream);
   delete m;
@@ -893,6 +893,57 @@ b12g_status b12g_invariant_measure(b12g_csr* m, uint32_t iters, double* v)
   CK(cudaStreamSynchronize(s));
   if (err & 2u) return fail(B12G_ERR_TIMEOUT, "invariant measure: grid barrier gave up");
   if (err & 4u) return fail(B12G_ERR_CAPACITY, "invariant measure: a block's rows exceed its shared memory");
+  return B12G_OK;
+}
+
+b12g_status b12g_invariant_measure_tol(b12g_csr* m, double tol, uint32_t max_iters, uint32_t check_every, double* v,
+                                       uint32_t* iters_done, double* last_change)
+{
+  if (!m) return fail(B12G_ERR_INVALID, "NULL matrix");
+  if (!(tol >= 0.0) || check_every == 0 || max_iters == 0)
+    return fail(B12G_ERR_INVALID, "tolerance >= 0, check_every >= 1 and max_iters >= 1 required");
+  const uint32_t n = m->n_rows;
+  if (iters_done) *iters_done = 0;
+  if (last_change) *last_change = 0.0;
+  if (n == 0) return B12G_OK;
+  cudaStream_t s = m->stream;
+  ST(ensure_transpose(m));
+  ST(m->w0.ensure(n, "measure"));
+  ST(m->w1.ensure(n, "measure"));
+  ST(m->vout.ensure(n, "measure"));
+  ST(m->vstart.ensure(n, "measure"));
+  const int slots = measure_partial_slots();
+  const int nchg = slots / 2;          // at least the largest grid of a launch
+  ST(m->partial.ensure(slots, "measure"));
+  ST(m->change.ensure(nchg, "measure"));
+  std::vector<double> chg(nchg);
+  uint32_t done = 0;
+  double change = 0.0;
+  const double* start = nullptr;
+  for (;;) {
+    const uint32_t k = std::min(check_every, max_iters - done);
+    CK(cudaMemsetAsync(m->change.p, 0, size_t(nchg) * 8, s));
+    CK(invariant_measure(m->tptr.p, m->trows.p, m->tvals.p, m->mid_list.p, m->n_mid, m->long_list.p, m->n_long, n,
+                         k, m->w0.p, m->w1.p, m->partial.p, uint32_t(slots), m->vout.p, m->ctr.p + 64, s, m->nnz,
+                         start, m->change.p));
+    count_launches(1);
+    uint32_t err = 0;
+    CK(cudaMemcpyAsync(chg.data(), m->change.p, size_t(nchg) * 8, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&err, m->ctr.p + 64 + 64, 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (err & 2u) return fail(B12G_ERR_TIMEOUT, "invariant measure: grid barrier gave up");
+    if (err & 4u) return fail(B12G_ERR_CAPACITY, "invariant measure: a block's rows exceed its shared memory");
+    change = 0.0;
+    for (double c : chg) change += c;          // fixed order: the same sum every run
+    done += k;
+    if (change <= tol || done >= max_iters) break;
+    CK(cudaMemcpyAsync(m->vstart.p, m->vout.p, size_t(n) * 8, cudaMemcpyDeviceToDevice, s));
+    start = m->vstart.p;
+  }
+  if (v) CK(cudaMemcpyAsync(v, m->vout.p, size_t(n) * 8, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (iters_done) *iters_done = done;
+  if (last_change) *last_change = change;
   return B12G_OK;
 }
 

@@ -114,6 +114,8 @@ struct MeasureArgs {
   unsigned* error;
   double* totals;            // 2 slots: the L1 norm of the last two iterates
   unsigned gen_seen;         // completed barriers before the current one
+  const double* start;       // first iterate (L1 norm 1), or nullptr: the uniform vector
+  double* change;            // nullptr, or per block: sum of |v_k - v_(k-1)| of the last iteration
 };
 
 // Grid barrier that also reduces: every block has written its partial sum; the last
@@ -162,9 +164,43 @@ __device__ bool barrier_sum(const MeasureArgs& a, const double* part, double* to
   return ok && !(*(volatile unsigned*)a.error & 2u);
 }
 
-__device__ __forceinline__ double iterate_value(const double* wp, uint32_t src, uint32_t it, double v0, double inv)
+__device__ __forceinline__ double iterate_value(const double* wp, const double* start, uint32_t src, uint32_t it,
+                                                double v0, double inv)
 {
-  return it == 0 ? v0 : __dmul_rn(__ldcg(wp + src), inv);
+  return it == 0 ? (start ? __ldg(start + src) : v0) : __dmul_rn(__ldcg(wp + src), inv);
+}
+
+// The result v = the last iterate scaled by 1/|.|_1 (the first iterate when iters == 0)
+// and, when asked for, each block's part of |v - previous normalised iterate|_1 (the
+// change made by the last iteration: the stopping test of a tolerance-driven run).
+__device__ void write_result(const MeasureArgs& a, double inv, double inv_prev)
+{
+  __shared__ double red_c[32];
+  const uint32_t n = a.n;
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
+  const double v0 = __ddiv_rn(1.0, double(n));
+  const double* wl = (a.iters & 1u) ? a.w0 : a.w1;     // iteration iters - 1
+  const double* wq = (a.iters & 1u) ? a.w1 : a.w0;     // iteration iters - 2
+  double c = 0.0;
+  for (uint32_t j = tid; j < n; j += nthreads) {
+    const double first = a.start ? __ldg(a.start + j) : v0;
+    const double x = a.iters ? __dmul_rn(__ldcg(wl + j), inv) : first;
+    a.out[j] = x;
+    if (a.change && a.iters) {
+      const double prev = a.iters >= 2 ? __dmul_rn(__ldcg(wq + j), inv_prev) : first;
+      c = __dadd_rn(c, fabs(__dsub_rn(x, prev)));
+    }
+  }
+  if (!a.change) return;
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) c = __dadd_rn(c, __shfl_xor_sync(0xFFFFFFFFu, c, d));
+  if ((threadIdx.x & 31) == 0) red_c[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (uint32_t i = 0; i < (blockDim.x >> 5); ++i) t = __dadd_rn(t, red_c[i]);
+    a.change[blockIdx.x] = t;
+  }
 }
 
 // sum of tvals[k] * v(trows[k]) over k = b + off, b + off + step, ... < e, with all
@@ -185,7 +221,7 @@ __device__ __forceinline__ double dot_strided(const MeasureArgs& a, const double
     }
     double v[8];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) v[q] = k0 + q * step < e ? iterate_value(wp, src[q], it, v0, inv) : 0.0;
+    for (int q = 0; q < 8; ++q) v[q] = k0 + q * step < e ? iterate_value(wp, a.start, src[q], it, v0, inv) : 0.0;
 #pragma unroll
     for (int q = 0; q < 8; ++q) acc = __fma_rn(val[q], v[q], acc);
   }
@@ -207,7 +243,7 @@ __global__ void __launch_bounds__(kMeasureThreads) invariant_measure_kernel(Meas
   const uint32_t warp = tid >> 5, nwarps = nthreads >> 5;
   const uint32_t group = tid >> 3, ngroups = nthreads >> 3, lane8 = threadIdx.x & 7;
   const double v0 = __ddiv_rn(1.0, double(n));
-  double inv = 1.0;
+  double inv = 1.0, inv_prev = 1.0;
   for (uint32_t it = 0; it < a.iters; ++it) {
     const double* wp = (it & 1u) ? a.w0 : a.w1;
     double* wc = (it & 1u) ? a.w1 : a.w0;
@@ -258,10 +294,10 @@ __global__ void __launch_bounds__(kMeasureThreads) invariant_measure_kernel(Meas
     a.gen_seen = it;  // the generation counts completed barriers
     double s_it;
     if (!barrier_sum(a, a.partial + (it & 1u) * gridDim.x, a.totals + (it & 1u), &s_it)) return;
+    inv_prev = inv;
     inv = __ddiv_rn(1.0, s_it);
   }
-  const double* wl = (a.iters & 1u) ? a.w0 : a.w1;
-  for (uint32_t j = tid; j < n; j += nthreads) a.out[j] = a.iters ? __dmul_rn(__ldcg(wl + j), inv) : v0;
+  write_result(a, inv, inv_prev);
 }
 
 // Grid barrier that also reduces, on a counter that only grows: every block publishes its
@@ -365,7 +401,7 @@ __global__ void __launch_bounds__(kMeasureThreads, 1) invariant_measure_smem_ker
   const bool head_open = k0 < k1 && k0 > 0 && s_row[k0 - 1] == s_row[k0];
   const bool tail_open = k0 < k1 && k1 < nloc && s_row[k1] == s_row[k1 - 1];
   const double v0 = __ddiv_rn(1.0, double(n));
-  double inv = 1.0;
+  double inv = 1.0, inv_prev = 1.0;
   for (uint32_t it = 0; it < a.iters; ++it) {
     const double* wp = (it & 1u) ? a.w0 : a.w1;
     double* wc = (it & 1u) ? a.w1 : a.w0;
@@ -374,7 +410,7 @@ __global__ void __launch_bounds__(kMeasureThreads, 1) invariant_measure_smem_ker
 #pragma unroll
     for (int q = 0; q < kSmemChunk; ++q) {
       const uint32_t k = k0 + q;
-      v[q] = k < k1 ? iterate_value(wp, s_src[k], it, v0, inv) : 0.0;
+      v[q] = k < k1 ? iterate_value(wp, a.start, s_src[k], it, v0, inv) : 0.0;
     }
     // walk the run: a row that ends inside it is written here unless it began earlier
     uint32_t row = k0 < k1 ? s_row[k0] : 0u;
@@ -422,11 +458,10 @@ __global__ void __launch_bounds__(kMeasureThreads, 1) invariant_measure_smem_ker
     }
     double s_it;
     if (!barrier_allsum(a, a.partial + (it & 1u) * gridDim.x, it, &s_it)) return;
+    inv_prev = inv;
     inv = __ddiv_rn(1.0, s_it);
   }
-  const double* wl = (a.iters & 1u) ? a.w0 : a.w1;
-  const uint32_t tid = blockIdx.x * blockDim.x + t, nthreads = gridDim.x * blockDim.x;
-  for (uint32_t j = tid; j < n; j += nthreads) a.out[j] = a.iters ? __dmul_rn(__ldcg(wl + j), inv) : v0;
+  write_result(a, inv, inv_prev);
 }
 
 // the rows of P^T of one length class (1: medium, 2: long), ascending (flag, scan, scatter)
@@ -531,7 +566,8 @@ MeasureLaunch measure_launch()
 cudaError_t invariant_measure(const uint32_t* tptr, const uint32_t* trows, const double* tvals,
                               const uint32_t* mid_list, uint32_t n_mid, const uint32_t* long_list, uint32_t n_long,
                               uint32_t n, uint32_t iters, double* w0, double* w1, double* partial,
-                              uint32_t partial_cap, double* out, unsigned* sync_words, cudaStream_t s, uint64_t nnz)
+                              uint32_t partial_cap, double* out, unsigned* sync_words, cudaStream_t s, uint64_t nnz,
+                              const double* start, double* change)
 {
   // the matrix on chip: one block per SM, every block's rows within its shared memory
   // (a row of P^T has at most kMidRow entries when there are no long rows)
@@ -541,7 +577,7 @@ cudaError_t invariant_measure(const uint32_t* tptr, const uint32_t* trows, const
       (nnz + blocks - 1) / blocks + kMidRow <= kSmemEntries && 2 * blocks + 2 <= partial_cap) {
     cudaMemsetAsync(sync_words, 0, 65 * sizeof(unsigned), s);
     MeasureArgs a{tptr, trows, tvals, mid_list, n_mid, long_list, 0u, kShortRow, n, iters, w0, w1, partial, out,
-                  sync_words, sync_words + 32, sync_words + 64, partial + 2 * size_t(blocks), 0u};
+                  sync_words, sync_words + 32, sync_words + 64, partial + 2 * size_t(blocks), 0u, start, change};
     uint32_t nnz32 = uint32_t(nnz);
     void* params[] = {&a, &nnz32};
     return cudaLaunchCooperativeKernel((const void*)invariant_measure_smem_kernel, dim3(blocks),
@@ -557,7 +593,7 @@ cudaError_t invariant_measure(const uint32_t* tptr, const uint32_t* trows, const
   const bool lists = mid_list && long_list;
   MeasureArgs a{tptr, trows, tvals, mid_list, lists ? n_mid : 0u, long_list, lists ? n_long : 0u,
                 lists ? kShortRow : 0xFFFFFFFFu, n, iters, w0, w1, partial, out, sync_words, sync_words + 32,
-                sync_words + 64, partial + 2 * size_t(grid), 0u};
+                sync_words + 64, partial + 2 * size_t(grid), 0u, start, change};
   void* params[] = {&a};
   return cudaLaunchCooperativeKernel((const void*)invariant_measure_kernel, dim3(grid), dim3(kMeasureThreads), params,
                                      0, s);

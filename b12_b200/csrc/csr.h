@@ -20,12 +20,15 @@ cudaError_t class_rows(const uint32_t* tptr, uint32_t n, uint32_t cls, uint32_t*
 
 // power iteration on the CSR of P^T with the medium and long rows listed by class_rows
 // (both lists nullptr: every row gets one thread); sync_words: 65 u32 (barrier count at
-// 0, generation at 32, error at 64: bit 1 = barrier timeout); partial: partial_cap doubles
+// 0, generation at 32, error at 64: bit 1 = barrier timeout); partial: partial_cap doubles.
+// start: the first iterate (nullptr: uniform); change: nullptr, or measure_partial_slots()
+// / 2 doubles, zeroed by the caller, that receive per launch block the L1 change made by
+// the last iteration (their sum is |v_iters - v_(iters-1)|_1)
 cudaError_t invariant_measure(const uint32_t* tptr, const uint32_t* trows, const double* tvals,
                               const uint32_t* mid_list, uint32_t n_mid, const uint32_t* long_list, uint32_t n_long,
                               uint32_t n, uint32_t iters, double* w0, double* w1, double* partial,
                               uint32_t partial_cap, double* out, unsigned* sync_words, cudaStream_t s,
-                              uint64_t nnz = 0);
+                              uint64_t nnz = 0, const double* start = nullptr, double* change = nullptr);
 int measure_partial_slots();
 
 }  // namespace b12g

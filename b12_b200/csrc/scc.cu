@@ -367,8 +367,9 @@ b12g_status b12g_fixed_boxes_run(b12g_tree* t, const b12g_scheme* sc, uint32_t s
 
 // chainRecurrentSet.m:18-44 and subdivisionByNim.m:22-66 as device loops (the SCC and
 // eigenvector steps of the Matlab drivers replaced by the functions above)
+// by_measure: 0 components, 1 measure of `iters` iterations, 2 measure to tolerance `tol`
 static b12g_status selection_run(b12g_tree* t, const b12g_scheme* sc, uint32_t steps, int by_measure, uint32_t iters,
-                                 uint32_t* counts)
+                                 uint32_t* counts, double tol = 0.0)
 {
   if (!t || !sc) return fail(B12G_ERR_INVALID, "NULL argument");
   uint32_t k = 0;
@@ -380,7 +381,8 @@ static b12g_status selection_run(b12g_tree* t, const b12g_scheme* sc, uint32_t s
     if (st == B12G_OK) st = b12g_transition_matrix(t, sc, 0, 0, &m);
     if (st == B12G_OK) {
       if (by_measure) {
-        st = b12g_invariant_measure(m, iters, nullptr);
+        st = by_measure == 2 ? b12g_invariant_measure_tol(m, tol, iters, 20, nullptr, nullptr, nullptr)
+                             : b12g_invariant_measure(m, iters, nullptr);
         if (st == B12G_OK) st = b12g_set_flags_by_measure(t, m, 1e-9 / double(m->n_rows), B12G_HIT, &k);
       } else {
         st = b12g_set_flags_by_components(t, m, 2, B12G_HIT, &k);
@@ -402,6 +404,12 @@ b12g_status b12g_chain_recurrent_run(b12g_tree* t, const b12g_scheme* sc, uint32
 b12g_status b12g_nim_run(b12g_tree* t, const b12g_scheme* sc, uint32_t steps, uint32_t iters, uint32_t* counts)
 {
   return selection_run(t, sc, steps, 1, iters, counts);
+}
+
+b12g_status b12g_nim_run_tol(b12g_tree* t, const b12g_scheme* sc, uint32_t steps, double tol, uint32_t max_iters,
+                             uint32_t* counts)
+{
+  return selection_run(t, sc, steps, 2, max_iters, counts, tol);
 }
 
 }  // extern "C"

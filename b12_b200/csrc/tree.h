@@ -181,6 +181,7 @@ struct b12g_csr {
   Buf<uint32_t> tptr, trows, work, tiles, long_flag, long_pos, long_list, mid_list;
   uint32_t n_long = 0, n_mid = 0;
   Buf<double> tvals, w0, w1, partial, vout;
+  Buf<double> vstart, change;   // tolerance-driven runs: the iterate carried between launches, change partials
   Buf<uint32_t> ctr;
   bool has_transpose = false;
 };
@@ -200,7 +201,6 @@ b12g_status read_ctr(b12g_tree* t, int first, int count);
 b12g_status set_ctr(b12g_tree* t, int slot, uint32_t v);
 b12g_status reserve(b12g_tree* t, uint64_t n_boxes);
 b12g_status prepare(b12g_tree* t, const b12g_scheme* sc, Prepared& pr);
-b12g_status leaf_sum(b12g_tree* t, unsigned long long* sum);
 bool stored_rows_fit(b12g_tree* t, const b12g_scheme* sc, const Prepared& pr);
 b12g_status check_depth(b12g_tree* t, uint8_t depth);
 b12g_status select_sources(b12g_tree* t, const b12g_scheme* sc, Prepared& pr, uint32_t& n_src);

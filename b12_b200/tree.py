@@ -136,6 +136,17 @@ class CsrMatrix:
         check(lib().b12g_invariant_measure(self._h, iters, v.ctypes.data), "invariant_measure")
         return v
 
+    def invariant_measure_tol(self, tol: float = 1e-14, max_iters: int = 1_000_000, check_every: int = 20,
+                              out=None):
+        """The power iteration until one iteration changes the measure by at most `tol` in
+        L1 (checked every `check_every` iterations); returns (measure, iterations, change)."""
+        v = np.zeros(self.n_rows, dtype=np.float64) if out is None else out
+        k = C.c_uint32()
+        ch = C.c_double()
+        check(lib().b12g_invariant_measure_tol(self._h, float(tol), int(max_iters), int(check_every), v.ctypes.data,
+                                               C.byref(k), C.byref(ch)), "invariant_measure_tol")
+        return v, k.value, ch.value
+
     def measure(self, out=None) -> np.ndarray:
         v = np.zeros(self.n_rows, dtype=np.float64) if out is None else out
         check(lib().b12g_csr_measure(self._h, v.ctypes.data), "csr_measure")
@@ -492,6 +503,14 @@ class ImplicitBoxTree:
         counts = np.zeros(max(steps, 1), dtype=np.uint32)
         s = scheme.to_c()
         check(lib().b12g_nim_run(self._h, C.byref(s), steps, power_iterations, counts.ctypes.data), "nim_run")
+        return counts[:steps]
+
+    def nim_run_tol(self, scheme: Scheme, steps: int, tol: float = 1e-14, max_iters: int = 1_000_000) -> np.ndarray:
+        """The NIM driver with every step's measure run to `tol` (checked every 20 iterations)."""
+        counts = np.zeros(max(steps, 1), dtype=np.uint32)
+        s = scheme.to_c()
+        check(lib().b12g_nim_run_tol(self._h, C.byref(s), steps, float(tol), int(max_iters), counts.ctypes.data),
+              "nim_run_tol")
         return counts[:steps]
 
     def set_flags_by_self_hit(self, scheme: Scheme, flags: int) -> int:

@@ -238,6 +238,14 @@ b12g_status b12g_csr_destroy(b12g_csr* csr);
  * FP64 (the eigenvector step of subdivisionByNim.m:30-58).  v: host array of n_rows,
  * or NULL to keep the result on the device (b12g_csr_measure copies it later). */
 b12g_status b12g_invariant_measure(b12g_csr* csr, uint32_t iters, double* v);
+/* the same power iteration run until it settles, as subdivisionByNim.m:30-45 asks of
+ * powerMethodMPE(P, 1e-14, 1e9) (not shipped with the reference): launches of
+ * check_every iterations, each continuing from the last iterate, until the L1 change
+ * made by one iteration, |v_k - v_(k-1)|_1, is at most `tol`, or max_iters iterations.
+ * v: host array of n_rows (or NULL, the result stays on the device); *iters_done and
+ * *last_change (either may be NULL) receive the iterations run and that change. */
+b12g_status b12g_invariant_measure_tol(b12g_csr* csr, double tol, uint32_t max_iters, uint32_t check_every,
+                                       double* v, uint32_t* iters_done, double* last_change);
 /* copy the last invariant measure of `csr` to the host array v (n_rows entries) */
 b12g_status b12g_csr_measure(const b12g_csr* csr, double* v);
 /* Allocation-free invariant measure (no counterpart in the reference): for callers that
@@ -298,6 +306,10 @@ b12g_status b12g_set_flags_by_self_hit(b12g_tree* tree, const b12g_scheme* schem
 b12g_status b12g_fixed_boxes_run(b12g_tree* tree, const b12g_scheme* scheme, uint32_t steps, uint32_t* counts);
 b12g_status b12g_nim_run(b12g_tree* tree, const b12g_scheme* scheme, uint32_t steps, uint32_t power_iterations,
                          uint32_t* counts);
+/* the NIM driver with the measure of every step run to the tolerance `tol`
+ * (b12g_invariant_measure_tol, checked every 20 iterations, at most max_iters) */
+b12g_status b12g_nim_run_tol(b12g_tree* tree, const b12g_scheme* scheme, uint32_t steps, double tol,
+                             uint32_t max_iters, uint32_t* counts);
 
 /* ---- JSON files in the reference's format ----------------------------------------------
  * Trees as written by ImplicitBoxTree::save (ImplicitBoxTree.hpp:435-528) and read by

@@ -644,6 +644,40 @@ void orc_invariant_measure(uint32_t n, const uint32_t* rowptr, const uint32_t* c
   free(w);
 }
 
+/* The same iteration run until it settles (subdivisionByNim.m:30-45 asks
+ * powerMethodMPE(P, 1e-14, 1e9), not shipped): after every check_every-th iteration, and
+ * after max_iters, the L1 change made by that iteration, |v_k - v_(k-1)|_1, is compared
+ * with tol; the run stops at the first check where it is at most tol. */
+void orc_invariant_measure_tol(uint32_t n, const uint32_t* rowptr, const uint32_t* cols, const double* vals,
+                               double tol, uint32_t max_iters, uint32_t check_every, double* v, uint32_t* iters_done,
+                               double* last_change)
+{
+  double* w = (double*)malloc((size_t)n * 8);
+  for (uint32_t i = 0; i < n; ++i) v[i] = 1.0 / (double)n;
+  uint32_t k = 0;
+  double change = 0.0;
+  while (k < max_iters) {
+    memset(w, 0, (size_t)n * 8);
+    for (uint32_t i = 0; i < n; ++i)
+      for (uint32_t e = rowptr[i]; e < rowptr[i + 1]; ++e)
+        if (cols[e] < n) w[cols[e]] += vals[e] * v[i];
+    double s = 0.0;
+    for (uint32_t j = 0; j < n; ++j) s += fabs(w[j]);
+    ++k;
+    const int check = k % check_every == 0 || k == max_iters;
+    change = 0.0;
+    for (uint32_t j = 0; j < n; ++j) {
+      const double x = w[j] / s;
+      if (check) change += fabs(x - v[j]);
+      v[j] = x;
+    }
+    if (check && change <= tol) break;
+  }
+  free(w);
+  *iters_done = k;
+  *last_change = change;
+}
+
 /* ------------------------------------------------------------------------------
  * continuation (insertByIterators at a uniform depth, ImplicitBoxTree.hpp:1615-1910,
  * makePointIteratorPairByFlags 2303-2341, insertByPoints 1927-1946, deleteDepth 1217-1228)

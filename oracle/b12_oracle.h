@@ -144,6 +144,9 @@ uint64_t orc_transition_matrix(const orc_tree* t, const orc_map* m, const orc_gr
 void orc_strong_components(uint32_t n, const uint32_t* rowptr, const uint32_t* cols, uint32_t* comp);
 void orc_invariant_measure(uint32_t n, const uint32_t* rowptr, const uint32_t* cols, const double* vals,
                            uint32_t iters, double* v);
+void orc_invariant_measure_tol(uint32_t n, const uint32_t* rowptr, const uint32_t* cols, const double* vals,
+                               double tol, uint32_t max_iters, uint32_t check_every, double* v, uint32_t* iters_done,
+                               double* last_change);
 
 /* whole subdivision loop; counts[k] = leaves after step k+1; returns box-images */
 uint64_t orc_subdivision(orc_tree* t, const orc_map* m, const orc_grid* g, uint32_t steps, uint32_t* counts);

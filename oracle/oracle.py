@@ -91,6 +91,8 @@ def lib():
             "orc_transition_matrix": (u64, [P(OrcTree), P(OrcMap), P(OrcGrid), C.c_int, C.c_int,
                                             P(u32), P(u32), P(dbl), P(u32)]),
             "orc_invariant_measure": (None, [u32, P(u32), P(u32), P(dbl), u32, P(dbl)]),
+            "orc_invariant_measure_tol": (None, [u32, P(u32), P(u32), P(dbl), dbl, u32, u32, P(dbl), P(u32),
+                                                 P(dbl)]),
             "orc_image_point_boxes": (None, [P(OrcTree), P(OrcMap), P(OrcGrid), P(u64), P(u8)]),
             "orc_search_point_boxes": (None, [P(OrcTree), P(u64), P(u8), u64, P(u32)]),
             "orc_set_flags_by_point_boxes": (u32, [P(OrcTree), P(u64), P(u8), u64, u8]),
@@ -377,6 +379,22 @@ def invariant_measure(rowptr, cols, vals, iters=200):
     return v
 
 
+def invariant_measure_tol(rowptr, cols, vals, tol, max_iters, check_every=20):
+    """The power iteration until the L1 change of one iteration, checked every
+    `check_every` iterations, is at most `tol`: (v, iterations run, last change)."""
+    n = len(rowptr) - 1
+    rowptr = np.ascontiguousarray(rowptr, dtype=np.uint32)
+    cols = np.ascontiguousarray(cols, dtype=np.uint32)
+    vals = np.ascontiguousarray(vals, dtype=np.float64)
+    v = np.zeros(n)
+    k = C.c_uint32()
+    ch = C.c_double()
+    lib().orc_invariant_measure_tol(n, _ptr(rowptr, C.c_uint32), _ptr(cols, C.c_uint32), _ptr(vals, C.c_double),
+                                    float(tol), int(max_iters), int(check_every), _ptr(v, C.c_double), C.byref(k),
+                                    C.byref(ch))
+    return v, k.value, ch.value
+
+
 def strong_components(rowptr, cols):
     """Component label (largest vertex of the component) of every row's box."""
     n = len(rowptr) - 1
@@ -405,16 +423,20 @@ def chain_recurrent(spec: dict, steps: int):
     return o, counts
 
 
-def nim_selection(spec: dict, steps: int, iters: int = 200):
+def nim_selection(spec: dict, steps: int, iters: int = 200, tol: float | None = None):
     """subdivisionByNim.m:22-66 with the FP64 power iteration for the eigenvector: keep the
-    boxes whose measure is at least 1e-9 / n; returns the oracle and per-step counts."""
+    boxes whose measure is at least 1e-9 / n; returns the oracle and per-step counts.
+    With `tol` the iteration runs to that tolerance (checked every 20, at most `iters`)."""
     o = Oracle(spec)
     o.set_flags(8)
     counts = []
     for _ in range(steps):
         o.subdivide(8)
         rowptr, cols, vals, _ = o.transition_matrix()
-        v = invariant_measure(rowptr, cols, vals, iters)
+        if tol is None:
+            v = invariant_measure(rowptr, cols, vals, iters)
+        else:
+            v = invariant_measure_tol(rowptr, cols, vals, tol, iters, 20)[0]
         o.set_flags_mask(v >= 1e-9 / len(v), 1)
         o.remove(1)
         o.unset_flags(1)

@@ -82,6 +82,48 @@ def test_nim_run_matches_oracle():
         np.testing.assert_array_equal(x, y)
 
 
+def checkpoint_changes(rowptr, cols, vals, tol, max_iters, every):
+    """The oracle's stopping point and the changes at its last two checks."""
+    v, k, ch = O.invariant_measure_tol(rowptr, cols, vals, tol, max_iters, every)
+    prev = O.invariant_measure_tol(rowptr, cols, vals, 0.0, k - every, every)[2] if k > every else np.inf
+    return v, k, ch, prev
+
+
+@pytest.mark.parametrize("spec,steps,tol", [(dict(map="henon"), 12, 1e-10), (dict(map="lorenz", rho=28.0, grid=5), 14,
+                                                                             1e-12)])
+def test_invariant_measure_to_tolerance_matches_oracle(spec, steps, tol):
+    """The tolerance-driven power iteration stops at the oracle's check (the changes at the
+    last two checks straddle tol by at least 10 % here) with the same vector, within the
+    measure tolerance of the other tests."""
+    c, r = domain(spec)
+    t = B.ImplicitBoxTree(c, r)
+    sc = scheme(spec)
+    t.subdivision_run(sc, steps)
+    m = t.transition_matrix(sc)
+    rowptr, cols, vals = m.to_host()
+    want, k, ch, prev = checkpoint_changes(rowptr, cols, vals, tol, 100000, 20)
+    assert ch <= 0.9 * tol and prev >= 1.1 * tol, (ch, prev)      # a decision no rounding can flip
+    v, k_gpu, ch_gpu = m.invariant_measure_tol(tol, 100000, 20)
+    assert k_gpu == k
+    assert abs(ch_gpu - ch) <= 1e-3 * tol + 1e-15
+    assert np.abs(v - want).sum() < 1e-12
+    # a cap below the stopping point ends the run there
+    v2, k2, _ = m.invariant_measure_tol(0.0, 50, 20)
+    assert k2 == 50
+    np.testing.assert_allclose(v2, O.invariant_measure(rowptr, cols, vals, 50), rtol=0, atol=1e-13)
+
+
+def test_nim_run_to_tolerance_matches_oracle():
+    spec = dict(map="henon")
+    c, r = domain(spec)
+    t = B.ImplicitBoxTree(c, r)
+    counts = t.nim_run_tol(scheme(spec), 12, 1e-12, 100000)
+    o, ocounts = O.nim_selection(oracle_spec(spec), 12, 100000, tol=1e-12)
+    assert list(counts) == ocounts
+    for x, y in zip(t.leaves(), o.leaves()):
+        np.testing.assert_array_equal(x, y)
+
+
 @pytest.mark.parametrize("spec,steps", [(dict(map="henon"), 16), (dict(map="lorenz", rho=28.0, grid=5), 14),
                                         (dict(map="forced_duffing", grid=4), 12)])
 def test_fixed_boxes_run_matches_oracle(spec, steps):
