@@ -107,6 +107,10 @@ _SIGS = {
     "b12g_csr_copy": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "b12g_csr_destroy": (C.c_int, [C.c_void_p]),
     "b12g_invariant_measure": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p]),
+    "b12g_route_point_boxes": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p,
+                                         C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "b12g_leaf_at": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint8),
+                               C.POINTER(C.c_uint8)]),
     "b12g_invariant_measure_tol": (C.c_int, [C.c_void_p, C.c_double, C.c_uint32, C.c_uint32, C.c_void_p,
                                              C.POINTER(C.c_uint32), C.POINTER(C.c_double)]),
     "b12g_csr_measure": (C.c_int, [C.c_void_p, C.c_void_p]),

@@ -81,9 +81,22 @@ b12g_status set_ctr(b12g_tree* t, int slot, uint32_t v)
   return B12G_OK;
 }
 
+b12g_status reserve_exact(b12g_tree* t, uint64_t n_boxes);
+
+// Room for n_boxes leaves.  A tree that has to grow gets room for twice as many (or, if
+// that much memory is not free, the exact need): trees grow step by step, and every
+// reallocation frees the old buffers (cudaFree synchronises the device).
 b12g_status reserve(b12g_tree* t, uint64_t n_boxes)
 {
   if (n_boxes > 0xFFFFFFF0ull) return fail(B12G_ERR_CAPACITY, "at most 2^32-16 boxes per tree");
+  if (n_boxes <= t->code[0].n && n_boxes <= t->code[1].n && n_boxes <= t->hit.n) return reserve_exact(t, n_boxes);
+  const uint64_t ample = std::min<uint64_t>(2 * n_boxes, 0xFFFFFFF0ull);
+  if (reserve_exact(t, ample) == B12G_OK) return B12G_OK;
+  return reserve_exact(t, n_boxes);
+}
+
+b12g_status reserve_exact(b12g_tree* t, uint64_t n_boxes)
+{
   const size_t keep = t->n;
   for (int b = 0; b < 2; ++b) {
     ST(t->code[b].grow_keep(n_boxes, b == t->cur ? keep : 0, t->stream, "leaf codes"));

@@ -74,6 +74,12 @@ struct Buf {
     }
     return B12G_OK;
   }
+  // ensure room for `count`, and when that means a new buffer, for `factor` times as
+  // many: for buffers that grow step by step (cudaFree synchronises the device)
+  b12g_status ensure_room(size_t count, const char* what, size_t factor = 2)
+  {
+    return ensure(count <= n ? count : factor * count, what);
+  }
   void release()
   {
     if (p) cudaFree(p);
@@ -135,6 +141,7 @@ struct b12g_tree {
   Buf<uint64_t> ins_code, ins_key[2], scan_code;
   Buf<uint32_t> ins_idx[2], ins_pos, ins_head;
   Buf<uint32_t> isrc_head, isrc_pos, isrc_and, isrc;   // scheme sources at an inner depth
+  Buf<uint32_t> route_runs, route_cnt;   // routing of point boxes to ranks: run starts and ranks, counts
   Buf<ulonglong2> hash;        // leaf lookup table
   Buf<uint64_t> pk;            // the leaves' packed per-dimension indices (the table's keys)
   uint32_t hash_tag = 0;       // tag of the last build (1..255; 0 = cleared)

@@ -65,8 +65,12 @@ class DeviceRun:
         return 0 if self.empty else self.tree.count()
 
     def start(self) -> int:
-        c, d, _ = self.tree.leaves_device(self.device)
-        return box_start(int(c[0].item()) & ((1 << 64) - 1), int(d[0].item()))
+        c, d, _ = self.tree.leaf_at(0)
+        return box_start(c, d)
+
+    def route_point_boxes(self, codes, valid, starts, ranks, world: int):
+        """The point boxes grouped by owner rank, on this GPU (b12g_route_point_boxes)."""
+        return self.tree.route_point_boxes(codes, valid, starts, ranks, world)
 
     def set_flags(self, flags: int) -> None:
         if not self.empty:
@@ -163,8 +167,15 @@ class PartitionedTree:
         self.table = (yield ("allgather", row)).to("cpu")
         return self.table
 
+    def _owned_runs(self):
+        """(ranks, unsigned first codes) of the non-empty runs, ascending."""
+        ranks = [r for r in range(self.world) if int(self.table[r, 0]) > 0]
+        starts = [(int(self.table[r, 1]) & ((1 << 64) - 1)) ^ (1 << 63) for r in ranks]
+        return ranks, starts
+
     def _owners(self, codes, valid):
-        """The rank that owns each point box (int16 tensor), or an int when one rank owns all."""
+        """The rank that owns each point box (int16 tensor), or an int when one rank owns all
+        (runs held on the host; a run on a GPU routes with its own kernels, _route_boxes)."""
         import torch
         n = self.table[:, 0]
         ranks = torch.nonzero(n > 0).flatten()
@@ -202,9 +213,18 @@ class PartitionedTree:
             parts.append(list(g.split(splits)))
         return slot, parts
 
+    def _route_boxes(self, codes, valid):
+        """(slot or None, per-rank codes, per-rank validity) of this rank's point boxes."""
+        ranks, starts = self._owned_runs()
+        route = getattr(self.run, "route_point_boxes", None)
+        if len(ranks) > 1 and route is not None:
+            slot, c_parts, v_parts = route(codes, valid, starts, ranks, self.world)
+            return slot, (c_parts, v_parts)
+        return self._route(self._owners(codes, valid), codes, valid)
+
     def _exchange_point_boxes(self, codes, valid):
         import torch
-        slot, (c_parts, v_parts) = self._route(self._owners(codes, valid), codes, valid)
+        slot, (c_parts, v_parts) = self._route_boxes(codes, valid)
         rc = yield ("alltoall", c_parts)
         rv = yield ("alltoall", v_parts)
         return slot, [x.numel() for x in rc], torch.cat(rc), torch.cat(rv)

@@ -220,6 +220,20 @@ b12g_status b12g_transition_rows(b12g_tree* tree, const uint32_t* targets, uint3
  * buffers alike */
 b12g_status b12g_load_leaves_device(b12g_tree* tree, const uint64_t* codes, const uint8_t* depths,
                                     const uint8_t* flags, uint32_t n);
+/* Routing of n point boxes (device buffers) to the ranks that own them (no counterpart
+ * in the reference, which runs on one device): run r of the tree's leaves starts at the
+ * depth-64 code run_starts[r] and lives on rank run_ranks[r] (host arrays of the n_runs
+ * non-empty runs, both ascending); a valid box goes to the last run starting at or below
+ * it, an invalid one to the last run.  out_codes / out_valid receive the boxes grouped by
+ * rank, in their order within each rank; slot (device, may be NULL) the position of box
+ * i in the output; counts (host, `world` entries) the boxes for each rank.  Uses the
+ * tree's stream and scratch and returns after the work has finished. */
+b12g_status b12g_route_point_boxes(b12g_tree* tree, const uint64_t* codes, const uint8_t* valid, uint64_t n,
+                                   const uint64_t* run_starts, const uint32_t* run_ranks, uint32_t n_runs,
+                                   uint32_t world, uint64_t* out_codes, uint8_t* out_valid, uint32_t* slot,
+                                   uint64_t* counts);
+/* one leaf (index in tree order) to the host: code, depth and flags (any may be NULL) */
+b12g_status b12g_leaf_at(b12g_tree* tree, uint32_t index, uint64_t* code, uint8_t* depth, uint8_t* flags);
 
 /* ---- transition matrix (ImplicitBoxTree.hpp:2934-3193, CooMatrix.hpp:14-56) ---------- */
 /* transitionMatrixForLeaves<double>(grid, map, absolute, rowMajor=true, invalid):

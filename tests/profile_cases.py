@@ -17,6 +17,8 @@ serve     a burst of --jobs served-stream jobs through the job server.
 mixed     a Lorenz tree (explicit FMA) refined to --depth (default 21), SD kept on the
           lower half in x, four selective steps (leaves of depths d..d+4), then one more
           subdivide and set_flags_by_image: the per-leaf-depth image kernel over the tree.
+partition one Lorenz job to --depth (default 27) over --world ranks emulated in one
+          process, against the fused single-tree loop (times of both, same results).
 
 Every case prints one line of sizes; none writes files.
 """
@@ -134,19 +136,62 @@ def case_mixed(args):
     t.close()
 
 
+def case_partition(args):
+    """One Lorenz job (explicit FMA) to --depth split over --world ranks emulated in this
+    process (their collectives answered on the host between launches), against the fused
+    single-tree loop: the same leaves and matrix, and the time of each."""
+    import torch
+    import b12_b200 as B
+    from b12_b200.partition import DeviceRun, PartitionedTree, drive_lockstep
+    from b12_b200.workloads import LORENZ_CENTER, LORENZ_RADIUS
+    sc = B.Scheme(B.lorenz(fma=True), B.inner_grid(5))
+    res = {}
+    for rep in range(2):                   # the second repetition is timed
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        t = B.ImplicitBoxTree(LORENZ_CENTER, LORENZ_RADIUS)
+        counts = t.subdivision_run(sc, args.depth)
+        m = t.transition_matrix(sc)
+        fused = time.perf_counter() - t0
+        nnz_fused = m.nnz
+        m.close()
+        runs = [DeviceRun(B.ImplicitBoxTree(LORENZ_CENTER, LORENZ_RADIUS), "cuda") for _ in range(args.world)]
+        for r in runs[1:]:
+            r.empty = True
+        parts = [PartitionedTree(r, i, args.world) for i, r in enumerate(runs)]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        pc = drive_lockstep([p.subdivision(sc, args.depth) for p in parts])
+        blocks = drive_lockstep([p.transition_matrix(sc) for p in parts])
+        torch.cuda.synchronize()
+        split = time.perf_counter() - t0
+        nnz = sum(b.rows.nnz for b in blocks if b.rows is not None)
+        assert list(pc[0]) == [int(c) for c in counts] and nnz == nnz_fused
+        res = dict(fused=fused, split=split, boxes=int(counts[-1]), nnz=nnz)
+        for b in blocks:
+            if b.rows is not None:
+                b.rows.close()
+        for r in runs:
+            r.tree.close()
+        t.close()
+    print(f"partition: Lorenz depth {args.depth}, {res['boxes']} boxes, {res['nnz']} nonzeros: fused single tree "
+          f"{1e3 * res['fused']:.1f} ms (fresh tree), {args.world} emulated ranks {1e3 * res['split']:.1f} ms")
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["image", "compact", "sort", "measure", "serve", "mixed"])
+    ap.add_argument("case", choices=["image", "compact", "sort", "measure", "serve", "mixed", "partition"])
     ap.add_argument("--depth", type=int, default=None)
     ap.add_argument("--instances", type=int, default=64)
     ap.add_argument("--jobs", type=int, default=300)
     ap.add_argument("--repeat", type=int, default=1, help="measure: timed calls after the first")
+    ap.add_argument("--world", type=int, default=2, help="partition: emulated ranks")
     args = ap.parse_args()
     if args.depth is None:
         args.depth = {"image": 23, "compact": 27, "sort": 24, "measure": 27, "serve": 0,
-                      "mixed": 21}[args.case]
+                      "mixed": 21, "partition": 27}[args.case]
     {"image": case_image, "compact": case_compact, "sort": case_sort, "measure": case_measure,
-     "serve": case_serve, "mixed": case_mixed}[args.case](args)
+     "serve": case_serve, "mixed": case_mixed, "partition": case_partition}[args.case](args)
 
 
 if __name__ == "__main__":

@@ -205,3 +205,34 @@ def test_partitioned_run_over_an_nccl_group_of_one(golden):
         block.rows.close()
     finally:
         dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,n_runs", [(2, 2), (4, 3), (300, 17)])
+def test_route_point_boxes_matches_a_stable_partition(world, n_runs):
+    """b12g_route_point_boxes against the definition: owner = the last run whose first
+    code is at or below the box (unsigned order), the last run for a box outside the
+    domain; the boxes grouped by owner, stable within each owner."""
+    import torch
+    rng = np.random.default_rng(world)
+    n = 100_003
+    codes = rng.integers(0, 2**63, n, dtype=np.int64).view(np.uint64) * np.uint64(2) + rng.integers(
+        0, 2, n).astype(np.uint64)
+    valid = (rng.random(n) > 0.05).astype(np.uint8)
+    ranks = np.sort(rng.choice(world, n_runs, replace=False)).astype(np.uint32)
+    starts = np.sort(rng.integers(1, 2**63, n_runs - 1, dtype=np.int64).view(np.uint64) * np.uint64(2))
+    starts = np.concatenate([[np.uint64(0)], starts]).astype(np.uint64)
+    pos = np.searchsorted(starts, codes, side="right") - 1
+    owner = np.where(valid != 0, ranks[pos], ranks[-1])
+    order = np.argsort(owner, kind="stable")
+    t = B.ImplicitBoxTree([0.0, 0.0], [1.0, 1.0])
+    d_codes = torch.from_numpy(codes.view(np.int64)).cuda()
+    d_valid = torch.from_numpy(valid).cuda()
+    slot, c_parts, v_parts = t.route_point_boxes(d_codes, d_valid, starts, ranks, world)
+    assert [p.numel() for p in c_parts] == np.bincount(owner, minlength=world).tolist()
+    got_c = torch.cat(c_parts).cpu().numpy().view(np.uint64)
+    got_v = torch.cat(v_parts).cpu().numpy()
+    np.testing.assert_array_equal(got_c, codes[order])
+    np.testing.assert_array_equal(got_v, valid[order])
+    inv = np.empty(n, dtype=np.int64)
+    inv[order] = np.arange(n)
+    np.testing.assert_array_equal(slot.cpu().numpy(), inv)
