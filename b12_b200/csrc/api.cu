@@ -292,7 +292,7 @@ b12g_status flag_call(b12g_tree* t, int op, uint8_t u, uint8_t f, uint8_t depth,
   return B12G_OK;
 }
 
-static uint32_t host_hash_log2(uint64_t n)
+uint32_t host_hash_log2(uint64_t n)
 {
   uint32_t l = 6;
   while ((1ull << l) < 2ull * n) ++l;

@@ -15,6 +15,7 @@ namespace b12g {
 
 constexpr uint32_t kInvalidIndex = 0xFFFFFFFFu;
 constexpr uint32_t kOutsideIndex = 0xFFFFFFFEu;   // stored image target: point left the domain
+constexpr uint32_t kAbsentIndex = 0xFFFFFFFDu;   // leaf table: present, index not recorded
 constexpr uint64_t kInvalidCode = ~uint64_t(0);
 
 // ---------------------------------------------------------------------------------

@@ -204,8 +204,17 @@ b12g_status insert_points_impl(b12g_tree* t, const double* points, uint64_t n_po
   return B12G_OK;
 }
 
+// A lookup table kept across the sweeps of a continuation: built for n leaves, it takes
+// each sweep's new boxes (marked present only: the insertion asks whether an image box is
+// a leaf, not which one) until the leaf count needs a larger table, when it is rebuilt.
+struct PresenceTable {
+  LeafHash h{};
+  uint32_t l = 0;       // log2 of the slots the table's lookups use
+  bool ok = false;
+};
+
 b12g_status insert_by_image_impl(b12g_tree* t, const b12g_scheme* sc, uint8_t depth, uint8_t ins, uint8_t hit_flags,
-                                 uint32_t* n_inserted)
+                                 uint32_t* n_inserted, PresenceTable* keep = nullptr)
 {
   if (!t || !sc) return fail(B12G_ERR_INVALID, "NULL argument");
   if (depth == 0) return fail(B12G_ERR_UNSUPPORTED_MIXED_DEPTH, "insertion of images at depth 0");
@@ -229,7 +238,20 @@ b12g_status insert_by_image_impl(b12g_tree* t, const b12g_scheme* sc, uint8_t de
     if (n_inserted) *n_inserted = 0;
     return B12G_OK;
   }
-  ST(build_current_hash(t, pr));
+  if (keep && !hit_flags) {
+    if (keep->ok && host_hash_log2(t->n) == keep->l) {
+      pr.a.hash = keep->h;
+    } else {
+      ST(build_current_hash(t, pr));
+      keep->ok = pr.a.hash.slots != nullptr;
+      keep->l = host_hash_log2(t->n);
+      keep->h = pr.a.hash;
+      keep->h.pk = nullptr;      // leaf indices move with every merge: sources from the codes
+    }
+    pr.a.hash.pk = nullptr;
+  } else {
+    ST(build_current_hash(t, pr));
+  }
   // room for every point to be a new box; grows (and the images are recomputed) on overflow
   uint64_t cap = std::min<uint64_t>(points, std::max<uint64_t>(uint64_t(t->cand.n), uint64_t(1) << 20));
   for (int attempt = 0; attempt < 8; ++attempt) {
@@ -257,6 +279,16 @@ b12g_status insert_by_image_impl(b12g_tree* t, const b12g_scheme* sc, uint8_t de
     uint32_t u = 0;
     ST(sort_unique_candidates(t, m, depth, &u));
     ST(merge_new(t, u, ins));
+    if (keep && keep->ok && u > 0) {
+      if (host_hash_log2(t->n) == keep->l) {
+        // the u new codes are still in t->cand2, their count at C_NNEW
+        CK(add_to_leaf_hash(t->cand2.p, t->ctr.p + C_NNEW, int(keep->l), int(depth), int(t->domain.dim), keep->h,
+                            t->ctr.p + C_ERROR, u, t->stream));
+        count_launches(1);
+      } else {
+        keep->ok = false;
+      }
+    }
     if (n_inserted) *n_inserted = u;
     return B12G_OK;
   }
@@ -291,9 +323,10 @@ b12g_status b12g_continuation_run(b12g_tree* t, const b12g_scheme* sc, const dou
   s.flags_to_check = B12G_EXPD;                                             // {grid, map, d, EXPD}
   uint32_t nb0 = 0, nb1 = t->depth == depth ? t->n : 0;
   uint32_t k = 0;
+  PresenceTable keep;
   while (nb1 > nb0 && k < max_sweeps) {
     ST(flag_call(t, 2, B12G_INS, B12G_EXPD, depth, nullptr));              // changeFlags('all', INS, EXPD, d)
-    ST(insert_by_image_impl(t, &s, depth, B12G_INS, B12G_NONE, nullptr));   // insert(scheme, d, INS, NONE)
+    ST(insert_by_image_impl(t, &s, depth, B12G_INS, B12G_NONE, nullptr, &keep));   // insert(scheme, d, INS, NONE)
     ST(flag_call(t, 1, 0, B12G_EXPD, B12G_LEAF_DEPTH, nullptr));           // unsetFlags('all', EXPD)
     nb0 = nb1;
     nb1 = t->n;

@@ -89,6 +89,10 @@ int device_sm_count();
 // for (error bit 0 otherwise)
 cudaError_t build_leaf_hash(const uint64_t* codes, const uint32_t* n, int depth, int dim, LeafHash h, uint32_t* error,
                             uint32_t max_n, cudaStream_t s);
+// the *n codes (depth `depth`) into a table built with log2 size l, marked present only
+// (their value is kAbsentIndex): lookups that need no leaf index, after a merge
+cudaError_t add_to_leaf_hash(const uint64_t* codes, const uint32_t* n, int l, int depth, int dim, LeafHash h,
+                             uint32_t* error, uint32_t max_n, cudaStream_t s);
 // flags |= f on hit leaves (hit cleared); *changed += leaves that lacked f
 cudaError_t apply_hits(uint8_t* flags, uint8_t* hit, const uint32_t* n, uint8_t f, uint32_t* changed,
                        uint32_t max_n, cudaStream_t s);

@@ -33,6 +33,7 @@ constexpr uint64_t kAggregate = 1ull << 62;       // status word: tile count pub
 constexpr uint64_t kInclusive = 2ull << 62;       // status word: inclusive prefix published
 constexpr uint64_t kFlagMask = 3ull << 62;
 constexpr uint32_t kLookbackPolls = 1u << 20;     // polls of one predecessor before giving up
+constexpr int kLookbackBatch = 8;                 // predecessor status words loaded together
 
 int grid_for(uint64_t work, int per_block, int blocks_per_sm)
 {
@@ -168,23 +169,37 @@ __global__ void __launch_bounds__(kThreads) onesweep_pass_kernel(const uint64_t*
   const uint32_t digit_base = block_exclusive_scan(sc.hist[pass * kBins + d], warp_sums);
   const uint32_t tile_start = block_exclusive_scan(cnt, warp_sums);   // digit d's first staging index
 
-  // 3. decoupled look-back over the preceding tiles for digit d
+  // 3. decoupled look-back over the preceding tiles for digit d, kLookbackBatch tiles at
+  // a time: their status words are loaded together (one memory latency per batch, not
+  // one per tile), then taken nearest first; a tile that has not published yet is polled
+  // (bounded) before the walk goes past it
   uint32_t excl = 0;
   if (t > 0) {
+    const uint64_t* region = sc.status[pass & 1] + d;
     int64_t j = int64_t(t) - 1;
-    while (j >= 0) {
-      const volatile unsigned long long* src =
-          reinterpret_cast<const volatile unsigned long long*>(sc.status[pass & 1] + size_t(j) * kBins + d);
-      uint64_t v = *src;
-      uint32_t polls = 0;
-      while ((v & kFlagMask) == 0) {
-        if (++polls > kLookbackPolls) break;
-        v = *src;
+    bool done = false;
+    while (!done && j >= 0) {
+      uint64_t v[kLookbackBatch];
+#pragma unroll
+      for (int q = 0; q < kLookbackBatch; ++q)
+        v[q] = j - q >= 0 ? *reinterpret_cast<const volatile unsigned long long*>(region + size_t(j - q) * kBins)
+                          : kInclusive;
+#pragma unroll
+      for (int q = 0; q < kLookbackBatch; ++q) {
+        if (done) break;
+        if (j - q < 0) { done = true; break; }
+        const volatile unsigned long long* src =
+            reinterpret_cast<const volatile unsigned long long*>(region + size_t(j - q) * kBins);
+        uint32_t polls = 0;
+        while ((v[q] & kFlagMask) == 0) {
+          if (++polls > kLookbackPolls) break;
+          v[q] = *src;
+        }
+        if ((v[q] & kFlagMask) == 0) { atomicOr(error, 2u); done = true; break; }
+        excl += uint32_t(v[q]);
+        if ((v[q] & kFlagMask) == kInclusive) done = true;
       }
-      if ((v & kFlagMask) == 0) { atomicOr(error, 2u); break; }
-      excl += uint32_t(v);
-      if ((v & kFlagMask) == kInclusive) break;
-      --j;
+      j -= kLookbackBatch;
     }
     __threadfence();
     __stcg(reinterpret_cast<unsigned long long*>(status + d), (unsigned long long)(kInclusive | (excl + cnt)));

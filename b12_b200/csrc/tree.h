@@ -212,6 +212,8 @@ bool stored_rows_fit(b12g_tree* t, const b12g_scheme* sc, const Prepared& pr);
 b12g_status check_depth(b12g_tree* t, uint8_t depth);
 b12g_status select_sources(b12g_tree* t, const b12g_scheme* sc, Prepared& pr, uint32_t& n_src);
 b12g_status check_error(b12g_tree* t, const char* where);
+// log2 of the lookup-table slots n leaves use (the device's hash_log2)
+uint32_t host_hash_log2(uint64_t n);
 b12g_status set_root(b12g_tree* t, uint8_t flags);
 b12g_status flag_call(b12g_tree* t, int op, uint8_t u, uint8_t f, uint8_t depth, uint32_t* n_changed);
 // make the lookup table hold up to max_n codes (clears it when it grows)

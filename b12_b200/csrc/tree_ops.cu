@@ -173,6 +173,39 @@ __global__ void hash_build_kernel(const uint64_t* codes, const uint32_t* n_ptr, 
   }
 }
 
+// New boxes into an existing table of log2 size l (the size the leaf count it was built
+// for asks for, which must still be the size hash_log2 gives for the grown count): only
+// their presence is recorded (value kAbsentIndex), for lookups that need no leaf index.
+template<int D>
+__global__ void hash_add_kernel(const uint64_t* codes, const uint32_t* n_ptr, int l, int depth, LeafHash h,
+                                uint32_t* error)
+{
+  const uint32_t n = *n_ptr;
+  const uint64_t mask = (1ull << l) - 1ull;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    uint32_t bits[D];
+#pragma unroll
+    for (int j = 0; j < D; ++j) bits[j] = deinterleave<D>(codes[i], depth, j);
+    const uint64_t pk = pack_bits<D>(bits, depth);
+    const unsigned long long key = (uint64_t(h.tag) << 56) | pk;
+    uint64_t s = hash_slot(pk, l);
+    bool done = false;
+    for (uint64_t step = 0; step <= 2 * mask + 64 && !done; ++step) {
+      unsigned long long* kw = reinterpret_cast<unsigned long long*>(&h.slots[s].x);
+      const unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(kw);
+      if ((cur >> 56) != h.tag) {
+        if (atomicCAS(kw, cur, key) == cur) {
+          h.slots[s].y = kAbsentIndex;
+          done = true;
+        }
+        continue;
+      }
+      s = (s + 1) & mask;
+    }
+    if (!done) atomicOr(error, 1u);
+  }
+}
+
 // ---------------------------------------------------------------------------------
 // compaction: tile counts -> single-block tile scan -> ordered scatter
 // ---------------------------------------------------------------------------------
@@ -450,6 +483,19 @@ cudaError_t build_leaf_hash(const uint64_t* codes, const uint32_t* n, int depth,
     case 2: hash_build_kernel<2><<<g, kThreads, 0, s>>>(codes, n, depth, h, error); break;
     case 3: hash_build_kernel<3><<<g, kThreads, 0, s>>>(codes, n, depth, h, error); break;
     case 4: hash_build_kernel<4><<<g, kThreads, 0, s>>>(codes, n, depth, h, error); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t add_to_leaf_hash(const uint64_t* codes, const uint32_t* n, int l, int depth, int dim, LeafHash h,
+                             uint32_t* error, uint32_t max_n, cudaStream_t s)
+{
+  const int g = grid_for(max_n, kThreads, 8);
+  switch (dim) {
+    case 2: hash_add_kernel<2><<<g, kThreads, 0, s>>>(codes, n, l, depth, h, error); break;
+    case 3: hash_add_kernel<3><<<g, kThreads, 0, s>>>(codes, n, l, depth, h, error); break;
+    case 4: hash_add_kernel<4><<<g, kThreads, 0, s>>>(codes, n, l, depth, h, error); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
