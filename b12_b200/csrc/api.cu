@@ -201,6 +201,7 @@ b12g_status prepare(b12g_tree* t, const b12g_scheme* sc, Prepared& pr)
   a.hit_cap = uint32_t(std::min<size_t>(t->hit.n, 0xFFFFFFFFu));
   a.error = t->ctr.p + C_ERROR;
   a.cand_count = t->ctr.p + C_CAND;
+  a.work = reinterpret_cast<unsigned long long*>(t->ctr.p + C_WORK);
   return B12G_OK;
 }
 

@@ -186,7 +186,9 @@ __device__ __forceinline__ uint64_t interleave(const uint32_t (&bits)[D], const 
 __device__ __forceinline__ void box_axis(const Domain& dom, int j, uint32_t bits, int k, double& c, double& r)
 {
   r = dom.r[j] * pow2(-k);
-  const double t = __dsub_rn(__dmul_rn(double(bits) * pow2(-k), 2.0), 1.0);
+  // t = 2 bits 2^-k - 1: the scalings are exact, so one fused rounding gives the value of
+  // the reference's rounded subtraction
+  const double t = __fma_rn(double(bits), pow2(1 - k), -1.0);
   c = __dadd_rn(__dadd_rn(__dmul_rn(t, dom.r[j]), dom.c[j]), r);
 }
 
@@ -232,18 +234,20 @@ __device__ __forceinline__ void unpack_bits(uint64_t p, int depth, uint32_t* bit
 // floor(RN(q + 1) 2^(k-1)) with q = RN(x / r), a non-decreasing function of q.  The fast
 // path replaces the division by qa = RN(x RN(1/r)): two roundings of relative size
 // 2^-53 each give |qa - x/r| <= 2^-52 |x/r| (1 + 2^-53), and |q - x/r| <= 2^-53 |x/r|,
-// so |q - qa| < 2^-50.9 for |x/r| <= 1 + 2^-50 (p inside the domain).  The two
-// roundings to RN(. + 1) in [0, 2] add at most 2^-52, so sa = RN(qa + 1) 2^(k-1) is
-// within 2^(k-51) of the exact s.  When sa is at least 2^(k-49) away from both
-// neighbouring integers, floor(s) = floor(sa); otherwise (probability about 2^(k-48))
-// the IEEE division decides, exactly as before.
+// so |q - qa| < 2^-50.9 for |x/r| <= 1 + 2^-50 (p inside the domain).  The fast path
+// takes sa = RN(x y 2^(k-1) + 2^(k-1)) (one fused operation; y 2^(k-1) is exact): it differs
+// from (q + 1) 2^(k-1) by the division's and the reciprocal's errors and one rounding,
+// and from the exact s = RN(q + 1) 2^(k-1) by less than 2^(k-50.5).  When sa is at least
+// 2^(k-49) away from both neighbouring integers, floor(s) = floor(sa); otherwise
+// (probability about 2^(k-48)) the IEEE division decides, exactly as before.
 __device__ __forceinline__ uint32_t axis_index(const Domain& dom, int j, double pj, int k)
 {
   const double x = __dsub_rn(pj, dom.c[j]);
   const double y = dom.inv_r[j];
   const unsigned long long mask = (1ull << k) - 1ull;
   if (y != 0.0) {
-    const double sa = __dmul_rn(__dadd_rn(__dmul_rn(x, y), 1.0), pow2(k - 1));
+    const double half = pow2(k - 1);
+    const double sa = __fma_rn(x, y * half, half);
     const double fl = floor(sa);
     const double f = __dsub_rn(sa, fl);
     const double eps = pow2(k - 49);

@@ -89,6 +89,7 @@ struct PointImage {
 };
 
 constexpr uint32_t kPointTable = 2048;  // doubles of grid-point table per block (16 KB)
+constexpr int kChunkTrips = 4;          // points per lane in a chunk of the image kernel's work queue
 
 // fills `pts` with the P x D grid points when they fit (returns true), else with the
 // 1-D coordinates for the per-point path
@@ -119,22 +120,15 @@ __global__ void __launch_bounds__(kThreads, 6) image_points_kernel(const ImageAr
   const uint32_t nboxes = a.n_src ? *a.n_src : (a.children ? 2u * n : n);
   const uint64_t P = a.points;
   const uint64_t total = uint64_t(nboxes) * P;
-  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
   const int lane = threadIdx.x & 31;
   if (M == ImageMode::Hit && a.children && 2ull * n > a.hit_cap) {
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(a.error, 1u);
     return;
   }
-  // point g = rank * P + k; (rank, k) advance by (stride / P, stride % P) per trip
-  const uint64_t g0 = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  uint64_t rank = g0 / P;
-  uint64_t k = g0 - rank * P;
-  const uint64_t rank_step = stride / P, k_step = stride - rank_step * P;
-
-  // the loop trip count is uniform per warp so that warp collectives stay converged
-  for (uint64_t base = g0 - lane; base < total; base += stride) {
-    const uint64_t g = base + lane;
-    const bool active = g < total;
+  // One point of the launch: g = rank * P + k (the source's rank among the sources, the
+  // point's index in its box).  Every lane of the warp calls it the same number of times
+  // (inactive lanes with active = false), so that the warp collectives stay converged.
+  auto point = [&](uint64_t g, uint64_t rank, uint64_t k, bool active) {
     uint32_t t = kInvalidIndex;
     uint32_t tbits[Map::D];
     bool valid = false;
@@ -145,9 +139,6 @@ __global__ void __launch_bounds__(kThreads, 6) image_points_kernel(const ImageAr
       valid = PI::image(a, pts, table, sbits, g, uint32_t(k), tbits);
       t = PI::target(a, n, valid, tbits);
     }
-    rank += rank_step;
-    k += k_step;
-    if (k >= P) { k -= P; ++rank; }
     if constexpr (M == ImageMode::Hit) {
       // one store per distinct target in the warp
       const unsigned peers = __match_any_sync(0xFFFFFFFFu, t);
@@ -179,6 +170,35 @@ __global__ void __launch_bounds__(kThreads, 6) image_points_kernel(const ImageAr
         if (pos < a.cand_cap) a.cand[pos] = tcode;
         else atomicOr(a.error, 1u);
       }
+    }
+  };
+
+  // A device work queue (a.work, zeroed by launch_image): every warp takes chunks of 32 x
+  // kChunkTrips consecutive points until none is left, so that warps that run ahead take
+  // more work and the SM stays full to the end (a static split leaves the slower warps
+  // alone at the end: 47 % of the warp slots were active on average, of 75 % possible).
+  constexpr uint64_t kChunk = 32ull * kChunkTrips;
+  const uint64_t chunks = (total + kChunk - 1) / kChunk;
+  for (;;) {
+    unsigned long long c = 0;
+    if (lane == 0) c = atomicAdd(a.work, 1ull);
+    c = __shfl_sync(0xFFFFFFFFu, c, 0);
+    if (c >= chunks) break;
+    const uint64_t g = c * kChunk + uint64_t(lane);
+    uint64_t rank, k;
+    if (total <= 0xFFFFFFFFull - kChunk) {
+      rank = uint32_t(g) / uint32_t(P);
+      k = uint32_t(g) - uint32_t(rank) * uint32_t(P);
+    } else {
+      rank = g / P;
+      k = g - rank * P;
+    }
+#pragma unroll 1
+    for (int j = 0; j < kChunkTrips; ++j) {
+      const uint64_t gj = g + 32ull * uint64_t(j);
+      point(gj, rank, k, gj < total);
+      k += 32;
+      while (k >= P) { k -= P; ++rank; }
     }
   }
 }
@@ -348,6 +368,9 @@ bool image_supported(uint32_t map_kind, uint32_t arith, uint32_t grid_kind, uint
 cudaError_t launch_image(uint32_t map_kind, uint32_t arith, uint32_t grid_kind, uint32_t dim, ImageMode mode,
                          const ImageArgs& a, uint64_t max_points, cudaStream_t s)
 {
+  if (!a.work) return cudaErrorInvalidValue;     // the image kernel takes its points from a work queue
+  const cudaError_t e = cudaMemsetAsync(a.work, 0, sizeof(unsigned long long), s);   // the queue starts empty
+  if (e != cudaSuccess) return e;
   return dispatch(map_kind, arith, grid_kind, dim, [&](auto map, auto grid) {
     return launch_image_t<decltype(map), decltype(grid)>(mode, a, max_points, s);
   });

@@ -40,6 +40,7 @@ struct ImageArgs {
   uint32_t* cand_count;
   uint32_t cand_cap;
   uint32_t* error;           // bit 0: capacity overflow
+  unsigned long long* work;  // the image kernel's work-queue counter (launch_image zeroes it)
 };
 
 // Transition rows: warp per source box, up to kMaxRowPoints points.

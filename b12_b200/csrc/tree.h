@@ -102,6 +102,7 @@ enum : int {
   C_SYNC = 9,      // 3 words for the grid barrier
   C_NNEW = 12,
   C_TGT = 13,      // the stored image targets overflowed their buffer
+  C_WORK = 14,     // 2 words (8-byte aligned): the image kernel's work-queue counter
   C_COUNT = 16
 };
 
