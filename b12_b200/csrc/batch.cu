@@ -118,16 +118,17 @@ struct BatchPoint {
   // W points: child[w], k[w]; returns their children-level targets (global child index,
   // kInvalidIndex when the image box is no child of a leaf, kOutsideIndex when the image
   // left the domain) and their instances
+  // inst[w]: the instance of child[w] (the caller tracks it along its points)
   static __device__ __forceinline__ void run(const BatchArgs& a, const uint32_t* off_s, const double* pts,
                                              const uint64_t (&child)[W], const uint32_t (&k)[W],
-                                             const bool (&act)[W], uint32_t (&target)[W], uint32_t (&inst)[W])
+                                             const bool (&act)[W], uint32_t (&target)[W],
+                                             const uint32_t (&inst)[W])
   {
     double x[W][D], y[W][D];
     int dep[W];
     MapParams mp[W];
 #pragma unroll
     for (int w = 0; w < W; ++w) {
-      inst[w] = act[w] ? find_instance(off_s, a.n_inst, child[w] >> 1) : 0u;
       dep[w] = a.inst_depth ? int(a.inst_depth[inst[w]]) : a.depth;
       const uint64_t c = child[w];
       const uint64_t code = act[w] ? ((a.codes[c >> 1] << 1) | (c & 1u)) : 0ull;
@@ -196,18 +197,30 @@ __global__ void __launch_bounds__(512) batch_image_kernel(const BatchArgs a)
     __syncthreads();
     if (start >= total) break;
     const uint64_t end = min(total, start + a.chunk);
+    // this thread's points g_w = start + threadIdx.x + w * blockDim.x + trip * span as
+    // (child, k) = (g / P, g % P), divided once per chunk and then advanced by span, with
+    // their instance found once and then followed along the (increasing) children
+    uint64_t child[W];
+    uint32_t k[W], inst[W];
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+      const uint64_t g = start + threadIdx.x + uint64_t(w) * blockDim.x;
+      if (total <= 0xFFFFFFFFull - span) {
+        child[w] = uint32_t(g) / uint32_t(P);
+        k[w] = uint32_t(g) - uint32_t(child[w]) * uint32_t(P);
+      } else {
+        child[w] = g / P;
+        k[w] = uint32_t(g - child[w] * P);
+      }
+      inst[w] = find_instance(off_s, a.n_inst, child[w] >> 1);
+    }
+    const uint64_t dchild = span / P;
+    const uint32_t dk = uint32_t(span - dchild * P);
     for (uint64_t base = start + threadIdx.x - lane; base < end; base += span) {
-      uint64_t child[W];
-      uint32_t k[W], target[W];
+      uint32_t target[W];
       bool act[W];
 #pragma unroll
-      for (int w = 0; w < W; ++w) {
-        const uint64_t g = base + lane + uint64_t(w) * blockDim.x;
-        act[w] = g < end;
-        child[w] = act[w] ? g / P : 0;
-        k[w] = act[w] ? uint32_t(g - child[w] * P) : 0u;
-      }
-      uint32_t inst[W];
+      for (int w = 0; w < W; ++w) act[w] = base + lane + uint64_t(w) * blockDim.x < end;
       BatchPoint<Map, Grid, W>::run(a, off_s, pts, child, k, act, target, inst);
 #pragma unroll
       for (int w = 0; w < W; ++w) {
@@ -223,6 +236,13 @@ __global__ void __launch_bounds__(512) batch_image_kernel(const BatchArgs a)
           const uint64_t tb = a.tgt_base[inst[w]];
           if (tb != ~0ull) a.targets[tb + (child[w] - 2ull * off_s[inst[w]]) * P + k[w]] = target[w];
         }
+      }
+#pragma unroll
+      for (int w = 0; w < W; ++w) {
+        child[w] += dchild;
+        k[w] += dk;
+        if (k[w] >= P) { k[w] -= uint32_t(P); ++child[w]; }
+        while (inst[w] + 1 < a.n_inst && (child[w] >> 1) >= off_s[inst[w] + 1]) ++inst[w];
       }
     }
   }
