@@ -481,9 +481,23 @@ def configs_mode(args, peak_tflops: float):
     sec, sweeps = _timed(lambda: t.continuation_run(sc, np.zeros(4), 24), 2)
     n = int(sweeps[-1])
     flop = 64 * 280
+    # one more run with CUDA events around every image launch (the insert-mode kernel)
+    t.profile(True)
+    t.profile_read(0)
+    t.continuation_run(sc, np.zeros(4), 24)
+    img_ms, img_n = t.profile_read(0)
+    t.profile(False)
+    img_tflops = n * flop / (img_ms * 1e-3) / 1e12 if img_ms > 0 else None
     out["coupled_duffing_continuation_d24"] = {
         "boxes": n, "sweeps": len(sweeps), "seconds": sec, "box_images": n,
         "box_images_per_s": n / sec, "tflops": n * flop / sec / 1e12, "flop_per_box_image": flop,
+        "roofline": {"bound": "fp64", "kernel": "image_points_kernel (insert mode, Stormer-Verlet, Philox grid)",
+                     "achieved": img_tflops, "peak": peak_tflops, "unit": "TFLOP/s",
+                     "frac": img_tflops / peak_tflops if img_tflops else None,
+                     "strict_cap": 0.5, "kernel_ms": img_ms, "launches": img_n,
+                     "note": "strict arithmetic (one rounding per operation, the reference's own "
+                             "SymplecticIntegratorAuto order): at most half the FMA peak; the rest of the run is "
+                             "the candidate sort, unique, merge and flag updates (launch list in profiles/)"},
         "note": "every box is imaged once, in the sweep after it was inserted"}
     if cpu:
         sweeps_ref = 20
