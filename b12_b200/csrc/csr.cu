@@ -300,19 +300,17 @@ __global__ void __launch_bounds__(kMeasureThreads) invariant_measure_kernel(Meas
   write_result(a, inv, inv_prev);
 }
 
-// Grid barrier that also reduces, on a counter that only grows: every block publishes its
-// partial sum and arrives; once the counter reaches (round + 1) x blocks every block adds
-// all partials itself, in the same fixed order (lane-strided, then a fixed shuffle tree),
-// so no block waits for a last arriver to publish the total.  Polls are bounded.
-__device__ bool barrier_allsum(const MeasureArgs& a, const double* part, uint32_t round, double* total)
+// Grid barrier on a counter that only grows, in two halves for a caller that has work to
+// start in between: the wait (every block publishes its partial sum and arrives with
+// release semantics, then polls with acquire loads, bounded) and the total (every block
+// adds all partials itself in one fixed order - lane-strided, then a fixed shuffle tree -
+// so no block waits for a last arriver to publish it).
+__device__ bool barrier_wait(const MeasureArgs& a, uint32_t round)
 {
   __shared__ int ok;
-  __shared__ double bcast;
   __syncthreads();
   if (threadIdx.x == 0) {
     ok = 1;
-    // arrive with release semantics (the block's stores, ordered by the block barrier,
-    // become visible first), then poll with acquire loads
     asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(a.bar_count) : "memory");
     const unsigned target = (round + 1u) * gridDim.x;
     unsigned long long polls = 0;
@@ -324,6 +322,12 @@ __device__ bool barrier_allsum(const MeasureArgs& a, const double* part, uint32_
     }
   }
   __syncthreads();
+  return ok && !(*(volatile unsigned*)a.error & 2u);
+}
+
+__device__ double barrier_total(const double* part)
+{
+  __shared__ double bcast;
   if (threadIdx.x < 32) {
     double x = 0.0;
     for (uint32_t i = threadIdx.x; i < gridDim.x; i += 32) x = __dadd_rn(x, __ldcg(part + i));
@@ -332,8 +336,9 @@ __device__ bool barrier_allsum(const MeasureArgs& a, const double* part, uint32_
     if (threadIdx.x == 0) bcast = x;
   }
   __syncthreads();
-  *total = bcast;
-  return ok && !(*(volatile unsigned*)a.error & 2u);
+  const double total = bcast;
+  __syncthreads();           // bcast is read by every thread before it can be written again
+  return total;
 }
 
 // The same iteration with the matrix held on chip.  Block b owns the rows of P^T whose
@@ -407,11 +412,22 @@ __global__ void __launch_bounds__(kMeasureThreads, 1) invariant_measure_smem_ker
     double* wc = (it & 1u) ? a.w1 : a.w0;
     double local = 0.0;
     double v[kSmemChunk];
+    // the gathers of the previous iterate go out first; the L1 norm of that iterate (the
+    // partial sums of the barrier before) is read while they are in flight, then every
+    // value is scaled by its inverse exactly as iterate_value scales it (the first
+    // iterate by 1, which leaves it unchanged)
 #pragma unroll
     for (int q = 0; q < kSmemChunk; ++q) {
       const uint32_t k = k0 + q;
-      v[q] = k < k1 ? iterate_value(wp, a.start, s_src[k], it, v0, inv) : 0.0;
+      v[q] = k < k1 ? (it == 0 ? (a.start ? __ldg(a.start + s_src[k]) : v0) : __ldcg(wp + s_src[k])) : 0.0;
     }
+    if (it > 0) {
+      const double s_prev = barrier_total(a.partial + ((it - 1) & 1u) * gridDim.x);
+      inv_prev = inv;
+      inv = __ddiv_rn(1.0, s_prev);
+    }
+#pragma unroll
+    for (int q = 0; q < kSmemChunk; ++q) v[q] = __dmul_rn(v[q], inv);
     // walk the run: a row that ends inside it is written here unless it began earlier
     uint32_t row = k0 < k1 ? s_row[k0] : 0u;
     double acc = 0.0, tail = 0.0;
@@ -456,10 +472,12 @@ __global__ void __launch_bounds__(kMeasureThreads, 1) invariant_measure_smem_ker
       for (int i = 0; i < kMeasureThreads / 32; ++i) sum = __dadd_rn(sum, red[i]);
       __stcg(a.partial + (it & 1u) * gridDim.x + blockIdx.x, sum);
     }
-    double s_it;
-    if (!barrier_allsum(a, a.partial + (it & 1u) * gridDim.x, it, &s_it)) return;
+    if (!barrier_wait(a, it)) return;
+  }
+  if (a.iters) {
+    const double s_last = barrier_total(a.partial + ((a.iters - 1) & 1u) * gridDim.x);
     inv_prev = inv;
-    inv = __ddiv_rn(1.0, s_it);
+    inv = __ddiv_rn(1.0, s_last);
   }
   write_result(a, inv, inv_prev);
 }
