@@ -388,7 +388,7 @@ def gpu_arm(args, rank: int, world: int, dist):
     import torch
     from b12_b200 import tree as T
 
-    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    dev = int(os.environ.get("LOCAL_RANK", "0")) % torch.cuda.device_count()
     torch.cuda.set_device(dev)
     # FP64 roofline denominator, measured on this device
     peak_tflops, _ = T.probe_fp64_fma(0.25)
@@ -397,6 +397,9 @@ def gpu_arm(args, rank: int, world: int, dist):
     cpu = cpu_baseline(cpu_cores()) if (rank == 0 and world == 1 and not args.no_cpu) else None
     configs = configs_mode(args, peak_tflops) if (rank == 0 and world == 1 and not args.no_configs) else None
     serving = serve_mode(args) if (rank == 0 and world == 1 and args.serve_jobs > 0) else None
+    # with several ranks, the workloads that shard by themselves (independent instances and
+    # jobs) are split over the ranks: every rank takes every world-th instance / job
+    sharded = sharded_mode(args, rank, world, dist, peak_tflops) if (world > 1 and not args.no_configs) else None
     if rank == 0:
         arith = "strict" if args.strict else "fma"
         line = {"metric": METRIC, "value": main["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -419,8 +422,59 @@ def gpu_arm(args, rank: int, world: int, dist):
             line["configs"] = configs
         if serving is not None:
             line["serving"] = serving
+        if sharded is not None:
+            line["sharded"] = sharded
         print(json.dumps(line), flush=True)
     return 0
+
+
+def sharded_mode(args, rank: int, world: int, dist, peak_tflops: float):
+    """The 512-instance Lorenz scan and the served stream split over the ranks (no
+    collective on the data path: each rank runs its own instances / jobs on its own GPU);
+    whole-job throughput = all ranks' units over the slowest rank's time.  Every rank
+    takes the same collective steps."""
+    import torch
+    import b12_b200 as B
+    from b12_b200.ranks import shard, throughput
+    from b12_b200.server import JobServer, replay
+    from b12_b200.workloads import LORENZ_CENTER, LORENZ_RADIUS, job_stream, lorenz_scan
+
+    dev = torch.cuda.current_device()
+    out = {}
+    rho, depth = lorenz_scan(512, 0)
+    mine = shard(range(512), world, rank)
+    b = B.Batch(LORENZ_CENTER, LORENZ_RADIUS, B.Scheme(B.lorenz(fma=True), B.inner_grid(5)),
+                [(10.0, rho[i], 8.0 / 3.0) for i in mine], [depth[i] for i in mine])
+    b.run()                                   # autotunes the launch shape
+    b.transition_matrices()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    b.run()
+    b.transition_matrices()
+    torch.cuda.synchronize()
+    sec = time.perf_counter() - t0
+    info = b.info()
+    b.close()
+    units = info["box_images"] + info["final_boxes"]
+    rate, total, slowest = throughput(dist, units, sec, dev)
+    out["lorenz_batch_512"] = {"instances_per_rank": len(mine), "box_images_per_s": rate, "box_images": total,
+                               "slowest_rank_s": slowest, "split": "instance i on rank i mod world",
+                               "scaling": "strong (the 512 instances are split)"}
+    if args.serve_jobs > 0:
+        jobs = [dict(j, arrival=0.0) for j in shard(job_stream(args.serve_jobs, 1.0, 0), world, rank)]
+        with JobServer(SERVE_CAP // world) as srv:
+            warm = [dict(j, arrival=0.0) for j in job_stream(min(len(jobs), 500), 1.0, 1)]
+            replay(srv, warm, lambda job, jid: srv.release(jid), timeout=SERVE_TIMEOUT)
+            if dist:
+                dist.barrier()
+            res = replay(srv, jobs, lambda job, jid: srv.release(jid), timeout=SERVE_TIMEOUT)
+        rate, total, slowest = throughput(dist, len(jobs), res["span"], dev)
+        out["served_stream"] = {"jobs_per_rank": len(jobs), "jobs_per_s": rate, "jobs": total,
+                                "slowest_rank_s": slowest, "split": "job j on rank j mod world, all submitted at once",
+                                "scaling": "strong (the stream is split)"}
+    return out
 
 
 # ------------------------------------------------------------------------------ other configurations
@@ -806,8 +860,10 @@ def main():
         import datetime
         import torch
         import torch.distributed as D
-        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        D.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")) % torch.cuda.device_count())
+        # B12_BENCH_BACKEND=gloo runs the ranks' timing collectives on the host (a check of
+        # the multi-rank steps on fewer GPUs than ranks; nothing on the data path waits)
+        D.init_process_group(os.environ.get("B12_BENCH_BACKEND", "nccl"), timeout=datetime.timedelta(seconds=120))
         dist = D
     try:
         return gpu_arm(args, rank, world, dist)
