@@ -462,17 +462,32 @@ def fixed_boxes(spec: dict, steps: int):
     return o, counts
 
 
+def count_at_depth(o: "Oracle", depth: int) -> int:
+    """ImplicitBoxTree::count(depth) (ImplicitBoxTree.hpp:1061-1095) for the trees the
+    continuation makes: 1 at depth 0, every leaf when all leaves have that depth, 0 for a
+    depth below every leaf (the remaining branch, boxes of an inner depth, is not needed)."""
+    if depth == 0:
+        return 1
+    d = o.leaves()[1]
+    if len(d) and (d == depth).all():
+        return o.n
+    if len(d) == 0 or depth > int(d.max()):
+        return 0
+    raise NotImplementedError("count at an inner depth of a tree of several depths")
+
+
 def continuation(spec: dict, depth: int, x0, max_sweeps: int = 10_000):
-    """continuation.m:13-44 at one depth; returns the oracle and per-sweep counts."""
+    """continuation.m:13-44 at one depth (its counts are count(d)); returns the oracle and
+    per-sweep counts."""
     o = Oracle(spec)
     o.delete_depth0()
     o.insert_points(np.asarray(x0, dtype=np.float64), depth, 2)
     counts = []
-    nb0, nb1 = 0, o.n
+    nb0, nb1 = 0, count_at_depth(o, depth)
     while nb1 > nb0 and len(counts) < max_sweeps:
         o.change_flags(2, 4)          # INS -> EXPD
         o.insert_by_image(4, 2, 0)    # insert images of EXPD boxes with INS
         o.unset_flags(4)              # drop EXPD
-        nb0, nb1 = nb1, o.n
+        nb0, nb1 = nb1, count_at_depth(o, depth)
         counts.append(nb1)
     return o, counts
