@@ -51,6 +51,72 @@ struct Domain {
   double inv_r[B12G_MAX_DIM];  // RN(1 / r) for the point-code fast path, 0 where it is not used
 };
 
+// Depth-dependent constants of dimension j at one depth, k = bisections of j: powers of
+// two and exact scalings, the same values whether the host computes them once for a
+// launch (the single-tree image kernels read them from their launch parameters) or a
+// kernel computes them for a depth of its own.
+struct AxisConst {
+  double rk;        // r_j 2^-k: the radius of a box
+  double s1k;       // 2^(1-k)
+  double yh;        // RN(1/r_j) 2^(k-1); 0 where the point-code fast path is off
+  double half;      // 2^(k-1)
+  double eps;       // 2^(k-49)
+  double one_eps;   // 1 - 2^(k-49)
+  double pk;        // 2^k
+  uint32_t mask;    // 2^k - 1, for k <= 32
+  int k;
+};
+
+// exact 2^e for |e| <= 1000
+__host__ __device__ __forceinline__ double pow2_hd(int e)
+{
+  const unsigned long long b = (unsigned long long)(1023 + e) << 52;
+#ifdef __CUDA_ARCH__
+  return __longlong_as_double((long long)b);
+#else
+  double d;
+  __builtin_memcpy(&d, &b, sizeof d);
+  return d;
+#endif
+}
+
+__host__ __device__ __forceinline__ AxisConst axis_const(const Domain& dom, int j, int k)
+{
+  AxisConst x;
+  x.rk = dom.r[j] * pow2_hd(-k);
+  x.s1k = pow2_hd(1 - k);
+  x.half = pow2_hd(k - 1);
+  x.yh = dom.inv_r[j] * x.half;
+  x.eps = pow2_hd(k - 49);
+  x.one_eps = 1.0 - x.eps;
+  x.pk = pow2_hd(k);
+  x.mask = uint32_t((k >= 64 ? ~0ull : (1ull << k) - 1ull) & 0xFFFFFFFFull);
+  x.k = k;
+  return x;
+}
+
+// every dimension's constants at a launch's depth, and the bisections one depth up (the
+// parents of children-mode launches)
+struct DepthConst {
+  AxisConst ax[B12G_MAX_DIM];
+  int k[B12G_MAX_DIM];       // bisections of each dimension at the depth
+  int kp[B12G_MAX_DIM];      // ... and at the depth above
+  int jd;                    // the dimension the depth's last bisection splits
+};
+
+// the constants of a launch at `depth` for a domain of `dim` dimensions
+inline void fill_depth_const(const Domain& dom, int dim, int depth, DepthConst& dc)
+{
+  auto bis = [&](int d, int j) { return d <= 0 ? 0 : d / dim + (j < d % dim ? 1 : 0); };
+  for (int j = 0; j < B12G_MAX_DIM; ++j) {
+    const int k = j < dim ? bis(depth, j) : 0;
+    dc.ax[j] = axis_const(dom, j < dim ? j : 0, k);
+    dc.k[j] = k;
+    dc.kp[j] = j < dim ? bis(depth - 1, j) : 0;
+  }
+  dc.jd = depth >= 1 ? (depth - 1) % dim : 0;
+}
+
 struct MapParams {
   double h, h2, h3, h6;      // step and h/2, h/3, h/6 (the reference divides at every use; same values)
   double p[6];
@@ -183,13 +249,19 @@ __device__ __forceinline__ uint64_t interleave(const uint32_t (&bits)[D], const 
 
 // centre and radius of dimension j of a box whose index in that dimension is `bits`
 // after k bisections
-__device__ __forceinline__ void box_axis(const Domain& dom, int j, uint32_t bits, int k, double& c, double& r)
+__device__ __forceinline__ void box_axis(const Domain& dom, const AxisConst& x, int j, uint32_t bits, double& c,
+                                         double& r)
 {
-  r = dom.r[j] * pow2(-k);
+  r = x.rk;
   // t = 2 bits 2^-k - 1: the scalings are exact, so one fused rounding gives the value of
   // the reference's rounded subtraction
-  const double t = __fma_rn(double(bits), pow2(1 - k), -1.0);
+  const double t = __fma_rn(double(bits), x.s1k, -1.0);
   c = __dadd_rn(__dadd_rn(__dmul_rn(t, dom.r[j]), dom.c[j]), r);
+}
+
+__device__ __forceinline__ void box_axis(const Domain& dom, int j, uint32_t bits, int k, double& c, double& r)
+{
+  box_axis(dom, axis_const(dom, j, k), j, bits, c, r);
 }
 
 // centre and radius of a box
@@ -211,6 +283,25 @@ __device__ __forceinline__ uint64_t pack_bits(const uint32_t* bits, int depth)
 #pragma unroll
   for (int j = 0; j < D; ++j) p = (p << bisections<D>(depth, j)) | uint64_t(bits[j]);
   return p;
+}
+
+template<int D>
+__device__ __forceinline__ uint64_t pack_bits_k(const uint32_t* bits, const int* k)
+{
+  uint64_t p = 0;
+#pragma unroll
+  for (int j = 0; j < D; ++j) p = (p << k[j]) | uint64_t(bits[j]);
+  return p;
+}
+
+template<int D>
+__device__ __forceinline__ void unpack_bits_k(uint64_t p, const int* k, uint32_t* bits)
+{
+#pragma unroll
+  for (int j = D - 1; j >= 0; --j) {
+    bits[j] = uint32_t(p & ((1ull << k[j]) - 1ull));
+    p >>= k[j];
+  }
 }
 
 template<int D>
@@ -240,22 +331,23 @@ __device__ __forceinline__ void unpack_bits(uint64_t p, int depth, uint32_t* bit
 // and from the exact s = RN(q + 1) 2^(k-1) by less than 2^(k-50.5).  When sa is at least
 // 2^(k-49) away from both neighbouring integers, floor(s) = floor(sa); otherwise
 // (probability about 2^(k-48)) the IEEE division decides, exactly as before.
-__device__ __forceinline__ uint32_t axis_index(const Domain& dom, int j, double pj, int k)
+// (k <= 32: the index is returned in 32 bits)
+__device__ __forceinline__ uint32_t axis_index(const Domain& dom, const AxisConst& a, int j, double pj)
 {
   const double x = __dsub_rn(pj, dom.c[j]);
-  const double y = dom.inv_r[j];
-  const unsigned long long mask = (1ull << k) - 1ull;
-  if (y != 0.0) {
-    const double half = pow2(k - 1);
-    const double sa = __fma_rn(x, y * half, half);
+  if (a.yh != 0.0) {
+    const double sa = __fma_rn(x, a.yh, a.half);
     const double fl = floor(sa);
     const double f = __dsub_rn(sa, fl);
-    const double eps = pow2(k - 49);
-    if (f >= eps && f <= __dsub_rn(1.0, eps)) return uint32_t((unsigned long long)fl & mask);
+    if (f >= a.eps && f <= a.one_eps) return uint32_t((unsigned long long)fl) & a.mask;
   }
   const double u = __dmul_rn(__dadd_rn(__ddiv_rn(x, dom.r[j]), 1.0), 0.5);
-  const double s = floor(u * pow2(k));
-  return uint32_t((unsigned long long)s & mask);
+  return uint32_t((unsigned long long)floor(u * a.pk)) & a.mask;
+}
+
+__device__ __forceinline__ uint32_t axis_index(const Domain& dom, int j, double pj, int k)
+{
+  return axis_index(dom, axis_const(dom, j, k), j, pj);
 }
 
 // per-dimension indices of the depth-d box that contains p; false if p lies outside
@@ -269,6 +361,19 @@ __device__ __forceinline__ bool point_bits(const Domain& dom, const double* p, i
   if (!inside) return false;
 #pragma unroll
   for (int j = 0; j < D; ++j) bits[j] = axis_index(dom, j, p[j], bisections<D>(depth, j));
+  return true;
+}
+
+// the same with the launch's constants of that depth
+template<int D>
+__device__ __forceinline__ bool point_bits(const Domain& dom, const DepthConst& dc, const double* p, uint32_t* bits)
+{
+  bool inside = true;
+#pragma unroll
+  for (int j = 0; j < D; ++j) inside = inside && (dom.lo[j] <= p[j]) && (p[j] < dom.hi[j]);
+  if (!inside) return false;
+#pragma unroll
+  for (int j = 0; j < D; ++j) bits[j] = axis_index(dom, dc.ax[j], j, p[j]);
   return true;
 }
 
@@ -335,10 +440,7 @@ constexpr int kHashMaxDepth = 56;
 // slots used for n keys: the smallest power of two >= 2n (load factor <= 1/2), >= 2^6
 __device__ __forceinline__ int hash_log2(uint32_t n)
 {
-  const uint64_t want = 2ull * n;
-  int l = 6;
-  while ((1ull << l) < want) ++l;
-  return l;
+  return n <= 32 ? 6 : 64 - __clzll(2ull * n - 1ull);   // 2^l >= 2n > 2^(l-1)
 }
 
 __device__ __forceinline__ uint64_t hash_slot(uint64_t code, int log2)
@@ -364,6 +466,19 @@ __device__ __forceinline__ uint32_t hash_locate(const LeafHash& h, uint32_t n, u
 // leaf index of the depth-d box with per-dimension indices `bits` (valid: inside the
 // domain) among the leaves of a single tree: the table of packed keys when built, the
 // binary search over the codes otherwise (with the out-of-domain rule of `locate`)
+// the same with the bisection counts of `depth` given
+template<int D>
+__device__ __forceinline__ uint32_t find_leaf_bits(const LeafHash& h, const uint64_t* codes, uint32_t n, bool valid,
+                                                   const uint32_t (&bits)[D], int depth, const int* k)
+{
+  if (h.slots && valid && n > 0) return hash_locate(h, n, pack_bits_k<D>(bits, k));
+  if (!valid || n == 0) return locate(codes, n, valid, 0);
+  int kk[D];
+#pragma unroll
+  for (int j = 0; j < D; ++j) kk[j] = k[j];
+  return locate(codes, n, true, interleave<D>(bits, kk, depth));
+}
+
 template<int D>
 __device__ __forceinline__ uint32_t find_leaf_bits(const LeafHash& h, const uint64_t* codes, uint32_t n, bool valid,
                                                    const uint32_t (&bits)[D], int depth)
@@ -392,10 +507,13 @@ __device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32
   }
 }
 
+// 2 m 2^-53 - 1 for the top 53 bits m of (hi, lo), exactly: with m = b 2^52 + f, the
+// double 1 + f 2^-52 has f as its fraction, and subtracting 2 - b from it is exact
+// (Sterbenz), so no integer-to-double conversion is needed
 __device__ __forceinline__ double philox_signed(uint32_t hi, uint32_t lo)
 {
-  const unsigned long long m = ((unsigned long long)hi << 32 | lo) >> 11;
-  return __dsub_rn(__dmul_rn(2.0, double(m) * 0x1p-53), 1.0);
+  const double x = __hiloint2double(int(0x3FF00000u | ((hi >> 11) & 0xFFFFFu)), int(__funnelshift_r(lo, hi, 11)));
+  return __dsub_rn(x, (hi >> 31) ? 1.0 : 2.0);
 }
 
 // Inner and full grids read a per-block table of the P grid points (dimension-major,
@@ -565,7 +683,7 @@ struct CoupledDuffingMap {
   static __device__ __forceinline__ void apply(const MapParams& m, const double* x, double* res)
   {
     double q0 = x[0], q1 = x[1], p0 = x[2], p1 = x[3];
-#pragma unroll 1
+#pragma unroll 2
     for (uint32_t s = 0; s < m.steps; ++s) {
       q0 = __dadd_rn(q0, __dmul_rn(__dmul_rn(0.5, p0), m.h));
       q1 = __dadd_rn(q1, __dmul_rn(__dmul_rn(0.5, p1), m.h));

@@ -24,13 +24,13 @@ struct PointImage {
   {
     if (a.hash.pk) {
       if (a.children) {
-        unpack_bits<D>(__ldg(a.hash.pk + (leaf >> 1)), a.depth - 1, bits);
-        const int jd = (a.depth - 1) % D;          // the last bisection splits dimension jd
+        unpack_bits_k<D>(__ldg(a.hash.pk + (leaf >> 1)), a.dc.kp, bits);
+        const int jd = a.dc.jd;                    // the last bisection splits dimension jd
 #pragma unroll
         for (int j = 0; j < D; ++j)                // (no dynamic index: the array stays in registers)
           if (j == jd) bits[j] = (bits[j] << 1) | (leaf & 1u);
       } else {
-        unpack_bits<D>(__ldg(a.hash.pk + leaf), a.depth, bits);
+        unpack_bits_k<D>(__ldg(a.hash.pk + leaf), a.dc.k, bits);
       }
       return;
     }
@@ -43,13 +43,11 @@ struct PointImage {
   // returns whether the image point lies in the domain; `tbits` its box's per-dimension
   // indices at a.depth.  `pts` is the block's grid-point table (dimension-major, P
   // entries per dimension) when the grid has one, else the 1-D coordinate table.
-  static __device__ __forceinline__ bool image(const ImageArgs& a, const double* pts, bool use_table,
-                                               const uint32_t (&sbits)[D], uint64_t i, uint32_t k,
-                                               uint32_t (&tbits)[D])
+  // the same from the source box's centre (its radius is the launch's)
+  static __device__ __forceinline__ bool image_at(const ImageArgs& a, const double* pts, bool use_table,
+                                                  const double (&c)[D], uint64_t i, uint32_t k, uint32_t (&tbits)[D])
   {
-    double c[D], r[D], g[D], x[D], y[D];
-#pragma unroll
-    for (int j = 0; j < D; ++j) box_axis(a.dom, j, sbits[j], bisections<D>(a.depth, j), c[j], r[j]);
+    double g[D], x[D], y[D];
     if (Grid::kTable && use_table) {
 #pragma unroll
       for (int j = 0; j < D; ++j) g[j] = pts[j * uint32_t(a.points) + k];
@@ -57,33 +55,48 @@ struct PointImage {
       Grid::template point<D>(a.grid, pts, i, k, g);
     }
 #pragma unroll
-    for (int j = 0; j < D; ++j) x[j] = __dadd_rn(c[j], __dmul_rn(g[j], r[j]));
+    for (int j = 0; j < D; ++j) x[j] = __dadd_rn(c[j], __dmul_rn(g[j], a.dc.ax[j].rk));
     Map::apply(a.map, x, y);
-    return point_bits<D>(a.dom, y, a.depth, tbits);
+    return point_bits<D>(a.dom, a.dc, y, tbits);
   }
 
-  // the depth-d code of a box (candidates of Insert mode)
-  static __device__ __forceinline__ uint64_t code_of(const ImageArgs& a, const uint32_t (&bits)[D])
+  static __device__ __forceinline__ bool image(const ImageArgs& a, const double* pts, bool use_table,
+                                               const uint32_t (&sbits)[D], uint64_t i, uint32_t k,
+                                               uint32_t (&tbits)[D])
   {
-    int k[D];
+    double c[D], r;
 #pragma unroll
-    for (int j = 0; j < D; ++j) k[j] = bisections<D>(a.depth, j);
-    return interleave<D>(bits, k, a.depth);
+    for (int j = 0; j < D; ++j) box_axis(a.dom, a.dc.ax[j], j, sbits[j], c[j], r);
+    return image_at(a, pts, use_table, c, i, k, tbits);
+  }
+
+  // centre of source `rank` from the launch's table
+  static __device__ __forceinline__ void source_centre(const ImageArgs& a, uint64_t rank, double (&c)[D])
+  {
+    const double2* p = reinterpret_cast<const double2*>(a.src_c + kSrcStride * rank);
+    const double2 c01 = __ldg(p);
+    c[0] = c01.x;
+    if (D > 1) c[D > 1 ? 1 : 0] = c01.y;
+    if (D > 2) {
+      const double2 c23 = __ldg(p + 1);
+      c[D > 2 ? 2 : 0] = c23.x;
+      if (D > 3) c[D > 3 ? 3 : 0] = c23.y;
+    }
   }
 
   static __device__ __forceinline__ uint32_t target(const ImageArgs& a, uint32_t n, bool valid,
                                                     const uint32_t (&tbits)[D])
   {
-    if (!a.children) return find_leaf_bits<D>(a.hash, a.codes, n, valid, tbits, a.depth);
+    if (!a.children) return find_leaf_bits<D>(a.hash, a.codes, n, valid, tbits, a.depth, a.dc.k);
     if (!valid) return kInvalidIndex;
-    const int jd = (a.depth - 1) % D;
+    const int jd = a.dc.jd;
     uint32_t pbits[D], child = 0;
 #pragma unroll
     for (int j = 0; j < D; ++j) {
       pbits[j] = j == jd ? tbits[j] >> 1 : tbits[j];
       if (j == jd) child = tbits[j] & 1u;
     }
-    const uint32_t p = find_leaf_bits<D>(a.hash, a.codes, n, true, pbits, a.depth - 1);
+    const uint32_t p = find_leaf_bits<D>(a.hash, a.codes, n, true, pbits, a.depth - 1, a.dc.kp);
     return p == kInvalidIndex ? kInvalidIndex : 2u * p + child;
   }
 };
@@ -133,10 +146,16 @@ __global__ void __launch_bounds__(kThreads, 6) image_points_kernel(const ImageAr
     uint32_t tbits[Map::D];
     bool valid = false;
     if (active) {
-      const uint32_t leaf = a.src ? __ldg(a.src + rank) : uint32_t(rank);
-      uint32_t sbits[Map::D];
-      PI::source_bits(a, leaf, sbits);
-      valid = PI::image(a, pts, table, sbits, g, uint32_t(k), tbits);
+      if constexpr (M == ImageMode::Insert) {   // Insert launches carry their source centres
+        double c[Map::D];
+        PI::source_centre(a, rank, c);
+        valid = PI::image_at(a, pts, table, c, g, uint32_t(k), tbits);
+      } else {
+        const uint32_t leaf = a.src ? __ldg(a.src + rank) : uint32_t(rank);
+        uint32_t sbits[Map::D];
+        PI::source_bits(a, leaf, sbits);
+        valid = PI::image(a, pts, table, sbits, g, uint32_t(k), tbits);
+      }
       t = PI::target(a, n, valid, tbits);
     }
     if constexpr (M == ImageMode::Hit) {
@@ -150,16 +169,18 @@ __global__ void __launch_bounds__(kThreads, 6) image_points_kernel(const ImageAr
     } else if constexpr (M == ImageMode::Search) {
       if (active) a.out[g] = t;
     } else {
-      // candidates: valid images that are not leaves; deduplicated within the warp and
-      // appended with one atomic per warp
+      // candidates: valid images that are not leaves, as packed keys (the caller turns them
+      // into codes); deduplicated within the warp and appended with one atomic per warp
       if (a.hit) {
         const unsigned hp = __match_any_sync(0xFFFFFFFFu, t);
         if (active && t != kInvalidIndex && lane == __ffs(hp) - 1) a.hit[t] = 1;
       }
       const bool is_cand = active && valid && t == kInvalidIndex;
-      const uint64_t tcode = is_cand ? PI::code_of(a, tbits) : 0ull;
+      const uint64_t tcode = is_cand ? pack_bits_k<Map::D>(tbits, a.dc.k) : 0ull;
       const uint64_t key = is_cand ? tcode : kInvalidCode;
-      const unsigned peers = __match_any_sync(0xFFFFFFFFu, key);
+      // (the lowest candidate lane of each key leads: a non-candidate lane may share the
+      // all-ones key)
+      const unsigned peers = __match_any_sync(0xFFFFFFFFu, key) & __ballot_sync(0xFFFFFFFFu, is_cand);
       const bool leader = is_cand && lane == __ffs(peers) - 1;
       const unsigned lead_mask = __ballot_sync(0xFFFFFFFFu, leader);
       uint32_t slot = 0;
@@ -371,16 +392,20 @@ cudaError_t launch_image(uint32_t map_kind, uint32_t arith, uint32_t grid_kind, 
   if (!a.work) return cudaErrorInvalidValue;     // the image kernel takes its points from a work queue
   const cudaError_t e = cudaMemsetAsync(a.work, 0, sizeof(unsigned long long), s);   // the queue starts empty
   if (e != cudaSuccess) return e;
+  ImageArgs b = a;
+  fill_depth_const(b.dom, int(dim), b.depth, b.dc);
   return dispatch(map_kind, arith, grid_kind, dim, [&](auto map, auto grid) {
-    return launch_image_t<decltype(map), decltype(grid)>(mode, a, max_points, s);
+    return launch_image_t<decltype(map), decltype(grid)>(mode, b, max_points, s);
   });
 }
 
 cudaError_t launch_rows(uint32_t map_kind, uint32_t arith, uint32_t grid_kind, uint32_t dim, const RowArgs& a,
                         uint32_t max_rows, cudaStream_t s)
 {
+  RowArgs b = a;
+  fill_depth_const(b.img.dom, int(dim), b.img.depth, b.img.dc);
   return dispatch(map_kind, arith, grid_kind, dim, [&](auto map, auto grid) {
-    return launch_rows_t<decltype(map), decltype(grid)>(a, max_rows, s);
+    return launch_rows_t<decltype(map), decltype(grid)>(b, max_rows, s);
   });
 }
 

@@ -9,6 +9,7 @@
 // and no candidate equals a leaf.
 #include <algorithm>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "sort.h"
@@ -64,6 +65,79 @@ cudaError_t launch_locate_points(uint32_t dim, const double* pts, uint32_t n_pts
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
+}
+
+// the centre of every source box by rank (kSrcStride doubles a source), for the image
+// kernel: its points then read the centre instead of decoding the code and rebuilding
+// the box for each point
+template<int D>
+__global__ void source_centres_kernel(const uint64_t* __restrict__ codes, const uint32_t* __restrict__ src,
+                                      const uint32_t* n_src, uint32_t n_all, Domain dom, DepthConst dc, int depth,
+                                      double* __restrict__ out)
+{
+  const uint32_t n = n_src ? *n_src : n_all;
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    const uint64_t code = __ldg(codes + (src ? __ldg(src + r) : r));
+    double c[kSrcStride] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int j = 0; j < D; ++j) {
+      double rr;
+      box_axis(dom, dc.ax[j], j, deinterleave<D>(code, depth, j), c[j], rr);
+    }
+    double2* o = reinterpret_cast<double2*>(out + size_t(kSrcStride) * r);
+    o[0] = make_double2(c[0], c[1]);
+    o[1] = make_double2(c[2], c[3]);
+  }
+}
+
+// packed keys (pack_bits at `depth`) -> depth-d codes, in place
+template<int D>
+__global__ void packed_to_codes_kernel(uint64_t* keys, const uint32_t* n_ptr, DepthConst dc, int depth)
+{
+  const uint32_t n = *n_ptr;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    uint32_t bits[D];
+    unpack_bits_k<D>(keys[i], dc.k, bits);
+    int k[D];
+#pragma unroll
+    for (int j = 0; j < D; ++j) k[j] = dc.k[j];
+    keys[i] = interleave<D>(bits, k, depth);
+  }
+}
+
+template<class F>
+cudaError_t by_dim(uint32_t dim, F&& f)
+{
+  switch (dim) {
+    case 1: return f(std::integral_constant<int, 1>{});
+    case 2: return f(std::integral_constant<int, 2>{});
+    case 3: return f(std::integral_constant<int, 3>{});
+    case 4: return f(std::integral_constant<int, 4>{});
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+int grid_over(uint64_t n, int per_sm = 8)
+{
+  const uint64_t want = std::max<uint64_t>((n + kThreads - 1) / kThreads, 1);
+  return int(std::min<uint64_t>(want, uint64_t(device_sm_count()) * per_sm));
+}
+
+// the source centres of an image launch over n_src sources (t->srcc)
+b12g_status source_centres(b12g_tree* t, Prepared& pr, uint32_t n_src)
+{
+  ST(t->srcc.ensure_room(uint64_t(std::max<uint32_t>(n_src, 1)) * kSrcStride, "source centres", 2));
+  DepthConst dc;
+  fill_depth_const(t->dom, int(t->domain.dim), t->depth, dc);
+  const int g = grid_over(n_src);
+  CK(by_dim(t->domain.dim, [&](auto d) {
+    source_centres_kernel<decltype(d)::value><<<g, kThreads, 0, t->stream>>>(
+        t->codes(), pr.a.src, pr.a.n_src, n_src, t->dom, dc, int(t->depth), t->srcc.p);
+    return cudaGetLastError();
+  }));
+  count_launches(1);
+  pr.a.src_c = t->srcc.p;
+  return B12G_OK;
 }
 
 // candidates (count in C_CAND) -> sorted unique codes in t->cand2 (count in C_NNEW)
@@ -252,6 +326,7 @@ b12g_status insert_by_image_impl(b12g_tree* t, const b12g_scheme* sc, uint8_t de
   } else {
     ST(build_current_hash(t, pr));
   }
+  ST(source_centres(t, pr, n_src));
   // room for every point to be a new box; grows (and the images are recomputed) on overflow
   uint64_t cap = std::min<uint64_t>(points, std::max<uint64_t>(uint64_t(t->cand.n), uint64_t(1) << 20));
   for (int attempt = 0; attempt < 8; ++attempt) {
@@ -274,6 +349,18 @@ b12g_status insert_by_image_impl(b12g_tree* t, const b12g_scheme* sc, uint8_t de
       ST(set_ctr(t, C_ERROR, 0));
       cap = std::min<uint64_t>(points, std::max<uint64_t>(uint64_t(m), cap * 2));
       continue;
+    }
+    if (m > 0) {
+      // the image kernel appends packed keys: codes for the sort and the merge
+      DepthConst dc;
+      fill_depth_const(t->dom, int(t->domain.dim), int(depth), dc);
+      const int g = grid_over(m);
+      CK(by_dim(t->domain.dim, [&](auto d) {
+        packed_to_codes_kernel<decltype(d)::value><<<g, kThreads, 0, t->stream>>>(t->cand.p, t->ctr.p + C_CAND, dc,
+                                                                                 int(depth));
+        return cudaGetLastError();
+      }));
+      count_launches(1);
     }
     ST(apply_hit_flags(t, hit_flags));
     uint32_t u = 0;

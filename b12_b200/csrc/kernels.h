@@ -16,6 +16,8 @@ enum class ImageMode : int {
 };
 
 // One box-image launch over a uniform-depth leaf set.
+constexpr int kSrcStride = 4;    // doubles per source in ImageArgs::src_c (two 16-byte loads)
+
 struct ImageArgs {
   Domain dom;
   MapParams map;
@@ -23,9 +25,12 @@ struct ImageArgs {
   const uint64_t* codes;     // sorted leaf codes (parents in children mode)
   const uint32_t* n_leaves;  // device count of `codes`
   int depth;                 // depth of the imaged boxes (children depth in children mode)
+  DepthConst dc;             // constants of `depth` (launch_image / launch_rows fill them in)
   int children;              // 1: boxes are the 2n children of `codes`, never materialised
   const uint32_t* src;       // source leaf ranks -> leaf index (nullptr: all leaves)
   const uint32_t* n_src;     // device count of sources (nullptr: all leaves / children)
+  const double* src_c;       // optional: the centre of every source box by rank, kSrcStride
+                             // doubles a source (the radius is dc's); nullptr: from the codes
   uint64_t points;           // points per box
   LeafHash hash;             // leaf lookup table (slots == nullptr: binary search)
   // outputs
@@ -36,7 +41,7 @@ struct ImageArgs {
   uint64_t targets_cap;      // entries of `targets`; a point beyond sets *targets_over
   uint32_t* targets_over;
   uint32_t* out;
-  uint64_t* cand;            // insert candidates (depth-d codes)
+  uint64_t* cand;            // insert candidates: packed keys (pack_bits) of depth-d boxes
   uint32_t* cand_count;
   uint32_t cand_cap;
   uint32_t* error;           // bit 0: capacity overflow

@@ -126,6 +126,7 @@ struct b12g_tree {
   Buf<uint32_t> tiles_a, tiles_b;
   Buf<uint32_t> src, out, stage_col, stage_cnt, row_count, rowptr;
   Buf<uint64_t> cand, cand2;
+  Buf<double> srcc;            // centres of an image launch's source boxes (kSrcStride a source)
   Buf<uint32_t> sort_idx;
   Buf<double> table;
   Buf<double> points;
