@@ -433,6 +433,8 @@ struct LeafHash {
   uint32_t log2_cap;         // table capacity (slots allocated) = 2^log2_cap
   uint64_t* pk;              // single-tree tables: every leaf's packed key (pack_bits), which
                              // the image kernels read as their source box's indices
+  uint32_t log2_use;         // nonzero: the table uses 2^log2_use slots whatever the leaf
+                             // count (a table kept while boxes are added to it)
 };
 
 constexpr int kHashMaxDepth = 56;
@@ -448,9 +450,15 @@ __device__ __forceinline__ uint64_t hash_slot(uint64_t code, int log2)
   return (code * 0x9E3779B97F4A7C15ull) >> (64 - log2);
 }
 
+// log2 of the slots a table of n keys uses
+__device__ __forceinline__ int table_log2(const LeafHash& h, uint32_t n)
+{
+  return h.log2_use ? int(h.log2_use) : hash_log2(n);
+}
+
 __device__ __forceinline__ uint32_t hash_locate(const LeafHash& h, uint32_t n, uint64_t code)
 {
-  const int l = hash_log2(n);
+  const int l = table_log2(h, n);
   const uint64_t mask = (1ull << l) - 1ull;
   const uint64_t key = (uint64_t(h.tag) << 56) | code;
   uint64_t s = hash_slot(code, l);
@@ -461,6 +469,37 @@ __device__ __forceinline__ uint32_t hash_locate(const LeafHash& h, uint32_t n, u
     s = (s + 1) & mask;
   }
   return kInvalidIndex;
+}
+
+// Claims the box of packed key `code` in a table kept while boxes are added to it
+// (h.log2_use set): true if this call added it (value kAbsentIndex: present, no leaf
+// index), false if it was there already.  Linear probing with a CAS on the key word; a
+// CAS lost to another claim re-reads the same slot.  Lookups running at the same time
+// may read a slot before a claim lands; they then try the claim too and see the key.
+// A table with no free slot sets bit 0 of `error`.
+__device__ __forceinline__ bool hash_claim(const LeafHash& h, uint64_t code, uint32_t* error)
+{
+  const uint64_t mask = (1ull << h.log2_use) - 1ull;
+  const unsigned long long key = (uint64_t(h.tag) << 56) | code;
+  uint64_t s = hash_slot(code, int(h.log2_use));
+  unsigned long long expect = 0;     // first guess for a slot: never used
+  for (uint64_t step = 0; step <= 2 * mask + 64; ++step) {
+    unsigned long long* kw = reinterpret_cast<unsigned long long*>(&h.slots[s].x);
+    const unsigned long long cur = atomicCAS(kw, expect, key);
+    if (cur == expect) {             // an empty slot (tag 0 or an old tag) now holds the key
+      h.slots[s].y = kAbsentIndex;
+      return true;
+    }
+    if (cur == key) return false;
+    if ((cur >> 56) != h.tag) {
+      expect = cur;                  // empty under an old tag: try it again with its value
+      continue;
+    }
+    s = (s + 1) & mask;
+    expect = 0;
+  }
+  atomicOr(error, 1u);
+  return false;
 }
 
 // leaf index of the depth-d box with per-dimension indices `bits` (valid: inside the

@@ -181,7 +181,8 @@ __global__ void __launch_bounds__(kThreads, 6) image_points_kernel(const ImageAr
       // (the lowest candidate lane of each key leads: a non-candidate lane may share the
       // all-ones key)
       const unsigned peers = __match_any_sync(0xFFFFFFFFu, key) & __ballot_sync(0xFFFFFFFFu, is_cand);
-      const bool leader = is_cand && lane == __ffs(peers) - 1;
+      bool leader = is_cand && lane == __ffs(peers) - 1;
+      if (a.claim && leader) leader = hash_claim(a.hash, tcode, a.error);
       const unsigned lead_mask = __ballot_sync(0xFFFFFFFFu, leader);
       uint32_t slot = 0;
       if (lane == 0 && lead_mask) slot = atomicAdd(a.cand_count, uint32_t(__popc(lead_mask)));

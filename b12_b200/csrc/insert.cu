@@ -123,28 +123,56 @@ int grid_over(uint64_t n, int per_sm = 8)
   return int(std::min<uint64_t>(want, uint64_t(device_sm_count()) * per_sm));
 }
 
-// the source centres of an image launch over n_src sources (t->srcc)
-b12g_status source_centres(b12g_tree* t, Prepared& pr, uint32_t n_src)
+// centres of the boxes codes[src[r]] (codes[r] without a list), r < *n_src (at most
+// max_src), at the tree's depth, into t->srcc
+b12g_status centres_of(b12g_tree* t, const uint64_t* codes, const uint32_t* src, const uint32_t* n_src,
+                       uint32_t max_src)
 {
-  ST(t->srcc.ensure_room(uint64_t(std::max<uint32_t>(n_src, 1)) * kSrcStride, "source centres", 2));
+  ST(t->srcc.ensure_room(uint64_t(std::max<uint32_t>(max_src, 1)) * kSrcStride, "source centres", 2));
   DepthConst dc;
   fill_depth_const(t->dom, int(t->domain.dim), t->depth, dc);
-  const int g = grid_over(n_src);
+  const int g = grid_over(max_src);
   CK(by_dim(t->domain.dim, [&](auto d) {
-    source_centres_kernel<decltype(d)::value><<<g, kThreads, 0, t->stream>>>(
-        t->codes(), pr.a.src, pr.a.n_src, n_src, t->dom, dc, int(t->depth), t->srcc.p);
+    source_centres_kernel<decltype(d)::value><<<g, kThreads, 0, t->stream>>>(codes, src, n_src, max_src, t->dom, dc,
+                                                                             int(t->depth), t->srcc.p);
     return cudaGetLastError();
   }));
   count_launches(1);
+  return B12G_OK;
+}
+
+// the source centres of an image launch over n_src sources
+b12g_status source_centres(b12g_tree* t, Prepared& pr, uint32_t n_src)
+{
+  ST(centres_of(t, t->codes(), pr.a.src, pr.a.n_src, n_src));
   pr.a.src_c = t->srcc.p;
   return B12G_OK;
 }
 
 // candidates (count in C_CAND) -> sorted unique codes in t->cand2 (count in C_NNEW)
-b12g_status sort_unique_candidates(b12g_tree* t, uint32_t m, uint8_t depth, uint32_t* u)
+b12g_status sort_unique_candidates(b12g_tree* t, uint32_t m, uint8_t depth, uint32_t* u, bool distinct = false)
 {
   *u = 0;
   if (m == 0) return set_ctr(t, C_NNEW, 0);
+  if (distinct) {
+    // candidates that are distinct already (claimed in the lookup table): the sort alone
+    const uint64_t cells = sort_scratch_u32(m);
+    ST(t->cand2.ensure(m, "candidate sort"));
+    ST(t->sort_idx.ensure(cells + 8, "candidate sort scratch"));
+    uint64_t* sorted = nullptr;
+    const int bits = std::max(8, ((int(depth) + 7) / 8) * 8);
+    // (its error bits go to C_DEFER, read with the next counter read-back)
+    CK(radix_sort_u64(t->cand.p, t->cand2.p, t->ctr.p + C_CAND, m, bits, t->sort_idx.p, t->ctr.p + C_DEFER, &sorted,
+                      t->stream));
+    count_launches(uint64_t(sort_launches(bits)));
+    if (sorted == t->cand.p) {     // merge_new reads t->cand2
+      std::swap(t->cand.p, t->cand2.p);
+      std::swap(t->cand.n, t->cand2.n);
+    }
+    CK(cudaMemcpyAsync(t->ctr.p + C_NNEW, t->ctr.p + C_CAND, sizeof(uint32_t), cudaMemcpyDeviceToDevice, t->stream));
+    *u = m;
+    return B12G_OK;
+  }
   const uint64_t cells = sort_scratch_u32(m);
   ST(t->cand2.ensure(m, "candidate sort"));
   ST(t->sort_idx.ensure(cells + 2 * (size_t(m) + 1) + compact_tiles(uint64_t(m) + 1) + 8, "candidate sort scratch"));
@@ -168,17 +196,18 @@ b12g_status sort_unique_candidates(b12g_tree* t, uint32_t m, uint8_t depth, uint
   return B12G_OK;
 }
 
-// merge the u unique new codes of t->cand2 into the leaves with flags `ins`
-b12g_status merge_new(b12g_tree* t, uint32_t u, uint8_t ins)
+// merge the u unique new codes of t->cand2 into the leaves with flags `ins`; the old
+// leaves' flags are ANDed with `a_keep`
+b12g_status merge_new(b12g_tree* t, uint32_t u, uint8_t ins, uint8_t a_keep = 0xFF, bool wait = true)
 {
   if (u == 0) return B12G_OK;
   const uint64_t total = uint64_t(t->n) + u;
   ST(reserve(t, total));
   const int o = 1 - t->cur, no = 1 - t->ncur;
-  CK(merge_sorted(t->codes(), t->flg(), t->dn(), t->cand2.p, ins, t->ctr.p + C_NNEW, uint32_t(total), t->code[o].p,
-                  t->flags[o].p, t->ctr.p + no, t->stream));
+  CK(merge_sorted(t->codes(), t->flg(), t->dn(), a_keep, t->cand2.p, ins, t->ctr.p + C_NNEW, uint32_t(total),
+                  t->code[o].p, t->flags[o].p, t->ctr.p + no, t->stream));
   count_launches(1);
-  ST(sync(t, "merge"));
+  if (wait) ST(sync(t, "merge"));
   t->cur = o;
   ++t->leaf_gen;
   t->ncur = no;
@@ -278,14 +307,108 @@ b12g_status insert_points_impl(b12g_tree* t, const double* points, uint64_t n_po
   return B12G_OK;
 }
 
-// A lookup table kept across the sweeps of a continuation: built for n leaves, it takes
-// each sweep's new boxes (marked present only: the insertion asks whether an image box is
-// a leaf, not which one) until the leaf count needs a larger table, when it is rebuilt.
+// A lookup table kept across the sweeps of a continuation: built for n leaves with
+// 2^l >= 4n slots (at least 2^16), it takes each sweep's new boxes as the image kernel
+// finds them (claimed: marked present only, since the insertion asks whether an image
+// box is a leaf, not which one), so the candidates come out distinct; a sweep that at
+// most doubles the count leaves it at most half full.  It is rebuilt when the leaf count
+// asks for a larger one, or one size up when a claim found no free slot.
 struct PresenceTable {
   LeafHash h{};
-  uint32_t l = 0;       // log2 of the slots the table's lookups use
+  uint32_t l = 0;       // log2 of the table's slots
+  uint32_t extra = 0;   // sizes added after a full table
   bool ok = false;
 };
+
+uint32_t presence_log2(uint32_t n, uint32_t extra)
+{
+  return std::max<uint32_t>(host_hash_log2(2ull * std::max<uint32_t>(n, 1)), 16) + extra;
+}
+
+b12g_status build_presence_table(b12g_tree* t, PresenceTable* keep)
+{
+  const uint32_t l = presence_log2(t->n, keep->extra);
+  ST(ensure_hash(t, uint64_t(1) << (l - 1)));      // >= 2^l slots
+  uint32_t tag = 0;
+  ST(next_hash_tag(t, &tag));
+  keep->h = LeafHash{t->hash.p, tag, t->hash_log2, t->pk.p, l};
+  CK(build_leaf_hash(t->codes(), t->dn(), int(t->depth), int(t->domain.dim), keep->h, t->ctr.p + C_ERROR, t->n,
+                     t->stream));
+  count_launches(1);
+  keep->h.pk = nullptr;      // leaf indices move with every merge
+  keep->l = l;
+  keep->ok = true;
+  return B12G_OK;
+}
+
+// the error bits C_DEFER collected (host copy read): a timeout or capacity failure of the
+// launch that set them
+b12g_status deferred_errors(b12g_tree* t)
+{
+  const uint32_t e = t->h_ctr[C_DEFER];
+  if (!e) return B12G_OK;
+  set_ctr(t, C_DEFER, 0);
+  if (e & 2u) return fail(B12G_ERR_TIMEOUT, "candidate sort: a bounded device wait gave up");
+  return fail(B12G_ERR_CAPACITY, "candidate sort: inconsistent digit counts");
+}
+
+// The image kernel in Insert mode over `points` points of the prepared sources (their
+// centres at pr.a.src_c), run again with more room when a buffer overflows; the
+// candidates end as depth-d codes in t->cand, *m of them (also at C_CAND).  With `keep`
+// (pr.a.claim set) they are distinct new boxes, claimed in its table.
+b12g_status image_candidates(b12g_tree* t, const b12g_scheme* sc, Prepared& pr, uint64_t points, uint8_t depth,
+                             uint8_t hit_flags, PresenceTable* keep, uint32_t* m_out)
+{
+  // room for every point to be a new box; grows (and the images are recomputed) on overflow
+  uint64_t cap = std::min<uint64_t>(points, std::max<uint64_t>(uint64_t(t->cand.n), uint64_t(1) << 20));
+  for (int attempt = 0; attempt < 8; ++attempt) {
+    ST(ensure_candidates(t, cap));
+    ST(set_ctr(t, C_CAND, 0));
+    pr.a.cand = t->cand.p;
+    pr.a.cand_count = t->ctr.p + C_CAND;
+    pr.a.cand_cap = uint32_t(std::min<size_t>(t->cand.n, 0xFFFFFFFFu));
+    pr.a.hit = hit_flags ? t->hit.p : nullptr;
+    prof_mark(t, 0);
+    CK(launch_image(sc->map.kind, sc->map.arith, sc->grid.kind, t->domain.dim, ImageMode::Insert, pr.a, points,
+                    t->stream));
+    prof_mark(t, 0);
+    count_launches(1);
+    // one read-back: the error word, the candidate count, and the deferred error bits of
+    // the launches before
+    ST(read_ctr(t, C_ERROR, C_DEFER - C_ERROR + 1));
+    ST(prof_collect(t));
+    ST(deferred_errors(t));
+    const uint32_t m = t->h_ctr[C_CAND];
+    if (t->h_ctr[C_ERROR] & 1u) {
+      ST(set_ctr(t, C_ERROR, 0));
+      if (keep) {
+        // the failed launch claimed boxes it did not keep: a fresh table, one size up if
+        // a claim found it full
+        if (m <= pr.a.cand_cap) ++keep->extra;
+        ST(build_presence_table(t, keep));
+        pr.a.hash = keep->h;
+      }
+      cap = std::min<uint64_t>(points, std::max<uint64_t>(uint64_t(m), cap * 2));
+      continue;
+    }
+    if (m > 0) {
+      // the image kernel appends packed keys: codes for the sort and the merge
+      DepthConst dc;
+      fill_depth_const(t->dom, int(t->domain.dim), int(depth), dc);
+      const int g = grid_over(m);
+      CK(by_dim(t->domain.dim, [&](auto d) {
+        packed_to_codes_kernel<decltype(d)::value><<<g, kThreads, 0, t->stream>>>(t->cand.p, t->ctr.p + C_CAND, dc,
+                                                                                 int(depth));
+        return cudaGetLastError();
+      }));
+      count_launches(1);
+    }
+    ST(apply_hit_flags(t, hit_flags));
+    *m_out = m;
+    return B12G_OK;
+  }
+  return fail(B12G_ERR_CAPACITY, "insert_by_image: candidate buffer retries exhausted");
+}
 
 b12g_status insert_by_image_impl(b12g_tree* t, const b12g_scheme* sc, uint8_t depth, uint8_t ins, uint8_t hit_flags,
                                  uint32_t* n_inserted, PresenceTable* keep = nullptr)
@@ -312,74 +435,53 @@ b12g_status insert_by_image_impl(b12g_tree* t, const b12g_scheme* sc, uint8_t de
     if (n_inserted) *n_inserted = 0;
     return B12G_OK;
   }
-  if (keep && !hit_flags) {
-    if (keep->ok && host_hash_log2(t->n) == keep->l) {
-      pr.a.hash = keep->h;
-    } else {
-      ST(build_current_hash(t, pr));
-      keep->ok = pr.a.hash.slots != nullptr;
-      keep->l = host_hash_log2(t->n);
-      keep->h = pr.a.hash;
-      keep->h.pk = nullptr;      // leaf indices move with every merge: sources from the codes
-    }
-    pr.a.hash.pk = nullptr;
+  const bool claim = keep && !hit_flags && t->depth <= kHashMaxDepth && t->domain.dim >= 2 && t->n > 0;
+  if (claim) {
+    if (!keep->ok || keep->l != presence_log2(t->n, keep->extra)) ST(build_presence_table(t, keep));
+    pr.a.hash = keep->h;
+    pr.a.claim = 1;
   } else {
     ST(build_current_hash(t, pr));
   }
   ST(source_centres(t, pr, n_src));
-  // room for every point to be a new box; grows (and the images are recomputed) on overflow
-  uint64_t cap = std::min<uint64_t>(points, std::max<uint64_t>(uint64_t(t->cand.n), uint64_t(1) << 20));
-  for (int attempt = 0; attempt < 8; ++attempt) {
-    ST(ensure_candidates(t, cap));
-    ST(set_ctr(t, C_CAND, 0));
-    pr.a.cand = t->cand.p;
-    pr.a.cand_count = t->ctr.p + C_CAND;
-    pr.a.cand_cap = uint32_t(std::min<size_t>(t->cand.n, 0xFFFFFFFFu));
-    pr.a.hit = hit_flags ? t->hit.p : nullptr;
-    prof_mark(t, 0);
-    CK(launch_image(sc->map.kind, sc->map.arith, sc->grid.kind, t->domain.dim, ImageMode::Insert, pr.a, points,
-                    t->stream));
-    prof_mark(t, 0);
-    count_launches(1);
-    ST(read_ctr(t, C_CAND, 1));
-    ST(prof_collect(t));
-    const uint32_t m = t->h_ctr[C_CAND];
-    ST(read_ctr(t, C_ERROR, 1));
-    if (t->h_ctr[C_ERROR] & 1u) {
-      ST(set_ctr(t, C_ERROR, 0));
-      cap = std::min<uint64_t>(points, std::max<uint64_t>(uint64_t(m), cap * 2));
-      continue;
-    }
-    if (m > 0) {
-      // the image kernel appends packed keys: codes for the sort and the merge
-      DepthConst dc;
-      fill_depth_const(t->dom, int(t->domain.dim), int(depth), dc);
-      const int g = grid_over(m);
-      CK(by_dim(t->domain.dim, [&](auto d) {
-        packed_to_codes_kernel<decltype(d)::value><<<g, kThreads, 0, t->stream>>>(t->cand.p, t->ctr.p + C_CAND, dc,
-                                                                                 int(depth));
-        return cudaGetLastError();
-      }));
-      count_launches(1);
-    }
-    ST(apply_hit_flags(t, hit_flags));
-    uint32_t u = 0;
-    ST(sort_unique_candidates(t, m, depth, &u));
-    ST(merge_new(t, u, ins));
-    if (keep && keep->ok && u > 0) {
-      if (host_hash_log2(t->n) == keep->l) {
-        // the u new codes are still in t->cand2, their count at C_NNEW
-        CK(add_to_leaf_hash(t->cand2.p, t->ctr.p + C_NNEW, int(keep->l), int(depth), int(t->domain.dim), keep->h,
-                            t->ctr.p + C_ERROR, u, t->stream));
-        count_launches(1);
-      } else {
-        keep->ok = false;
-      }
-    }
-    if (n_inserted) *n_inserted = u;
-    return B12G_OK;
-  }
-  return fail(B12G_ERR_CAPACITY, "insert_by_image: candidate buffer retries exhausted");
+  uint32_t m = 0, u = 0;
+  ST(image_candidates(t, sc, pr, points, depth, hit_flags, claim ? keep : nullptr, &m));
+  ST(sort_unique_candidates(t, m, depth, &u, claim));
+  ST(merge_new(t, u, ins));          // (claimed boxes are in the table already)
+  if (n_inserted) *n_inserted = u;
+  return B12G_OK;
+}
+
+// One sweep of the continuation on a tree of one depth whose sources are given by their
+// centres (t->srcc, n_src of them: the boxes the sweep before inserted, which carry INS
+// and no other leaf does): the images of their points claim the new boxes in the kept
+// presence table, the new boxes are sorted and merged in with INS while every old leaf
+// loses INS and EXPD, and their centres become the next sweep's sources.  This is
+// changeFlags(INS -> EXPD), insert(scheme of the EXPD boxes, INS) and unsetFlags(EXPD)
+// with the flag passes folded into the merge; a sweep that inserts nothing leaves the
+// flags to the caller.
+b12g_status continuation_sweep(b12g_tree* t, const b12g_scheme* sc, uint8_t depth, PresenceTable* keep,
+                               uint32_t n_src, uint32_t* u_out)
+{
+  *u_out = 0;
+  Prepared pr;
+  ST(prepare(t, sc, pr));
+  const uint64_t points = uint64_t(n_src) * pr.P;
+  if (points == 0) return B12G_OK;
+  ST(set_ctr(t, C_NSRC, n_src));
+  pr.a.src = nullptr;
+  pr.a.n_src = t->ctr.p + C_NSRC;
+  pr.a.src_c = t->srcc.p;
+  if (!keep->ok || keep->l != presence_log2(t->n, keep->extra)) ST(build_presence_table(t, keep));
+  pr.a.hash = keep->h;
+  pr.a.claim = 1;
+  uint32_t m = 0, u = 0;
+  ST(image_candidates(t, sc, pr, points, depth, 0, keep, &m));
+  ST(sort_unique_candidates(t, m, depth, &u, true));
+  ST(merge_new(t, u, B12G_INS, uint8_t(~(B12G_INS | B12G_EXPD)), false));
+  if (u > 0) ST(centres_of(t, t->cand2.p, nullptr, t->ctr.p + C_NNEW, u));
+  *u_out = u;
+  return B12G_OK;
 }
 
 }  // namespace
@@ -411,15 +513,34 @@ b12g_status b12g_continuation_run(b12g_tree* t, const b12g_scheme* sc, const dou
   uint32_t nb0 = 0, nb1 = t->depth == depth ? t->n : 0;
   uint32_t k = 0;
   PresenceTable keep;
+  // a tree of one depth (every leaf carries INS after the insertion): the sweeps take
+  // their sources from the boxes the sweep before inserted
+  const bool fast = nb1 > 0 && !t->mixed && depth <= kHashMaxDepth && t->domain.dim >= 2;
+  uint32_t n_src = 0;
+  if (fast) {
+    ST(centres_of(t, t->codes(), nullptr, t->dn(), t->n));
+    n_src = t->n;
+  }
   while (nb1 > nb0 && k < max_sweeps) {
-    ST(flag_call(t, 2, B12G_INS, B12G_EXPD, depth, nullptr));              // changeFlags('all', INS, EXPD, d)
-    ST(insert_by_image_impl(t, &s, depth, B12G_INS, B12G_NONE, nullptr, &keep));   // insert(scheme, d, INS, NONE)
-    ST(flag_call(t, 1, 0, B12G_EXPD, B12G_LEAF_DEPTH, nullptr));           // unsetFlags('all', EXPD)
+    if (fast) {
+      uint32_t u = 0;
+      ST(continuation_sweep(t, &s, depth, &keep, n_src, &u));
+      // nothing new: the sources lose INS (and EXPD) as the flag passes would have it
+      if (u == 0) ST(flag_call(t, 1, 0, uint8_t(B12G_INS | B12G_EXPD), B12G_LEAF_DEPTH, nullptr));
+      n_src = u;
+    } else {
+      ST(flag_call(t, 2, B12G_INS, B12G_EXPD, depth, nullptr));              // changeFlags('all', INS, EXPD, d)
+      ST(insert_by_image_impl(t, &s, depth, B12G_INS, B12G_NONE, nullptr, &keep));   // insert(scheme, d, INS, NONE)
+      ST(flag_call(t, 1, 0, B12G_EXPD, B12G_LEAF_DEPTH, nullptr));           // unsetFlags('all', EXPD)
+    }
     nb0 = nb1;
     nb1 = t->n;
     if (counts) counts[k] = nb1;
     ++k;
   }
+  // the last sweep's sort and merge ran without a read-back
+  ST(read_ctr(t, C_ERROR, C_DEFER - C_ERROR + 1));
+  ST(deferred_errors(t));
   if (n_sweeps) *n_sweeps = k;
   return B12G_OK;
 }

@@ -44,6 +44,8 @@ struct ImageArgs {
   uint64_t* cand;            // insert candidates: packed keys (pack_bits) of depth-d boxes
   uint32_t* cand_count;
   uint32_t cand_cap;
+  int claim;                 // Insert mode: claim each new box in `hash` (a kept table,
+                             // log2_use set), so every candidate is a distinct new box
   uint32_t* error;           // bit 0: capacity overflow
   unsigned long long* work;  // the image kernel's work-queue counter (launch_image zeroes it)
 };
@@ -92,13 +94,10 @@ int device_sm_count();
 // insert the n leaves of one depth (dim 2..4, depth <= kHashMaxDepth) into the lookup
 // table with tag h.tag, keyed by their packed per-dimension indices (pack_bits), which
 // also go to h.pk[i]; table slots = 2^h.log2_cap must be >= the slots hash_log2(n) asks
-// for (error bit 0 otherwise)
+// for, or 2^h.log2_use when set (error bit 0 otherwise)
 cudaError_t build_leaf_hash(const uint64_t* codes, const uint32_t* n, int depth, int dim, LeafHash h, uint32_t* error,
                             uint32_t max_n, cudaStream_t s);
-// the *n codes (depth `depth`) into a table built with log2 size l, marked present only
-// (their value is kAbsentIndex): lookups that need no leaf index, after a merge
-cudaError_t add_to_leaf_hash(const uint64_t* codes, const uint32_t* n, int l, int depth, int dim, LeafHash h,
-                             uint32_t* error, uint32_t max_n, cudaStream_t s);
+
 // flags |= f on hit leaves (hit cleared); *changed += leaves that lacked f
 cudaError_t apply_hits(uint8_t* flags, uint8_t* hit, const uint32_t* n, uint8_t f, uint32_t* changed,
                        uint32_t max_n, cudaStream_t s);

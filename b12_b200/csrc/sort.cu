@@ -323,37 +323,134 @@ __global__ void head_scatter_kernel(const uint64_t* keys, const uint32_t* n_ptr,
   if (blockIdx.x == 0 && threadIdx.x == 0) *n_out = pos[n];
 }
 
-// merge of two sorted, disjoint code arrays by rank: a[i] goes to i + |{b < a[i]}|,
-// b[j] to j + |{a < b[j]}|; the new entries (b) get flags `fb`
-__device__ __forceinline__ uint32_t lower_bound_u64(const uint64_t* v, uint32_t n, uint64_t x)
+// Merge of two sorted code arrays (merge path: Odeh, Green, Mwassi, Shmueli, Birk,
+// "Merge Path - Parallel Merging Made Simple", 2012).  The output is cut into tiles of
+// kMergeTile positions; two warps of the tile's block find its first and last a-element
+// by a 33-way co-rank search on the global arrays (a few rounds of loads, the range being
+// at most the shorter array), the tile's a- and b-runs are staged in shared memory, every
+// thread merges kMergeItems consecutive outputs after a co-rank search in shared memory
+// and stores them with vector stores.  Equal keys take a first.  a's flags
+// are ANDed with `a_keep`; b's entries get flags `fb`.
+constexpr int kMergeThreads = 256;
+constexpr int kMergeItems = 8;
+constexpr uint32_t kMergeTile = kMergeThreads * kMergeItems;
+
+// the number of a-elements among the first d outputs (one thread)
+__device__ __forceinline__ uint32_t co_rank(const uint64_t* a, uint32_t na, const uint64_t* b, uint32_t nb, uint32_t d)
 {
-  uint32_t lo = 0, len = n;
-  while (len > 0) {
-    const uint32_t half = len >> 1;
-    if (v[lo + half] < x) { lo += half + 1; len -= half + 1; }
-    else len = half;
+  uint32_t lo = d > nb ? d - nb : 0, hi = d < na ? d : na;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (a[mid] <= b[d - 1 - mid]) lo = mid + 1;
+    else hi = mid;
   }
   return lo;
 }
 
-__global__ void merge_kernel(const uint64_t* a, const uint8_t* fa, const uint32_t* na_ptr, const uint64_t* b,
-                             uint8_t fb, const uint32_t* nb_ptr, uint64_t* out, uint8_t* fout, uint32_t* n_out)
+// the same by a whole warp: each round tests 32 evenly spaced candidates of the range
+// (the predicate a[i] <= b[d-1-i] holds for a prefix of it) and keeps the gap where it
+// turns false
+__device__ __forceinline__ uint32_t co_rank_warp(const uint64_t* a, uint32_t na, const uint64_t* b, uint32_t nb,
+                                                 uint32_t d, int lane)
 {
-  const uint32_t na = *na_ptr, nb = *nb_ptr;
-  const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < na + nb; i += stride) {
-    if (i < na) {
-      const uint32_t p = i + lower_bound_u64(b, nb, a[i]);
-      out[p] = a[i];
-      fout[p] = fa[i];
-    } else {
-      const uint32_t j = i - na;
-      const uint32_t p = j + lower_bound_u64(a, na, b[j]);
-      out[p] = b[j];
-      fout[p] = fb;
-    }
+  uint32_t lo = d > nb ? d - nb : 0, hi = d < na ? d : na;
+  while (hi - lo > 32) {
+    const uint64_t span = hi - lo;
+    const uint32_t m = lo + uint32_t(span * uint64_t(lane + 1) / 33ull);     // lo <= m < hi, increasing
+    const bool p = __ldg(a + m) <= __ldg(b + (d - 1 - m));
+    const int c = __popc(__ballot_sync(0xFFFFFFFFu, p));
+    const uint32_t m_lo = __shfl_sync(0xFFFFFFFFu, m, c > 0 ? c - 1 : 0);
+    const uint32_t m_hi = __shfl_sync(0xFFFFFFFFu, m, c < 32 ? c : 31);
+    if (c > 0) lo = m_lo + 1;
+    if (c < 32) hi = m_hi;
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) *n_out = na + nb;
+  const uint32_t m = lo + uint32_t(lane);
+  const bool p = m < hi && __ldg(a + m) <= __ldg(b + (d - 1 - m));
+  return lo + uint32_t(__popc(__ballot_sync(0xFFFFFFFFu, p)));
+}
+
+__global__ void __launch_bounds__(kMergeThreads) merge_path_kernel(const uint64_t* __restrict__ a,
+                                                                   const uint8_t* __restrict__ fa,
+                                                                   const uint32_t* na_ptr, uint8_t a_keep,
+                                                                   const uint64_t* __restrict__ b, uint8_t fb,
+                                                                   const uint32_t* nb_ptr,
+                                                                   uint64_t* __restrict__ out,
+                                                                   uint8_t* __restrict__ fout, uint32_t* n_out)
+{
+  __shared__ uint64_t s_in[kMergeTile];     // the tile's a-run, then its b-run
+  __shared__ uint8_t s_fa[kMergeTile];
+  __shared__ uint32_t s_split[2];
+  const uint32_t na = *na_ptr, nb = *nb_ptr, total = na + nb;
+  const uint32_t tiles = (total + kMergeTile - 1) / kMergeTile;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+    const uint32_t d0 = t * kMergeTile, d1 = min(d0 + kMergeTile, total);
+    if (w < 2) {
+      const uint32_t r = co_rank_warp(a, na, b, nb, w == 0 ? d0 : d1, lane);
+      if (lane == 0) s_split[w] = r;
+    }
+    __syncthreads();
+    const uint32_t i0 = s_split[0], i1 = s_split[1];
+    const uint32_t j0 = d0 - i0, j1 = d1 - i1;
+    const uint32_t la = i1 - i0, lb = j1 - j0;
+    const uint32_t len = la + lb;
+    // all loads of the tile first (kMergeItems per thread), then the shared-memory stores
+    uint64_t v[kMergeItems];
+    uint8_t f[kMergeItems];
+#pragma unroll
+    for (int q = 0; q < kMergeItems; ++q) {
+      const uint32_t k = threadIdx.x + uint32_t(q) * kMergeThreads;
+      v[q] = 0;
+      f[q] = 0;
+      if (k < la) {
+        v[q] = __ldg(a + i0 + k);
+        f[q] = __ldg(fa + i0 + k);
+      } else if (k < len) {
+        v[q] = __ldg(b + j0 + (k - la));
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kMergeItems; ++q) {
+      const uint32_t k = threadIdx.x + uint32_t(q) * kMergeThreads;
+      if (k < len) s_in[k] = v[q];
+      if (k < la) s_fa[k] = f[q] & a_keep;
+    }
+    __syncthreads();
+    const uint32_t dl = min(threadIdx.x * uint32_t(kMergeItems), len);
+    uint32_t ia = co_rank(s_in, la, s_in + la, lb, dl);
+    uint32_t ib = dl - ia;
+    uint64_t o[kMergeItems];
+    uint8_t of[kMergeItems];
+#pragma unroll
+    for (int q = 0; q < kMergeItems; ++q) {
+      const bool take_a = ib >= lb || (ia < la && s_in[ia] <= s_in[la + ib]);
+      o[q] = take_a ? s_in[ia < la ? ia : 0] : s_in[la + ib];
+      of[q] = take_a ? s_fa[ia < la ? ia : 0] : fb;
+      if (take_a) ++ia;
+      else ++ib;
+    }
+    // a thread's outputs are consecutive: 16-byte stores of its codes, one 8-byte store of
+    // its flags (tile starts are multiples of kMergeTile, so both are aligned)
+    if (dl + kMergeItems <= len) {
+      uint4* op = reinterpret_cast<uint4*>(out + d0 + dl);
+#pragma unroll
+      for (int q = 0; q < kMergeItems; q += 2)
+        op[q / 2] = make_uint4(uint32_t(o[q]), uint32_t(o[q] >> 32), uint32_t(o[q + 1]), uint32_t(o[q + 1] >> 32));
+      uint64_t fw = 0;
+#pragma unroll
+      for (int q = 0; q < kMergeItems; ++q) fw |= uint64_t(of[q]) << (8 * q);
+      *reinterpret_cast<uint64_t*>(fout + d0 + dl) = fw;
+    } else {
+#pragma unroll
+      for (int q = 0; q < kMergeItems; ++q)
+        if (dl + q < len) {
+          out[d0 + dl + q] = o[q];
+          fout[d0 + dl + q] = of[q];
+        }
+    }
+    __syncthreads();
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *n_out = total;
 }
 
 }  // namespace
@@ -369,11 +466,14 @@ cudaError_t unique_sorted_u64(const uint64_t* keys, const uint32_t* n, uint32_t 
   return cudaGetLastError();
 }
 
-cudaError_t merge_sorted(const uint64_t* a, const uint8_t* fa, const uint32_t* na, const uint64_t* b, uint8_t fb,
-                         const uint32_t* nb, uint32_t max_total, uint64_t* out, uint8_t* fout, uint32_t* n_out,
-                         cudaStream_t s)
+cudaError_t merge_sorted(const uint64_t* a, const uint8_t* fa, const uint32_t* na, uint8_t a_keep, const uint64_t* b,
+                         uint8_t fb, const uint32_t* nb, uint32_t max_total, uint64_t* out, uint8_t* fout,
+                         uint32_t* n_out, cudaStream_t s)
 {
-  merge_kernel<<<grid_for(max_total, kThreads, 8), kThreads, 0, s>>>(a, fa, na, b, fb, nb, out, fout, n_out);
+  const uint64_t tiles = (uint64_t(max_total) + kMergeTile - 1) / kMergeTile;
+  const uint64_t cap = uint64_t(device_sm_count()) * 5;   // resident blocks a SM (48 registers)
+  const unsigned grid = unsigned(tiles < 1 ? 1 : (tiles < cap ? tiles : cap));
+  merge_path_kernel<<<grid, kMergeThreads, 0, s>>>(a, fa, na, a_keep, b, fb, nb, out, fout, n_out);
   return cudaGetLastError();
 }
 

@@ -29,9 +29,10 @@ cudaError_t radix_sort_u64_values(uint64_t* keys, uint64_t* alt, uint32_t* vals,
 cudaError_t unique_sorted_u64(const uint64_t* keys, const uint32_t* n, uint32_t max_n, uint64_t* out, uint32_t* n_out,
                               uint32_t* flag, uint32_t* pos, uint32_t* scan_tiles, cudaStream_t s);
 
-// merge two sorted arrays with no common value; entries of b get flags fb
-cudaError_t merge_sorted(const uint64_t* a, const uint8_t* fa, const uint32_t* na, const uint64_t* b, uint8_t fb,
-                         const uint32_t* nb, uint32_t max_total, uint64_t* out, uint8_t* fout, uint32_t* n_out,
-                         cudaStream_t s);
+// merge two sorted arrays (equal values: a first); a's flags are ANDed with a_keep,
+// entries of b get flags fb
+cudaError_t merge_sorted(const uint64_t* a, const uint8_t* fa, const uint32_t* na, uint8_t a_keep, const uint64_t* b,
+                         uint8_t fb, const uint32_t* nb, uint32_t max_total, uint64_t* out, uint8_t* fout,
+                         uint32_t* n_out, cudaStream_t s);
 
 }  // namespace b12g

@@ -103,7 +103,8 @@ enum : int {
   C_NNEW = 12,
   C_TGT = 13,      // the stored image targets overflowed their buffer
   C_WORK = 14,     // 2 words (8-byte aligned): the image kernel's work-queue counter
-  C_COUNT = 16
+  C_DEFER = 16,    // error bits of launches whose status is read with a later read-back
+  C_COUNT = 18
 };
 
 }  // namespace host

@@ -130,9 +130,10 @@ __global__ void split_kernel(const uint64_t* code, const uint8_t* flags, const u
 }
 
 // ---------------------------------------------------------------------------------
-// leaf lookup table: linear-probing inserts with a 64-bit CAS on the key word; a CAS
-// that loses to another insert re-reads the same slot (which now carries the current
-// tag) and moves on, so every insert ends within the table size
+// leaf lookup table: linear-probing inserts with a 64-bit CAS on the key word (guessing
+// an empty slot is zero, else retrying with the old-tag value the CAS returned); a CAS
+// that loses to another insert sees the current tag and moves on, so every insert ends
+// within the table size
 // ---------------------------------------------------------------------------------
 // The keys are the leaves' packed per-dimension indices (pack_bits at `depth`), also
 // written to h.pk for the image kernels.
@@ -141,7 +142,7 @@ __global__ void hash_build_kernel(const uint64_t* codes, const uint32_t* n_ptr, 
                                   uint32_t* error)
 {
   const uint32_t n = *n_ptr;
-  const int l = hash_log2(n);
+  const int l = table_log2(h, n);
   if (l > int(h.log2_cap)) {
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(error, 1u);
     return;
@@ -157,50 +158,19 @@ __global__ void hash_build_kernel(const uint64_t* codes, const uint32_t* n_ptr, 
     const unsigned long long key = (uint64_t(h.tag) << 56) | pk;
     uint64_t s = hash_slot(pk, l);
     bool done = false;
+    unsigned long long expect = 0;   // first guess for a slot: never used
     for (uint64_t step = 0; step <= 2 * mask + 64 && !done; ++step) {
       unsigned long long* kw = reinterpret_cast<unsigned long long*>(&h.slots[s].x);
-      const unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(kw);
-      if ((cur >> 56) != h.tag) {
-        if (atomicCAS(kw, cur, key) == cur) {
-          h.slots[s].y = i;
-          done = true;
-        }
-        continue;  // lost the slot to another insert: look at it again
+      const unsigned long long cur = atomicCAS(kw, expect, key);
+      if (cur == expect) {           // an empty slot (tag 0 or an old tag) now holds the key
+        h.slots[s].y = i;
+        done = true;
+      } else if ((cur >> 56) != h.tag) {
+        expect = cur;                // empty under an old tag: try it again with its value
+      } else {
+        s = (s + 1) & mask;
+        expect = 0;
       }
-      s = (s + 1) & mask;
-    }
-    if (!done) atomicOr(error, 1u);
-  }
-}
-
-// New boxes into an existing table of log2 size l (the size the leaf count it was built
-// for asks for, which must still be the size hash_log2 gives for the grown count): only
-// their presence is recorded (value kAbsentIndex), for lookups that need no leaf index.
-template<int D>
-__global__ void hash_add_kernel(const uint64_t* codes, const uint32_t* n_ptr, int l, int depth, LeafHash h,
-                                uint32_t* error)
-{
-  const uint32_t n = *n_ptr;
-  const uint64_t mask = (1ull << l) - 1ull;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    uint32_t bits[D];
-#pragma unroll
-    for (int j = 0; j < D; ++j) bits[j] = deinterleave<D>(codes[i], depth, j);
-    const uint64_t pk = pack_bits<D>(bits, depth);
-    const unsigned long long key = (uint64_t(h.tag) << 56) | pk;
-    uint64_t s = hash_slot(pk, l);
-    bool done = false;
-    for (uint64_t step = 0; step <= 2 * mask + 64 && !done; ++step) {
-      unsigned long long* kw = reinterpret_cast<unsigned long long*>(&h.slots[s].x);
-      const unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(kw);
-      if ((cur >> 56) != h.tag) {
-        if (atomicCAS(kw, cur, key) == cur) {
-          h.slots[s].y = kAbsentIndex;
-          done = true;
-        }
-        continue;
-      }
-      s = (s + 1) & mask;
     }
     if (!done) atomicOr(error, 1u);
   }
@@ -488,18 +458,6 @@ cudaError_t build_leaf_hash(const uint64_t* codes, const uint32_t* n, int depth,
   return cudaGetLastError();
 }
 
-cudaError_t add_to_leaf_hash(const uint64_t* codes, const uint32_t* n, int l, int depth, int dim, LeafHash h,
-                             uint32_t* error, uint32_t max_n, cudaStream_t s)
-{
-  const int g = grid_for(max_n, kThreads, 8);
-  switch (dim) {
-    case 2: hash_add_kernel<2><<<g, kThreads, 0, s>>>(codes, n, l, depth, h, error); break;
-    case 3: hash_add_kernel<3><<<g, kThreads, 0, s>>>(codes, n, l, depth, h, error); break;
-    case 4: hash_add_kernel<4><<<g, kThreads, 0, s>>>(codes, n, l, depth, h, error); break;
-    default: return cudaErrorInvalidValue;
-  }
-  return cudaGetLastError();
-}
 
 cudaError_t compact(const CompactArgs& args, const CompactScratch& sc, uint32_t max_in, cudaStream_t s)
 {
