@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(kThreads, 6) image_points_kernel(const ImageAr
     uint32_t tbits[Map::D];
     bool valid = false;
     if (active) {
-      if constexpr (M == ImageMode::Insert) {   // Insert launches carry their source centres
+      if constexpr (M == ImageMode::Insert || M == ImageMode::Mark) {   // these carry their source centres
         double c[Map::D];
         PI::source_centre(a, rank, c);
         valid = PI::image_at(a, pts, table, c, g, uint32_t(k), tbits);
@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(kThreads, 6) image_points_kernel(const ImageAr
         PI::source_bits(a, leaf, sbits);
         valid = PI::image(a, pts, table, sbits, g, uint32_t(k), tbits);
       }
-      t = PI::target(a, n, valid, tbits);
+      if constexpr (M != ImageMode::Mark) t = PI::target(a, n, valid, tbits);
     }
     if constexpr (M == ImageMode::Hit) {
       // one store per distinct target in the warp
@@ -168,6 +168,28 @@ __global__ void __launch_bounds__(kThreads, 6) image_points_kernel(const ImageAr
       }
     } else if constexpr (M == ImageMode::Search) {
       if (active) a.out[g] = t;
+    } else if constexpr (M == ImageMode::Mark) {
+      // the image's box, unless its bit is set already (a stale read only sends the point
+      // on to the atomic), deduplicated within the warp; the lane whose atomic sets the bit
+      // marks the box in `fresh`, and the warp counts its new boxes with one atomic
+      uint64_t code = kInvalidCode;
+      bool fresh = false;
+      if (active && valid) {
+        int k[Map::D];
+#pragma unroll
+        for (int j = 0; j < Map::D; ++j) k[j] = a.dc.k[j];
+        code = interleave<Map::D>(tbits, k, a.depth);
+        fresh = !((a.bits[code >> 5] >> uint32_t(code & 31u)) & 1u);
+      }
+      const unsigned peers = __match_any_sync(0xFFFFFFFFu, fresh ? code : kInvalidCode) & __ballot_sync(0xFFFFFFFFu, fresh);
+      bool leader = fresh && lane == __ffs(peers) - 1;
+      if (leader) {
+        const uint32_t m = 1u << uint32_t(code & 31u);
+        leader = !(atomicOr(a.bits + (code >> 5), m) & m);
+        if (leader) atomicOr(a.fresh + (code >> 5), m);
+      }
+      const unsigned lead_mask = __ballot_sync(0xFFFFFFFFu, leader);
+      if (lane == 0 && lead_mask) atomicAdd(a.cand_count, uint32_t(__popc(lead_mask)));
     } else {
       // candidates: valid images that are not leaves, as packed keys (the caller turns them
       // into codes); deduplicated within the warp and appended with one atomic per warp
@@ -276,7 +298,7 @@ __global__ void __launch_bounds__(kThreads) transition_rows_kernel(const RowArgs
 template<class Map, class Grid>
 cudaError_t launch_image_t(ImageMode mode, const ImageArgs& a, uint64_t max_points, cudaStream_t s)
 {
-  static int blocks_per_sm[3] = {0, 0, 0};
+  static int blocks_per_sm[4] = {0, 0, 0, 0};
   const int m = int(mode);
   if (!blocks_per_sm[m]) {
     int b = 0;
@@ -284,8 +306,10 @@ cudaError_t launch_image_t(ImageMode mode, const ImageArgs& a, uint64_t max_poin
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, image_points_kernel<Map, Grid, ImageMode::Hit>, kThreads, 0);
     else if (mode == ImageMode::Search)
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, image_points_kernel<Map, Grid, ImageMode::Search>, kThreads, 0);
-    else
+    else if (mode == ImageMode::Insert)
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, image_points_kernel<Map, Grid, ImageMode::Insert>, kThreads, 0);
+    else
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, image_points_kernel<Map, Grid, ImageMode::Mark>, kThreads, 0);
     blocks_per_sm[m] = b > 0 ? b : 1;
   }
   const uint64_t want = (max_points + kThreads - 1) / kThreads;
@@ -293,7 +317,8 @@ cudaError_t launch_image_t(ImageMode mode, const ImageArgs& a, uint64_t max_poin
   const unsigned grid = unsigned(want < 1 ? 1 : (want < cap ? want : cap));
   if (mode == ImageMode::Hit) image_points_kernel<Map, Grid, ImageMode::Hit><<<grid, kThreads, 0, s>>>(a);
   else if (mode == ImageMode::Search) image_points_kernel<Map, Grid, ImageMode::Search><<<grid, kThreads, 0, s>>>(a);
-  else image_points_kernel<Map, Grid, ImageMode::Insert><<<grid, kThreads, 0, s>>>(a);
+  else if (mode == ImageMode::Insert) image_points_kernel<Map, Grid, ImageMode::Insert><<<grid, kThreads, 0, s>>>(a);
+  else image_points_kernel<Map, Grid, ImageMode::Mark><<<grid, kThreads, 0, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -484,6 +484,222 @@ b12g_status continuation_sweep(b12g_tree* t, const b12g_scheme* sc, uint8_t dept
   return B12G_OK;
 }
 
+// ---------------------------------------------------------------------------------
+// Continuation over a bitmap of every box of the depth (depth <= kBitmapMaxDepth: at most
+// 2^30 bits, 128 MB; 2 MB at depth 24, resident in L2): bit c is set when the box of
+// code c is a leaf.  A sweep is one image launch in Mark mode over the boxes the sweep
+// before added: an image box whose bit it sets first is new and is marked in a second
+// bitmap too, whose set bits, read in code order, are the next sweep's sources (in leaf
+// order, as the reference iterates them, which fixes each point's index in the grid).
+// Nothing is sorted or merged while the sweeps run; the sorted leaves are the set bits
+// in code order, written once at the end.
+// ---------------------------------------------------------------------------------
+constexpr int kBitmapMaxDepth = 30;
+
+__global__ void set_bits_kernel(const uint64_t* __restrict__ codes, const uint32_t* n_ptr, uint32_t* bits)
+{
+  const uint32_t n = *n_ptr;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint64_t c = codes[i];
+    atomicOr(bits + (c >> 5), 1u << uint32_t(c & 31u));
+  }
+}
+
+// Bitmap compaction: a count of set bits per tile of kWordTile words; the tiles' first
+// positions (each tile sums the counts before it when there are at most kLocalTiles
+// tiles, else a scan of the counts); then every tile scans its words and writes the
+// codes of its set bits in order, with flags when asked (f where a second bitmap has the
+// bit, else 0), clearing its words when asked.
+constexpr uint32_t kWordTile = 1024;
+constexpr int kWordsPerThread = kWordTile / kThreads;   // 4
+constexpr uint32_t kLocalTiles = 4096;
+
+__device__ __forceinline__ uint32_t block_sum_u32(uint32_t v, uint32_t* red)
+{
+  for (int d = 16; d > 0; d >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, d);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  uint32_t t = 0;
+  for (int w = 0; w < kThreads / 32; ++w) t += red[w];
+  __syncthreads();
+  return t;
+}
+
+__global__ void __launch_bounds__(kThreads) tile_count_kernel(const uint32_t* __restrict__ bits, uint32_t words,
+                                                              uint32_t* __restrict__ tile_count)
+{
+  __shared__ uint32_t red[kThreads / 32];
+  const uint32_t tiles = (words + kWordTile - 1) / kWordTile;
+  for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+    uint32_t c = 0;
+    for (uint32_t w = t * kWordTile + threadIdx.x; w < min(words, (t + 1) * kWordTile); w += kThreads)
+      c += __popc(bits[w]);
+    c = block_sum_u32(c, red);
+    if (threadIdx.x == 0) tile_count[t] = c;
+  }
+}
+
+// tile_first: the tiles' first positions (a scan of the counts), or nullptr: summed here
+__global__ void __launch_bounds__(kThreads) tile_scatter_kernel(uint32_t* __restrict__ bits, uint32_t words,
+                                                                const uint32_t* __restrict__ tile_count,
+                                                                const uint32_t* __restrict__ tile_first,
+                                                                uint64_t* __restrict__ out, int clear,
+                                                                const uint32_t* __restrict__ mark,
+                                                                uint8_t* __restrict__ flags, uint8_t f)
+{
+  __shared__ uint32_t red[kThreads / 32];
+  __shared__ uint32_t wsum[kThreads / 32];
+  const uint32_t tiles = (words + kWordTile - 1) / kWordTile;
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+  for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+    uint32_t before = 0;
+    if (tile_first) {
+      before = tile_first[t];
+    } else {
+      for (uint32_t q = threadIdx.x; q < t; q += kThreads) before += tile_count[q];
+      before = block_sum_u32(before, red);
+    }
+    // thread i holds words t*kWordTile + 4i .. 4i+3
+    const uint32_t w0 = t * kWordTile + threadIdx.x * kWordsPerThread;
+    uint32_t v[kWordsPerThread];
+    uint32_t c = 0;
+#pragma unroll
+    for (int q = 0; q < kWordsPerThread; ++q) {
+      v[q] = w0 + q < words ? bits[w0 + q] : 0u;
+      c += __popc(v[q]);
+    }
+    uint32_t x = c;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d);
+      if (lane >= d) x += y;
+    }
+    if (lane == 31) wsum[wp] = x;
+    __syncthreads();
+    uint32_t p = before + x - c;
+    for (int q = 0; q < wp; ++q) p += wsum[q];
+#pragma unroll
+    for (int q = 0; q < kWordsPerThread; ++q) {
+      uint32_t b = v[q];
+      const uint32_t mk = (mark && b) ? mark[w0 + q] : 0u;
+      while (b) {
+        const int bit = __ffs(b) - 1;
+        out[p] = (uint64_t(w0 + q) << 5) | uint64_t(bit);
+        if (flags) flags[p] = ((mk >> bit) & 1u) ? f : uint8_t(0);
+        ++p;
+        b &= b - 1u;
+      }
+      if (clear && v[q]) bits[w0 + q] = 0u;
+    }
+    __syncthreads();
+  }
+}
+
+// the codes of the set bits of `bits` (words u32) in increasing order into `out`, and
+// flags into `flags` when not null (f where `mark` has the bit); clears the bitmap when
+// asked
+b12g_status bitmap_codes(b12g_tree* t, uint32_t* bits, uint32_t words, uint64_t* out, bool clear,
+                         const uint32_t* mark = nullptr, uint8_t* flags = nullptr, uint8_t f = 0)
+{
+  const uint32_t tiles = (words + kWordTile - 1) / kWordTile;
+  ST(t->sort_idx.ensure(2 * (size_t(tiles) + 1) + compact_tiles(uint64_t(tiles) + 1) + 8, "bitmap tile counts"));
+  uint32_t* count = t->sort_idx.p;
+  uint32_t* first = nullptr;
+  const int g = int(std::min<uint64_t>(tiles, uint64_t(device_sm_count()) * 8));
+  tile_count_kernel<<<g, kThreads, 0, t->stream>>>(bits, words, count);
+  CK(cudaGetLastError());
+  count_launches(1);
+  if (tiles > kLocalTiles) {
+    first = count + tiles + 1;
+    ST(set_ctr(t, C_TMP, tiles));
+    CK(exclusive_scan_u32(count, first, t->ctr.p + C_TMP, first + tiles + 1, tiles, t->stream));
+    count_launches(3);
+  }
+  tile_scatter_kernel<<<g, kThreads, 0, t->stream>>>(bits, words, count, first, out, clear ? 1 : 0, mark, flags, f);
+  CK(cudaGetLastError());
+  count_launches(1);
+  return B12G_OK;
+}
+
+// the sweeps of continuation.m:29-44 on a tree of one depth whose leaves all carry INS
+// (the boxes of the start points); leaves the tree as the flag passes would: every
+// leaf's flags 0, except INS on the last sweep's new boxes when max_sweeps ended the run
+b12g_status continuation_bitmap(b12g_tree* t, const b12g_scheme* s, uint8_t depth, uint32_t max_sweeps,
+                                uint32_t* counts, uint32_t* n_sweeps)
+{
+  const uint64_t boxes = uint64_t(1) << depth;
+  const uint32_t words = uint32_t(std::max<uint64_t>(boxes >> 5, 1));
+  ST(t->bits.ensure(2 * size_t(words), "box bitmaps"));
+  uint32_t* bits = t->bits.p;            // every leaf
+  uint32_t* fresh = t->bits.p + words;   // the boxes the running sweep adds
+  CK(cudaMemsetAsync(t->bits.p, 0, 2 * size_t(words) * 4, t->stream));
+  set_bits_kernel<<<grid_over(t->n), kThreads, 0, t->stream>>>(t->codes(), t->dn(), bits);
+  CK(cudaGetLastError());
+  count_launches(1);
+  ST(centres_of(t, t->codes(), nullptr, t->dn(), t->n));   // the first sources: every leaf
+  Prepared pr;
+  ST(prepare(t, s, pr));
+  pr.a.src = nullptr;
+  pr.a.n_src = t->ctr.p + C_NSRC;
+  pr.a.bits = bits;
+  pr.a.fresh = fresh;
+  pr.a.cand_count = t->ctr.p + C_CAND;
+  uint64_t n = t->n;
+  uint32_t n_src = t->n, u = 0, k = 0, nb0 = 0, nb1 = t->n;
+  while (nb1 > nb0 && k < max_sweeps) {
+    const uint64_t points = uint64_t(n_src) * pr.P;
+    ST(set_ctr(t, C_CAND, 0));
+    ST(set_ctr(t, C_NSRC, n_src));
+    pr.a.src_c = t->srcc.p;
+    u = 0;
+    if (points > 0) {
+      prof_mark(t, 0);
+      CK(launch_image(s->map.kind, s->map.arith, s->grid.kind, t->domain.dim, ImageMode::Mark, pr.a, points,
+                      t->stream));
+      prof_mark(t, 0);
+      count_launches(1);
+      ST(read_ctr(t, C_ERROR, C_DEFER - C_ERROR + 1));
+      ST(prof_collect(t));
+      if (t->h_ctr[C_ERROR]) {
+        set_ctr(t, C_ERROR, 0);
+        return fail(B12G_ERR_CAPACITY, "continuation: device error bits %u", t->h_ctr[C_ERROR]);
+      }
+      u = t->h_ctr[C_CAND];
+      if (u > 0) {
+        // the next sources: the new boxes in code order, their codes and centres
+        ST(t->cand.ensure_room(u, "new boxes", 2));
+        ST(bitmap_codes(t, fresh, words, t->cand.p, true));
+        ST(centres_of(t, t->cand.p, nullptr, t->ctr.p + C_CAND, u));
+      }
+    }
+    n += u;
+    n_src = u;
+    nb0 = nb1;
+    nb1 = uint32_t(n);
+    if (counts) counts[k] = nb1;
+    ++k;
+  }
+  *n_sweeps = k;
+  if (k == 0) return B12G_OK;
+  // the leaves: the set bits in code order; flags 0, INS on the last sweep's new boxes
+  // when max_sweeps ended the run while boxes were still being added
+  ST(reserve(t, n));
+  const int o = 1 - t->cur, no = 1 - t->ncur;
+  if (u > 0) {
+    set_bits_kernel<<<grid_over(u), kThreads, 0, t->stream>>>(t->cand.p, t->ctr.p + C_CAND, fresh);
+    CK(cudaGetLastError());
+    count_launches(1);
+  }
+  ST(bitmap_codes(t, bits, words, t->code[o].p, false, u > 0 ? fresh : nullptr, t->flags[o].p, B12G_INS));
+  ST(set_ctr(t, no, uint32_t(n)));
+  ST(sync(t, "continuation leaves"));
+  t->cur = o;
+  t->ncur = no;
+  t->n = uint32_t(n);
+  ++t->leaf_gen;
+  return B12G_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -512,6 +728,11 @@ b12g_status b12g_continuation_run(b12g_tree* t, const b12g_scheme* sc, const dou
   s.flags_to_check = B12G_EXPD;                                             // {grid, map, d, EXPD}
   uint32_t nb0 = 0, nb1 = t->depth == depth ? t->n : 0;
   uint32_t k = 0;
+  if (nb1 > 0 && !t->mixed && depth <= kBitmapMaxDepth && t->domain.dim >= 2) {
+    ST(continuation_bitmap(t, &s, depth, max_sweeps, counts, &k));
+    if (n_sweeps) *n_sweeps = k;
+    return B12G_OK;
+  }
   PresenceTable keep;
   // a tree of one depth (every leaf carries INS after the insertion): the sweeps take
   // their sources from the boxes the sweep before inserted

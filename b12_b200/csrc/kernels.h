@@ -13,6 +13,8 @@ enum class ImageMode : int {
   Hit = 0,     // hit[leaf] = 1                       (setFlagsByIterators)
   Search = 1,  // out[point] = leaf index or invalid  (searchByIterators)
   Insert = 2,  // not found -> candidate code         (insertByIterators)
+  Mark = 3,    // the image's box marked in a bitmap of every box of the depth; the
+               // boxes this launch marks first also in `fresh`, and counted
 };
 
 // One box-image launch over a uniform-depth leaf set.
@@ -44,6 +46,8 @@ struct ImageArgs {
   uint64_t* cand;            // insert candidates: packed keys (pack_bits) of depth-d boxes
   uint32_t* cand_count;
   uint32_t cand_cap;
+  uint32_t* bits;            // Mark mode: bit c = the box of depth-d code c is a leaf
+  uint32_t* fresh;           // Mark mode: bit c = the box of code c was added by this launch
   int claim;                 // Insert mode: claim each new box in `hash` (a kept table,
                              // log2_use set), so every candidate is a distinct new box
   uint32_t* error;           // bit 0: capacity overflow

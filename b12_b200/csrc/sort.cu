@@ -33,7 +33,11 @@ constexpr uint64_t kAggregate = 1ull << 62;       // status word: tile count pub
 constexpr uint64_t kInclusive = 2ull << 62;       // status word: inclusive prefix published
 constexpr uint64_t kFlagMask = 3ull << 62;
 constexpr uint32_t kLookbackPolls = 1u << 20;     // polls of one predecessor before giving up
-constexpr int kLookbackBatch = 8;                 // predecessor status words loaded together
+// predecessor status words loaded together in the look-back: 8 when tiles run in
+// several waves (the registers allow two blocks a SM), 32 when every tile runs at once,
+// where a tile's walk back to tile 0 is the chain that bounds the pass
+constexpr int kBatchWaves = 8;
+constexpr int kBatchOneWave = 32;
 
 int grid_for(uint64_t work, int per_block, int blocks_per_sm)
 {
@@ -100,8 +104,8 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* w
 // key index of (warp w, round r, lane) within a tile: each warp owns 512 consecutive keys
 __device__ __forceinline__ uint32_t tile_index(int w, int r, int lane) { return uint32_t(w * 512 + r * 32 + lane); }
 
-template<bool kValues>
-__global__ void __launch_bounds__(kThreads) onesweep_pass_kernel(const uint64_t* __restrict__ keys,
+template<bool kValues, int kLookbackBatch>
+__global__ void __launch_bounds__(kThreads, kLookbackBatch == kBatchOneWave ? 1 : 2) onesweep_pass_kernel(const uint64_t* __restrict__ keys,
                                                                  const uint32_t* __restrict__ vals,
                                                                  const uint32_t* n_ptr, int pass, SortScratch sc,
                                                                  uint64_t* out, uint32_t* vout, uint32_t* error)
@@ -267,8 +271,12 @@ cudaError_t onesweep(uint64_t* keys, uint64_t* alt, uint32_t* vals, uint32_t* va
   uint32_t* vsrc = vals;
   uint32_t* vdst = valt;
   const unsigned grid = tiles < 1 ? 1u : tiles;
+  const bool one_wave = grid <= unsigned(device_sm_count());
   for (int p = 0; p < passes; ++p) {
-    onesweep_pass_kernel<kValues><<<grid, kThreads, 0, s>>>(src, vsrc, n, p, sc, dst, vdst, error);
+    if (one_wave)
+      onesweep_pass_kernel<kValues, kBatchOneWave><<<grid, kThreads, 0, s>>>(src, vsrc, n, p, sc, dst, vdst, error);
+    else
+      onesweep_pass_kernel<kValues, kBatchWaves><<<grid, kThreads, 0, s>>>(src, vsrc, n, p, sc, dst, vdst, error);
     std::swap(src, dst);
     if constexpr (kValues) std::swap(vsrc, vdst);
   }

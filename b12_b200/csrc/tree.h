@@ -128,6 +128,7 @@ struct b12g_tree {
   Buf<uint32_t> src, out, stage_col, stage_cnt, row_count, rowptr;
   Buf<uint64_t> cand, cand2;
   Buf<double> srcc;            // centres of an image launch's source boxes (kSrcStride a source)
+  Buf<uint32_t> bits;          // continuation: a bit for every box of the depth
   Buf<uint32_t> sort_idx;
   Buf<double> table;
   Buf<double> points;

@@ -59,6 +59,45 @@ def test_continuation_step_api_matches_reference_each_sweep(golden, name):
         assert sha(codes) == st["codes_sha256"] and sha(flags) == st["flags_sha256"], st["step"]
 
 
+@pytest.mark.parametrize("sweeps", [1, 7, 30])
+def test_continuation_cut_short_matches_reference_at_that_sweep(golden, sweeps):
+    """max_sweeps ends the run while boxes are still being added: the leaves and flags
+    (INS on the last sweep's new boxes) of that sweep of the reference's run."""
+    meta, _ = golden("coupled_duffing_cont_d24")
+    spec = meta["spec"]
+    t = make_tree(spec)
+    counts = t.continuation_run(scheme(spec), np.zeros(4), spec["depth"], max_sweeps=sweeps)
+    ref = [s for s in meta["steps"] if 0 < s["step"] <= sweeps]
+    assert list(counts) == [s["n"] for s in ref]
+    codes, _, flags = t.leaves()
+    assert sha(codes) == ref[-1]["codes_sha256"] and sha(flags) == ref[-1]["flags_sha256"]
+    assert (flags == B.INS).sum() == ref[-1]["n"] - (ref[-2]["n"] if len(ref) > 1 else 1)
+
+
+@pytest.mark.parametrize("depth", [31, 40])
+def test_continuation_deeper_than_the_bitmap_matches_oracle(depth):
+    """Depths above the box bitmap's (30) take the lookup-table sweeps."""
+    spec = dict(map="coupled_duffing", points=64, seed=0)
+    t = make_tree(spec)
+    counts = t.continuation_run(scheme(spec), np.zeros(4), depth, max_sweeps=6)
+    o, oc = O.continuation(oracle_spec(spec), depth, np.zeros(4), max_sweeps=6)
+    assert list(counts) == oc
+    for x, y in zip(t.leaves(), o.leaves()):
+        np.testing.assert_array_equal(x, y)
+
+
+def test_henon_continuation_matches_oracle():
+    """A two-dimensional continuation (the Henon map from its fixed point) to the end."""
+    spec = dict(map="henon", a=1.4, b=0.3, grid=4)
+    x0 = np.array([0.6313544770895048, 0.18940634312685142])
+    t = make_tree(spec)
+    counts = t.continuation_run(scheme(spec), x0, 16)
+    o, oc = O.continuation(oracle_spec(spec), 16, x0)
+    assert list(counts) == oc and len(oc) > 3
+    for x, y in zip(t.leaves(), o.leaves()):
+        np.testing.assert_array_equal(x, y)
+
+
 def test_continuation_depth16_matches_oracle():
     spec = dict(map="coupled_duffing", points=64, seed=0)
     t = make_tree(spec)
