@@ -102,6 +102,9 @@ struct DepthConst {
   int k[B12G_MAX_DIM];       // bisections of each dimension at the depth
   int kp[B12G_MAX_DIM];      // ... and at the depth above
   int jd;                    // the dimension the depth's last bisection splits
+  int ks[B12G_MAX_DIM];      // code assembly: dimension j's bits move up by ks[j] = K - k[j]
+  int cs;                    // ... and the spread code down by cs = D K - depth (K = ceil(depth / D))
+  int c32;                   // 1: D K <= 32 and K is within the 32-bit spreading's range
 };
 
 // the constants of a launch at `depth` for a domain of `dim` dimensions
@@ -115,6 +118,11 @@ inline void fill_depth_const(const Domain& dom, int dim, int depth, DepthConst& 
     dc.kp[j] = j < dim ? bis(depth - 1, j) : 0;
   }
   dc.jd = depth >= 1 ? (depth - 1) % dim : 0;
+  const int K = (depth + dim - 1) / dim;
+  for (int j = 0; j < B12G_MAX_DIM; ++j) dc.ks[j] = j < dim ? K - dc.k[j] : 0;
+  dc.cs = dim * K - depth;
+  const int kmax = dim == 2 ? 16 : dim == 3 ? 10 : dim == 4 ? 8 : 0;
+  dc.c32 = (depth > 0 && K <= kmax && dim * K <= 32) ? 1 : 0;
 }
 
 struct MapParams {
@@ -227,6 +235,42 @@ __device__ __forceinline__ uint32_t deinterleave(uint64_t code, int depth, int j
   return bits;
 }
 
+// the same spreading in 32 bits, for codes of at most 32 bits (D*K <= 32); the steps for
+// three dimensions are the usual 10-bit Morton ones
+template<int D> struct Spread32;
+template<> struct Spread32<2> {
+  static constexpr int kMax = 16;
+  static __device__ __forceinline__ uint32_t f(uint32_t x)
+  {
+    x &= 0xFFFFu;
+    x = (x | (x << 8)) & 0x00FF00FFu;
+    x = (x | (x << 4)) & 0x0F0F0F0Fu;
+    x = (x | (x << 2)) & 0x33333333u;
+    return (x | (x << 1)) & 0x55555555u;
+  }
+};
+template<> struct Spread32<3> {
+  static constexpr int kMax = 10;
+  static __device__ __forceinline__ uint32_t f(uint32_t x)
+  {
+    x &= 0x3FFu;
+    x = (x | (x << 16)) & 0xFF0000FFu;
+    x = (x | (x << 8)) & 0x0300F00Fu;
+    x = (x | (x << 4)) & 0x030C30C3u;
+    return (x | (x << 2)) & 0x09249249u;
+  }
+};
+template<> struct Spread32<4> {
+  static constexpr int kMax = 8;
+  static __device__ __forceinline__ uint32_t f(uint32_t x)
+  {
+    x &= 0xFFu;
+    x = (x | (x << 12)) & 0x000F000Fu;
+    x = (x | (x << 6)) & 0x03030303u;
+    return (x | (x << 3)) & 0x11111111u;
+  }
+};
+
 template<int D>
 __device__ __forceinline__ uint64_t interleave(const uint32_t (&bits)[D], const int (&k)[D], int depth)
 {
@@ -245,6 +289,25 @@ __device__ __forceinline__ uint64_t interleave(const uint32_t (&bits)[D], const 
       if (m * D + j < depth) code = (code << 1) | uint64_t((bits[j] >> (k[j] - 1 - m)) & 1u);
   }
   return code;
+}
+
+// the depth-d code of per-dimension indices with a launch's constants (32-bit spreading
+// where the code fits 32 bits)
+template<int D>
+__device__ __forceinline__ uint64_t code_of_bits(const DepthConst& dc, const uint32_t (&bits)[D], int depth)
+{
+  if constexpr (D >= 2) {
+    if (dc.c32) {
+      uint32_t x = 0;
+#pragma unroll
+      for (int j = 0; j < D; ++j) x |= Spread32<D>::f(bits[j] << dc.ks[j]) << (D - 1 - j);
+      return uint64_t(x >> dc.cs);
+    }
+  }
+  int k[D];
+#pragma unroll
+  for (int j = 0; j < D; ++j) k[j] = dc.k[j];
+  return interleave<D>(bits, k, depth);
 }
 
 // centre and radius of dimension j of a box whose index in that dimension is `bits`

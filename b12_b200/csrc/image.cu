@@ -132,6 +132,7 @@ __global__ void __launch_bounds__(kThreads, 6) image_points_kernel(const ImageAr
   const uint32_t n = *a.n_leaves;
   const uint32_t nboxes = a.n_src ? *a.n_src : (a.children ? 2u * n : n);
   const uint64_t P = a.points;
+  const uint32_t P32 = uint32_t(P);
   const uint64_t total = uint64_t(nboxes) * P;
   const int lane = threadIdx.x & 31;
   if (M == ImageMode::Hit && a.children && 2ull * n > a.hit_cap) {
@@ -141,7 +142,7 @@ __global__ void __launch_bounds__(kThreads, 6) image_points_kernel(const ImageAr
   // One point of the launch: g = rank * P + k (the source's rank among the sources, the
   // point's index in its box).  Every lane of the warp calls it the same number of times
   // (inactive lanes with active = false), so that the warp collectives stay converged.
-  auto point = [&](uint64_t g, uint64_t rank, uint64_t k, bool active) {
+  auto point = [&](uint64_t g, uint32_t rank, uint32_t k, bool active) {
     uint32_t t = kInvalidIndex;
     uint32_t tbits[Map::D];
     bool valid = false;
@@ -175,10 +176,7 @@ __global__ void __launch_bounds__(kThreads, 6) image_points_kernel(const ImageAr
       uint64_t code = kInvalidCode;
       bool fresh = false;
       if (active && valid) {
-        int k[Map::D];
-#pragma unroll
-        for (int j = 0; j < Map::D; ++j) k[j] = a.dc.k[j];
-        code = interleave<Map::D>(tbits, k, a.depth);
+        code = code_of_bits<Map::D>(a.dc, tbits, a.depth);
         fresh = !((a.bits[code >> 5] >> uint32_t(code & 31u)) & 1u);
       }
       const unsigned peers = __match_any_sync(0xFFFFFFFFu, fresh ? code : kInvalidCode) & __ballot_sync(0xFFFFFFFFu, fresh);
@@ -228,21 +226,22 @@ __global__ void __launch_bounds__(kThreads, 6) image_points_kernel(const ImageAr
     if (lane == 0) c = atomicAdd(a.work, 1ull);
     c = __shfl_sync(0xFFFFFFFFu, c, 0);
     if (c >= chunks) break;
+    // (sources and points per box both fit 32 bits: the rank and the point index do)
     const uint64_t g = c * kChunk + uint64_t(lane);
-    uint64_t rank, k;
+    uint32_t rank, k;
     if (total <= 0xFFFFFFFFull - kChunk) {
-      rank = uint32_t(g) / uint32_t(P);
-      k = uint32_t(g) - uint32_t(rank) * uint32_t(P);
+      rank = uint32_t(g) / P32;
+      k = uint32_t(g) - rank * P32;
     } else {
-      rank = g / P;
-      k = g - rank * P;
+      rank = uint32_t(g / P);
+      k = uint32_t(g - uint64_t(rank) * P);
     }
 #pragma unroll 1
     for (int j = 0; j < kChunkTrips; ++j) {
       const uint64_t gj = g + 32ull * uint64_t(j);
       point(gj, rank, k, gj < total);
       k += 32;
-      while (k >= P) { k -= P; ++rank; }
+      while (k >= P32) { k -= P32; ++rank; }
     }
   }
 }
