@@ -6,10 +6,10 @@
 // digit position of every key at once; then each digit takes ONE pass in which a tile
 // of 4096 keys (tile number drawn from an atomic counter, so that lower tiles are always
 // already running) ranks its keys stably in shared memory, publishes its per-digit
-// count, adds its predecessors' counts by decoupled look-back (a predecessor that has
-// already published its inclusive prefix ends the walk), and writes its keys out in
-// digit order from shared memory, so a warp's stores are runs of consecutive
-// addresses.  Every look-back wait is bounded: a tile that gives up sets bit 2 of the
+// count, stages its keys in digit order in shared memory, adds its predecessors' counts
+// by decoupled look-back (a predecessor that has already published its inclusive prefix
+// ends the walk), and writes its keys out from shared memory, so a warp's stores are
+// runs of consecutive addresses.  Every look-back wait is bounded: a tile that gives up sets bit 2 of the
 // caller's error word (the caller reports a timeout) and the result is not used.
 // This replaces the reference's thrust::sort / sort_by_key on codes
 // (helpFunctions.hpp:40-98 via sortBoxes, used by insertByIterators at
@@ -33,11 +33,11 @@ constexpr uint64_t kAggregate = 1ull << 62;       // status word: tile count pub
 constexpr uint64_t kInclusive = 2ull << 62;       // status word: inclusive prefix published
 constexpr uint64_t kFlagMask = 3ull << 62;
 constexpr uint32_t kLookbackPolls = 1u << 20;     // polls of one predecessor before giving up
-// predecessor status words loaded together in the look-back: 8 when tiles run in
-// several waves (the registers allow two blocks a SM), 32 when every tile runs at once,
-// where a tile's walk back to tile 0 is the chain that bounds the pass
-constexpr int kBatchWaves = 8;
-constexpr int kBatchOneWave = 32;
+// predecessor status words loaded together in the look-back: every tile of a wave
+// publishes its counts at about the same time, so a tile walks back over the wave's
+// earlier tiles until one has its inclusive prefix; 32 a round take the last tile of a
+// wave of 296 (two blocks a SM) there in 4 rounds, 8 a round in 9
+constexpr int kLookbackBatch = 32;
 
 int grid_for(uint64_t work, int per_block, int blocks_per_sm)
 {
@@ -104,8 +104,8 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* w
 // key index of (warp w, round r, lane) within a tile: each warp owns 512 consecutive keys
 __device__ __forceinline__ uint32_t tile_index(int w, int r, int lane) { return uint32_t(w * 512 + r * 32 + lane); }
 
-template<bool kValues, int kLookbackBatch>
-__global__ void __launch_bounds__(kThreads, kLookbackBatch == kBatchOneWave ? 1 : 2) onesweep_pass_kernel(const uint64_t* __restrict__ keys,
+template<bool kValues>
+__global__ void __launch_bounds__(kThreads, 2) onesweep_pass_kernel(const uint64_t* __restrict__ keys,
                                                                  const uint32_t* __restrict__ vals,
                                                                  const uint32_t* n_ptr, int pass, SortScratch sc,
                                                                  uint64_t* out, uint32_t* vout, uint32_t* error)
@@ -172,8 +172,28 @@ __global__ void __launch_bounds__(kThreads, kLookbackBatch == kBatchOneWave ? 1 
   __stcg(reinterpret_cast<unsigned long long*>(sc.status[(pass + 1) & 1] + size_t(t) * kBins + d), 0ull);
   const uint32_t digit_base = block_exclusive_scan(sc.hist[pass * kBins + d], warp_sums);
   const uint32_t tile_start = block_exclusive_scan(cnt, warp_sums);   // digit d's first staging index
+  for (int q = 0; q < kWarps; ++q) wcount[q][d] += tile_start;
+  __syncthreads();
 
-  // 3. decoupled look-back over the preceding tiles for digit d, kLookbackBatch tiles at
+  // 3. stage the tile in digit order (the positions are the tile's own), before the
+  // look-back, so that the keys' registers are free while it runs
+  uint32_t pos[kValues ? kRounds : 1];
+#pragma unroll
+  for (int r = 0; r < kRounds; ++r) {
+    const uint32_t li = tile_index(w, r, lane);
+    uint32_t p = kTile;
+    if (li < tile_n) {
+      const uint32_t dg = uint32_t((key[r] >> shift) & 0xFFu);
+      p = wcount[w][dg] + rank[r];
+      if (p < kTile) {
+        s_key[p] = key[r];
+        s_dig[p] = uint8_t(dg);
+      }
+    }
+    if constexpr (kValues) pos[r] = p;
+  }
+
+  // 4. decoupled look-back over the preceding tiles for digit d, kLookbackBatch tiles at
   // a time: their status words are loaded together (one memory latency per batch, not
   // one per tile), then taken nearest first; a tile that has not published yet is polled
   // (bounded) before the walk goes past it
@@ -209,23 +229,9 @@ __global__ void __launch_bounds__(kThreads, kLookbackBatch == kBatchOneWave ? 1 
     __stcg(reinterpret_cast<unsigned long long*>(status + d), (unsigned long long)(kInclusive | (excl + cnt)));
   }
   s_gofs[d] = digit_base + excl - tile_start;
-  for (int q = 0; q < kWarps; ++q) wcount[q][d] += tile_start;
   __syncthreads();
 
-  // 4. stage the tile in digit order, then write runs of consecutive addresses
-#pragma unroll
-  for (int r = 0; r < kRounds; ++r) {
-    const uint32_t li = tile_index(w, r, lane);
-    if (li < tile_n) {
-      const uint32_t dg = uint32_t((key[r] >> shift) & 0xFFu);
-      const uint32_t p = wcount[w][dg] + rank[r];
-      if (p < kTile) {
-        s_key[p] = key[r];
-        s_dig[p] = uint8_t(dg);
-      }
-    }
-  }
-  __syncthreads();
+  // 5. write runs of consecutive addresses
   // (a position past n would mean inconsistent counts: recorded as a capacity error, not written)
   for (uint32_t i = threadIdx.x; i < tile_n; i += kThreads) {
     const uint32_t g = s_gofs[s_dig[i]] + i;
@@ -237,13 +243,8 @@ __global__ void __launch_bounds__(kThreads, kLookbackBatch == kBatchOneWave ? 1 
     uint32_t* s_val = reinterpret_cast<uint32_t*>(s_key);
     __syncthreads();
 #pragma unroll
-    for (int r = 0; r < kRounds; ++r) {
-      const uint32_t li = tile_index(w, r, lane);
-      if (li < tile_n) {
-        const uint32_t p = wcount[w][(key[r] >> shift) & 0xFFu] + rank[r];
-        if (p < kTile) s_val[p] = val[r];
-      }
-    }
+    for (int r = 0; r < kRounds; ++r)
+      if (pos[r] < kTile) s_val[pos[r]] = val[r];
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < tile_n; i += kThreads) {
       const uint32_t g = s_gofs[s_dig[i]] + i;
@@ -271,12 +272,8 @@ cudaError_t onesweep(uint64_t* keys, uint64_t* alt, uint32_t* vals, uint32_t* va
   uint32_t* vsrc = vals;
   uint32_t* vdst = valt;
   const unsigned grid = tiles < 1 ? 1u : tiles;
-  const bool one_wave = grid <= unsigned(device_sm_count());
   for (int p = 0; p < passes; ++p) {
-    if (one_wave)
-      onesweep_pass_kernel<kValues, kBatchOneWave><<<grid, kThreads, 0, s>>>(src, vsrc, n, p, sc, dst, vdst, error);
-    else
-      onesweep_pass_kernel<kValues, kBatchWaves><<<grid, kThreads, 0, s>>>(src, vsrc, n, p, sc, dst, vdst, error);
+    onesweep_pass_kernel<kValues><<<grid, kThreads, 0, s>>>(src, vsrc, n, p, sc, dst, vdst, error);
     std::swap(src, dst);
     if constexpr (kValues) std::swap(vsrc, vdst);
   }

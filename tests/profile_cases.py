@@ -9,8 +9,13 @@ image     a Lorenz tree subdivided to --depth - 1 (default 23), then one subdivi
 compact   64 Lorenz instances (rho = 28, explicit FMA) batched to depth 27: the last
           steps compact ~20 M children (code 8 B + flags 1 B + hit 1 B each), well
           beyond the 126 MB L2, so the compaction's DRAM traffic is meaningful.
-sort      the coupled-Duffing continuation at depth 24 (64 Philox points per box):
-          each sweep radix-sorts 64 candidate codes per expanded box.
+continuation
+          the coupled-Duffing continuation at depth 24 (64 Philox points per box) over
+          the bitmap of the depth's boxes.
+sort      --points uniform random 4-D points inserted at depth 24 into the boxes of 12
+          sweeps of that continuation: the candidate codes of the points in no leaf
+          are radix-sorted (one histogram pass, three digit passes), made unique and
+          merged into the leaves.
 measure   one Lorenz job to --depth (default 27), its transition matrix and 200 power
           iterations; depth 32 gives ~2.6 M boxes, a matrix of ~0.25 GB (HBM-bound SpMV).
 serve     a burst of --jobs served-stream jobs through the job server.
@@ -72,18 +77,29 @@ def case_compact(args):
     b.close()
 
 
-def case_sort(args):
+def case_continuation(args):
     import b12_b200 as B
     t = B.ImplicitBoxTree((0.0,) * 4, (2.0,) * 4)
     t.reserve(16 << 20)
     sc = B.Scheme(B.coupled_duffing(), B.philox_grid(64, 0))
     t0 = time.perf_counter()
     sweeps = t.continuation_run(sc, np.zeros(4), args.depth)
-    # sweep s sorts 64 candidates per box inserted by sweep s - 1
-    grown = np.diff(np.concatenate([[0, 1], sweeps.astype(np.int64)]))[:-1]
-    big = int(np.argmax(grown))
-    print(f"sort: continuation depth {args.depth}: {int(sweeps[-1])} boxes in {len(sweeps)} sweeps, "
-          f"{time.perf_counter() - t0:.3f} s; largest sort: sweep {big} ({64 * int(grown[big])} candidates)")
+    print(f"continuation: depth {args.depth}: {int(sweeps[-1])} boxes in {len(sweeps)} sweeps, "
+          f"{time.perf_counter() - t0:.3f} s")
+    t.close()
+
+
+def case_sort(args):
+    import b12_b200 as B
+    t = B.ImplicitBoxTree((0.0,) * 4, (2.0,) * 4)
+    sc = B.Scheme(B.coupled_duffing(), B.philox_grid(64, 0))
+    sweeps = t.continuation_run(sc, np.zeros(4), args.depth, max_sweeps=12)
+    rng = np.random.default_rng(0)
+    pts = rng.uniform(-2.0, 2.0, size=(args.points, 4))
+    t0 = time.perf_counter()
+    new = t.insert_points(pts, args.depth, B.INS, B.NONE)
+    print(f"sort: {args.points} random points into {int(sweeps[-1])} boxes of depth {args.depth} "
+          f"(12 continuation sweeps): {new} new boxes, {time.perf_counter() - t0:.3f} s")
     t.close()
 
 
@@ -180,7 +196,9 @@ def case_partition(args):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["image", "compact", "sort", "measure", "serve", "mixed", "partition"])
+    ap.add_argument("case", choices=["image", "compact", "continuation", "sort", "measure", "serve", "mixed",
+                                     "partition"])
+    ap.add_argument("--points", type=int, default=8 << 20, help="sort: random points inserted")
     ap.add_argument("--depth", type=int, default=None)
     ap.add_argument("--instances", type=int, default=64)
     ap.add_argument("--jobs", type=int, default=300)
@@ -188,9 +206,9 @@ def main():
     ap.add_argument("--world", type=int, default=2, help="partition: emulated ranks")
     args = ap.parse_args()
     if args.depth is None:
-        args.depth = {"image": 23, "compact": 27, "sort": 24, "measure": 27, "serve": 0,
+        args.depth = {"image": 23, "compact": 27, "continuation": 24, "sort": 24, "measure": 27, "serve": 0,
                       "mixed": 21, "partition": 27}[args.case]
-    {"image": case_image, "compact": case_compact, "sort": case_sort, "measure": case_measure,
+    {"image": case_image, "compact": case_compact, "continuation": case_continuation, "sort": case_sort, "measure": case_measure,
      "serve": case_serve, "mixed": case_mixed, "partition": case_partition}[args.case](args)
 
 
