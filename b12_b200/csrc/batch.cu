@@ -127,13 +127,19 @@ struct BatchPoint {
     double x[W][D], y[W][D];
     int dep[W];
     MapParams mp[W];
+    const bool uni = a.inst_depth == nullptr;   // one depth: the launch's constants
 #pragma unroll
     for (int w = 0; w < W; ++w) {
-      dep[w] = a.inst_depth ? int(a.inst_depth[inst[w]]) : a.depth;
+      dep[w] = uni ? a.depth : int(a.inst_depth[inst[w]]);
       const uint64_t c = child[w];
       const uint64_t code = act[w] ? ((a.codes[c >> 1] << 1) | (c & 1u)) : 0ull;
       double cc[D], r[D];
-      box_coordinates<D>(a.dom, code, dep[w], cc, r);
+      if (uni) {
+#pragma unroll
+        for (int j = 0; j < D; ++j) box_axis(a.dom, a.dc.ax[j], j, deinterleave<D>(code, a.depth, j), cc[j], r[j]);
+      } else {
+        box_coordinates<D>(a.dom, code, dep[w], cc, r);
+      }
 #pragma unroll
       for (int j = 0; j < D; ++j) x[w][j] = __dadd_rn(cc[j], __dmul_rn(pts[j * uint32_t(a.points) + k[w]], r[j]));
       mp[w] = a.map;
@@ -159,7 +165,14 @@ struct BatchPoint {
 #pragma unroll
     for (int w = 0; w < W; ++w) {
       uint64_t tcode = 0;
-      const bool inside = act[w] && point_code<D>(a.dom, y[w], dep[w], tcode);
+      bool inside = false;
+      if (uni) {
+        uint32_t tb[D];
+        inside = act[w] && point_bits<D>(a.dom, a.dc, y[w], tb);
+        if (inside) tcode = code_of_bits<D>(a.dc, tb, a.depth);
+      } else {
+        inside = act[w] && point_code<D>(a.dom, y[w], dep[w], tcode);
+      }
       uint32_t t = act[w] ? kOutsideIndex : kInvalidIndex;
       if (inside) {
         const uint32_t p = hash_locate(a.hash, off_s[a.n_inst], inst_key(inst[w], tcode >> 1));
@@ -454,8 +467,17 @@ int batch_grid(const void* kernel, int threads)
 namespace b12g {
 
 cudaError_t launch_batch_image(uint32_t map_kind, uint32_t arith, uint32_t grid_kind, const Tuning& tu,
-                               const BatchArgs& a, cudaStream_t s)
+                               const BatchArgs& args, cudaStream_t s)
 {
+  BatchArgs a = args;
+  if (!a.inst_depth) {
+    int dim = 0;
+    batch_dispatch(map_kind, arith, grid_kind, [&](auto map, auto) -> cudaError_t {
+      dim = decltype(map)::D;
+      return cudaSuccess;
+    });
+    if (dim > 0) fill_depth_const(a.dom, dim, a.depth, a.dc);
+  }
   return batch_dispatch(map_kind, arith, grid_kind, [&](auto map, auto grid) -> cudaError_t {
     using Map = decltype(map);
     using Grid = decltype(grid);

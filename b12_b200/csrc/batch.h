@@ -29,6 +29,8 @@ struct BatchArgs {
   const uint64_t* codes;            // parents
   int depth;                        // depth of the children (subdivision step)
   const uint8_t* inst_depth;        // per-instance children depth (nullptr: `depth` for all)
+  DepthConst dc;                    // constants of `depth` when every instance has it
+                                    // (launch_batch_image fills them in)
   LeafHash hash;
   uint8_t* hit;
   uint32_t hit_cap;
