@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(kThreads, 6) image_points_kernel(const ImageAr
   const bool table = load_points<Grid, Map::D>(a.grid, a.points, pts);
 
   const uint32_t n = *a.n_leaves;
-  const uint32_t nboxes = a.n_src ? *a.n_src : (a.children ? 2u * n : n);
+  const uint32_t nboxes = M == ImageMode::Mark ? a.n_src_value : a.n_src ? *a.n_src : (a.children ? 2u * n : n);
   const uint64_t P = a.points;
   const uint32_t P32 = uint32_t(P);
   const uint64_t total = uint64_t(nboxes) * P;

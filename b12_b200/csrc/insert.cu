@@ -540,12 +540,15 @@ __global__ void __launch_bounds__(kThreads) tile_count_kernel(const uint32_t* __
 }
 
 // tile_first: the tiles' first positions (a scan of the counts), or nullptr: summed here
+template<int D>
 __global__ void __launch_bounds__(kThreads) tile_scatter_kernel(uint32_t* __restrict__ bits, uint32_t words,
                                                                 const uint32_t* __restrict__ tile_count,
                                                                 const uint32_t* __restrict__ tile_first,
                                                                 uint64_t* __restrict__ out, int clear,
                                                                 const uint32_t* __restrict__ mark,
-                                                                uint8_t* __restrict__ flags, uint8_t f)
+                                                                uint8_t* __restrict__ flags, uint8_t f,
+                                                                double* __restrict__ centres, Domain dom,
+                                                                DepthConst dc, int depth)
 {
   __shared__ uint32_t red[kThreads / 32];
   __shared__ uint32_t wsum[kThreads / 32];
@@ -584,8 +587,20 @@ __global__ void __launch_bounds__(kThreads) tile_scatter_kernel(uint32_t* __rest
       const uint32_t mk = (mark && b) ? mark[w0 + q] : 0u;
       while (b) {
         const int bit = __ffs(b) - 1;
-        out[p] = (uint64_t(w0 + q) << 5) | uint64_t(bit);
+        const uint64_t code = (uint64_t(w0 + q) << 5) | uint64_t(bit);
+        out[p] = code;
         if (flags) flags[p] = ((mk >> bit) & 1u) ? f : uint8_t(0);
+        if (centres) {
+          double cc[kSrcStride] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+          for (int j = 0; j < D; ++j) {
+            double rr;
+            box_axis(dom, dc.ax[j], j, deinterleave<D>(code, depth, j), cc[j], rr);
+          }
+          double2* o = reinterpret_cast<double2*>(centres + size_t(kSrcStride) * p);
+          o[0] = make_double2(cc[0], cc[1]);
+          o[1] = make_double2(cc[2], cc[3]);
+        }
         ++p;
         b &= b - 1u;
       }
@@ -595,11 +610,12 @@ __global__ void __launch_bounds__(kThreads) tile_scatter_kernel(uint32_t* __rest
   }
 }
 
-// the codes of the set bits of `bits` (words u32) in increasing order into `out`, and
-// flags into `flags` when not null (f where `mark` has the bit); clears the bitmap when
-// asked
+// the codes of the set bits of `bits` (words u32) in increasing order into `out`, flags
+// into `flags` when not null (f where `mark` has the bit), the boxes' centres at the
+// tree's depth into `centres` when not null; clears the bitmap when asked
 b12g_status bitmap_codes(b12g_tree* t, uint32_t* bits, uint32_t words, uint64_t* out, bool clear,
-                         const uint32_t* mark = nullptr, uint8_t* flags = nullptr, uint8_t f = 0)
+                         const uint32_t* mark = nullptr, uint8_t* flags = nullptr, uint8_t f = 0,
+                         double* centres = nullptr)
 {
   const uint32_t tiles = (words + kWordTile - 1) / kWordTile;
   ST(t->sort_idx.ensure(2 * (size_t(tiles) + 1) + compact_tiles(uint64_t(tiles) + 1) + 8, "bitmap tile counts"));
@@ -615,8 +631,18 @@ b12g_status bitmap_codes(b12g_tree* t, uint32_t* bits, uint32_t words, uint64_t*
     CK(exclusive_scan_u32(count, first, t->ctr.p + C_TMP, first + tiles + 1, tiles, t->stream));
     count_launches(3);
   }
-  tile_scatter_kernel<<<g, kThreads, 0, t->stream>>>(bits, words, count, first, out, clear ? 1 : 0, mark, flags, f);
-  CK(cudaGetLastError());
+  DepthConst dc;
+  fill_depth_const(t->dom, int(t->domain.dim), t->depth, dc);
+  CK(by_dim(t->domain.dim, [&](auto d) {
+    constexpr int kD = decltype(d)::value;
+    if constexpr (kD < 2) {
+      return cudaErrorInvalidValue;      // (the image kernels' maps have two or more dimensions)
+    } else {
+      tile_scatter_kernel<kD><<<g, kThreads, 0, t->stream>>>(bits, words, count, first, out, clear ? 1 : 0, mark,
+                                                            flags, f, centres, t->dom, dc, int(t->depth));
+      return cudaGetLastError();
+    }
+  }));
   count_launches(1);
   return B12G_OK;
 }
@@ -640,7 +666,7 @@ b12g_status continuation_bitmap(b12g_tree* t, const b12g_scheme* s, uint8_t dept
   Prepared pr;
   ST(prepare(t, s, pr));
   pr.a.src = nullptr;
-  pr.a.n_src = t->ctr.p + C_NSRC;
+  pr.a.n_src = nullptr;
   pr.a.bits = bits;
   pr.a.fresh = fresh;
   pr.a.cand_count = t->ctr.p + C_CAND;
@@ -649,7 +675,7 @@ b12g_status continuation_bitmap(b12g_tree* t, const b12g_scheme* s, uint8_t dept
   while (nb1 > nb0 && k < max_sweeps) {
     const uint64_t points = uint64_t(n_src) * pr.P;
     ST(set_ctr(t, C_CAND, 0));
-    ST(set_ctr(t, C_NSRC, n_src));
+    pr.a.n_src_value = n_src;
     pr.a.src_c = t->srcc.p;
     u = 0;
     if (points > 0) {
@@ -668,8 +694,8 @@ b12g_status continuation_bitmap(b12g_tree* t, const b12g_scheme* s, uint8_t dept
       if (u > 0) {
         // the next sources: the new boxes in code order, their codes and centres
         ST(t->cand.ensure_room(u, "new boxes", 2));
-        ST(bitmap_codes(t, fresh, words, t->cand.p, true));
-        ST(centres_of(t, t->cand.p, nullptr, t->ctr.p + C_CAND, u));
+        ST(t->srcc.ensure_room(uint64_t(u) * kSrcStride, "source centres", 2));
+        ST(bitmap_codes(t, fresh, words, t->cand.p, true, nullptr, nullptr, 0, t->srcc.p));
       }
     }
     n += u;

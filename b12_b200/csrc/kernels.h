@@ -31,6 +31,7 @@ struct ImageArgs {
   int children;              // 1: boxes are the 2n children of `codes`, never materialised
   const uint32_t* src;       // source leaf ranks -> leaf index (nullptr: all leaves)
   const uint32_t* n_src;     // device count of sources (nullptr: all leaves / children)
+  uint32_t n_src_value;      // Mark mode: the count of sources itself (n_src unused)
   const double* src_c;       // optional: the centre of every source box by rank, kSrcStride
                              // doubles a source (the radius is dc's); nullptr: from the codes
   uint64_t points;           // points per box
