@@ -97,6 +97,8 @@ _SIGS = {
     "b12g_transition_matrix": (C.c_int, [C.c_void_p, C.POINTER(Scheme), C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
     "b12g_image_point_boxes": (C.c_int, [C.c_void_p, C.POINTER(Scheme), C.c_void_p, C.c_void_p, C.c_uint64,
                                          C.POINTER(C.c_uint64)]),
+    "b12g_image_distinct_point_boxes": (C.c_int, [C.c_void_p, C.POINTER(Scheme), C.c_uint8, C.c_void_p,
+                                                  C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),
     "b12g_search_point_boxes": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p]),
     "b12g_set_flags_by_point_boxes": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint8,
                                                 C.POINTER(C.c_uint32)]),

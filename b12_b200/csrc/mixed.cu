@@ -672,6 +672,9 @@ struct MixedArgs {
   uint32_t* out;               // Search: leaf index of every point
   uint64_t* p64_out;           // Codes: depth-64 code of every image point
   uint8_t* valid_out;          //        1 if it lies in the domain
+  uint32_t* n_out;             // Distinct codes: how many were written (at most p64_cap)
+  uint64_t p64_cap;
+  uint64_t p64_keep;           //        the bits of a code kept: its first bisections
   const uint32_t* box_pos;     // inner depth: scan of the box heads (box of leaf j: box_pos[j + 1] - 1)
   uint32_t inner_depth;
   uint8_t* box_hit;            //              hit marks of the boxes
@@ -740,7 +743,10 @@ __device__ __forceinline__ uint32_t image_of(const MixedArgs& a, const double* p
 
 // kMode 0: hit marks of the leaves hit; 1: leaf index of every point; 2: the points'
 // depth-64 codes and validity (the point boxes of an insertion); 3: hit marks of the
-// boxes at the inner depth a.inner_depth; 4: box index at that depth of every point
+// boxes at the inner depth a.inner_depth; 4: box index at that depth of every point;
+// 5: the point boxes of mode 2 cut to their first bisections (a.p64_keep), each distinct
+// (code, validity) pair of a warp's 32 points once, appended in no fixed order (the set
+// the flags of a step need)
 template<class Map, class Grid, int kMode>
 __global__ void __launch_bounds__(kThreads) mixed_image_kernel(const MixedArgs a)
 {
@@ -748,26 +754,64 @@ __global__ void __launch_bounds__(kThreads) mixed_image_kernel(const MixedArgs a
   const bool table = load_table<Grid, Map::D>(a.grid, a.points, pts);
   const uint64_t P = a.points;
   const uint64_t total = uint64_t(a.n_src) * P;
-  for (uint64_t g = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < total; g += uint64_t(gridDim.x) * blockDim.x) {
-    const uint64_t rank = g / P;
-    const uint32_t k = uint32_t(g - rank * P);
-    const uint32_t leaf = a.src ? __ldg(a.src + rank) : uint32_t(rank);
-    if constexpr (kMode == 2) {
-      uint64_t p64;
-      const bool valid = image_code<Map, Grid>(a, pts, table, leaf, k, g, p64);
-      a.valid_out[g] = valid ? 1 : 0;
-      a.p64_out[g] = valid ? p64 : ~0ull;   // the invalid box (~0, 255) of PointToBox
-    } else if constexpr (kMode >= 3) {
-      uint64_t p64;
-      const bool valid = image_code<Map, Grid>(a, pts, table, leaf, k, g, p64);
-      const uint32_t b = inner_box_of(CmpIndex{a.cmp, a.tab, a.n, a.tab_bits}, a.code, a.dep, a.box_pos,
-                                      a.inner_depth, valid, p64);
-      if constexpr (kMode == 4) a.out[g] = b;
-      else if (b != kInvalidIndex) a.box_hit[b] = 1;
-    } else {
-      const uint32_t t = image_of<Map, Grid>(a, pts, table, leaf, k, g);
-      if constexpr (kMode == 1) a.out[g] = t;
-      else if (t != kInvalidIndex) a.hit[t] = 1;
+  if constexpr (kMode == 5) {
+    // whole warps take the loop's trips together (the warp collectives stay converged)
+    const int lane = threadIdx.x & 31;
+    for (uint64_t g0 = uint64_t(blockIdx.x) * blockDim.x + (threadIdx.x & ~31u); g0 < total;
+         g0 += uint64_t(gridDim.x) * blockDim.x) {
+      const uint64_t g = g0 + uint64_t(lane);
+      const bool active = g < total;
+      uint64_t key = 0;
+      bool valid = false;
+      if (active) {
+        const uint64_t rank = g / P;
+        const uint32_t k = uint32_t(g - rank * P);
+        const uint32_t leaf = a.src ? __ldg(a.src + rank) : uint32_t(rank);
+        uint64_t p64;
+        valid = image_code<Map, Grid>(a, pts, table, leaf, k, g, p64);
+        key = valid ? (p64 & a.p64_keep) : ~0ull;   // the invalid box (~0, 255) of PointToBox
+      }
+      // a valid box of code ~0 and the invalid box differ in validity: keys of both kinds
+      // lead separately
+      const unsigned act = __ballot_sync(0xFFFFFFFFu, active);
+      const unsigned vmask = __ballot_sync(0xFFFFFFFFu, active && valid);
+      const unsigned same = __match_any_sync(0xFFFFFFFFu, key) & act & (valid ? vmask : ~vmask);
+      const bool leader = active && lane == __ffs(same) - 1;
+      const unsigned lead = __ballot_sync(0xFFFFFFFFu, leader);
+      uint32_t slot = 0;
+      if (lane == 0 && lead) slot = atomicAdd(a.n_out, uint32_t(__popc(lead)));
+      slot = __shfl_sync(0xFFFFFFFFu, slot, 0);
+      if (leader) {
+        const uint64_t pos = uint64_t(slot) + __popc(lead & ((1u << lane) - 1u));
+        if (pos < a.p64_cap) {
+          a.p64_out[pos] = key;
+          a.valid_out[pos] = valid ? 1 : 0;
+        }
+      }
+    }
+  } else {
+    for (uint64_t g = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < total;
+         g += uint64_t(gridDim.x) * blockDim.x) {
+      const uint64_t rank = g / P;
+      const uint32_t k = uint32_t(g - rank * P);
+      const uint32_t leaf = a.src ? __ldg(a.src + rank) : uint32_t(rank);
+      if constexpr (kMode == 2) {
+        uint64_t p64;
+        const bool valid = image_code<Map, Grid>(a, pts, table, leaf, k, g, p64);
+        a.valid_out[g] = valid ? 1 : 0;
+        a.p64_out[g] = valid ? p64 : ~0ull;   // the invalid box (~0, 255) of PointToBox
+      } else if constexpr (kMode >= 3) {
+        uint64_t p64;
+        const bool valid = image_code<Map, Grid>(a, pts, table, leaf, k, g, p64);
+        const uint32_t b = inner_box_of(CmpIndex{a.cmp, a.tab, a.n, a.tab_bits}, a.code, a.dep, a.box_pos,
+                                        a.inner_depth, valid, p64);
+        if constexpr (kMode == 4) a.out[g] = b;
+        else if (b != kInvalidIndex) a.box_hit[b] = 1;
+      } else {
+        const uint32_t t = image_of<Map, Grid>(a, pts, table, leaf, k, g);
+        if constexpr (kMode == 1) a.out[g] = t;
+        else if (t != kInvalidIndex) a.hit[t] = 1;
+      }
     }
   }
 }
@@ -1491,7 +1535,7 @@ b12g_status mixed_image_boxes(b12g_tree* t, const b12g_scheme* sc, uint64_t* n_p
 // the point boxes of the images of the scheme's sources into the caller's device buffers
 // (codes, validity), source-major; CAPACITY with *n_points set when they do not fit
 b12g_status mixed_image_point_boxes(b12g_tree* t, const b12g_scheme* sc, uint64_t* codes, uint8_t* valid,
-                                    uint64_t capacity, uint64_t* n_points)
+                                    uint64_t capacity, uint64_t* n_points, bool distinct, uint8_t keep_depth)
 {
   ST(mixed_enter(t));
   MixedArgs a;
@@ -1510,14 +1554,26 @@ b12g_status mixed_image_point_boxes(b12g_tree* t, const b12g_scheme* sc, uint64_
   }
   a.p64_out = codes;
   a.valid_out = valid;
+  a.p64_cap = capacity;
+  a.p64_keep = keep_depth >= 64 ? ~0ull : keep_depth == 0 ? 0ull : ~((uint64_t(1) << (64 - keep_depth)) - 1ull);
+  a.n_out = t->ctr.p + C_TMP;
   if (np) {
+    if (distinct) ST(set_ctr(t, C_TMP, 0));
     CK(dispatch(sc->map.kind, sc->map.arith, sc->grid.kind, t->domain.dim, [&](auto map, auto grid) -> cudaError_t {
-      mixed_image_kernel<decltype(map), decltype(grid), 2><<<grid_for_n(np), kThreads, 0, t->stream>>>(a);
+      if (distinct)
+        mixed_image_kernel<decltype(map), decltype(grid), 5><<<grid_for_n(np), kThreads, 0, t->stream>>>(a);
+      else
+        mixed_image_kernel<decltype(map), decltype(grid), 2><<<grid_for_n(np), kThreads, 0, t->stream>>>(a);
       return cudaGetLastError();
     }));
     count_launches(1);
   }
-  ST(sync(t, "image point boxes"));
+  if (distinct && np) {
+    ST(read_ctr(t, C_TMP, 1));
+    *n_points = t->h_ctr[C_TMP];
+  } else {
+    ST(sync(t, "image point boxes"));
+  }
   return mixed_settle(t);
 }
 

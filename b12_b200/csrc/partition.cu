@@ -147,6 +147,14 @@ b12g_status b12g_image_point_boxes(b12g_tree* t, const b12g_scheme* sc, uint64_t
   return mixed_image_point_boxes(t, sc, codes, valid, capacity, n_points);
 }
 
+b12g_status b12g_image_distinct_point_boxes(b12g_tree* t, const b12g_scheme* sc, uint8_t depth, uint64_t* codes,
+                                            uint8_t* valid, uint64_t capacity, uint64_t* n_boxes)
+{
+  if (!t || !sc || !n_boxes) return fail(B12G_ERR_INVALID, "NULL argument");
+  if (depth > 64) return fail(B12G_ERR_INVALID, "depth %u above 64", depth);
+  return mixed_image_point_boxes(t, sc, codes, valid, capacity, n_boxes, true, depth);
+}
+
 b12g_status b12g_search_point_boxes(b12g_tree* t, const uint64_t* codes, const uint8_t* valid, uint64_t n,
                                     uint32_t* index)
 {

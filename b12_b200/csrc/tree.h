@@ -265,9 +265,12 @@ b12g_status mixed_insert_boxes(b12g_tree* t, uint64_t np, uint8_t depth, uint8_t
 b12g_status mixed_point_boxes(b12g_tree* t, const double* points, uint64_t n_points);
 b12g_status mixed_image_boxes(b12g_tree* t, const b12g_scheme* sc, uint64_t* n_points);
 // point boxes in the caller's device buffers (range-partitioned trees): the images of the
-// scheme's sources, the leaf of each given point box, or flags set on the leaves hit
+// scheme's sources (every point, or each warp's distinct point boxes once, cut to their
+// first keep_depth bisections), the leaf of each given point box, or flags set on the
+// leaves hit
 b12g_status mixed_image_point_boxes(b12g_tree* t, const b12g_scheme* sc, uint64_t* codes, uint8_t* valid,
-                                    uint64_t capacity, uint64_t* n_points);
+                                    uint64_t capacity, uint64_t* n_points, bool distinct = false,
+                                    uint8_t keep_depth = 64);
 b12g_status mixed_point_box_search(b12g_tree* t, const uint64_t* codes, const uint8_t* valid, uint64_t n,
                                    uint32_t* index, uint8_t flags, uint32_t* n_changed);
 // leaves from device memory, checked for order and nesting on the device

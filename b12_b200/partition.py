@@ -101,6 +101,19 @@ class DeviceRun:
                     torch.empty(0, dtype=torch.uint8, device=self.device))
         return self.tree.image_point_boxes(scheme, self.device)
 
+    def max_depth(self) -> int:
+        return 0 if self.empty else self.tree.depth()
+
+    def image_hit_boxes(self, scheme, depth: int):
+        """The point boxes of image_point_boxes cut to `depth` (at least every leaf's depth,
+        on every rank) as a set (each warp's distinct boxes once): all that setting the
+        flags of the leaves they hit needs, in fewer boxes to send."""
+        import torch
+        if self.empty:
+            return (torch.empty(0, dtype=torch.int64, device=self.device),
+                    torch.empty(0, dtype=torch.uint8, device=self.device))
+        return self.tree.image_distinct_point_boxes(scheme, self.device, depth)
+
     def set_flags_by_point_boxes(self, codes, valid, flags: int) -> int:
         return 0 if self.empty else self.tree.set_flags_by_point_boxes(codes, valid, flags)
 
@@ -163,7 +176,8 @@ class PartitionedTree:
         import torch
         n = self.run.n
         start = _ordered(self.run.start()) if n else 0
-        row = torch.tensor([n, start], dtype=torch.int64, device=self.run.device)
+        depth = self.run.max_depth() if hasattr(self.run, "max_depth") else 64
+        row = torch.tensor([n, start, depth], dtype=torch.int64, device=self.run.device)
         self.table = (yield ("allgather", row)).to("cpu")
         return self.table
 
@@ -282,9 +296,15 @@ class PartitionedTree:
             yield from self.start()
         self.run.set_flags(L.SD)
         counts = []
+        # a run that can send its image boxes as a set does, cut to the depth of the
+        # deepest leaf on any rank after the subdivision (the flags need no more)
+        hit_boxes = getattr(self.run, "image_hit_boxes", None)
         for _ in range(steps):
             self.run.subdivide(L.SD)
-            codes, valid = self.run.image_point_boxes(scheme)
+            if hit_boxes is not None:
+                codes, valid = hit_boxes(scheme, min(64, int(self.table[:, 2].max()) + 1))
+            else:
+                codes, valid = self.run.image_point_boxes(scheme)
             _, _, rc, rv = yield from self._exchange_point_boxes(codes, valid)
             self.run.set_flags_by_point_boxes(rc, rv, L.HIT)
             self.run.remove(L.HIT)

@@ -419,6 +419,21 @@ class ImplicitBoxTree:
                                            C.byref(n)), "image_point_boxes")
         return codes[: n.value], valid[: n.value]
 
+    def image_distinct_point_boxes(self, scheme: Scheme, device, depth: int = 64):
+        """(codes, valid): the point boxes of image_point_boxes cut to their first `depth`
+        bisections, as a set (each distinct box of 32 consecutive points once, in no fixed
+        order), for the flags of a step over leaves no deeper than `depth`."""
+        import torch
+        room = self.count() * scheme.grid.points_per_box(self.dim)
+        codes = torch.empty(max(room, 1), dtype=torch.int64, device=device)
+        valid = torch.empty(max(room, 1), dtype=torch.uint8, device=device)
+        n = C.c_uint64()
+        s = scheme.to_c()
+        self._ready(codes)
+        check(lib().b12g_image_distinct_point_boxes(self._h, C.byref(s), depth, codes.data_ptr(), valid.data_ptr(),
+                                                    room, C.byref(n)), "image_distinct_point_boxes")
+        return codes[: n.value], valid[: n.value]
+
     def search_point_boxes(self, codes, valid):
         """searchByIterators over point boxes: an int64 tensor of leaf indices (-1: none)."""
         import torch

@@ -201,6 +201,14 @@ b12g_status b12g_insert_by_image(b12g_tree* tree, const b12g_scheme* scheme, uin
  * source-major; CAPACITY with *n_points set when capacity is too small */
 b12g_status b12g_image_point_boxes(b12g_tree* tree, const b12g_scheme* scheme, uint64_t* codes, uint8_t* valid,
                                    uint64_t capacity, uint64_t* n_points);
+/* the same point boxes as a set for setFlagsByIterators (ImplicitBoxTree.hpp:2167-2196),
+ * each code cut to its first `depth` bisections (the lower bits zero: the same leaves
+ * hold it when no leaf is deeper than `depth`), each distinct (code, validity) pair of
+ * 32 consecutive points once, in no fixed order; *n_boxes = how many were written;
+ * capacity must hold one box per point (the number b12g_image_point_boxes reports),
+ * else CAPACITY */
+b12g_status b12g_image_distinct_point_boxes(b12g_tree* tree, const b12g_scheme* scheme, uint8_t depth,
+                                            uint64_t* codes, uint8_t* valid, uint64_t capacity, uint64_t* n_boxes);
 /* searchByIterators over n point boxes at the leaf depth (ImplicitBoxTree.hpp:2394-2432):
  * the leaf holding each, or B12G_INVALID_INDEX */
 b12g_status b12g_search_point_boxes(b12g_tree* tree, const uint64_t* codes, const uint8_t* valid, uint64_t n,

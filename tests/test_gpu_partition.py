@@ -69,6 +69,39 @@ def test_point_box_entries_match_oracle(golden, name):
         ref.close()
 
 
+@pytest.mark.parametrize("name", ["henon_d12_lost", "lorenz_d15"])
+def test_distinct_point_boxes_are_the_set_of_the_point_boxes(golden, name):
+    """The image boxes as a set (each warp's distinct boxes once): the same set of
+    (code, validity) pairs as every point's box, each at most once per 32 points, and the
+    same flags set from them."""
+    _, spec, t, sc, o = _grown(name, golden)
+    oc, ov = o.image_point_boxes()
+    codes, valid = t.image_distinct_point_boxes(sc, "cuda")
+    dc, dv = codes.cpu().numpy().view(np.uint64), valid.cpu().numpy()
+    assert set(zip(dc.tolist(), dv.tolist())) == set(zip(oc.tolist(), ov.tolist()))
+    assert len(dc) <= len(oc)
+    # no pair twice within one group of 32 consecutive points: at most as many entries
+    # as the groups' distinct pairs summed
+    groups = sum(len(set(zip(oc[i:i + 32].tolist(), ov[i:i + 32].tolist()))) for i in range(0, len(oc), 32))
+    assert len(dc) <= groups
+    assert t.set_flags_by_point_boxes(codes, valid, B.EQU) == o.set_flags_by_point_boxes(oc, ov, 0x10)
+    for x, y in zip(t.leaves(), o.leaves()):
+        np.testing.assert_array_equal(x, y)
+    # cut to the leaves' depth: far fewer boxes, the same leaves hit
+    d = t.depth()
+    keep = ~np.uint64(0) if d >= 64 else ~np.uint64((1 << (64 - d)) - 1)
+    cc, cv = t.image_distinct_point_boxes(sc, "cuda", d)
+    hc, hv = cc.cpu().numpy().view(np.uint64), cv.cpu().numpy()
+    want = set(zip(np.where(ov != 0, oc & keep, oc).tolist(), ov.tolist()))
+    assert set(zip(hc.tolist(), hv.tolist())) == want
+    assert len(hc) < len(oc) // 4
+    t.unset_flags(B.EQU)
+    o.unset_flags(0x10)
+    assert t.set_flags_by_point_boxes(cc, cv, B.EQU) == o.set_flags_by_point_boxes(oc, ov, 0x10)
+    for x, y in zip(t.leaves(), o.leaves()):
+        np.testing.assert_array_equal(x, y)
+
+
 def test_point_boxes_of_a_tree_of_several_depths(golden):
     meta, arrays = golden("henon_d14_mixed8")
     spec = meta["spec"]
