@@ -68,9 +68,9 @@ class DeviceRun:
         c, d, _ = self.tree.leaf_at(0)
         return box_start(c, d)
 
-    def route_point_boxes(self, codes, valid, starts, ranks, world: int):
+    def route_point_boxes(self, codes, valid, starts, ranks, world: int, want_slot: bool = True):
         """The point boxes grouped by owner rank, on this GPU (b12g_route_point_boxes)."""
-        return self.tree.route_point_boxes(codes, valid, starts, ranks, world)
+        return self.tree.route_point_boxes(codes, valid, starts, ranks, world, want_slot)
 
     def set_flags(self, flags: int) -> None:
         if not self.empty:
@@ -227,18 +227,18 @@ class PartitionedTree:
             parts.append(list(g.split(splits)))
         return slot, parts
 
-    def _route_boxes(self, codes, valid):
+    def _route_boxes(self, codes, valid, want_slot=True):
         """(slot or None, per-rank codes, per-rank validity) of this rank's point boxes."""
         ranks, starts = self._owned_runs()
         route = getattr(self.run, "route_point_boxes", None)
         if len(ranks) > 1 and route is not None:
-            slot, c_parts, v_parts = route(codes, valid, starts, ranks, self.world)
+            slot, c_parts, v_parts = route(codes, valid, starts, ranks, self.world, want_slot)
             return slot, (c_parts, v_parts)
         return self._route(self._owners(codes, valid), codes, valid)
 
-    def _exchange_point_boxes(self, codes, valid):
+    def _exchange_point_boxes(self, codes, valid, want_slot=True):
         import torch
-        slot, (c_parts, v_parts) = self._route_boxes(codes, valid)
+        slot, (c_parts, v_parts) = self._route_boxes(codes, valid, want_slot)
         rc = yield ("alltoall", c_parts)
         rv = yield ("alltoall", v_parts)
         return slot, [x.numel() for x in rc], torch.cat(rc), torch.cat(rv)
@@ -305,7 +305,7 @@ class PartitionedTree:
                 codes, valid = hit_boxes(scheme, min(64, int(self.table[:, 2].max()) + 1))
             else:
                 codes, valid = self.run.image_point_boxes(scheme)
-            _, _, rc, rv = yield from self._exchange_point_boxes(codes, valid)
+            _, _, rc, rv = yield from self._exchange_point_boxes(codes, valid, want_slot=False)
             self.run.set_flags_by_point_boxes(rc, rv, L.HIT)
             self.run.remove(L.HIT)
             self.run.unset_flags(L.HIT)

@@ -459,26 +459,28 @@ class ImplicitBoxTree:
                                          int(invalid_column), C.byref(h)), "transition_rows")
         return CsrMatrix(h)
 
-    def route_point_boxes(self, codes, valid, starts, ranks, world: int):
+    def route_point_boxes(self, codes, valid, starts, ranks, world: int, want_slot: bool = True):
         """The point boxes grouped by the rank that owns them (b12g_route_point_boxes):
-        (slot int64 tensor: position of box i in the output, per-rank code tensors,
-        per-rank validity tensors).  starts: unsigned depth-64 first codes of the non-empty
-        runs, ranks: their ranks (both ascending)."""
+        (slot int64 tensor: position of box i in the output, or None when not wanted,
+        per-rank code tensors, per-rank validity tensors).  starts: unsigned depth-64 first
+        codes of the non-empty runs, ranks: their ranks (both ascending)."""
         import torch
         n = codes.numel()
         out_c = torch.empty(max(n, 1), dtype=torch.int64, device=codes.device)
         out_v = torch.empty(max(n, 1), dtype=torch.uint8, device=codes.device)
-        slot = torch.empty(max(n, 1), dtype=torch.int32, device=codes.device)
+        slot = torch.empty(max(n, 1), dtype=torch.int32, device=codes.device) if want_slot else None
         st = np.ascontiguousarray(starts, dtype=np.uint64)
         rk = np.ascontiguousarray(ranks, dtype=np.uint32)
         cnt = np.zeros(world, dtype=np.uint64)
         c, v = codes.contiguous(), valid.contiguous()
         self._ready(c, v)
         check(lib().b12g_route_point_boxes(self._h, c.data_ptr(), v.data_ptr(), n, st.ctypes.data, rk.ctypes.data,
-                                           len(st), world, out_c.data_ptr(), out_v.data_ptr(), slot.data_ptr(),
-                                           cnt.ctypes.data), "route_point_boxes")
+                                           len(st), world, out_c.data_ptr(), out_v.data_ptr(),
+                                           slot.data_ptr() if slot is not None else None, cnt.ctypes.data),
+              "route_point_boxes")
         sizes = [int(x) for x in cnt]
-        return slot[:n].to(torch.int64), list(out_c[:n].split(sizes)), list(out_v[:n].split(sizes))
+        return (slot[:n].to(torch.int64) if slot is not None else None, list(out_c[:n].split(sizes)),
+                list(out_v[:n].split(sizes)))
 
     def leaf_at(self, index: int):
         """(code, depth, flags) of leaf `index` in tree order."""
