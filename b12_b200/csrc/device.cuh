@@ -785,8 +785,7 @@ struct CoupledDuffingMap {
   static __device__ __forceinline__ void apply(const MapParams& m, const double* x, double* res)
   {
     double q0 = x[0], q1 = x[1], p0 = x[2], p1 = x[3];
-#pragma unroll 2
-    for (uint32_t s = 0; s < m.steps; ++s) {
+    auto step = [&]() {
       q0 = __dadd_rn(q0, __dmul_rn(__dmul_rn(0.5, p0), m.h));
       q1 = __dadd_rn(q1, __dmul_rn(__dmul_rn(0.5, p1), m.h));
       const double f0 = __dsub_rn(__dsub_rn(q0, __dmul_rn(__dmul_rn(q0, q0), q0)),
@@ -796,6 +795,14 @@ struct CoupledDuffingMap {
       p1 = __dadd_rn(p1, __dmul_rn(f1, m.h));
       q0 = __dadd_rn(q0, __dmul_rn(__dmul_rn(0.5, p0), m.h));
       q1 = __dadd_rn(q1, __dmul_rn(__dmul_rn(0.5, p1), m.h));
+    };
+    if (m.steps == 10) {
+      // the configured step count, without the loop's own instructions
+#pragma unroll
+      for (int s = 0; s < 10; ++s) step();
+    } else {
+#pragma unroll 2
+      for (uint32_t s = 0; s < m.steps; ++s) step();
     }
     res[0] = q0; res[1] = q1; res[2] = p0; res[3] = p1;
   }

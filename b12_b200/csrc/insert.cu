@@ -540,15 +540,12 @@ __global__ void __launch_bounds__(kThreads) tile_count_kernel(const uint32_t* __
 }
 
 // tile_first: the tiles' first positions (a scan of the counts), or nullptr: summed here
-template<int D>
 __global__ void __launch_bounds__(kThreads) tile_scatter_kernel(uint32_t* __restrict__ bits, uint32_t words,
                                                                 const uint32_t* __restrict__ tile_count,
                                                                 const uint32_t* __restrict__ tile_first,
                                                                 uint64_t* __restrict__ out, int clear,
                                                                 const uint32_t* __restrict__ mark,
-                                                                uint8_t* __restrict__ flags, uint8_t f,
-                                                                double* __restrict__ centres, Domain dom,
-                                                                DepthConst dc, int depth)
+                                                                uint8_t* __restrict__ flags, uint8_t f)
 {
   __shared__ uint32_t red[kThreads / 32];
   __shared__ uint32_t wsum[kThreads / 32];
@@ -587,20 +584,8 @@ __global__ void __launch_bounds__(kThreads) tile_scatter_kernel(uint32_t* __rest
       const uint32_t mk = (mark && b) ? mark[w0 + q] : 0u;
       while (b) {
         const int bit = __ffs(b) - 1;
-        const uint64_t code = (uint64_t(w0 + q) << 5) | uint64_t(bit);
-        out[p] = code;
+        out[p] = (uint64_t(w0 + q) << 5) | uint64_t(bit);
         if (flags) flags[p] = ((mk >> bit) & 1u) ? f : uint8_t(0);
-        if (centres) {
-          double cc[kSrcStride] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-          for (int j = 0; j < D; ++j) {
-            double rr;
-            box_axis(dom, dc.ax[j], j, deinterleave<D>(code, depth, j), cc[j], rr);
-          }
-          double2* o = reinterpret_cast<double2*>(centres + size_t(kSrcStride) * p);
-          o[0] = make_double2(cc[0], cc[1]);
-          o[1] = make_double2(cc[2], cc[3]);
-        }
         ++p;
         b &= b - 1u;
       }
@@ -610,12 +595,11 @@ __global__ void __launch_bounds__(kThreads) tile_scatter_kernel(uint32_t* __rest
   }
 }
 
-// the codes of the set bits of `bits` (words u32) in increasing order into `out`, flags
-// into `flags` when not null (f where `mark` has the bit), the boxes' centres at the
-// tree's depth into `centres` when not null; clears the bitmap when asked
+// the codes of the set bits of `bits` (words u32) in increasing order into `out`, and
+// flags into `flags` when not null (f where `mark` has the bit); clears the bitmap when
+// asked
 b12g_status bitmap_codes(b12g_tree* t, uint32_t* bits, uint32_t words, uint64_t* out, bool clear,
-                         const uint32_t* mark = nullptr, uint8_t* flags = nullptr, uint8_t f = 0,
-                         double* centres = nullptr)
+                         const uint32_t* mark = nullptr, uint8_t* flags = nullptr, uint8_t f = 0)
 {
   const uint32_t tiles = (words + kWordTile - 1) / kWordTile;
   ST(t->sort_idx.ensure(2 * (size_t(tiles) + 1) + compact_tiles(uint64_t(tiles) + 1) + 8, "bitmap tile counts"));
@@ -631,18 +615,8 @@ b12g_status bitmap_codes(b12g_tree* t, uint32_t* bits, uint32_t words, uint64_t*
     CK(exclusive_scan_u32(count, first, t->ctr.p + C_TMP, first + tiles + 1, tiles, t->stream));
     count_launches(3);
   }
-  DepthConst dc;
-  fill_depth_const(t->dom, int(t->domain.dim), t->depth, dc);
-  CK(by_dim(t->domain.dim, [&](auto d) {
-    constexpr int kD = decltype(d)::value;
-    if constexpr (kD < 2) {
-      return cudaErrorInvalidValue;      // (the image kernels' maps have two or more dimensions)
-    } else {
-      tile_scatter_kernel<kD><<<g, kThreads, 0, t->stream>>>(bits, words, count, first, out, clear ? 1 : 0, mark,
-                                                            flags, f, centres, t->dom, dc, int(t->depth));
-      return cudaGetLastError();
-    }
-  }));
+  tile_scatter_kernel<<<g, kThreads, 0, t->stream>>>(bits, words, count, first, out, clear ? 1 : 0, mark, flags, f);
+  CK(cudaGetLastError());
   count_launches(1);
   return B12G_OK;
 }
@@ -693,9 +667,12 @@ b12g_status continuation_bitmap(b12g_tree* t, const b12g_scheme* s, uint8_t dept
       u = t->h_ctr[C_CAND];
       if (u > 0) {
         // the next sources: the new boxes in code order, their codes and centres
+        // (the centres by a thread per box: inside the compaction's loop over a word's
+        // bits they would serialise, 1.9 ms against 0.95 ms for the run's compactions and
+        // centres apart)
         ST(t->cand.ensure_room(u, "new boxes", 2));
-        ST(t->srcc.ensure_room(uint64_t(u) * kSrcStride, "source centres", 2));
-        ST(bitmap_codes(t, fresh, words, t->cand.p, true, nullptr, nullptr, 0, t->srcc.p));
+        ST(bitmap_codes(t, fresh, words, t->cand.p, true));
+        ST(centres_of(t, t->cand.p, nullptr, t->ctr.p + C_CAND, u));
       }
     }
     n += u;

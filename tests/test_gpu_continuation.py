@@ -98,6 +98,20 @@ def test_henon_continuation_matches_oracle():
         np.testing.assert_array_equal(x, y)
 
 
+@pytest.mark.parametrize("fma", [False, True])
+def test_lorenz_continuation_matches_oracle(fma):
+    """A three-dimensional continuation (Lorenz, inner grid 3^3) from a point near the
+    attractor: the box bitmap's 3-D code assembly and the leaves it writes."""
+    spec = dict(map="lorenz", rho=28.0, fma=fma, grid=3)
+    x0 = np.array([[-8.5, -8.5, 27.0]])
+    t = make_tree(spec)
+    counts = t.continuation_run(scheme(spec), x0, 18, max_sweeps=40)
+    o, oc = O.continuation(oracle_spec(spec), 18, x0, max_sweeps=40)
+    assert list(counts) == oc and len(oc) > 10
+    for x, y in zip(t.leaves(), o.leaves()):
+        np.testing.assert_array_equal(x, y)
+
+
 def test_continuation_depth16_matches_oracle():
     spec = dict(map="coupled_duffing", points=64, seed=0)
     t = make_tree(spec)
