@@ -341,6 +341,15 @@ __device__ double barrier_total(const double* part)
   return total;
 }
 
+// The shared-memory iteration sums an iterate's L1 norm (and the next iteration scales by
+// its inverse) every kNormalisePeriod iterations and at the last two
+constexpr uint32_t kNormalisePeriod = 8;
+
+__device__ __forceinline__ bool measure_normalises(uint32_t it, uint32_t iters)
+{
+  return it % kNormalisePeriod == kNormalisePeriod - 1 || it + 2 >= iters;
+}
+
 // The same iteration with the matrix held on chip.  Block b owns the rows of P^T whose
 // first entry lies in [b * per, (b + 1) * per) (per = nnz / blocks, rounded up), keeps
 // their entries (source, value, row) in shared memory for all iterations, and gives each
@@ -412,22 +421,24 @@ __global__ void __launch_bounds__(kMeasureThreads, 1) invariant_measure_smem_ker
     double* wc = (it & 1u) ? a.w1 : a.w0;
     double local = 0.0;
     double v[kSmemChunk];
-    // the gathers of the previous iterate go out first; the L1 norm of that iterate (the
-    // partial sums of the barrier before) is read while they are in flight, then every
-    // value is scaled by its inverse exactly as iterate_value scales it (the first
-    // iterate by 1, which leaves it unchanged)
+    // the gathers of the previous iterate go out first; when that iterate's L1 norm was
+    // summed (the partial sums of the barrier before), it is read while they are in
+    // flight and every value is scaled by its inverse exactly as iterate_value scales it;
+    // the iterates between two normalisations are left unscaled (the same direction: the
+    // scaling is linear; the last two iterates are always normalised, for the result and
+    // its change)
 #pragma unroll
     for (int q = 0; q < kSmemChunk; ++q) {
       const uint32_t k = k0 + q;
       v[q] = k < k1 ? (it == 0 ? (a.start ? __ldg(a.start + s_src[k]) : v0) : __ldcg(wp + s_src[k])) : 0.0;
     }
-    if (it > 0) {
+    if (it > 0 && measure_normalises(it - 1, a.iters)) {
       const double s_prev = barrier_total(a.partial + ((it - 1) & 1u) * gridDim.x);
       inv_prev = inv;
       inv = __ddiv_rn(1.0, s_prev);
-    }
 #pragma unroll
-    for (int q = 0; q < kSmemChunk; ++q) v[q] = __dmul_rn(v[q], inv);
+      for (int q = 0; q < kSmemChunk; ++q) v[q] = __dmul_rn(v[q], inv);
+    }
     // walk the run: a row that ends inside it is written here unless it began earlier
     uint32_t row = k0 < k1 ? s_row[k0] : 0u;
     double acc = 0.0, tail = 0.0;
@@ -463,14 +474,16 @@ __global__ void __launch_bounds__(kMeasureThreads, 1) invariant_measure_smem_ker
       __stcg(wc + row, sum);
       local = __dadd_rn(local, fabs(sum));
     }
+    if (measure_normalises(it, a.iters)) {
 #pragma unroll
-    for (int d = 16; d > 0; d >>= 1) local = __dadd_rn(local, __shfl_xor_sync(0xFFFFFFFFu, local, d));
-    if (lane == 0) red[t >> 5] = local;
-    __syncthreads();
-    if (t == 0) {
-      double sum = 0.0;
-      for (int i = 0; i < kMeasureThreads / 32; ++i) sum = __dadd_rn(sum, red[i]);
-      __stcg(a.partial + (it & 1u) * gridDim.x + blockIdx.x, sum);
+      for (int d = 16; d > 0; d >>= 1) local = __dadd_rn(local, __shfl_xor_sync(0xFFFFFFFFu, local, d));
+      if (lane == 0) red[t >> 5] = local;
+      __syncthreads();
+      if (t == 0) {
+        double sum = 0.0;
+        for (int i = 0; i < kMeasureThreads / 32; ++i) sum = __dadd_rn(sum, red[i]);
+        __stcg(a.partial + (it & 1u) * gridDim.x + blockIdx.x, sum);
+      }
     }
     if (!barrier_wait(a, it)) return;
   }

@@ -81,6 +81,9 @@ def test_route_point_boxes_with_no_boxes_and_with_boxes_outside():
 
 
 def test_measure_to_tolerance_shorter_than_a_check_equals_the_fixed_count():
+    """A tolerance run capped at k iterations is the fixed k-iteration run: the same launch
+    when k fits one check (bit for bit), two launches otherwise (each normalises its last
+    two iterates, so the vectors agree to rounding)."""
     spec = dict(map="henon", a=1.4, b=0.3, grid=4)
     t = make_tree(spec)
     sc = scheme(spec)
@@ -89,5 +92,9 @@ def test_measure_to_tolerance_shorter_than_a_check_equals_the_fixed_count():
     for k in (1, 7, 20, 33):
         v, done, _ = m.invariant_measure_tol(0.0, k, 20)
         assert done == k
-        np.testing.assert_array_equal(v, m.invariant_measure(k))
+        fixed = m.invariant_measure(k)
+        if k <= 20:
+            np.testing.assert_array_equal(v, fixed)
+        else:
+            assert np.abs(v - fixed).sum() < 1e-14
     m.close()
