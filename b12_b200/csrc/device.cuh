@@ -702,10 +702,7 @@ struct LorenzMap {
   {
     double x0_ = x0[0], x1 = x0[1], x2 = x0[2];
     double x[3] = {x0_, x1, x2}, k[3], a[3];
-    // four steps per trip: the loop's own counter and branch instructions would otherwise
-    // take a twentieth of the issue slots at 20 steps
-#pragma unroll 4
-    for (uint32_t s = 0; s < m.steps; ++s) {
+    auto step = [&]() {
       rhs(m, x, k);
 #pragma unroll
       for (int j = 0; j < 3; ++j) { res[j] = A::madd(m.h6, k[j], x[j]); a[j] = A::madd(m.h2, k[j], x[j]); }
@@ -718,6 +715,16 @@ struct LorenzMap {
       rhs(m, a, k);
 #pragma unroll
       for (int j = 0; j < 3; ++j) { res[j] = A::madd(m.h6, k[j], res[j]); x[j] = res[j]; }
+    };
+    if (m.steps == 20) {
+      // the configured step count with no loop instructions between the steps
+#pragma unroll
+      for (int s = 0; s < 20; ++s) step();
+    } else {
+      // four steps per trip: the loop's own counter and branch instructions would
+      // otherwise take a twentieth of the issue slots at 20 steps
+#pragma unroll 4
+      for (uint32_t s = 0; s < m.steps; ++s) step();
     }
   }
 };
