@@ -231,7 +231,7 @@ b12g_status select_sources(b12g_tree* t, const b12g_scheme* sc, Prepared& pr, ui
   ca.out_cap = uint32_t(t->src.n);
   ca.error = t->ctr.p + C_ERROR;
   CK(compact(ca, {t->tiles_a.p, t->tiles_b.p}, t->n, t->stream));
-  count_launches(3);
+  count_launches(compact_launches(false, t->n));
   ST(read_ctr(t, C_NSRC, 1));
   n_src = t->h_ctr[C_NSRC];
   pr.a.src = t->src.p;
@@ -586,7 +586,7 @@ b12g_status b12g_remove(b12g_tree* t, uint8_t flags, uint32_t* n_removed)
   ca.out_cap = uint32_t(std::min<size_t>(t->code[o].n, t->flags[o].n));
   ca.error = t->ctr.p + C_ERROR;
   CK(compact(ca, {t->tiles_a.p, t->tiles_b.p}, t->n, t->stream));
-  count_launches(3);
+  count_launches(compact_launches(false, t->n));
   ST(read_ctr(t, no, 1));
   ST(check_error(t, "remove"));
   const uint32_t kept = t->h_ctr[no];
@@ -1095,7 +1095,8 @@ b12g_status b12g_subdivision_run(b12g_tree* t, const b12g_scheme* sc, uint32_t s
       cudaGraphDestroy(g);
       if (e3 != cudaSuccess) { t->sub_graph = nullptr; return cuda_fail(e3, "instantiate"); }
       t->sub_key = key;
-      t->sub_graph_kernels = (use_hash ? 5ull : 4ull) * steps;
+      t->sub_graph_kernels =
+          uint64_t((use_hash ? 2 : 1) + compact_launches(true, uint32_t(std::min<uint64_t>(cap, 0xFFFFFFFFu)))) * steps;
       // the events recorded during capture belong to the graph from now on
       for (int k = 0; k < 2; ++k) {
         t->graph_prof[k].assign(t->prof_events[k].begin(), t->prof_events[k].begin() + t->prof_used[k]);

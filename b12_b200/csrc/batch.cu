@@ -750,10 +750,11 @@ cudaError_t enqueue_step(b12g_batch* b, uint32_t k, const Tuning& tu, bool with_
   return cudaGetLastError();
 }
 
-// kernels per step in the graph: hash, image, count, 3 compaction, offsets, (copy)
+// kernels per step in the graph: hash, image, count, the compaction's, offsets, (copy)
 uint64_t step_kernels(const b12g_batch* b, uint32_t k)
 {
-  return 7 + (b->active[k + 1] < b->active[k] ? 1 : 0);
+  const uint32_t capu = uint32_t(std::min<uint64_t>(b->cap, 0xFFFFFFFFu));
+  return 4 + compact_launches(true, capu) + (b->active[k + 1] < b->active[k] ? 1 : 0);
 }
 
 // time every candidate shape on the batch's own steps (first run) and keep the fastest

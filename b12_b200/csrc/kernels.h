@@ -147,6 +147,9 @@ struct CompactArgs {
   uint32_t* error;
 };
 cudaError_t compact(const CompactArgs& a, const CompactScratch& sc, uint32_t max_in, cudaStream_t s);
+// kernels one compaction launches: count and scatter, and a scan between them when the
+// elements make more than 4,096 tiles
+int compact_launches(bool children, uint32_t max_in);
 
 // exclusive scan of u32 -> u32 (out has n+1 entries; out[n] = total)
 cudaError_t exclusive_scan_u32(const uint32_t* in, uint32_t* out, const uint32_t* n, uint32_t* tile_sums,

@@ -685,7 +685,7 @@ b12g_status engine_tick(Engine* e, const std::vector<Job*>& joining)
       e->children.p, e->flags_b.p, e->new_off.p, A, e->depth_child.p + kMaxSlots, e->keep_off.p, e->fin_off.p,
       e->fin_rank.p, e->parents.p, e->flags_a.p, e->arena.p, capu,
       uint32_t(std::min<size_t>(e->arena.n, 0xFFFFFFFFu)), e->ctr.p + E_ERROR);
-  count_launches(8);
+  count_launches(5 + compact_launches(true, uint32_t(parents)));   // hash, image, counts, compaction, split
   CK(cudaGetLastError());
   // this step's counts and the counters
   CK(cudaMemcpyAsync(e->h + kHostCounts, e->cnt.p, size_t(A) * 4, cudaMemcpyDeviceToHost, e->stream));

@@ -233,6 +233,17 @@ __global__ void __launch_bounds__(kThreads) compact_count_kernel(const CompactAr
 
 // one block: exclusive scan of the tile counts; total -> *n_out.  Each thread sums a
 // contiguous group of tiles first, so the block scans once.
+// the compaction's totals once the survivors' count (carry) is known: the counts, the
+// last rank and the capacity check (one thread)
+__device__ __forceinline__ void compact_finish(const CompactArgs& a, uint32_t n, uint32_t carry)
+{
+  if (carry > a.out_cap || (a.children && 2ull * *a.n > a.hit_cap)) atomicOr(a.error, 1u);
+  if (a.out_rank) a.out_rank[n] = carry;
+  if (carry > a.out_cap) carry = a.out_cap;
+  *a.n_out = carry;
+  if (a.n_out2) *a.n_out2 = carry;
+}
+
 __global__ void compact_scan_kernel(const CompactArgs a, const uint32_t* tile_counts, uint32_t* tile_offsets)
 {
   __shared__ uint32_t red[32];
@@ -249,17 +260,14 @@ __global__ void compact_scan_kernel(const CompactArgs a, const uint32_t* tile_co
     tile_offsets[t] = off;
     off += v;
   }
-  if (threadIdx.x == 0) {
-    if (carry > a.out_cap || (a.children && 2ull * *a.n > a.hit_cap)) atomicOr(a.error, 1u);
-    if (a.out_rank) a.out_rank[n] = carry;
-    if (carry > a.out_cap) carry = a.out_cap;
-    *a.n_out = carry;
-    if (a.n_out2) *a.n_out2 = carry;
-  }
+  if (threadIdx.x == 0) compact_finish(a, n, carry);
 }
 
-// survivors of a tile staged in shared memory in order, then written out coalesced
-__global__ void __launch_bounds__(kThreads) compact_scatter_kernel(const CompactArgs a, const uint32_t* tile_offsets)
+// survivors of a tile staged in shared memory in order, then written out coalesced.
+// tile_offsets null: each block sums the counts of the tiles before its own (few tiles),
+// and the block of the last tile writes the totals the scan kernel would have
+__global__ void __launch_bounds__(kThreads) compact_scatter_kernel(const CompactArgs a, const uint32_t* tile_offsets,
+                                                                   const uint32_t* tile_counts)
 {
   __shared__ uint32_t red[32];
   __shared__ uint64_t s_code[kCompactTile];     // codes, or kept indices in out_index mode
@@ -267,12 +275,21 @@ __global__ void __launch_bounds__(kThreads) compact_scatter_kernel(const Compact
   const uint32_t n = compact_n(a);
   const uint32_t tiles = (n + kCompactTile - 1) / kCompactTile;
   const bool vec = a.vec != 0;
+  if (!tile_offsets && tiles == 0 && blockIdx.x == 0 && threadIdx.x == 0) compact_finish(a, n, 0);
   for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+    uint32_t off;
+    if (tile_offsets) {
+      off = tile_offsets[t];
+    } else {
+      uint32_t b = 0;
+      for (uint32_t q = threadIdx.x; q < t; q += kThreads) b += tile_counts[q];
+      off = block_sum(b, red);
+    }
     const uint32_t base = t * kCompactTile + threadIdx.x * kItems;
     const uint32_t m = run_mask(a, base, n, vec);
     uint32_t total;
     uint32_t at = block_exclusive(__popc(m), red, &total);
-    const uint32_t off = tile_offsets[t];
+    if (!tile_offsets && t + 1 == tiles && threadIdx.x == 0) compact_finish(a, n, off + total);
     if (a.out_rank) {
       // rank of element base + j: survivors before it
       uint32_t r[16];
@@ -459,6 +476,14 @@ cudaError_t build_leaf_hash(const uint64_t* codes, const uint32_t* n, int depth,
 }
 
 
+constexpr uint64_t kLocalScanTiles = 4096;
+
+int compact_launches(bool children, uint32_t max_in)
+{
+  const uint64_t elems = children ? 2ull * max_in : uint64_t(max_in);
+  return (elems + kCompactTile - 1) / kCompactTile <= kLocalScanTiles ? 2 : 3;
+}
+
 cudaError_t compact(const CompactArgs& args, const CompactScratch& sc, uint32_t max_in, cudaStream_t s)
 {
   CompactArgs a = args;
@@ -469,8 +494,11 @@ cudaError_t compact(const CompactArgs& args, const CompactScratch& sc, uint32_t 
   const uint64_t elems = a.children ? 2ull * max_in : uint64_t(max_in);
   const int g = grid_for(elems, kCompactTile, 4);
   compact_count_kernel<<<g, kThreads, 0, s>>>(a, sc.tile_counts);
-  compact_scan_kernel<<<1, 1024, 0, s>>>(a, sc.tile_counts, sc.tile_offsets);
-  compact_scatter_kernel<<<g, kThreads, 0, s>>>(a, sc.tile_offsets);
+  // up to kLocalScanTiles tiles every scatter block sums the counts before its tile
+  // itself (at most 16 loads a thread): no scan launch between the two
+  const bool local = (elems + kCompactTile - 1) / kCompactTile <= kLocalScanTiles;
+  if (!local) compact_scan_kernel<<<1, 1024, 0, s>>>(a, sc.tile_counts, sc.tile_offsets);
+  compact_scatter_kernel<<<g, kThreads, 0, s>>>(a, local ? nullptr : sc.tile_offsets, sc.tile_counts);
   return cudaGetLastError();
 }
 
