@@ -367,16 +367,6 @@ __device__ __forceinline__ void unpack_bits_k(uint64_t p, const int* k, uint32_t
   }
 }
 
-template<int D>
-__device__ __forceinline__ void unpack_bits(uint64_t p, int depth, uint32_t* bits)
-{
-#pragma unroll
-  for (int j = D - 1; j >= 0; --j) {
-    const int k = bisections<D>(depth, j);
-    bits[j] = uint32_t(p & ((1ull << k) - 1ull));
-    p >>= k;
-  }
-}
 
 // depth-d code of the box that contains p; false if p lies outside the domain.
 // floor(u * 2^64bits) >> (64bits - k) == floor(u * 2^k) for u >= 0 and exact scaling,
