@@ -1044,21 +1044,16 @@ b12g_status b12g_subdivision_run(b12g_tree* t, const b12g_scheme* sc, uint32_t s
       CK(cudaStreamBeginCapture(t->stream, cudaStreamCaptureModeThreadLocal));
       int cur = t->cur, ncur = t->ncur;
       cudaError_t err = cudaSuccess;
-      // the lookup table starts clean at every replay; step s's table has tag s + 1 and is
-      // built by the step before's compaction (as it writes the leaves), or by its own
-      // launch for the first step or where the compaction cannot
+      // the lookup table starts clean at every replay; step s builds with tag s + 1
       if (use_hash) err = cudaMemsetAsync(t->hash.p, 0, t->hash.n * sizeof(ulonglong2), t->stream);
-      const uint32_t capu = uint32_t(std::min<uint64_t>(cap, 0xFFFFFFFFu));
-      const bool chained = use_hash && compact_builds_table(true, capu);
       for (uint32_t s = 0; s < steps && err == cudaSuccess; ++s) {
         const int o = 1 - cur, no = 1 - ncur;
         ImageArgs a = pr.a;
         a.hash = LeafHash{nullptr, 0, 0, nullptr};
         if (use_hash) {
           a.hash = LeafHash{t->hash.p, s + 1, t->hash_log2, t->pk.p};
-          if (s == 0 || !chained)
-            err = build_leaf_hash(t->code[cur].p, t->ctr.p + ncur, int(d0) + int(s), int(t->domain.dim), a.hash,
-                                  t->ctr.p + C_ERROR, capu, t->stream);
+          err = build_leaf_hash(t->code[cur].p, t->ctr.p + ncur, int(d0) + int(s), int(t->domain.dim), a.hash,
+                                t->ctr.p + C_ERROR, uint32_t(std::min<uint64_t>(cap, 0xFFFFFFFFu)), t->stream);
           if (err != cudaSuccess) break;
         }
         a.codes = t->code[cur].p;
@@ -1089,12 +1084,7 @@ b12g_status b12g_subdivision_run(b12g_tree* t, const b12g_scheme* sc, uint32_t s
         ca.out_cap = uint32_t(std::min<size_t>(t->code[o].n, 0xFFFFFFFFu));
         ca.error = t->ctr.p + C_ERROR;
         ca.out_rank = last ? store_rank : nullptr;
-        if (chained && !last) {
-          ca.next_hash = LeafHash{t->hash.p, s + 2, t->hash_log2, t->pk.p};
-          ca.next_depth = int(d0) + int(s) + 1;
-          ca.next_dim = int(t->domain.dim);
-        }
-        err = compact(ca, {t->tiles_a.p, t->tiles_b.p}, capu, t->stream);
+        err = compact(ca, {t->tiles_a.p, t->tiles_b.p}, uint32_t(std::min<uint64_t>(cap, 0xFFFFFFFFu)), t->stream);
         cur = o;
         ncur = no;
       }
@@ -1105,10 +1095,8 @@ b12g_status b12g_subdivision_run(b12g_tree* t, const b12g_scheme* sc, uint32_t s
       cudaGraphDestroy(g);
       if (e3 != cudaSuccess) { t->sub_graph = nullptr; return cuda_fail(e3, "instantiate"); }
       t->sub_key = key;
-      // per step: the image and the compaction, and a table build where the compaction
-      // does not build the next one
-      t->sub_graph_kernels = uint64_t(1 + compact_launches(true, capu)) * steps +
-                             (use_hash ? (chained ? 1ull : uint64_t(steps)) : 0ull);
+      t->sub_graph_kernels =
+          uint64_t((use_hash ? 2 : 1) + compact_launches(true, uint32_t(std::min<uint64_t>(cap, 0xFFFFFFFFu)))) * steps;
       // the events recorded during capture belong to the graph from now on
       for (int k = 0; k < 2; ++k) {
         t->graph_prof[k].assign(t->prof_events[k].begin(), t->prof_events[k].begin() + t->prof_used[k]);

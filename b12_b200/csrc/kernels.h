@@ -145,20 +145,11 @@ struct CompactArgs {
   int vec;                   // set by compact(): the mask and rank arrays take 16-byte accesses
   uint32_t out_cap;
   uint32_t* error;
-  // optional: the survivors (codes of depth next_depth, dim next_dim) also go into this
-  // lookup table at their new indices, with their packed keys into next_hash.pk (the
-  // table the next step's image kernel reads); only where the scatter sums the tiles'
-  // counts itself (at most 4,096 tiles, compact_builds_table)
-  LeafHash next_hash;
-  int next_depth;
-  int next_dim;
 };
 cudaError_t compact(const CompactArgs& a, const CompactScratch& sc, uint32_t max_in, cudaStream_t s);
 // kernels one compaction launches: count and scatter, and a scan between them when the
 // elements make more than 4,096 tiles
 int compact_launches(bool children, uint32_t max_in);
-// whether a compaction of max_in inputs can fill CompactArgs::next_hash
-bool compact_builds_table(bool children, uint32_t max_in);
 
 // exclusive scan of u32 -> u32 (out has n+1 entries; out[n] = total)
 cudaError_t exclusive_scan_u32(const uint32_t* in, uint32_t* out, const uint32_t* n, uint32_t* tile_sums,

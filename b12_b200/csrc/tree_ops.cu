@@ -263,37 +263,6 @@ __global__ void compact_scan_kernel(const CompactArgs a, const uint32_t* tile_co
   if (threadIdx.x == 0) compact_finish(a, n, carry);
 }
 
-// one survivor of a compaction into the next step's lookup table (the insert of
-// hash_build_kernel, with the table's size from the survivors' total)
-template<int D>
-__device__ __forceinline__ void table_insert(const CompactArgs& a, uint64_t code, uint32_t index, int l,
-                                             uint64_t mask)
-{
-  uint32_t bits[D];
-#pragma unroll
-  for (int j = 0; j < D; ++j) bits[j] = deinterleave<D>(code, a.next_depth, j);
-  const uint64_t pk = pack_bits<D>(bits, a.next_depth);
-  a.next_hash.pk[index] = pk;
-  const unsigned long long key = (uint64_t(a.next_hash.tag) << 56) | pk;
-  uint64_t s = hash_slot(pk, l);
-  unsigned long long expect = 0;
-  for (uint64_t step = 0; step <= 2 * mask + 64; ++step) {
-    unsigned long long* kw = reinterpret_cast<unsigned long long*>(&a.next_hash.slots[s].x);
-    const unsigned long long cur = atomicCAS(kw, expect, key);
-    if (cur == expect) {
-      a.next_hash.slots[s].y = index;
-      return;
-    }
-    if ((cur >> 56) != a.next_hash.tag) {
-      expect = cur;
-    } else {
-      s = (s + 1) & mask;
-      expect = 0;
-    }
-  }
-  atomicOr(a.error, 1u);
-}
-
 // survivors of a tile staged in shared memory in order, then written out coalesced.
 // tile_offsets null: each block sums the counts of the tiles before its own (few tiles),
 // and the block of the last tile writes the totals the scan kernel would have
@@ -308,18 +277,13 @@ __global__ void __launch_bounds__(kThreads) compact_scatter_kernel(const Compact
   const bool vec = a.vec != 0;
   if (!tile_offsets && tiles == 0 && blockIdx.x == 0 && threadIdx.x == 0) compact_finish(a, n, 0);
   for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
-    uint32_t off, all = 0;
+    uint32_t off;
     if (tile_offsets) {
       off = tile_offsets[t];
     } else {
-      uint32_t b = 0, c = 0;
-      for (uint32_t q = threadIdx.x; q < tiles; q += kThreads) {
-        const uint32_t v = tile_counts[q];
-        if (q < t) b += v;
-        c += v;
-      }
+      uint32_t b = 0;
+      for (uint32_t q = threadIdx.x; q < t; q += kThreads) b += tile_counts[q];
       off = block_sum(b, red);
-      if (a.next_hash.slots) all = block_sum(c, red);     // the survivors' total: the table's size
     }
     const uint32_t base = t * kCompactTile + threadIdx.x * kItems;
     const uint32_t m = run_mask(a, base, n, vec);
@@ -385,10 +349,6 @@ __global__ void __launch_bounds__(kThreads) compact_scatter_kernel(const Compact
       mm &= mm - 1;
     }
     __syncthreads();
-    const bool table = a.next_hash.slots != nullptr && !tile_offsets;
-    const int l = table ? hash_log2(min(all, a.out_cap)) : 0;
-    const uint64_t lmask = (1ull << l) - 1ull;
-    if (table && threadIdx.x == 0 && l > int(a.next_hash.log2_cap)) atomicOr(a.error, 1u);
     for (uint32_t x = threadIdx.x; x < total; x += kThreads) {
       const uint32_t pos = off + x;
       if (pos >= a.out_cap) break;
@@ -397,11 +357,6 @@ __global__ void __launch_bounds__(kThreads) compact_scatter_kernel(const Compact
       } else {
         a.out_code[pos] = s_code[x];
         a.out_flags[pos] = s_flags[x];
-        if (table && l <= int(a.next_hash.log2_cap)) {
-          if (a.next_dim == 2) table_insert<2>(a, s_code[x], pos, l, lmask);
-          else if (a.next_dim == 3) table_insert<3>(a, s_code[x], pos, l, lmask);
-          else table_insert<4>(a, s_code[x], pos, l, lmask);
-        }
       }
     }
     __syncthreads();
@@ -522,12 +477,6 @@ cudaError_t build_leaf_hash(const uint64_t* codes, const uint32_t* n, int depth,
 
 
 constexpr uint64_t kLocalScanTiles = 4096;
-
-bool compact_builds_table(bool children, uint32_t max_in)
-{
-  const uint64_t elems = children ? 2ull * max_in : uint64_t(max_in);
-  return (elems + kCompactTile - 1) / kCompactTile <= kLocalScanTiles;
-}
 
 int compact_launches(bool children, uint32_t max_in)
 {
