@@ -116,6 +116,9 @@ struct MeasureArgs {
   unsigned gen_seen;         // completed barriers before the current one
   const double* start;       // first iterate (L1 norm 1), or nullptr: the uniform vector
   double* change;            // nullptr, or per block: sum of |v_k - v_(k-1)| of the last iteration
+  unsigned* epoch;           // shared-memory kernel: per block, the iterations it has completed
+  unsigned* dep_mask;        // shared-memory kernel: per block, kDepWords words: the blocks
+                             // owning the sources its rows gather
 };
 
 // Grid barrier that also reduces: every block has written its partial sum; the last
@@ -304,13 +307,13 @@ __global__ void __launch_bounds__(kMeasureThreads) invariant_measure_kernel(Meas
 // start in between: the wait (every block publishes its partial sum and arrives with
 // release semantics, then polls with acquire loads, bounded) and the total (every block
 // adds all partials itself in one fixed order - lane-strided, then a fixed shuffle tree -
-// so no block waits for a last arriver to publish it).
+// so no block waits for a last arriver to publish it).  A block whose wait gives up sets
+// error bit 1 and returns; the others then give up at their next wait, bounded as well.
 __device__ bool barrier_wait(const MeasureArgs& a, uint32_t round)
 {
-  __shared__ int ok;
   __syncthreads();
+  bool ok = true;
   if (threadIdx.x == 0) {
-    ok = 1;
     asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(a.bar_count) : "memory");
     const unsigned target = (round + 1u) * gridDim.x;
     unsigned long long polls = 0;
@@ -318,11 +321,58 @@ __device__ bool barrier_wait(const MeasureArgs& a, uint32_t round)
     for (;;) {
       asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(seen) : "l"(a.bar_count) : "memory");
       if (seen >= target) break;
-      if (++polls > kBarrierPolls) { atomicOr(a.error, 2u); ok = 0; break; }
+      if (++polls > kBarrierPolls) { atomicOr(a.error, 2u); ok = false; break; }
     }
   }
+  return __syncthreads_and(ok);
+}
+
+// Point-to-point waits between barriers.  A block that has written its rows of an iterate
+// publishes the count of iterations it has completed (release); before its next
+// iteration a block waits (acquire, bounded) only for the blocks whose rows it gathers -
+// their rows of the previous iterate must be written - and for the blocks that gather its
+// rows - they must have read the previous iterate before it is overwritten (two buffers).
+constexpr int kDepWords = 8;   // blocks the dependency masks can name: 256
+constexpr uint32_t kEpochStride = 32;  // u32 words between two blocks' epochs: a 128-byte line each
+
+__device__ __forceinline__ void epoch_publish(const MeasureArgs& a, unsigned done)
+{
   __syncthreads();
-  return ok && !(*(volatile unsigned*)a.error & 2u);
+  if (threadIdx.x == 0)
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(a.epoch + blockIdx.x * kEpochStride), "r"(done)
+                 : "memory");
+}
+
+// thread j waits for block j when `waits` (j < gridDim.x, j named by this block's masks)
+__device__ __forceinline__ bool epoch_wait(const MeasureArgs& a, bool waits, unsigned done)
+{
+  bool ok = true;
+  if (waits) {
+    unsigned long long polls = 0;
+    unsigned seen;
+    for (;;) {
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];"
+                   : "=r"(seen)
+                   : "l"(a.epoch + threadIdx.x * kEpochStride)
+                   : "memory");
+      if (seen >= done) break;
+      if (++polls > kBarrierPolls) { atomicOr(a.error, 2u); ok = false; break; }
+    }
+  }
+  return __syncthreads_and(ok);
+}
+
+// the block owning row s: the last j < nb with bnd[j] <= s (bnd ascending, bnd[0] = 0;
+// block j owns the rows [bnd[j], bnd[j + 1]))
+__device__ __forceinline__ uint32_t owner_block(const uint32_t* bnd, uint32_t nb, uint32_t s)
+{
+  uint32_t lo = 0, len = nb;
+  while (len > 0) {
+    const uint32_t half = len >> 1;
+    if (bnd[lo + half] <= s) { lo += half + 1; len -= half + 1; }
+    else len = half;
+  }
+  return lo - 1;
 }
 
 __device__ double barrier_total(const double* part)
@@ -356,7 +406,9 @@ __device__ __forceinline__ bool measure_normalises(uint32_t it, uint32_t iters)
 // thread a run of at most kSmemChunk consecutive entries: one round of gathers of the
 // previous iterate per iteration, whatever the row lengths.  A row split over several
 // threads is summed by the thread holding its first entry, adding the other threads'
-// parts in thread order, so the result does not depend on scheduling.
+// parts in thread order, so the result does not depend on scheduling.  A grid barrier
+// ends only the normalising iterations (every block needs every partial sum); the others
+// end with the block's epoch, and the next iteration waits for the blocks it depends on.
 constexpr int kSmemChunk = 13;
 constexpr uint32_t kSmemEntries = uint32_t(kSmemChunk) * kMeasureThreads;
 constexpr size_t kSmemMeasureBytes = size_t(kSmemEntries) * (8 + 4 + 4) + size_t(kMeasureThreads) * (8 + 4);
@@ -381,17 +433,17 @@ __global__ void __launch_bounds__(kMeasureThreads, 1) invariant_measure_smem_ker
   double* s_head = reinterpret_cast<double*>(s_row + kSmemEntries);
   uint32_t* s_head_end = reinterpret_cast<uint32_t*>(s_head + kMeasureThreads);
   __shared__ double red[kMeasureThreads / 32];
-  __shared__ uint32_t s_range[2];
+  __shared__ uint32_t s_bnd[32 * kDepWords + 1];
+  __shared__ uint32_t s_dep[kDepWords];
   const uint32_t n = a.n;
   const uint32_t t = threadIdx.x, lane = t & 31;
   const uint32_t per = (nnz + gridDim.x - 1) / gridDim.x;
-  if (t == 0) {
-    // lower bounds over the n + 1 row starts, at most n (a block past the last entry gets no rows)
-    s_range[0] = min(lower_bound_u32(a.tptr, n + 1, blockIdx.x * per), n);
-    s_range[1] = blockIdx.x + 1 == gridDim.x ? n : min(lower_bound_u32(a.tptr, n + 1, (blockIdx.x + 1) * per), n);
-  }
+  // every block's first row: lower bounds over the n + 1 row starts, at most n (a block
+  // past the last entry gets no rows)
+  if (t <= gridDim.x) s_bnd[t] = t == gridDim.x ? n : min(lower_bound_u32(a.tptr, n + 1, t * per), n);
+  if (t < kDepWords) s_dep[t] = 0u;
   __syncthreads();
-  const uint32_t r0 = s_range[0], r1 = max(s_range[0], s_range[1]);
+  const uint32_t r0 = s_bnd[blockIdx.x], r1 = max(r0, s_bnd[blockIdx.x + 1]);
   const uint32_t e0 = __ldg(a.tptr + r0), e1 = __ldg(a.tptr + r1);
   uint32_t nloc = e1 - e0;
   if (nloc > kSmemEntries) {
@@ -414,13 +466,39 @@ __global__ void __launch_bounds__(kMeasureThreads, 1) invariant_measure_smem_ker
   const uint32_t k0 = min(t * chunk, nloc), k1 = min(k0 + chunk, nloc);
   const bool head_open = k0 < k1 && k0 > 0 && s_row[k0 - 1] == s_row[k0];
   const bool tail_open = k0 < k1 && k1 < nloc && s_row[k1] == s_row[k1 - 1];
+  // the blocks owning this block's sources, published for the blocks whose rows they are
+  {
+    uint32_t m[kDepWords] = {};
+    for (uint32_t k = k0; k < k1; ++k) {
+      const uint32_t o = owner_block(s_bnd, gridDim.x, s_src[k]);
+#pragma unroll
+      for (int w = 0; w < kDepWords; ++w) m[w] |= (o >> 5) == uint32_t(w) ? 1u << (o & 31u) : 0u;
+    }
+#pragma unroll
+    for (int w = 0; w < kDepWords; ++w) {
+      m[w] = __reduce_or_sync(0xFFFFFFFFu, m[w]);
+      if (lane == 0 && m[w]) atomicOr(s_dep + w, m[w]);
+    }
+  }
+  __syncthreads();
+  if (t < kDepWords) a.dep_mask[blockIdx.x * kDepWords + t] = s_dep[t];
+  if (t == 0) a.epoch[blockIdx.x * kEpochStride] = 0u;
+  uint32_t bars = 0;         // full barriers passed
+  if (!barrier_wait(a, bars++)) return;
+  const uint32_t me = blockIdx.x;
+  const bool waits = t < gridDim.x && t != me &&
+                     (((s_dep[t >> 5] >> (t & 31u)) & 1u) ||
+                      ((__ldcg(a.dep_mask + t * kDepWords + (me >> 5)) >> (me & 31u)) & 1u));
   const double v0 = __ddiv_rn(1.0, double(n));
   double inv = 1.0, inv_prev = 1.0;
+  uint32_t norms = 0;        // normalising iterations done: their partial sums alternate slots
+  bool after_barrier = true;
   for (uint32_t it = 0; it < a.iters; ++it) {
     const double* wp = (it & 1u) ? a.w0 : a.w1;
     double* wc = (it & 1u) ? a.w1 : a.w0;
     double local = 0.0;
     double v[kSmemChunk];
+    if (!after_barrier && !epoch_wait(a, waits, it)) return;
     // the gathers of the previous iterate go out first; when that iterate's L1 norm was
     // summed (the partial sums of the barrier before), it is read while they are in
     // flight and every value is scaled by its inverse exactly as iterate_value scales it;
@@ -433,7 +511,7 @@ __global__ void __launch_bounds__(kMeasureThreads, 1) invariant_measure_smem_ker
       v[q] = k < k1 ? (it == 0 ? (a.start ? __ldg(a.start + s_src[k]) : v0) : __ldcg(wp + s_src[k])) : 0.0;
     }
     if (it > 0 && measure_normalises(it - 1, a.iters)) {
-      const double s_prev = barrier_total(a.partial + ((it - 1) & 1u) * gridDim.x);
+      const double s_prev = barrier_total(a.partial + ((norms - 1u) & 1u) * gridDim.x);
       inv_prev = inv;
       inv = __ddiv_rn(1.0, s_prev);
 #pragma unroll
@@ -482,13 +560,21 @@ __global__ void __launch_bounds__(kMeasureThreads, 1) invariant_measure_smem_ker
       if (t == 0) {
         double sum = 0.0;
         for (int i = 0; i < kMeasureThreads / 32; ++i) sum = __dadd_rn(sum, red[i]);
-        __stcg(a.partial + (it & 1u) * gridDim.x + blockIdx.x, sum);
+        __stcg(a.partial + (norms & 1u) * gridDim.x + blockIdx.x, sum);
       }
+      // every block reads the partial sums at the start of the next iteration; a slot is
+      // written again only after the next barrier, which every reader passes afterwards
+      if (!barrier_wait(a, bars++)) return;
+      ++norms;
+      after_barrier = true;
+    } else {
+      epoch_publish(a, it + 1u);
+      after_barrier = false;
     }
-    if (!barrier_wait(a, it)) return;
   }
   if (a.iters) {
-    const double s_last = barrier_total(a.partial + ((a.iters - 1) & 1u) * gridDim.x);
+    // the last iteration normalises: a barrier ended it
+    const double s_last = barrier_total(a.partial + ((norms - 1u) & 1u) * gridDim.x);
     inv_prev = inv;
     inv = __ddiv_rn(1.0, s_last);
   }
@@ -604,11 +690,18 @@ cudaError_t invariant_measure(const uint32_t* tptr, const uint32_t* trows, const
   // (a row of P^T has at most kMidRow entries when there are no long rows)
   const MeasureLaunch cfg = measure_launch();
   const uint32_t blocks = uint32_t(device_sm_count());
+  // partial: 2 x blocks partial sums, 2 totals, then (as u32) the blocks' epochs, a
+  // 128-byte line each, and their dependency masks
+  const uint32_t epoch_words = blocks * kEpochStride;
+  const uint64_t smem_slots = 2ull * blocks + 2 + (epoch_words + uint64_t(kDepWords) * blocks + 1) / 2;
   if (cfg.smem_ok && mid_list && long_list && n_long == 0 && nnz > 0 &&
-      (nnz + blocks - 1) / blocks + kMidRow <= kSmemEntries && 2 * blocks + 2 <= partial_cap) {
+      (nnz + blocks - 1) / blocks + kMidRow <= kSmemEntries && blocks <= 32u * kDepWords &&
+      smem_slots <= partial_cap) {
     cudaMemsetAsync(sync_words, 0, 65 * sizeof(unsigned), s);
+    unsigned* words = reinterpret_cast<unsigned*>(partial + 2 * size_t(blocks) + 2);
     MeasureArgs a{tptr, trows, tvals, mid_list, n_mid, long_list, 0u, kShortRow, n, iters, w0, w1, partial, out,
-                  sync_words, sync_words + 32, sync_words + 64, partial + 2 * size_t(blocks), 0u, start, change};
+                  sync_words, sync_words + 32, sync_words + 64, partial + 2 * size_t(blocks), 0u, start, change,
+                  words, words + epoch_words};
     uint32_t nnz32 = uint32_t(nnz);
     void* params[] = {&a, &nnz32};
     return cudaLaunchCooperativeKernel((const void*)invariant_measure_smem_kernel, dim3(blocks),
@@ -632,7 +725,7 @@ cudaError_t invariant_measure(const uint32_t* tptr, const uint32_t* trows, const
 
 int measure_partial_slots()
 {
-  return 2 * device_sm_count() * 8;
+  return 2 * device_sm_count() * 12;
 }
 
 }  // namespace b12g
