@@ -5,7 +5,8 @@
 //                        the count -> probability division of ImplicitBoxTree.hpp:3147-3158)
 //   transpose          - CSR of P -> CSR of P^T with sources ascending in every row
 //   invariant_measure  - FP64 power iteration v <- P^T v / |P^T v|_1 in one persistent
-//                        cooperative launch with a bounded grid barrier
+//                        cooperative launch with bounded grid barriers (and, with the
+//                        matrix on chip, bounded waits between dependent blocks)
 #include <cooperative_groups.h>
 
 #include <mutex>
@@ -70,18 +71,39 @@ __global__ void transpose_fill_kernel(const uint32_t* rowptr, const uint32_t* co
   }
 }
 
-// the atomic fill leaves each transposed row in arrival order: sort it by source
+// the atomic fill leaves each transposed row in arrival order: sort it by source.  A warp
+// per row: a row of up to 32 entries is held one entry a lane, and every entry goes to its
+// rank (the entries before it in source order, ties by lane: the sources of a row are
+// distinct); a longer row is sorted by insertion by one lane.
 __global__ void transpose_sort_kernel(const uint32_t* tptr, uint32_t n_cols, uint32_t* trows, double* tvals)
 {
-  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < n_cols; c += gridDim.x * blockDim.x) {
-    const uint32_t b = tptr[c], e = tptr[c + 1];
-    for (uint32_t i = b + 1; i < e; ++i) {
-      const uint32_t r = trows[i];
-      const double v = tvals[i];
-      uint32_t j = i;
-      while (j > b && trows[j - 1] > r) { trows[j] = trows[j - 1]; tvals[j] = tvals[j - 1]; --j; }
-      trows[j] = r;
-      tvals[j] = v;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < n_cols; c += nwarps) {
+    const uint32_t b = tptr[c], e = tptr[c + 1], len = e - b;
+    if (len <= 1) continue;
+    if (len <= 32) {
+      const bool have = lane < len;
+      const uint32_t r = have ? trows[b + lane] : 0u;
+      const double v = have ? tvals[b + lane] : 0.0;
+      uint32_t rank = 0;
+      for (uint32_t j = 0; j < len; ++j) {
+        const uint32_t rj = __shfl_sync(0xFFFFFFFFu, r, int(j));
+        rank += rj < r || (rj == r && j < lane);
+      }
+      if (have) {
+        trows[b + rank] = r;
+        tvals[b + rank] = v;
+      }
+    } else if (lane == 0) {
+      for (uint32_t i = b + 1; i < e; ++i) {
+        const uint32_t r = trows[i];
+        const double v = tvals[i];
+        uint32_t j = i;
+        while (j > b && trows[j - 1] > r) { trows[j] = trows[j - 1]; tvals[j] = tvals[j - 1]; --j; }
+        trows[j] = r;
+        tvals[j] = v;
+      }
     }
   }
 }
@@ -625,7 +647,8 @@ cudaError_t transpose_csr(const uint32_t* rowptr, const uint32_t* cols, const do
   cudaMemsetAsync(work, 0, (size_t(n_cols) + 1) * sizeof(uint32_t), s);
   transpose_fill_kernel<<<grid_for(max_rows, kThreads, 8), kThreads, 0, s>>>(rowptr, cols, vals, n_rows, n_cols,
                                                                              tptr, work, trows, tvals);
-  transpose_sort_kernel<<<grid_for(n_cols, kThreads, 8), kThreads, 0, s>>>(tptr, n_cols, trows, tvals);
+  transpose_sort_kernel<<<grid_for(uint64_t(n_cols) * 32, kThreads, 8), kThreads, 0, s>>>(tptr, n_cols, trows,
+                                                                                           tvals);
   return cudaGetLastError();
 }
 
