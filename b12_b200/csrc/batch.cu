@@ -416,13 +416,25 @@ __global__ void __launch_bounds__(256) target_rows_kernel(const TargetRowArgs a)
     const uint32_t row = a.row_off[q] + (rc - r0);
     // a point outside the domain is found in a last leaf of code 0
     const bool zero_leaf = a.arena[a.row_off[q] + n_i - 1] == 0;
-#pragma unroll 1
+    // every load of the row goes out before any is used: the targets, then their ranks
+    uint32_t tg[4], lo[4], hi[4];
+#pragma unroll
     for (int u = 0; u < 4; ++u) {
       const uint32_t k = uint32_t(lane) + 32u * u;
+      tg[u] = k < P ? a.targets[size_t(j) * P + k] : kInvalidIndex;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const bool in = tg[u] < kOutsideIndex;
+      lo[u] = in ? a.rank[tg[u]] : 0u;
+      hi[u] = in ? a.rank[tg[u] + 1] : 0u;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const uint32_t k = uint32_t(lane) + 32u * u, t = tg[u];
       uint32_t key = kPadKey;
       if (k < P) {
-        const uint32_t t = a.targets[size_t(j) * P + k];
-        if (t < kOutsideIndex) key = a.rank[t + 1] != a.rank[t] ? a.rank[t] - r0 : kLostKey;
+        if (t < kOutsideIndex) key = hi[u] != lo[u] ? lo[u] - r0 : kLostKey;
         else key = (t == kOutsideIndex && zero_leaf) ? n_i - 1 : kLostKey;
       }
       s[lane + 32 * u] = key;

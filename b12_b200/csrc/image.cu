@@ -377,13 +377,25 @@ __global__ void __launch_bounds__(kThreads) stored_rows_kernel(const StoredRowAr
   for (uint32_t c = blockIdx.x * kRowWarps + w; c < a.n_children; c += gridDim.x * kRowWarps) {
     const uint32_t row = __ldg(a.rank + c);
     if (__ldg(a.rank + c + 1) == row) continue;        // removed: no row (warp-uniform)
-#pragma unroll 1
+    // every load of the row goes out before any is used: the targets, then their ranks
+    uint32_t tg[4], lo[4], hi[4];
+#pragma unroll
     for (int q = 0; q < 4; ++q) {
       const uint32_t k = uint32_t(lane) + 32u * q;
+      tg[q] = k < P ? __ldg(a.targets + size_t(c) * P + k) : kInvalidIndex;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const bool in = tg[q] < kOutsideIndex;
+      lo[q] = in ? __ldg(a.rank + tg[q]) : 0u;
+      hi[q] = in ? __ldg(a.rank + tg[q] + 1) : 0u;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t k = uint32_t(lane) + 32u * q, t = tg[q];
       uint32_t key = kPadKey;
       if (k < P) {
-        const uint32_t t = __ldg(a.targets + size_t(c) * P + k);
-        if (t < kOutsideIndex) key = __ldg(a.rank + t + 1) != __ldg(a.rank + t) ? __ldg(a.rank + t) : kLostKey;
+        if (t < kOutsideIndex) key = hi[q] != lo[q] ? lo[q] : kLostKey;
         else key = (t == kOutsideIndex && zero_leaf) ? n - 1 : kLostKey;
       }
       s[lane + 32 * q] = key;
