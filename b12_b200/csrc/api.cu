@@ -865,12 +865,14 @@ b12g_status ensure_transpose(b12g_csr* m)
     ST(m->long_pos.ensure(n + 1, "row classes"));
     ST(m->long_list.ensure(n + 1, "row classes"));
     ST(m->mid_list.ensure(n + 1, "row classes"));
+    // both classes' counts (each at long_pos[n] after its pass) gathered in two counter
+    // words and read back together: one host round trip
     uint32_t counts[2] = {0, 0};
     CK(class_rows(m->tptr.p, n, 1, m->long_flag.p, m->long_pos.p, m->mid_list.p, m->ctr.p, m->tiles.p, s));
-    CK(cudaMemcpyAsync(&counts[0], m->long_pos.p + n, 4, cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
+    CK(cudaMemcpyAsync(m->ctr.p + 4, m->long_pos.p + n, 4, cudaMemcpyDeviceToDevice, s));
     CK(class_rows(m->tptr.p, n, 2, m->long_flag.p, m->long_pos.p, m->long_list.p, m->ctr.p, m->tiles.p, s));
-    CK(cudaMemcpyAsync(&counts[1], m->long_pos.p + n, 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(m->ctr.p + 5, m->long_pos.p + n, 4, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(counts, m->ctr.p + 4, sizeof counts, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     m->n_mid = counts[0];
     m->n_long = counts[1];

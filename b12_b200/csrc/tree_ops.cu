@@ -400,20 +400,50 @@ __global__ void scan_tile_offsets_kernel(const uint32_t* n_ptr, uint32_t* tile_s
   if (threadIdx.x == 0) out[n] = carry;
 }
 
-__global__ void scan_down_kernel(const uint32_t* in, const uint32_t* n_ptr, const uint32_t* tile_offsets, uint32_t* out)
+// each thread takes 16 consecutive elements of the tile (four 16-byte loads when `vec`:
+// both arrays 16-byte aligned), so a tile costs one block scan of the threads' sums
+__global__ void scan_down_kernel(const uint32_t* in, const uint32_t* n_ptr, const uint32_t* tile_offsets, uint32_t* out,
+                                 int vec)
 {
   __shared__ uint32_t red[32];
   const uint32_t n = *n_ptr;
   const uint32_t tiles = (n + kCompactTile - 1) / kCompactTile;
   for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
-    uint32_t off = tile_offsets[t];
+    const uint32_t i0 = t * kCompactTile + threadIdx.x * kItems;
+    const bool whole = vec && i0 + kItems <= n;
+    uint32_t v[kItems];
+    if (whole) {
+#pragma unroll
+      for (int q = 0; q < kItems / 4; ++q) {
+        const uint4 x = reinterpret_cast<const uint4*>(in + i0)[q];
+        v[4 * q] = x.x;
+        v[4 * q + 1] = x.y;
+        v[4 * q + 2] = x.z;
+        v[4 * q + 3] = x.w;
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < kItems; ++k) v[k] = i0 + k < n ? in[i0 + k] : 0u;
+    }
+    uint32_t sum = 0;
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) sum += v[k];
+    uint32_t total;
+    uint32_t run = tile_offsets[t] + block_exclusive(sum, red, &total);
+#pragma unroll
     for (int k = 0; k < kItems; ++k) {
-      const uint32_t i = t * kCompactTile + k * kThreads + threadIdx.x;
-      const uint32_t v = i < n ? in[i] : 0u;
-      uint32_t total;
-      const uint32_t ex = block_exclusive(v, red, &total);
-      if (i < n) out[i] = off + ex;
-      off += total;
+      const uint32_t x = v[k];
+      v[k] = run;
+      run += x;
+    }
+    if (whole) {
+#pragma unroll
+      for (int q = 0; q < kItems / 4; ++q)
+        reinterpret_cast<uint4*>(out + i0)[q] = make_uint4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+    } else {
+#pragma unroll
+      for (int k = 0; k < kItems; ++k)
+        if (i0 + k < n) out[i0 + k] = v[k];
     }
   }
 }
@@ -508,7 +538,8 @@ cudaError_t exclusive_scan_u32(const uint32_t* in, uint32_t* out, const uint32_t
   const int g = grid_for(max_n, kCompactTile, 4);
   scan_tiles_kernel<<<g, kThreads, 0, s>>>(in, n, tile_sums);
   scan_tile_offsets_kernel<<<1, 1024, 0, s>>>(n, tile_sums, out);
-  scan_down_kernel<<<g, kThreads, 0, s>>>(in, n, tile_sums, out);
+  const int vec = ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15u) == 0;
+  scan_down_kernel<<<g, kThreads, 0, s>>>(in, n, tile_sums, out, vec);
   return cudaGetLastError();
 }
 
