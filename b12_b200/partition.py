@@ -74,11 +74,11 @@ class DeviceRun:
 
     def set_flags(self, flags: int) -> None:
         if not self.empty:
-            self.tree.set_flags(flags)
+            self.tree.set_flags(flags, count=False)
 
     def unset_flags(self, flags: int) -> None:
         if not self.empty:
-            self.tree.unset_flags(flags)
+            self.tree.unset_flags(flags, count=False)   # the count is not needed: no round trip
 
     def subdivide(self, flags: int) -> None:
         if not self.empty:

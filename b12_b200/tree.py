@@ -335,10 +335,18 @@ class ImplicitBoxTree:
         check(getattr(lib(), fn)(self._h, *args, C.byref(c)), fn)
         return c.value
 
-    def set_flags(self, flags: int, depth: int = LEAF) -> int:
+    def set_flags(self, flags: int, depth: int = LEAF, count: bool = True):
+        """Returns the leaves that changed, or None with count=False (no device read-back)."""
+        if not count:
+            check(lib().b12g_set_flags(self._h, flags, depth, None), "b12g_set_flags")
+            return None
         return self._n("b12g_set_flags", flags, depth)
 
-    def unset_flags(self, flags: int, depth: int = LEAF) -> int:
+    def unset_flags(self, flags: int, depth: int = LEAF, count: bool = True):
+        """Returns the leaves that changed, or None with count=False (no device read-back)."""
+        if not count:
+            check(lib().b12g_unset_flags(self._h, flags, depth, None), "b12g_unset_flags")
+            return None
         return self._n("b12g_unset_flags", flags, depth)
 
     def change_flags(self, to_unset: int, to_set: int, depth: int = LEAF) -> int:

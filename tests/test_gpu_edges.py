@@ -98,3 +98,31 @@ def test_measure_to_tolerance_shorter_than_a_check_equals_the_fixed_count():
         else:
             assert np.abs(v - fixed).sum() < 1e-14
     m.close()
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_flag_updates_without_a_count_change_the_same_leaves(mixed):
+    """set_flags / unset_flags with count=False (no read-back of the changed leaves) leave
+    the same flags as the counting calls, on a tree of one depth and one of mixed depths."""
+    spec = dict(map="lorenz", grid=3)
+    trees = []
+    for _ in range(2):
+        t = make_tree(spec)
+        t.subdivision_run(scheme(spec), 9)
+        if mixed:
+            t.set_flags(B.SD)
+            codes, depth, flags = t.leaves()
+            half = np.zeros_like(flags)
+            half[: len(half) // 2] = B.SD
+            t.load_leaves(codes, depth, half)
+            t.subdivide(B.SD)
+        trees.append(t)
+    a, b = trees
+    assert a.set_flags(B.HIT) > 0
+    assert b.set_flags(B.HIT, count=False) is None
+    assert a.unset_flags(B.HIT | B.SD) > 0
+    assert b.unset_flags(B.HIT | B.SD, count=False) is None
+    assert a.set_flags(B.INS) > 0
+    assert b.set_flags(B.INS, count=False) is None
+    for x, y in zip(a.leaves(), b.leaves()):
+        np.testing.assert_array_equal(x, y)
