@@ -865,18 +865,29 @@ b12g_status ensure_transpose(b12g_csr* m)
     ST(m->long_pos.ensure(n + 1, "row classes"));
     ST(m->long_list.ensure(n + 1, "row classes"));
     ST(m->mid_list.ensure(n + 1, "row classes"));
-    // both classes' counts (each at long_pos[n] after its pass) gathered in two counter
-    // words and read back together: one host round trip
-    uint32_t counts[2] = {0, 0};
-    CK(class_rows(m->tptr.p, n, 1, m->long_flag.p, m->long_pos.p, m->mid_list.p, m->ctr.p, m->tiles.p, s));
-    CK(cudaMemcpyAsync(m->ctr.p + 4, m->long_pos.p + n, 4, cudaMemcpyDeviceToDevice, s));
-    CK(class_rows(m->tptr.p, n, 2, m->long_flag.p, m->long_pos.p, m->long_list.p, m->ctr.p, m->tiles.p, s));
-    CK(cudaMemcpyAsync(m->ctr.p + 5, m->long_pos.p + n, 4, cudaMemcpyDeviceToDevice, s));
-    CK(cudaMemcpyAsync(counts, m->ctr.p + 4, sizeof counts, cudaMemcpyDeviceToHost, s));
+    CK(max_row_length(m->tptr.p, n, m->ctr.p + 6, s));
+    count_launches(7);
+    uint32_t max_row = 0;
+    CK(cudaMemcpyAsync(&max_row, m->ctr.p + 6, 4, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
-    m->n_mid = counts[0];
-    m->n_long = counts[1];
-    count_launches(16);
+    if (measure_on_chip(m->nnz, max_row, uint32_t(measure_partial_slots()))) {
+      // the power iteration keeps the matrix on chip and reads no row-class lists
+      m->n_mid = 0;
+      m->n_long = 0;
+    } else {
+      // both classes' counts (each at long_pos[n] after its pass) gathered in two counter
+      // words and read back together
+      uint32_t counts[2] = {0, 0};
+      CK(class_rows(m->tptr.p, n, 1, m->long_flag.p, m->long_pos.p, m->mid_list.p, m->ctr.p, m->tiles.p, s));
+      CK(cudaMemcpyAsync(m->ctr.p + 4, m->long_pos.p + n, 4, cudaMemcpyDeviceToDevice, s));
+      CK(class_rows(m->tptr.p, n, 2, m->long_flag.p, m->long_pos.p, m->long_list.p, m->ctr.p, m->tiles.p, s));
+      CK(cudaMemcpyAsync(m->ctr.p + 5, m->long_pos.p + n, 4, cudaMemcpyDeviceToDevice, s));
+      CK(cudaMemcpyAsync(counts, m->ctr.p + 4, sizeof counts, cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      m->n_mid = counts[0];
+      m->n_long = counts[1];
+      count_launches(10);
+    }
     m->has_transpose = true;
   }
   return B12G_OK;

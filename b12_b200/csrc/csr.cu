@@ -108,6 +108,16 @@ __global__ void transpose_sort_kernel(const uint32_t* tptr, uint32_t n_cols, uin
   }
 }
 
+// the longest row of P^T (*out must be 0 before)
+__global__ void max_row_kernel(const uint32_t* tptr, uint32_t n, uint32_t* out)
+{
+  uint32_t m = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    m = max(m, tptr[i + 1] - tptr[i]);
+  m = __reduce_max_sync(0xFFFFFFFFu, m);
+  if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
+}
+
 // ---- power iteration ----------------------------------------------------------------
 // A sense-reversal grid barrier whose waits give up after a bounded number of polls;
 // co-residency of all blocks is guaranteed by the cooperative launch.
@@ -703,6 +713,25 @@ MeasureLaunch measure_launch()
 
 }  // namespace
 
+bool measure_on_chip(uint64_t nnz, uint32_t max_row, uint32_t partial_cap)
+{
+  const MeasureLaunch cfg = measure_launch();
+  const uint32_t blocks = uint32_t(device_sm_count());
+  // partial: 2 x blocks partial sums, 2 totals, then (as u32) the blocks' epochs, a
+  // 128-byte line each, and their dependency masks
+  const uint64_t slots = 2ull * blocks + 2 + (uint64_t(blocks) * kEpochStride + uint64_t(kDepWords) * blocks + 1) / 2;
+  // a block's rows begin in its share of the entries and have at most kMidRow entries
+  return cfg.smem_ok && max_row <= kMidRow && nnz > 0 && (nnz + blocks - 1) / blocks + kMidRow <= kSmemEntries &&
+         blocks <= 32u * kDepWords && slots <= partial_cap;
+}
+
+cudaError_t max_row_length(const uint32_t* tptr, uint32_t n, uint32_t* out, cudaStream_t s)
+{
+  cudaMemsetAsync(out, 0, sizeof(uint32_t), s);
+  max_row_kernel<<<grid_for(n, kThreads, 8), kThreads, 0, s>>>(tptr, n, out);
+  return cudaGetLastError();
+}
+
 cudaError_t invariant_measure(const uint32_t* tptr, const uint32_t* trows, const double* tvals,
                               const uint32_t* mid_list, uint32_t n_mid, const uint32_t* long_list, uint32_t n_long,
                               uint32_t n, uint32_t iters, double* w0, double* w1, double* partial,
@@ -713,13 +742,8 @@ cudaError_t invariant_measure(const uint32_t* tptr, const uint32_t* trows, const
   // (a row of P^T has at most kMidRow entries when there are no long rows)
   const MeasureLaunch cfg = measure_launch();
   const uint32_t blocks = uint32_t(device_sm_count());
-  // partial: 2 x blocks partial sums, 2 totals, then (as u32) the blocks' epochs, a
-  // 128-byte line each, and their dependency masks
   const uint32_t epoch_words = blocks * kEpochStride;
-  const uint64_t smem_slots = 2ull * blocks + 2 + (epoch_words + uint64_t(kDepWords) * blocks + 1) / 2;
-  if (cfg.smem_ok && mid_list && long_list && n_long == 0 && nnz > 0 &&
-      (nnz + blocks - 1) / blocks + kMidRow <= kSmemEntries && blocks <= 32u * kDepWords &&
-      smem_slots <= partial_cap) {
+  if (mid_list && long_list && n_long == 0 && measure_on_chip(nnz, 0u, partial_cap)) {
     cudaMemsetAsync(sync_words, 0, 65 * sizeof(unsigned), s);
     unsigned* words = reinterpret_cast<unsigned*>(partial + 2 * size_t(blocks) + 2);
     MeasureArgs a{tptr, trows, tvals, mid_list, n_mid, long_list, 0u, kShortRow, n, iters, w0, w1, partial, out,

@@ -30,5 +30,10 @@ cudaError_t invariant_measure(const uint32_t* tptr, const uint32_t* trows, const
                               uint32_t partial_cap, double* out, unsigned* sync_words, cudaStream_t s,
                               uint64_t nnz = 0, const double* start = nullptr, double* change = nullptr);
 int measure_partial_slots();
+// true when invariant_measure keeps a matrix of nnz entries whose longest row of P^T has
+// max_row entries on chip (one block per SM; it then reads no row-class lists)
+bool measure_on_chip(uint64_t nnz, uint32_t max_row, uint32_t partial_cap);
+// *out = the longest row of the n rows of tptr (asynchronous)
+cudaError_t max_row_length(const uint32_t* tptr, uint32_t n, uint32_t* out, cudaStream_t s);
 
 }  // namespace b12g
