@@ -279,19 +279,24 @@ def measure_mode(args, rank, world, dist, fma: bool, peak_tflops: float):
     bi_sub, n_final = box_images_of(counts)
     box_images = bi_sub          # imaged boxes only: the matrix's rows come from stored targets
 
-    # phase breakdown of one job (host clock around the synchronous API calls)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    tree.delete_depth(0)
-    t1 = time.perf_counter()
-    tree.subdivision_run(sc, DEPTH)
-    t2 = time.perf_counter()
-    state["csr"] = tree.transition_matrix(sc, into=state["csr"])
-    t3 = time.perf_counter()
-    state["csr"].invariant_measure(MEASURE_ITERS, keep_on_device=True)
-    t4 = time.perf_counter()
-    phases = {"reset_ms": 1e3 * (t1 - t0), "subdivision_ms": 1e3 * (t2 - t1), "transition_matrix_ms": 1e3 * (t3 - t2),
-              "invariant_measure_ms": 1e3 * (t4 - t3)}
+    # phase breakdown of a job (host clock around the synchronous API calls): the median
+    # of three jobs per phase, so that one host stall does not make the breakdown
+    samples = []
+    for _ in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        tree.delete_depth(0)
+        t1 = time.perf_counter()
+        tree.subdivision_run(sc, DEPTH)
+        t2 = time.perf_counter()
+        state["csr"] = tree.transition_matrix(sc, into=state["csr"])
+        t3 = time.perf_counter()
+        state["csr"].invariant_measure(MEASURE_ITERS, keep_on_device=True)
+        t4 = time.perf_counter()
+        samples.append((t1 - t0, t2 - t1, t3 - t2, t4 - t3))
+    med = [1e3 * sorted(x[i] for x in samples)[1] for i in range(4)]
+    phases = {"reset_ms": med[0], "subdivision_ms": med[1], "transition_matrix_ms": med[2],
+              "invariant_measure_ms": med[3], "jobs": len(samples)}
 
     tree.profile(True)
     tree.profile_read(0)
