@@ -145,6 +145,8 @@ b12g_status b12g_load_leaves(b12g_tree* tree, const uint64_t* codes, const uint8
                              const uint8_t* flags, uint32_t n);
 
 /* ---- flags (ImplicitBoxTree.hpp:2684-2688, 3208-3411, 787-1058) ----------------- */
+/* n_changed may be NULL: for the leaves' own depth (B12G_LEAF_DEPTH, or a one-depth
+ * tree's depth) the update is then queued on the tree's stream without a read-back */
 /* setFlags(flags, depth): returns the number of boxes that did not have them */
 b12g_status b12g_set_flags(b12g_tree* tree, uint8_t flags, uint8_t depth, uint32_t* n_changed);
 /* unsetFlags(flags, depth): returns the number of boxes that had any of them */
