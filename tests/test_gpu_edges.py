@@ -126,3 +126,45 @@ def test_flag_updates_without_a_count_change_the_same_leaves(mixed):
     assert b.set_flags(B.INS, count=False) is None
     for x, y in zip(a.leaves(), b.leaves()):
         np.testing.assert_array_equal(x, y)
+
+
+def _write_coo_json(path, n, rows, cols, vals):
+    """A transition matrix in the reference's CooMatrix file layout (row-major entries)."""
+    def block(name, xs):
+        body = ",\n".join(f"    {x!r}" for x in xs)
+        return f'  "{name}": [\n{body}\n  ],'      # the reference's writer ends every list with a comma
+    text = "{\n" + f'  "nRows": {n},\n  "nColumns": {n},\n  "nnz": {len(vals)},\n'
+    text += block("rowIndices", rows) + "\n" + block("columnIndices", cols) + "\n" + block("values", vals)
+    with open(path, "w") as f:
+        f.write(text + "\n}")
+
+
+def test_measure_of_a_matrix_with_long_rows_matches_oracle(tmp_path):
+    """A matrix whose transpose has a row of 300 entries and one of 30 is iterated by the
+    kernel that lists its rows by length class (the matrix-on-chip kernel takes rows of
+    up to 64 entries only); its measure equals the oracle's."""
+    n = 300
+    rows, cols, vals = [], [], []
+    for i in range(n):
+        entry = {0: 0.5}
+        other = 2 + (7 * i) % (n - 2)
+        if i % 10 == 0:
+            entry[1] = 0.25
+            entry[other] = 0.25
+        else:
+            entry[other] = 0.5
+        for c in sorted(entry):
+            rows.append(i)
+            cols.append(c)
+            vals.append(entry[c])
+    path = tmp_path / "long_rows_tm.json"
+    _write_coo_json(path, n, rows, cols, vals)
+    m = B.CsrMatrix.load(str(path))
+    rowptr, c, v = m.to_host()
+    np.testing.assert_array_equal(c, np.array(cols, dtype=c.dtype))
+    np.testing.assert_array_equal(v, np.array(vals))
+    got = m.invariant_measure(200)
+    want = O.invariant_measure(rowptr, c, v, 200)
+    assert np.abs(got - want).sum() < 1e-12
+    np.testing.assert_array_equal(got, m.invariant_measure(200))
+    m.close()
